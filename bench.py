@@ -1,0 +1,351 @@
+#!/usr/bin/env python3
+"""Benchmark of the batched joint X/Z BP Monte-Carlo decoder on B200.
+
+Workload (the reference's batched Monte-Carlo configuration): the shipped [[9216,4612]]
+(3,12)-regular APM code, i.i.d. depolarizing noise p=0.04, max-iter 1000 with per-trial
+early exit, damping 0, no post-processing (--no-pp), FP32 messages.  One step decodes one
+batch of `--batch` seeded trials; trial indices never repeat across steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun each rank decodes its own trial range (weak scaling; no collective on the
+data path) and rank 0 prints one JSON line.  `--impl reference` times the reference's own
+CPU decoder (oracle/_ref/jointbp_ets built from the reference sources, one process per
+host core) on the same workload.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+PARAMS = ROOT / "joint_bp_plus_pp_b200" / "data" / "H_P768_J3_L12_dmax3_nc0-3_1-2_seed11579811919164041.txt"
+REF_BIN = ROOT / "oracle" / "_ref" / "jointbp_ets"
+N_QUBITS, EDGES = 9216, 2 * 27648
+METRIC = "trials/s at p=0.04 (FP32+learned vs plain FP64 BP+PP, same GPU, equal LER)"
+UNIT = "trials/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--batch", type=int, default=131072, help="trials per step")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16", "fp64"])
+    ap.add_argument("--p", type=float, default=0.04)
+    ap.add_argument("--max-iter", type=int, default=1000)
+    ap.add_argument("--seed", type=int, default=106)
+    ap.add_argument("--fp64-batch", type=int, default=32768, help="trials of the FP64 comparison step (0 = skip)")
+    ap.add_argument("--e2e-batch", type=int, default=65536, help="trials per end-to-end step (0 = skip)")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
+    ap.add_argument("--slots", type=int, default=0)
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- helpers
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_rate(p, max_iter, seconds, procs=None, seed0=1000):
+    """Reference CPU decoder, one process per host core, for about `seconds` (trials/s summed)."""
+    if not REF_BIN.exists():
+        return None
+    procs = procs or os.cpu_count() or 1
+    # probe the per-process rate with a short run, then size the sample to `seconds`
+    probe = _run_ref(p, max_iter, 24, seed0 - 1)
+    rate1 = probe[0] / max(probe[1], 1e-9) if probe else 30.0
+    trials = max(8, int(rate1 * seconds))
+    outs = []
+    ths = []
+    for k in range(procs):
+        th = threading.Thread(target=lambda k=k: outs.append(_run_ref(p, max_iter, trials, seed0 + k)))
+        th.start()
+        ths.append(th)
+    for th in ths:
+        th.join()
+    outs = [o for o in outs if o]
+    if not outs:
+        return None
+    rate = sum(t / e for t, e, _ in outs if e > 0)
+    iters = sum(i for _, _, i in outs)
+    return {"value": rate, "unit": UNIT, "cores": len(outs), "kind": "reference",
+            "sample": f"{len(outs)} processes x {trials} trials of jointbp_ets --simulate --p {p} --max-iter {max_iter} "
+                      f"--no-pp (distinct seeds), {iters} BP iterations in total"}
+
+
+def _run_ref(p, max_iter, trials, seed):
+    cmd = [str(REF_BIN), "--params", str(PARAMS), "--simulate", "--p", str(p), "--trials", str(trials), "--max-iter",
+           str(max_iter), "--no-pp", "--seed", str(seed), "--report-every", "0"]
+    r = subprocess.run(cmd, capture_output=True, text=True, cwd=str(PARAMS.parent))
+    m = re.search(r"trials=(\d+).*?iters=(\d+).*?elapsed_s=([0-9.]+)s", r.stdout)
+    if not m:
+        return None
+    return int(m.group(1)), float(m.group(3)), int(m.group(2))
+
+
+# ----------------------------------------------------------------------------- reference arm
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    if not REF_BIN.exists():
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU binary oracle/_ref/jointbp_ets not built"}))
+        return 0
+    per_step = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_reference_rate(args.p, args.max_iter, per_step / 4)
+    vals = []
+    last = None
+    for _ in range(args.steps):
+        last = cpu_reference_rate(args.p, args.max_iter, per_step)
+        vals.append(last["value"])
+    value = statistics.median(vals)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference mt19937_64 depolarizing noise)",
+            "impl": "reference",
+            "config": {"workload": "batched Monte Carlo, [[9216,4612]] APM code, p=0.04, max-iter 1000, --no-pp, "
+                                   "reference CPU decoder (FP64)", "p": args.p, "max_iter": args.max_iter},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": last["cores"], "kind": "reference",
+                             "sample": last["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ----------------------------------------------------------------------------- b200 arm
+
+def main():
+    args = parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    else:
+        dist = None
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    sys.path.insert(0, str(ROOT))
+    from joint_bp_plus_pp_b200 import Decoder, Options, sample_reference_errors, wilson_interval
+
+    dec = Decoder.from_params(device=local)
+    opts = Options(precision=args.precision, max_iter=args.max_iter, enable_pp=False, slots=args.slots, profile=True)
+    B = args.batch
+    stride = B * (args.warmup + args.steps + 2)
+    base = 1 + rank * stride          # distinct trial ranges per rank
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for w in range(args.warmup):
+        dec.simulate(args.seed, B, args.p, opts, first_trial=base + w * B, per_trial=False)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    barrier()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    agg = {"trials": 0, "failures": 0, "total_iters": 0, "check_ms": 0.0, "var_ms": 0.0, "kernel_launches": 0,
+           "bp_trial_iterations": 0, "profiled_iterations": 0}
+    for k in range(args.steps):
+        st, _ = dec.simulate(args.seed, B, args.p, opts, first_trial=base + (args.warmup + k) * B, per_trial=False)
+        for key in agg:
+            agg[key] += st[key]
+    ev1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        tr = torch.tensor([agg["trials"]], device=dev, dtype=torch.float64)
+        dist.all_reduce(tr)
+        total_trials = float(tr.item())
+    else:
+        total_trials = float(agg["trials"])
+    value = total_trials / (ms / 1000.0)
+
+    # dominant kernel roofline (algorithmic bytes: one read + one write of a message per edge)
+    es = {"fp32": 4, "fp16": 2, "fp64": 16}[args.precision]
+    bytes_per_trial_iter = 2 * EDGES * es          # per kernel (check or variable)
+    kname, kms = ("check", agg["check_ms"]) if agg["check_ms"] >= agg["var_ms"] else ("variable", agg["var_ms"])
+    peak, peak_kind = measured_peaks()
+    achieved = agg["bp_trial_iterations"] * bytes_per_trial_iter / (kms / 1000.0) / 1e9 if kms > 0 else None
+    launches = agg["profiled_iterations"]
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        tj = json.loads(tfile.read_text())
+        traffic = tj.get(f"{args.precision}_{kname}_bytes_per_trial_iteration")
+        if traffic is not None and launches:
+            traffic = traffic * agg["bp_trial_iterations"] / launches
+
+    # FP64 comparison (plain FP64 BP, same workload, one step)
+    fp64 = None
+    if args.fp64_batch > 0 and rank == 0:
+        o64 = Options(precision="fp64", max_iter=args.max_iter, enable_pp=False)
+        dec.simulate(args.seed, args.fp64_batch // 4, args.p, o64, first_trial=10 ** 9, per_trial=False)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        st64, _ = dec.simulate(args.seed, args.fp64_batch, args.p, o64, first_trial=base + 10 ** 8, per_trial=False)
+        b.record()
+        torch.cuda.synchronize()
+        fp64 = {"value": st64["trials"] / (a.elapsed_time(b) / 1000.0), "trials": st64["trials"],
+                "failures": st64["failures"], "avg_iter": st64["total_iters"] / max(1, st64["trials"])}
+
+    # end to end through the C ABI with host buffers (reference-sampled errors in pinned memory)
+    e2e = None
+    if args.e2e_batch > 0:
+        E = args.e2e_batch
+        host = torch.empty((E, N_QUBITS), dtype=torch.uint8, pin_memory=True).numpy()
+        host[:] = sample_reference_errors(N_QUBITS, args.seed, base + 5 * 10 ** 8, E, args.p)
+        oe = Options(precision=args.precision, max_iter=args.max_iter, enable_pp=False, slots=args.slots)
+        dec.decode_errors(host[: max(32, E // 8)], args.p, oe, want_est=False)
+        torch.cuda.synchronize()
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        nsteps = max(1, min(args.steps, 3))
+        done = 0
+        for _ in range(nsteps):
+            st, res, _ = dec.decode_errors(host, args.p, oe, want_est=False)
+            done += st["trials"]
+            agg["kernel_launches"] += st["kernel_launches"]
+        b.record()
+        torch.cuda.synchronize()
+        ems = a.elapsed_time(b)
+        if dist is not None:
+            t = torch.tensor([ems], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+            done *= world
+        e2e = {"value": done / (ems / 1000.0), "unit": UNIT, "h2d_bytes_per_step": E * N_QUBITS,
+               "d2h_bytes_per_step": E * 16, "path": "jbp_decode_errors (host errors, pinned) -> results to host"}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu = cpu_reference_rate(args.p, args.max_iter, args.cpu_seconds)
+
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    lo, hi = wilson_interval(agg["trials"], agg["failures"])
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": {"fp32": "f32", "fp16": "f16-storage/f32", "fp64": "f64"}[args.precision],
+        "data": "synthetic: Philox4x32-10 depolarizing noise keyed by (seed, trial index)",
+        "config": {"workload": "batched Monte Carlo, [[9216,4612]] APM code, p=0.04, max-iter 1000, no-pp, "
+                               f"{args.precision} messages", "p": args.p, "max_iter": args.max_iter,
+                   "trials_per_step": B, "slots": None, "l2": "message state (>= 7 GB) larger than L2",
+                   "parallelism": f"replica trial ranges x{world}"},
+        "gpu_launches": agg["kernel_launches"],
+        "roofline": {"bound": "hbm", "kernel": f"{kname} node ({args.precision})", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "bytes_per_trial_iteration": bytes_per_trial_iter,
+                     "trial_iterations": agg["bp_trial_iterations"], "launches": launches,
+                     "check_ms": agg["check_ms"], "var_ms": agg["var_ms"]},
+        "ler": {"trials": agg["trials"], "failures": agg["failures"], "ci95": [lo, hi],
+                "avg_iter": agg["total_iters"] / max(1, agg["trials"])},
+        "fp64": fp64,
+        "clocks": clk,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    if fp64:
+        line["fp32_over_fp64"] = value / fp64["value"]
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,137 @@
+/* jbp_b200.h -- C ABI of the B200 joint X/Z BP + post-processing decoder.
+ *
+ * Plain C types only.  One context per code and device; a context is not thread-safe
+ * (calls on one context must not overlap).  Every entry point returns JBP_OK (0) or an
+ * error code; jbp_last_error() gives the message of the calling thread's last failure.
+ * No entry point falls back to the CPU: a missing or failing GPU is an error.
+ *
+ * Reference interfaces replaced (file:line in NagatsukiSep/joint_BP_plus_PP):
+ *   jbp_create_*      <- cuda_bp_create            jointbp_cuda.h:46, jointbp_cuda.cu:589-642
+ *                        + code construction       jointbp_ets.cpp:162-180, 98-160, 628-648
+ *   jbp_add_ets_group <- read_ets_file / ETS load  jointbp_ets.cpp:3199-3258, 5212-5337
+ *   jbp_destroy       <- cuda_bp_destroy           jointbp_cuda.h:47, jointbp_cuda.cu:644-679
+ *   jbp_decode_*      <- cuda_bp_decode            jointbp_cuda.h:48-62, jointbp_cuda.cu:681-1104
+ *                        (batched; + post-processing and success test the reference
+ *                        runs on the CPU: jointbp_ets.cpp:5487-5730)
+ *   jbp_simulate      <- the --simulate trial loop jointbp_ets.cpp:5931-6449
+ */
+#ifndef JBP_B200_H
+#define JBP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JBP_OK 0
+#define JBP_ERR_ARG 1          /* invalid argument or size mismatch */
+#define JBP_ERR_CUDA 2         /* CUDA runtime error or no usable device */
+#define JBP_ERR_IO 3           /* file missing or malformed */
+#define JBP_ERR_UNSUPPORTED 4  /* combination not built for the GPU */
+#define JBP_ERR_TIMEOUT 5      /* device watchdog expired (see jbp_options.watchdog_ms) */
+
+#define JBP_PREC_FP64 0        /* probability-domain messages, bit-exact with the reference CPU */
+#define JBP_PREC_FP32 1        /* LLR messages in FP32 */
+#define JBP_PREC_FP16 2        /* LLR messages stored in FP16, FP32 arithmetic */
+
+#define JBP_SAMPLER_PHILOX 0   /* counter-based Philox4x32-10 keyed by (seed, trial index) */
+#define JBP_SAMPLER_MT19937 1  /* the reference stream: splitmix64 seed -> mt19937_64 per trial */
+
+typedef struct jbp_ctx jbp_ctx;
+
+typedef struct {
+    int precision;         /* JBP_PREC_* (default FP64) */
+    int max_iter;          /* >= 1 (default 50, as --max-iter) */
+    double damping;        /* 0..1 (default 0, as --damping) */
+    int flip_hist;         /* flip-history window (default 5, as --flip-hist; clamped >= 0) */
+    int enable_pp;         /* ETS / flip / OSD post-processing (default 1; 0 = --no-pp) */
+    int freeze_syn;        /* --freeze-syn */
+    int check_warmup;      /* --cuda-check-warmup (default 0) */
+    int check_interval;    /* --cuda-check-interval (default 1, clamped >= 1) */
+    int slots;             /* trials in flight; 0 = automatic */
+    int iters_per_launch;  /* BP iterations per CUDA-graph launch; 0 = automatic */
+    int watchdog_ms;       /* abort a run after this much wall time (0 = none) */
+    int profile;           /* time the check and variable kernels with CUDA events (jbp_stats) */
+} jbp_options;
+
+/* Per-trial outcome (16 bytes). */
+typedef struct {
+    int32_t iterations;    /* as the reference CPU reports: convergence iteration, else max_iter */
+    uint8_t syndrome_ok;   /* final estimate reproduces the syndrome */
+    uint8_t bp_ok;         /* plain BP converged */
+    uint8_t success;       /* syndrome_ok and residual is a stabilizer (needs the true error) */
+    uint8_t exact;         /* estimate equals the true error */
+    uint8_t stab_equiv;    /* residual in the stabilizer row space */
+    uint8_t pp_success;    /* counted in pp_success */
+    uint8_t pp_ets;        /* ETS stage produced the final estimate */
+    uint8_t pp_flip;       /* flip stage produced the final estimate */
+    uint8_t pp_osd;        /* OSD counted (reference osd_success) */
+    uint8_t ets_used_flags;/* bit0 ETS used, bit1 size 6, bit2 size 12, bit3 post-BP ETS applied */
+    uint8_t pp_in_decode;  /* post-processing succeeded inside the BP loop */
+    uint8_t reserved;
+} jbp_trial_result;
+
+/* Run counters with the reference Run Summary keys (jointbp_ets.cpp:6428-6449). */
+typedef struct {
+    long long trials, failures, bp_fail, pp_success, flip_pp_success, osd_pp_success, stab_success;
+    long long ets_used, ets_saved, ets6_used, ets6_saved, ets12_used, ets12_saved;
+    long long exact, total_iters;
+    double device_ms;          /* device time of the run (CUDA events) */
+    long long kernel_launches; /* this library's kernels launched by the run */
+    long long bp_trial_iterations; /* BP iterations summed over trials */
+    double check_ms;           /* with profile: device time of all check-node kernel launches */
+    double var_ms;             /* with profile: device time of all variable-node kernel launches */
+    long long profiled_iterations; /* with profile: BP iterations (launch pairs) timed */
+    long long slots;           /* trials in flight used by the run */
+} jbp_stats;
+
+void jbp_default_options(jbp_options *opt);
+const char *jbp_last_error(void);
+const char *jbp_version(void);
+
+int jbp_create_from_params(const char *params_path, const char *ets_dir, int device, jbp_ctx **out);
+int jbp_create_from_checks(int n, int mx, const int *x_off, const int *x_var, int mz, const int *z_off,
+                           const int *z_var, int device, jbp_ctx **out);
+int jbp_add_ets_group(jbp_ctx *ctx, int size, const char *label, const char *path_x, const char *path_z);
+void jbp_destroy(jbp_ctx *ctx);
+
+/* n, mx, mz, rank_x, rank_z, number of ETS groups loaded (any pointer may be null). */
+int jbp_code_info(jbp_ctx *ctx, int *n, int *mx, int *mz, int *rank_x, int *rank_z, int *ets_groups);
+/* Check lists (check-major, x_var has x_off[mx] entries); sizes from jbp_code_info. */
+int jbp_code_checks(jbp_ctx *ctx, int side, int *off, int *var);
+
+/* Monte Carlo: trials first_trial .. first_trial+ntrials-1 of base seed `seed` at error rate p.
+ * per_trial (host, ntrials entries) and iter_hist (host, max_iter+1 entries) may be null. */
+int jbp_simulate(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed, long long first_trial, long long ntrials,
+                 double p, int sampler, jbp_stats *stats, jbp_trial_result *per_trial, long long *iter_hist);
+
+/* Decode known errors (host buffers): err is ntrials x n bytes in {0,1,2,3}; the syndromes
+ * are computed on the device.  est_out (ntrials x n, may be null) receives the estimates. */
+int jbp_decode_errors(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *err, double p,
+                      uint8_t *est_out, jbp_trial_result *res, jbp_stats *stats);
+
+/* Decode syndromes (host buffers): sx is ntrials x mx bits (one byte each), sz ntrials x mz.
+ * success/exact/stab fields stay 0 (no true error). */
+int jbp_decode_syndromes(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *sx,
+                         const uint8_t *sz, double p, uint8_t *est_out, jbp_trial_result *res, jbp_stats *stats);
+
+/* Device-resident variants: every pointer is device memory of the context's device and
+ * the call is ordered on `stream` (a cudaStream_t, 0 = legacy default stream). */
+int jbp_decode_errors_device(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *d_err,
+                             double p, uint8_t *d_est_out, jbp_trial_result *d_res, jbp_stats *stats, void *stream);
+
+/* Errors of trials first_trial.. drawn by a device sampler (JBP_SAMPLER_*), copied to the host
+ * buffer err (ntrials x n).  The same streams jbp_simulate decodes. */
+int jbp_sample_errors(jbp_ctx *ctx, uint64_t seed, long long first_trial, long long ntrials, double p, int sampler,
+                      uint8_t *err);
+
+/* Host-side sampler of the reference stream (splitmix64 + mt19937_64 + libstdc++ uniform),
+ * for feeding reference-sampled errors: trials first_trial.. into err (ntrials x n). */
+int jbp_sample_reference_errors(int n, uint64_t seed, long long first_trial, long long ntrials, double p,
+                                uint8_t *err, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

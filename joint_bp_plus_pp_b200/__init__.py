@@ -1,0 +1,259 @@
+"""joint_bp_plus_pp_b200 -- B200-native joint X/Z BP + post-processing Monte-Carlo decoder.
+
+Python mirror of the C ABI in include/jbp_b200.h (ctypes).  The decoding runs in the
+in-tree CUDA library lib/libjbp_b200.so; importing this package never falls back to a
+CPU implementation: if the library is missing, Decoder() raises.
+
+    from joint_bp_plus_pp_b200 import Decoder, Options
+    dec = Decoder.from_params()                       # the shipped [[9216,4612]] code
+    stats, per_trial = dec.simulate(seed=106, ntrials=10000, p=0.04,
+                                    opts=Options(precision="fp32", max_iter=1000, enable_pp=False))
+"""
+import ctypes
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libjbp_b200.so"
+DATA_DIR = PKG / "data"
+DEFAULT_PARAMS = DATA_DIR / "H_P768_J3_L12_dmax3_nc0-3_1-2_seed11579811919164041.txt"
+
+PREC = {"fp64": 0, "fp32": 1, "fp16": 2}
+SAMPLER = {"philox": 0, "mt19937": 1}
+ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "I/O error", 4: "unsupported", 5: "timeout"}
+
+
+class JbpError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"jbp error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class COptions(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("max_iter", ctypes.c_int), ("damping", ctypes.c_double),
+                ("flip_hist", ctypes.c_int), ("enable_pp", ctypes.c_int), ("freeze_syn", ctypes.c_int),
+                ("check_warmup", ctypes.c_int), ("check_interval", ctypes.c_int), ("slots", ctypes.c_int),
+                ("iters_per_launch", ctypes.c_int), ("watchdog_ms", ctypes.c_int), ("profile", ctypes.c_int)]
+
+
+TRIAL_DTYPE = np.dtype([("iterations", np.int32), ("syndrome_ok", np.uint8), ("bp_ok", np.uint8),
+                        ("success", np.uint8), ("exact", np.uint8), ("stab_equiv", np.uint8),
+                        ("pp_success", np.uint8), ("pp_ets", np.uint8), ("pp_flip", np.uint8),
+                        ("pp_osd", np.uint8), ("ets_used_flags", np.uint8), ("pp_in_decode", np.uint8),
+                        ("reserved", np.uint8)])
+assert TRIAL_DTYPE.itemsize == 16
+
+STAT_FIELDS = ["trials", "failures", "bp_fail", "pp_success", "flip_pp_success", "osd_pp_success", "stab_success",
+               "ets_used", "ets_saved", "ets6_used", "ets6_saved", "ets12_used", "ets12_saved", "exact",
+               "total_iters"]
+
+
+class CStats(ctypes.Structure):
+    _fields_ = [(f, ctypes.c_longlong) for f in STAT_FIELDS] + [("device_ms", ctypes.c_double),
+                                                                ("kernel_launches", ctypes.c_longlong),
+                                                                ("bp_trial_iterations", ctypes.c_longlong),
+                                                                ("check_ms", ctypes.c_double),
+                                                                ("var_ms", ctypes.c_double),
+                                                                ("profiled_iterations", ctypes.c_longlong),
+                                                                ("slots", ctypes.c_longlong)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+@dataclass
+class Options:
+    """Decoder options with the reference CLI defaults (jointbp_ets.cpp:4841-4866)."""
+    precision: str = "fp64"
+    max_iter: int = 50
+    damping: float = 0.0
+    flip_hist: int = 5
+    enable_pp: bool = True
+    freeze_syn: bool = False
+    check_warmup: int = 0
+    check_interval: int = 1
+    slots: int = 0
+    iters_per_launch: int = 0
+    watchdog_ms: int = 0
+    profile: bool = False
+
+    def to_c(self):
+        return COptions(PREC[self.precision], self.max_iter, self.damping, self.flip_hist, int(self.enable_pp),
+                        int(self.freeze_syn), self.check_warmup, self.check_interval, self.slots,
+                        self.iters_per_launch, self.watchdog_ms, int(self.profile))
+
+
+_lib = None
+
+
+def load_library(path=None):
+    """Loads lib/libjbp_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(f"{p} not built: run `python -m joint_bp_plus_pp_b200.build`")
+    lib = ctypes.CDLL(str(p))
+    vp, i, ll, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_double
+    lib.jbp_last_error.restype = ctypes.c_char_p
+    lib.jbp_version.restype = ctypes.c_char_p
+    lib.jbp_create_from_params.argtypes = [ctypes.c_char_p, ctypes.c_char_p, i, ctypes.POINTER(vp)]
+    lib.jbp_create_from_checks.argtypes = [i, i, vp, vp, i, vp, vp, i, ctypes.POINTER(vp)]
+    lib.jbp_add_ets_group.argtypes = [vp, i, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p]
+    lib.jbp_destroy.argtypes = [vp]
+    lib.jbp_destroy.restype = None
+    lib.jbp_code_info.argtypes = [vp] + [ctypes.POINTER(i)] * 6
+    lib.jbp_code_checks.argtypes = [vp, i, vp, vp]
+    lib.jbp_simulate.argtypes = [vp, ctypes.POINTER(COptions), ctypes.c_uint64, ll, ll, d, i, ctypes.POINTER(CStats),
+                                 vp, vp]
+    lib.jbp_decode_errors.argtypes = [vp, ctypes.POINTER(COptions), ll, vp, d, vp, vp, ctypes.POINTER(CStats)]
+    lib.jbp_decode_syndromes.argtypes = [vp, ctypes.POINTER(COptions), ll, vp, vp, d, vp, vp, ctypes.POINTER(CStats)]
+    lib.jbp_decode_errors_device.argtypes = [vp, ctypes.POINTER(COptions), ll, vp, d, vp, vp, ctypes.POINTER(CStats),
+                                             vp]
+    lib.jbp_sample_errors.argtypes = [vp, ctypes.c_uint64, ll, ll, d, i, vp]
+    lib.jbp_sample_reference_errors.argtypes = [i, ctypes.c_uint64, ll, ll, d, vp, i]
+    lib.jbp_default_options.argtypes = [ctypes.POINTER(COptions)]
+    lib.jbp_default_options.restype = None
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _check(lib, rc):
+    if rc != 0:
+        raise JbpError(rc, lib.jbp_last_error().decode(errors="replace"))
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def sample_reference_errors(n, seed, first_trial, ntrials, p, threads=0):
+    """Errors of the reference stream (mt19937_64 per trial) sampled on the host."""
+    lib = load_library()
+    err = np.empty((ntrials, n), np.uint8)
+    _check(lib, lib.jbp_sample_reference_errors(n, seed, first_trial, ntrials, p, _ptr(err), threads))
+    return err
+
+
+class Decoder:
+    """One code on one GPU (the C context jbp_ctx)."""
+
+    def __init__(self, handle, lib):
+        self._h = handle
+        self._lib = lib
+        n, mx, mz, rx, rz, ng = (ctypes.c_int() for _ in range(6))
+        _check(lib, lib.jbp_code_info(handle, *(ctypes.byref(v) for v in (n, mx, mz, rx, rz, ng))))
+        self.n, self.mx, self.mz = n.value, mx.value, mz.value
+        self.rank_x, self.rank_z, self.ets_groups = rx.value, rz.value, ng.value
+
+    @classmethod
+    def from_params(cls, params=DEFAULT_PARAMS, ets_dir="default", device=0):
+        lib = load_library()
+        if ets_dir == "default":
+            ets_dir = str(Path(params).with_suffix(""))
+        h = ctypes.c_void_p()
+        _check(lib, lib.jbp_create_from_params(str(params).encode(), ets_dir.encode() if ets_dir else None, device,
+                                               ctypes.byref(h)))
+        return cls(h, lib)
+
+    @classmethod
+    def from_checks(cls, n, x_off, x_var, z_off, z_var, device=0):
+        lib = load_library()
+        arrs = [np.ascontiguousarray(a, np.int32) for a in (x_off, x_var, z_off, z_var)]
+        h = ctypes.c_void_p()
+        _check(lib, lib.jbp_create_from_checks(n, len(arrs[0]) - 1, _ptr(arrs[0]), _ptr(arrs[1]), len(arrs[2]) - 1,
+                                               _ptr(arrs[2]), _ptr(arrs[3]), device, ctypes.byref(h)))
+        return cls(h, lib)
+
+    def close(self):
+        if self._h:
+            self._lib.jbp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def checks(self, side):
+        m = self.mx if side == 0 else self.mz
+        off = np.zeros(m + 1, np.int32)
+        _check(self._lib, self._lib.jbp_code_checks(self._h, side, _ptr(off), None))
+        var = np.zeros(int(off[-1]), np.int32)
+        _check(self._lib, self._lib.jbp_code_checks(self._h, side, None, _ptr(var)))
+        return off, var
+
+    def simulate(self, seed, ntrials, p, opts=None, first_trial=1, sampler="philox", per_trial=True, hist=False):
+        opts = opts or Options()
+        st = CStats()
+        res = np.zeros(ntrials, TRIAL_DTYPE) if per_trial else None
+        h = np.zeros(opts.max_iter + 1, np.int64) if hist else None
+        co = opts.to_c()
+        _check(self._lib, self._lib.jbp_simulate(self._h, ctypes.byref(co), seed, first_trial, ntrials, p,
+                                                 SAMPLER[sampler], ctypes.byref(st), _ptr(res), _ptr(h)))
+        out = st.as_dict()
+        if hist:
+            out["hist"] = h
+        return out, res
+
+    def sample_errors(self, seed, first_trial, ntrials, p, sampler="philox"):
+        """Errors drawn by a device sampler (the streams simulate() decodes)."""
+        err = np.zeros((ntrials, self.n), np.uint8)
+        _check(self._lib, self._lib.jbp_sample_errors(self._h, seed, first_trial, ntrials, p, SAMPLER[sampler],
+                                                      _ptr(err)))
+        return err
+
+    def decode_errors(self, err, p, opts=None, want_est=True):
+        err = np.ascontiguousarray(err, np.uint8).reshape(-1, self.n)
+        opts = opts or Options()
+        t = err.shape[0]
+        est = np.zeros((t, self.n), np.uint8) if want_est else None
+        res = np.zeros(t, TRIAL_DTYPE)
+        st = CStats()
+        co = opts.to_c()
+        _check(self._lib, self._lib.jbp_decode_errors(self._h, ctypes.byref(co), t, _ptr(err), p, _ptr(est),
+                                                      _ptr(res), ctypes.byref(st)))
+        return st.as_dict(), res, est
+
+    def decode_syndromes(self, sx, sz, p, opts=None, want_est=True):
+        sx = np.ascontiguousarray(sx, np.uint8).reshape(-1, self.mx)
+        sz = np.ascontiguousarray(sz, np.uint8).reshape(-1, self.mz)
+        opts = opts or Options()
+        t = sx.shape[0]
+        est = np.zeros((t, self.n), np.uint8) if want_est else None
+        res = np.zeros(t, TRIAL_DTYPE)
+        st = CStats()
+        co = opts.to_c()
+        _check(self._lib, self._lib.jbp_decode_syndromes(self._h, ctypes.byref(co), t, _ptr(sx), _ptr(sz), p,
+                                                         _ptr(est), _ptr(res), ctypes.byref(st)))
+        return st.as_dict(), res, est
+
+    def decode_errors_device(self, d_err_ptr, ntrials, p, d_est_ptr, d_res_ptr, opts=None, stream=0):
+        """Device-resident decode: pointers are device addresses (ints), ordered on `stream`."""
+        opts = opts or Options()
+        st = CStats()
+        co = opts.to_c()
+        _check(self._lib, self._lib.jbp_decode_errors_device(self._h, ctypes.byref(co), ntrials,
+                                                             ctypes.c_void_p(d_err_ptr), p,
+                                                             ctypes.c_void_p(d_est_ptr) if d_est_ptr else None,
+                                                             ctypes.c_void_p(d_res_ptr), ctypes.byref(st),
+                                                             ctypes.c_void_p(stream)))
+        return st.as_dict()
+
+
+def wilson_interval(n, k, z=1.96):
+    """Wilson score interval (jointbp_ets.cpp:4388-4399)."""
+    if n <= 0:
+        return None
+    ph = k / n
+    z2 = z * z
+    den = 1.0 + z2 / n
+    center = (ph + z2 / (2.0 * n)) / den
+    half = z * ((ph * (1.0 - ph) + z2 / (4.0 * n)) / n) ** 0.5 / den
+    return max(0.0, center - half), min(1.0, center + half)

@@ -1,0 +1,350 @@
+// C ABI (include/jbp_b200.h) over the batched engine.
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <random>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/jbp_b200.h"
+#include "engine.hpp"
+
+struct jbp_ctx {
+    jbp::Engine engine;
+    // cached device staging for host-buffer calls
+    uint8_t *d_in = nullptr, *d_in2 = nullptr, *d_est = nullptr;
+    size_t in_bytes = 0, in2_bytes = 0, est_bytes = 0;
+    jbp_trial_result *d_res = nullptr;
+    size_t res_count = 0;
+    unsigned long long *d_hist = nullptr;
+    size_t hist_count = 0;
+    ~jbp_ctx() {
+        cudaFree(d_in);
+        cudaFree(d_in2);
+        cudaFree(d_est);
+        cudaFree(d_res);
+        cudaFree(d_hist);
+    }
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int engine_fail(const std::string &msg) {
+    if (msg.find("not available") != std::string::npos || msg.find("no GPU kernel") != std::string::npos ||
+        msg.find("need a code") != std::string::npos)
+        return fail(JBP_ERR_UNSUPPORTED, msg);
+    if (msg.find("watchdog") != std::string::npos) return fail(JBP_ERR_TIMEOUT, msg);
+    if (msg.find(':') != std::string::npos && msg.find("must") == std::string::npos) return fail(JBP_ERR_CUDA, msg);
+    return fail(JBP_ERR_ARG, msg);
+}
+
+template <typename T>
+int grow(T **p, size_t *have, size_t need) {
+    if (*have >= need && *p) return JBP_OK;
+    cudaFree(*p);
+    *p = nullptr;
+    *have = 0;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), std::max<size_t>(need, 1) * sizeof(T));
+    if (e != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(e, "cudaMalloc(staging)"));
+    *have = need;
+    return JBP_OK;
+}
+
+jbp_options normalized(const jbp_options *opt) {
+    jbp_options o;
+    jbp_default_options(&o);
+    if (opt) o = *opt;
+    if (o.flip_hist < 0) o.flip_hist = 0;
+    if (o.check_warmup < 0) o.check_warmup = 0;
+    if (o.check_interval <= 0) o.check_interval = 1;
+    return o;
+}
+
+int finish_create(jbp::CodeModel &&m, const std::string &ets_dir, int device, jbp_ctx **out) {
+    if (!ets_dir.empty()) {
+        std::string e = m.load_ets_dir(ets_dir);
+        if (!e.empty()) return fail(JBP_ERR_IO, e);
+    }
+    auto ctx = std::make_unique<jbp_ctx>();
+    std::string e = ctx->engine.init(std::move(m), device);
+    if (!e.empty()) return fail(JBP_ERR_CUDA, e);
+    *out = ctx.release();
+    return JBP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void jbp_default_options(jbp_options *o) {
+    std::memset(o, 0, sizeof(*o));
+    o->precision = JBP_PREC_FP64;
+    o->max_iter = 50;
+    o->damping = 0.0;
+    o->flip_hist = 5;
+    o->enable_pp = 1;
+    o->freeze_syn = 0;
+    o->check_warmup = 0;
+    o->check_interval = 1;
+    o->slots = 0;
+    o->iters_per_launch = 0;
+    o->watchdog_ms = 0;
+    o->profile = 0;
+}
+
+const char *jbp_last_error(void) { return g_last_error.c_str(); }
+
+const char *jbp_version(void) { return "jbp_b200 0.1 (sm_100a)"; }
+
+int jbp_create_from_params(const char *params_path, const char *ets_dir, int device, jbp_ctx **out) {
+    if (!params_path || !out) return fail(JBP_ERR_ARG, "null argument");
+    *out = nullptr;
+    jbp::CodeModel m;
+    std::string e = m.build_from_params(params_path);
+    if (!e.empty()) return fail(JBP_ERR_IO, e);
+    return finish_create(std::move(m), ets_dir ? ets_dir : "", device, out);
+}
+
+int jbp_create_from_checks(int n, int mx, const int *x_off, const int *x_var, int mz, const int *z_off,
+                           const int *z_var, int device, jbp_ctx **out) {
+    if (!out || !x_off || !z_off || n <= 0 || mx < 0 || mz < 0) return fail(JBP_ERR_ARG, "invalid code arguments");
+    *out = nullptr;
+    std::vector<int> xo(x_off, x_off + mx + 1), zo(z_off, z_off + mz + 1);
+    if (xo[mx] < 0 || zo[mz] < 0) return fail(JBP_ERR_ARG, "invalid check offsets");
+    std::vector<int> xv(x_var, x_var + xo[mx]), zv(z_var, z_var + zo[mz]);
+    jbp::CodeModel m;
+    std::string e = m.build_from_checks(n, xo, xv, zo, zv);
+    if (!e.empty()) return fail(JBP_ERR_ARG, e);
+    return finish_create(std::move(m), "", device, out);
+}
+
+int jbp_add_ets_group(jbp_ctx *ctx, int size, const char *label, const char *path_x, const char *path_z) {
+    if (!ctx) return fail(JBP_ERR_ARG, "null context");
+    auto &m = const_cast<jbp::CodeModel &>(ctx->engine.model());
+    std::string e = m.add_ets_group(size, label ? label : std::to_string(size), path_x ? path_x : "",
+                                    path_z ? path_z : "");
+    if (!e.empty()) return fail(JBP_ERR_IO, e);
+    return JBP_OK;
+}
+
+void jbp_destroy(jbp_ctx *ctx) { delete ctx; }
+
+int jbp_code_info(jbp_ctx *ctx, int *n, int *mx, int *mz, int *rank_x, int *rank_z, int *ets_groups) {
+    if (!ctx) return fail(JBP_ERR_ARG, "null context");
+    const auto &m = ctx->engine.model();
+    if (n) *n = m.n;
+    if (mx) *mx = m.side[0].m;
+    if (mz) *mz = m.side[1].m;
+    if (rank_x) *rank_x = m.basis[0].rank;
+    if (rank_z) *rank_z = m.basis[1].rank;
+    if (ets_groups) *ets_groups = static_cast<int>(m.ets.size());
+    return JBP_OK;
+}
+
+int jbp_code_checks(jbp_ctx *ctx, int side, int *off, int *var) {
+    if (!ctx || side < 0 || side > 1) return fail(JBP_ERR_ARG, "invalid argument");
+    const auto &g = ctx->engine.model().side[side];
+    if (off) std::copy(g.chk_off.begin(), g.chk_off.end(), off);
+    if (var) std::copy(g.chk_var.begin(), g.chk_var.end(), var);
+    return JBP_OK;
+}
+
+int jbp_simulate(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed, long long first_trial, long long ntrials,
+                 double p, int sampler, jbp_stats *stats, jbp_trial_result *per_trial, long long *iter_hist) {
+    if (!ctx || ntrials < 0) return fail(JBP_ERR_ARG, "invalid argument");
+    if (sampler != JBP_SAMPLER_PHILOX && sampler != JBP_SAMPLER_MT19937) return fail(JBP_ERR_ARG, "unknown sampler");
+    jbp::RunRequest rq;
+    rq.opt = normalized(opt);
+    rq.source = sampler == JBP_SAMPLER_PHILOX ? jbp::kSrcPhilox : jbp::kSrcMt19937;
+    rq.seed = seed;
+    rq.first_trial = first_trial;
+    rq.ntrials = ntrials;
+    rq.p = p;
+    cudaSetDevice(ctx->engine.device());
+    if (per_trial) {
+        if (int rc = grow(&ctx->d_res, &ctx->res_count, static_cast<size_t>(ntrials))) return rc;
+        rq.d_res_out = ctx->d_res;
+    }
+    if (iter_hist) {
+        if (rq.opt.max_iter < 1) return fail(JBP_ERR_ARG, "max_iter must be >= 1");
+        if (int rc = grow(&ctx->d_hist, &ctx->hist_count, static_cast<size_t>(rq.opt.max_iter) + 1)) return rc;
+        cudaMemset(ctx->d_hist, 0, sizeof(unsigned long long) * (rq.opt.max_iter + 1));
+        rq.d_hist = ctx->d_hist;
+    }
+    jbp_stats st;
+    std::string e = ctx->engine.run(rq, st);
+    if (!e.empty()) return engine_fail(e);
+    if (per_trial && ntrials > 0) {
+        cudaError_t ce = cudaMemcpy(per_trial, ctx->d_res, sizeof(jbp_trial_result) * ntrials, cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(ce, "copy results"));
+    }
+    if (iter_hist) {
+        std::vector<unsigned long long> h(rq.opt.max_iter + 1);
+        cudaError_t ce = cudaMemcpy(h.data(), ctx->d_hist, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(ce, "copy histogram"));
+        for (size_t i = 0; i < h.size(); ++i) iter_hist[i] = static_cast<long long>(h[i]);
+    }
+    if (stats) *stats = st;
+    return JBP_OK;
+}
+
+static int decode_host(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *err, const uint8_t *sx,
+                       const uint8_t *sz, double p, uint8_t *est_out, jbp_trial_result *res, jbp_stats *stats) {
+    if (!ctx || ntrials < 0 || !res) return fail(JBP_ERR_ARG, "invalid argument");
+    const auto &m = ctx->engine.model();
+    const long long n = m.n, mx = m.side[0].m, mz = m.side[1].m;
+    cudaSetDevice(ctx->engine.device());
+    jbp_stats total;
+    std::memset(&total, 0, sizeof(total));
+    // chunks bound the staging memory; each chunk is one engine run
+    const long long chunk = std::max<long long>(1, std::min<long long>(ntrials, 1LL << 17));
+    for (long long base = 0; base < ntrials; base += chunk) {
+        const long long cnt = std::min(chunk, ntrials - base);
+        jbp::RunRequest rq;
+        rq.opt = normalized(opt);
+        rq.p = p;
+        rq.first_trial = 0;
+        rq.ntrials = cnt;
+        cudaError_t ce;
+        if (err) {
+            if (int rc = grow(&ctx->d_in, &ctx->in_bytes, static_cast<size_t>(cnt * n))) return rc;
+            ce = cudaMemcpy(ctx->d_in, err + base * n, static_cast<size_t>(cnt * n), cudaMemcpyHostToDevice);
+            if (ce != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(ce, "copy errors"));
+            rq.source = jbp::kSrcErrors;
+            rq.d_err = ctx->d_in;
+        } else {
+            if (!sx || !sz) return fail(JBP_ERR_ARG, "null syndrome");
+            if (int rc = grow(&ctx->d_in, &ctx->in_bytes, static_cast<size_t>(cnt * mx))) return rc;
+            if (int rc = grow(&ctx->d_in2, &ctx->in2_bytes, static_cast<size_t>(cnt * mz))) return rc;
+            ce = cudaMemcpy(ctx->d_in, sx + base * mx, static_cast<size_t>(cnt * mx), cudaMemcpyHostToDevice);
+            if (ce == cudaSuccess)
+                ce = cudaMemcpy(ctx->d_in2, sz + base * mz, static_cast<size_t>(cnt * mz), cudaMemcpyHostToDevice);
+            if (ce != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(ce, "copy syndromes"));
+            rq.source = jbp::kSrcSyndromes;
+            rq.d_sx = ctx->d_in;
+            rq.d_sz = ctx->d_in2;
+        }
+        if (est_out) {
+            if (int rc = grow(&ctx->d_est, &ctx->est_bytes, static_cast<size_t>(cnt * n))) return rc;
+            rq.d_est_out = ctx->d_est;
+        }
+        if (int rc = grow(&ctx->d_res, &ctx->res_count, static_cast<size_t>(cnt))) return rc;
+        rq.d_res_out = ctx->d_res;
+        jbp_stats st;
+        std::string e = ctx->engine.run(rq, st);
+        if (!e.empty()) return engine_fail(e);
+        ce = cudaMemcpy(res + base, ctx->d_res, sizeof(jbp_trial_result) * cnt, cudaMemcpyDeviceToHost);
+        if (ce == cudaSuccess && est_out)
+            ce = cudaMemcpy(est_out + base * n, ctx->d_est, static_cast<size_t>(cnt * n), cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(ce, "copy results"));
+        long long *a = &total.trials;
+        const long long *b = &st.trials;
+        for (int i = 0; i < 15; ++i) a[i] += b[i];
+        total.device_ms += st.device_ms;
+        total.kernel_launches += st.kernel_launches;
+        total.bp_trial_iterations += st.bp_trial_iterations;
+        total.check_ms += st.check_ms;
+        total.var_ms += st.var_ms;
+        total.profiled_iterations += st.profiled_iterations;
+        total.slots = std::max(total.slots, st.slots);
+    }
+    if (stats) *stats = total;
+    return JBP_OK;
+}
+
+int jbp_decode_errors(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *err, double p,
+                      uint8_t *est_out, jbp_trial_result *res, jbp_stats *stats) {
+    if (!err) return fail(JBP_ERR_ARG, "null error buffer");
+    if (ctx) {
+        const long long n = ctx->engine.model().n;
+        for (long long i = 0; i < ntrials * n; ++i)
+            if (err[i] > 3) return fail(JBP_ERR_ARG, "error vector has invalid value");
+    }
+    return decode_host(ctx, opt, ntrials, err, nullptr, nullptr, p, est_out, res, stats);
+}
+
+int jbp_decode_syndromes(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *sx,
+                         const uint8_t *sz, double p, uint8_t *est_out, jbp_trial_result *res, jbp_stats *stats) {
+    return decode_host(ctx, opt, ntrials, nullptr, sx, sz, p, est_out, res, stats);
+}
+
+int jbp_decode_errors_device(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *d_err, double p,
+                             uint8_t *d_est_out, jbp_trial_result *d_res, jbp_stats *stats, void *stream) {
+    if (!ctx || !d_err || !d_res || ntrials < 0) return fail(JBP_ERR_ARG, "invalid argument");
+    jbp::RunRequest rq;
+    rq.opt = normalized(opt);
+    rq.source = jbp::kSrcErrors;
+    rq.first_trial = 0;
+    rq.ntrials = ntrials;
+    rq.p = p;
+    rq.d_err = d_err;
+    rq.d_est_out = d_est_out;
+    rq.d_res_out = d_res;
+    rq.stream = static_cast<cudaStream_t>(stream);
+    cudaSetDevice(ctx->engine.device());
+    jbp_stats st;
+    std::string e = ctx->engine.run(rq, st);
+    if (!e.empty()) return engine_fail(e);
+    if (stats) *stats = st;
+    return JBP_OK;
+}
+
+int jbp_sample_errors(jbp_ctx *ctx, uint64_t seed, long long first_trial, long long ntrials, double p, int sampler,
+                      uint8_t *err) {
+    if (!ctx || !err || ntrials < 0) return fail(JBP_ERR_ARG, "invalid argument");
+    if (sampler != JBP_SAMPLER_PHILOX && sampler != JBP_SAMPLER_MT19937) return fail(JBP_ERR_ARG, "unknown sampler");
+    const long long n = ctx->engine.model().n;
+    cudaSetDevice(ctx->engine.device());
+    if (int rc = grow(&ctx->d_in, &ctx->in_bytes, static_cast<size_t>(ntrials * n))) return rc;
+    std::string e = ctx->engine.sample_errors(seed, first_trial, ntrials, p,
+                                              sampler == JBP_SAMPLER_PHILOX ? jbp::kSrcPhilox : jbp::kSrcMt19937,
+                                              ctx->d_in);
+    if (!e.empty()) return engine_fail(e);
+    cudaError_t ce = cudaMemcpy(err, ctx->d_in, static_cast<size_t>(ntrials * n), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(ce, "copy errors"));
+    return JBP_OK;
+}
+
+// The reference sampler, run on the host with libstdc++'s mt19937_64 and
+// uniform_real_distribution<double> (jointbp_ets.cpp:4401-4411, 5931-5946).
+int jbp_sample_reference_errors(int n, uint64_t seed, long long first_trial, long long ntrials, double p,
+                                uint8_t *err, int threads) {
+    if (n <= 0 || ntrials < 0 || !err) return fail(JBP_ERR_ARG, "invalid argument");
+    if (threads <= 0) threads = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+    threads = static_cast<int>(std::min<long long>(threads, std::max<long long>(ntrials, 1)));
+    auto work = [&](long long lo, long long hi) {
+        std::uniform_real_distribution<double> dist(0.0, 1.0);
+        for (long long t = lo; t < hi; ++t) {
+            const unsigned long long idx = static_cast<unsigned long long>(first_trial + t);
+            std::mt19937_64 rng(jbp::splitmix64(seed ^ (idx * 0x9e3779b97f4a7c15ull)));
+            uint8_t *e = err + t * n;
+            for (int i = 0; i < n; ++i) {
+                const double u = dist(rng);
+                if (u < 1.0 - p) {
+                    e[i] = 0;
+                } else {
+                    const double v = (u - (1.0 - p)) / p;
+                    e[i] = v < 1.0 / 3.0 ? 1 : (v < 2.0 / 3.0 ? 2 : 3);
+                }
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    const long long per = (ntrials + threads - 1) / threads;
+    for (int k = 0; k < threads; ++k) {
+        const long long lo = k * per, hi = std::min(ntrials, lo + per);
+        if (lo < hi) pool.emplace_back(work, lo, hi);
+    }
+    for (auto &t : pool) t.join();
+    return JBP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,439 @@
+// Batched joint BP engine: device buffers, per-iteration CUDA graph and the run loop.
+#include "engine.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <sstream>
+
+#include "kernels_bp.cuh"
+#include "kernels_slots.cuh"
+
+namespace jbp {
+
+std::string cuda_err(cudaError_t e, const char *what) {
+    std::ostringstream os;
+    os << what << ": " << cudaGetErrorString(e);
+    return os.str();
+}
+
+#define JBP_CUDA_TRY(expr, what)                                  \
+    do {                                                          \
+        cudaError_t e_ = (expr);                                  \
+        if (e_ != cudaSuccess) return cuda_err(e_, what);         \
+    } while (0)
+
+namespace {
+
+template <typename T>
+std::string dev_upload(std::vector<void *> &allocs, const std::vector<T> &h, T **out) {
+    *out = nullptr;
+    size_t bytes = sizeof(T) * std::max<size_t>(h.size(), 1);
+    JBP_CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(out), bytes), "cudaMalloc(code)");
+    allocs.push_back(*out);
+    if (!h.empty()) JBP_CUDA_TRY(cudaMemcpy(*out, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice), "upload code");
+    return "";
+}
+
+// ---------------------------------------------------------------- kernel selection
+
+using CheckFn = void (*)(DevCode, DevRun, DevMsgs);
+using VarF64Fn = void (*)(DevCode, DevRun, DevMsgs, double);
+using VarLlrFn = void (*)(DevCode, DevRun, DevMsgs, float);
+
+struct KernelSet {
+    CheckFn check = nullptr;
+    VarF64Fn var64 = nullptr;
+    VarLlrFn varllr = nullptr;
+};
+
+template <int DC, int DV>
+KernelSet kernels_for(int precision, bool damp) {
+    KernelSet k;
+    if (precision == JBP_PREC_FP64) {
+        k.check = damp ? k_check_f64<DC, true> : k_check_f64<DC, false>;
+        k.var64 = damp ? k_var_f64<DV, true> : k_var_f64<DV, false>;
+    } else if (precision == JBP_PREC_FP32) {
+        k.check = k_check_llr<float, DC>;
+        k.varllr = damp ? k_var_llr<float, DV, true> : k_var_llr<float, DV, false>;
+    } else {
+        k.check = k_check_llr<__half, DC>;
+        k.varllr = damp ? k_var_llr<__half, DV, true> : k_var_llr<__half, DV, false>;
+    }
+    return k;
+}
+
+// Regular (dc, dv) pairs built for the GPU.
+bool select_kernels(int dc, int dv, int precision, bool damp, KernelSet &k) {
+#define JBP_CASE(DC, DV) \
+    if (dc == DC && dv == DV) { k = kernels_for<DC, DV>(precision, damp); return true; }
+    JBP_CASE(12, 3)
+    JBP_CASE(8, 3)
+    JBP_CASE(6, 3)
+    JBP_CASE(4, 2)
+    JBP_CASE(6, 2)
+    JBP_CASE(10, 3)
+    JBP_CASE(12, 4)
+    JBP_CASE(16, 4)
+#undef JBP_CASE
+    return false;
+}
+
+size_t msg_elem_bytes(int precision) {
+    return precision == JBP_PREC_FP64 ? sizeof(double2) : (precision == JBP_PREC_FP32 ? sizeof(float) : sizeof(__half));
+}
+
+}  // namespace
+
+Engine::~Engine() {
+    free_buffers();
+    for (void *p : code_allocs_) cudaFree(p);
+}
+
+std::string Engine::init(CodeModel model, int device) {
+    model_ = std::move(model);
+    device_ = device;
+    int ndev = 0;
+    JBP_CUDA_TRY(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+    if (device < 0 || device >= ndev) return "CUDA device " + std::to_string(device) + " not available";
+    JBP_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+    JBP_CUDA_TRY(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device), "device attributes");
+    dcode_.n = model_.n;
+    dcode_.words = (model_.n + 63) / 64;
+    for (int s = 0; s < 2; ++s) {
+        const SideGraph &g = model_.side[s];
+        DevSide &d = dcode_.s[s];
+        d.m = g.m;
+        d.edges = g.edges;
+        d.dc = g.dc_max;
+        d.dv = g.dv_max;
+        int *p = nullptr;
+        std::string e = dev_upload(code_allocs_, g.chk_var, &p);
+        if (!e.empty()) return e;
+        d.chk_var = p;
+        e = dev_upload(code_allocs_, g.var_edge, &p);
+        if (!e.empty()) return e;
+        d.var_edge = p;
+        uint64_t *rows = nullptr;
+        e = dev_upload(code_allocs_, model_.basis[s].rows, &rows);
+        if (!e.empty()) return e;
+        dcode_.basis_rows[s] = rows;
+        e = dev_upload(code_allocs_, model_.basis[s].pivot_row, &p);
+        if (!e.empty()) return e;
+        dcode_.pivot_row[s] = p;
+    }
+    return "";
+}
+
+void Engine::free_buffers() {
+    for (void *&p : buf_.msg) { cudaFree(p); p = nullptr; }
+    cudaFree(buf_.trial); cudaFree(buf_.iter); cudaFree(buf_.flags); cudaFree(buf_.unsat);
+    cudaFree(buf_.prior); cudaFree(buf_.lprior); cudaFree(buf_.err); cudaFree(buf_.est); cudaFree(buf_.syn);
+    cudaFree(buf_.res_iters); cudaFree(buf_.res_flags); cudaFree(buf_.lists); cudaFree(buf_.counts);
+    cudaFree(buf_.cnt);
+    if (buf_.h_done) cudaFreeHost(buf_.h_done);
+    buf_ = Buffers{};
+}
+
+std::string Engine::ensure_buffers(int S, int precision, bool damp) {
+    if (buf_.S == S && buf_.precision == precision && buf_.damp == damp) return "";
+    free_buffers();
+    const int n = model_.n, M = model_.side[0].m + model_.side[1].m;
+    const size_t es = msg_elem_bytes(precision);
+    for (int s = 0; s < 2; ++s) {
+        const size_t bytes = es * static_cast<size_t>(model_.side[s].edges) * S;
+        JBP_CUDA_TRY(cudaMalloc(&buf_.msg[s], bytes), "cudaMalloc(c2v)");
+        JBP_CUDA_TRY(cudaMalloc(&buf_.msg[2 + s], bytes), "cudaMalloc(v2c)");
+        if (precision == JBP_PREC_FP64 && damp) JBP_CUDA_TRY(cudaMalloc(&buf_.msg[4 + s], bytes), "cudaMalloc(v2c hi)");
+        buf_.msg_bytes += bytes * (precision == JBP_PREC_FP64 && damp ? 3 : 2);
+    }
+    JBP_CUDA_TRY(cudaMalloc(&buf_.trial, sizeof(long long) * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.iter, sizeof(int) * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.flags, sizeof(int) * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.unsat, sizeof(int) * 2 * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.prior, sizeof(double) * 4 * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.lprior, sizeof(float) * 8 * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.err, static_cast<size_t>(n) * S), "cudaMalloc(err)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.est, static_cast<size_t>(n) * S), "cudaMalloc(est)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.syn, static_cast<size_t>(M) * S), "cudaMalloc(syn)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.res_iters, sizeof(int) * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.res_flags, sizeof(int) * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.lists, sizeof(int) * (3 * S)), "cudaMalloc(lists)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.counts, sizeof(int) * 4), "cudaMalloc(lists)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.cnt, sizeof(DevCounters)), "cudaMalloc(counters)");
+    JBP_CUDA_TRY(cudaMallocHost(&buf_.h_done, sizeof(unsigned long long) * 2), "cudaMallocHost");
+    buf_.S = S;
+    buf_.precision = precision;
+    buf_.damp = damp;
+    return "";
+}
+
+int Engine::choose_slots(const jbp_options &opt, long long ntrials) const {
+    long long S = opt.slots;
+    if (S <= 0) S = opt.precision == JBP_PREC_FP64 ? 8192 : 16384;
+    long long need = (std::max<long long>(ntrials, 1) + kGroup - 1) / kGroup * kGroup;
+    S = std::min(S, need);
+    S = (S + kGroup - 1) / kGroup * kGroup;
+    return static_cast<int>(std::max<long long>(S, kGroup));
+}
+
+std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
+    std::memset(&stats, 0, sizeof(stats));
+    const jbp_options &o = rq.opt;
+    if (rq.ntrials <= 0) return "";
+    if (o.max_iter < 1) return "max_iter must be >= 1";
+    if (o.precision < JBP_PREC_FP64 || o.precision > JBP_PREC_FP16) return "unknown precision";
+    if (!(rq.p > 0.0 && rq.p < 1.0)) return "p must be in (0, 1)";
+    if (o.damping < 0.0 || o.damping > 1.0) return "damping must be in [0, 1]";
+    if (o.enable_pp) return "post-processing on the GPU is not available in this build (use enable_pp = 0)";
+    if (o.freeze_syn) return "freeze-syn is not available on the GPU in this build";
+    const SideGraph &gx = model_.side[0], &gz = model_.side[1];
+    if (!gx.regular || !gz.regular || gx.dc_max != gz.dc_max || gx.dv_max != gz.dv_max)
+        return "the GPU kernels need a code with equal regular degrees on both sides";
+    const bool damp = o.damping > 0.0;
+    KernelSet ks;
+    if (!select_kernels(gx.dc_max, gx.dv_max, o.precision, damp, ks))
+        return "no GPU kernel built for check degree " + std::to_string(gx.dc_max) + " / variable degree " +
+               std::to_string(gx.dv_max);
+    JBP_CUDA_TRY(cudaSetDevice(device_), "cudaSetDevice");
+    const int S = choose_slots(o, rq.ntrials);
+    std::string e = ensure_buffers(S, o.precision, damp);
+    if (!e.empty()) return e;
+
+    cudaStream_t st = rq.stream;
+    const int n = model_.n, M = gx.m + gz.m;
+    DevRun r{};
+    r.S = S;
+    r.max_iter = o.max_iter;
+    r.check_warmup = std::max(0, o.check_warmup);
+    r.check_interval = std::max(1, o.check_interval);
+    r.source = rq.source;
+    r.p = rq.p;
+    r.seed = rq.seed;
+    r.first_trial = rq.first_trial;
+    r.ntrials = rq.ntrials;
+    r.src_err = rq.d_err;
+    r.src_sx = rq.d_sx;
+    r.src_sz = rq.d_sz;
+    r.est_out = rq.d_est_out;
+    r.res_out = rq.d_res_out;
+    r.hist = rq.d_hist;
+    r.trial = buf_.trial;
+    r.iter = buf_.iter;
+    r.flags = buf_.flags;
+    r.unsat = buf_.unsat;
+    r.prior = buf_.prior;
+    r.lprior = buf_.lprior;
+    r.err = buf_.err;
+    r.est = buf_.est;
+    r.syn = buf_.syn;
+    r.res_iters = buf_.res_iters;
+    r.res_flags = buf_.res_flags;
+    r.retired = buf_.lists;
+    r.fresh = buf_.lists + S;
+    r.groups = buf_.lists + 2 * S;
+    r.n_retired = buf_.counts;
+    r.n_fresh = buf_.counts + 1;
+    r.n_groups = buf_.counts + 2;
+    r.cnt = buf_.cnt;
+    DevMsgs msg{};
+    for (int s = 0; s < 2; ++s) {
+        msg.c2v[s] = buf_.msg[s];
+        msg.v2c[s] = buf_.msg[2 + s];
+        msg.v2c_hi[s] = buf_.msg[4 + s];
+    }
+
+    // launch shapes
+    const int tpb = 256;
+    const int big_grid = sm_count_ * 8;                         // grid-stride message kernels
+    const int slot_blocks = (S / kGroup + (tpb / 32) - 1) / (tpb / 32);
+    const int classify_tpb = 128;
+    const size_t classify_smem = static_cast<size_t>(classify_tpb / 32) * 2 * dcode_.words * sizeof(uint64_t);
+    if (classify_smem > 48 * 1024) {
+        JBP_CUDA_TRY(cudaFuncSetAttribute(k_classify, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(classify_smem)), "smem attribute");
+    }
+    const int list_grid = std::max(1, std::min((S + tpb - 1) / tpb, sm_count_ * 4));
+    const int sample_grid = sm_count_ * 4;
+    long long launches = 0;
+
+    cudaEvent_t ev0, ev1;
+    JBP_CUDA_TRY(cudaEventCreate(&ev0), "cudaEventCreate");
+    JBP_CUDA_TRY(cudaEventCreate(&ev1), "cudaEventCreate");
+    cudaEvent_t poll_ev[2];
+    JBP_CUDA_TRY(cudaEventCreateWithFlags(&poll_ev[0], cudaEventDisableTiming), "cudaEventCreate");
+    JBP_CUDA_TRY(cudaEventCreateWithFlags(&poll_ev[1], cudaEventDisableTiming), "cudaEventCreate");
+
+    auto enqueue_refill = [&](cudaStream_t s) {
+        cudaMemsetAsync(r.n_fresh, 0, sizeof(int), s);
+        k_refill<<<list_grid, tpb, 0, s>>>(r, o.precision);
+        if (rq.source == kSrcMt19937) k_sample_mt<<<sample_grid, 256, 0, s>>>(dcode_, r);
+        else if (rq.source != kSrcSyndromes) k_sample<<<sample_grid, tpb, 0, s>>>(dcode_, r);
+        k_fresh_syndrome<<<sample_grid, tpb, 0, s>>>(dcode_, r);
+        cudaMemsetAsync(r.n_groups, 0, sizeof(int), s);
+        k_groups<<<slot_blocks, tpb, 0, s>>>(r);
+        launches += rq.source == kSrcSyndromes ? 3 : 4;
+    };
+    auto enqueue_iteration = [&](cudaStream_t s, cudaEvent_t *e3) {
+        if (e3) cudaEventRecordWithFlags(e3[0], s, cudaEventRecordExternal);
+        ks.check<<<big_grid, tpb, 0, s>>>(dcode_, r, msg);
+        if (e3) cudaEventRecordWithFlags(e3[1], s, cudaEventRecordExternal);
+        if (o.precision == JBP_PREC_FP64) ks.var64<<<big_grid, tpb, 0, s>>>(dcode_, r, msg, o.damping);
+        else ks.varllr<<<big_grid, tpb, 0, s>>>(dcode_, r, msg, static_cast<float>(o.damping));
+        if (e3) cudaEventRecordWithFlags(e3[2], s, cudaEventRecordExternal);
+        k_syndrome_check<<<big_grid, tpb, 0, s>>>(dcode_, r);
+        cudaMemsetAsync(r.n_retired, 0, sizeof(int), s);
+        k_retire<<<slot_blocks, tpb, 0, s>>>(r);
+        k_classify<<<sm_count_ * 2, classify_tpb, classify_smem, s>>>(dcode_, r);
+        launches += 5;
+        enqueue_refill(s);
+    };
+
+    JBP_CUDA_TRY(cudaEventRecord(ev0, st), "cudaEventRecord");
+    JBP_CUDA_TRY(cudaMemsetAsync(buf_.cnt, 0, sizeof(DevCounters), st), "memset counters");
+    k_init_slots<<<list_grid, tpb, 0, st>>>(r);
+    launches += 1;
+    enqueue_refill(st);
+    JBP_CUDA_TRY(cudaGetLastError(), "initial launches");
+
+    // CUDA graph of R iterations.  With profiling on, every captured iteration also records
+    // event nodes around the check and variable kernels; two graph instances alternate so
+    // that the events of a finished graph are read while the next one runs.
+    int R = o.iters_per_launch > 0 ? o.iters_per_launch : 4;
+    R = std::min(R, o.max_iter);
+    const bool prof = o.profile != 0;
+    const int nsets = prof ? 2 : 1;
+    std::vector<cudaEvent_t> pev(prof ? 2 * R * 3 : 0);
+    for (auto &ev : pev) JBP_CUDA_TRY(cudaEventCreate(&ev), "cudaEventCreate");
+    cudaStream_t cap;
+    JBP_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "cudaStreamCreate");
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    const long long launches_before = launches;
+    long long per_graph = 0;
+    cudaError_t ce = cudaSuccess;
+    for (int set = 0; set < nsets && ce == cudaSuccess; ++set) {
+        launches = launches_before;
+        ce = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        if (ce != cudaSuccess) break;
+        for (int i = 0; i < R; ++i) {
+            cudaEvent_t *e3 = prof ? &pev[(set * R + i) * 3] : nullptr;
+            enqueue_iteration(cap, e3);
+        }
+        ce = cudaStreamEndCapture(cap, &graph[set]);
+        if (ce == cudaSuccess) ce = cudaGraphInstantiate(&exec[set], graph[set], 0);
+        per_graph = launches - launches_before;
+    }
+    launches = launches_before;
+    double check_ms = 0.0, var_ms = 0.0;
+    long long prof_iters = 0;
+    auto read_profile = [&](long long gidx) {
+        if (!prof) return;
+        const int set = static_cast<int>(gidx & 1);
+        for (int i = 0; i < R; ++i) {
+            float a = 0.0f, b = 0.0f;
+            cudaEvent_t *e3 = &pev[(set * R + i) * 3];
+            if (cudaEventElapsedTime(&a, e3[0], e3[1]) == cudaSuccess &&
+                cudaEventElapsedTime(&b, e3[1], e3[2]) == cudaSuccess) {
+                check_ms += a;
+                var_ms += b;
+                prof_iters++;
+            }
+        }
+    };
+
+    const long long max_iters_total =
+        (rq.ntrials * static_cast<long long>(o.max_iter)) / std::max(1, S) + 2LL * o.max_iter + 2 * R + 8;
+    const long long max_graphs = max_iters_total / R + 2;
+    auto t0 = std::chrono::steady_clock::now();
+    std::string err;
+    if (ce != cudaSuccess) err = cuda_err(ce, "graph capture");
+    long long g = 0;
+    bool finished = false;
+    for (; err.empty() && g < max_graphs && !finished; ++g) {
+        ce = cudaGraphLaunch(exec[g % nsets], st);
+        if (ce != cudaSuccess) { err = cuda_err(ce, "graph launch"); break; }
+        launches += per_graph;
+        cudaMemcpyAsync(&buf_.h_done[g & 1], &buf_.cnt->done, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+        cudaEventRecord(poll_ev[g & 1], st);
+        if (g >= 1) {
+            ce = cudaEventSynchronize(poll_ev[(g - 1) & 1]);
+            if (ce != cudaSuccess) { err = cuda_err(ce, "run"); break; }
+            read_profile(g - 1);
+            if (buf_.h_done[(g - 1) & 1] >= static_cast<unsigned long long>(rq.ntrials)) finished = true;
+        }
+        if (o.watchdog_ms > 0) {
+            double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            if (wall > o.watchdog_ms) { err = "watchdog expired after " + std::to_string(wall) + " ms"; break; }
+        }
+    }
+    if (err.empty() && !finished && g >= 1) {
+        ce = cudaEventSynchronize(poll_ev[(g - 1) & 1]);
+        if (ce == cudaSuccess && buf_.h_done[(g - 1) & 1] >= static_cast<unsigned long long>(rq.ntrials)) finished = true;
+        if (!finished) err = "run did not complete within the iteration bound (internal error)";
+    }
+    cudaEventRecord(ev1, st);
+    ce = cudaEventSynchronize(ev1);
+    if (err.empty() && ce != cudaSuccess) err = cuda_err(ce, "run");
+    if (err.empty() && g >= 1) read_profile(g - 1);
+    if (err.empty()) {
+        ce = cudaGetLastError();
+        if (ce != cudaSuccess) err = cuda_err(ce, "run");
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    DevCounters hc{};
+    if (err.empty()) {
+        ce = cudaMemcpy(&hc, buf_.cnt, sizeof(hc), cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) err = cuda_err(ce, "read counters");
+    }
+    for (int set = 0; set < 2; ++set) {
+        if (exec[set]) cudaGraphExecDestroy(exec[set]);
+        if (graph[set]) cudaGraphDestroy(graph[set]);
+    }
+    for (auto &ev : pev) cudaEventDestroy(ev);
+    cudaStreamDestroy(cap);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    cudaEventDestroy(poll_ev[0]);
+    cudaEventDestroy(poll_ev[1]);
+    if (!err.empty()) return err;
+    stats.trials = static_cast<long long>(hc.done);
+    stats.failures = static_cast<long long>(hc.failures);
+    stats.bp_fail = static_cast<long long>(hc.bp_fail);
+    stats.pp_success = static_cast<long long>(hc.pp_success);
+    stats.flip_pp_success = static_cast<long long>(hc.flip_pp_success);
+    stats.osd_pp_success = static_cast<long long>(hc.osd_pp_success);
+    stats.stab_success = static_cast<long long>(hc.stab_success);
+    stats.ets_used = static_cast<long long>(hc.ets_used);
+    stats.ets_saved = static_cast<long long>(hc.ets_saved);
+    stats.ets6_used = static_cast<long long>(hc.ets6_used);
+    stats.ets6_saved = static_cast<long long>(hc.ets6_saved);
+    stats.ets12_used = static_cast<long long>(hc.ets12_used);
+    stats.ets12_saved = static_cast<long long>(hc.ets12_saved);
+    stats.exact = static_cast<long long>(hc.exact);
+    stats.total_iters = static_cast<long long>(hc.total_iters);
+    stats.bp_trial_iterations = static_cast<long long>(hc.bp_trial_iterations);
+    stats.device_ms = ms;
+    stats.kernel_launches = launches;
+    stats.check_ms = check_ms;
+    stats.var_ms = var_ms;
+    stats.profiled_iterations = prof_iters;
+    stats.slots = S;
+    (void)n;
+    (void)M;
+    return "";
+}
+
+std::string Engine::sample_errors(unsigned long long seed, long long first, long long count, double p, int source,
+                                  uint8_t *d_out) {
+    if (count <= 0) return "";
+    if (!(p > 0.0 && p < 1.0)) return "p must be in (0, 1)";
+    JBP_CUDA_TRY(cudaSetDevice(device_), "cudaSetDevice");
+    k_sample_out<<<sm_count_ * 4, 256>>>(model_.n, seed, first, count, p, source, d_out);
+    JBP_CUDA_TRY(cudaGetLastError(), "sample launch");
+    JBP_CUDA_TRY(cudaDeviceSynchronize(), "sample");
+    return "";
+}
+
+}  // namespace jbp

@@ -1,0 +1,77 @@
+// Host side of the batched engine.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "code_model.hpp"
+#include "engine.cuh"
+
+namespace jbp {
+
+struct RunRequest {
+    jbp_options opt{};
+    int source = kSrcPhilox;
+    unsigned long long seed = 0;
+    long long first_trial = 1;
+    long long ntrials = 0;
+    double p = 0.05;
+    const uint8_t *d_err = nullptr;     // source buffers (device)
+    const uint8_t *d_sx = nullptr;
+    const uint8_t *d_sz = nullptr;
+    uint8_t *d_est_out = nullptr;       // outputs (device, optional)
+    jbp_trial_result *d_res_out = nullptr;
+    unsigned long long *d_hist = nullptr;
+    cudaStream_t stream = nullptr;
+};
+
+class Engine {
+public:
+    Engine() = default;
+    ~Engine();
+    Engine(const Engine &) = delete;
+    Engine &operator=(const Engine &) = delete;
+
+    std::string init(CodeModel model, int device);
+    const CodeModel &model() const { return model_; }
+    int device() const { return device_; }
+    std::string run(const RunRequest &rq, jbp_stats &stats);
+    // Device sampler output (trial-major) into a device buffer.
+    std::string sample_errors(unsigned long long seed, long long first, long long count, double p, int source,
+                              uint8_t *d_out);
+
+private:
+    struct Buffers {
+        int S = 0, precision = -1;
+        bool damp = false;
+        size_t msg_bytes = 0;
+        void *msg[6] = {};            // c2v x/z, v2c x/z, v2c_hi x/z
+        long long *trial = nullptr;
+        int *iter = nullptr, *flags = nullptr, *unsat = nullptr;
+        double *prior = nullptr;
+        float *lprior = nullptr;
+        uint8_t *err = nullptr, *est = nullptr, *syn = nullptr;
+        int *res_iters = nullptr, *res_flags = nullptr;
+        int *lists = nullptr;         // retired | fresh | groups
+        int *counts = nullptr;        // n_retired, n_fresh, n_groups
+        DevCounters *cnt = nullptr;
+        unsigned long long *h_done = nullptr;  // pinned
+    };
+
+    std::string ensure_buffers(int S, int precision, bool damp);
+    void free_buffers();
+    int choose_slots(const jbp_options &opt, long long ntrials) const;
+
+    int device_ = 0;
+    int sm_count_ = 0;
+    CodeModel model_;
+    DevCode dcode_{};
+    std::vector<void *> code_allocs_;
+    Buffers buf_;
+};
+
+std::string cuda_err(cudaError_t e, const char *what);
+
+}  // namespace jbp

@@ -1,0 +1,399 @@
+// Slot lifecycle kernels: hard-decision syndrome test, retirement, success classification,
+// refill from the trial source, error sampling and fresh-trial syndromes.
+#pragma once
+
+#include "engine.cuh"
+
+namespace jbp {
+
+__device__ __forceinline__ int xbit(int s) { return s & 1; }          // X or Y
+__device__ __forceinline__ int zbit(int s) { return (s >> 1) & 1; }   // Z or Y
+
+// ------------------------------------------------------------------ samplers
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): 10 rounds of the 4x32 bijection.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+        const uint32_t hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += W0;
+        k.y += W1;
+    }
+    return c;
+}
+
+// Depolarizing channel as the reference maps a uniform u in [0,1) (jointbp_ets.cpp:5937-5945).
+__device__ __forceinline__ uint8_t pauli_from_uniform(double u, double p) {
+    const double q = __dsub_rn(1.0, p);
+    if (u < q) return 0;
+    const double v = __ddiv_rn(__dsub_rn(u, q), p);
+    return v < 1.0 / 3.0 ? 1 : (v < 2.0 / 3.0 ? 2 : 3);
+}
+
+// Philox stream: qubit v of trial t uses half of block (v/2, t); 53-bit uniform.
+__device__ __forceinline__ uint8_t sample_philox(unsigned long long seed, long long t, int v, double p) {
+    const uint4 r = philox4x32_10(make_uint4(static_cast<uint32_t>(v >> 1), static_cast<uint32_t>(t),
+                                             static_cast<uint32_t>(static_cast<unsigned long long>(t) >> 32),
+                                             0x4A425042u),
+                                  make_uint2(static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32)));
+    const unsigned long long x = (v & 1) ? (static_cast<unsigned long long>(r.w) << 32 | r.z)
+                                         : (static_cast<unsigned long long>(r.y) << 32 | r.x);
+    const double u = static_cast<double>(x >> 11) * 0x1.0p-53;
+    return pauli_from_uniform(u, p);
+}
+
+// ------------------------------------------------------------------ per-iteration kernels
+
+// Hard-decision syndrome of every running slot that is due a check: unsatisfied checks
+// are counted per slot and side (jointbp_ets.cpp:2521-2525; check schedule of
+// jointbp_cuda.cu:971-975).
+__global__ void __launch_bounds__(256) k_syndrome_check(DevCode code, DevRun run) {
+    const int lane = threadIdx.x & 31;
+    const int S = run.S;
+    const int mx = code.s[0].m, M = mx + code.s[1].m;
+    const long long total = static_cast<long long>(*run.n_groups) * M;
+    for (long long w = warp_global_id(); w < total; w += warps_total()) {
+        const int gi = static_cast<int>(w / M);
+        const int row = static_cast<int>(w - static_cast<long long>(gi) * M);
+        const int slot = run.groups[gi] * kGroup + lane;
+        if (!(run.flags[slot] & kRunning)) continue;
+        const int k1 = run.iter[slot] + 1;
+        const bool due = k1 >= run.max_iter ||
+                         (k1 > run.check_warmup && (k1 - run.check_warmup) % run.check_interval == 0);
+        if (!due) continue;
+        const int side = row >= mx;
+        const int ch = side ? row - mx : row;
+        const DevSide &g = code.s[side];
+        int par = 0;
+        for (int i = 0; i < g.dc; ++i) {
+            const int v = g.chk_var[ch * g.dc + i];
+            const int s = run.est[static_cast<size_t>(v) * S + slot];
+            par ^= side ? zbit(s) : xbit(s);
+        }
+        if (par != run.syn[static_cast<size_t>(row) * S + slot]) atomicAdd(&run.unsat[side * S + slot], 1);
+    }
+}
+
+// Counts the finished iteration; a slot retires when its checked syndrome matches or it
+// reaches max_iter (the CPU's iteration accounting, jointbp_ets.cpp:2733-2735, 3078).
+__global__ void k_retire(DevRun run) {
+    const int gi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (gi >= *run.n_groups) return;
+    const int slot = run.groups[gi] * kGroup + (threadIdx.x & 31);
+    if (!(run.flags[slot] & kRunning)) return;
+    const int S = run.S;
+    const int k1 = run.iter[slot] + 1;
+    run.iter[slot] = k1;
+    const bool due = k1 >= run.max_iter ||
+                     (k1 > run.check_warmup && (k1 - run.check_warmup) % run.check_interval == 0);
+    const bool conv = due && run.unsat[slot] == 0 && run.unsat[S + slot] == 0;
+    run.unsat[slot] = 0;
+    run.unsat[S + slot] = 0;
+    if (conv || k1 >= run.max_iter) {
+        run.res_iters[slot] = k1;
+        run.res_flags[slot] = conv ? 3 : 0;
+        run.flags[slot] = kFinished;
+        run.retired[atomicAdd(run.n_retired, 1)] = slot;
+    }
+}
+
+// Warp-wide test of vec (smem, `words` 64-bit words) for membership in a row space given
+// in echelon form by its highest bits (in_row_space, jointbp_ets.cpp:904-920): repeatedly
+// clear the highest set bit with the basis row that has it as pivot; a bit with no such
+// row means the vector is outside the space.  vec is destroyed.
+__device__ bool warp_in_row_space(uint64_t *vec, int words, const uint64_t *rows, const int *pivot_row) {
+    const int lane = threadIdx.x & 31;
+    for (int guard = 0; guard < 1 << 20; ++guard) {
+        int hw = -1;
+        for (int w = lane; w < words; w += 32)
+            if (vec[w]) hw = w;
+        hw = __reduce_max_sync(0xffffffffu, hw + 1) - 1;
+        if (hw < 0) return true;
+        const uint64_t top = vec[hw];
+        const int bit = hw * 64 + 63 - __clzll(static_cast<long long>(top));
+        const int r = pivot_row[bit];
+        __syncwarp();
+        if (r < 0) return false;
+        const uint64_t *row = rows + static_cast<size_t>(r) * words;
+        for (int w = lane; w <= hw; w += 32) vec[w] ^= row[w];
+        __syncwarp();
+    }
+    return false;
+}
+
+// Classifies each retired trial (jointbp_ets.cpp:6199-6245): exact match, stabilizer
+// equivalence of the residual (x-part in rowspace(Hz), z-part in rowspace(Hx)), success;
+// writes the per-trial record and estimate and updates the run counters.
+__global__ void k_classify(DevCode code, DevRun run) {
+    extern __shared__ uint64_t smem_words[];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    const int words = code.words;
+    uint64_t *dx = smem_words + static_cast<size_t>(wib) * 2 * words;
+    uint64_t *dz = dx + words;
+    const int nret = *run.n_retired;
+    const int n = code.n, S = run.S;
+    const bool have_err = run.source != kSrcSyndromes;
+    for (int r = blockIdx.x * wpb + wib; r < nret; r += gridDim.x * wpb) {
+        const int slot = run.retired[r];
+        const long long local = run.trial[slot] - run.first_trial;
+        const int iters = run.res_iters[slot];
+        const bool ok = run.res_flags[slot] & 1;
+        for (int w = lane; w < words; w += 32) { dx[w] = 0; dz[w] = 0; }
+        __syncwarp();
+        bool exact = true;
+        const uint8_t *err = run.err + static_cast<size_t>(slot) * n;
+        for (int base = 0; base < n; base += 32) {
+            const int v = base + lane;
+            const bool in = v < n;
+            const int e = in ? run.est[static_cast<size_t>(v) * S + slot] : 0;
+            const int t = (in && have_err) ? err[v] : e;
+            if (in && run.est_out) run.est_out[local * n + v] = static_cast<uint8_t>(e);
+            if (t != e) exact = false;
+            const unsigned bx = __ballot_sync(0xffffffffu, xbit(t) != xbit(e));
+            const unsigned bz = __ballot_sync(0xffffffffu, zbit(t) != zbit(e));
+            if (lane == 0) {
+                const int sh = base & 32;  // which half of the 64-bit word
+                dx[base >> 6] |= static_cast<uint64_t>(bx) << sh;
+                dz[base >> 6] |= static_cast<uint64_t>(bz) << sh;
+            }
+        }
+        exact = __all_sync(0xffffffffu, exact) && have_err;
+        __syncwarp();
+        bool stab = false;
+        if (have_err && ok) {
+            stab = warp_in_row_space(dx, words, code.basis_rows[1], code.pivot_row[1]);
+            if (stab) stab = warp_in_row_space(dz, words, code.basis_rows[0], code.pivot_row[0]);
+        }
+        const bool success = have_err ? (ok && stab) : ok;
+        if (lane == 0) {
+            DevCounters *c = run.cnt;
+            atomicAdd(&c->done, 1ull);
+            atomicAdd(&c->total_iters, static_cast<unsigned long long>(iters));
+            atomicAdd(&c->bp_trial_iterations, static_cast<unsigned long long>(iters));
+            if (!success) atomicAdd(&c->failures, 1ull);
+            if (!(run.res_flags[slot] & 2)) atomicAdd(&c->bp_fail, 1ull);
+            if (exact) atomicAdd(&c->exact, 1ull);
+            if (ok) atomicAdd(&c->syndrome_ok, 1ull);
+            if (success && !exact && stab) atomicAdd(&c->stab_success, 1ull);
+            if (run.hist && iters >= 1 && iters <= run.max_iter) atomicAdd(&run.hist[iters], 1ull);
+            if (run.res_out) {
+                jbp_trial_result rec;
+                rec.iterations = iters;
+                rec.syndrome_ok = ok;
+                rec.bp_ok = (run.res_flags[slot] >> 1) & 1;
+                rec.success = success;
+                rec.exact = exact;
+                rec.stab_equiv = stab;
+                rec.pp_success = 0;
+                rec.pp_ets = 0;
+                rec.pp_flip = 0;
+                rec.pp_osd = 0;
+                rec.ets_used_flags = 0;
+                rec.pp_in_decode = 0;
+                rec.reserved = 0;
+                run.res_out[local] = rec;
+            }
+            run.flags[slot] = 0;
+        }
+        __syncwarp();
+    }
+}
+
+// Hands the next trials of the source to the retired (or never used) slots.
+__global__ void k_refill(DevRun run, int precision) {
+    const int nret = *run.n_retired;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nret; r += gridDim.x * blockDim.x) {
+        const int slot = run.retired[r];
+        const unsigned long long t = atomicAdd(&run.cnt->next_trial, 1ull);
+        if (t < static_cast<unsigned long long>(run.ntrials)) {
+            run.trial[slot] = run.first_trial + static_cast<long long>(t);
+            run.iter[slot] = 0;
+            run.flags[slot] = kRunning;
+            // prior = normalize(1-p, p/3, p/3, p/3) (jointbp_ets.cpp:5484-5485)
+            double p0 = __dsub_rn(1.0, run.p), p1 = __ddiv_rn(run.p, 3.0), p2 = p1, p3 = p1;
+            double s = __dadd_rn(__dadd_rn(__dadd_rn(p0, p1), p2), p3);
+            if (s <= 0.0) { p0 = p1 = p2 = p3 = 0.25; }
+            else { p0 = __ddiv_rn(p0, s); p1 = __ddiv_rn(p1, s); p2 = __ddiv_rn(p2, s); p3 = __ddiv_rn(p3, s); }
+            if (precision == JBP_PREC_FP64) {
+                double *pr = run.prior + 4 * slot;
+                pr[0] = p0; pr[1] = p1; pr[2] = p2; pr[3] = p3;
+            } else {
+                float *lp = run.lprior + 8 * slot;
+                lp[0] = static_cast<float>(log(p0));
+                lp[1] = static_cast<float>(log(p1));
+                lp[2] = static_cast<float>(log(p2));
+                lp[3] = static_cast<float>(log(p3));
+                lp[4] = static_cast<float>(log((p0 + p2) / (p1 + p3)));   // v2c prior LLR of an x-bit
+                lp[5] = static_cast<float>(log((p0 + p1) / (p2 + p3)));   // v2c prior LLR of a z-bit
+                lp[6] = lp[7] = 0.0f;
+            }
+            run.fresh[atomicAdd(run.n_fresh, 1)] = slot;
+        } else {
+            run.trial[slot] = -1;
+            run.flags[slot] = 0;
+        }
+    }
+}
+
+// Errors of fresh trials: Philox, or copied from a device buffer of known errors.
+__global__ void k_sample(DevCode code, DevRun run) {
+    const int nf = *run.n_fresh;
+    const int n = code.n;
+    const long long total = static_cast<long long>(nf) * n;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int f = static_cast<int>(i / n);
+        const int v = static_cast<int>(i - static_cast<long long>(f) * n);
+        const int slot = run.fresh[f];
+        const long long t = run.trial[slot];
+        uint8_t e = 0;
+        if (run.source == kSrcPhilox) e = sample_philox(run.seed, t, v, run.p);
+        else if (run.source == kSrcErrors) e = run.src_err[(t - run.first_trial) * n + v];
+        run.err[static_cast<size_t>(slot) * n + v] = e;
+    }
+}
+
+// The reference stream on the device: splitmix64 seed, mt19937_64 and libstdc++'s
+// uniform_real_distribution<double> (one draw, x * 2^-64, clamped below 1), for one trial
+// per warp; s is the warp's 312-word state.  The twist runs in two dependency-free halves:
+// words 0..155 read only words of the previous block, words 156..311 read words 0..155 of
+// this block.
+__device__ void warp_mt_trial(unsigned long long *s, unsigned long long base_seed, long long t, double p, int n,
+                              uint8_t *out) {
+    const int lane = threadIdx.x & 31;
+    const unsigned long long seed =
+        splitmix64(base_seed ^ (static_cast<unsigned long long>(t) * 0x9e3779b97f4a7c15ull));
+    if (lane == 0) {
+        s[0] = seed;
+        for (int i = 1; i < 312; ++i) s[i] = 6364136223846793005ull * (s[i - 1] ^ (s[i - 1] >> 62)) + i;
+    }
+    __syncwarp();
+    const unsigned long long hi = 0xFFFFFFFF80000000ull, lo = 0x7FFFFFFFull, A = 0xB5026F5AA96619E9ull;
+    for (int base = 0; base < n; base += 312) {
+        unsigned long long nv[5];
+        for (int j = 0; j < 5; ++j) {
+            const int k = lane + 32 * j;
+            if (k < 156) {
+                const unsigned long long y = (s[k] & hi) | (s[k + 1] & lo);
+                nv[j] = s[k + 156] ^ (y >> 1) ^ ((y & 1) ? A : 0ull);
+            }
+        }
+        __syncwarp();
+        for (int j = 0; j < 5; ++j) {
+            const int k = lane + 32 * j;
+            if (k < 156) s[k] = nv[j];
+        }
+        __syncwarp();
+        for (int j = 0; j < 5; ++j) {
+            const int k = 156 + lane + 32 * j;
+            if (k < 312) {
+                const unsigned long long y = (s[k] & hi) | (s[(k + 1) % 312] & lo);
+                nv[j] = s[k - 156] ^ (y >> 1) ^ ((y & 1) ? A : 0ull);
+            }
+        }
+        __syncwarp();
+        for (int j = 0; j < 5; ++j) {
+            const int k = 156 + lane + 32 * j;
+            if (k < 312) s[k] = nv[j];
+        }
+        __syncwarp();
+        for (int k = lane; k < 312 && base + k < n; k += 32) {
+            unsigned long long x = s[k];
+            x ^= (x >> 29) & 0x5555555555555555ull;
+            x ^= (x << 17) & 0x71D67FFFEDA60000ull;
+            x ^= (x << 37) & 0xFFF7EEE000000000ull;
+            x ^= x >> 43;
+            double u = static_cast<double>(x) * 0x1.0p-64;
+            if (u >= 1.0) u = 0x1.fffffffffffffp-1;
+            out[base + k] = pauli_from_uniform(u, p);
+        }
+        __syncwarp();
+    }
+}
+
+__global__ void k_sample_mt(DevCode code, DevRun run) {
+    __shared__ unsigned long long st[8][312];
+    const int wib = threadIdx.x >> 5;
+    const int nf = *run.n_fresh;
+    for (int f = blockIdx.x * 8 + wib; f < nf; f += gridDim.x * 8) {
+        const int slot = run.fresh[f];
+        warp_mt_trial(st[wib], run.seed, run.trial[slot], run.p, code.n, run.err + static_cast<size_t>(slot) * code.n);
+    }
+}
+
+// Errors of trials first..first+count-1 written trial-major (jbp_sample_errors).
+__global__ void k_sample_out(int n, unsigned long long seed, long long first, long long count, double p, int sampler,
+                             uint8_t *out) {
+    __shared__ unsigned long long st[8][312];
+    if (sampler == kSrcMt19937) {
+        const int wib = threadIdx.x >> 5;
+        for (long long t = blockIdx.x * 8LL + wib; t < count; t += gridDim.x * 8LL)
+            warp_mt_trial(st[wib], seed, first + t, p, n, out + t * n);
+    } else {
+        const long long total = count * n;
+        for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+             i += static_cast<long long>(gridDim.x) * blockDim.x) {
+            const long long t = i / n;
+            out[i] = sample_philox(seed, first + t, static_cast<int>(i - t * n), p);
+        }
+    }
+}
+
+// Syndromes of fresh trials, from their errors or copied from the source.
+__global__ void k_fresh_syndrome(DevCode code, DevRun run) {
+    const int nf = *run.n_fresh;
+    const int mx = code.s[0].m, M = mx + code.s[1].m;
+    const int n = code.n, S = run.S;
+    const long long total = static_cast<long long>(nf) * M;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int f = static_cast<int>(i / M);
+        const int row = static_cast<int>(i - static_cast<long long>(f) * M);
+        const int slot = run.fresh[f];
+        const int side = row >= mx;
+        const int ch = side ? row - mx : row;
+        uint8_t bit;
+        if (run.source == kSrcSyndromes) {
+            const long long local = run.trial[slot] - run.first_trial;
+            bit = side ? run.src_sz[local * code.s[1].m + ch] : run.src_sx[local * mx + ch];
+            bit &= 1;
+        } else {
+            const DevSide &g = code.s[side];
+            const uint8_t *err = run.err + static_cast<size_t>(slot) * n;
+            int par = 0;
+            for (int k = 0; k < g.dc; ++k) {
+                const int s = err[g.chk_var[ch * g.dc + k]];
+                par ^= side ? zbit(s) : xbit(s);
+            }
+            bit = static_cast<uint8_t>(par);
+        }
+        run.syn[static_cast<size_t>(row) * S + slot] = bit;
+    }
+}
+
+// Compacts the groups that still hold a running slot.
+__global__ void k_groups(DevRun run) {
+    const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (g >= run.S / kGroup) return;
+    const int lane = threadIdx.x & 31;
+    const bool any = __any_sync(0xffffffffu, run.flags[g * kGroup + lane] & kRunning);
+    if (any && lane == 0) run.groups[atomicAdd(run.n_groups, 1)] = g;
+}
+
+__global__ void k_init_slots(DevRun run) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < run.S; s += gridDim.x * blockDim.x) {
+        run.retired[s] = s;
+        run.flags[s] = 0;
+        run.trial[s] = -1;
+        run.iter[s] = 0;
+        run.unsat[s] = 0;
+        run.unsat[run.S + s] = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *run.n_retired = run.S;
+}
+
+}  // namespace jbp

@@ -1,0 +1,141 @@
+"""Generates the golden fixtures in tests/golden/ from the reference itself.
+
+Runs in a container that has the reference sources (built into oracle/_ref/ by
+`make -C oracle`): the per-trial records come from the harness over the unmodified
+reference decoder (oracle/_ref/libjbp_ref.so), the run summaries from the unmodified
+reference CLI (oracle/_ref/jointbp_ets).  The fixtures are small JSON/NPZ files that
+travel with the repository; the GPU tests read them without the reference present.
+
+    python tests/golden/make_golden.py [--quick]
+"""
+import argparse
+import hashlib
+import json
+import re
+import subprocess
+import sys
+import zlib
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parent))
+from oracle_bind import ETS_DIR, PARAMS, REF_DIR, Reference  # noqa: E402
+
+# (name, seed, p, max_iter, enable_pp, flip_hist, trials, vectors_for_first)
+SIM_CASES = [
+    ("p050_mi50_nopp_s1", 1, 0.05, 50, False, 5, range(1, 201), 16),
+    ("p040_mi1000_nopp_s106", 106, 0.04, 1000, False, 5, range(1, 101), 16),
+    ("p050_mi200_pp_s305", 305, 0.05, 200, True, 5, range(1, 41), 40),
+    ("p060_mi120_pp_s7", 7, 0.06, 120, True, 5, range(1, 25), 24),
+    ("p055_mi150_pp_fh0_s11", 11, 0.055, 150, True, 0, range(1, 21), 20),
+]
+
+
+def crc(a):
+    return zlib.crc32(np.ascontiguousarray(a, np.uint8).tobytes()) & 0xFFFFFFFF
+
+
+def run_cli(args):
+    exe = REF_DIR / "jointbp_ets"
+    out = subprocess.run([str(exe), "--params", str(PARAMS)] + args, capture_output=True, text=True,
+                         cwd=str(PARAMS.parent), check=False)
+    line = [l for l in out.stdout.splitlines() if l.startswith("trials=")]
+    return out.returncode, line[-1] if line else None, out.stdout
+
+
+def parse_summary(line):
+    d = {}
+    for k, v in re.findall(r"(\w+)=(\[[^\]]*\]|\S+)", line):
+        d[k] = v
+    return d
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--quick", action="store_true", help="skip the 1000-trial CLI summary")
+    args = ap.parse_args()
+    ref = Reference()
+    lib = ref.lib
+
+    # --- code known answers (README start-up block) ---
+    import ctypes
+    cnt = np.zeros(64, np.int32)
+    labels = ctypes.create_string_buffer(32 * 8)
+    ng = lib.ref_ets_counts(cnt.ctypes.data_as(ctypes.c_void_p), 32, labels, 8)
+    groups = []
+    for i in range(ng):
+        groups.append({"label": labels.raw[i * 8:(i + 1) * 8].split(b"\0")[0].decode(),
+                       "x": int(cnt[2 * i]), "z": int(cnt[2 * i + 1])})
+    xchk = np.zeros(ref.m[0] * 12, np.int32)
+    zchk = np.zeros(ref.m[1] * 12, np.int32)
+    lib.ref_checks(0, xchk.ctypes.data_as(ctypes.c_void_p))
+    lib.ref_checks(1, zchk.ctypes.data_as(ctypes.c_void_p))
+    kat = {"n": ref.n, "mx": ref.m[0], "mz": ref.m[1], "rank_x": lib.ref_rank_x(), "rank_z": lib.ref_rank_z(),
+           "girth_x": lib.ref_girth(0), "girth_z": lib.ref_girth(1), "ets_groups": groups,
+           "x_checks_sha256": hashlib.sha256(xchk.tobytes()).hexdigest(),
+           "z_checks_sha256": hashlib.sha256(zchk.tobytes()).hexdigest()}
+    kat["k"] = kat["n"] - kat["rank_x"] - kat["rank_z"]
+
+    # --- sampler goldens ---
+    samp = {}
+    for seed, p, idxs in ((106, 0.04, (1, 2, 3, 1000, 999999)), (1, 0.05, (1, 7)), (2 ** 63 + 5, 0.01, (4,))):
+        for i in idxs:
+            e = ref.sample(seed, i, p)
+            samp[f"{seed}:{p}:{i}"] = {"crc": crc(e), "weight": int((e != 0).sum()),
+                                       "counts": [int((e == s).sum()) for s in range(4)]}
+    kat["sampler"] = samp
+    (HERE / "kat.json").write_text(json.dumps(kat, indent=1))
+
+    # --- per-trial simulate records ---
+    for name, seed, p, mi, pp, fh, trials, nvec in SIM_CASES:
+        recs, errs, ests = [], [], []
+        for k, t in enumerate(trials):
+            d = ref.simulate_trial(seed, t, p, mi, flip_hist=fh, enable_pp=pp, want_vectors=True)
+            e, s = d.pop("err"), d.pop("est")
+            d["err_crc"], d["est_crc"] = crc(e), crc(s)
+            recs.append(d)
+            if k < nvec:
+                errs.append(e)
+                ests.append(s)
+        meta = {"seed": seed, "p": p, "max_iter": mi, "enable_pp": pp, "flip_hist": fh, "records": recs}
+        (HERE / f"sim_{name}.json").write_text(json.dumps(meta))
+        np.savez_compressed(HERE / f"vec_{name}.npz", err=np.array(errs, np.uint8), est=np.array(ests, np.uint8))
+        print(name, "failures", sum(1 - r["success"] for r in recs), "pp", sum(r["pp_success_this"] for r in recs),
+              flush=True)
+
+    # --- |LLR| goldens (last-iteration |LLR| of plain BP; they order the OSD columns) ---
+    llr = {}
+    for seed, p, t, mi in ((305, 0.05, 19, 30), (1, 0.05, 3, 12)):
+        e = ref.sample(seed, t, p)
+        sx = np.zeros(ref.m[0], np.int32)
+        sz = np.zeros(ref.m[1], np.int32)
+        lib.ref_syndrome(e.astype(np.int32).ctypes.data_as(ctypes.c_void_p), sx.ctypes.data_as(ctypes.c_void_p),
+                         sz.ctypes.data_as(ctypes.c_void_p))
+        r = ref.bp_decode(sx, sz, p, mi, want_llr=True)
+        llr[f"s{seed}_t{t}_mi{mi}"] = (r["abs_llr_x"], r["abs_llr_z"], r["est"], r["iterations"])
+    np.savez_compressed(HERE / "llr_golden.npz",
+                        **{k + "_x": v[0] for k, v in llr.items()}, **{k + "_z": v[1] for k, v in llr.items()},
+                        **{k + "_est": v[2] for k, v in llr.items()},
+                        **{k + "_iters": np.array([v[3]]) for k, v in llr.items()})
+
+    # --- reference CLI run summaries ---
+    summaries = {}
+    cli_cases = [("p050_mi50_nopp_s1_t200", ["--simulate", "--p", "0.05", "--trials", "200", "--max-iter", "50",
+                                             "--no-pp", "--seed", "1", "--report-every", "0"]),
+                 ("p050_mi200_pp_s305_t40", ["--simulate", "--p", "0.05", "--trials", "40", "--max-iter", "200",
+                                             "--flip-hist", "5", "--seed", "305", "--report-every", "0"])]
+    if not args.quick:
+        cli_cases.append(("p050_mi50_nopp_s1_t1000", ["--simulate", "--p", "0.05", "--trials", "1000",
+                                                      "--max-iter", "50", "--no-pp", "--seed", "1",
+                                                      "--report-every", "0"]))
+    for name, a in cli_cases:
+        rc, line, _ = run_cli(a)
+        summaries[name] = {"args": a, "rc": rc, "summary": parse_summary(line) if line else None}
+        print(name, line, flush=True)
+    (HERE / "cli_summaries.json").write_text(json.dumps(summaries, indent=1))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,85 @@
+"""C-ABI library checks that need no GPU: it loads, exports every declared symbol, and its
+host-side pieces (reference-stream sampler, error paths) behave."""
+import ctypes
+import json
+import re
+import subprocess
+import zlib
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT
+
+INCLUDE = ROOT / "include"
+LIBDIR = ROOT / "joint_bp_plus_pp_b200" / "lib"
+
+
+def declared_functions(header):
+    text = re.sub(r"/\*.*?\*/", "", header.read_text(), flags=re.S)
+    text = re.sub(r"//[^\n]*", "", text)
+    names = re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\([^;{]*\)\s*;", text)
+    return sorted(set(n for n in names if not n.startswith("__")))
+
+
+def exported(lib):
+    out = subprocess.run(["nm", "-D", "--defined-only", str(lib)], capture_output=True, text=True, check=True).stdout
+    return {line.split()[-1] for line in out.splitlines() if line.strip()}
+
+
+def test_library_exports_all_declared_symbols():
+    lib = LIBDIR / "libjbp_b200.so"
+    assert lib.exists(), "run python -m joint_bp_plus_pp_b200.build"
+    decl = declared_functions(INCLUDE / "jbp_b200.h")
+    assert "jbp_simulate" in decl and "jbp_decode_errors" in decl
+    missing = [d for d in decl if d not in exported(lib)]
+    assert not missing, missing
+    ctypes.CDLL(str(lib))
+
+
+def test_shim_exports_reference_boundary():
+    lib = LIBDIR / "libjointbp_cuda.so"
+    if not lib.exists():
+        pytest.skip("shim not built")
+    syms = exported(lib)
+    # C++ symbols of jointbp_cuda.h (Itanium mangling of the reference signatures)
+    for name in ("cuda_bp_create", "cuda_bp_destroy", "cuda_bp_decode"):
+        assert any(name in s for s in syms), name
+
+
+def test_version_and_error_strings():
+    from joint_bp_plus_pp_b200 import load_library
+    lib = load_library()
+    assert b"sm_100a" in lib.jbp_version()
+    h = ctypes.c_void_p()
+    rc = lib.jbp_create_from_params(b"/nonexistent/params.txt", None, 0, ctypes.byref(h))
+    assert rc == 3 and b"cannot open" in lib.jbp_last_error()
+    assert not h.value
+
+
+def test_host_reference_sampler_matches_golden():
+    from joint_bp_plus_pp_b200 import sample_reference_errors
+    kat = json.loads((GOLDEN / "kat.json").read_text())
+    for key, exp in kat["sampler"].items():
+        seed, p, idx = key.split(":")
+        e = sample_reference_errors(9216, int(seed), int(idx), 1, float(p), threads=1)[0]
+        assert zlib.crc32(e.tobytes()) & 0xFFFFFFFF == exp["crc"], key
+
+
+def test_host_reference_sampler_threads_agree():
+    from joint_bp_plus_pp_b200 import sample_reference_errors
+    a = sample_reference_errors(9216, 106, 1, 24, 0.04, threads=1)
+    b = sample_reference_errors(9216, 106, 1, 24, 0.04, threads=5)
+    assert (a == b).all()
+
+
+def test_no_gpu_is_an_error_not_a_fallback():
+    """Without a usable device the library reports a CUDA error; it never decodes on the CPU."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from joint_bp_plus_pp_b200 import Decoder, JbpError
+    with pytest.raises(JbpError) as ei:
+        Decoder.from_params()
+    assert ei.value.code == 2

@@ -1,0 +1,152 @@
+"""GPU parity: the CUDA path against the oracle and the reference's golden fixtures.
+
+FP64: bit-exact estimates, iteration counts and outcome flags (integer/byte work, so the
+bar is equality).  FP32/FP16: decisions and logical error rate against FP64 within the
+stated tolerances.
+"""
+import zlib
+
+import numpy as np
+import pytest
+
+from conftest import load_sim_case
+
+pytestmark = pytest.mark.gpu
+
+NOPP_CASES = ["p050_mi50_nopp_s1", "p040_mi1000_nopp_s106"]
+
+
+def crc(a):
+    return zlib.crc32(np.ascontiguousarray(a, np.uint8).tobytes()) & 0xFFFFFFFF
+
+
+def opts(**kw):
+    from joint_bp_plus_pp_b200 import Options
+    base = dict(precision="fp64", enable_pp=False)
+    base.update(kw)
+    return Options(**base)
+
+
+@pytest.mark.parametrize("name", NOPP_CASES)
+def test_fp64_decode_errors_bit_exact_vs_golden(decoder, name):
+    meta, errs, ests = load_sim_case(name)
+    st, res, est = decoder.decode_errors(errs, meta["p"], opts(max_iter=meta["max_iter"]))
+    recs = meta["records"][:len(errs)]
+    assert (est == ests).all()
+    assert list(res["iterations"]) == [r["iterations"] for r in recs]
+    assert list(res["bp_ok"]) == [r["bp_ok"] for r in recs]
+    assert list(res["success"]) == [r["success"] for r in recs]
+    assert list(res["exact"]) == [r["exact"] for r in recs]
+    assert list(res["stab_equiv"]) == [r["stab_equiv"] for r in recs]
+
+
+@pytest.mark.parametrize("name", NOPP_CASES)
+def test_fp64_simulate_device_mt_sampler_matches_golden(decoder, name):
+    """Monte Carlo with the reference error stream generated on the device."""
+    meta, _, _ = load_sim_case(name)
+    recs = meta["records"]
+    first = recs[0]["trial_idx"]
+    st, res = decoder.simulate(meta["seed"], len(recs), meta["p"], opts(max_iter=meta["max_iter"]), first_trial=first,
+                               sampler="mt19937")
+    for r, g in zip(res, recs):
+        assert (r["iterations"], r["bp_ok"], r["success"], r["exact"], r["stab_equiv"]) == \
+               (g["iterations"], g["bp_ok"], g["success"], g["exact"], g["stab_equiv"]), g["trial_idx"]
+    assert st["trials"] == len(recs)
+    assert st["failures"] == sum(1 - g["success"] for g in recs)
+    assert st["total_iters"] == sum(g["iterations"] for g in recs)
+
+
+def test_fp64_vs_oracle_fresh_trials(decoder, oracle):
+    """Fresh trials at a high error rate (many non-converging trials) against the oracle."""
+    from joint_bp_plus_pp_b200 import sample_reference_errors
+    for seed, p, mi, k in ((9001, 0.065, 35, 48), (31337, 0.03, 25, 64)):
+        err = sample_reference_errors(decoder.n, seed, 1, k, p)
+        st, res, est = decoder.decode_errors(err, p, opts(max_iter=mi))
+        for t in range(k):
+            sx, sz = oracle.syndrome(err[t])
+            o = oracle.decode(sx, sz, p, mi, enable_pp=False)
+            assert (o["est"] == est[t]).all(), (seed, t)
+            assert o["iterations"] == res["iterations"][t]
+            assert o["syndrome_ok"] == res["syndrome_ok"][t]
+
+
+def test_fp64_decode_syndromes(decoder, oracle):
+    meta, errs, ests = load_sim_case("p050_mi50_nopp_s1")
+    sx = np.stack([oracle.syndrome(e)[0] for e in errs[:8]])
+    sz = np.stack([oracle.syndrome(e)[1] for e in errs[:8]])
+    st, res, est = decoder.decode_syndromes(sx, sz, meta["p"], opts(max_iter=meta["max_iter"]))
+    assert (est == ests[:8]).all()
+    assert list(res["iterations"]) == [r["iterations"] for r in meta["records"][:8]]
+    assert list(res["syndrome_ok"]) == [r["syndrome_ok"] for r in meta["records"][:8]]
+
+
+def test_fp64_damping_vs_oracle(decoder, oracle):
+    from joint_bp_plus_pp_b200 import sample_reference_errors
+    p, mi, d = 0.05, 30, 0.3
+    err = sample_reference_errors(decoder.n, 5, 1, 16, p)
+    st, res, est = decoder.decode_errors(err, p, opts(max_iter=mi, damping=d))
+    for t in range(16):
+        sx, sz = oracle.syndrome(err[t])
+        o = oracle.decode(sx, sz, p, mi, damping=d, enable_pp=False)
+        assert (o["est"] == est[t]).all() and o["iterations"] == res["iterations"][t], t
+
+
+def test_check_interval_schedule(decoder):
+    """--cuda-check-interval N: convergence is only tested on iterations warmup + kN or max_iter."""
+    from joint_bp_plus_pp_b200 import sample_reference_errors
+    p = 0.04
+    err = sample_reference_errors(decoder.n, 106, 1, 64, p)
+    _, base, _ = decoder.decode_errors(err, p, opts(max_iter=60), want_est=False)
+    _, res, _ = decoder.decode_errors(err, p, opts(max_iter=60, check_interval=4, check_warmup=2), want_est=False)
+    for b, r in zip(base, res):
+        if b["syndrome_ok"]:
+            it = r["iterations"]
+            assert it == 60 or (it > 2 and (it - 2) % 4 == 0)
+            assert it >= b["iterations"]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+def test_llr_precision_agreement(decoder, prec):
+    """FP32/FP16 LLR decoders against FP64 on the same reference-sampled errors at p=0.04."""
+    from joint_bp_plus_pp_b200 import sample_reference_errors
+    p, k = 0.04, 512
+    err = sample_reference_errors(decoder.n, 106, 1, k, p)
+    _, r64, e64 = decoder.decode_errors(err, p, opts(max_iter=200))
+    _, rlo, elo = decoder.decode_errors(err, p, opts(max_iter=200, precision=prec))
+    same = (e64 == elo).all(axis=1)
+    assert same.mean() >= 0.99, same.mean()
+    assert abs(int(r64["success"].sum()) - int(rlo["success"].sum())) <= 3
+    assert np.abs(r64["iterations"].astype(int) - rlo["iterations"].astype(int)).mean() < 0.5
+
+
+def test_device_mt_sampler_equals_host_reference_stream(decoder):
+    from joint_bp_plus_pp_b200 import sample_reference_errors
+    for seed, p in ((106, 0.04), (2 ** 64 - 3, 0.013)):
+        dev = decoder.sample_errors(seed, 1, 40, p, sampler="mt19937")
+        host = sample_reference_errors(decoder.n, seed, 1, 40, p)
+        assert (dev == host).all()
+
+
+def test_philox_sampler_statistics(decoder):
+    """Device Philox errors: weights and X/Z/Y shares of i.i.d. depolarizing noise."""
+    p, k, n = 0.04, 4096, decoder.n
+    e = decoder.sample_errors(123, 1, k, p, sampler="philox")
+    w = (e != 0).sum(axis=1)
+    mean, sd = n * p, (n * p * (1 - p)) ** 0.5
+    assert abs(w.mean() - mean) < 5 * sd / k ** 0.5
+    assert abs(w.std() - sd) < 0.1 * sd
+    counts = np.array([(e == s).sum() for s in (1, 2, 3)], float)
+    frac = counts / counts.sum()
+    assert np.all(np.abs(frac - 1 / 3) < 5 * (1 / 3 * 2 / 3 / counts.sum()) ** 0.5)
+    assert (decoder.sample_errors(123, 1, k, p, sampler="philox") == e).all()       # deterministic
+    assert not (decoder.sample_errors(124, 1, 4, p, sampler="philox") == e[:4]).all()  # keyed by seed
+    assert (decoder.sample_errors(123, 11, 4, p, sampler="philox") == e[10:14]).all()  # keyed by trial index
+
+
+def test_simulate_counts_and_hist(decoder):
+    st, res = decoder.simulate(106, 2000, 0.04, opts(max_iter=1000, precision="fp32"), hist=True)
+    assert st["trials"] == 2000
+    assert st["total_iters"] == int(res["iterations"].sum())
+    assert int(st["hist"].sum()) == 2000
+    assert 7.0 < st["total_iters"] / 2000 < 12.0
+    assert st["failures"] <= 2
