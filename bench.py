@@ -310,7 +310,7 @@ def main():
                "d2h_bytes_per_step": E * 16, "path": "jbp_decode_errors (host errors, pinned) -> results to host"}
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and args.cpu_seconds > 0:
         cpu = cpu_reference_rate(args.p, args.max_iter, args.cpu_seconds)
 
     if dist is not None:

@@ -52,13 +52,13 @@ KernelSet kernels_for(int precision, bool damp) {
     KernelSet k;
     if (precision == JBP_PREC_FP64) {
         k.check = damp ? k_check_f64<DC, true> : k_check_f64<DC, false>;
-        k.var64 = damp ? k_var_f64<DV, true> : k_var_f64<DV, false>;
+        k.var64 = damp ? k_var_f64<DC, DV, true> : k_var_f64<DC, DV, false>;
     } else if (precision == JBP_PREC_FP32) {
         k.check = k_check_llr<float, DC>;
-        k.varllr = damp ? k_var_llr<float, DV, true> : k_var_llr<float, DV, false>;
+        k.varllr = damp ? k_var_llr<float, DC, DV, true> : k_var_llr<float, DC, DV, false>;
     } else {
         k.check = k_check_llr<__half, DC>;
-        k.varllr = damp ? k_var_llr<__half, DV, true> : k_var_llr<__half, DV, false>;
+        k.varllr = damp ? k_var_llr<__half, DC, DV, true> : k_var_llr<__half, DC, DV, false>;
     }
     return k;
 }
@@ -128,7 +128,8 @@ std::string Engine::init(CodeModel model, int device) {
 void Engine::free_buffers() {
     for (void *&p : buf_.msg) { cudaFree(p); p = nullptr; }
     cudaFree(buf_.trial); cudaFree(buf_.iter); cudaFree(buf_.flags); cudaFree(buf_.unsat);
-    cudaFree(buf_.prior); cudaFree(buf_.lprior); cudaFree(buf_.err); cudaFree(buf_.est); cudaFree(buf_.syn);
+    cudaFree(buf_.prior); cudaFree(buf_.lprior); cudaFree(buf_.err);
+    cudaFree(buf_.unsat_mask); cudaFree(buf_.estx); cudaFree(buf_.estz); cudaFree(buf_.synm);
     cudaFree(buf_.res_iters); cudaFree(buf_.res_flags); cudaFree(buf_.lists); cudaFree(buf_.counts);
     cudaFree(buf_.cnt);
     if (buf_.h_done) cudaFreeHost(buf_.h_done);
@@ -154,8 +155,12 @@ std::string Engine::ensure_buffers(int S, int precision, bool damp) {
     JBP_CUDA_TRY(cudaMalloc(&buf_.prior, sizeof(double) * 4 * S), "cudaMalloc(slots)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.lprior, sizeof(float) * 8 * S), "cudaMalloc(slots)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.err, static_cast<size_t>(n) * S), "cudaMalloc(err)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.est, static_cast<size_t>(n) * S), "cudaMalloc(est)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.syn, static_cast<size_t>(M) * S), "cudaMalloc(syn)");
+    const size_t G = static_cast<size_t>(S) / kGroup;
+    JBP_CUDA_TRY(cudaMalloc(&buf_.estx, sizeof(unsigned) * G * n), "cudaMalloc(est)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.estz, sizeof(unsigned) * G * n), "cudaMalloc(est)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.synm, sizeof(unsigned) * G * M), "cudaMalloc(syn)");
+    JBP_CUDA_TRY(cudaMemset(buf_.synm, 0, sizeof(unsigned) * G * M), "memset(syn)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.unsat_mask, sizeof(unsigned) * 2 * G), "cudaMalloc(unsat)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.res_iters, sizeof(int) * S), "cudaMalloc(slots)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.res_flags, sizeof(int) * S), "cudaMalloc(slots)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.lists, sizeof(int) * (3 * S)), "cudaMalloc(lists)");
@@ -225,8 +230,10 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     r.prior = buf_.prior;
     r.lprior = buf_.lprior;
     r.err = buf_.err;
-    r.est = buf_.est;
-    r.syn = buf_.syn;
+    r.estx = buf_.estx;
+    r.estz = buf_.estz;
+    r.synm = buf_.synm;
+    r.unsat_mask = buf_.unsat_mask;
     r.res_iters = buf_.res_iters;
     r.res_flags = buf_.res_flags;
     r.retired = buf_.lists;

@@ -73,12 +73,17 @@ struct DevRun {
     long long *trial;               // [S]
     int *iter;                      // [S] completed iterations
     int *flags;                     // [S]
-    int *unsat;                     // [2][S]
+    int *unsat;                     // [2][S] unsatisfied-check counts (kept when PP needs them)
+    unsigned *unsat_mask;           // [2][G] slots of a group with an unsatisfied check, per side
     double *prior;                  // [S][4] normalized prior (FP64 path)
     float *lprior;                  // [S][8] log prior x4, prior LLR x/z (FP32 path)
     uint8_t *err;                   // [S][n] true error of the slot's trial
-    uint8_t *est;                   // [n][S]
-    uint8_t *syn;                   // [(mx+mz)][S]
+    // Hard decisions as bit planes: bit (slot % 32) of estx[g * n + v] is the x-bit of
+    // variable v in slot g * 32 + slot % 32 (estz: the z-bit).  One 32-slot word per
+    // variable makes the syndrome test an XOR of words and keeps a group's decisions in
+    // one contiguous row.
+    unsigned *estx, *estz;          // [G][n]
+    unsigned *synm;                 // [(mx+mz)][G] target syndrome bits, same slot bit order
     int *res_iters;                 // [S] iterations at retirement
     int *res_flags;                 // [S] bit0 syndrome_ok, bit1 bp_ok
     // work lists

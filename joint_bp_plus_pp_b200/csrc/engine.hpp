@@ -50,9 +50,10 @@ private:
         void *msg[6] = {};            // c2v x/z, v2c x/z, v2c_hi x/z
         long long *trial = nullptr;
         int *iter = nullptr, *flags = nullptr, *unsat = nullptr;
+        unsigned *unsat_mask = nullptr, *estx = nullptr, *estz = nullptr, *synm = nullptr;
         double *prior = nullptr;
         float *lprior = nullptr;
-        uint8_t *err = nullptr, *est = nullptr, *syn = nullptr;
+        uint8_t *err = nullptr;
         int *res_iters = nullptr, *res_flags = nullptr;
         int *lists = nullptr;         // retired | fresh | groups
         int *counts = nullptr;        // n_retired, n_fresh, n_groups

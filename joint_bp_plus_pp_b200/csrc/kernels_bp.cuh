@@ -1,5 +1,10 @@
 // BP message kernels (check and variable updates) for the three precisions.
 //
+// Message layout.  Edge e = c * dc + pos of a side (check-major, as the reference numbers
+// edges) of slot s = g * 32 + lane lives at ((c * G + g) * dc + pos) * 32 + lane, G = S / 32.
+// A check-node warp therefore reads and writes one contiguous block (dc x 32 messages);
+// a variable-node warp gathers dv such 32-message chunks per side.
+//
 // FP64 path: the reference CPU decoder's arithmetic, operation by operation
 // (jointbp_ets.cpp:2373-2519), with explicit round-to-nearest intrinsics so that the
 // compiler cannot contract a multiply and an add into an FMA.  Messages are kept in the
@@ -9,9 +14,12 @@
 //                                                 -> stored as (q0, q1)
 // With damping the full v2c 4-vector is kept, since scaled_mix needs the old message.
 //
-// FP32/FP16 path: log-likelihood ratios.  Check: sign product and the phi-sum rule
-// (phi(x) = -log tanh(x/2), its own inverse) over prefix/suffix sums; variable: sums of
-// incoming LLRs with the exact joint 4-ary coupling of the X and Z sides.
+// FP32/FP16 path: log-likelihood ratios in base 2 (y = log2(q0/q1)), so that the
+// exponentials and logarithms are single ex2/lg2 operations.  Check node: the tanh rule,
+// t = tanh(y ln2 / 2) = (1 - 2^-|y|) / (1 + 2^-|y|) with the sign of y, excluded products
+// from prefix/suffix passes, output lg2((1 + |T|) / (1 - |T|)) clamped (|T| -> 1 saturates
+// at about 25 in base 2); the syndrome bit flips the sign.  Variable node: sums of the
+// incoming LLRs and the exact joint 4-ary coupling of the X and Z sides.
 #pragma once
 
 #include <cuda_fp16.h>
@@ -38,47 +46,59 @@ __device__ __forceinline__ void norm4(double &m0, double &m1, double &m2, double
     m3 = ddiv(m3, s);
 }
 
-// Work item of a (row, group) loop: warps walk rows fastest, groups slowest.
-struct WarpItem {
-    int row, slot, lane;
-};
-
 __device__ __forceinline__ int warp_global_id() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }
 __device__ __forceinline__ int warps_total() { return (gridDim.x * blockDim.x) >> 5; }
+
+// Offset of message (edge e of a side with check degree DC, slot group g, lane).
+template <int DC>
+__device__ __forceinline__ size_t msg_off(int e, int G, int g, int lane) {
+    const int c = e / DC, pos = e - c * DC;
+    return ((static_cast<size_t>(c) * G + g) * DC + pos) * kGroup + lane;
+}
+
+// Hard decisions of one variable for the warp's 32 slots, as x-bit and z-bit planes.
+// Called by all lanes; lanes of slots that are not running contribute 0 bits.
+__device__ __forceinline__ void store_est_bits(const DevRun &run, int group, int n, int v, int best, bool active) {
+    const unsigned xm = __ballot_sync(0xffffffffu, active && (best & 1));
+    const unsigned zm = __ballot_sync(0xffffffffu, active && (best & 2));
+    const int lane = threadIdx.x & 31;
+    if (lane == 0) run.estx[static_cast<size_t>(group) * n + v] = xm;
+    if (lane == 1) run.estz[static_cast<size_t>(group) * n + v] = zm;
+}
 
 // ------------------------------------------------------------------ FP64, bit-exact
 
 template <int DC, bool DAMP>
 __global__ void __launch_bounds__(256) k_check_f64(DevCode code, DevRun run, DevMsgs msg) {
     const int lane = threadIdx.x & 31;
-    const int S = run.S;
+    const int G = run.S / kGroup;
     const int mx = code.s[0].m, M = mx + code.s[1].m;
-    const long long total = static_cast<long long>(*run.n_groups) * M;
-    for (long long w = warp_global_id(); w < total; w += warps_total()) {
-        const int gi = static_cast<int>(w / M);
-        const int row = static_cast<int>(w - static_cast<long long>(gi) * M);
-        const int slot = run.groups[gi] * kGroup + lane;
-        const int flags = run.flags[slot];
-        if (!(flags & kRunning)) continue;
+    const unsigned total = static_cast<unsigned>(*run.n_groups) * M;
+    for (unsigned w = warp_global_id(); w < total; w += warps_total()) {
+        const int gi = static_cast<int>(w / static_cast<unsigned>(M));
+        const int row = static_cast<int>(w - static_cast<unsigned>(gi) * M);
+        const int group = run.groups[gi];
+        const int slot = group * kGroup + lane;
+        if (!(run.flags[slot] & kRunning)) continue;
         const int side = row >= mx;
         const int ch = side ? row - mx : row;
         const bool fresh = run.iter[slot] == 0;
-        const double2 *v2c = static_cast<const double2 *>(msg.v2c[side]);
-        const double2 *v2c_hi = static_cast<const double2 *>(msg.v2c_hi[side]);
-        double2 *c2v = static_cast<double2 *>(msg.c2v[side]);
+        const size_t base = (static_cast<size_t>(ch) * G + group) * DC * kGroup + lane;
+        const double2 *v2c = static_cast<const double2 *>(side ? msg.v2c[1] : msg.v2c[0]) + base;
+        const double2 *v2c_hi = static_cast<const double2 *>(side ? msg.v2c_hi[1] : msg.v2c_hi[0]) + base;
+        double2 *c2v = static_cast<double2 *>(side ? msg.c2v[1] : msg.c2v[0]) + base;
         const double *pr = run.prior + 4 * slot;
         double q0[DC], q1[DC];
 #pragma unroll
         for (int i = 0; i < DC; ++i) {
-            const size_t idx = static_cast<size_t>(ch * DC + i) * S + slot;
             double m0, m1, m2, m3;
             if (fresh) {
                 m0 = pr[0]; m1 = pr[1]; m2 = pr[2]; m3 = pr[3];
             } else if (DAMP) {
-                double2 lo = v2c[idx], hi = v2c_hi[idx];
+                double2 lo = v2c[i * kGroup], hi = v2c_hi[i * kGroup];
                 m0 = lo.x; m1 = lo.y; m2 = hi.x; m3 = hi.y;
             } else {
-                double2 q = v2c[idx];
+                double2 q = v2c[i * kGroup];
                 q0[i] = q.x;
                 q1[i] = q.y;
                 continue;
@@ -94,7 +114,7 @@ __global__ void __launch_bounds__(256) k_check_f64(DevCode code, DevRun run, Dev
             se[i] = dadd(dmul(se[i + 1], q0[i]), dmul(so[i + 1], q1[i]));
             so[i] = dadd(dmul(se[i + 1], q1[i]), dmul(so[i + 1], q0[i]));
         }
-        const int s = run.syn[static_cast<size_t>(row) * S + slot];
+        const int s = (run.synm[static_cast<size_t>(row) * G + group] >> lane) & 1;
         double pe = 1.0, po = 0.0;
 #pragma unroll
         for (int i = 0; i < DC; ++i) {
@@ -111,7 +131,7 @@ __global__ void __launch_bounds__(256) k_check_f64(DevCode code, DevRun run, Dev
                 out.x = ddiv(v0, sum);
                 out.y = ddiv(v1, sum);
             }
-            c2v[static_cast<size_t>(ch * DC + i) * S + slot] = out;
+            c2v[i * kGroup] = out;
             const double ne = dadd(dmul(pe, q0[i]), dmul(po, q1[i]));
             const double no = dadd(dmul(pe, q1[i]), dmul(po, q0[i]));
             pe = ne;
@@ -146,83 +166,88 @@ __device__ __forceinline__ void store_v2c_f64(double2 *v2c, double2 *v2c_hi, siz
     }
 }
 
-template <int DV, bool DAMP>
+template <int DC, int DV, bool DAMP>
 __global__ void __launch_bounds__(256) k_var_f64(DevCode code, DevRun run, DevMsgs msg, double damping) {
     const int lane = threadIdx.x & 31;
-    const int S = run.S, n = code.n;
-    const long long total = static_cast<long long>(*run.n_groups) * n;
+    const int G = run.S / kGroup, n = code.n;
+    const unsigned total = static_cast<unsigned>(*run.n_groups) * n;
     const double2 *c2vx = static_cast<const double2 *>(msg.c2v[0]);
     const double2 *c2vz = static_cast<const double2 *>(msg.c2v[1]);
-    for (long long w = warp_global_id(); w < total; w += warps_total()) {
-        const int gi = static_cast<int>(w / n);
-        const int v = static_cast<int>(w - static_cast<long long>(gi) * n);
-        const int slot = run.groups[gi] * kGroup + lane;
-        if (!(run.flags[slot] & kRunning)) continue;
-        const bool fresh = run.iter[slot] == 0;
-        const double *pr = run.prior + 4 * slot;
-        const double p0 = pr[0], p1 = pr[1], p2 = pr[2], p3 = pr[3];
-        int ex[DV], ez[DV];
-        double ax[DV], bx[DV], az[DV], bz[DV];
-#pragma unroll
-        for (int k = 0; k < DV; ++k) {
-            ex[k] = code.s[0].var_edge[v * DV + k];
-            ez[k] = code.s[1].var_edge[v * DV + k];
-            const double2 cx = c2vx[static_cast<size_t>(ex[k]) * S + slot];
-            const double2 cz = c2vz[static_cast<size_t>(ez[k]) * S + slot];
-            ax[k] = cx.x; bx[k] = cx.y; az[k] = cz.x; bz[k] = cz.y;
-        }
-        // prefix / suffix products of the X messages (a, b, a, b) and Z messages (a, a, b, b)
-        double PA[DV + 1], PB[DV + 1], SA[DV + 1], SB[DV + 1];
-        double QA[DV + 1], QB[DV + 1], TA[DV + 1], TB[DV + 1];
-        PA[0] = PB[0] = QA[0] = QB[0] = 1.0;
-        SA[DV] = SB[DV] = TA[DV] = TB[DV] = 1.0;
-#pragma unroll
-        for (int k = 0; k < DV; ++k) {
-            PA[k + 1] = dmul(PA[k], ax[k]); PB[k + 1] = dmul(PB[k], bx[k]);
-            QA[k + 1] = dmul(QA[k], az[k]); QB[k + 1] = dmul(QB[k], bz[k]);
-        }
-#pragma unroll
-        for (int k = DV - 1; k >= 0; --k) {
-            SA[k] = dmul(SA[k + 1], ax[k]); SB[k] = dmul(SB[k + 1], bx[k]);
-            TA[k] = dmul(TA[k + 1], az[k]); TB[k] = dmul(TB[k + 1], bz[k]);
-        }
-        const double XA = PA[DV], XB = PB[DV], ZA = QA[DV], ZB = QB[DV];
-        // total = normalize(prior * (PX * PZ)); est = first argmax
-        double t0 = dmul(p0, dmul(XA, ZA)), t1 = dmul(p1, dmul(XB, ZA));
-        double t2 = dmul(p2, dmul(XA, ZB)), t3 = dmul(p3, dmul(XB, ZB));
-        norm4(t0, t1, t2, t3);
+    for (unsigned w = warp_global_id(); w < total; w += warps_total()) {
+        const int gi = static_cast<int>(w / static_cast<unsigned>(n));
+        const int v = static_cast<int>(w - static_cast<unsigned>(gi) * n);
+        const int group = run.groups[gi];
+        const int slot = group * kGroup + lane;
+        const bool active = run.flags[slot] & kRunning;
+        if (!__any_sync(0xffffffffu, active)) continue;
         int best = 0;
-        double bv = t0;
-        if (t1 > bv) { best = 1; bv = t1; }
-        if (t2 > bv) { best = 2; bv = t2; }
-        if (t3 > bv) { best = 3; }
-        run.est[static_cast<size_t>(v) * S + slot] = static_cast<uint8_t>(best);
-        double2 *v2cx = static_cast<double2 *>(msg.v2c[0]);
-        double2 *v2cz = static_cast<double2 *>(msg.v2c[1]);
-        double2 *v2cx_hi = static_cast<double2 *>(msg.v2c_hi[0]);
-        double2 *v2cz_hi = static_cast<double2 *>(msg.v2c_hi[1]);
+        if (active) {
+            const bool fresh = run.iter[slot] == 0;
+            const double *pr = run.prior + 4 * slot;
+            const double p0 = pr[0], p1 = pr[1], p2 = pr[2], p3 = pr[3];
+            size_t ox[DV], oz[DV];
+            double ax[DV], bx[DV], az[DV], bz[DV];
 #pragma unroll
-        for (int k = 0; k < DV; ++k) {
-            const double EA = dmul(PA[k], SA[k + 1]), EB = dmul(PB[k], SB[k + 1]);
-            double n0 = dmul(dmul(p0, EA), ZA), n1 = dmul(dmul(p1, EB), ZA);
-            double n2 = dmul(dmul(p2, EA), ZB), n3 = dmul(dmul(p3, EB), ZB);
-            norm4(n0, n1, n2, n3);
-            store_v2c_f64<DAMP>(v2cx, v2cx_hi, static_cast<size_t>(ex[k]) * S + slot, 0, n0, n1, n2, n3, fresh, pr,
-                                damping);
-        }
+            for (int k = 0; k < DV; ++k) {
+                ox[k] = msg_off<DC>(__ldg(code.s[0].var_edge + v * DV + k), G, group, lane);
+                oz[k] = msg_off<DC>(__ldg(code.s[1].var_edge + v * DV + k), G, group, lane);
+            }
 #pragma unroll
-        for (int k = 0; k < DV; ++k) {
-            const double FA = dmul(QA[k], TA[k + 1]), FB = dmul(QB[k], TB[k + 1]);
-            double n0 = dmul(dmul(p0, XA), FA), n1 = dmul(dmul(p1, XB), FA);
-            double n2 = dmul(dmul(p2, XA), FB), n3 = dmul(dmul(p3, XB), FB);
-            norm4(n0, n1, n2, n3);
-            store_v2c_f64<DAMP>(v2cz, v2cz_hi, static_cast<size_t>(ez[k]) * S + slot, 1, n0, n1, n2, n3, fresh, pr,
-                                damping);
+            for (int k = 0; k < DV; ++k) {
+                const double2 cx = c2vx[ox[k]];
+                const double2 cz = c2vz[oz[k]];
+                ax[k] = cx.x; bx[k] = cx.y; az[k] = cz.x; bz[k] = cz.y;
+            }
+            // prefix / suffix products of the X messages (a, b, a, b) and Z messages (a, a, b, b)
+            double PA[DV + 1], PB[DV + 1], SA[DV + 1], SB[DV + 1];
+            double QA[DV + 1], QB[DV + 1], TA[DV + 1], TB[DV + 1];
+            PA[0] = PB[0] = QA[0] = QB[0] = 1.0;
+            SA[DV] = SB[DV] = TA[DV] = TB[DV] = 1.0;
+#pragma unroll
+            for (int k = 0; k < DV; ++k) {
+                PA[k + 1] = dmul(PA[k], ax[k]); PB[k + 1] = dmul(PB[k], bx[k]);
+                QA[k + 1] = dmul(QA[k], az[k]); QB[k + 1] = dmul(QB[k], bz[k]);
+            }
+#pragma unroll
+            for (int k = DV - 1; k >= 0; --k) {
+                SA[k] = dmul(SA[k + 1], ax[k]); SB[k] = dmul(SB[k + 1], bx[k]);
+                TA[k] = dmul(TA[k + 1], az[k]); TB[k] = dmul(TB[k + 1], bz[k]);
+            }
+            const double XA = PA[DV], XB = PB[DV], ZA = QA[DV], ZB = QB[DV];
+            // total = normalize(prior * (PX * PZ)); est = first argmax
+            double t0 = dmul(p0, dmul(XA, ZA)), t1 = dmul(p1, dmul(XB, ZA));
+            double t2 = dmul(p2, dmul(XA, ZB)), t3 = dmul(p3, dmul(XB, ZB));
+            norm4(t0, t1, t2, t3);
+            double bv = t0;
+            if (t1 > bv) { best = 1; bv = t1; }
+            if (t2 > bv) { best = 2; bv = t2; }
+            if (t3 > bv) { best = 3; }
+            double2 *v2cx = static_cast<double2 *>(msg.v2c[0]);
+            double2 *v2cz = static_cast<double2 *>(msg.v2c[1]);
+            double2 *v2cx_hi = static_cast<double2 *>(msg.v2c_hi[0]);
+            double2 *v2cz_hi = static_cast<double2 *>(msg.v2c_hi[1]);
+#pragma unroll
+            for (int k = 0; k < DV; ++k) {
+                const double EA = dmul(PA[k], SA[k + 1]), EB = dmul(PB[k], SB[k + 1]);
+                double n0 = dmul(dmul(p0, EA), ZA), n1 = dmul(dmul(p1, EB), ZA);
+                double n2 = dmul(dmul(p2, EA), ZB), n3 = dmul(dmul(p3, EB), ZB);
+                norm4(n0, n1, n2, n3);
+                store_v2c_f64<DAMP>(v2cx, v2cx_hi, ox[k], 0, n0, n1, n2, n3, fresh, pr, damping);
+            }
+#pragma unroll
+            for (int k = 0; k < DV; ++k) {
+                const double FA = dmul(QA[k], TA[k + 1]), FB = dmul(QB[k], TB[k + 1]);
+                double n0 = dmul(dmul(p0, XA), FA), n1 = dmul(dmul(p1, XB), FA);
+                double n2 = dmul(dmul(p2, XA), FB), n3 = dmul(dmul(p3, XB), FB);
+                norm4(n0, n1, n2, n3);
+                store_v2c_f64<DAMP>(v2cz, v2cz_hi, oz[k], 1, n0, n1, n2, n3, fresh, pr, damping);
+            }
         }
+        store_est_bits(run, group, n, v, best, active);
     }
 }
 
-// ------------------------------------------------------------------ FP32 / FP16 LLR
+// ------------------------------------------------------------------ FP32 / FP16 LLR (base 2)
 
 template <typename T>
 __device__ __forceinline__ float ld_msg(const T *p);
@@ -237,22 +262,28 @@ __device__ __forceinline__ void st_msg<float>(float *p, float v) { *p = v; }
 template <>
 __device__ __forceinline__ void st_msg<__half>(__half *p, float v) { *p = __float2half_rn(v); }
 
-constexpr float kLlrMax = 30.0f;     // message LLR clamp
-constexpr float kPhiArgMin = 1e-12f; // phi(1e-12) ~ 28.3
+constexpr float kLlrMax = 43.0f;     // message clamp, base 2 (~30 in natural units)
 
-// phi(x) = log((1 + e^-x) / (1 - e^-x)) for x >= 0, an involution on (0, inf).
-__device__ __forceinline__ float phi_f(float x) {
-    x = fmaxf(x, kPhiArgMin);
-    if (x > 15.0f) return 2.0f * __expf(-x);
-    float t;  // 1 - e^-x without cancellation for small x
-    if (x < 0.1f) t = x * (1.0f - x * (0.5f - x * (0.16666667f - x * (0.041666668f - x * 0.008333334f))));
-    else t = 1.0f - __expf(-x);
-    return __logf(__fdividef(2.0f - t, t));
+// Single special-function-unit operations.
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float lg2_approx(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
 }
 
+// log2(2^a + 2^b)
 __device__ __forceinline__ float lse2(float a, float b) {
-    const float m = fmaxf(a, b);
-    return m + __logf(1.0f + __expf(-fabsf(a - b)));
+    return fmaxf(a, b) + lg2_approx(1.0f + ex2_approx(-fabsf(a - b)));
 }
 
 __device__ __forceinline__ float clamp_llr(float x) { return fminf(fmaxf(x, -kLlrMax), kLlrMax); }
@@ -260,102 +291,126 @@ __device__ __forceinline__ float clamp_llr(float x) { return fminf(fmaxf(x, -kLl
 template <typename T, int DC>
 __global__ void __launch_bounds__(256) k_check_llr(DevCode code, DevRun run, DevMsgs msg) {
     const int lane = threadIdx.x & 31;
-    const int S = run.S;
+    const int G = run.S / kGroup;
     const int mx = code.s[0].m, M = mx + code.s[1].m;
-    const long long total = static_cast<long long>(*run.n_groups) * M;
-    for (long long w = warp_global_id(); w < total; w += warps_total()) {
-        const int gi = static_cast<int>(w / M);
-        const int row = static_cast<int>(w - static_cast<long long>(gi) * M);
-        const int slot = run.groups[gi] * kGroup + lane;
+    const unsigned total = static_cast<unsigned>(*run.n_groups) * M;
+    for (unsigned w = warp_global_id(); w < total; w += warps_total()) {
+        const int gi = static_cast<int>(w / static_cast<unsigned>(M));
+        const int row = static_cast<int>(w - static_cast<unsigned>(gi) * M);
+        const int group = run.groups[gi];
+        const int slot = group * kGroup + lane;
         if (!(run.flags[slot] & kRunning)) continue;
         const int side = row >= mx;
         const int ch = side ? row - mx : row;
         const bool fresh = run.iter[slot] == 0;
-        const T *v2c = static_cast<const T *>(msg.v2c[side]);
-        T *c2v = static_cast<T *>(msg.c2v[side]);
+        const size_t base = (static_cast<size_t>(ch) * G + group) * DC * kGroup + lane;
+        const T *v2c = static_cast<const T *>(side ? msg.v2c[1] : msg.v2c[0]) + base;
+        T *c2v = static_cast<T *>(side ? msg.c2v[1] : msg.c2v[0]) + base;
         const float lp = run.lprior[8 * slot + 4 + side];
-        float a[DC];
-        unsigned neg = 0;
+        float t[DC];
 #pragma unroll
         for (int i = 0; i < DC; ++i) {
-            const float L = fresh ? lp : ld_msg<T>(v2c + static_cast<size_t>(ch * DC + i) * S + slot);
-            neg |= (L < 0.0f ? 1u : 0u) << i;
-            a[i] = phi_f(fabsf(L));
+            const float y = fresh ? lp : ld_msg<T>(v2c + i * kGroup);
+            const float u = ex2_approx(-fabsf(y));
+            t[i] = copysignf((1.0f - u) * rcp_approx(1.0f + u), y);
         }
         float suf[DC + 1];
-        suf[DC] = 0.0f;
+        suf[DC] = 1.0f;
 #pragma unroll
-        for (int i = DC - 1; i >= 0; --i) suf[i] = suf[i + 1] + a[i];
-        const unsigned par = (__popc(neg) & 1u) ^ static_cast<unsigned>(run.syn[static_cast<size_t>(row) * S + slot]);
-        float pre = 0.0f;
+        for (int i = DC - 1; i >= 0; --i) suf[i] = suf[i + 1] * t[i];
+        float pre = ((run.synm[static_cast<size_t>(row) * G + group] >> lane) & 1u) ? -1.0f : 1.0f;
 #pragma unroll
         for (int i = 0; i < DC; ++i) {
-            const float mag = fminf(phi_f(pre + suf[i + 1]), kLlrMax);
-            const unsigned sg = par ^ ((neg >> i) & 1u);
-            st_msg<T>(c2v + static_cast<size_t>(ch * DC + i) * S + slot, sg ? -mag : mag);
-            pre += a[i];
+            const float tt = pre * suf[i + 1];
+            const float a = fabsf(tt);
+            const float mag = fminf(lg2_approx((1.0f + a) * rcp_approx(1.0f - a)), kLlrMax);
+            st_msg<T>(c2v + i * kGroup, copysignf(mag, tt));
+            pre *= t[i];
         }
     }
 }
 
-__device__ __forceinline__ float sigm(float x) { return __fdividef(1.0f, 1.0f + __expf(-x)); }
+__device__ __forceinline__ float sigm2(float y) { return rcp_approx(1.0f + ex2_approx(-y)); }
 
-template <typename T, int DV, bool DAMP>
-__global__ void __launch_bounds__(256) k_var_llr(DevCode code, DevRun run, DevMsgs msg, float damping) {
-    const int lane = threadIdx.x & 31;
-    const int S = run.S, n = code.n;
-    const long long total = static_cast<long long>(*run.n_groups) * n;
+// One variable of the LLR variable update: sums of the incoming X and Z messages, hard
+// decision, and the extrinsic outputs with the 4-ary coupling of the two sides.
+template <typename T, int DC, int DV, bool DAMP>
+__device__ __forceinline__ int var_llr_one(const DevCode &code, const DevRun &run, const DevMsgs &msg, int v, int group,
+                                           int lane, float damping) {
+    const int G = run.S / kGroup;
+    const int slot = group * kGroup + lane;
     const T *c2vx = static_cast<const T *>(msg.c2v[0]);
     const T *c2vz = static_cast<const T *>(msg.c2v[1]);
     T *v2cx = static_cast<T *>(msg.v2c[0]);
     T *v2cz = static_cast<T *>(msg.v2c[1]);
-    for (long long w = warp_global_id(); w < total; w += warps_total()) {
-        const int gi = static_cast<int>(w / n);
-        const int v = static_cast<int>(w - static_cast<long long>(gi) * n);
-        const int slot = run.groups[gi] * kGroup + lane;
-        if (!(run.flags[slot] & kRunning)) continue;
-        int ex[DV], ez[DV];
-        float lx[DV], lz[DV];
-        float Lam = 0.0f, Mu = 0.0f;
+    size_t ox[DV], oz[DV];
+    float lx[DV], lz[DV];
 #pragma unroll
-        for (int k = 0; k < DV; ++k) {
-            ex[k] = code.s[0].var_edge[v * DV + k];
-            ez[k] = code.s[1].var_edge[v * DV + k];
-            lx[k] = ld_msg<T>(c2vx + static_cast<size_t>(ex[k]) * S + slot);
-            lz[k] = ld_msg<T>(c2vz + static_cast<size_t>(ez[k]) * S + slot);
+    for (int k = 0; k < DV; ++k) {
+        ox[k] = msg_off<DC>(__ldg(code.s[0].var_edge + v * DV + k), G, group, lane);
+        oz[k] = msg_off<DC>(__ldg(code.s[1].var_edge + v * DV + k), G, group, lane);
+    }
+#pragma unroll
+    for (int k = 0; k < DV; ++k) {
+        lx[k] = ld_msg<T>(c2vx + ox[k]);
+        lz[k] = ld_msg<T>(c2vz + oz[k]);
+    }
+    float Lam = 0.0f, Mu = 0.0f;
+#pragma unroll
+    for (int k = 0; k < DV; ++k) { Lam += lx[k]; Mu += lz[k]; }
+    const float4 lp = *reinterpret_cast<const float4 *>(run.lprior + 8 * slot);
+    // log2 weights of I, X, Z, Y up to a common constant; first maximum wins
+    const float w0 = lp.x, w1 = lp.y - Lam, w2 = lp.z - Mu, w3 = lp.w - Lam - Mu;
+    int best = 0;
+    float bv = w0;
+    if (w1 > bv) { best = 1; bv = w1; }
+    if (w2 > bv) { best = 2; bv = w2; }
+    if (w3 > bv) { best = 3; }
+    const float Gx = lse2(lp.x, lp.z - Mu) - lse2(lp.y, lp.w - Mu);   // x-bit coupling through Z
+    const float Hz = lse2(lp.x, lp.y - Lam) - lse2(lp.z, lp.w - Lam); // z-bit coupling through X
+#pragma unroll
+    for (int k = 0; k < DV; ++k) {
+        float ox_v = clamp_llr(Lam - lx[k] + Gx);
+        float oz_v = clamp_llr(Mu - lz[k] + Hz);
+        if (DAMP) {
+            // scaled_mix on the binary marginal: q0 = (1-d) q0_new + d q0_old
+            const bool fresh = run.iter[slot] == 0;
+            const float oldx = fresh ? run.lprior[8 * slot + 4] : ld_msg<T>(v2cx + ox[k]);
+            const float oldz = fresh ? run.lprior[8 * slot + 5] : ld_msg<T>(v2cz + oz[k]);
+            const float d = damping, e = 1.0f - damping;
+            const float qx0 = e * sigm2(ox_v) + d * sigm2(oldx), qx1 = e * sigm2(-ox_v) + d * sigm2(-oldx);
+            const float qz0 = e * sigm2(oz_v) + d * sigm2(oldz), qz1 = e * sigm2(-oz_v) + d * sigm2(-oldz);
+            ox_v = clamp_llr(lg2_approx(fmaxf(qx0, 1e-30f)) - lg2_approx(fmaxf(qx1, 1e-30f)));
+            oz_v = clamp_llr(lg2_approx(fmaxf(qz0, 1e-30f)) - lg2_approx(fmaxf(qz1, 1e-30f)));
         }
-#pragma unroll
-        for (int k = 0; k < DV; ++k) { Lam += lx[k]; Mu += lz[k]; }
-        const float *lp = run.lprior + 8 * slot;
-        // log weights of I, X, Z, Y up to a common constant; first maximum wins
-        const float w0 = lp[0], w1 = lp[1] - Lam, w2 = lp[2] - Mu, w3 = lp[3] - Lam - Mu;
-        int best = 0;
-        float bv = w0;
-        if (w1 > bv) { best = 1; bv = w1; }
-        if (w2 > bv) { best = 2; bv = w2; }
-        if (w3 > bv) { best = 3; }
-        run.est[static_cast<size_t>(v) * S + slot] = static_cast<uint8_t>(best);
-        const float G = lse2(lp[0], lp[2] - Mu) - lse2(lp[1], lp[3] - Mu);   // x-bit coupling through Z
-        const float H = lse2(lp[0], lp[1] - Lam) - lse2(lp[2], lp[3] - Lam); // z-bit coupling through X
-        const bool fresh = run.iter[slot] == 0;
-#pragma unroll
-        for (int k = 0; k < DV; ++k) {
-            float ox = clamp_llr(Lam - lx[k] + G);
-            float oz = clamp_llr(Mu - lz[k] + H);
-            T *px = v2cx + static_cast<size_t>(ex[k]) * S + slot;
-            T *pz = v2cz + static_cast<size_t>(ez[k]) * S + slot;
-            if (DAMP) {
-                const float oldx = fresh ? lp[4] : ld_msg<T>(px);
-                const float oldz = fresh ? lp[5] : ld_msg<T>(pz);
-                const float d = damping, e = 1.0f - damping;
-                const float qx0 = e * sigm(ox) + d * sigm(oldx), qx1 = e * sigm(-ox) + d * sigm(-oldx);
-                const float qz0 = e * sigm(oz) + d * sigm(oldz), qz1 = e * sigm(-oz) + d * sigm(-oldz);
-                ox = clamp_llr(__logf(fmaxf(qx0, 1e-30f)) - __logf(fmaxf(qx1, 1e-30f)));
-                oz = clamp_llr(__logf(fmaxf(qz0, 1e-30f)) - __logf(fmaxf(qz1, 1e-30f)));
-            }
-            st_msg<T>(px, ox);
-            st_msg<T>(pz, oz);
+        st_msg<T>(v2cx + ox[k], ox_v);
+        st_msg<T>(v2cz + oz[k], oz_v);
+    }
+    return best;
+}
+
+// Variable-node update over (variable pair, group) warp items: two variables per item keep
+// twelve independent message loads in flight per thread.
+template <typename T, int DC, int DV, bool DAMP>
+__global__ void __launch_bounds__(256) k_var_llr(DevCode code, DevRun run, DevMsgs msg, float damping) {
+    const int lane = threadIdx.x & 31;
+    const int n = code.n;
+    const int pairs = (n + 1) >> 1;
+    const unsigned total = static_cast<unsigned>(*run.n_groups) * pairs;
+    for (unsigned w = warp_global_id(); w < total; w += warps_total()) {
+        const int gi = static_cast<int>(w / static_cast<unsigned>(pairs));
+        const int v0 = 2 * static_cast<int>(w - static_cast<unsigned>(gi) * pairs);
+        const int group = run.groups[gi];
+        const bool active = run.flags[group * kGroup + lane] & kRunning;
+        if (!__any_sync(0xffffffffu, active)) continue;
+        int b0 = 0, b1 = 0;
+        const bool has1 = v0 + 1 < n;
+        if (active) {
+            b0 = var_llr_one<T, DC, DV, DAMP>(code, run, msg, v0, group, lane, damping);
+            if (has1) b1 = var_llr_one<T, DC, DV, DAMP>(code, run, msg, v0 + 1, group, lane, damping);
         }
+        store_est_bits(run, group, n, v0, b0, active);
+        if (has1) store_est_bits(run, group, n, v0 + 1, b1, active);
     }
 }
 

@@ -47,33 +47,47 @@ __device__ __forceinline__ uint8_t sample_philox(unsigned long long seed, long l
 
 // ------------------------------------------------------------------ per-iteration kernels
 
-// Hard-decision syndrome of every running slot that is due a check: unsatisfied checks
-// are counted per slot and side (jointbp_ets.cpp:2521-2525; check schedule of
-// jointbp_cuda.cu:971-975).
+// Whether iteration k1 (1-based) of a slot ends with a syndrome test: always at max_iter,
+// else every check_interval iterations after check_warmup (jointbp_cuda.cu:971-975; the
+// defaults 0 and 1 test every iteration as the CPU decoder does).
+__device__ __forceinline__ bool check_due(const DevRun &run, int k1) {
+    return k1 >= run.max_iter || (k1 > run.check_warmup && (k1 - run.check_warmup) % run.check_interval == 0);
+}
+
+// Hard-decision syndrome test (jointbp_ets.cpp:2521-2525) on bit planes.  A warp takes one
+// group and 32 consecutive check rows: lane r XORs the decision words of its row's
+// variables, which gives the row's parity for all 32 slots at once; slots whose parity
+// differs from the target are OR-ed into the group's unsatisfied mask of that side.
 __global__ void __launch_bounds__(256) k_syndrome_check(DevCode code, DevRun run) {
     const int lane = threadIdx.x & 31;
-    const int S = run.S;
+    const int n = code.n, G = run.S / kGroup;
     const int mx = code.s[0].m, M = mx + code.s[1].m;
-    const long long total = static_cast<long long>(*run.n_groups) * M;
-    for (long long w = warp_global_id(); w < total; w += warps_total()) {
-        const int gi = static_cast<int>(w / M);
-        const int row = static_cast<int>(w - static_cast<long long>(gi) * M);
-        const int slot = run.groups[gi] * kGroup + lane;
-        if (!(run.flags[slot] & kRunning)) continue;
-        const int k1 = run.iter[slot] + 1;
-        const bool due = k1 >= run.max_iter ||
-                         (k1 > run.check_warmup && (k1 - run.check_warmup) % run.check_interval == 0);
-        if (!due) continue;
-        const int side = row >= mx;
-        const int ch = side ? row - mx : row;
-        const DevSide &g = code.s[side];
-        int par = 0;
-        for (int i = 0; i < g.dc; ++i) {
-            const int v = g.chk_var[ch * g.dc + i];
-            const int s = run.est[static_cast<size_t>(v) * S + slot];
-            par ^= side ? zbit(s) : xbit(s);
+    const int blocks = (M + 31) >> 5;
+    const unsigned total = static_cast<unsigned>(*run.n_groups) * blocks;
+    for (unsigned w = warp_global_id(); w < total; w += warps_total()) {
+        const int gi = static_cast<int>(w / static_cast<unsigned>(blocks));
+        const int rb = static_cast<int>(w - static_cast<unsigned>(gi) * blocks);
+        const int group = run.groups[gi];
+        const int slot = group * kGroup + lane;
+        const bool due = (run.flags[slot] & kRunning) && check_due(run, run.iter[slot] + 1);
+        const unsigned due_mask = __ballot_sync(0xffffffffu, due);
+        if (!due_mask) continue;
+        const int row = rb * 32 + lane;
+        unsigned mm[2] = {0u, 0u};
+        if (row < M) {
+            const int side = row >= mx;
+            const int ch = side ? row - mx : row;
+            const int dc = side ? code.s[1].dc : code.s[0].dc;
+            const int *chk_var = side ? code.s[1].chk_var : code.s[0].chk_var;
+            const unsigned *planes = (side ? run.estz : run.estx) + static_cast<size_t>(group) * n;
+            unsigned par = 0;
+            for (int i = 0; i < dc; ++i) par ^= planes[__ldg(chk_var + ch * dc + i)];
+            mm[side] = (par ^ run.synm[static_cast<size_t>(row) * G + group]) & due_mask;
         }
-        if (par != run.syn[static_cast<size_t>(row) * S + slot]) atomicAdd(&run.unsat[side * S + slot], 1);
+        const unsigned ux = __reduce_or_sync(0xffffffffu, mm[0]);
+        const unsigned uz = __reduce_or_sync(0xffffffffu, mm[1]);
+        if (lane == 0 && ux) atomicOr(&run.unsat_mask[group], ux);
+        if (lane == 1 && uz) atomicOr(&run.unsat_mask[G + group], uz);
     }
 }
 
@@ -82,16 +96,20 @@ __global__ void __launch_bounds__(256) k_syndrome_check(DevCode code, DevRun run
 __global__ void k_retire(DevRun run) {
     const int gi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (gi >= *run.n_groups) return;
-    const int slot = run.groups[gi] * kGroup + (threadIdx.x & 31);
+    const int lane = threadIdx.x & 31;
+    const int group = run.groups[gi];
+    const int slot = group * kGroup + lane;
+    const int G = run.S / kGroup;
+    const unsigned bad = run.unsat_mask[group] | run.unsat_mask[G + group];
+    __syncwarp();
+    if (lane == 0) {
+        run.unsat_mask[group] = 0u;
+        run.unsat_mask[G + group] = 0u;
+    }
     if (!(run.flags[slot] & kRunning)) return;
-    const int S = run.S;
     const int k1 = run.iter[slot] + 1;
     run.iter[slot] = k1;
-    const bool due = k1 >= run.max_iter ||
-                     (k1 > run.check_warmup && (k1 - run.check_warmup) % run.check_interval == 0);
-    const bool conv = due && run.unsat[slot] == 0 && run.unsat[S + slot] == 0;
-    run.unsat[slot] = 0;
-    run.unsat[S + slot] = 0;
+    const bool conv = check_due(run, k1) && !((bad >> lane) & 1u);
     if (conv || k1 >= run.max_iter) {
         run.res_iters[slot] = k1;
         run.res_flags[slot] = conv ? 3 : 0;
@@ -135,7 +153,7 @@ __global__ void k_classify(DevCode code, DevRun run) {
     uint64_t *dx = smem_words + static_cast<size_t>(wib) * 2 * words;
     uint64_t *dz = dx + words;
     const int nret = *run.n_retired;
-    const int n = code.n, S = run.S;
+    const int n = code.n;
     const bool have_err = run.source != kSrcSyndromes;
     for (int r = blockIdx.x * wpb + wib; r < nret; r += gridDim.x * wpb) {
         const int slot = run.retired[r];
@@ -146,19 +164,37 @@ __global__ void k_classify(DevCode code, DevRun run) {
         __syncwarp();
         bool exact = true;
         const uint8_t *err = run.err + static_cast<size_t>(slot) * n;
-        for (int base = 0; base < n; base += 32) {
-            const int v = base + lane;
-            const bool in = v < n;
-            const int e = in ? run.est[static_cast<size_t>(v) * S + slot] : 0;
-            const int t = (in && have_err) ? err[v] : e;
-            if (in && run.est_out) run.est_out[local * n + v] = static_cast<uint8_t>(e);
-            if (t != e) exact = false;
-            const unsigned bx = __ballot_sync(0xffffffffu, xbit(t) != xbit(e));
-            const unsigned bz = __ballot_sync(0xffffffffu, zbit(t) != zbit(e));
-            if (lane == 0) {
-                const int sh = base & 32;  // which half of the 64-bit word
-                dx[base >> 6] |= static_cast<uint64_t>(bx) << sh;
-                dz[base >> 6] |= static_cast<uint64_t>(bz) << sh;
+        const unsigned *px = run.estx + static_cast<size_t>(slot / kGroup) * n;
+        const unsigned *pz = run.estz + static_cast<size_t>(slot / kGroup) * n;
+        const int bit = slot % kGroup;
+        constexpr int U = 8;  // chunks of 32 variables whose loads are issued together
+        for (int base0 = 0; base0 < n; base0 += 32 * U) {
+            unsigned xw[U], zw[U];
+            int tv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int v = base0 + u * 32 + lane;
+                const bool in = v < n;
+                xw[u] = in ? px[v] : 0u;
+                zw[u] = in ? pz[v] : 0u;
+                tv[u] = (in && have_err) ? err[v] : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int base = base0 + u * 32;
+                const int v = base + lane;
+                const bool in = v < n;
+                const int e = in ? static_cast<int>(((xw[u] >> bit) & 1u) | (((zw[u] >> bit) & 1u) << 1)) : 0;
+                const int t = tv[u] >= 0 ? tv[u] : e;
+                if (in && run.est_out) run.est_out[local * n + v] = static_cast<uint8_t>(e);
+                if (t != e) exact = false;
+                const unsigned bx = __ballot_sync(0xffffffffu, xbit(t) != xbit(e));
+                const unsigned bz = __ballot_sync(0xffffffffu, zbit(t) != zbit(e));
+                if (lane == 0 && base < n) {
+                    const int sh = base & 32;  // which half of the 64-bit word
+                    dx[base >> 6] |= static_cast<uint64_t>(bx) << sh;
+                    dz[base >> 6] |= static_cast<uint64_t>(bz) << sh;
+                }
             }
         }
         exact = __all_sync(0xffffffffu, exact) && have_err;
@@ -222,13 +258,14 @@ __global__ void k_refill(DevRun run, int precision) {
                 double *pr = run.prior + 4 * slot;
                 pr[0] = p0; pr[1] = p1; pr[2] = p2; pr[3] = p3;
             } else {
+                // base-2 log prior and the prior LLRs (base 2) that seed fresh v2c messages
                 float *lp = run.lprior + 8 * slot;
-                lp[0] = static_cast<float>(log(p0));
-                lp[1] = static_cast<float>(log(p1));
-                lp[2] = static_cast<float>(log(p2));
-                lp[3] = static_cast<float>(log(p3));
-                lp[4] = static_cast<float>(log((p0 + p2) / (p1 + p3)));   // v2c prior LLR of an x-bit
-                lp[5] = static_cast<float>(log((p0 + p1) / (p2 + p3)));   // v2c prior LLR of a z-bit
+                lp[0] = static_cast<float>(log2(p0));
+                lp[1] = static_cast<float>(log2(p1));
+                lp[2] = static_cast<float>(log2(p2));
+                lp[3] = static_cast<float>(log2(p3));
+                lp[4] = static_cast<float>(log2((p0 + p2) / (p1 + p3)));   // x-bit
+                lp[5] = static_cast<float>(log2((p0 + p1) / (p2 + p3)));   // z-bit
                 lp[6] = lp[7] = 0.0f;
             }
             run.fresh[atomicAdd(run.n_fresh, 1)] = slot;
@@ -362,16 +399,20 @@ __global__ void k_fresh_syndrome(DevCode code, DevRun run) {
             bit = side ? run.src_sz[local * code.s[1].m + ch] : run.src_sx[local * mx + ch];
             bit &= 1;
         } else {
-            const DevSide &g = code.s[side];
+            const int dc = side ? code.s[1].dc : code.s[0].dc;
+            const int *chk_var = side ? code.s[1].chk_var : code.s[0].chk_var;
             const uint8_t *err = run.err + static_cast<size_t>(slot) * n;
             int par = 0;
-            for (int k = 0; k < g.dc; ++k) {
-                const int s = err[g.chk_var[ch * g.dc + k]];
+            for (int k = 0; k < dc; ++k) {
+                const int s = err[chk_var[ch * dc + k]];
                 par ^= side ? zbit(s) : xbit(s);
             }
             bit = static_cast<uint8_t>(par);
         }
-        run.syn[static_cast<size_t>(row) * S + slot] = bit;
+        unsigned *word = run.synm + static_cast<size_t>(row) * (S / kGroup) + slot / kGroup;
+        const unsigned m = 1u << (slot % kGroup);
+        if (bit) atomicOr(word, m);
+        else atomicAnd(word, ~m);
     }
 }
 
@@ -392,6 +433,7 @@ __global__ void k_init_slots(DevRun run) {
         run.iter[s] = 0;
         run.unsat[s] = 0;
         run.unsat[run.S + s] = 0;
+        if (s < 2 * (run.S / kGroup)) run.unsat_mask[s] = 0u;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *run.n_retired = run.S;
 }

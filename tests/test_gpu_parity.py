@@ -119,6 +119,22 @@ def test_llr_precision_agreement(decoder, prec):
     assert np.abs(r64["iterations"].astype(int) - rlo["iterations"].astype(int)).mean() < 0.5
 
 
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+def test_llr_precision_ler_not_worse(decoder, prec):
+    """Logical error rate of the LLR decoders is not worse than FP64 within the 95% Wilson
+    interval, on the same 8192 reference-sampled errors at p=0.05, max-iter 50 (~3% FER)."""
+    from joint_bp_plus_pp_b200 import sample_reference_errors, wilson_interval
+    p, k, mi = 0.05, 8192, 50
+    err = sample_reference_errors(decoder.n, 2024, 1, k, p)
+    s64, r64, _ = decoder.decode_errors(err, p, opts(max_iter=mi), want_est=False)
+    slo, rlo, _ = decoder.decode_errors(err, p, opts(max_iter=mi, precision=prec), want_est=False)
+    lo64, hi64 = wilson_interval(k, s64["failures"])
+    assert s64["failures"] > 50
+    assert slo["failures"] / k <= hi64, (slo["failures"], s64["failures"])
+    # per-trial outcome disagreement stays small
+    assert (r64["success"] != rlo["success"]).mean() < 0.02
+
+
 def test_device_mt_sampler_equals_host_reference_stream(decoder):
     from joint_bp_plus_pp_b200 import sample_reference_errors
     for seed, p in ((106, 0.04), (2 ** 64 - 3, 0.013)):
