@@ -8,25 +8,8 @@
 #include <vector>
 
 #include "../../include/jbp_b200.h"
+#include "ctx.hpp"
 #include "engine.hpp"
-
-struct jbp_ctx {
-    jbp::Engine engine;
-    // cached device staging for host-buffer calls
-    uint8_t *d_in = nullptr, *d_in2 = nullptr, *d_est = nullptr;
-    size_t in_bytes = 0, in2_bytes = 0, est_bytes = 0;
-    jbp_trial_result *d_res = nullptr;
-    size_t res_count = 0;
-    unsigned long long *d_hist = nullptr;
-    size_t hist_count = 0;
-    ~jbp_ctx() {
-        cudaFree(d_in);
-        cudaFree(d_in2);
-        cudaFree(d_est);
-        cudaFree(d_res);
-        cudaFree(d_hist);
-    }
-};
 
 namespace {
 
@@ -81,6 +64,8 @@ int finish_create(jbp::CodeModel &&m, const std::string &ets_dir, int device, jb
 }
 
 }  // namespace
+
+int jbp::set_last_error(int code, const std::string &msg) { return fail(code, msg); }
 
 extern "C" {
 

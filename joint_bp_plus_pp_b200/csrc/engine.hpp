@@ -41,6 +41,8 @@ public:
     // Device sampler output (trial-major) into a device buffer.
     std::string sample_errors(unsigned long long seed, long long first, long long count, double p, int source,
                               uint8_t *d_out);
+    const DevCode &dev_code() const { return dcode_; }
+    int sm_count() const { return sm_count_; }
 
 private:
     struct Buffers {

@@ -58,7 +58,7 @@ __device__ __forceinline__ bool check_due(const DevRun &run, int k1) {
 // group and 32 consecutive check rows: lane r XORs the decision words of its row's
 // variables, which gives the row's parity for all 32 slots at once; slots whose parity
 // differs from the target are OR-ed into the group's unsatisfied mask of that side.
-__global__ void __launch_bounds__(256) k_syndrome_check(DevCode code, DevRun run) {
+static __global__ void __launch_bounds__(256) k_syndrome_check(DevCode code, DevRun run) {
     const int lane = threadIdx.x & 31;
     const int n = code.n, G = run.S / kGroup;
     const int mx = code.s[0].m, M = mx + code.s[1].m;
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(256) k_syndrome_check(DevCode code, DevRun run
 
 // Counts the finished iteration; a slot retires when its checked syndrome matches or it
 // reaches max_iter (the CPU's iteration accounting, jointbp_ets.cpp:2733-2735, 3078).
-__global__ void k_retire(DevRun run) {
+static __global__ void k_retire(DevRun run) {
     const int gi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (gi >= *run.n_groups) return;
     const int lane = threadIdx.x & 31;
@@ -122,7 +122,7 @@ __global__ void k_retire(DevRun run) {
 // in echelon form by its highest bits (in_row_space, jointbp_ets.cpp:904-920): repeatedly
 // clear the highest set bit with the basis row that has it as pivot; a bit with no such
 // row means the vector is outside the space.  vec is destroyed.
-__device__ bool warp_in_row_space(uint64_t *vec, int words, const uint64_t *rows, const int *pivot_row) {
+static __device__ bool warp_in_row_space(uint64_t *vec, int words, const uint64_t *rows, const int *pivot_row) {
     const int lane = threadIdx.x & 31;
     for (int guard = 0; guard < 1 << 20; ++guard) {
         int hw = -1;
@@ -145,7 +145,7 @@ __device__ bool warp_in_row_space(uint64_t *vec, int words, const uint64_t *rows
 // Classifies each retired trial (jointbp_ets.cpp:6199-6245): exact match, stabilizer
 // equivalence of the residual (x-part in rowspace(Hz), z-part in rowspace(Hx)), success;
 // writes the per-trial record and estimate and updates the run counters.
-__global__ void k_classify(DevCode code, DevRun run) {
+static __global__ void k_classify(DevCode code, DevRun run) {
     extern __shared__ uint64_t smem_words[];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
@@ -240,7 +240,7 @@ __global__ void k_classify(DevCode code, DevRun run) {
 }
 
 // Hands the next trials of the source to the retired (or never used) slots.
-__global__ void k_refill(DevRun run, int precision) {
+static __global__ void k_refill(DevRun run, int precision) {
     const int nret = *run.n_retired;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nret; r += gridDim.x * blockDim.x) {
         const int slot = run.retired[r];
@@ -277,7 +277,7 @@ __global__ void k_refill(DevRun run, int precision) {
 }
 
 // Errors of fresh trials: Philox, or copied from a device buffer of known errors.
-__global__ void k_sample(DevCode code, DevRun run) {
+static __global__ void k_sample(DevCode code, DevRun run) {
     const int nf = *run.n_fresh;
     const int n = code.n;
     const long long total = static_cast<long long>(nf) * n;
@@ -299,7 +299,7 @@ __global__ void k_sample(DevCode code, DevRun run) {
 // per warp; s is the warp's 312-word state.  The twist runs in two dependency-free halves:
 // words 0..155 read only words of the previous block, words 156..311 read words 0..155 of
 // this block.
-__device__ void warp_mt_trial(unsigned long long *s, unsigned long long base_seed, long long t, double p, int n,
+static __device__ void warp_mt_trial(unsigned long long *s, unsigned long long base_seed, long long t, double p, int n,
                               uint8_t *out) {
     const int lane = threadIdx.x & 31;
     const unsigned long long seed =
@@ -352,7 +352,7 @@ __device__ void warp_mt_trial(unsigned long long *s, unsigned long long base_see
     }
 }
 
-__global__ void k_sample_mt(DevCode code, DevRun run) {
+static __global__ void k_sample_mt(DevCode code, DevRun run) {
     __shared__ unsigned long long st[8][312];
     const int wib = threadIdx.x >> 5;
     const int nf = *run.n_fresh;
@@ -363,7 +363,7 @@ __global__ void k_sample_mt(DevCode code, DevRun run) {
 }
 
 // Errors of trials first..first+count-1 written trial-major (jbp_sample_errors).
-__global__ void k_sample_out(int n, unsigned long long seed, long long first, long long count, double p, int sampler,
+static __global__ void k_sample_out(int n, unsigned long long seed, long long first, long long count, double p, int sampler,
                              uint8_t *out) {
     __shared__ unsigned long long st[8][312];
     if (sampler == kSrcMt19937) {
@@ -381,7 +381,7 @@ __global__ void k_sample_out(int n, unsigned long long seed, long long first, lo
 }
 
 // Syndromes of fresh trials, from their errors or copied from the source.
-__global__ void k_fresh_syndrome(DevCode code, DevRun run) {
+static __global__ void k_fresh_syndrome(DevCode code, DevRun run) {
     const int nf = *run.n_fresh;
     const int mx = code.s[0].m, M = mx + code.s[1].m;
     const int n = code.n, S = run.S;
@@ -417,7 +417,7 @@ __global__ void k_fresh_syndrome(DevCode code, DevRun run) {
 }
 
 // Compacts the groups that still hold a running slot.
-__global__ void k_groups(DevRun run) {
+static __global__ void k_groups(DevRun run) {
     const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (g >= run.S / kGroup) return;
     const int lane = threadIdx.x & 31;
@@ -425,7 +425,7 @@ __global__ void k_groups(DevRun run) {
     if (any && lane == 0) run.groups[atomicAdd(run.n_groups, 1)] = g;
 }
 
-__global__ void k_init_slots(DevRun run) {
+static __global__ void k_init_slots(DevRun run) {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < run.S; s += gridDim.x * blockDim.x) {
         run.retired[s] = s;
         run.flags[s] = 0;

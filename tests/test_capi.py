@@ -19,6 +19,7 @@ LIBDIR = ROOT / "joint_bp_plus_pp_b200" / "lib"
 def declared_functions(header):
     text = re.sub(r"/\*.*?\*/", "", header.read_text(), flags=re.S)
     text = re.sub(r"//[^\n]*", "", text)
+    text = re.sub(r"^\s*#[^\n]*", "", text, flags=re.M)
     names = re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\([^;{]*\)\s*;", text)
     return sorted(set(n for n in names if not n.startswith("__")))
 
