@@ -8,6 +8,7 @@
 
 #include "kernels_bp.cuh"
 #include "kernels_slots.cuh"
+#include "kernels_pp.cuh"
 
 namespace jbp {
 
@@ -88,6 +89,7 @@ size_t msg_elem_bytes(int precision) {
 Engine::~Engine() {
     free_buffers();
     for (void *p : code_allocs_) cudaFree(p);
+    for (void *p : ets_allocs_) cudaFree(p);
 }
 
 std::string Engine::init(CodeModel model, int device) {
@@ -132,12 +134,54 @@ void Engine::free_buffers() {
     cudaFree(buf_.unsat_mask); cudaFree(buf_.estx); cudaFree(buf_.estz); cudaFree(buf_.synm);
     cudaFree(buf_.res_iters); cudaFree(buf_.res_flags); cudaFree(buf_.lists); cudaFree(buf_.counts);
     cudaFree(buf_.cnt);
+    cudaFree(buf_.it);
+    cudaFree(buf_.llr); cudaFree(buf_.act_k); cudaFree(buf_.pstate); cudaFree(buf_.stall_same);
+    cudaFree(buf_.pp_list); cudaFree(buf_.pp_mode); cudaFree(buf_.us_hist); cudaFree(buf_.dprev);
+    cudaFree(buf_.dpprev); cudaFree(buf_.pp_scratch);
     if (buf_.h_done) cudaFreeHost(buf_.h_done);
     buf_ = Buffers{};
 }
 
-std::string Engine::ensure_buffers(int S, int precision, bool damp) {
-    if (buf_.S == S && buf_.precision == precision && buf_.damp == damp) return "";
+// Flattens the loaded ETS groups into device arrays (DevEts), in load order.
+std::string Engine::upload_ets() {
+    if (ets_uploaded_ == model_.ets.size()) return "";
+    for (void *p : ets_allocs_) cudaFree(p);
+    ets_allocs_.clear();
+    dets_ = DevEts{};
+    if (model_.ets.size() > static_cast<size_t>(kMaxEtsGroups)) return "too many ETS groups";
+    std::vector<unsigned long long> keys;
+    std::vector<int> vars, var_first;
+    dets_.ngroups = static_cast<int>(model_.ets.size());
+    for (int g = 0; g < dets_.ngroups; ++g) {
+        const EtsGroup &grp = model_.ets[g];
+        dets_.size[g] = grp.size;
+        for (int s = 0; s < 2; ++s) {
+            dets_.first[g][s] = static_cast<int>(keys.size());
+            dets_.count[g][s] = grp.loaded[s] ? grp.tab[s].count() : 0;
+            if (!grp.loaded[s]) continue;
+            for (int e = 0; e < grp.tab[s].count(); ++e) {
+                keys.push_back(grp.tab[s].key[e]);
+                var_first.push_back(static_cast<int>(vars.size()));
+                const int *v = grp.tab[s].vars.data() + static_cast<size_t>(e) * grp.tab[s].var_count;
+                vars.insert(vars.end(), v, v + grp.tab[s].var_count);
+            }
+        }
+    }
+    unsigned long long *dk = nullptr;
+    int *dv = nullptr, *df = nullptr;
+    std::string e = dev_upload(ets_allocs_, keys, &dk);
+    if (e.empty()) e = dev_upload(ets_allocs_, vars, &dv);
+    if (e.empty()) e = dev_upload(ets_allocs_, var_first, &df);
+    if (!e.empty()) return e;
+    dets_.key = dk;
+    dets_.vars = dv;
+    dets_.var_first = df;
+    ets_uploaded_ = model_.ets.size();
+    return "";
+}
+
+std::string Engine::ensure_buffers(int S, int precision, bool damp, bool pp, int R) {
+    if (buf_.S == S && buf_.precision == precision && buf_.damp == damp && buf_.pp == pp && buf_.R == R) return "";
     free_buffers();
     const int n = model_.n, M = model_.side[0].m + model_.side[1].m;
     const size_t es = msg_elem_bytes(precision);
@@ -156,8 +200,26 @@ std::string Engine::ensure_buffers(int S, int precision, bool damp) {
     JBP_CUDA_TRY(cudaMalloc(&buf_.lprior, sizeof(float) * 8 * S), "cudaMalloc(slots)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.err, static_cast<size_t>(n) * S), "cudaMalloc(err)");
     const size_t G = static_cast<size_t>(S) / kGroup;
-    JBP_CUDA_TRY(cudaMalloc(&buf_.estx, sizeof(unsigned) * G * n), "cudaMalloc(est)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.estz, sizeof(unsigned) * G * n), "cudaMalloc(est)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.estx, sizeof(unsigned) * R * G * n), "cudaMalloc(est)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.estz, sizeof(unsigned) * R * G * n), "cudaMalloc(est)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.it, sizeof(int)), "cudaMalloc(it)");
+    if (pp) {
+        const int mmax = std::max(model_.side[0].m, model_.side[1].m);
+        JBP_CUDA_TRY(cudaMalloc(&buf_.llr, sizeof(double) * 2 * S * n), "cudaMalloc(llr)");
+        JBP_CUDA_TRY(cudaMalloc(&buf_.act_k, sizeof(int) * S), "cudaMalloc(pp)");
+        JBP_CUDA_TRY(cudaMalloc(&buf_.pstate, sizeof(int) * S), "cudaMalloc(pp)");
+        JBP_CUDA_TRY(cudaMalloc(&buf_.stall_same, sizeof(int) * S), "cudaMalloc(pp)");
+        JBP_CUDA_TRY(cudaMalloc(&buf_.pp_list, sizeof(int) * S), "cudaMalloc(pp)");
+        JBP_CUDA_TRY(cudaMalloc(&buf_.pp_mode, sizeof(int) * S), "cudaMalloc(pp)");
+        JBP_CUDA_TRY(cudaMalloc(&buf_.us_hist, sizeof(unsigned short) * 100 * S), "cudaMalloc(pp)");
+        JBP_CUDA_TRY(cudaMalloc(&buf_.dprev, sizeof(unsigned) * G), "cudaMalloc(pp)");
+        JBP_CUDA_TRY(cudaMalloc(&buf_.dpprev, sizeof(unsigned) * G), "cudaMalloc(pp)");
+        JBP_CUDA_TRY(cudaMemset(buf_.dprev, 0, sizeof(unsigned) * G), "memset(pp)");
+        JBP_CUDA_TRY(cudaMemset(buf_.dpprev, 0, sizeof(unsigned) * G), "memset(pp)");
+        buf_.pp_stride = pp_scratch_bytes(n, mmax);
+        buf_.pp_blocks = std::min(sm_count_, static_cast<int>(S));
+        JBP_CUDA_TRY(cudaMalloc(&buf_.pp_scratch, buf_.pp_stride * buf_.pp_blocks), "cudaMalloc(pp scratch)");
+    }
     JBP_CUDA_TRY(cudaMalloc(&buf_.synm, sizeof(unsigned) * G * M), "cudaMalloc(syn)");
     JBP_CUDA_TRY(cudaMemset(buf_.synm, 0, sizeof(unsigned) * G * M), "memset(syn)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.unsat_mask, sizeof(unsigned) * 2 * G), "cudaMalloc(unsat)");
@@ -170,6 +232,8 @@ std::string Engine::ensure_buffers(int S, int precision, bool damp) {
     buf_.S = S;
     buf_.precision = precision;
     buf_.damp = damp;
+    buf_.pp = pp;
+    buf_.R = R;
     return "";
 }
 
@@ -190,11 +254,13 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     if (o.precision < JBP_PREC_FP64 || o.precision > JBP_PREC_FP16) return "unknown precision";
     if (!(rq.p > 0.0 && rq.p < 1.0)) return "p must be in (0, 1)";
     if (o.damping < 0.0 || o.damping > 1.0) return "damping must be in [0, 1]";
-    if (o.enable_pp) return "post-processing on the GPU is not available in this build (use enable_pp = 0)";
     if (o.freeze_syn) return "freeze-syn is not available on the GPU in this build";
     const SideGraph &gx = model_.side[0], &gz = model_.side[1];
     if (!gx.regular || !gz.regular || gx.dc_max != gz.dc_max || gx.dv_max != gz.dv_max)
         return "the GPU kernels need a code with equal regular degrees on both sides";
+    const bool pp = o.enable_pp != 0;
+    if (pp && (o.check_interval != 1 || o.check_warmup != 0))
+        return "post-processing needs a syndrome test every iteration (check interval 1, warmup 0)";
     const bool damp = o.damping > 0.0;
     KernelSet ks;
     if (!select_kernels(gx.dc_max, gx.dv_max, o.precision, damp, ks))
@@ -202,7 +268,18 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
                std::to_string(gx.dv_max);
     JBP_CUDA_TRY(cudaSetDevice(device_), "cudaSetDevice");
     const int S = choose_slots(o, rq.ntrials);
-    std::string e = ensure_buffers(S, o.precision, damp);
+    const int H = std::max(0, o.flip_hist);
+    const int R = pp ? std::max(H + 1, 3) : 1;
+    if (pp) {
+        const int mmax = std::max(gx.m, gz.m);
+        const size_t smem = pp_smem_bytes(model_.n, gx.m + gz.m, mmax);
+        if (smem > 200 * 1024) return "code too large for GPU post-processing";
+        JBP_CUDA_TRY(cudaFuncSetAttribute(k_postprocess, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(smem)), "smem attribute");
+        std::string ee = upload_ets();
+        if (!ee.empty()) return ee;
+    }
+    std::string e = ensure_buffers(S, o.precision, damp, pp, R);
     if (!e.empty()) return e;
 
     cudaStream_t st = rq.stream;
@@ -243,6 +320,26 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     r.n_fresh = buf_.counts + 1;
     r.n_groups = buf_.counts + 2;
     r.cnt = buf_.cnt;
+    r.R = R;
+    r.it = buf_.it;
+    r.pp = pp ? 1 : 0;
+    r.flip_hist = H;
+    r.llr_from = std::min(100, o.max_iter);
+    if (pp) {
+        r.llr = buf_.llr;
+        r.act_k = buf_.act_k;
+        r.pstate = buf_.pstate;
+        r.stall_same = buf_.stall_same;
+        r.us_hist = buf_.us_hist;
+        r.dprev = buf_.dprev;
+        r.dpprev = buf_.dpprev;
+        r.pp_list = buf_.pp_list;
+        r.n_pp = buf_.counts + 3;
+        r.pp_mode = buf_.pp_mode;
+        r.ets = dets_;
+        r.pp_scratch = buf_.pp_scratch;
+        r.pp_scratch_stride = buf_.pp_stride;
+    }
     DevMsgs msg{};
     for (int s = 0; s < 2; ++s) {
         msg.c2v[s] = buf_.msg[s];
@@ -288,9 +385,19 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
         if (o.precision == JBP_PREC_FP64) ks.var64<<<big_grid, tpb, 0, s>>>(dcode_, r, msg, o.damping);
         else ks.varllr<<<big_grid, tpb, 0, s>>>(dcode_, r, msg, static_cast<float>(o.damping));
         if (e3) cudaEventRecordWithFlags(e3[2], s, cudaEventRecordExternal);
+        if (pp) {
+            k_stall_compare<<<big_grid, tpb, 0, s>>>(dcode_, r);
+            launches += 1;
+        }
         k_syndrome_check<<<big_grid, tpb, 0, s>>>(dcode_, r);
         cudaMemsetAsync(r.n_retired, 0, sizeof(int), s);
+        if (pp) cudaMemsetAsync(r.n_pp, 0, sizeof(int), s);
         k_retire<<<slot_blocks, tpb, 0, s>>>(r);
+        if (pp) {
+            k_postprocess<<<buf_.pp_blocks, kPpThreads,
+                            pp_smem_bytes(n, M, std::max(gx.m, gz.m)), s>>>(dcode_, r);
+            launches += 1;
+        }
         k_classify<<<sm_count_ * 2, classify_tpb, classify_smem, s>>>(dcode_, r);
         launches += 5;
         enqueue_refill(s);
@@ -298,19 +405,20 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
 
     JBP_CUDA_TRY(cudaEventRecord(ev0, st), "cudaEventRecord");
     JBP_CUDA_TRY(cudaMemsetAsync(buf_.cnt, 0, sizeof(DevCounters), st), "memset counters");
+    JBP_CUDA_TRY(cudaMemsetAsync(buf_.it, 0, sizeof(int), st), "memset it");
     k_init_slots<<<list_grid, tpb, 0, st>>>(r);
     launches += 1;
     enqueue_refill(st);
     JBP_CUDA_TRY(cudaGetLastError(), "initial launches");
 
-    // CUDA graph of R iterations.  With profiling on, every captured iteration also records
+    // CUDA graph of GI iterations.  With profiling on, every captured iteration also records
     // event nodes around the check and variable kernels; two graph instances alternate so
     // that the events of a finished graph are read while the next one runs.
-    int R = o.iters_per_launch > 0 ? o.iters_per_launch : 4;
-    R = std::min(R, o.max_iter);
+    int GI = o.iters_per_launch > 0 ? o.iters_per_launch : 4;
+    GI = std::min(GI, o.max_iter);
     const bool prof = o.profile != 0;
     const int nsets = prof ? 2 : 1;
-    std::vector<cudaEvent_t> pev(prof ? 2 * R * 3 : 0);
+    std::vector<cudaEvent_t> pev(prof ? 2 * GI * 3 : 0);
     for (auto &ev : pev) JBP_CUDA_TRY(cudaEventCreate(&ev), "cudaEventCreate");
     cudaStream_t cap;
     JBP_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -323,8 +431,8 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
         launches = launches_before;
         ce = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
         if (ce != cudaSuccess) break;
-        for (int i = 0; i < R; ++i) {
-            cudaEvent_t *e3 = prof ? &pev[(set * R + i) * 3] : nullptr;
+        for (int i = 0; i < GI; ++i) {
+            cudaEvent_t *e3 = prof ? &pev[(set * GI + i) * 3] : nullptr;
             enqueue_iteration(cap, e3);
         }
         ce = cudaStreamEndCapture(cap, &graph[set]);
@@ -337,9 +445,9 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     auto read_profile = [&](long long gidx) {
         if (!prof) return;
         const int set = static_cast<int>(gidx & 1);
-        for (int i = 0; i < R; ++i) {
+        for (int i = 0; i < GI; ++i) {
             float a = 0.0f, b = 0.0f;
-            cudaEvent_t *e3 = &pev[(set * R + i) * 3];
+            cudaEvent_t *e3 = &pev[(set * GI + i) * 3];
             if (cudaEventElapsedTime(&a, e3[0], e3[1]) == cudaSuccess &&
                 cudaEventElapsedTime(&b, e3[1], e3[2]) == cudaSuccess) {
                 check_ms += a;
@@ -350,8 +458,8 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     };
 
     const long long max_iters_total =
-        (rq.ntrials * static_cast<long long>(o.max_iter)) / std::max(1, S) + 2LL * o.max_iter + 2 * R + 8;
-    const long long max_graphs = max_iters_total / R + 2;
+        (rq.ntrials * static_cast<long long>(o.max_iter)) / std::max(1, S) + 2LL * o.max_iter + 2 * GI + 8;
+    const long long max_graphs = max_iters_total / GI + 2;
     auto t0 = std::chrono::steady_clock::now();
     std::string err;
     if (ce != cudaSuccess) err = cuda_err(ce, "graph capture");

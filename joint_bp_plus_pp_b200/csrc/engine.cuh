@@ -1,11 +1,9 @@
 // Batched joint X/Z BP engine for sm_100a: shared declarations.
 //
-// Trials live in "slots".  All per-edge state is stored edge-major and slot-minor,
-// msg[edge * S + slot], so a warp that handles one check (or one variable) for 32
-// consecutive slots makes one contiguous access per edge.  Slots are grouped by 32
-// (one warp); only groups with a running slot are scheduled.  Each BP iteration is a
-// fixed sequence of kernels captured in a CUDA graph; converged or exhausted trials are
-// retired, classified and replaced by fresh trials on the device, so the host only
+// Trials live in "slots", grouped by 32 (one warp per group); only groups with a running
+// slot are scheduled.  Message layout: see kernels_bp.cuh.  Each BP iteration is a fixed
+// sequence of kernels captured in a CUDA graph; converged or exhausted trials are retired,
+// post-processed, classified and replaced by fresh trials on the device, so the host only
 // watches a completion counter.
 #pragma once
 
@@ -46,6 +44,39 @@ struct DevCode {
     const int *pivot_row[2];        // [n] basis row with that pivot column, or -1
 };
 
+// All loaded ETS tables, flattened (group order = reference load order).
+constexpr int kMaxEtsGroups = 16;
+struct DevEts {
+    int ngroups;
+    int size[kMaxEtsGroups];                 // variables per entry
+    int first[kMaxEtsGroups][2];             // first entry of (group, side)
+    int count[kMaxEtsGroups][2];             // entries of (group, side), 0 when not loaded
+    const unsigned long long *key;           // per entry: (c0 << 32) | c1
+    const int *vars;                         // per entry: size sorted variables at var_first
+    const int *var_first;
+};
+
+// Result bits of a trial (res_flags), shared by retirement, post-processing and
+// classification.
+enum ResultBit : int {
+    kResSyndromeOk = 1 << 0,
+    kResBpOk = 1 << 1,
+    kResPpInDecode = 1 << 2,     // in-loop post-processing succeeded
+    kResPpInEts = 1 << 3,
+    kResPpInFlip = 1 << 4,
+    kResUsedAny = 1 << 5,        // an ETS correction was applied (the reference's used_any)
+    kResUsed6 = 1 << 6,
+    kResUsed12 = 1 << 7,
+    kResEtsPost = 1 << 8,        // post-BP ETS applied
+    kResEtsOk = 1 << 9,          // ets_pp_ok of the simulate loop
+    kResFlipOk = 1 << 10,
+    kResOsdOk = 1 << 11,
+    kResPostEntered = 1 << 12,   // post-BP stages ran
+};
+
+// Post-processing request kinds (pp_mode).
+enum PpMode : int { kPpInLoop = 1, kPpPost = 2 };
+
 struct DevCounters {
     unsigned long long next_trial;  // trials handed to slots
     unsigned long long done;        // trials classified
@@ -78,20 +109,44 @@ struct DevRun {
     double *prior;                  // [S][4] normalized prior (FP64 path)
     float *lprior;                  // [S][8] log prior x4, prior LLR x/z (FP32 path)
     uint8_t *err;                   // [S][n] true error of the slot's trial
-    // Hard decisions as bit planes: bit (slot % 32) of estx[g * n + v] is the x-bit of
-    // variable v in slot g * 32 + slot % 32 (estz: the z-bit).  One 32-slot word per
-    // variable makes the syndrome test an XOR of words and keeps a group's decisions in
-    // one contiguous row.
-    unsigned *estx, *estz;          // [G][n]
+    // Hard decisions as bit planes: bit (slot % 32) of plane[g * n + v] is the x-bit (estx)
+    // or z-bit (estz) of variable v in slot g * 32 + slot % 32.  One 32-slot word per
+    // variable makes the syndrome test an XOR of words and keeps a group's decisions in one
+    // contiguous row.  The planes form a ring of R iterations ([R][G][n]); the planes of the
+    // current global iteration are (*it % R).  A running slot advances one iteration per
+    // global iteration, so its decisions d iterations back are in plane (*it - d) % R.
+    unsigned *estx, *estz;
+    int R;
+    int *it;                        // global BP iteration counter
     unsigned *synm;                 // [(mx+mz)][G] target syndrome bits, same slot bit order
     int *res_iters;                 // [S] iterations at retirement
-    int *res_flags;                 // [S] bit0 syndrome_ok, bit1 bp_ok
+    int *res_flags;                 // [S] ResultBit flags
     // work lists
     int *retired, *n_retired;
     int *fresh, *n_fresh;
     int *groups, *n_groups;
     DevCounters *cnt;
+    // post-processing (enabled when pp != 0)
+    int pp;
+    int flip_hist;                  // flip-history window H (R >= H + 1)
+    int llr_from;                   // first 1-based iteration whose |LLR| is kept: min(100, max_iter)
+    double *llr;                    // [2][S][n] |LLR| of the latest kept iteration
+    int *act_k;                     // [S] iteration the flip window started (0: not started)
+    int *pstate;                    // [S] bit0 stall, bit1 oscillation, bit2 us-oscillation active
+    int *stall_same;                // [S]
+    unsigned short *us_hist;        // [S][100] max(us_x, us_z) by iteration (mod 100)
+    unsigned *dprev, *dpprev;       // [G] slots whose decisions differ from 1 / 2 iterations back
+    int *pp_list, *n_pp;            // slots to post-process this iteration
+    int *pp_mode;                   // [S] PpMode
+    DevEts ets;
+    unsigned char *pp_scratch;      // per post-processing block
+    size_t pp_scratch_stride;
 };
+
+__device__ __forceinline__ size_t plane_offset(const DevRun &run, int n, int back) {
+    const int r = ((*run.it - back) % run.R + run.R) % run.R;
+    return static_cast<size_t>(r) * (run.S / 32) * n;
+}
 
 // Messages of one run.  FP64: c2v as (a, b) pairs, v2c as (q0, q1) pairs, or the full
 // 4-vector (two pairs) when damping is on.  FP32/FP16: one LLR per edge and direction.

@@ -58,12 +58,24 @@ private:
         uint8_t *err = nullptr;
         int *res_iters = nullptr, *res_flags = nullptr;
         int *lists = nullptr;         // retired | fresh | groups
-        int *counts = nullptr;        // n_retired, n_fresh, n_groups
+        int *counts = nullptr;        // n_retired, n_fresh, n_groups, n_pp
         DevCounters *cnt = nullptr;
         unsigned long long *h_done = nullptr;  // pinned
+        int *it = nullptr;            // global iteration counter
+        // post-processing state (allocated when a run enables it)
+        bool pp = false;
+        int R = 1;
+        double *llr = nullptr;
+        int *act_k = nullptr, *pstate = nullptr, *stall_same = nullptr, *pp_list = nullptr, *pp_mode = nullptr;
+        unsigned short *us_hist = nullptr;
+        unsigned *dprev = nullptr, *dpprev = nullptr;
+        unsigned char *pp_scratch = nullptr;
+        size_t pp_stride = 0;
+        int pp_blocks = 0;
     };
 
-    std::string ensure_buffers(int S, int precision, bool damp);
+    std::string ensure_buffers(int S, int precision, bool damp, bool pp, int R);
+    std::string upload_ets();
     void free_buffers();
     int choose_slots(const jbp_options &opt, long long ntrials) const;
 
@@ -73,6 +85,9 @@ private:
     DevCode dcode_{};
     std::vector<void *> code_allocs_;
     Buffers buf_;
+    DevEts dets_{};
+    size_t ets_uploaded_ = static_cast<size_t>(-1);  // ETS groups in dets_
+    std::vector<void *> ets_allocs_;
 };
 
 std::string cuda_err(cudaError_t e, const char *what);

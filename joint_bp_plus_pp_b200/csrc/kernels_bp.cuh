@@ -25,6 +25,7 @@
 #include <cuda_fp16.h>
 
 #include "engine.cuh"
+#include "numerics.cuh"
 
 namespace jbp {
 
@@ -56,14 +57,22 @@ __device__ __forceinline__ size_t msg_off(int e, int G, int g, int lane) {
     return ((static_cast<size_t>(c) * G + g) * DC + pos) * kGroup + lane;
 }
 
-// Hard decisions of one variable for the warp's 32 slots, as x-bit and z-bit planes.
-// Called by all lanes; lanes of slots that are not running contribute 0 bits.
-__device__ __forceinline__ void store_est_bits(const DevRun &run, int group, int n, int v, int best, bool active) {
+// Hard decisions of one variable for the warp's 32 slots, as x-bit and z-bit planes of the
+// current iteration (plane = plane_offset(run, n, 0)).  Called by all lanes; lanes of slots
+// that are not running contribute 0 bits.
+__device__ __forceinline__ void store_est_bits(const DevRun &run, size_t plane, int group, int n, int v, int best,
+                                               bool active) {
     const unsigned xm = __ballot_sync(0xffffffffu, active && (best & 1));
     const unsigned zm = __ballot_sync(0xffffffffu, active && (best & 2));
     const int lane = threadIdx.x & 31;
-    if (lane == 0) run.estx[static_cast<size_t>(group) * n + v] = xm;
-    if (lane == 1) run.estz[static_cast<size_t>(group) * n + v] = zm;
+    if (lane == 0) run.estx[plane + static_cast<size_t>(group) * n + v] = xm;
+    if (lane == 1) run.estz[plane + static_cast<size_t>(group) * n + v] = zm;
+}
+
+// Whether a slot's iteration k1 (1-based) keeps its |LLR| for post-processing: in-loop
+// post-processing starts at iteration 100 or at max_iter (jointbp_ets.cpp:2563).
+__device__ __forceinline__ bool keeps_llr(const DevRun &run, int slot) {
+    return run.pp && run.iter[slot] + 1 >= run.llr_from;
 }
 
 // ------------------------------------------------------------------ FP64, bit-exact
@@ -171,6 +180,7 @@ __global__ void __launch_bounds__(256) k_var_f64(DevCode code, DevRun run, DevMs
     const int lane = threadIdx.x & 31;
     const int G = run.S / kGroup, n = code.n;
     const unsigned total = static_cast<unsigned>(*run.n_groups) * n;
+    const size_t plane = plane_offset(run, n, 0);
     const double2 *c2vx = static_cast<const double2 *>(msg.c2v[0]);
     const double2 *c2vz = static_cast<const double2 *>(msg.c2v[1]);
     for (unsigned w = warp_global_id(); w < total; w += warps_total()) {
@@ -222,6 +232,15 @@ __global__ void __launch_bounds__(256) k_var_f64(DevCode code, DevRun run, DevMs
             if (t1 > bv) { best = 1; bv = t1; }
             if (t2 > bv) { best = 2; bv = t2; }
             if (t3 > bv) { best = 3; }
+            if (keeps_llr(run, slot)) {
+                // |LLR| of the x and z bits (jointbp_ets.cpp:2484-2492)
+                const double eps = 1e-300;
+                const double px1 = dadd(t1, t3), px0 = dadd(t0, t2), pz1 = dadd(t2, t3), pz0 = dadd(t0, t1);
+                const double lx = dsub(log_dd(px1 > eps ? px1 : eps), log_dd(px0 > eps ? px0 : eps));
+                const double lz = dsub(log_dd(pz1 > eps ? pz1 : eps), log_dd(pz0 > eps ? pz0 : eps));
+                run.llr[static_cast<size_t>(slot) * n + v] = fabs(lx);
+                run.llr[(static_cast<size_t>(run.S) + slot) * n + v] = fabs(lz);
+            }
             double2 *v2cx = static_cast<double2 *>(msg.v2c[0]);
             double2 *v2cz = static_cast<double2 *>(msg.v2c[1]);
             double2 *v2cx_hi = static_cast<double2 *>(msg.v2c_hi[0]);
@@ -243,7 +262,7 @@ __global__ void __launch_bounds__(256) k_var_f64(DevCode code, DevRun run, DevMs
                 store_v2c_f64<DAMP>(v2cz, v2cz_hi, oz[k], 1, n0, n1, n2, n3, fresh, pr, damping);
             }
         }
-        store_est_bits(run, group, n, v, best, active);
+        store_est_bits(run, plane, group, n, v, best, active);
     }
 }
 
@@ -368,6 +387,12 @@ __device__ __forceinline__ int var_llr_one(const DevCode &code, const DevRun &ru
     if (w3 > bv) { best = 3; }
     const float Gx = lse2(lp.x, lp.z - Mu) - lse2(lp.y, lp.w - Mu);   // x-bit coupling through Z
     const float Hz = lse2(lp.x, lp.y - Lam) - lse2(lp.z, lp.w - Lam); // z-bit coupling through X
+    if (keeps_llr(run, slot)) {
+        // |LLR| of the x and z bits of the total (base 2; the OSD order is scale-free)
+        const int n = code.n;
+        run.llr[static_cast<size_t>(slot) * n + v] = fabsf(lse2(w1, w3) - lse2(w0, w2));
+        run.llr[(static_cast<size_t>(run.S) + slot) * n + v] = fabsf(lse2(w2, w3) - lse2(w0, w1));
+    }
 #pragma unroll
     for (int k = 0; k < DV; ++k) {
         float ox_v = clamp_llr(Lam - lx[k] + Gx);
@@ -397,6 +422,7 @@ __global__ void __launch_bounds__(256) k_var_llr(DevCode code, DevRun run, DevMs
     const int n = code.n;
     const int pairs = (n + 1) >> 1;
     const unsigned total = static_cast<unsigned>(*run.n_groups) * pairs;
+    const size_t plane = plane_offset(run, n, 0);
     for (unsigned w = warp_global_id(); w < total; w += warps_total()) {
         const int gi = static_cast<int>(w / static_cast<unsigned>(pairs));
         const int v0 = 2 * static_cast<int>(w - static_cast<unsigned>(gi) * pairs);
@@ -409,8 +435,8 @@ __global__ void __launch_bounds__(256) k_var_llr(DevCode code, DevRun run, DevMs
             b0 = var_llr_one<T, DC, DV, DAMP>(code, run, msg, v0, group, lane, damping);
             if (has1) b1 = var_llr_one<T, DC, DV, DAMP>(code, run, msg, v0 + 1, group, lane, damping);
         }
-        store_est_bits(run, group, n, v0, b0, active);
-        if (has1) store_est_bits(run, group, n, v0 + 1, b1, active);
+        store_est_bits(run, plane, group, n, v0, b0, active);
+        if (has1) store_est_bits(run, plane, group, n, v0 + 1, b1, active);
     }
 }
 

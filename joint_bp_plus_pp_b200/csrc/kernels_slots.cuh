@@ -64,6 +64,7 @@ static __global__ void __launch_bounds__(256) k_syndrome_check(DevCode code, Dev
     const int mx = code.s[0].m, M = mx + code.s[1].m;
     const int blocks = (M + 31) >> 5;
     const unsigned total = static_cast<unsigned>(*run.n_groups) * blocks;
+    const size_t plane = plane_offset(run, n, 0);
     for (unsigned w = warp_global_id(); w < total; w += warps_total()) {
         const int gi = static_cast<int>(w / static_cast<unsigned>(blocks));
         const int rb = static_cast<int>(w - static_cast<unsigned>(gi) * blocks);
@@ -79,7 +80,7 @@ static __global__ void __launch_bounds__(256) k_syndrome_check(DevCode code, Dev
             const int ch = side ? row - mx : row;
             const int dc = side ? code.s[1].dc : code.s[0].dc;
             const int *chk_var = side ? code.s[1].chk_var : code.s[0].chk_var;
-            const unsigned *planes = (side ? run.estz : run.estx) + static_cast<size_t>(group) * n;
+            const unsigned *planes = (side ? run.estz : run.estx) + plane + static_cast<size_t>(group) * n;
             unsigned par = 0;
             for (int i = 0; i < dc; ++i) par ^= planes[__ldg(chk_var + ch * dc + i)];
             mm[side] = (par ^ run.synm[static_cast<size_t>(row) * G + group]) & due_mask;
@@ -88,11 +89,85 @@ static __global__ void __launch_bounds__(256) k_syndrome_check(DevCode code, Dev
         const unsigned uz = __reduce_or_sync(0xffffffffu, mm[1]);
         if (lane == 0 && ux) atomicOr(&run.unsat_mask[group], ux);
         if (lane == 1 && uz) atomicOr(&run.unsat_mask[G + group], uz);
+        if (run.pp && (ux | uz)) {
+            // per-slot unsatisfied counts (post-processing gates and the us history):
+            // lane s gathers bit s of the 32 rows' mismatch masks
+            for (int side = 0; side < 2; ++side) {
+                const unsigned any = side ? uz : ux;
+                if (!any) continue;
+                int cnt = 0;
+                for (int b = 0; b < 32; ++b) {
+                    const unsigned col = __ballot_sync(0xffffffffu, (mm[side] >> b) & 1u);
+                    if (lane == b) cnt = __popc(col);
+                }
+                if (cnt) atomicAdd(&run.unsat[side * run.S + slot], cnt);
+            }
+        }
+    }
+}
+
+// Post-processing bookkeeping: slots whose decisions differ from 1 and 2 iterations back
+// (the reference's est == prev_est / prev_prev_est, jointbp_ets.cpp:2555-2556), for groups
+// holding a slot at or past the first iteration that can trigger post-processing.
+static __global__ void __launch_bounds__(256) k_stall_compare(DevCode code, DevRun run) {
+    const int lane = threadIdx.x & 31;
+    const int n = code.n;
+    const int chunks = (n + 31) >> 5;
+    const unsigned total = static_cast<unsigned>(*run.n_groups) * chunks;
+    const size_t p0 = plane_offset(run, n, 0), p1 = plane_offset(run, n, 1), p2 = plane_offset(run, n, 2);
+    for (unsigned w = warp_global_id(); w < total; w += warps_total()) {
+        const int gi = static_cast<int>(w / static_cast<unsigned>(chunks));
+        const int cb = static_cast<int>(w - static_cast<unsigned>(gi) * chunks);
+        const int group = run.groups[gi];
+        const int slot = group * kGroup + lane;
+        const bool late = (run.flags[slot] & kRunning) && run.iter[slot] + 1 >= run.llr_from;
+        if (!__any_sync(0xffffffffu, late)) continue;
+        const int v = cb * 32 + lane;
+        unsigned d1 = 0, d2 = 0;
+        if (v < n) {
+            const size_t o = static_cast<size_t>(group) * n + v;
+            const unsigned cx = run.estx[p0 + o], cz = run.estz[p0 + o];
+            d1 = (cx ^ run.estx[p1 + o]) | (cz ^ run.estz[p1 + o]);
+            d2 = (cx ^ run.estx[p2 + o]) | (cz ^ run.estz[p2 + o]);
+        }
+        d1 = __reduce_or_sync(0xffffffffu, d1);
+        d2 = __reduce_or_sync(0xffffffffu, d2);
+        if (lane == 0 && d1) atomicOr(&run.dprev[group], d1);
+        if (lane == 1 && d2) atomicOr(&run.dpprev[group], d2);
     }
 }
 
 // Counts the finished iteration; a slot retires when its checked syndrome matches or it
 // reaches max_iter (the CPU's iteration accounting, jointbp_ets.cpp:2733-2735, 3078).
+// detect_us_oscillation (jointbp_ets.cpp:2021-2053) over the last 100 samples of
+// max(us_x, us_z), kept by iteration number modulo 100 (samples k1-99 .. k1).
+static __device__ bool us_oscillation(const unsigned short *h, int k1) {
+    if (k1 < 100) return false;
+    int mn = h[(k1 - 99) % 100], mx = mn;
+    long long sum = 0;
+    for (int j = k1 - 99; j <= k1; ++j) {
+        const int v = h[j % 100];
+        mn = v < mn ? v : mn;
+        mx = v > mx ? v : mx;
+        sum += v;
+    }
+    const double mean = static_cast<double>(sum) / 100.0;
+    if (mean <= 0.0) return false;
+    int min_range = static_cast<int>(mean * 0.2);
+    if (min_range < 10) min_range = 10;
+    if (mx - mn < min_range) return false;
+    int prev_sign = 0, turns = 0;
+    for (int j = k1 - 98; j <= k1; ++j) {
+        const int d = static_cast<int>(h[j % 100]) - static_cast<int>(h[(j - 1) % 100]);
+        const int sg = d > 0 ? 1 : (d < 0 ? -1 : 0);
+        if (sg) {
+            if (prev_sign && sg != prev_sign) turns++;
+            prev_sign = sg;
+        }
+    }
+    return turns >= 2;
+}
+
 static __global__ void k_retire(DevRun run) {
     const int gi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (gi >= *run.n_groups) return;
@@ -101,15 +176,51 @@ static __global__ void k_retire(DevRun run) {
     const int slot = group * kGroup + lane;
     const int G = run.S / kGroup;
     const unsigned bad = run.unsat_mask[group] | run.unsat_mask[G + group];
+    const unsigned dp = run.pp ? run.dprev[group] : 0u, dpp = run.pp ? run.dpprev[group] : 0u;
     __syncwarp();
     if (lane == 0) {
         run.unsat_mask[group] = 0u;
         run.unsat_mask[G + group] = 0u;
+        if (run.pp) {
+            run.dprev[group] = 0u;
+            run.dpprev[group] = 0u;
+        }
     }
     if (!(run.flags[slot] & kRunning)) return;
     const int k1 = run.iter[slot] + 1;
     run.iter[slot] = k1;
     const bool conv = check_due(run, k1) && !((bad >> lane) & 1u);
+    if (run.pp) {
+        const int S = run.S;
+        const int ux = run.unsat[slot], uz = run.unsat[S + slot];
+        run.unsat[slot] = 0;
+        run.unsat[S + slot] = 0;
+        if (!conv) {
+            // stall / oscillation triggers and the flip window (jointbp_ets.cpp:2536-2633)
+            const int sig = ux > uz ? ux : uz;
+            unsigned short *h = run.us_hist + static_cast<size_t>(slot) * 100;
+            h[k1 % 100] = static_cast<unsigned short>(sig > 65535 ? 65535 : sig);
+            const bool same = k1 >= 2 && !((dp >> lane) & 1u);
+            const bool osc = k1 >= 3 && !((dpp >> lane) & 1u) && !same;
+            const bool allow = k1 >= 100 || k1 == run.max_iter;
+            const int ss = same ? run.stall_same[slot] + 1 : 0;
+            run.stall_same[slot] = ss;
+            int st = run.pstate[slot];
+            bool act = false;
+            if (!(st & 1) && (ss >= 1 || k1 == run.max_iter) && allow) { st |= 1; act = true; }
+            if (!(st & 2) && osc && allow) { st |= 2; act = true; }
+            if (!(st & 4) && allow && us_oscillation(h, k1)) { st |= 4; act = true; }
+            run.pstate[slot] = st;
+            if (act && run.act_k[slot] == 0 && run.flip_hist > 0) run.act_k[slot] = k1;
+            int mode = 0;
+            if (st && sig <= 20) mode = kPpInLoop;
+            else if (k1 >= run.max_iter) mode = kPpPost;
+            if (mode) {
+                run.pp_mode[slot] = mode;
+                run.pp_list[atomicAdd(run.n_pp, 1)] = slot;
+            }
+        }
+    }
     if (conv || k1 >= run.max_iter) {
         run.res_iters[slot] = k1;
         run.res_flags[slot] = conv ? 3 : 0;
@@ -155,17 +266,19 @@ static __global__ void k_classify(DevCode code, DevRun run) {
     const int nret = *run.n_retired;
     const int n = code.n;
     const bool have_err = run.source != kSrcSyndromes;
+    const size_t plane = plane_offset(run, n, 0);
     for (int r = blockIdx.x * wpb + wib; r < nret; r += gridDim.x * wpb) {
         const int slot = run.retired[r];
         const long long local = run.trial[slot] - run.first_trial;
         const int iters = run.res_iters[slot];
-        const bool ok = run.res_flags[slot] & 1;
+        const int rf = run.res_flags[slot];
+        const bool ok = rf & kResSyndromeOk;
         for (int w = lane; w < words; w += 32) { dx[w] = 0; dz[w] = 0; }
         __syncwarp();
         bool exact = true;
         const uint8_t *err = run.err + static_cast<size_t>(slot) * n;
-        const unsigned *px = run.estx + static_cast<size_t>(slot / kGroup) * n;
-        const unsigned *pz = run.estz + static_cast<size_t>(slot / kGroup) * n;
+        const unsigned *px = run.estx + plane + static_cast<size_t>(slot / kGroup) * n;
+        const unsigned *pz = run.estz + plane + static_cast<size_t>(slot / kGroup) * n;
         const int bit = slot % kGroup;
         constexpr int U = 8;  // chunks of 32 variables whose loads are issued together
         for (int base0 = 0; base0 < n; base0 += 32 * U) {
@@ -206,31 +319,60 @@ static __global__ void k_classify(DevCode code, DevRun run) {
         }
         const bool success = have_err ? (ok && stab) : ok;
         if (lane == 0) {
+            // Run Summary counters exactly as the simulate loop derives them
+            // (jointbp_ets.cpp:6012-6019, 6070-6080, 6199-6224)
+            const bool in_dec = rf & kResPpInDecode;
+            const bool used_any = rf & kResUsedAny, used6 = rf & kResUsed6, used12 = rf & kResUsed12;
+            const bool post = rf & kResPostEntered;
+            const bool ets_ok = in_dec ? (rf & kResPpInEts) : (rf & kResEtsOk);
+            const bool flip_ok = in_dec ? (rf & kResPpInFlip) : (rf & kResFlipOk);
+            const bool osd_ok = rf & kResOsdOk;
+            const bool osd_success = osd_ok || (in_dec && !(rf & kResPpInEts) && !(rf & kResPpInFlip));
+            const bool pp_this = success && (in_dec || ets_ok || flip_ok || osd_ok);
             DevCounters *c = run.cnt;
             atomicAdd(&c->done, 1ull);
             atomicAdd(&c->total_iters, static_cast<unsigned long long>(iters));
             atomicAdd(&c->bp_trial_iterations, static_cast<unsigned long long>(iters));
             if (!success) atomicAdd(&c->failures, 1ull);
-            if (!(run.res_flags[slot] & 2)) atomicAdd(&c->bp_fail, 1ull);
+            if (!(rf & kResBpOk)) atomicAdd(&c->bp_fail, 1ull);
             if (exact) atomicAdd(&c->exact, 1ull);
             if (ok) atomicAdd(&c->syndrome_ok, 1ull);
             if (success && !exact && stab) atomicAdd(&c->stab_success, 1ull);
+            if (in_dec && used_any) {
+                atomicAdd(&c->ets_used, 1ull);
+                if (used6) atomicAdd(&c->ets6_used, 1ull);
+                if (used12) atomicAdd(&c->ets12_used, 1ull);
+            }
+            if (post) {
+                if (rf & kResEtsPost) atomicAdd(&c->ets_used, 1ull);
+                if (used6) atomicAdd(&c->ets6_used, 1ull);
+                if (used12) atomicAdd(&c->ets12_used, 1ull);
+            }
+            if (success && ets_ok) {
+                atomicAdd(&c->ets_saved, 1ull);
+                if (used6) atomicAdd(&c->ets6_saved, 1ull);
+                if (used12) atomicAdd(&c->ets12_saved, 1ull);
+            }
+            if (success && flip_ok) atomicAdd(&c->flip_pp_success, 1ull);
+            if (pp_this) atomicAdd(&c->pp_success, 1ull);
+            if (success && osd_success) atomicAdd(&c->osd_pp_success, 1ull);
             if (run.hist && iters >= 1 && iters <= run.max_iter) atomicAdd(&run.hist[iters], 1ull);
             if (run.res_out) {
                 jbp_trial_result rec;
                 rec.iterations = iters;
                 rec.syndrome_ok = ok;
-                rec.bp_ok = (run.res_flags[slot] >> 1) & 1;
+                rec.bp_ok = (rf & kResBpOk) ? 1 : 0;
                 rec.success = success;
                 rec.exact = exact;
                 rec.stab_equiv = stab;
-                rec.pp_success = 0;
-                rec.pp_ets = 0;
-                rec.pp_flip = 0;
-                rec.pp_osd = 0;
-                rec.ets_used_flags = 0;
-                rec.pp_in_decode = 0;
-                rec.reserved = 0;
+                rec.pp_success = pp_this;
+                rec.pp_ets = ets_ok;
+                rec.pp_flip = flip_ok;
+                rec.pp_osd = osd_success;
+                rec.ets_used_flags = static_cast<uint8_t>((used_any ? 1 : 0) | (used6 ? 2 : 0) | (used12 ? 4 : 0) |
+                                                          ((rf & kResEtsPost) ? 8 : 0) | (post ? 16 : 0));
+                rec.pp_in_decode = in_dec;
+                rec.reserved = osd_ok;
                 run.res_out[local] = rec;
             }
             run.flags[slot] = 0;
@@ -249,6 +391,11 @@ static __global__ void k_refill(DevRun run, int precision) {
             run.trial[slot] = run.first_trial + static_cast<long long>(t);
             run.iter[slot] = 0;
             run.flags[slot] = kRunning;
+            if (run.pp) {
+                run.act_k[slot] = 0;
+                run.pstate[slot] = 0;
+                run.stall_same[slot] = 0;
+            }
             // prior = normalize(1-p, p/3, p/3, p/3) (jointbp_ets.cpp:5484-5485)
             double p0 = __dsub_rn(1.0, run.p), p1 = __ddiv_rn(run.p, 3.0), p2 = p1, p3 = p1;
             double s = __dadd_rn(__dadd_rn(__dadd_rn(p0, p1), p2), p3);
@@ -416,8 +563,10 @@ static __global__ void k_fresh_syndrome(DevCode code, DevRun run) {
     }
 }
 
-// Compacts the groups that still hold a running slot.
+// Compacts the groups that still hold a running slot and advances the global iteration
+// counter (the last kernel of an iteration).
 static __global__ void k_groups(DevRun run) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *run.it += 1;
     const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (g >= run.S / kGroup) return;
     const int lane = threadIdx.x & 31;

@@ -120,6 +120,8 @@ size_t layout(const jbp::DevCode &code, int S, int precision, unsigned char *bas
     r.n_fresh = counts ? counts + 1 : nullptr;
     r.n_groups = counts ? counts + 2 : nullptr;
     r.cnt = cv.take<jbp::DevCounters>(1);
+    r.it = cv.take<int>(1);
+    r.R = 1;
     return cv.off;
 }
 

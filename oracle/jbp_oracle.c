@@ -1171,15 +1171,15 @@ int jbo_decode(const jbo_code *c, const jbo_ets_set *ets, jbo_work *w, const uin
 
 /* ---------------------------------------------------------------- Monte-Carlo trial */
 
-int jbo_simulate_trial(const jbo_code *c, const jbo_ets_set *ets, const jbo_basis *bx, const jbo_basis *bz,
-                       jbo_work *w, uint64_t seed, long long trial_idx, double p, int max_iter, int flip_hist,
-                       double damping, int freeze_syn, int enable_pp, jbo_trial_record *rec, uint8_t *err_out,
-                       uint8_t *est_out) {
+/* One trial of the simulate loop body (5947-6245) from a known error. */
+int jbo_error_trial(const jbo_code *c, const jbo_ets_set *ets, const jbo_basis *bx, const jbo_basis *bz,
+                    jbo_work *w, const uint8_t *err_in, long long trial_idx, double p, int max_iter, int flip_hist,
+                    double damping, int freeze_syn, int enable_pp, jbo_trial_record *rec, uint8_t *est_out) {
     int n = c->n;
     uint8_t *err = (uint8_t *)malloc(n), *est = (uint8_t *)malloc(n);
     uint8_t *sx = (uint8_t *)malloc(c->m[0]), *sz = (uint8_t *)malloc(c->m[1]);
     double *lx = (double *)malloc(sizeof(double) * n), *lz = (double *)malloc(sizeof(double) * n);
-    jbo_sample(seed, trial_idx, p, n, err);
+    memcpy(err, err_in, n);
     jbo_syndrome(c, 0, err, sx);
     jbo_syndrome(c, 1, err, sz);
     jbo_result r;
@@ -1254,10 +1254,23 @@ int jbo_simulate_trial(const jbo_code *c, const jbo_ets_set *ets, const jbo_basi
     rec->ets_applied_post = ets_applied;
     rec->pp_success_this = success && (r.pp_success || ets_ok || flip_ok || osd_ok);
     rec->osd_success = osd_ok || (r.pp_success && !r.pp_success_ets && !r.pp_success_flip);
-    if (err_out) memcpy(err_out, err, n);
     if (est_out) memcpy(est_out, est, n);
     free(err); free(est); free(sx); free(sz); free(lx); free(lz);
     return 0;
+}
+
+/* Sampled trial (5931-5946) followed by jbo_error_trial. */
+int jbo_simulate_trial(const jbo_code *c, const jbo_ets_set *ets, const jbo_basis *bx, const jbo_basis *bz,
+                       jbo_work *w, uint64_t seed, long long trial_idx, double p, int max_iter, int flip_hist,
+                       double damping, int freeze_syn, int enable_pp, jbo_trial_record *rec, uint8_t *err_out,
+                       uint8_t *est_out) {
+    uint8_t *err = (uint8_t *)malloc(c->n);
+    jbo_sample(seed, trial_idx, p, c->n, err);
+    int rc = jbo_error_trial(c, ets, bx, bz, w, err, trial_idx, p, max_iter, flip_hist, damping, freeze_syn, enable_pp,
+                             rec, est_out);
+    if (err_out) memcpy(err_out, err, c->n);
+    free(err);
+    return rc;
 }
 
 int jbo_wilson(long long n, long long k, double z, double *lo, double *hi) {

@@ -114,6 +114,11 @@ int jbo_ets_fix_multi(const jbo_code *c, const jbo_ets_set *ets, int side, const
 int jbo_flip_pp(const jbo_code *c, int side, const int *vars, int nv, const uint8_t *target, uint8_t *est);
 int jbo_osd_pp(const jbo_code *c, int side, const double *abs_llr, const uint8_t *target, uint8_t *est);
 
+/* Trial body from a known error (syndrome, decode, post-BP PP, classification). */
+int jbo_error_trial(const jbo_code *c, const jbo_ets_set *ets, const jbo_basis *bx, const jbo_basis *bz,
+                    jbo_work *w, const uint8_t *err, long long trial_idx, double p, int max_iter, int flip_hist,
+                    double damping, int freeze_syn, int enable_pp, jbo_trial_record *rec, uint8_t *est_out);
+
 /* Full trial (sample, decode, post-BP PP, classification) like the reference simulate loop. */
 int jbo_simulate_trial(const jbo_code *c, const jbo_ets_set *ets, const jbo_basis *bx, const jbo_basis *bz,
                        jbo_work *w, uint64_t seed, long long trial_idx, double p, int max_iter, int flip_hist,

@@ -208,14 +208,13 @@ int ref_bp_decode(const int *sx_in, const int *sz_in, double p, int max_iter, do
     return res.iterations;
 }
 
-// One Monte-Carlo trial exactly as the reference --simulate loop runs it.
-int ref_simulate_trial(unsigned long long seed, long long trial_idx, double p, int max_iter, int flip_hist,
-                       double damping, int freeze_syn, int enable_pp, RefTrialRecord *rec, int *err_out,
-                       int *est_out) {
+// The body of one Monte-Carlo trial from a known error, as the reference --simulate loop
+// runs it after sampling.
+int ref_error_trial(const int *err_in, long long trial_idx, double p, int max_iter, int flip_hist, double damping,
+                    int freeze_syn, int enable_pp, RefTrialRecord *rec, int *est_out) {
     using namespace refh;
     if (!g.ready) return 1;
-    std::vector<int> err(g.nvars);
-    ref_sample(seed, trial_idx, p, err.data());
+    std::vector<int> err(err_in, err_in + g.nvars);
     auto sx = compute_syndrome(g.x_checks, err, true);
     auto sz = compute_syndrome(g.z_checks, err, false);
     Msg prior{1.0 - p, p / 3.0, p / 3.0, p / 3.0};
@@ -307,9 +306,21 @@ int ref_simulate_trial(unsigned long long seed, long long trial_idx, double p, i
     rec->ets_applied_post = ets_applied;
     rec->pp_success_this = success && (res.pp_success || ets_pp_ok || flip_pp_ok || osd_pp_ok);
     rec->osd_success = osd_success;
-    if (err_out) std::copy(err.begin(), err.end(), err_out);
     if (est_out) std::copy(res.est.begin(), res.est.end(), est_out);
     return 0;
+}
+
+// One Monte-Carlo trial exactly as the reference --simulate loop runs it.
+int ref_simulate_trial(unsigned long long seed, long long trial_idx, double p, int max_iter, int flip_hist,
+                       double damping, int freeze_syn, int enable_pp, RefTrialRecord *rec, int *err_out,
+                       int *est_out) {
+    if (!refh::g.ready) return 1;
+    std::vector<int> err(refh::g.nvars);
+    ref_sample(seed, trial_idx, p, err.data());
+    int rc = ref_error_trial(err.data(), trial_idx, p, max_iter, flip_hist, damping, freeze_syn, enable_pp, rec,
+                             est_out);
+    if (err_out) std::copy(err.begin(), err.end(), err_out);
+    return rc;
 }
 
 }  // extern "C"

@@ -17,6 +17,8 @@ import sys
 import zlib
 from pathlib import Path
 
+import ctypes
+
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
@@ -52,15 +54,92 @@ def parse_summary(line):
     return d
 
 
+# Sampled trials on which in-loop post-processing saves the decode (seed, p, max_iter, trial):
+# flip at 2001/78, 2001/550, 2002/130, 2002/629, 2002/1042; OSD on the others.
+PP_SAVED_TRIALS = [(2001, 0.05, 130, 78), (2001, 0.05, 130, 550), (2002, 0.055, 130, 130),
+                   (2002, 0.055, 130, 133), (2002, 0.055, 130, 169), (2002, 0.055, 130, 311),
+                   (2002, 0.055, 130, 355), (2002, 0.055, 130, 358), (2002, 0.055, 130, 629),
+                   (2002, 0.055, 130, 693), (2002, 0.055, 130, 773), (2002, 0.055, 130, 999),
+                   (2002, 0.055, 130, 1042)]
+
+
+def sparse(v):
+    nz = np.nonzero(v)[0]
+    return [[int(i), int(v[i])] for i in nz]
+
+
+def ets_entries(path, P):
+    """(side, vars, unsat checks) of each line of an ETS file; ids are block * P + offset."""
+    out = []
+    for ln in path.read_text().splitlines():
+        m_v, m_u = re.search(r"vars=(\S+)", ln), re.search(r"unsat=(\S+)", ln)
+        if not m_v or not m_u:
+            continue
+        ids = lambda s: [int(t[1:].split(":")[0]) * P + int(t.split(":")[1]) for t in s.split(",")]
+        out.append((ln.split()[0], ids(m_v.group(1)), ids(m_u.group(1))))
+    return out
+
+
+def stage_trials(ref):
+    """Per-trial reference records on errors that make post-processing act.
+
+    Constructed cases put one ETS entry's variables in error (Pauli X, Z or Y, whichever
+    leaves exactly that entry's two checks unsatisfied on its side) and decode with a small
+    iteration cap, so the in-loop ETS, flip and OSD stages and the post-BP ETS all fire.
+    Sampled cases are the PP_SAVED_TRIALS plus the first post-processed failures of seed 2002.
+    """
+    cases = []
+    P = 768
+    for path in sorted(ETS_DIR.glob("ets_*.txt")):
+        for side, vs, uc in ets_entries(path, P)[:3]:
+            for st in (1, 2, 3):
+                e = np.zeros(ref.n, np.uint8)
+                e[sorted(set(vs))] = st
+                sx = np.zeros(ref.m[0], np.int32)
+                sz = np.zeros(ref.m[1], np.int32)
+                ref.lib.ref_syndrome(e.astype(np.int32).ctypes.data_as(ctypes.c_void_p),
+                                     sx.ctypes.data_as(ctypes.c_void_p), sz.ctypes.data_as(ctypes.c_void_p))
+                s = sx if side == "X" else sz
+                if sorted(np.nonzero(s)[0].tolist()) != sorted(uc):
+                    continue
+                for mi in (1, 2, 5, 20):
+                    d = ref.error_trial(e, 0.05, mi, flip_hist=5, enable_pp=True)
+                    est = d.pop("est")
+                    cases.append({"label": f"{path.stem}:{side}:{st}", "p": 0.05, "max_iter": mi, "flip_hist": 5,
+                                  "err": sparse(e), "est": sparse(est), "record": d})
+    fails = 0
+    sampled = list(PP_SAVED_TRIALS)
+    for t in range(1, 400):
+        if fails >= 8:
+            break
+        d = ref.simulate_trial(2002, t, 0.055, 130, enable_pp=True)
+        if not d["success"] and d["pp_in_decode"]:
+            sampled.append((2002, 0.055, 130, t))
+            fails += 1
+    for seed, p, mi, t in sampled:
+        d = ref.simulate_trial(seed, t, p, mi, flip_hist=5, enable_pp=True, want_vectors=True)
+        e, est = d.pop("err"), d.pop("est")
+        cases.append({"label": f"seed{seed}:trial{t}", "p": p, "max_iter": mi, "flip_hist": 5,
+                      "err": sparse(e), "est": sparse(est), "record": d})
+    (HERE / "pp_stage_trials.json").write_text(json.dumps(cases))
+    print("stage trials", len(cases), "ets_pp", sum(c["record"]["ets_pp_ok"] for c in cases),
+          "flip_pp", sum(c["record"]["flip_pp_ok"] for c in cases),
+          "osd", sum(c["record"]["osd_success"] for c in cases),
+          "post", sum(c["record"]["ets_applied_post"] for c in cases), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--quick", action="store_true", help="skip the 1000-trial CLI summary")
+    ap.add_argument("--stage-only", action="store_true", help="regenerate only pp_stage_trials.json")
     args = ap.parse_args()
     ref = Reference()
     lib = ref.lib
+    if args.stage_only:
+        stage_trials(ref)
+        return
 
     # --- code known answers (README start-up block) ---
-    import ctypes
     cnt = np.zeros(64, np.int32)
     labels = ctypes.create_string_buffer(32 * 8)
     ng = lib.ref_ets_counts(cnt.ctypes.data_as(ctypes.c_void_p), 32, labels, 8)
@@ -135,6 +214,7 @@ def main():
         summaries[name] = {"args": a, "rc": rc, "summary": parse_summary(line) if line else None}
         print(name, line, flush=True)
     (HERE / "cli_summaries.json").write_text(json.dumps(summaries, indent=1))
+    stage_trials(ref)
 
 
 if __name__ == "__main__":

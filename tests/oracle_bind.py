@@ -82,6 +82,9 @@ class Oracle:
                                                                    ctypes.c_double, ctypes.c_int, ctypes.c_int] + \
             [ctypes.c_void_p] * 3
         lib.jbo_wilson.argtypes = [ctypes.c_longlong, ctypes.c_longlong, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
+        lib.jbo_error_trial.argtypes = [ctypes.c_void_p] * 6 + [ctypes.c_longlong, ctypes.c_double, ctypes.c_int,
+                                                               ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                                               ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         self.code = _Code()
         if params is not None:
             rc = lib.jbo_code_from_params(str(params).encode(), ctypes.byref(self.code))
@@ -173,6 +176,18 @@ class Oracle:
             d["err"], d["est"] = err, est
         return d
 
+    def error_trial(self, err, p, max_iter, flip_hist=5, damping=0.0, freeze_syn=False, enable_pp=False):
+        """The simulate-loop body on a known error: record and final estimate."""
+        err = np.ascontiguousarray(err, np.uint8)
+        rec = TrialRecord()
+        est = np.zeros(self.n, np.uint8)
+        self.lib.jbo_error_trial(ctypes.byref(self.code), self.ets, ctypes.byref(self.bx), ctypes.byref(self.bz),
+                                 self.work, _ptr(err), 0, p, max_iter, flip_hist, damping, int(freeze_syn),
+                                 int(enable_pp), ctypes.byref(rec), _ptr(est))
+        d = rec.as_dict()
+        d["est"] = est
+        return d
+
     def wilson(self, n, k, z=1.96):
         lo, hi = ctypes.c_double(), ctypes.c_double()
         self.lib.jbo_wilson(n, k, z, ctypes.byref(lo), ctypes.byref(hi))
@@ -193,6 +208,8 @@ class Reference:
         lib.ref_simulate_trial.argtypes = [ctypes.c_ulonglong, ctypes.c_longlong, ctypes.c_double, ctypes.c_int,
                                            ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        lib.ref_error_trial.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         if lib.ref_init(str(params).encode(), None) != 0:
             raise RuntimeError("ref_init failed")
         self.n = lib.ref_nvars()
@@ -227,6 +244,17 @@ class Reference:
         d = rec.as_dict()
         if want_vectors:
             d["err"], d["est"] = err.astype(np.uint8), est.astype(np.uint8)
+        return d
+
+
+    def error_trial(self, err, p, max_iter, flip_hist=5, damping=0.0, freeze_syn=False, enable_pp=False):
+        e = np.ascontiguousarray(err, np.int32)
+        rec = TrialRecord()
+        est = np.zeros(self.n, np.int32)
+        self.lib.ref_error_trial(_ptr(e), 0, p, max_iter, flip_hist, damping, int(freeze_syn), int(enable_pp),
+                                 ctypes.byref(rec), _ptr(est))
+        d = rec.as_dict()
+        d["est"] = est.astype(np.uint8)
         return d
 
 

@@ -122,3 +122,24 @@ def test_oracle_matches_reference_fresh_trials(oracle):
             assert (a.pop("est") == b.pop("est")).all()
             assert (a.pop("err") == b.pop("err")).all()
             assert a == b, (seed, t)
+
+
+def test_pp_stage_trials_golden(oracle):
+    """Post-processing stages (in-loop ETS, flip, OSD, post-BP ETS) on the reference's
+    stage fixtures: constructed ETS errors and sampled trials that post-processing saves."""
+    cases = json.loads((GOLDEN / "pp_stage_trials.json").read_text())
+    seen = {"ets_pp_ok": 0, "flip_pp_ok": 0, "osd_success": 0, "ets_applied_post": 0, "used6": 0, "used12": 0}
+    for c in cases:
+        e = np.zeros(oracle.n, np.uint8)
+        for v, s in c["err"]:
+            e[v] = s
+        d = oracle.error_trial(e, c["p"], c["max_iter"], flip_hist=c["flip_hist"], enable_pp=True)
+        est = d.pop("est")
+        assert sorted([int(v), int(est[v])] for v in np.nonzero(est)[0]) == sorted(c["est"]), c["label"]
+        rec = dict(c["record"])
+        rec.pop("trial_idx", None)
+        d.pop("trial_idx", None)
+        assert d == rec, (c["label"], c["max_iter"])
+        for k in seen:
+            seen[k] += rec[k]
+    assert all(v > 0 for k, v in seen.items() if k != "used12"), seen
