@@ -1,10 +1,12 @@
 #!/usr/bin/env python3
 """Benchmark of the batched joint X/Z BP Monte-Carlo decoder on B200.
 
-Workload (the reference's batched Monte-Carlo configuration): the shipped [[9216,4612]]
-(3,12)-regular APM code, i.i.d. depolarizing noise p=0.04, max-iter 1000 with per-trial
-early exit, damping 0, no post-processing (--no-pp), FP32 messages.  One step decodes one
-batch of `--batch` seeded trials; trial indices never repeat across steps.
+Workload (the reference's full post-processing configuration): the shipped [[9216,4612]]
+(3,12)-regular APM code with its ETS tables, i.i.d. depolarizing noise p=0.04, max-iter 1000
+with per-trial early exit, damping 0, --flip-hist 5, post-processing on (ETS, flip and OSD
+in the loop after the stall triggers and after BP), FP32 messages.  The same GPU also runs
+the plain FP64 BP+PP decoder on the same workload for the FP32/FP64 ratio.  One step decodes
+one batch of `--batch` seeded trials; trial indices never repeat across steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -43,6 +45,8 @@ def parse_args():
     ap.add_argument("--p", type=float, default=0.04)
     ap.add_argument("--max-iter", type=int, default=1000)
     ap.add_argument("--seed", type=int, default=106)
+    ap.add_argument("--no-pp", action="store_true", help="plain BP without post-processing")
+    ap.add_argument("--flip-hist", type=int, default=5)
     ap.add_argument("--fp64-batch", type=int, default=32768, help="trials of the FP64 comparison step (0 = skip)")
     ap.add_argument("--e2e-batch", type=int, default=65536, help="trials per end-to-end step (0 = skip)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
@@ -118,19 +122,19 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference_rate(p, max_iter, seconds, procs=None, seed0=1000):
+def cpu_reference_rate(p, max_iter, seconds, pp=True, flip_hist=5, procs=None, seed0=1000):
     """Reference CPU decoder, one process per host core, for about `seconds` (trials/s summed)."""
     if not REF_BIN.exists():
         return None
     procs = procs or os.cpu_count() or 1
     # probe the per-process rate with a short run, then size the sample to `seconds`
-    probe = _run_ref(p, max_iter, 24, seed0 - 1)
+    probe = _run_ref(p, max_iter, 24, seed0 - 1, pp, flip_hist)
     rate1 = probe[0] / max(probe[1], 1e-9) if probe else 30.0
     trials = max(8, int(rate1 * seconds))
     outs = []
     ths = []
     for k in range(procs):
-        th = threading.Thread(target=lambda k=k: outs.append(_run_ref(p, max_iter, trials, seed0 + k)))
+        th = threading.Thread(target=lambda k=k: outs.append(_run_ref(p, max_iter, trials, seed0 + k, pp, flip_hist)))
         th.start()
         ths.append(th)
     for th in ths:
@@ -142,12 +146,16 @@ def cpu_reference_rate(p, max_iter, seconds, procs=None, seed0=1000):
     iters = sum(i for _, _, i in outs)
     return {"value": rate, "unit": UNIT, "cores": len(outs), "kind": "reference",
             "sample": f"{len(outs)} processes x {trials} trials of jointbp_ets --simulate --p {p} --max-iter {max_iter} "
-                      f"--no-pp (distinct seeds), {iters} BP iterations in total"}
+                      f"{_pp_flags(pp, flip_hist)} (distinct seeds), {iters} BP iterations in total"}
 
 
-def _run_ref(p, max_iter, trials, seed):
+def _pp_flags(pp, flip_hist):
+    return f"--flip-hist {flip_hist}" if pp else "--no-pp"
+
+
+def _run_ref(p, max_iter, trials, seed, pp, flip_hist):
     cmd = [str(REF_BIN), "--params", str(PARAMS), "--simulate", "--p", str(p), "--trials", str(trials), "--max-iter",
-           str(max_iter), "--no-pp", "--seed", str(seed), "--report-every", "0"]
+           str(max_iter), "--seed", str(seed), "--report-every", "0"] + _pp_flags(pp, flip_hist).split()
     r = subprocess.run(cmd, capture_output=True, text=True, cwd=str(PARAMS.parent))
     m = re.search(r"trials=(\d+).*?iters=(\d+).*?elapsed_s=([0-9.]+)s", r.stdout)
     if not m:
@@ -165,24 +173,29 @@ def run_reference(args, rank, world):
         return 0
     per_step = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
-        cpu_reference_rate(args.p, args.max_iter, per_step / 4)
+        cpu_reference_rate(args.p, args.max_iter, per_step / 4, not args.no_pp, args.flip_hist)
     vals = []
     last = None
     for _ in range(args.steps):
-        last = cpu_reference_rate(args.p, args.max_iter, per_step)
+        last = cpu_reference_rate(args.p, args.max_iter, per_step, not args.no_pp, args.flip_hist)
         vals.append(last["value"])
     value = statistics.median(vals)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference mt19937_64 depolarizing noise)",
             "impl": "reference",
-            "config": {"workload": "batched Monte Carlo, [[9216,4612]] APM code, p=0.04, max-iter 1000, --no-pp, "
-                                   "reference CPU decoder (FP64)", "p": args.p, "max_iter": args.max_iter},
+            "config": {"workload": workload_name(args, "reference CPU decoder (FP64)"), "p": args.p,
+                       "max_iter": args.max_iter, "enable_pp": not args.no_pp, "flip_hist": args.flip_hist},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": last["cores"], "kind": "reference",
                              "sample": last["sample"]},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+def workload_name(args, decoder):
+    pp = f"BP+PP (ETS, flip, OSD), flip-hist {args.flip_hist}" if not args.no_pp else "plain BP (--no-pp)"
+    return f"batched Monte Carlo, [[9216,4612]] APM code, p={args.p}, max-iter {args.max_iter}, {pp}, {decoder}"
 
 
 # ----------------------------------------------------------------------------- b200 arm
@@ -207,7 +220,9 @@ def main():
     from joint_bp_plus_pp_b200 import Decoder, Options, sample_reference_errors, wilson_interval
 
     dec = Decoder.from_params(device=local)
-    opts = Options(precision=args.precision, max_iter=args.max_iter, enable_pp=False, slots=args.slots, profile=True)
+    pp = not args.no_pp
+    opts = Options(precision=args.precision, max_iter=args.max_iter, enable_pp=pp, flip_hist=args.flip_hist,
+                   slots=args.slots, profile=True)
     B = args.batch
     stride = B * (args.warmup + args.steps + 2)
     base = 1 + rank * stride          # distinct trial ranges per rank
@@ -267,7 +282,7 @@ def main():
     # FP64 comparison (plain FP64 BP, same workload, one step)
     fp64 = None
     if args.fp64_batch > 0 and rank == 0:
-        o64 = Options(precision="fp64", max_iter=args.max_iter, enable_pp=False)
+        o64 = Options(precision="fp64", max_iter=args.max_iter, enable_pp=pp, flip_hist=args.flip_hist)
         dec.simulate(args.seed, args.fp64_batch // 4, args.p, o64, first_trial=10 ** 9, per_trial=False)
         torch.cuda.synchronize()
         a = torch.cuda.Event(enable_timing=True)
@@ -285,7 +300,8 @@ def main():
         E = args.e2e_batch
         host = torch.empty((E, N_QUBITS), dtype=torch.uint8, pin_memory=True).numpy()
         host[:] = sample_reference_errors(N_QUBITS, args.seed, base + 5 * 10 ** 8, E, args.p)
-        oe = Options(precision=args.precision, max_iter=args.max_iter, enable_pp=False, slots=args.slots)
+        oe = Options(precision=args.precision, max_iter=args.max_iter, enable_pp=pp, flip_hist=args.flip_hist,
+                     slots=args.slots)
         dec.decode_errors(host[: max(32, E // 8)], args.p, oe, want_est=False)
         torch.cuda.synchronize()
         barrier()
@@ -311,7 +327,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_seconds > 0:
-        cpu = cpu_reference_rate(args.p, args.max_iter, args.cpu_seconds)
+        cpu = cpu_reference_rate(args.p, args.max_iter, args.cpu_seconds, pp, args.flip_hist)
 
     if dist is not None:
         dist.destroy_process_group()
@@ -323,8 +339,8 @@ def main():
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": {"fp32": "f32", "fp16": "f16-storage/f32", "fp64": "f64"}[args.precision],
         "data": "synthetic: Philox4x32-10 depolarizing noise keyed by (seed, trial index)",
-        "config": {"workload": "batched Monte Carlo, [[9216,4612]] APM code, p=0.04, max-iter 1000, no-pp, "
-                               f"{args.precision} messages", "p": args.p, "max_iter": args.max_iter,
+        "config": {"workload": workload_name(args, f"{args.precision} messages"), "p": args.p,
+                   "max_iter": args.max_iter, "enable_pp": pp, "flip_hist": args.flip_hist,
                    "trials_per_step": B, "slots": None, "l2": "message state (>= 7 GB) larger than L2",
                    "parallelism": f"replica trial ranges x{world}"},
         "gpu_launches": agg["kernel_launches"],

@@ -53,6 +53,8 @@ typedef struct {
     int iters_per_launch;  /* BP iterations per CUDA-graph launch; 0 = automatic */
     int watchdog_ms;       /* abort a run after this much wall time (0 = none) */
     int profile;           /* time the check and variable kernels with CUDA events (jbp_stats) */
+    int use_prior;         /* 1: decode with `prior` below instead of normalize(1-p, p/3, p/3, p/3) */
+    double prior[4];       /* probabilities of I, X, Z, Y (used as given, as cuda_bp_decode does) */
 } jbp_options;
 
 /* Per-trial outcome (16 bytes). */

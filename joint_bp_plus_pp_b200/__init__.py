@@ -36,7 +36,8 @@ class COptions(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("max_iter", ctypes.c_int), ("damping", ctypes.c_double),
                 ("flip_hist", ctypes.c_int), ("enable_pp", ctypes.c_int), ("freeze_syn", ctypes.c_int),
                 ("check_warmup", ctypes.c_int), ("check_interval", ctypes.c_int), ("slots", ctypes.c_int),
-                ("iters_per_launch", ctypes.c_int), ("watchdog_ms", ctypes.c_int), ("profile", ctypes.c_int)]
+                ("iters_per_launch", ctypes.c_int), ("watchdog_ms", ctypes.c_int), ("profile", ctypes.c_int),
+                ("use_prior", ctypes.c_int), ("prior", ctypes.c_double * 4)]
 
 
 TRIAL_DTYPE = np.dtype([("iterations", np.int32), ("syndrome_ok", np.uint8), ("bp_ok", np.uint8),
@@ -79,11 +80,13 @@ class Options:
     iters_per_launch: int = 0
     watchdog_ms: int = 0
     profile: bool = False
+    prior: tuple = None    # (I, X, Z, Y) probabilities used as given instead of those of p
 
     def to_c(self):
+        pr = (ctypes.c_double * 4)(*(self.prior or (0.0, 0.0, 0.0, 0.0)))
         return COptions(PREC[self.precision], self.max_iter, self.damping, self.flip_hist, int(self.enable_pp),
                         int(self.freeze_syn), self.check_warmup, self.check_interval, self.slots,
-                        self.iters_per_launch, self.watchdog_ms, int(self.profile))
+                        self.iters_per_launch, self.watchdog_ms, int(self.profile), int(self.prior is not None), pr)
 
 
 _lib = None

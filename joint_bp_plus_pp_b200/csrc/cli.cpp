@@ -1,0 +1,521 @@
+// jointbp_b200: the reference command line (jointbp_ets.cpp:4733-6449) over the batched GPU
+// decoder of include/jbp_b200.h.
+//
+// Same flags, params/ETS/vector file formats, modes (--simulate, --err, --sx/--sz) and exit
+// codes (0 ok, 2 single decode failed, 1 usage or input error), and the same Run Summary line
+// (jointbp_ets.cpp:6427-6448).  Unlike the reference, --cuda is not required and post-
+// processing runs on the GPU too (the reference allows --cuda only with --no-pp,
+// jointbp_ets.cpp:5408).  Monte Carlo trials run in batches of --batch trials on the device;
+// by default they use the reference's error stream (splitmix64 + mt19937_64 per trial index)
+// and FP64 messages, so counts equal the reference CPU run's.
+//
+// Extra flags: --precision fp64|fp32|fp16, --sampler mt19937|philox, --slots N, --batch N,
+// --ets-dir DIR.  Flags of the reference's per-iteration CPU diagnostics (--verbose,
+// --verbose-all, --report-ets, --report-fail, --save-fail-prefix) are accepted and ignored.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <ctime>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <sys/stat.h>
+#include <vector>
+
+#include "jbp_b200.h"
+
+namespace {
+
+struct Args {
+    std::string params, sx_path, sz_path, err_path, est_path, hist_out, progress_tsv, ets_dir;
+    std::string ets6_x, ets6_z, ets12_x, ets12_z, ets8_path4;
+    double p = 0.05, damping = 0.0;
+    int max_iter = 50, flip_hist = 5, device = 0, check_warmup = 0, check_interval = 1;
+    bool freeze_syn = false, simulate = false, enable_pp = true, seed_set = false;
+    unsigned long long seed = 0;
+    long long trials = 1, min_fails = 0, report_every = 100, progress_every = 100, trial_index = -1;
+    int precision = JBP_PREC_FP64, sampler = JBP_SAMPLER_MT19937, slots = 0;
+    long long batch = 1 << 18;
+};
+
+void usage(const char *prog) {
+    std::cout << "Usage: " << prog << " --params FILE [mode] [options]\n"
+              << "Modes:\n"
+              << "  --simulate               Monte Carlo over seeded depolarizing errors\n"
+              << "  --err FILE               decode the syndrome of an error vector (0..3 per qubit)\n"
+              << "  --sx FILE --sz FILE      decode a syndrome pair (one bit per check)\n"
+              << "Options (reference defaults):\n"
+              << "  --p P (0.05)  --max-iter N (50)  --flip-hist H (5)  --damping D (0)  --freeze-syn\n"
+              << "  --no-pp  --seed S  --trials N (1)  --trial-index I  --min-fails N  --est FILE\n"
+              << "  --report-every N (100)  --progress-every N (100)  --progress-tsv FILE  --iter-hist-out FILE\n"
+              << "  --ets6-x F --ets6-z F --ets12-x F --ets12-z F --ets-x F --ets-z F --ets8-path4 F\n"
+              << "  --cuda --cuda-graph (accepted; decoding always runs on the GPU)  --cuda-device D\n"
+              << "  --cuda-check-warmup N (0)  --cuda-check-interval N (1)\n"
+              << "Extra options:\n"
+              << "  --precision fp64|fp32|fp16 (fp64)  --sampler mt19937|philox (mt19937)\n"
+              << "  --slots N (trials in flight, 0 = auto)  --batch N (trials per GPU call, 262144)\n"
+              << "  --ets-dir DIR (default: the params path without extension)\n";
+}
+
+// format_scaled_unit / format_latency (jointbp_ets.cpp:203-237)
+std::string scaled_unit(double value, double scale, const char *suffix) {
+    const double s = value / scale, a = std::fabs(s);
+    const int prec = a < 10.0 ? 2 : (a < 100.0 ? 1 : 0);
+    std::ostringstream o;
+    o << std::fixed << std::setprecision(prec) << s << suffix;
+    return o.str();
+}
+std::string latency_str(double sec) {
+    return std::fabs(sec) < 1e-3 ? scaled_unit(sec, 1e-6, "us") : scaled_unit(sec, 1e-3, "ms");
+}
+
+// Wilson score interval (jointbp_ets.cpp:4388-4399)
+bool wilson(long long n, long long k, double z, double &lo, double &hi) {
+    if (n <= 0) return false;
+    const double ph = static_cast<double>(k) / n, z2 = z * z;
+    const double den = 1.0 + z2 / n;
+    const double c = (ph + z2 / (2.0 * n)) / den;
+    const double m = z * std::sqrt(ph * (1.0 - ph) / n + z2 / (4.0 * n * n)) / den;
+    lo = std::max(0.0, c - m);
+    hi = std::min(1.0, c + m);
+    return true;
+}
+
+std::string basename_no_ext(const std::string &path) {
+    const size_t dot = path.find_last_of('.'), slash = path.find_last_of('/');
+    if (dot == std::string::npos || (slash != std::string::npos && dot < slash)) return path;
+    return path.substr(0, dot);
+}
+
+bool exists(const std::string &p) {
+    struct stat st;
+    return stat(p.c_str(), &st) == 0;
+}
+
+bool read_ints(const std::string &path, std::vector<int> &out) {
+    std::ifstream in(path);
+    if (!in) return false;
+    out.clear();
+    int v = 0;
+    while (in >> v) out.push_back(v);
+    return true;
+}
+
+bool write_vector(const std::string &path, const uint8_t *v, int n) {
+    std::ofstream o(path);
+    if (!o) return false;
+    for (int i = 0; i < n; ++i) o << static_cast<int>(v[i]) << "\n";
+    return true;
+}
+
+const char *tf(bool b) { return b ? "true" : "false"; }
+
+// returns 0 on success, 1 on a usage error (message printed)
+int parse(int argc, char **argv, Args &a) {
+    auto need = [&](int &i, const char *flag) -> const char * {
+        if (i + 1 >= argc) {
+            std::cerr << "Missing value for " << flag << "\n";
+            return nullptr;
+        }
+        return argv[++i];
+    };
+    for (int i = 1; i < argc; ++i) {
+        const std::string f = argv[i];
+        const char *v = nullptr;
+#define VAL()                             \
+    do {                                  \
+        if (!(v = need(i, f.c_str()))) { \
+            return 1;                     \
+        }                                 \
+    } while (0)
+        try {
+            if (f == "--help" || f == "-h") { usage(argv[0]); return 2; }
+            else if (f == "--params") { VAL(); a.params = v; }
+            else if (f == "--sx") { VAL(); a.sx_path = v; }
+            else if (f == "--sz") { VAL(); a.sz_path = v; }
+            else if (f == "--err") { VAL(); a.err_path = v; }
+            else if (f == "--est") { VAL(); a.est_path = v; }
+            else if (f == "--p") { VAL(); a.p = std::stod(v); }
+            else if (f == "--max-iter") { VAL(); a.max_iter = std::stoi(v); }
+            else if (f == "--flip-hist") { VAL(); a.flip_hist = std::max(0, std::stoi(v)); }
+            else if (f == "--freeze-syn") a.freeze_syn = true;
+            else if (f == "--damping") { VAL(); a.damping = std::stod(v); }
+            else if (f == "--simulate") a.simulate = true;
+            else if (f == "--verbose") { if (i + 1 < argc && argv[i + 1][0] != '-') ++i; }
+            else if (f == "--verbose-all" || f == "--report-fail" || f == "--report-ets") {}
+            else if (f == "--seed") { VAL(); a.seed = std::stoull(v); a.seed_set = true; }
+            else if (f == "--ets6-x") { VAL(); a.ets6_x = v; }
+            else if (f == "--ets6-z") { VAL(); a.ets6_z = v; }
+            else if (f == "--ets12-x" || f == "--ets-x") { VAL(); a.ets12_x = v; }
+            else if (f == "--ets12-z" || f == "--ets-z") { VAL(); a.ets12_z = v; }
+            else if (f == "--ets8-path4") { VAL(); a.ets8_path4 = v; }
+            else if (f == "--trials") { VAL(); a.trials = std::stoll(v); }
+            else if (f == "--min-fails") { VAL(); a.min_fails = std::stoll(v); }
+            else if (f == "--report-every") { VAL(); a.report_every = std::stoll(v); }
+            else if (f == "--progress-every") { VAL(); a.progress_every = std::stoll(v); }
+            else if (f == "--iter-hist-out") { VAL(); a.hist_out = v; }
+            else if (f == "--save-fail-prefix") { VAL(); }
+            else if (f == "--progress-tsv") { VAL(); a.progress_tsv = v; }
+            else if (f == "--no-pp") a.enable_pp = false;
+            else if (f == "--cuda" || f == "--cuda-graph") {}
+            else if (f == "--cuda-device") { VAL(); a.device = std::stoi(v); }
+            else if (f == "--cuda-check-warmup") { VAL(); a.check_warmup = std::max(0, std::stoi(v)); }
+            else if (f == "--cuda-check-interval") { VAL(); a.check_interval = std::max(1, std::stoi(v)); }
+            else if (f == "--trial-index") { VAL(); a.trial_index = std::stoll(v); }
+            else if (f == "--precision") {
+                VAL();
+                const std::string s = v;
+                if (s == "fp64") a.precision = JBP_PREC_FP64;
+                else if (s == "fp32") a.precision = JBP_PREC_FP32;
+                else if (s == "fp16") a.precision = JBP_PREC_FP16;
+                else { std::cerr << "--precision must be fp64, fp32 or fp16\n"; return 1; }
+            } else if (f == "--sampler") {
+                VAL();
+                const std::string s = v;
+                if (s == "mt19937") a.sampler = JBP_SAMPLER_MT19937;
+                else if (s == "philox") a.sampler = JBP_SAMPLER_PHILOX;
+                else { std::cerr << "--sampler must be mt19937 or philox\n"; return 1; }
+            } else if (f == "--slots") { VAL(); a.slots = std::stoi(v); }
+            else if (f == "--batch") { VAL(); a.batch = std::max(1LL, std::stoll(v)); }
+            else if (f == "--ets-dir") { VAL(); a.ets_dir = v; }
+            else {
+                std::cerr << "Unknown argument: " << f << "\n";
+                usage(argv[0]);
+                return 1;
+            }
+        } catch (const std::exception &) {
+            std::cerr << "Invalid value for " << f << "\n";
+            return 1;
+        }
+#undef VAL
+    }
+    return 0;
+}
+
+// ETS groups in the reference order and default paths (jointbp_ets.cpp:5031-5337), with the
+// per-file overrides of --ets6-x/-z, --ets12-x/-z and --ets8-path4.
+int load_ets(jbp_ctx *ctx, const Args &a) {
+    const std::string dir = a.ets_dir.empty() ? basename_no_ext(a.params) : a.ets_dir;
+    const int sizes[] = {6, 8, 10, 12, 14, 16, 18, 20, 22};
+    for (int s : sizes) {
+        const std::string def = dir + "/ets_" + std::to_string(s) + "_2.txt";
+        std::string px = def, pz = def;
+        if (s == 6) {
+            if (!a.ets6_x.empty()) px = a.ets6_x;
+            if (!a.ets6_z.empty()) pz = a.ets6_z;
+        } else if (s == 12) {
+            if (!a.ets12_x.empty()) px = a.ets12_x;
+            if (!a.ets12_z.empty()) pz = a.ets12_z;
+        }
+        if (jbp_add_ets_group(ctx, s, std::to_string(s).c_str(), px.c_str(), pz.c_str()) != JBP_OK) return 1;
+        if (s == 8) {
+            const std::string p4 = a.ets8_path4.empty() ? dir + "/ets_8_2_path4.txt" : a.ets8_path4;
+            if (jbp_add_ets_group(ctx, 8, "8p4", p4.c_str(), p4.c_str()) != JBP_OK) return 1;
+        }
+    }
+    return 0;
+}
+
+jbp_options options(const Args &a) {
+    jbp_options o;
+    jbp_default_options(&o);
+    o.precision = a.precision;
+    o.max_iter = a.max_iter;
+    o.damping = a.damping;
+    o.flip_hist = a.flip_hist;
+    o.enable_pp = a.enable_pp ? 1 : 0;
+    o.freeze_syn = a.freeze_syn ? 1 : 0;
+    o.check_warmup = a.check_warmup;
+    o.check_interval = a.check_interval;
+    o.slots = a.slots;
+    return o;
+}
+
+void add_stats(jbp_stats &acc, const jbp_stats &s) {
+    acc.trials += s.trials;
+    acc.failures += s.failures;
+    acc.bp_fail += s.bp_fail;
+    acc.pp_success += s.pp_success;
+    acc.flip_pp_success += s.flip_pp_success;
+    acc.osd_pp_success += s.osd_pp_success;
+    acc.stab_success += s.stab_success;
+    acc.ets_used += s.ets_used;
+    acc.ets_saved += s.ets_saved;
+    acc.ets6_used += s.ets6_used;
+    acc.ets6_saved += s.ets6_saved;
+    acc.ets12_used += s.ets12_used;
+    acc.ets12_saved += s.ets12_saved;
+    acc.exact += s.exact;
+    acc.total_iters += s.total_iters;
+    acc.device_ms += s.device_ms;
+}
+
+void print_section(const char *name) { std::cout << "== " << name << " ==\n"; }
+
+int decode_single(jbp_ctx *ctx, const Args &a, int n, int mx, int mz) {
+    const jbp_options o = options(a);
+    std::vector<uint8_t> est(n);
+    jbp_trial_result r{};
+    jbp_stats st{};
+    const auto t0 = std::chrono::steady_clock::now();
+    int rc;
+    if (!a.err_path.empty()) {
+        std::vector<int> e;
+        if (!read_ints(a.err_path, e)) {
+            std::cerr << "Failed to read error vector from " << a.err_path << "\n";
+            return 1;
+        }
+        if (static_cast<int>(e.size()) != n) {
+            std::cerr << "Error vector size mismatch\n";
+            return 1;
+        }
+        std::vector<uint8_t> e8(n);
+        for (int i = 0; i < n; ++i) {
+            if (e[i] < 0 || e[i] > 3) {
+                std::cerr << "Error vector has invalid value\n";
+                return 1;
+            }
+            e8[i] = static_cast<uint8_t>(e[i]);
+        }
+        rc = jbp_decode_errors(ctx, &o, 1, e8.data(), a.p, est.data(), &r, &st);
+    } else {
+        if (a.sx_path.empty() || a.sz_path.empty()) {
+            std::cerr << "--sx and --sz are required unless --simulate is set\n";
+            return 1;
+        }
+        std::vector<int> sx, sz;
+        if (!read_ints(a.sx_path, sx) || !read_ints(a.sz_path, sz)) {
+            std::cerr << "Failed to read syndrome files\n";
+            return 1;
+        }
+        if (static_cast<int>(sx.size()) != mx || static_cast<int>(sz.size()) != mz) {
+            std::cerr << "Syndrome size mismatch\n";
+            return 1;
+        }
+        std::vector<uint8_t> sx8(mx), sz8(mz);
+        for (int i = 0; i < mx; ++i) sx8[i] = sx[i] ? 1 : 0;
+        for (int i = 0; i < mz; ++i) sz8[i] = sz[i] ? 1 : 0;
+        rc = jbp_decode_syndromes(ctx, &o, 1, sx8.data(), sz8.data(), a.p, est.data(), &r, &st);
+    }
+    if (rc != JBP_OK) {
+        std::cerr << "decode failed: " << jbp_last_error() << "\n";
+        return 1;
+    }
+    const double lat = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    const bool ok = r.syndrome_ok;
+    const bool with_err = !a.err_path.empty();
+    const bool success = with_err ? r.success != 0 : ok;
+    // single-decode flags (jointbp_ets.cpp:5732-5735): ets_pp_ok / flip_pp_ok of this decode
+    const bool ets_ok = r.pp_ets, flip_ok = r.pp_flip, osd_ok = r.reserved;
+    const bool pp_success = success && (r.pp_in_decode || ets_ok || flip_ok || osd_ok);
+    print_section("Decode Result");
+    std::cout << "iterations=" << r.iterations << " syndrome_match=" << tf(ok) << "\n";
+    std::cout << "decode_success=" << tf(success) << "\n";
+    std::cout << "pp_enabled=" << tf(a.enable_pp) << "\n";
+    std::cout << "pp_success=" << tf(pp_success) << "\n";
+    std::cout << "pp_success_ets=" << tf(success && ets_ok) << "\n";
+    std::cout << "pp_success_flip=" << tf(success && flip_ok) << "\n";
+    std::cout << "avg_latency=" << latency_str(lat) << "\n";
+    if (with_err) {
+        std::cout << "exact_match=" << tf(r.exact) << "\n";
+        std::cout << "stabilizer_equiv=" << tf(r.stab_equiv) << "\n";
+    }
+    if (!a.est_path.empty()) {
+        if (!write_vector(a.est_path, est.data(), n)) {
+            std::cerr << "Failed to write estimate to " << a.est_path << "\n";
+            return 1;
+        }
+        std::cout << "Saved estimate: " << a.est_path << "\n";
+    }
+    if (!a.hist_out.empty() && a.max_iter >= 1 && r.iterations >= 1 && r.iterations <= a.max_iter) {
+        std::ofstream h(a.hist_out);
+        h << "# costs " << std::fixed << std::setprecision(8) << 0.0 << " " << 0.0 << "\n# iter fraction\n";
+        h << r.iterations << " " << std::setprecision(10) << 1.0 << "\n";
+    }
+    return success ? 0 : 2;
+}
+
+void progress_line(std::ostream &os, const jbp_stats &s, double elapsed) {
+    const double fer = s.trials ? static_cast<double>(s.failures) / s.trials : 0.0;
+    os << "progress trials=" << s.trials << " failures=" << s.failures << " bp_fail=" << s.bp_fail
+       << " pp_success=" << s.pp_success << " fer=" << std::fixed << std::setprecision(6) << fer
+       << " fps=" << std::setprecision(2) << (elapsed > 0 ? s.trials / elapsed : 0.0) << " avg_iter="
+       << (s.trials ? static_cast<double>(s.total_iters) / s.trials : 0.0) << " gpu_ms=" << s.device_ms << "\n";
+}
+
+int simulate(jbp_ctx *ctx, const Args &a, int n) {
+    if (a.trials <= 0) {
+        std::cerr << "--trials must be positive in --simulate mode\n";
+        return 1;
+    }
+    if (a.trials != 1 && !a.est_path.empty()) {
+        std::cerr << "--est is only supported with --trials 1\n";
+        return 1;
+    }
+    const jbp_options o = options(a);
+    const long long first = a.trial_index >= 0 ? a.trial_index : 1;
+    std::vector<long long> hist(static_cast<size_t>(a.max_iter) + 1, 0), chunk_hist(hist.size());
+    std::vector<jbp_trial_result> per;
+    std::ofstream tsv;
+    if (!a.progress_tsv.empty()) tsv.open(a.progress_tsv);
+    jbp_stats acc{};
+    const auto t0 = std::chrono::steady_clock::now();
+    long long done = 0, next_report = a.report_every > 0 ? a.report_every : -1;
+    while (done < a.trials) {
+        const long long cnt = std::min(a.batch, a.trials - done);
+        jbp_stats st{};
+        std::fill(chunk_hist.begin(), chunk_hist.end(), 0);
+        if (a.min_fails > 0) per.resize(cnt);
+        if (jbp_simulate(ctx, &o, a.seed, first + done, cnt, a.p, a.sampler, &st, a.min_fails > 0 ? per.data() : nullptr,
+                         chunk_hist.data()) != JBP_OK) {
+            std::cerr << "simulate failed: " << jbp_last_error() << "\n";
+            return 1;
+        }
+        if (a.min_fails > 0 && acc.failures + st.failures >= a.min_fails) {
+            // stop at the trial that reaches --min-fails, as the reference loop does: decode the
+            // prefix again (same trial indices, same errors) for its exact counters
+            long long need = a.min_fails - acc.failures, cut = 0;
+            for (long long t = 0; t < cnt && need > 0; ++t, ++cut) need -= per[t].success ? 0 : 1;
+            std::fill(chunk_hist.begin(), chunk_hist.end(), 0);
+            if (jbp_simulate(ctx, &o, a.seed, first + done, cut, a.p, a.sampler, &st, nullptr, chunk_hist.data()) !=
+                JBP_OK) {
+                std::cerr << "simulate failed: " << jbp_last_error() << "\n";
+                return 1;
+            }
+            add_stats(acc, st);
+            for (size_t i = 0; i < hist.size(); ++i) hist[i] += chunk_hist[i];
+            done += cut;
+            break;
+        }
+        add_stats(acc, st);
+        for (size_t i = 0; i < hist.size(); ++i) hist[i] += chunk_hist[i];
+        done += cnt;
+        const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (next_report > 0 && done >= next_report) {
+            progress_line(std::cout, acc, el);
+            while (next_report <= done) next_report += a.report_every;
+        }
+        if (tsv) {
+            const double fer = static_cast<double>(acc.failures) / acc.trials;
+            tsv << static_cast<long long>(std::time(nullptr)) << "\t" << acc.trials << "\t" << acc.failures << "\t"
+                << acc.pp_success << "\t" << acc.ets_saved << "\t" << acc.flip_pp_success << "\t" << acc.stab_success
+                << "\t" << std::fixed << std::setprecision(2) << static_cast<double>(acc.total_iters) / acc.trials
+                << "\t" << acc.total_iters << "\t" << std::setprecision(6) << fer << "\t" << std::setprecision(2)
+                << (el > 0 ? acc.trials / el : 0.0) << "\tbatch\n";
+        }
+    }
+    const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (!a.est_path.empty()) {
+        std::vector<uint8_t> err(n), est(n);
+        jbp_trial_result r{};
+        jbp_stats st{};
+        if (jbp_sample_errors(ctx, a.seed, first, 1, a.p, a.sampler, err.data()) != JBP_OK ||
+            jbp_decode_errors(ctx, &o, 1, err.data(), a.p, est.data(), &r, &st) != JBP_OK) {
+            std::cerr << "decode failed: " << jbp_last_error() << "\n";
+            return 1;
+        }
+        if (!write_vector(a.est_path, est.data(), n)) {
+            std::cerr << "Failed to write estimate to " << a.est_path << "\n";
+            return 1;
+        }
+        std::cout << "Saved estimate: " << a.est_path << "\n";
+    }
+    // Run Summary (jointbp_ets.cpp:6419-6448)
+    const long long d = acc.trials;
+    const double fer = d ? static_cast<double>(acc.failures) / d : 0.0;
+    double lo = 0.0, hi = 0.0;
+    const bool ci = wilson(d, acc.failures, 1.96, lo, hi);
+    print_section("Run Summary");
+    std::cout << "trials=" << d << " failures=" << acc.failures << " bp_fail=" << acc.bp_fail
+              << " pp_success=" << acc.pp_success << " flip_pp_success=" << acc.flip_pp_success
+              << " stab_success=" << acc.stab_success << " ets_used=" << acc.ets_used << " ets_saved=" << acc.ets_saved
+              << " ets6_used=" << acc.ets6_used << " ets6_saved=" << acc.ets6_saved << " ets12_used=" << acc.ets12_used
+              << " ets12_saved=" << acc.ets12_saved << " fer=" << std::setprecision(8) << std::fixed << fer;
+    if (ci) std::cout << " ci95=[" << std::setprecision(8) << lo << "," << hi << "]";
+    std::cout << " iters=" << acc.total_iters << " avg_iter=" << std::setprecision(2)
+              << (d ? static_cast<double>(acc.total_iters) / d : 0.0)
+              << " avg_latency=" << latency_str(d ? elapsed / d : 0.0) << " exact_rate=" << std::setprecision(6)
+              << (d ? static_cast<double>(acc.exact) / d : 0.0) << " elapsed_s=" << std::setprecision(2) << elapsed
+              << "s\n";
+    std::cout << "gpu: precision=" << (a.precision == JBP_PREC_FP64 ? "fp64" : a.precision == JBP_PREC_FP32 ? "fp32"
+                                                                                                               : "fp16")
+              << " sampler=" << (a.sampler == JBP_SAMPLER_MT19937 ? "mt19937" : "philox") << " device_ms="
+              << std::setprecision(2) << acc.device_ms << " trials_per_s=" << (elapsed > 0 ? d / elapsed : 0.0)
+              << "\n";
+    if (!a.hist_out.empty() && d > 0 && hist.size() > 1) {
+        std::ofstream h(a.hist_out);
+        if (!h) {
+            std::cerr << "Failed to write histogram output: " << a.hist_out << "\n";
+        } else {
+            h << "# costs " << std::fixed << std::setprecision(8) << 0.0 << " " << 0.0 << "\n# iter fraction\n";
+            for (size_t i = 1; i < hist.size(); ++i)
+                if (hist[i]) h << i << " " << std::setprecision(10) << static_cast<double>(hist[i]) / d << "\n";
+        }
+    }
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+    Args a;
+    const int prc = parse(argc, argv, a);
+    if (prc == 2) return 0;
+    if (prc) return 1;
+    if (!a.seed_set) {
+        a.seed = static_cast<unsigned long long>(std::chrono::duration_cast<std::chrono::microseconds>(
+                                                     std::chrono::system_clock::now().time_since_epoch())
+                                                     .count());
+    }
+    if (a.params.empty()) {
+        std::cerr << "--params is required\n";
+        return 1;
+    }
+    if (a.simulate && !a.err_path.empty()) {
+        std::cerr << "--err cannot be used with --simulate\n";
+        return 1;
+    }
+    if (a.simulate && a.trial_index >= 0 && (a.trials != 1 || a.min_fails > 0)) {
+        std::cerr << "--trial-index requires --trials 1 and no --min-fails\n";
+        return 1;
+    }
+    if (!a.simulate) {
+        if (a.trials != 1 || a.min_fails > 0) {
+            std::cerr << "--trials/--min-fails are only valid with --simulate\n";
+            return 1;
+        }
+        if (!a.err_path.empty() && (!a.sx_path.empty() || !a.sz_path.empty())) {
+            std::cerr << "--err cannot be combined with --sx/--sz\n";
+            return 1;
+        }
+    }
+    if (!exists(a.params)) {
+        std::cerr << "Failed to read params: " << a.params << "\n";
+        return 1;
+    }
+    jbp_ctx *ctx = nullptr;
+    if (jbp_create_from_params(a.params.c_str(), nullptr, a.device, &ctx) != JBP_OK) {
+        std::cerr << "init failed: " << jbp_last_error() << "\n";
+        return 1;
+    }
+    if (a.enable_pp && load_ets(ctx, a)) {
+        std::cerr << "ETS load failed: " << jbp_last_error() << "\n";
+        jbp_destroy(ctx);
+        return 1;
+    }
+    int n = 0, mx = 0, mz = 0, rx = 0, rz = 0, ng = 0;
+    jbp_code_info(ctx, &n, &mx, &mz, &rx, &rz, &ng);
+    print_section("Code Summary");
+    const int k = n - rx - rz;
+    std::cout << "p=" << std::fixed << std::setprecision(6) << a.p << " n=" << n << " mx=" << mx << " mz=" << mz
+              << " rank_x=" << rx << " rank_z=" << rz << " stab_rank=" << rx + rz << " k=" << k
+              << " rate=" << (n ? static_cast<double>(k) / n : 0.0) << " ets_groups=" << ng << "\n";
+    const int rc = a.simulate ? simulate(ctx, a, n) : decode_single(ctx, a, n, mx, mz);
+    jbp_destroy(ctx);
+    return rc;
+}

@@ -129,7 +129,7 @@ std::string Engine::init(CodeModel model, int device) {
 
 void Engine::free_buffers() {
     for (void *&p : buf_.msg) { cudaFree(p); p = nullptr; }
-    cudaFree(buf_.trial); cudaFree(buf_.iter); cudaFree(buf_.flags); cudaFree(buf_.unsat);
+    cudaFree(buf_.trial); cudaFree(buf_.iter); cudaFree(buf_.flags); cudaFree(buf_.frz); cudaFree(buf_.unsat);
     cudaFree(buf_.prior); cudaFree(buf_.lprior); cudaFree(buf_.err);
     cudaFree(buf_.unsat_mask); cudaFree(buf_.estx); cudaFree(buf_.estz); cudaFree(buf_.synm);
     cudaFree(buf_.res_iters); cudaFree(buf_.res_flags); cudaFree(buf_.lists); cudaFree(buf_.counts);
@@ -195,6 +195,7 @@ std::string Engine::ensure_buffers(int S, int precision, bool damp, bool pp, int
     JBP_CUDA_TRY(cudaMalloc(&buf_.trial, sizeof(long long) * S), "cudaMalloc(slots)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.iter, sizeof(int) * S), "cudaMalloc(slots)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.flags, sizeof(int) * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.frz, sizeof(int) * S), "cudaMalloc(slots)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.unsat, sizeof(int) * 2 * S), "cudaMalloc(slots)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.prior, sizeof(double) * 4 * S), "cudaMalloc(slots)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.lprior, sizeof(float) * 8 * S), "cudaMalloc(slots)");
@@ -252,9 +253,13 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     if (rq.ntrials <= 0) return "";
     if (o.max_iter < 1) return "max_iter must be >= 1";
     if (o.precision < JBP_PREC_FP64 || o.precision > JBP_PREC_FP16) return "unknown precision";
-    if (!(rq.p > 0.0 && rq.p < 1.0)) return "p must be in (0, 1)";
+    if (o.use_prior) {
+        for (int i = 0; i < 4; ++i)
+            if (!(o.prior[i] >= 0.0 && o.prior[i] <= 1.0)) return "prior entries must be in [0, 1]";
+    } else if (!(rq.p > 0.0 && rq.p < 1.0)) {
+        return "p must be in (0, 1)";
+    }
     if (o.damping < 0.0 || o.damping > 1.0) return "damping must be in [0, 1]";
-    if (o.freeze_syn) return "freeze-syn is not available on the GPU in this build";
     const SideGraph &gx = model_.side[0], &gz = model_.side[1];
     if (!gx.regular || !gz.regular || gx.dc_max != gz.dc_max || gx.dv_max != gz.dv_max)
         return "the GPU kernels need a code with equal regular degrees on both sides";
@@ -303,6 +308,10 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     r.trial = buf_.trial;
     r.iter = buf_.iter;
     r.flags = buf_.flags;
+    r.freeze_syn = o.freeze_syn ? 1 : 0;
+    r.frz = buf_.frz;
+    r.use_prior = o.use_prior ? 1 : 0;
+    for (int i = 0; i < 4; ++i) r.prior4[i] = o.prior[i];
     r.unsat = buf_.unsat;
     r.prior = buf_.prior;
     r.lprior = buf_.lprior;

@@ -119,6 +119,13 @@ struct DevRun {
     int R;
     int *it;                        // global BP iteration counter
     unsigned *synm;                 // [(mx+mz)][G] target syndrome bits, same slot bit order
+    // freeze-syn (jointbp_ets.cpp:1884-1901, 2526-2535): once a side's syndrome matches at a
+    // check, its messages become deterministic copies of the decisions and stop updating.
+    int freeze_syn;
+    int *frz;                       // [S] bit0/1 X/Z frozen, bit2/3 X/Z frozen at the last check
+    // explicit prior (the jointbp_cuda.h interface passes it instead of p)
+    int use_prior;
+    double prior4[4];
     int *res_iters;                 // [S] iterations at retirement
     int *res_flags;                 // [S] ResultBit flags
     // work lists

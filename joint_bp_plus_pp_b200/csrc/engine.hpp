@@ -51,7 +51,7 @@ private:
         size_t msg_bytes = 0;
         void *msg[6] = {};            // c2v x/z, v2c x/z, v2c_hi x/z
         long long *trial = nullptr;
-        int *iter = nullptr, *flags = nullptr, *unsat = nullptr;
+        int *iter = nullptr, *flags = nullptr, *frz = nullptr, *unsat = nullptr;
         unsigned *unsat_mask = nullptr, *estx = nullptr, *estz = nullptr, *synm = nullptr;
         double *prior = nullptr;
         float *lprior = nullptr;

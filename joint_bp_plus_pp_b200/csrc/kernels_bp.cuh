@@ -75,6 +75,22 @@ __device__ __forceinline__ bool keeps_llr(const DevRun &run, int slot) {
     return run.pp && run.iter[slot] + 1 >= run.llr_from;
 }
 
+// freeze-syn state of a slot's side in a check kernel: 0 = update normally, 1 = frozen
+// (skip), 2 = frozen at the last check (write the deterministic messages, then skip).
+__device__ __forceinline__ int frozen_state(const DevRun &run, int slot, int side) {
+    if (!run.freeze_syn) return 0;
+    const int f = run.frz[slot];
+    if (!((f >> side) & 1)) return 0;
+    return ((f >> (2 + side)) & 1) ? 2 : 1;
+}
+
+// Decision bit (x-bit for side 0, z-bit for side 1) of variable v of a slot in the previous
+// iteration's planes, i.e. the estimate the freeze saw (freeze_side_msgs, jointbp_ets.cpp:1884).
+__device__ __forceinline__ int frozen_bit(const DevRun &run, int n, int side, int group, int lane, int v) {
+    const unsigned *planes = side ? run.estz : run.estx;
+    return (planes[plane_offset(run, n, 1) + static_cast<size_t>(group) * n + v] >> lane) & 1u;
+}
+
 // ------------------------------------------------------------------ FP64, bit-exact
 
 template <int DC, bool DAMP>
@@ -96,6 +112,18 @@ __global__ void __launch_bounds__(256) k_check_f64(DevCode code, DevRun run, Dev
         const double2 *v2c = static_cast<const double2 *>(side ? msg.v2c[1] : msg.v2c[0]) + base;
         const double2 *v2c_hi = static_cast<const double2 *>(side ? msg.v2c_hi[1] : msg.v2c_hi[0]) + base;
         double2 *c2v = static_cast<double2 *>(side ? msg.c2v[1] : msg.c2v[0]) + base;
+        const int fz = frozen_state(run, slot, side);
+        if (fz) {
+            // det_msg_xbit / det_msg_zbit: bit 0 -> (a, b) = (0.5, 0), bit 1 -> (0, 0.5)
+            if (fz == 2) {
+#pragma unroll
+                for (int i = 0; i < DC; ++i) {
+                    const int b = frozen_bit(run, code.n, side, group, lane, __ldg(code.s[side].chk_var + ch * DC + i));
+                    c2v[i * kGroup] = b ? make_double2(0.0, 0.5) : make_double2(0.5, 0.0);
+                }
+            }
+            continue;
+        }
         const double *pr = run.prior + 4 * slot;
         double q0[DC], q1[DC];
 #pragma unroll
@@ -245,8 +273,10 @@ __global__ void __launch_bounds__(256) k_var_f64(DevCode code, DevRun run, DevMs
             double2 *v2cz = static_cast<double2 *>(msg.v2c[1]);
             double2 *v2cx_hi = static_cast<double2 *>(msg.v2c_hi[0]);
             double2 *v2cz_hi = static_cast<double2 *>(msg.v2c_hi[1]);
+            const int frz = run.freeze_syn ? run.frz[slot] : 0;
 #pragma unroll
             for (int k = 0; k < DV; ++k) {
+                if (frz & 1) break;
                 const double EA = dmul(PA[k], SA[k + 1]), EB = dmul(PB[k], SB[k + 1]);
                 double n0 = dmul(dmul(p0, EA), ZA), n1 = dmul(dmul(p1, EB), ZA);
                 double n2 = dmul(dmul(p2, EA), ZB), n3 = dmul(dmul(p3, EB), ZB);
@@ -255,6 +285,7 @@ __global__ void __launch_bounds__(256) k_var_f64(DevCode code, DevRun run, DevMs
             }
 #pragma unroll
             for (int k = 0; k < DV; ++k) {
+                if (frz & 2) break;
                 const double FA = dmul(QA[k], TA[k + 1]), FB = dmul(QB[k], TB[k + 1]);
                 double n0 = dmul(dmul(p0, XA), FA), n1 = dmul(dmul(p1, XB), FA);
                 double n2 = dmul(dmul(p2, XA), FB), n3 = dmul(dmul(p3, XB), FB);
@@ -325,6 +356,18 @@ __global__ void __launch_bounds__(256) k_check_llr(DevCode code, DevRun run, Dev
         const size_t base = (static_cast<size_t>(ch) * G + group) * DC * kGroup + lane;
         const T *v2c = static_cast<const T *>(side ? msg.v2c[1] : msg.v2c[0]) + base;
         T *c2v = static_cast<T *>(side ? msg.c2v[1] : msg.c2v[0]) + base;
+        const int fz = frozen_state(run, slot, side);
+        if (fz) {
+            // deterministic messages: bit 0 -> +max, bit 1 -> -max
+            if (fz == 2) {
+#pragma unroll
+                for (int i = 0; i < DC; ++i) {
+                    const int b = frozen_bit(run, code.n, side, group, lane, __ldg(code.s[side].chk_var + ch * DC + i));
+                    st_msg<T>(c2v + i * kGroup, b ? -kLlrMax : kLlrMax);
+                }
+            }
+            continue;
+        }
         const float lp = run.lprior[8 * slot + 4 + side];
         float t[DC];
 #pragma unroll
@@ -393,6 +436,7 @@ __device__ __forceinline__ int var_llr_one(const DevCode &code, const DevRun &ru
         run.llr[static_cast<size_t>(slot) * n + v] = fabsf(lse2(w1, w3) - lse2(w0, w2));
         run.llr[(static_cast<size_t>(run.S) + slot) * n + v] = fabsf(lse2(w2, w3) - lse2(w0, w1));
     }
+    const int frz = run.freeze_syn ? run.frz[slot] : 0;
 #pragma unroll
     for (int k = 0; k < DV; ++k) {
         float ox_v = clamp_llr(Lam - lx[k] + Gx);
@@ -408,8 +452,8 @@ __device__ __forceinline__ int var_llr_one(const DevCode &code, const DevRun &ru
             ox_v = clamp_llr(lg2_approx(fmaxf(qx0, 1e-30f)) - lg2_approx(fmaxf(qx1, 1e-30f)));
             oz_v = clamp_llr(lg2_approx(fmaxf(qz0, 1e-30f)) - lg2_approx(fmaxf(qz1, 1e-30f)));
         }
-        st_msg<T>(v2cx + ox[k], ox_v);
-        st_msg<T>(v2cz + oz[k], oz_v);
+        if (!(frz & 1)) st_msg<T>(v2cx + ox[k], ox_v);
+        if (!(frz & 2)) st_msg<T>(v2cz + oz[k], oz_v);
     }
     return best;
 }

@@ -175,7 +175,8 @@ static __global__ void k_retire(DevRun run) {
     const int group = run.groups[gi];
     const int slot = group * kGroup + lane;
     const int G = run.S / kGroup;
-    const unsigned bad = run.unsat_mask[group] | run.unsat_mask[G + group];
+    const unsigned ux_mask = run.unsat_mask[group], uz_mask = run.unsat_mask[G + group];
+    const unsigned bad = ux_mask | uz_mask;
     const unsigned dp = run.pp ? run.dprev[group] : 0u, dpp = run.pp ? run.dpprev[group] : 0u;
     __syncwarp();
     if (lane == 0) {
@@ -190,6 +191,16 @@ static __global__ void k_retire(DevRun run) {
     const int k1 = run.iter[slot] + 1;
     run.iter[slot] = k1;
     const bool conv = check_due(run, k1) && !((bad >> lane) & 1u);
+    if (run.freeze_syn) {
+        // a side whose syndrome matches at this check freezes; the check kernel of the next
+        // iteration writes its deterministic messages (bits 2, 3) once
+        int f = run.frz[slot] & 3;
+        if (check_due(run, k1)) {
+            if (!((ux_mask >> lane) & 1u) && !(f & 1)) f |= 1 | 4;
+            if (!((uz_mask >> lane) & 1u) && !(f & 2)) f |= 2 | 8;
+        }
+        run.frz[slot] = f;
+    }
     if (run.pp) {
         const int S = run.S;
         const int ux = run.unsat[slot], uz = run.unsat[S + slot];
@@ -396,11 +407,17 @@ static __global__ void k_refill(DevRun run, int precision) {
                 run.pstate[slot] = 0;
                 run.stall_same[slot] = 0;
             }
-            // prior = normalize(1-p, p/3, p/3, p/3) (jointbp_ets.cpp:5484-5485)
-            double p0 = __dsub_rn(1.0, run.p), p1 = __ddiv_rn(run.p, 3.0), p2 = p1, p3 = p1;
-            double s = __dadd_rn(__dadd_rn(__dadd_rn(p0, p1), p2), p3);
-            if (s <= 0.0) { p0 = p1 = p2 = p3 = 0.25; }
-            else { p0 = __ddiv_rn(p0, s); p1 = __ddiv_rn(p1, s); p2 = __ddiv_rn(p2, s); p3 = __ddiv_rn(p3, s); }
+            if (run.freeze_syn) run.frz[slot] = 0;
+            // prior = normalize(1-p, p/3, p/3, p/3) (jointbp_ets.cpp:5484-5485), or the given one
+            double p0, p1, p2, p3;
+            if (run.use_prior) {
+                p0 = run.prior4[0]; p1 = run.prior4[1]; p2 = run.prior4[2]; p3 = run.prior4[3];
+            } else {
+                p0 = __dsub_rn(1.0, run.p); p1 = __ddiv_rn(run.p, 3.0); p2 = p1; p3 = p1;
+                const double s = __dadd_rn(__dadd_rn(__dadd_rn(p0, p1), p2), p3);
+                if (s <= 0.0) { p0 = p1 = p2 = p3 = 0.25; }
+                else { p0 = __ddiv_rn(p0, s); p1 = __ddiv_rn(p1, s); p2 = __ddiv_rn(p2, s); p3 = __ddiv_rn(p3, s); }
+            }
             if (precision == JBP_PREC_FP64) {
                 double *pr = run.prior + 4 * slot;
                 pr[0] = p0; pr[1] = p1; pr[2] = p2; pr[3] = p3;

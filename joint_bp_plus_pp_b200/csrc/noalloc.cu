@@ -135,7 +135,7 @@ extern "C" int jbp_decode_syndromes_noalloc(jbp_ctx *ctx, const jbp_options *opt
         return set_last_error(JBP_ERR_ARG, "jbp_decode_syndromes_noalloc: invalid argument");
     if (ntrials == 0) return JBP_OK;
     if (opt->max_iter < 1) return set_last_error(JBP_ERR_ARG, "max_iter must be >= 1");
-    if (!(p > 0.0 && p < 1.0)) return set_last_error(JBP_ERR_ARG, "p must be in (0, 1)");
+    if (!opt->use_prior && !(p > 0.0 && p < 1.0)) return set_last_error(JBP_ERR_ARG, "p must be in (0, 1)");
     if (opt->enable_pp || opt->freeze_syn || opt->damping > 0.0)
         return set_last_error(JBP_ERR_UNSUPPORTED,
                               "jbp_decode_syndromes_noalloc decodes plain BP only (no post-processing, "
@@ -173,6 +173,8 @@ extern "C" int jbp_decode_syndromes_noalloc(jbp_ctx *ctx, const jbp_options *opt
     r.check_warmup = opt->check_warmup > 0 ? opt->check_warmup : 0;
     r.check_interval = opt->check_interval > 0 ? opt->check_interval : 1;
     r.source = kSrcSyndromes;
+    r.use_prior = opt->use_prior ? 1 : 0;
+    for (int i = 0; i < 4; ++i) r.prior4[i] = opt->prior[i];
     r.p = p;
     r.first_trial = 0;
     r.ntrials = ntrials;

@@ -25,13 +25,15 @@ HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parent))
 from oracle_bind import ETS_DIR, PARAMS, REF_DIR, Reference  # noqa: E402
 
-# (name, seed, p, max_iter, enable_pp, flip_hist, trials, vectors_for_first)
+# (name, seed, p, max_iter, enable_pp, flip_hist, trials, vectors_for_first[, freeze_syn])
 SIM_CASES = [
     ("p050_mi50_nopp_s1", 1, 0.05, 50, False, 5, range(1, 201), 16),
     ("p040_mi1000_nopp_s106", 106, 0.04, 1000, False, 5, range(1, 101), 16),
     ("p050_mi200_pp_s305", 305, 0.05, 200, True, 5, range(1, 41), 40),
     ("p060_mi120_pp_s7", 7, 0.06, 120, True, 5, range(1, 25), 24),
     ("p055_mi150_pp_fh0_s11", 11, 0.055, 150, True, 0, range(1, 21), 20),
+    ("p055_mi60_nopp_frz_s21", 21, 0.055, 60, False, 5, range(1, 121), 32, True),
+    ("p060_mi130_pp_frz_s23", 23, 0.06, 130, True, 5, range(1, 25), 24, True),
 ]
 
 
@@ -128,15 +130,67 @@ def stage_trials(ref):
           "post", sum(c["record"]["ets_applied_post"] for c in cases), flush=True)
 
 
+def simulate_cases(ref, cases):
+    """Per-trial reference records (and the first vectors) of seeded simulate runs."""
+    for case in cases:
+        name, seed, p, mi, pp, fh, trials, nvec = case[:8]
+        frz = bool(case[8]) if len(case) > 8 else False
+        recs, errs, ests = [], [], []
+        for k, t in enumerate(trials):
+            d = ref.simulate_trial(seed, t, p, mi, flip_hist=fh, enable_pp=pp, freeze_syn=frz, want_vectors=True)
+            e, s = d.pop("err"), d.pop("est")
+            d["err_crc"], d["est_crc"] = crc(e), crc(s)
+            recs.append(d)
+            if k < nvec:
+                errs.append(e)
+                ests.append(s)
+        meta = {"seed": seed, "p": p, "max_iter": mi, "enable_pp": pp, "flip_hist": fh, "freeze_syn": frz,
+                "records": recs}
+        (HERE / f"sim_{name}.json").write_text(json.dumps(meta))
+        np.savez_compressed(HERE / f"vec_{name}.npz", err=np.array(errs, np.uint8), est=np.array(ests, np.uint8))
+        print(name, "failures", sum(1 - r["success"] for r in recs), "pp", sum(r["pp_success_this"] for r in recs),
+              flush=True)
+
+
+def cli_summaries(quick):
+    """Run Summary lines of the unmodified reference CLI (cli_summaries.json)."""
+    summaries = {}
+    cli_cases = [("p050_mi50_nopp_s1_t200", ["--simulate", "--p", "0.05", "--trials", "200", "--max-iter", "50",
+                                             "--no-pp", "--seed", "1", "--report-every", "0"]),
+                 ("p050_mi200_pp_s305_t40", ["--simulate", "--p", "0.05", "--trials", "40", "--max-iter", "200",
+                                             "--flip-hist", "5", "--seed", "305", "--report-every", "0"]),
+                 ("p055_mi60_nopp_frz_s21_t60", ["--simulate", "--p", "0.055", "--trials", "60", "--max-iter", "60",
+                                                 "--no-pp", "--freeze-syn", "--seed", "21", "--report-every", "0"]),
+                 ("p050_mi50_nopp_s1_t20", ["--simulate", "--p", "0.05", "--trials", "20", "--max-iter", "50",
+                                            "--no-pp", "--seed", "1", "--report-every", "0"])]
+    if not quick:
+        cli_cases.append(("p050_mi50_nopp_s1_t1000", ["--simulate", "--p", "0.05", "--trials", "1000",
+                                                      "--max-iter", "50", "--no-pp", "--seed", "1",
+                                                      "--report-every", "0"]))
+    for name, a in cli_cases:
+        rc, line, _ = run_cli(a)
+        summaries[name] = {"args": a, "rc": rc, "summary": parse_summary(line) if line else None}
+        print(name, line, flush=True)
+    (HERE / "cli_summaries.json").write_text(json.dumps(summaries, indent=1))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--quick", action="store_true", help="skip the 1000-trial CLI summary")
     ap.add_argument("--stage-only", action="store_true", help="regenerate only pp_stage_trials.json")
+    ap.add_argument("--cli-only", action="store_true", help="regenerate only cli_summaries.json")
+    ap.add_argument("--sim", action="append", default=[], help="regenerate only these simulate cases")
     args = ap.parse_args()
     ref = Reference()
     lib = ref.lib
     if args.stage_only:
         stage_trials(ref)
+        return
+    if args.cli_only:
+        cli_summaries(args.quick)
+        return
+    if args.sim:
+        simulate_cases(ref, [c for c in SIM_CASES if c[0] in args.sim])
         return
 
     # --- code known answers (README start-up block) ---
@@ -167,22 +221,7 @@ def main():
     kat["sampler"] = samp
     (HERE / "kat.json").write_text(json.dumps(kat, indent=1))
 
-    # --- per-trial simulate records ---
-    for name, seed, p, mi, pp, fh, trials, nvec in SIM_CASES:
-        recs, errs, ests = [], [], []
-        for k, t in enumerate(trials):
-            d = ref.simulate_trial(seed, t, p, mi, flip_hist=fh, enable_pp=pp, want_vectors=True)
-            e, s = d.pop("err"), d.pop("est")
-            d["err_crc"], d["est_crc"] = crc(e), crc(s)
-            recs.append(d)
-            if k < nvec:
-                errs.append(e)
-                ests.append(s)
-        meta = {"seed": seed, "p": p, "max_iter": mi, "enable_pp": pp, "flip_hist": fh, "records": recs}
-        (HERE / f"sim_{name}.json").write_text(json.dumps(meta))
-        np.savez_compressed(HERE / f"vec_{name}.npz", err=np.array(errs, np.uint8), est=np.array(ests, np.uint8))
-        print(name, "failures", sum(1 - r["success"] for r in recs), "pp", sum(r["pp_success_this"] for r in recs),
-              flush=True)
+    simulate_cases(ref, SIM_CASES)
 
     # --- |LLR| goldens (last-iteration |LLR| of plain BP; they order the OSD columns) ---
     llr = {}
@@ -199,21 +238,7 @@ def main():
                         **{k + "_est": v[2] for k, v in llr.items()},
                         **{k + "_iters": np.array([v[3]]) for k, v in llr.items()})
 
-    # --- reference CLI run summaries ---
-    summaries = {}
-    cli_cases = [("p050_mi50_nopp_s1_t200", ["--simulate", "--p", "0.05", "--trials", "200", "--max-iter", "50",
-                                             "--no-pp", "--seed", "1", "--report-every", "0"]),
-                 ("p050_mi200_pp_s305_t40", ["--simulate", "--p", "0.05", "--trials", "40", "--max-iter", "200",
-                                             "--flip-hist", "5", "--seed", "305", "--report-every", "0"])]
-    if not args.quick:
-        cli_cases.append(("p050_mi50_nopp_s1_t1000", ["--simulate", "--p", "0.05", "--trials", "1000",
-                                                      "--max-iter", "50", "--no-pp", "--seed", "1",
-                                                      "--report-every", "0"]))
-    for name, a in cli_cases:
-        rc, line, _ = run_cli(a)
-        summaries[name] = {"args": a, "rc": rc, "summary": parse_summary(line) if line else None}
-        print(name, line, flush=True)
-    (HERE / "cli_summaries.json").write_text(json.dumps(summaries, indent=1))
+    cli_summaries(args.quick)
     stage_trials(ref)
 
 

@@ -29,6 +29,25 @@ def exported(lib):
     return {line.split()[-1] for line in out.splitlines() if line.strip()}
 
 
+def test_dropin_library_exports_the_reference_boundary():
+    """lib/libjointbp_cuda.so exports the three jointbp_cuda.h functions with the reference's
+    C++ signatures (jointbp_cuda.h:46-62), so the reference host program links against it."""
+    lib = LIBDIR / "libjointbp_cuda.so"
+    assert lib.exists(), "run python -m joint_bp_plus_pp_b200.build"
+    out = subprocess.run(["nm", "-DC", "--defined-only", str(lib)], capture_output=True, text=True,
+                         check=True).stdout
+    sigs = {re.sub(r"^\S+\s+\S+\s+", "", l) for l in out.splitlines() if "cuda_bp_" in l}
+    s = "std::__cxx11::basic_string<char, std::char_traits<char>, std::allocator<char> >*"
+    v = "std::vector<int, std::allocator<int> > const&"
+    assert f"cuda_bp_create(CudaBPGraph const&, int, {s})" in sigs
+    assert "cuda_bp_destroy(CudaBPContext*)" in sigs
+    assert (f"cuda_bp_decode(CudaBPContext*, {v}, {v}, CudaMsg const&, int, int, int, bool, bool, bool, double, "
+            f"CudaBPResult&, {s})") in sigs
+    for name in declared_functions(INCLUDE / "jointbp_cuda.h"):
+        assert any(x.startswith(name + "(") for x in sigs), name
+    ctypes.CDLL(str(lib))
+
+
 def test_library_exports_all_declared_symbols():
     lib = LIBDIR / "libjbp_b200.so"
     assert lib.exists(), "run python -m joint_bp_plus_pp_b200.build"

@@ -1,0 +1,112 @@
+"""bin/jointbp_b200, the reference command line over the batched GPU decoder.
+
+GPU runs are compared with the unmodified reference CLI's Run Summaries and per-trial records
+(golden fixtures), including post-processing, which the reference runs only on its CPU path.
+"""
+import json
+import re
+import subprocess
+import zlib
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT, load_sim_case
+
+CLI = ROOT / "joint_bp_plus_pp_b200" / "bin" / "jointbp_b200"
+PARAMS = ROOT / "joint_bp_plus_pp_b200" / "data" / "H_P768_J3_L12_dmax3_nc0-3_1-2_seed11579811919164041.txt"
+SUMMARY_KEYS = ("trials", "failures", "bp_fail", "pp_success", "flip_pp_success", "stab_success", "ets_used",
+                "ets_saved", "ets6_used", "ets6_saved", "ets12_used", "ets12_saved", "fer", "ci95", "iters",
+                "avg_iter", "exact_rate")
+
+pytestmark = pytest.mark.skipif(not CLI.exists(), reason="CLI not built")
+
+
+def run(args, timeout=900):
+    r = subprocess.run([str(CLI), "--params", str(PARAMS)] + args, capture_output=True, text=True, timeout=timeout,
+                       cwd=str(PARAMS.parent))
+    line = [l for l in r.stdout.splitlines() if l.startswith("trials=")]
+    s = dict(re.findall(r"(\w+)=(\[[^\]]*\]|\S+)", line[-1])) if line else None
+    return r, s
+
+
+def crc(a):
+    return zlib.crc32(np.ascontiguousarray(a, np.uint8).tobytes()) & 0xFFFFFFFF
+
+
+def test_help_and_usage_errors():
+    r = subprocess.run([str(CLI), "--help"], capture_output=True, text=True)
+    assert r.returncode == 0 and "--simulate" in r.stdout
+    r = subprocess.run([str(CLI), "--params", str(PARAMS), "--bogus"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Unknown argument" in r.stderr
+    r = subprocess.run([str(CLI), "--simulate"], capture_output=True, text=True)
+    assert r.returncode == 1 and "--params is required" in r.stderr
+    r = subprocess.run([str(CLI), "--params", str(PARAMS), "--trials", "5"], capture_output=True, text=True)
+    assert r.returncode == 1 and "only valid with --simulate" in r.stderr
+
+
+def test_without_gpu_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    r, s = run(["--simulate", "--p", "0.05", "--trials", "4", "--seed", "1"])
+    assert r.returncode == 1 and "init failed" in r.stderr and s is None
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["p050_mi50_nopp_s1_t200", "p050_mi200_pp_s305_t40", "p055_mi60_nopp_frz_s21_t60"])
+def test_run_summary_equals_reference(name):
+    g = json.loads((GOLDEN / "cli_summaries.json").read_text())[name]
+    r, s = run(g["args"] + ["--batch", "64"])
+    assert r.returncode == 0, r.stderr
+    for k in SUMMARY_KEYS:
+        assert s[k] == g["summary"][k], (k, s[k], g["summary"][k])
+
+
+@pytest.mark.gpu
+def test_min_fails_stops_at_the_reference_trial():
+    meta, _, _ = load_sim_case("p050_mi50_nopp_s1")
+    recs = meta["records"]
+    fails = np.cumsum([1 - r["success"] for r in recs])
+    cut = int(np.searchsorted(fails, 2) + 1)
+    r, s = run(["--simulate", "--p", "0.05", "--max-iter", "50", "--no-pp", "--seed", "1", "--trials", "100000",
+                "--min-fails", "2", "--batch", "1024", "--report-every", "0"])
+    assert r.returncode == 0, r.stderr
+    assert int(s["trials"]) == cut and int(s["failures"]) == 2
+    assert int(s["iters"]) == sum(x["iterations"] for x in recs[:cut])
+
+
+@pytest.mark.gpu
+def test_err_and_syndrome_modes(tmp_path, oracle):
+    meta, errs, ests = load_sim_case("p050_mi50_nopp_s1")
+    k = next(i for i, r in enumerate(meta["records"][:len(errs)]) if not r["success"])
+    for i in (0, k):
+        ef = tmp_path / f"err{i}.txt"
+        ef.write_text("\n".join(str(int(v)) for v in errs[i]) + "\n")
+        out = tmp_path / f"est{i}.txt"
+        r, _ = run(["--err", str(ef), "--p", "0.05", "--max-iter", "50", "--no-pp", "--est", str(out)])
+        ok = meta["records"][i]["success"]
+        assert r.returncode == (0 if ok else 2), r.stderr
+        assert f"decode_success={'true' if ok else 'false'}" in r.stdout
+        est = np.array([int(x) for x in out.read_text().split()], np.uint8)
+        assert (est == ests[i]).all()
+        sx, sz = oracle.syndrome(errs[i])
+        (tmp_path / "sx.txt").write_text("\n".join(map(str, sx)) + "\n")
+        (tmp_path / "sz.txt").write_text("\n".join(map(str, sz)) + "\n")
+        out2 = tmp_path / f"est_s{i}.txt"
+        r, _ = run(["--sx", str(tmp_path / "sx.txt"), "--sz", str(tmp_path / "sz.txt"), "--p", "0.05",
+                    "--max-iter", "50", "--no-pp", "--est", str(out2)])
+        assert r.returncode in (0, 2), r.stderr
+        assert out2.read_text() == out.read_text()
+
+
+@pytest.mark.gpu
+def test_trial_index_with_post_processing():
+    """Trial 19 of seed 305 is saved by in-loop flip post-processing in the reference."""
+    meta, _, _ = load_sim_case("p050_mi200_pp_s305")
+    rec = next(r for r in meta["records"] if r["trial_idx"] == 19)
+    assert rec["flip_pp_ok"] == 1
+    r, s = run(["--simulate", "--p", "0.05", "--max-iter", "200", "--flip-hist", "5", "--seed", "305",
+                "--trials", "1", "--trial-index", "19", "--est", "/dev/stdout"])
+    assert r.returncode == 0, r.stderr
+    assert int(s["pp_success"]) == 1 and int(s["flip_pp_success"]) == 1 and int(s["iters"]) == rec["iterations"]

@@ -13,7 +13,7 @@ from conftest import load_sim_case
 
 pytestmark = pytest.mark.gpu
 
-NOPP_CASES = ["p050_mi50_nopp_s1", "p040_mi1000_nopp_s106"]
+NOPP_CASES = ["p050_mi50_nopp_s1", "p040_mi1000_nopp_s106", "p055_mi60_nopp_frz_s21"]
 
 
 def crc(a):
@@ -27,10 +27,14 @@ def opts(**kw):
     return Options(**base)
 
 
+def meta_opts(meta, **kw):
+    return opts(max_iter=meta["max_iter"], freeze_syn=meta.get("freeze_syn", False), **kw)
+
+
 @pytest.mark.parametrize("name", NOPP_CASES)
 def test_fp64_decode_errors_bit_exact_vs_golden(decoder, name):
     meta, errs, ests = load_sim_case(name)
-    st, res, est = decoder.decode_errors(errs, meta["p"], opts(max_iter=meta["max_iter"]))
+    st, res, est = decoder.decode_errors(errs, meta["p"], meta_opts(meta))
     recs = meta["records"][:len(errs)]
     assert (est == ests).all()
     assert list(res["iterations"]) == [r["iterations"] for r in recs]
@@ -46,7 +50,7 @@ def test_fp64_simulate_device_mt_sampler_matches_golden(decoder, name):
     meta, _, _ = load_sim_case(name)
     recs = meta["records"]
     first = recs[0]["trial_idx"]
-    st, res = decoder.simulate(meta["seed"], len(recs), meta["p"], opts(max_iter=meta["max_iter"]), first_trial=first,
+    st, res = decoder.simulate(meta["seed"], len(recs), meta["p"], meta_opts(meta), first_trial=first,
                                sampler="mt19937")
     for r, g in zip(res, recs):
         assert (r["iterations"], r["bp_ok"], r["success"], r["exact"], r["stab_equiv"]) == \
@@ -74,7 +78,7 @@ def test_fp64_decode_syndromes(decoder, oracle):
     meta, errs, ests = load_sim_case("p050_mi50_nopp_s1")
     sx = np.stack([oracle.syndrome(e)[0] for e in errs[:8]])
     sz = np.stack([oracle.syndrome(e)[1] for e in errs[:8]])
-    st, res, est = decoder.decode_syndromes(sx, sz, meta["p"], opts(max_iter=meta["max_iter"]))
+    st, res, est = decoder.decode_syndromes(sx, sz, meta["p"], meta_opts(meta))
     assert (est == ests[:8]).all()
     assert list(res["iterations"]) == [r["iterations"] for r in meta["records"][:8]]
     assert list(res["syndrome_ok"]) == [r["syndrome_ok"] for r in meta["records"][:8]]
@@ -89,6 +93,41 @@ def test_fp64_damping_vs_oracle(decoder, oracle):
         sx, sz = oracle.syndrome(err[t])
         o = oracle.decode(sx, sz, p, mi, damping=d, enable_pp=False)
         assert (o["est"] == est[t]).all() and o["iterations"] == res["iterations"][t], t
+
+
+def test_fp64_freeze_damping_vs_oracle(decoder, oracle):
+    """freeze-syn together with damping (the full v2c 4-vectors) and explicit priors."""
+    from joint_bp_plus_pp_b200 import sample_reference_errors
+    p, mi, d = 0.055, 40, 0.25
+    err = sample_reference_errors(decoder.n, 9, 1, 24, p)
+    st, res, est = decoder.decode_errors(err, p, opts(max_iter=mi, damping=d, freeze_syn=True))
+    for t in range(24):
+        sx, sz = oracle.syndrome(err[t])
+        o = oracle.decode(sx, sz, p, mi, damping=d, freeze_syn=True, enable_pp=False)
+        assert (o["est"] == est[t]).all() and o["iterations"] == res["iterations"][t], t
+
+
+def test_explicit_prior_equals_p(decoder):
+    """A prior passed as probabilities decodes exactly like the prior the decoder derives from p."""
+    from joint_bp_plus_pp_b200 import sample_reference_errors
+    p = 0.05
+    q = [1 - p, p / 3, p / 3, p / 3]
+    s = ((q[0] + q[1]) + q[2]) + q[3]
+    prior = tuple(x / s for x in q)
+    err = sample_reference_errors(decoder.n, 3, 1, 64, p)
+    _, r1, e1 = decoder.decode_errors(err, p, opts(max_iter=50))
+    _, r2, e2 = decoder.decode_errors(err, 0.3, opts(max_iter=50, prior=prior))
+    assert (e1 == e2).all() and (r1["iterations"] == r2["iterations"]).all()
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+def test_llr_freeze_runs(decoder, prec):
+    """freeze-syn behind the LLR decoders: outcomes close to FP64 freeze-syn on the same errors."""
+    meta, errs, _ = load_sim_case("p055_mi60_nopp_frz_s21")
+    s64, r64, _ = decoder.decode_errors(errs, meta["p"], meta_opts(meta), want_est=False)
+    slo, rlo, _ = decoder.decode_errors(errs, meta["p"], meta_opts(meta, precision=prec), want_est=False)
+    assert slo["trials"] == len(errs)
+    assert abs(slo["failures"] - s64["failures"]) <= max(3, len(errs) // 5)
 
 
 def test_check_interval_schedule(decoder):

@@ -37,7 +37,7 @@ def golden_record(g):
 def opts_for(meta, precision="fp64"):
     from joint_bp_plus_pp_b200 import Options
     return Options(precision=precision, max_iter=meta["max_iter"], flip_hist=meta["flip_hist"],
-                   enable_pp=meta["enable_pp"])
+                   enable_pp=meta["enable_pp"], freeze_syn=meta.get("freeze_syn", False))
 
 
 @pytest.mark.parametrize("name", PP_CASES)

@@ -60,7 +60,8 @@ def test_simulate_records_golden(oracle, name):
     meta, errs, ests = load_sim_case(name)
     for k, rec in enumerate(meta["records"]):
         d = oracle.simulate_trial(meta["seed"], rec["trial_idx"], meta["p"], meta["max_iter"],
-                                  flip_hist=meta["flip_hist"], enable_pp=meta["enable_pp"], want_vectors=True)
+                                  flip_hist=meta["flip_hist"], enable_pp=meta["enable_pp"],
+                                  freeze_syn=meta.get("freeze_syn", False), want_vectors=True)
         err, est = d.pop("err"), d.pop("est")
         exp = dict(rec)
         assert crc(err) == exp.pop("err_crc"), (name, rec["trial_idx"])
@@ -114,11 +115,12 @@ def test_cli_summary_counts_match_records():
 @pytest.mark.skipif(not reference_available(), reason="reference harness not built here")
 def test_oracle_matches_reference_fresh_trials(oracle):
     ref = Reference()
-    cases = [(4242, 0.045, 60, False, range(1, 13)), (77, 0.058, 110, True, range(1, 5))]
-    for seed, p, mi, pp, idxs in cases:
+    cases = [(4242, 0.045, 60, False, 0.0, False, range(1, 13)), (77, 0.058, 110, True, 0.0, False, range(1, 5)),
+             (9, 0.055, 40, False, 0.25, True, range(1, 9))]
+    for seed, p, mi, pp, damp, frz, idxs in cases:
         for t in idxs:
-            a = oracle.simulate_trial(seed, t, p, mi, enable_pp=pp, want_vectors=True)
-            b = ref.simulate_trial(seed, t, p, mi, enable_pp=pp, want_vectors=True)
+            a = oracle.simulate_trial(seed, t, p, mi, enable_pp=pp, damping=damp, freeze_syn=frz, want_vectors=True)
+            b = ref.simulate_trial(seed, t, p, mi, enable_pp=pp, damping=damp, freeze_syn=frz, want_vectors=True)
             assert (a.pop("est") == b.pop("est")).all()
             assert (a.pop("err") == b.pop("err")).all()
             assert a == b, (seed, t)
