@@ -35,6 +35,14 @@ extern "C" {
 #define JBP_PREC_FP32 1        /* LLR messages in FP32 */
 #define JBP_PREC_FP16 2        /* LLR messages stored in FP16, FP32 arithmetic */
 
+/* Decoding engines.  RESIDENT: one persistent thread block per SM keeps a whole trial's BP
+ * state in shared memory (FP16 precision on quasi-cyclic affine codes such as the shipped APM
+ * code).  SLOTS: trials in HBM-resident slots, one kernel per BP phase (every precision and
+ * option).  AUTO picks RESIDENT where it applies, else SLOTS. */
+#define JBP_ENGINE_AUTO 0
+#define JBP_ENGINE_RESIDENT 1
+#define JBP_ENGINE_SLOTS 2
+
 #define JBP_SAMPLER_PHILOX 0   /* counter-based Philox4x32-10 keyed by (seed, trial index) */
 #define JBP_SAMPLER_MT19937 1  /* the reference stream: splitmix64 seed -> mt19937_64 per trial */
 
@@ -55,6 +63,7 @@ typedef struct {
     int profile;           /* time the check and variable kernels with CUDA events (jbp_stats) */
     int use_prior;         /* 1: decode with `prior` below instead of normalize(1-p, p/3, p/3, p/3) */
     double prior[4];       /* probabilities of I, X, Z, Y (used as given, as cuda_bp_decode does) */
+    int engine;            /* JBP_ENGINE_* (default AUTO) */
 } jbp_options;
 
 /* Per-trial outcome (16 bytes). */

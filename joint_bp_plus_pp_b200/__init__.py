@@ -23,6 +23,7 @@ DEFAULT_PARAMS = DATA_DIR / "H_P768_J3_L12_dmax3_nc0-3_1-2_seed11579811919164041
 
 PREC = {"fp64": 0, "fp32": 1, "fp16": 2}
 SAMPLER = {"philox": 0, "mt19937": 1}
+ENGINE = {"auto": 0, "resident": 1, "slots": 2}
 ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "I/O error", 4: "unsupported", 5: "timeout"}
 
 
@@ -37,7 +38,7 @@ class COptions(ctypes.Structure):
                 ("flip_hist", ctypes.c_int), ("enable_pp", ctypes.c_int), ("freeze_syn", ctypes.c_int),
                 ("check_warmup", ctypes.c_int), ("check_interval", ctypes.c_int), ("slots", ctypes.c_int),
                 ("iters_per_launch", ctypes.c_int), ("watchdog_ms", ctypes.c_int), ("profile", ctypes.c_int),
-                ("use_prior", ctypes.c_int), ("prior", ctypes.c_double * 4)]
+                ("use_prior", ctypes.c_int), ("prior", ctypes.c_double * 4), ("engine", ctypes.c_int)]
 
 
 TRIAL_DTYPE = np.dtype([("iterations", np.int32), ("syndrome_ok", np.uint8), ("bp_ok", np.uint8),
@@ -81,12 +82,14 @@ class Options:
     watchdog_ms: int = 0
     profile: bool = False
     prior: tuple = None    # (I, X, Z, Y) probabilities used as given instead of those of p
+    engine: str = "auto"   # "auto", "resident" (shared-memory trial-resident tier) or "slots"
 
     def to_c(self):
         pr = (ctypes.c_double * 4)(*(self.prior or (0.0, 0.0, 0.0, 0.0)))
         return COptions(PREC[self.precision], self.max_iter, self.damping, self.flip_hist, int(self.enable_pp),
                         int(self.freeze_syn), self.check_warmup, self.check_interval, self.slots,
-                        self.iters_per_launch, self.watchdog_ms, int(self.profile), int(self.prior is not None), pr)
+                        self.iters_per_launch, self.watchdog_ms, int(self.profile), int(self.prior is not None), pr,
+                        ENGINE[self.engine])
 
 
 _lib = None

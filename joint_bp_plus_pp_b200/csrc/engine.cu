@@ -2,6 +2,7 @@
 #include "engine.hpp"
 
 #include <algorithm>
+#include <memory>
 #include <chrono>
 #include <cstring>
 #include <sstream>
@@ -9,6 +10,7 @@
 #include "kernels_bp.cuh"
 #include "kernels_slots.cuh"
 #include "kernels_pp.cuh"
+#include "kernels_resident.cuh"
 
 namespace jbp {
 
@@ -88,6 +90,8 @@ size_t msg_elem_bytes(int precision) {
 
 Engine::~Engine() {
     free_buffers();
+    delete rcode_;
+    cudaFree(res_cnt_);
     for (void *p : code_allocs_) cudaFree(p);
     for (void *p : ets_allocs_) cudaFree(p);
 }
@@ -100,6 +104,8 @@ std::string Engine::init(CodeModel model, int device) {
     if (device < 0 || device >= ndev) return "CUDA device " + std::to_string(device) + " not available";
     JBP_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
     JBP_CUDA_TRY(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device), "device attributes");
+    JBP_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin_, cudaDevAttrMaxSharedMemoryPerBlockOptin, device),
+                 "device attributes");
     dcode_.n = model_.n;
     dcode_.words = (model_.n + 63) / 64;
     for (int s = 0; s < 2; ++s) {
@@ -124,6 +130,165 @@ std::string Engine::init(CodeModel model, int device) {
         if (!e.empty()) return e;
         dcode_.pivot_row[s] = p;
     }
+    res_code_why_ = build_res_code();
+    res_code_ok_ = res_code_why_.empty();
+    return "";
+}
+
+// ---------------------------------------------------------------- trial-resident tier
+
+namespace {
+
+long long host_mod(long long x, long long m) {
+    x %= m;
+    return x < 0 ? x + m : x;
+}
+
+bool host_inverse(long long a, long long m, long long &inv) {
+    long long t0 = 0, t1 = 1, r0 = m, r1 = host_mod(a, m);
+    while (r1 != 0) {
+        const long long q = r0 / r1;
+        long long t = t0 - q * t1; t0 = t1; t1 = t;
+        long long r = r0 - q * r1; r0 = r1; r1 = r;
+    }
+    if (r0 != 1) return false;
+    inv = host_mod(t0, m);
+    return true;
+}
+
+}  // namespace
+
+// Recognises a quasi-cyclic code with affine permutation blocks from its check lists: check
+// j*P + x has, at position l, variable l*P + ((fa*x + fb) mod P) on both sides, J = m/P block
+// rows and L = n/P block columns.  Returns why not, or "" and fills rcode_.
+std::string Engine::build_res_code() {
+    const int P = model_.P;
+    if (P <= 0) return "the code is not quasi-cyclic (built from check lists)";
+    const int n = model_.n, m = model_.side[0].m;
+    if (n % P || m % P || model_.side[1].m != m) return "block structure does not match P";
+    const int J = m / P, L = n / P;
+    if (J > kResMaxJ || L > kResMaxL) return "block dimensions beyond the resident kernels";
+    if (P > 65535) return "circulant size too large";
+    auto rc = std::make_unique<ResCode>();
+    std::memset(rc.get(), 0, sizeof(ResCode));
+    rc->P = P; rc->J = J; rc->L = L; rc->n = n; rc->m = m;
+    rc->magic = static_cast<unsigned>(((1ull << 32) + P - 1) / P);
+    for (int s = 0; s < 2; ++s) {
+        const SideGraph &g = model_.side[s];
+        if (!g.regular || g.dc_max != L || g.dv_max != J) return "side degrees do not match the block structure";
+        for (int j = 0; j < J; ++j)
+            for (int l = 0; l < L; ++l) {
+                auto var_at = [&](int x) { return g.chk_var[static_cast<size_t>(g.chk_off[j * P + x]) + l]; };
+                const long long b = var_at(0) - static_cast<long long>(l) * P;
+                const long long a = P > 1 ? host_mod(var_at(1) - static_cast<long long>(l) * P - b, P) : 0;
+                if (b < 0 || b >= P) return "block column order does not match";
+                for (int x = 0; x < P; ++x)
+                    if (var_at(x) != l * P + host_mod(a * x + b, P)) return "a block is not an affine permutation";
+                long long ia = 0;
+                if (!host_inverse(a, P, ia)) return "a block multiplier has no inverse";
+                rc->fa[s][j][l] = static_cast<unsigned short>(a);
+                rc->fb[s][j][l] = static_cast<unsigned short>(b);
+                rc->ia[s][j][l] = static_cast<unsigned short>(ia);
+                rc->ib[s][j][l] = static_cast<unsigned short>(host_mod(-ia * b, P));
+            }
+    }
+    // the device modulo: x - umulhi(x, magic) * P, corrected once, for every x the kernels form
+    for (unsigned long long x = 0; x < static_cast<unsigned long long>(P) * P; ++x) {
+        const unsigned q = static_cast<unsigned>((x * rc->magic) >> 32);
+        long long r = static_cast<long long>(x) - static_cast<long long>(q) * P;
+        if (r < 0) r += P;
+        if (r != static_cast<long long>(x % P)) return "modular reduction check failed";
+    }
+    rc->words = dcode_.words;
+    for (int s = 0; s < 2; ++s) {
+        rc->basis_rows[s] = dcode_.basis_rows[s];
+        rc->pivot_row[s] = dcode_.pivot_row[s];
+    }
+    if (!(J == 3 && L == 12)) return "no resident kernel built for J=" + std::to_string(J) + ", L=" + std::to_string(L);
+    const size_t smem = res_smem_bytes(n, m, L, sizeof(__half));
+    if (smem > static_cast<size_t>(smem_optin_) - 1024) return "trial state does not fit in shared memory";
+    rcode_ = rc.release();
+    return "";
+}
+
+bool Engine::resident_applies(const jbp_options &o, std::string *why) const {
+    auto no = [&](const std::string &w) {
+        if (why) *why = w;
+        return false;
+    };
+    if (!res_code_ok_) return no(res_code_why_);
+    if (o.precision != JBP_PREC_FP16) return no("the resident tier stores messages in FP16 (precision FP16)");
+    if (o.enable_pp) return no("post-processing runs on the slot tier");
+    if (o.damping > 0.0) return no("damping runs on the slot tier");
+    if (o.freeze_syn) return no("freeze-syn runs on the slot tier");
+    return true;
+}
+
+std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
+    std::memset(&stats, 0, sizeof(stats));
+    const jbp_options &o = rq.opt;
+    JBP_CUDA_TRY(cudaSetDevice(device_), "cudaSetDevice");
+    if (!res_cnt_) JBP_CUDA_TRY(cudaMalloc(&res_cnt_, sizeof(DevCounters)), "cudaMalloc(counters)");
+    const ResCode &rc = *rcode_;
+    auto kern = k_resident<3, 12, StoreHalf>;
+    const size_t smem = res_smem_bytes(rc.n, rc.m, rc.L, sizeof(__half));
+    JBP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+                 "smem attribute");
+    int per_sm = 0;
+    JBP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kResThreads, smem), "occupancy");
+    if (per_sm < 1) return "the resident kernel does not fit on an SM";
+    const long long want = std::max<long long>(1, std::min<long long>(rq.ntrials, 1LL << 30));
+    const int grid = static_cast<int>(std::min<long long>(static_cast<long long>(per_sm) * sm_count_, want));
+    ResRun r{};
+    r.max_iter = o.max_iter;
+    r.check_warmup = std::max(0, o.check_warmup);
+    r.check_interval = std::max(1, o.check_interval);
+    r.source = rq.source;
+    r.p = rq.p;
+    r.use_prior = o.use_prior ? 1 : 0;
+    for (int i = 0; i < 4; ++i) r.prior4[i] = o.prior[i];
+    r.seed = rq.seed;
+    r.first_trial = rq.first_trial;
+    r.ntrials = rq.ntrials;
+    r.trial_list = nullptr;
+    r.src_err = rq.d_err;
+    r.src_sx = rq.d_sx;
+    r.src_sz = rq.d_sz;
+    r.est_out = rq.d_est_out;
+    r.res_out = rq.d_res_out;
+    r.hist = rq.d_hist;
+    r.cnt = res_cnt_;
+    cudaStream_t st = rq.stream;
+    cudaEvent_t ev0, ev1;
+    JBP_CUDA_TRY(cudaEventCreate(&ev0), "cudaEventCreate");
+    JBP_CUDA_TRY(cudaEventCreate(&ev1), "cudaEventCreate");
+    std::string err;
+    cudaError_t ce = cudaEventRecord(ev0, st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(res_cnt_, 0, sizeof(DevCounters), st);
+    if (ce == cudaSuccess) {
+        kern<<<grid, kResThreads, smem, st>>>(rc, r);
+        ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cudaEventRecord(ev1, st);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(ev1);
+    DevCounters hc{};
+    if (ce == cudaSuccess) ce = cudaMemcpy(&hc, res_cnt_, sizeof(hc), cudaMemcpyDeviceToHost);
+    float ms = 0.0f;
+    if (ce == cudaSuccess) cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    if (ce != cudaSuccess) return cuda_err(ce, "resident run");
+    if (hc.done != static_cast<unsigned long long>(rq.ntrials)) return "resident run finished an unexpected number of trials";
+    stats.trials = static_cast<long long>(hc.done);
+    stats.failures = static_cast<long long>(hc.failures);
+    stats.bp_fail = static_cast<long long>(hc.bp_fail);
+    stats.stab_success = static_cast<long long>(hc.stab_success);
+    stats.exact = static_cast<long long>(hc.exact);
+    stats.total_iters = static_cast<long long>(hc.total_iters);
+    stats.bp_trial_iterations = static_cast<long long>(hc.bp_trial_iterations);
+    stats.device_ms = ms;
+    stats.kernel_launches = 1;
+    stats.slots = grid;
     return "";
 }
 
@@ -260,6 +425,12 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
         return "p must be in (0, 1)";
     }
     if (o.damping < 0.0 || o.damping > 1.0) return "damping must be in [0, 1]";
+    if (o.engine < JBP_ENGINE_AUTO || o.engine > JBP_ENGINE_SLOTS) return "unknown engine";
+    if (o.engine != JBP_ENGINE_SLOTS) {
+        std::string why;
+        if (resident_applies(o, &why)) return run_resident(rq, stats);
+        if (o.engine == JBP_ENGINE_RESIDENT) return "resident engine not available: " + why;
+    }
     const SideGraph &gx = model_.side[0], &gz = model_.side[1];
     if (!gx.regular || !gz.regular || gx.dc_max != gz.dc_max || gx.dv_max != gz.dv_max)
         return "the GPU kernels need a code with equal regular degrees on both sides";

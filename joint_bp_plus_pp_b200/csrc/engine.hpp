@@ -11,6 +11,8 @@
 
 namespace jbp {
 
+struct ResCode;
+
 struct RunRequest {
     jbp_options opt{};
     int source = kSrcPhilox;
@@ -74,6 +76,11 @@ private:
         int pp_blocks = 0;
     };
 
+    // Trial-resident tier (kernels_resident.cuh): whether a run can use it, and the run.
+    bool resident_applies(const jbp_options &o, std::string *why) const;
+    std::string run_resident(const RunRequest &rq, jbp_stats &stats);
+    std::string build_res_code();
+
     std::string ensure_buffers(int S, int precision, bool damp, bool pp, int R);
     std::string upload_ets();
     void free_buffers();
@@ -81,6 +88,11 @@ private:
 
     int device_ = 0;
     int sm_count_ = 0;
+    int smem_optin_ = 0;
+    bool res_code_ok_ = false;
+    std::string res_code_why_;
+    ResCode *rcode_ = nullptr;
+    DevCounters *res_cnt_ = nullptr;
     CodeModel model_;
     DevCode dcode_{};
     std::vector<void *> code_allocs_;

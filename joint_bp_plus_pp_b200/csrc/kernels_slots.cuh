@@ -45,6 +45,19 @@ __device__ __forceinline__ uint8_t sample_philox(unsigned long long seed, long l
     return pauli_from_uniform(u, p);
 }
 
+// Both qubits 2*vp and 2*vp+1 of one Philox block (the same stream as sample_philox).
+__device__ __forceinline__ void sample_philox_pair(unsigned long long seed, long long t, int vp, double p, uint8_t &e0,
+                                                   uint8_t &e1) {
+    const uint4 r = philox4x32_10(make_uint4(static_cast<uint32_t>(vp), static_cast<uint32_t>(t),
+                                             static_cast<uint32_t>(static_cast<unsigned long long>(t) >> 32),
+                                             0x4A425042u),
+                                  make_uint2(static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32)));
+    const unsigned long long x0 = static_cast<unsigned long long>(r.y) << 32 | r.x;
+    const unsigned long long x1 = static_cast<unsigned long long>(r.w) << 32 | r.z;
+    e0 = pauli_from_uniform(static_cast<double>(x0 >> 11) * 0x1.0p-53, p);
+    e1 = pauli_from_uniform(static_cast<double>(x1 >> 11) * 0x1.0p-53, p);
+}
+
 // ------------------------------------------------------------------ per-iteration kernels
 
 // Whether iteration k1 (1-based) of a slot ends with a syndrome test: always at max_iter,

@@ -188,6 +188,29 @@ class Oracle:
         d["est"] = est
         return d
 
+    def classify(self, err, est):
+        """(syndrome_ok, exact, stab_equiv, success) of a final estimate against the true error
+        (jointbp_ets.cpp:6199-6211): the x-part of the residual must lie in rowspace(Hz) and the
+        z-part in rowspace(Hx)."""
+        err = np.ascontiguousarray(err, np.uint8)
+        est = np.ascontiguousarray(est, np.uint8)
+        sx, sz = self.syndrome(err)
+        ex, ez = self.syndrome(est)
+        ok = bool((sx == ex).all() and (sz == ez).all())
+        exact = bool((err == est).all())
+        stab = False
+        if ok:
+            words = (self.n + 63) // 64
+            stab = True
+            for part, basis in ((1, self.bz), (2, self.bx)):
+                bits = np.zeros(words * 64, np.uint8)
+                bits[:self.n] = ((err ^ est) & part) != 0
+                vec = np.packbits(bits.reshape(-1, 8)[:, ::-1], axis=1).reshape(-1).view(np.uint64).copy()
+                if not self.lib.jbo_in_row_space(ctypes.byref(basis), _ptr(vec)):
+                    stab = False
+                    break
+        return ok, exact, stab, ok and stab
+
     def wilson(self, n, k, z=1.96):
         lo, hi = ctypes.c_double(), ctypes.c_double()
         self.lib.jbo_wilson(n, k, z, ctypes.byref(lo), ctypes.byref(hi))

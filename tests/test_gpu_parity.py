@@ -144,29 +144,32 @@ def test_check_interval_schedule(decoder):
             assert it >= b["iterations"]
 
 
-@pytest.mark.parametrize("prec", ["fp32", "fp16"])
-def test_llr_precision_agreement(decoder, prec):
+LLR_ENGINES = [("fp32", "slots"), ("fp16", "slots"), ("fp16", "resident")]
+
+
+@pytest.mark.parametrize("prec,engine", LLR_ENGINES)
+def test_llr_precision_agreement(decoder, prec, engine):
     """FP32/FP16 LLR decoders against FP64 on the same reference-sampled errors at p=0.04."""
     from joint_bp_plus_pp_b200 import sample_reference_errors
     p, k = 0.04, 512
     err = sample_reference_errors(decoder.n, 106, 1, k, p)
     _, r64, e64 = decoder.decode_errors(err, p, opts(max_iter=200))
-    _, rlo, elo = decoder.decode_errors(err, p, opts(max_iter=200, precision=prec))
+    _, rlo, elo = decoder.decode_errors(err, p, opts(max_iter=200, precision=prec, engine=engine))
     same = (e64 == elo).all(axis=1)
     assert same.mean() >= 0.99, same.mean()
     assert abs(int(r64["success"].sum()) - int(rlo["success"].sum())) <= 3
     assert np.abs(r64["iterations"].astype(int) - rlo["iterations"].astype(int)).mean() < 0.5
 
 
-@pytest.mark.parametrize("prec", ["fp32", "fp16"])
-def test_llr_precision_ler_not_worse(decoder, prec):
+@pytest.mark.parametrize("prec,engine", LLR_ENGINES)
+def test_llr_precision_ler_not_worse(decoder, prec, engine):
     """Logical error rate of the LLR decoders is not worse than FP64 within the 95% Wilson
     interval, on the same 8192 reference-sampled errors at p=0.05, max-iter 50 (~3% FER)."""
     from joint_bp_plus_pp_b200 import sample_reference_errors, wilson_interval
     p, k, mi = 0.05, 8192, 50
     err = sample_reference_errors(decoder.n, 2024, 1, k, p)
     s64, r64, _ = decoder.decode_errors(err, p, opts(max_iter=mi), want_est=False)
-    slo, rlo, _ = decoder.decode_errors(err, p, opts(max_iter=mi, precision=prec), want_est=False)
+    slo, rlo, _ = decoder.decode_errors(err, p, opts(max_iter=mi, precision=prec, engine=engine), want_est=False)
     lo64, hi64 = wilson_interval(k, s64["failures"])
     assert s64["failures"] > 50
     assert slo["failures"] / k <= hi64, (slo["failures"], s64["failures"])

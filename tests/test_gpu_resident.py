@@ -1,0 +1,109 @@
+"""GPU tests of the trial-resident engine (one thread block per SM holds a whole trial in
+shared memory; FP32 arithmetic, FP16 message storage).
+
+It is an LLR decoder, so it is held to the same bars as the slot engine's LLR paths
+(test_gpu_parity.py: >= 99% identical estimates and FER within the FP64 Wilson bound); on top,
+its integer work is checked exactly: every reported outcome flag is recomputed by the oracle
+from the returned estimate, and the same inputs give the same outputs through every entry
+point (device sampler, host errors, host syndromes).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def ropts(**kw):
+    from joint_bp_plus_pp_b200 import Options
+    base = dict(precision="fp16", enable_pp=False, engine="resident")
+    base.update(kw)
+    return Options(**base)
+
+
+def test_resident_is_one_launch(decoder):
+    st, res = decoder.simulate(106, 1000, 0.04, ropts(max_iter=200))
+    assert st["trials"] == 1000 and st["kernel_launches"] == 1
+    assert st["total_iters"] == int(res["iterations"].sum())
+
+
+def test_resident_flags_match_oracle_classification(decoder, oracle):
+    """At p=0.06 many trials fail; every flag is recomputed from the estimate on the CPU."""
+    from joint_bp_plus_pp_b200 import sample_reference_errors
+    p, mi, k = 0.06, 40, 96
+    err = sample_reference_errors(decoder.n, 77, 1, k, p)
+    st, res, est = decoder.decode_errors(err, p, ropts(max_iter=mi))
+    assert 0 < int(res["syndrome_ok"].sum()) < k
+    for t in range(k):
+        ok, exact, stab, success = oracle.classify(err[t], est[t])
+        r = res[t]
+        assert (r["syndrome_ok"], r["bp_ok"], r["exact"], r["success"]) == (ok, ok, exact, success), t
+        if ok:
+            assert r["stab_equiv"] == stab and 1 <= r["iterations"] <= mi
+        else:
+            assert r["iterations"] == mi
+    assert st["failures"] == int((res["success"] == 0).sum())
+    assert st["exact"] == int(res["exact"].sum())
+    assert st["bp_fail"] == int((res["bp_ok"] == 0).sum())
+
+
+def test_resident_entry_points_agree(decoder, oracle):
+    """Device Philox sampler, host errors and host syndromes decode identically."""
+    p, mi, k = 0.05, 60, 64
+    err = decoder.sample_errors(4242, 11, k, p, sampler="philox")
+    st1, r1 = decoder.simulate(4242, k, p, ropts(max_iter=mi), first_trial=11)
+    st2, r2, e2 = decoder.decode_errors(err, p, ropts(max_iter=mi))
+    assert (r1 == r2).all()
+    sx = np.stack([oracle.syndrome(e)[0] for e in err])
+    sz = np.stack([oracle.syndrome(e)[1] for e in err])
+    _, r3, e3 = decoder.decode_syndromes(sx, sz, p, ropts(max_iter=mi))
+    assert (e3 == e2).all()
+    assert (r3["iterations"] == r2["iterations"]).all() and (r3["syndrome_ok"] == r2["syndrome_ok"]).all()
+
+
+def test_resident_mt_sampler_equals_host_stream(decoder):
+    from joint_bp_plus_pp_b200 import sample_reference_errors
+    p, mi, k = 0.05, 50, 40
+    st1, r1 = decoder.simulate(1, k, p, ropts(max_iter=mi), sampler="mt19937")
+    _, r2, _ = decoder.decode_errors(sample_reference_errors(decoder.n, 1, 1, k, p), p, ropts(max_iter=mi))
+    assert (r1 == r2).all()
+
+
+def test_resident_check_interval_schedule(decoder):
+    from joint_bp_plus_pp_b200 import sample_reference_errors
+    p = 0.04
+    err = sample_reference_errors(decoder.n, 106, 1, 64, p)
+    _, base, _ = decoder.decode_errors(err, p, ropts(max_iter=60), want_est=False)
+    _, res, _ = decoder.decode_errors(err, p, ropts(max_iter=60, check_interval=4, check_warmup=2), want_est=False)
+    for b, r in zip(base, res):
+        if b["syndrome_ok"]:
+            it = r["iterations"]
+            assert it == 60 or (it > 2 and (it - 2) % 4 == 0)
+            assert it >= b["iterations"]
+
+
+def test_resident_counts_and_hist(decoder):
+    st, res = decoder.simulate(106, 4000, 0.04, ropts(max_iter=1000), hist=True)
+    assert st["trials"] == 4000
+    assert int(st["hist"].sum()) == 4000
+    assert st["total_iters"] == int(res["iterations"].sum()) == st["bp_trial_iterations"]
+    assert 7.0 < st["total_iters"] / 4000 < 12.0
+    assert st["failures"] <= 2
+
+
+def test_resident_explicit_prior_equals_p(decoder):
+    from joint_bp_plus_pp_b200 import sample_reference_errors
+    p = 0.05
+    q = [1 - p, p / 3, p / 3, p / 3]
+    s = ((q[0] + q[1]) + q[2]) + q[3]
+    err = sample_reference_errors(decoder.n, 3, 1, 64, p)
+    _, r1, e1 = decoder.decode_errors(err, p, ropts(max_iter=50))
+    _, r2, e2 = decoder.decode_errors(err, 0.3, ropts(max_iter=50, prior=tuple(x / s for x in q)))
+    assert (e1 == e2).all() and (r1["iterations"] == r2["iterations"]).all()
+
+
+def test_resident_refuses_what_it_does_not_run(decoder):
+    from joint_bp_plus_pp_b200 import JbpError
+    for bad in (dict(damping=0.2), dict(freeze_syn=True), dict(precision="fp32")):
+        with pytest.raises(JbpError) as e:
+            decoder.simulate(1, 4, 0.05, ropts(max_iter=10, **bad))
+        assert e.value.code == 4
