@@ -204,7 +204,9 @@ std::string Engine::build_res_code() {
         rc->basis_rows[s] = dcode_.basis_rows[s];
         rc->pivot_row[s] = dcode_.pivot_row[s];
     }
-    if (!(J == 3 && L == 12)) return "no resident kernel built for J=" + std::to_string(J) + ", L=" + std::to_string(L);
+    if (!(P == 768 && J == 3 && L == 12))
+        return "no resident kernel built for P=" + std::to_string(P) + ", J=" + std::to_string(J) + ", L=" +
+               std::to_string(L);
     const size_t smem = res_smem_bytes(n, m, L, sizeof(__half));
     if (smem > static_cast<size_t>(smem_optin_) - 1024) return "trial state does not fit in shared memory";
     rcode_ = rc.release();
@@ -230,7 +232,7 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     JBP_CUDA_TRY(cudaSetDevice(device_), "cudaSetDevice");
     if (!res_cnt_) JBP_CUDA_TRY(cudaMalloc(&res_cnt_, sizeof(DevCounters)), "cudaMalloc(counters)");
     const ResCode &rc = *rcode_;
-    auto kern = k_resident<3, 12, StoreHalf>;
+    auto kern = k_resident<768, 3, 12, StoreHalf>;
     const size_t smem = res_smem_bytes(rc.n, rc.m, rc.L, sizeof(__half));
     JBP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
                  "smem attribute");

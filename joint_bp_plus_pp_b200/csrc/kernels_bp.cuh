@@ -15,11 +15,12 @@
 // With damping the full v2c 4-vector is kept, since scaled_mix needs the old message.
 //
 // FP32/FP16 path: log-likelihood ratios in base 2 (y = log2(q0/q1)), so that the
-// exponentials and logarithms are single ex2/lg2 operations.  Check node: the tanh rule,
-// t = tanh(y ln2 / 2) = (1 - 2^-|y|) / (1 + 2^-|y|) with the sign of y, excluded products
-// from prefix/suffix passes, output lg2((1 + |T|) / (1 - |T|)) clamped (|T| -> 1 saturates
-// at about 25 in base 2); the syndrome bit flips the sign.  Variable node: sums of the
-// incoming LLRs and the exact joint 4-ary coupling of the X and Z sides.
+// exponentials and logarithms are single ex2/lg2 operations.  Check node: the tanh rule in a
+// cancellation-free form: per edge u = 2^-|y| (t = (1 - u) / (1 + u)), sets of edges carried as
+// (PN, Q) = (prod (1 - u), prod (1 + u) - prod (1 - u)), joined as Q = PD_a Q_b + PN_b Q_a; the
+// output over the other edges is log2((2 PN + Q) / Q), clamped at 110; the syndrome bit flips
+// the sign.  Variable node: sums of the incoming LLRs and the exact joint 4-ary coupling of
+// the X and Z sides; variable-to-check messages are clamped at 120 (2^-120 stays normal).
 #pragma once
 
 #include <cuda_fp16.h>
@@ -312,7 +313,8 @@ __device__ __forceinline__ void st_msg<float>(float *p, float v) { *p = v; }
 template <>
 __device__ __forceinline__ void st_msg<__half>(__half *p, float v) { *p = __float2half_rn(v); }
 
-constexpr float kLlrMax = 43.0f;     // message clamp, base 2 (~30 in natural units)
+constexpr float kLlrMax = 110.0f;    // check-to-variable magnitude clamp, base 2 (exact in FP16 storage)
+constexpr float kLlrInMax = 120.0f;  // variable-to-check magnitude clamp (2^-120 is a normal float)
 
 // Single special-function-unit operations.
 __device__ __forceinline__ float ex2_approx(float x) {
@@ -336,7 +338,7 @@ __device__ __forceinline__ float lse2(float a, float b) {
     return fmaxf(a, b) + lg2_approx(1.0f + ex2_approx(-fabsf(a - b)));
 }
 
-__device__ __forceinline__ float clamp_llr(float x) { return fminf(fmaxf(x, -kLlrMax), kLlrMax); }
+__device__ __forceinline__ float clamp_llr(float x) { return fminf(fmaxf(x, -kLlrInMax), kLlrInMax); }
 
 template <typename T, int DC>
 __global__ void __launch_bounds__(256) k_check_llr(DevCode code, DevRun run, DevMsgs msg) {
@@ -369,25 +371,38 @@ __global__ void __launch_bounds__(256) k_check_llr(DevCode code, DevRun run, Dev
             continue;
         }
         const float lp = run.lprior[8 * slot + 4 + side];
-        float t[DC];
+        // stable tanh rule (PN, Q = prod D - prod N) over u = 2^-|y|, N = 1 - u, D = 1 + u:
+        // the output log2((2 PN + Q) / Q) keeps its precision when the product of the other
+        // edges' tanh is close to 1 (see kernels_resident.cuh)
+        float u[DC];
+        unsigned sgn = ((run.synm[static_cast<size_t>(row) * G + group] >> lane) & 1u) << 31;
 #pragma unroll
         for (int i = 0; i < DC; ++i) {
             const float y = fresh ? lp : ld_msg<T>(v2c + i * kGroup);
-            const float u = ex2_approx(-fabsf(y));
-            t[i] = copysignf((1.0f - u) * rcp_approx(1.0f + u), y);
+            const unsigned sy = __float_as_uint(y) & 0x80000000u;
+            sgn ^= sy;
+            u[i] = __uint_as_float(__float_as_uint(ex2_approx(-fminf(fabsf(y), kLlrInMax))) | sy);
         }
-        float suf[DC + 1];
-        suf[DC] = 1.0f;
+        float sPN[DC + 1], sQ[DC + 1];
+        sPN[DC] = 1.0f;
+        sQ[DC] = 0.0f;
 #pragma unroll
-        for (int i = DC - 1; i >= 0; --i) suf[i] = suf[i + 1] * t[i];
-        float pre = ((run.synm[static_cast<size_t>(row) * G + group] >> lane) & 1u) ? -1.0f : 1.0f;
+        for (int i = DC - 1; i >= 0; --i) {
+            const float au = fabsf(u[i]);
+            sQ[i] = fmaf(1.0f + au, sQ[i + 1], sPN[i + 1] * (au + au));
+            sPN[i] = (1.0f - au) * sPN[i + 1];
+        }
+        float pPN = 1.0f, pQ = 0.0f;
 #pragma unroll
         for (int i = 0; i < DC; ++i) {
-            const float tt = pre * suf[i + 1];
-            const float a = fabsf(tt);
-            const float mag = fminf(lg2_approx((1.0f + a) * rcp_approx(1.0f - a)), kLlrMax);
-            st_msg<T>(c2v + i * kGroup, copysignf(mag, tt));
-            pre *= t[i];
+            const float ePN = pPN * sPN[i + 1];
+            const float eQ = fmaf(pPN + pQ, sQ[i + 1], sPN[i + 1] * pQ);
+            const float mag = fminf(lg2_approx(fmaf(2.0f, ePN, eQ) * rcp_approx(eQ)), kLlrMax);
+            st_msg<T>(c2v + i * kGroup,
+                      __uint_as_float(__float_as_uint(mag) ^ ((sgn ^ __float_as_uint(u[i])) & 0x80000000u)));
+            const float au = fabsf(u[i]);
+            pQ = fmaf(pPN + pQ, au + au, (1.0f - au) * pQ);
+            pPN *= 1.0f - au;
         }
     }
 }

@@ -108,7 +108,8 @@ __device__ __forceinline__ float res_lse2(float a, float b) {
     return fmaxf(a, b) + res_lg2(1.0f + res_ex2(-fabsf(a - b)));
 }
 
-constexpr float kResLlrMax = 43.0f;   // same clamp as the slot engine's LLR kernels
+constexpr float kResVinMax = 120.0f;   // variable-to-check magnitude clamp (2^-120 is a normal float)
+constexpr float kResCmax = 110.0f;     // check-to-variable magnitude clamp (exact in FP16 storage)
 
 __device__ __forceinline__ float with_bit(float a, unsigned b) {
     return __uint_as_float((__float_as_uint(a) & ~1u) | b);
@@ -119,107 +120,127 @@ __host__ __device__ inline size_t res_smem_bytes(int n, int m, int L, size_t sto
     const size_t c2v = (2ull * L * m * store_bytes + 15) / 16 * 16;
     const size_t A = 2ull * n * 4;
     const size_t err = (static_cast<size_t>(n) + 15) / 16 * 16;
-    const size_t syn = (2ull * ((m + 31) / 32) * 4 + 15) / 16 * 16;
+    const size_t syn = (2ull * ((m + 31) / 32) + 3) / 4 * 4 * 4;
     return c2v + A + err + syn + 64;
 }
 
-struct ResShared {
-    void *c2v;
-    float *A;        // [2][n]
-    uint8_t *err;    // [n]
-    unsigned *syn;   // [2][mw]
-    int *ints;       // [16]
-};
 
-// Check phase of one side: new c2v from A and the old c2v; with `test`, also the parity of
-// the decision bits of every check against its target.  Returns whether a tested check of
-// this thread failed.
-template <int J, int L, class ST>
-__device__ __forceinline__ bool res_check_side(const ResCode &code, const ResShared &sh, int side, bool test) {
-    using T = typename ST::T;
-    const int P = code.P, m = code.m, n = code.n;
-    const int mw = (m + 31) >> 5;
-    T *c2v = static_cast<T *>(sh.c2v) + static_cast<size_t>(side) * L * m;
-    const float *A = sh.A + static_cast<size_t>(side) * n;
-    const unsigned *syn = sh.syn + side * mw;
-    bool bad = false;
-#pragma unroll 1
-    for (int j = 0; j < J; ++j) {
-#pragma unroll 1
-        for (int x = threadIdx.x; x < P; x += blockDim.x) {
-            const int c = j * P + x;
-            const unsigned sbit = (syn[c >> 5] >> (c & 31)) & 1u;
-            float u[L];
-            unsigned neg = 0, par = 0;
+// Check phase, one block row JJ of side SIDE, check offset x: new c2v of the row's L edges
+// from A and the old c2v; with `test`, also the parity of the decision bits against the
+// target.  Returns whether the tested check failed.
+//
+// Stable tanh rule.  Per edge u = 2^-|y|, N = 1 - u, D = 1 + u, t = N / D.  A set of edges is
+// carried as (PN, Q) with PN = prod N and Q = prod D - prod N, so prod D = PN + Q and
+// 1 - T = Q / prod D; joining two sets, Q = PD_a * Q_b + PN_b * Q_a, is a sum of positive terms
+// and keeps full relative precision however close T is to 1.  A single edge has Q = 2u exactly.
+// The output magnitude log2((1 + T) / (1 - T)) = log2((2 PN + Q) / Q) over the other edges
+// therefore grows like min |y| instead of saturating where 1 - T rounds to zero.
+template <int P, int J, int L, class ST, int SIDE, int JJ>
+__device__ __forceinline__ bool res_check_row(const ResCode &code, typename ST::T *c2v_all, const float *A_all,
+                                              const unsigned *syn_all, int x, bool test) {
+    constexpr int m = J * P, n = L * P, mw = (m + 31) / 32;
+    typename ST::T *c2v = c2v_all + SIDE * L * m + JJ * P + x;
+    const float *A = A_all + SIDE * n;
+    const int c = JJ * P + x;
+    const unsigned sbit = (syn_all[SIDE * mw + (c >> 5)] >> (c & 31)) & 1u;
+    float u[L];
+    unsigned sgn = 0u, par = 0u;
 #pragma unroll
-            for (int l = 0; l < L; ++l) {
-                const unsigned y = res_mod(static_cast<unsigned>(code.fa[side][j][l]) * x + code.fb[side][j][l], P,
-                                           code.magic);
-                const float a = A[l * P + y];
-                par ^= __float_as_uint(a) & 1u;
-                const float v = fminf(fmaxf(a - ST::ld(c2v + l * m + c), -kResLlrMax), kResLlrMax);
-                neg |= (__float_as_uint(v) >> 31) << l;
-                u[l] = res_ex2(-fabsf(v));
-            }
-            if (test) bad |= (par & 1u) != sbit;
-            // suffix products of N = 1 - u and D = 1 + u
-            float sN[L + 1], sD[L + 1];
-            sN[L] = 1.0f;
-            sD[L] = 1.0f;
+    for (int l = 0; l < L; ++l) {
+        const unsigned y = (static_cast<unsigned>(code.fa[SIDE][JJ][l]) * static_cast<unsigned>(x) +
+                            code.fb[SIDE][JJ][l]) % static_cast<unsigned>(P);
+        const float a = A[l * P + y];
+        par ^= __float_as_uint(a);
+        const float v = a - ST::ld(c2v + l * m);
+        const unsigned sv = __float_as_uint(v) & 0x80000000u;
+        sgn ^= sv;
+        // sign of the edge kept in u's sign bit, |u| = 2^-min(|v|, kResVinMax)
+        u[l] = __uint_as_float(__float_as_uint(res_ex2(-fminf(fabsf(v), kResVinMax))) | sv);
+    }
+    const bool bad = test && ((par & 1u) != sbit);
+    float sPN[L + 1], sQ[L + 1];
+    sPN[L] = 1.0f;
+    sQ[L] = 0.0f;
 #pragma unroll
-            for (int l = L - 1; l >= 0; --l) {
-                sN[l] = sN[l + 1] * (1.0f - u[l]);
-                sD[l] = sD[l + 1] * (1.0f + u[l]);
-            }
-            const unsigned sg = (__popc(neg) & 1u) ^ sbit;
-            float pN = 1.0f, pD = 1.0f;
+    for (int l = L - 1; l >= 0; --l) {
+        const float au = fabsf(u[l]);
+        const float N = 1.0f - au, D = 1.0f + au, Q = au + au;
+        sQ[l] = fmaf(D, sQ[l + 1], sPN[l + 1] * Q);
+        sPN[l] = N * sPN[l + 1];
+    }
+    sgn ^= sbit << 31;
+    float pPN = 1.0f, pQ = 0.0f;
 #pragma unroll
-            for (int l = 0; l < L; ++l) {
-                const float eN = pN * sN[l + 1], eD = pD * sD[l + 1];
-                const float mag = fminf(res_lg2((eD + eN) * res_rcp(eD - eN)), kResLlrMax);
-                const unsigned s = sg ^ ((neg >> l) & 1u);
-                ST::st(c2v + l * m + c, s ? -mag : mag);
-                pN *= 1.0f - u[l];
-                pD *= 1.0f + u[l];
-            }
-        }
+    for (int l = 0; l < L; ++l) {
+        const float ePN = pPN * sPN[l + 1];
+        const float eQ = fmaf(pPN + pQ, sQ[l + 1], sPN[l + 1] * pQ);
+        const float mag = fminf(res_lg2(fmaf(2.0f, ePN, eQ) * res_rcp(eQ)), kResCmax);
+        ST::st(c2v + l * m, __uint_as_float(__float_as_uint(mag) ^ ((sgn ^ __float_as_uint(u[l])) & 0x80000000u)));
+        const float au = fabsf(u[l]);
+        const float N = 1.0f - au, Q = au + au;
+        pQ = fmaf(pPN + pQ, Q, N * pQ);
+        pPN *= N;
     }
     return bad;
 }
 
-// Variable phase: sums, hard decision, and the new A of both sides.
-template <int J, int L, class ST>
-__device__ __forceinline__ void res_var(const ResCode &code, const ResShared &sh, const float4 lp) {
-    using T = typename ST::T;
-    const int P = code.P, m = code.m, n = code.n;
-    const T *c2vx = static_cast<const T *>(sh.c2v);
-    const T *c2vz = c2vx + static_cast<size_t>(L) * m;
-    float *Ax = sh.A, *Az = sh.A + n;
-#pragma unroll 1
-    for (int l = 0; l < L; ++l) {
-#pragma unroll 1
-        for (int y = threadIdx.x; y < P; y += blockDim.x) {
-            float Lam = 0.0f, Mu = 0.0f;
-#pragma unroll
-            for (int j = 0; j < J; ++j) {
-                const unsigned xx = res_mod(static_cast<unsigned>(code.ia[0][j][l]) * y + code.ib[0][j][l], P, code.magic);
-                const unsigned xz = res_mod(static_cast<unsigned>(code.ia[1][j][l]) * y + code.ib[1][j][l], P, code.magic);
-                Lam += ST::ld(c2vx + l * m + j * P + xx);
-                Mu += ST::ld(c2vz + l * m + j * P + xz);
-            }
-            const float w0 = lp.x, w1 = lp.y - Lam, w2 = lp.z - Mu, w3 = lp.w - Lam - Mu;
-            unsigned best = 0;
-            float bv = w0;
-            if (w1 > bv) { best = 1; bv = w1; }
-            if (w2 > bv) { best = 2; bv = w2; }
-            if (w3 > bv) { best = 3; }
-            const float Gx = res_lse2(lp.x, lp.z - Mu) - res_lse2(lp.y, lp.w - Mu);
-            const float Hz = res_lse2(lp.x, lp.y - Lam) - res_lse2(lp.z, lp.w - Lam);
-            const int v = l * P + y;
-            Ax[v] = with_bit(Lam + Gx, best & 1u);
-            Az[v] = with_bit(Mu + Hz, best >> 1);
-        }
+template <int P, int J, int L, class ST, int SIDE>
+__device__ __forceinline__ bool res_check_side(const ResCode &code, typename ST::T *c2v, const float *A,
+                                               const unsigned *syn, bool test) {
+    bool bad = false;
+    for (int x = threadIdx.x; x < P; x += blockDim.x) {
+        bad |= res_check_row<P, J, L, ST, SIDE, 0>(code, c2v, A, syn, x, test);
+        if (J > 1) bad |= res_check_row<P, J, L, ST, SIDE, (J > 1 ? 1 : 0)>(code, c2v, A, syn, x, test);
+        if (J > 2) bad |= res_check_row<P, J, L, ST, SIDE, (J > 2 ? 2 : 0)>(code, c2v, A, syn, x, test);
+        if (J > 3) bad |= res_check_row<P, J, L, ST, SIDE, (J > 3 ? 3 : 0)>(code, c2v, A, syn, x, test);
     }
+    return bad;
+}
+
+// log2((c0 + c1 2^-s) / (c2 + c3 2^-s)) for any sign of s, with one ex2 and two lg2:
+// the x-bit coupling Gx (s = Mu; c = P0, P2, P1, P3) and the z-bit coupling Hz (s = Lam;
+// c = P0, P1, P2, P3), where P = the prior probabilities.
+__device__ __forceinline__ float res_couple(float s, float c0, float c1, float c2, float c3) {
+    const float e = res_ex2(-fabsf(s));
+    const bool pos = s >= 0.0f;
+    const float num = pos ? fmaf(c1, e, c0) : fmaf(c0, e, c1);
+    const float den = pos ? fmaf(c3, e, c2) : fmaf(c2, e, c3);
+    return res_lg2(num) - res_lg2(den);
+}
+
+// Variable phase for block column LL, variable offset y: sums, hard decision, new A.
+template <int P, int J, int L, class ST, int LL>
+__device__ __forceinline__ void res_var_col(const ResCode &code, const typename ST::T *c2v, float *A, int y,
+                                            const float4 lp, const float4 pr) {
+    constexpr int m = J * P, n = L * P;
+    float Lam = 0.0f, Mu = 0.0f;
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+        const unsigned xx = (static_cast<unsigned>(code.ia[0][j][LL]) * static_cast<unsigned>(y) + code.ib[0][j][LL]) %
+                            static_cast<unsigned>(P);
+        const unsigned xz = (static_cast<unsigned>(code.ia[1][j][LL]) * static_cast<unsigned>(y) + code.ib[1][j][LL]) %
+                            static_cast<unsigned>(P);
+        Lam += ST::ld(c2v + LL * m + j * P + xx);
+        Mu += ST::ld(c2v + (L + LL) * m + j * P + xz);
+    }
+    const float w0 = lp.x, w1 = lp.y - Lam, w2 = lp.z - Mu, w3 = lp.w - Lam - Mu;
+    unsigned best = 0;
+    float bv = w0;
+    if (w1 > bv) { best = 1; bv = w1; }
+    if (w2 > bv) { best = 2; bv = w2; }
+    if (w3 > bv) { best = 3; }
+    const float Gx = res_couple(Mu, pr.x, pr.z, pr.y, pr.w);
+    const float Hz = res_couple(Lam, pr.x, pr.y, pr.z, pr.w);
+    const int v = LL * P + y;
+    A[v] = with_bit(Lam + Gx, best & 1u);
+    A[n + v] = with_bit(Mu + Hz, best >> 1);
+}
+
+template <int P, int J, int L, class ST, int LL>
+__device__ __forceinline__ void res_var_cols(const ResCode &code, const typename ST::T *c2v, float *A, int y,
+                                             const float4 lp, const float4 pr) {
+    res_var_col<P, J, L, ST, LL>(code, c2v, A, y, lp, pr);
+    if constexpr (LL + 1 < L) res_var_cols<P, J, L, ST, LL + 1>(code, c2v, A, y, lp, pr);
 }
 
 // Block-wide membership test of vec (shared memory, `words` 64-bit words) in a row space
@@ -237,44 +258,42 @@ __device__ __forceinline__ bool res_in_row_space(uint64_t *vec, int words, const
     return r;
 }
 
-template <int J, int L, class ST>
+template <int P, int J, int L, class ST>
 __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRun run) {
     extern __shared__ __align__(16) unsigned char res_smem[];
     using T = typename ST::T;
-    const int P = code.P, m = code.m, n = code.n;
-    const int mw = (m + 31) >> 5;
-    ResShared sh;
-    {
-        size_t o = 0;
-        sh.c2v = res_smem + o; o += (2ull * L * m * sizeof(T) + 15) / 16 * 16;
-        sh.A = reinterpret_cast<float *>(res_smem + o); o += 2ull * n * 4;
-        sh.err = res_smem + o; o += (static_cast<size_t>(n) + 15) / 16 * 16;
-        sh.syn = reinterpret_cast<unsigned *>(res_smem + o); o += (2ull * mw * 4 + 15) / 16 * 16;
-        sh.ints = reinterpret_cast<int *>(res_smem + o);
-    }
+    constexpr int m = J * P, n = L * P, mw = (m + 31) / 32;
+    T *const c2v = reinterpret_cast<T *>(res_smem);
+    constexpr size_t c2v_bytes = (2ull * L * m * sizeof(T) + 15) / 16 * 16;
+    float *const A = reinterpret_cast<float *>(res_smem + c2v_bytes);
+    uint8_t *const err = res_smem + c2v_bytes + 2ull * n * 4;
+    unsigned *const syn = reinterpret_cast<unsigned *>(err + (n + 15) / 16 * 16);
+    int *const ints = reinterpret_cast<int *>(syn + (2 * mw + 3) / 4 * 4);
     __shared__ long long trial_sh;
-    __shared__ float4 lp_sh;
+    __shared__ float4 lp_sh, pr_sh;
     __shared__ float lpx_sh, lpz_sh;
     const bool have_err = run.source != kSrcSyndromes;
 
-    // log2 prior weights (FP64 prior as the slot engine's refill, then rounded to FP32)
+    // prior: FP64 as the slot engine's refill, then its log2 weights and probabilities in FP32
     if (threadIdx.x == 0) {
-        double p0, p1, p2, p3;
+        double q[4];
         if (run.use_prior) {
-            p0 = run.prior4[0]; p1 = run.prior4[1]; p2 = run.prior4[2]; p3 = run.prior4[3];
+            for (int i = 0; i < 4; ++i) q[i] = run.prior4[i];
         } else {
-            p0 = 1.0 - run.p; p1 = run.p / 3.0; p2 = p1; p3 = p1;
-            const double s = ((p0 + p1) + p2) + p3;
-            if (s <= 0.0) { p0 = p1 = p2 = p3 = 0.25; }
-            else { p0 /= s; p1 /= s; p2 /= s; p3 /= s; }
+            q[0] = 1.0 - run.p; q[1] = run.p / 3.0; q[2] = q[1]; q[3] = q[1];
+            const double s = ((q[0] + q[1]) + q[2]) + q[3];
+            for (int i = 0; i < 4; ++i) q[i] = s > 0.0 ? q[i] / s : 0.25;
         }
-        lp_sh = make_float4(static_cast<float>(log2(p0)), static_cast<float>(log2(p1)), static_cast<float>(log2(p2)),
-                            static_cast<float>(log2(p3)));
-        lpx_sh = static_cast<float>(log2((p0 + p2) / (p1 + p3)));
-        lpz_sh = static_cast<float>(log2((p0 + p1) / (p2 + p3)));
+        for (int i = 0; i < 4; ++i) q[i] = fmax(q[i], 1e-30);
+        lp_sh = make_float4(static_cast<float>(log2(q[0])), static_cast<float>(log2(q[1])),
+                            static_cast<float>(log2(q[2])), static_cast<float>(log2(q[3])));
+        pr_sh = make_float4(static_cast<float>(q[0]), static_cast<float>(q[1]), static_cast<float>(q[2]),
+                            static_cast<float>(q[3]));
+        lpx_sh = static_cast<float>(log2((q[0] + q[2]) / (q[1] + q[3])));
+        lpz_sh = static_cast<float>(log2((q[0] + q[1]) / (q[2] + q[3])));
     }
     __syncthreads();
-    const float4 lp = lp_sh;
+    const float4 lp = lp_sh, pr = pr_sh;
     const float lpx = lpx_sh, lpz = lpz_sh;
 
     for (;;) {
@@ -289,52 +308,51 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
         const long long local = t - run.first_trial;
 
         // ---- error and target syndrome
-        for (int w = threadIdx.x; w < 2 * mw; w += blockDim.x) sh.syn[w] = 0u;
+        for (int w = threadIdx.x; w < 2 * mw; w += blockDim.x) syn[w] = 0u;
         if (run.source == kSrcPhilox) {
             for (int v2 = threadIdx.x; 2 * v2 < n; v2 += blockDim.x) {
                 uint8_t e0, e1;
                 sample_philox_pair(run.seed, t, v2, run.p, e0, e1);
-                sh.err[2 * v2] = e0;
-                if (2 * v2 + 1 < n) sh.err[2 * v2 + 1] = e1;
+                err[2 * v2] = e0;
+                if (2 * v2 + 1 < n) err[2 * v2 + 1] = e1;
             }
         } else if (run.source == kSrcErrors) {
             const uint8_t *src = run.src_err + local * n;
-            for (int v = threadIdx.x; v < n; v += blockDim.x) sh.err[v] = src[v];
+            for (int v = threadIdx.x; v < n; v += blockDim.x) err[v] = src[v];
         } else if (run.source == kSrcMt19937) {
-            if (threadIdx.x < 32) warp_mt_trial(reinterpret_cast<unsigned long long *>(sh.A), run.seed, t, run.p, n, sh.err);
+            if (threadIdx.x < 32) warp_mt_trial(reinterpret_cast<unsigned long long *>(A), run.seed, t, run.p, n, err);
         }
         __syncthreads();
         if (run.source == kSrcSyndromes) {
             for (int c = threadIdx.x; c < m; c += blockDim.x) {
-                if (run.src_sx[local * m + c] & 1) atomicOr(&sh.syn[c >> 5], 1u << (c & 31));
-                if (run.src_sz[local * m + c] & 1) atomicOr(&sh.syn[mw + (c >> 5)], 1u << (c & 31));
+                if (run.src_sx[local * m + c] & 1) atomicOr(&syn[c >> 5], 1u << (c & 31));
+                if (run.src_sz[local * m + c] & 1) atomicOr(&syn[mw + (c >> 5)], 1u << (c & 31));
             }
         } else {
-            for (int side = 0; side < 2; ++side)
-                for (int j = 0; j < code.J; ++j)
-                    for (int x = threadIdx.x; x < P; x += blockDim.x) {
-                        unsigned par = 0;
+            for (int r = threadIdx.x; r < 2 * m; r += blockDim.x) {
+                const int side = r >= m, c = r - side * m, j = c / P, x = c - j * P;
+                unsigned par = 0;
 #pragma unroll
-                        for (int l = 0; l < L; ++l) {
-                            const unsigned y = res_mod(static_cast<unsigned>(code.fa[side][j][l]) * x + code.fb[side][j][l],
-                                                       P, code.magic);
-                            par ^= (sh.err[l * P + y] >> side) & 1u;
-                        }
-                        const int c = j * P + x;
-                        if (par) atomicOr(&sh.syn[side * mw + (c >> 5)], 1u << (c & 31));
-                    }
+                for (int l = 0; l < L; ++l) {
+                    const unsigned y = (static_cast<unsigned>(code.fa[side][j][l]) * static_cast<unsigned>(x) +
+                                        code.fb[side][j][l]) % static_cast<unsigned>(P);
+                    par ^= (err[l * P + y] >> side) & 1u;
+                }
+                if (par) atomicOr(&syn[side * mw + (c >> 5)], 1u << (c & 31));
+            }
         }
         // ---- BP state: c2v = 0, A = prior LLR of each side's bit
         {
-            uint4 *z = static_cast<uint4 *>(sh.c2v);
-            const int nz = static_cast<int>((2ull * L * m * sizeof(T)) / 16);
+            uint4 *z = reinterpret_cast<uint4 *>(c2v);
+            constexpr int nz = static_cast<int>(c2v_bytes / 16);
             for (int i = threadIdx.x; i < nz; i += blockDim.x) z[i] = make_uint4(0u, 0u, 0u, 0u);
             const float ax = with_bit(lpx, 0u), az = with_bit(lpz, 0u);
-            for (int v = threadIdx.x; v < n; v += blockDim.x) { sh.A[v] = ax; sh.A[n + v] = az; }
+            for (int v = threadIdx.x; v < n; v += blockDim.x) { A[v] = ax; A[n + v] = az; }
         }
         __syncthreads();
 
-        // ---- BP iterations (it = completed iterations)
+        // ---- BP iterations (it = completed iterations); the check phase of iteration it+1
+        // also tests the decisions of iteration it
         int it = 0;
         bool ok = false;
         for (;;) {
@@ -342,37 +360,33 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
                                           (it > run.check_warmup && (it - run.check_warmup) % run.check_interval == 0));
             bool bad = false;
             if (it < run.max_iter) {
-                bad = res_check_side<J, L, ST>(code, sh, 0, test);
-                bad |= res_check_side<J, L, ST>(code, sh, 1, test);
+                bad = res_check_side<P, J, L, ST, 0>(code, c2v, A, syn, test);
+                bad |= res_check_side<P, J, L, ST, 1>(code, c2v, A, syn, test);
             } else {
-                // final test only
-                for (int side = 0; side < 2; ++side)
-                    for (int j = 0; j < code.J; ++j)
-                        for (int x = threadIdx.x; x < P; x += blockDim.x) {
-                            unsigned par = 0;
-                            const float *A = sh.A + static_cast<size_t>(side) * n;
+                for (int r = threadIdx.x; r < 2 * m; r += blockDim.x) {
+                    const int side = r >= m, c = r - side * m, j = c / P, x = c - j * P;
+                    unsigned par = 0;
 #pragma unroll
-                            for (int l = 0; l < L; ++l) {
-                                const unsigned y = res_mod(static_cast<unsigned>(code.fa[side][j][l]) * x +
-                                                               code.fb[side][j][l], P, code.magic);
-                                par ^= __float_as_uint(A[l * P + y]) & 1u;
-                            }
-                            const int c = j * P + x;
-                            bad |= (par & 1u) != ((sh.syn[side * mw + (c >> 5)] >> (c & 31)) & 1u);
-                        }
+                    for (int l = 0; l < L; ++l) {
+                        const unsigned y = (static_cast<unsigned>(code.fa[side][j][l]) * static_cast<unsigned>(x) +
+                                            code.fb[side][j][l]) % static_cast<unsigned>(P);
+                        par ^= __float_as_uint(A[side * n + l * P + y]);
+                    }
+                    bad |= (par & 1u) != ((syn[side * mw + (c >> 5)] >> (c & 31)) & 1u);
+                }
             }
             bad = __syncthreads_or(bad);
             if (test && !bad) { ok = true; break; }
             if (it >= run.max_iter) break;
-            res_var<J, L, ST>(code, sh, lp);
+            for (int y = threadIdx.x; y < P; y += blockDim.x) res_var_cols<P, J, L, ST, 0>(code, c2v, A, y, lp, pr);
             __syncthreads();
             ++it;
         }
         const int iters = ok ? it : run.max_iter;
 
         // ---- classification (jointbp_ets.cpp:6199-6245): exact, stabilizer-equivalent residual
-        unsigned *rx = reinterpret_cast<unsigned *>(sh.c2v);     // BP state is no longer needed
-        const int w32 = 2 * code.words;
+        const int words = (n + 63) / 64, w32 = 2 * words;
+        unsigned *rx = reinterpret_cast<unsigned *>(c2v);     // BP state is no longer needed
         unsigned *rz = rx + w32;
         for (int w = threadIdx.x; w < 2 * w32; w += blockDim.x) rx[w] = 0u;
         __syncthreads();
@@ -380,8 +394,8 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
         for (int base = (threadIdx.x >> 5) * 32; base < n; base += blockDim.x) {
             const int v = base + (threadIdx.x & 31);
             const bool in = v < n;
-            const unsigned e = in ? ((__float_as_uint(sh.A[v]) & 1u) | ((__float_as_uint(sh.A[n + v]) & 1u) << 1)) : 0u;
-            const unsigned tv = in && have_err ? sh.err[v] : e;
+            const unsigned e = in ? ((__float_as_uint(A[v]) & 1u) | ((__float_as_uint(A[n + v]) & 1u) << 1)) : 0u;
+            const unsigned tv = in && have_err ? err[v] : e;
             if (in && run.est_out) run.est_out[local * n + v] = static_cast<uint8_t>(e);
             exact &= tv == e;
             const unsigned bx = __ballot_sync(0xffffffffu, ((tv ^ e) & 1u) != 0);
@@ -391,25 +405,24 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
         exact = __syncthreads_and(exact) && have_err;
         bool stab = false;
         if (have_err && ok && !exact) {
-            stab = res_in_row_space(reinterpret_cast<uint64_t *>(rx), code.words, code.basis_rows[1], code.pivot_row[1],
-                                    sh.ints);
+            stab = res_in_row_space(reinterpret_cast<uint64_t *>(rx), words, code.basis_rows[1], code.pivot_row[1], ints);
             if (stab)
-                stab = res_in_row_space(reinterpret_cast<uint64_t *>(rz), code.words, code.basis_rows[0],
-                                        code.pivot_row[0], sh.ints);
+                stab = res_in_row_space(reinterpret_cast<uint64_t *>(rz), words, code.basis_rows[0], code.pivot_row[0],
+                                        ints);
         } else if (have_err && ok) {
             stab = true;   // exact: the residual is zero
         }
         const bool success = have_err ? (ok && stab) : ok;
         if (threadIdx.x == 0) {
-            DevCounters *c = run.cnt;
-            atomicAdd(&c->done, 1ull);
-            atomicAdd(&c->total_iters, static_cast<unsigned long long>(iters));
-            atomicAdd(&c->bp_trial_iterations, static_cast<unsigned long long>(iters));
-            if (!success) atomicAdd(&c->failures, 1ull);
-            if (!ok) atomicAdd(&c->bp_fail, 1ull);
-            if (exact) atomicAdd(&c->exact, 1ull);
-            if (ok) atomicAdd(&c->syndrome_ok, 1ull);
-            if (success && !exact && stab) atomicAdd(&c->stab_success, 1ull);
+            DevCounters *cn = run.cnt;
+            atomicAdd(&cn->done, 1ull);
+            atomicAdd(&cn->total_iters, static_cast<unsigned long long>(iters));
+            atomicAdd(&cn->bp_trial_iterations, static_cast<unsigned long long>(iters));
+            if (!success) atomicAdd(&cn->failures, 1ull);
+            if (!ok) atomicAdd(&cn->bp_fail, 1ull);
+            if (exact) atomicAdd(&cn->exact, 1ull);
+            if (ok) atomicAdd(&cn->syndrome_ok, 1ull);
+            if (success && !exact && stab) atomicAdd(&cn->stab_success, 1ull);
             if (run.hist && iters >= 1 && iters <= run.max_iter) atomicAdd(&run.hist[iters], 1ull);
             if (run.res_out) {
                 jbp_trial_result rec{};
