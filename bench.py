@@ -41,13 +41,16 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--batch", type=int, default=131072, help="trials per step")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16", "fp64"])
+    ap.add_argument("--precision", default="fp16", choices=["fp32", "fp16", "fp64"],
+                    help="fp16 = FP32 arithmetic with FP16 message storage (the trial-resident engine)")
+    ap.add_argument("--engine", default="auto", choices=["auto", "resident", "slots"])
     ap.add_argument("--p", type=float, default=0.04)
     ap.add_argument("--max-iter", type=int, default=1000)
     ap.add_argument("--seed", type=int, default=106)
     ap.add_argument("--no-pp", action="store_true", help="plain BP without post-processing")
     ap.add_argument("--flip-hist", type=int, default=5)
-    ap.add_argument("--fp64-batch", type=int, default=32768, help="trials of the FP64 comparison step (0 = skip)")
+    ap.add_argument("--fp64-batch", type=int, default=131072,
+                    help="trials of the FP64 comparison step, the same trials as the first timed step (0 = skip)")
     ap.add_argument("--e2e-batch", type=int, default=65536, help="trials per end-to-end step (0 = skip)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--slots", type=int, default=0)
@@ -222,7 +225,7 @@ def main():
     dec = Decoder.from_params(device=local)
     pp = not args.no_pp
     opts = Options(precision=args.precision, max_iter=args.max_iter, enable_pp=pp, flip_hist=args.flip_hist,
-                   slots=args.slots, profile=True)
+                   slots=args.slots, profile=True, engine=args.engine)
     B = args.batch
     stride = B * (args.warmup + args.steps + 2)
     base = 1 + rank * stride          # distinct trial ranges per rank
@@ -243,9 +246,13 @@ def main():
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record()
     agg = {"trials": 0, "failures": 0, "total_iters": 0, "check_ms": 0.0, "var_ms": 0.0, "kernel_launches": 0,
-           "bp_trial_iterations": 0, "profiled_iterations": 0}
+           "bp_trial_iterations": 0, "profiled_iterations": 0, "device_ms": 0.0, "pp_success": 0}
+    first_res = None
     for k in range(args.steps):
-        st, _ = dec.simulate(args.seed, B, args.p, opts, first_trial=base + (args.warmup + k) * B, per_trial=False)
+        st, res = dec.simulate(args.seed, B, args.p, opts, first_trial=base + (args.warmup + k) * B,
+                               per_trial=(k == 0))
+        if k == 0:
+            first_res = res
         for key in agg:
             agg[key] += st[key]
     ev1.record()
@@ -264,35 +271,66 @@ def main():
         total_trials = float(agg["trials"])
     value = total_trials / (ms / 1000.0)
 
-    # dominant kernel roofline (algorithmic bytes: one read + one write of a message per edge)
-    es = {"fp32": 4, "fp16": 2, "fp64": 16}[args.precision]
-    bytes_per_trial_iter = 2 * EDGES * es          # per kernel (check or variable)
-    kname, kms = ("check", agg["check_ms"]) if agg["check_ms"] >= agg["var_ms"] else ("variable", agg["var_ms"])
     peak, peak_kind = measured_peaks()
-    achieved = agg["bp_trial_iterations"] * bytes_per_trial_iter / (kms / 1000.0) / 1e9 if kms > 0 else None
-    launches = agg["profiled_iterations"]
-    traffic = None
-    tfile = ROOT / "profiles" / "traffic.json"
-    if tfile.exists():
-        tj = json.loads(tfile.read_text())
-        traffic = tj.get(f"{args.precision}_{kname}_bytes_per_trial_iteration")
+    traffic_tab = json.loads((ROOT / "profiles" / "traffic.json").read_text()) if (ROOT / "profiles" / "traffic.json").exists() else {}
+    resident = agg["kernel_launches"] == args.steps and agg["check_ms"] == 0.0
+    if resident:
+        # trial-resident kernel: no message traffic to HBM; bound by the special-function unit
+        # (MUFU: ex2 per edge input, rcp + lg2 per edge output, 1 ex2 + 2 lg2 per coupling)
+        mufu_per_ti = 3 * EDGES + 6 * N_QUBITS
+        kms = agg["device_ms"]
+        sm_mhz = clk.get("sm_mhz") or 1965.0
+        n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+        sfu_peak = 16 * n_sm * sm_mhz / 1e3          # Gop/s: 16 MUFU results / clk / SM
+        achieved = agg["bp_trial_iterations"] * mufu_per_ti / (kms / 1000.0) / 1e9 if kms > 0 else None
+        tr = traffic_tab.get("resident_dram_bytes_per_trial")
+        roofline = {"bound": "sfu", "kernel": "k_resident (trial in shared memory, FP16 c2v)", "achieved": achieved,
+                    "peak": sfu_peak, "unit": "Gop/s", "frac": achieved / sfu_peak if achieved else None,
+                    "traffic": tr * agg["trials"] / args.steps if tr is not None else None,
+                    "peak_kind": f"derived: 16 MUFU results/clk/SM x {n_sm} SMs x median SM clock {sm_mhz:.0f} MHz",
+                    "mufu_ops_per_trial_iteration": mufu_per_ti, "trial_iterations": agg["bp_trial_iterations"],
+                    "launches": agg["kernel_launches"], "kernel_ms": kms,
+                    "hbm_equivalent_gbs": agg["bp_trial_iterations"] * 2 * 2 * EDGES * 2 / (kms / 1000.0) / 1e9,
+                    "hbm_peak_gbs": peak}
+    else:
+        # slot engine: dominant kernel, algorithmic bytes = one read + one write of a message per edge
+        es = {"fp32": 4, "fp16": 2, "fp64": 16}[args.precision]
+        bytes_per_trial_iter = 2 * EDGES * es          # per kernel (check or variable)
+        kname, kms = ("check", agg["check_ms"]) if agg["check_ms"] >= agg["var_ms"] else ("variable", agg["var_ms"])
+        achieved = agg["bp_trial_iterations"] * bytes_per_trial_iter / (kms / 1000.0) / 1e9 if kms > 0 else None
+        launches = agg["profiled_iterations"]
+        traffic = traffic_tab.get(f"{args.precision}_{kname}_bytes_per_trial_iteration")
         if traffic is not None and launches:
             traffic = traffic * agg["bp_trial_iterations"] / launches
+        roofline = {"bound": "hbm", "kernel": f"{kname} node ({args.precision})", "achieved": achieved,
+                    "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                    "traffic": traffic, "peak_kind": peak_kind, "bytes_per_trial_iteration": bytes_per_trial_iter,
+                    "trial_iterations": agg["bp_trial_iterations"], "launches": launches,
+                    "check_ms": agg["check_ms"], "var_ms": agg["var_ms"]}
 
-    # FP64 comparison (plain FP64 BP, same workload, one step)
+    # FP64 comparison: plain FP64 BP(+PP) on the same GPU, on the trials of the first timed step
     fp64 = None
     if args.fp64_batch > 0 and rank == 0:
         o64 = Options(precision="fp64", max_iter=args.max_iter, enable_pp=pp, flip_hist=args.flip_hist)
-        dec.simulate(args.seed, args.fp64_batch // 4, args.p, o64, first_trial=10 ** 9, per_trial=False)
+        dec.simulate(args.seed, max(32, args.fp64_batch // 16), args.p, o64, first_trial=10 ** 9, per_trial=False)
         torch.cuda.synchronize()
+        F = min(args.fp64_batch, B)
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record()
-        st64, _ = dec.simulate(args.seed, args.fp64_batch, args.p, o64, first_trial=base + 10 ** 8, per_trial=False)
+        st64, r64 = dec.simulate(args.seed, F, args.p, o64, first_trial=base + args.warmup * B)
         b.record()
         torch.cuda.synchronize()
+        rlo = first_res[:F]
+        f64, flo = int(st64["failures"]), int((rlo["success"] == 0).sum())
         fp64 = {"value": st64["trials"] / (a.elapsed_time(b) / 1000.0), "trials": st64["trials"],
-                "failures": st64["failures"], "avg_iter": st64["total_iters"] / max(1, st64["trials"])}
+                "failures": f64, "ci95": list(wilson_interval(F, f64)),
+                "avg_iter": st64["total_iters"] / max(1, st64["trials"]),
+                "same_trials": {"trials": F, "failures_this": flo, "failures_fp64": f64,
+                                "ci95_this": list(wilson_interval(F, flo)),
+                                "outcome_disagreements": int((rlo["success"] != r64["success"]).sum()),
+                                "iteration_disagreements": int((rlo["iterations"] != r64["iterations"]).sum()),
+                                "ler_difference": (flo - f64) / F}}
 
     # end to end through the C ABI with host buffers (reference-sampled errors in pinned memory)
     e2e = None
@@ -301,7 +339,7 @@ def main():
         host = torch.empty((E, N_QUBITS), dtype=torch.uint8, pin_memory=True).numpy()
         host[:] = sample_reference_errors(N_QUBITS, args.seed, base + 5 * 10 ** 8, E, args.p)
         oe = Options(precision=args.precision, max_iter=args.max_iter, enable_pp=pp, flip_hist=args.flip_hist,
-                     slots=args.slots)
+                     slots=args.slots, engine=args.engine)
         dec.decode_errors(host[: max(32, E // 8)], args.p, oe, want_est=False)
         torch.cuda.synchronize()
         barrier()
@@ -334,22 +372,22 @@ def main():
     if rank != 0:
         return 0
     lo, hi = wilson_interval(agg["trials"], agg["failures"])
+    
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": {"fp32": "f32", "fp16": "f16-storage/f32", "fp64": "f64"}[args.precision],
+        "dtype": {"fp32": "f32", "fp16": "f32 arithmetic, f16 message storage", "fp64": "f64"}[args.precision],
         "data": "synthetic: Philox4x32-10 depolarizing noise keyed by (seed, trial index)",
-        "config": {"workload": workload_name(args, f"{args.precision} messages"), "p": args.p,
+        "config": {"workload": workload_name(args, {"fp16": "FP32 arithmetic with FP16 message storage",
+                                                    "fp32": "FP32 messages", "fp64": "FP64 messages"}[args.precision]),
+                   "p": args.p,
                    "max_iter": args.max_iter, "enable_pp": pp, "flip_hist": args.flip_hist,
-                   "trials_per_step": B, "slots": None, "l2": "message state (>= 7 GB) larger than L2",
+                   "trials_per_step": B, "engine": "resident" if resident else "slots",
+                   "l2": ("trial state in shared memory; no message traffic to HBM" if resident
+                          else "message state (>= 7 GB) larger than L2"),
                    "parallelism": f"replica trial ranges x{world}"},
         "gpu_launches": agg["kernel_launches"],
-        "roofline": {"bound": "hbm", "kernel": f"{kname} node ({args.precision})", "achieved": achieved,
-                     "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                     "traffic": traffic, "peak_kind": peak_kind,
-                     "bytes_per_trial_iteration": bytes_per_trial_iter,
-                     "trial_iterations": agg["bp_trial_iterations"], "launches": launches,
-                     "check_ms": agg["check_ms"], "var_ms": agg["var_ms"]},
+        "roofline": roofline,
         "ler": {"trials": agg["trials"], "failures": agg["failures"], "ci95": [lo, hi],
                 "avg_iter": agg["total_iters"] / max(1, agg["trials"])},
         "fp64": fp64,

@@ -86,12 +86,33 @@ size_t msg_elem_bytes(int precision) {
     return precision == JBP_PREC_FP64 ? sizeof(double2) : (precision == JBP_PREC_FP32 ? sizeof(float) : sizeof(__half));
 }
 
+// Run Summary counters of a finished run.
+void fill_stats(const DevCounters &hc, jbp_stats &stats) {
+    stats.trials = static_cast<long long>(hc.done);
+    stats.failures = static_cast<long long>(hc.failures);
+    stats.bp_fail = static_cast<long long>(hc.bp_fail);
+    stats.pp_success = static_cast<long long>(hc.pp_success);
+    stats.flip_pp_success = static_cast<long long>(hc.flip_pp_success);
+    stats.osd_pp_success = static_cast<long long>(hc.osd_pp_success);
+    stats.stab_success = static_cast<long long>(hc.stab_success);
+    stats.ets_used = static_cast<long long>(hc.ets_used);
+    stats.ets_saved = static_cast<long long>(hc.ets_saved);
+    stats.ets6_used = static_cast<long long>(hc.ets6_used);
+    stats.ets6_saved = static_cast<long long>(hc.ets6_saved);
+    stats.ets12_used = static_cast<long long>(hc.ets12_used);
+    stats.ets12_saved = static_cast<long long>(hc.ets12_saved);
+    stats.exact = static_cast<long long>(hc.exact);
+    stats.total_iters = static_cast<long long>(hc.total_iters);
+    stats.bp_trial_iterations = static_cast<long long>(hc.bp_trial_iterations);
+}
+
 }  // namespace
 
 Engine::~Engine() {
     free_buffers();
     delete rcode_;
     cudaFree(res_cnt_);
+    cudaFree(res_pp_scratch_);
     for (void *p : code_allocs_) cudaFree(p);
     for (void *p : ets_allocs_) cudaFree(p);
 }
@@ -207,7 +228,7 @@ std::string Engine::build_res_code() {
     if (!(P == 768 && J == 3 && L == 12))
         return "no resident kernel built for P=" + std::to_string(P) + ", J=" + std::to_string(J) + ", L=" +
                std::to_string(L);
-    const size_t smem = res_smem_bytes(n, m, L, sizeof(__half));
+    const size_t smem = res_smem_bytes(n, m, L, sizeof(__half), true);
     if (smem > static_cast<size_t>(smem_optin_) - 1024) return "trial state does not fit in shared memory";
     rcode_ = rc.release();
     return "";
@@ -220,7 +241,8 @@ bool Engine::resident_applies(const jbp_options &o, std::string *why) const {
     };
     if (!res_code_ok_) return no(res_code_why_);
     if (o.precision != JBP_PREC_FP16) return no("the resident tier stores messages in FP16 (precision FP16)");
-    if (o.enable_pp) return no("post-processing runs on the slot tier");
+    if (o.enable_pp && (o.check_interval != 1 || o.check_warmup != 0))
+        return no("post-processing needs a syndrome test every iteration");
     if (o.damping > 0.0) return no("damping runs on the slot tier");
     if (o.freeze_syn) return no("freeze-syn runs on the slot tier");
     return true;
@@ -232,8 +254,9 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     JBP_CUDA_TRY(cudaSetDevice(device_), "cudaSetDevice");
     if (!res_cnt_) JBP_CUDA_TRY(cudaMalloc(&res_cnt_, sizeof(DevCounters)), "cudaMalloc(counters)");
     const ResCode &rc = *rcode_;
-    auto kern = k_resident<768, 3, 12, StoreHalf>;
-    const size_t smem = res_smem_bytes(rc.n, rc.m, rc.L, sizeof(__half));
+    const bool pp = o.enable_pp != 0;
+    auto kern = pp ? k_resident<768, 3, 12, StoreHalf, true> : k_resident<768, 3, 12, StoreHalf, false>;
+    const size_t smem = res_smem_bytes(rc.n, rc.m, rc.L, sizeof(__half), pp);
     JBP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
                  "smem attribute");
     int per_sm = 0;
@@ -241,6 +264,22 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     if (per_sm < 1) return "the resident kernel does not fit on an SM";
     const long long want = std::max<long long>(1, std::min<long long>(rq.ntrials, 1LL << 30));
     const int grid = static_cast<int>(std::min<long long>(static_cast<long long>(per_sm) * sm_count_, want));
+    const int H = std::max(0, o.flip_hist);
+    const int R = std::max(H + 1, 3);
+    size_t stride = 0;
+    if (pp) {
+        std::string ee = upload_ets();
+        if (!ee.empty()) return ee;
+        stride = pp_align(res_pp_scratch_bytes(rc.n, rc.m, R));
+        const size_t need = stride * grid;
+        if (res_pp_bytes_ < need) {
+            cudaFree(res_pp_scratch_);
+            res_pp_scratch_ = nullptr;
+            res_pp_bytes_ = 0;
+            JBP_CUDA_TRY(cudaMalloc(&res_pp_scratch_, need), "cudaMalloc(post-processing scratch)");
+            res_pp_bytes_ = need;
+        }
+    }
     ResRun r{};
     r.max_iter = o.max_iter;
     r.check_warmup = std::max(0, o.check_warmup);
@@ -260,6 +299,11 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     r.res_out = rq.d_res_out;
     r.hist = rq.d_hist;
     r.cnt = res_cnt_;
+    r.flip_hist = H;
+    r.dc = dcode_;
+    r.ets = dets_;
+    r.pp_scratch = pp ? res_pp_scratch_ : nullptr;
+    r.pp_scratch_stride = stride;
     cudaStream_t st = rq.stream;
     cudaEvent_t ev0, ev1;
     JBP_CUDA_TRY(cudaEventCreate(&ev0), "cudaEventCreate");
@@ -280,14 +324,9 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
     if (ce != cudaSuccess) return cuda_err(ce, "resident run");
+    if (hc.bad_input) return "error vector has invalid value";
     if (hc.done != static_cast<unsigned long long>(rq.ntrials)) return "resident run finished an unexpected number of trials";
-    stats.trials = static_cast<long long>(hc.done);
-    stats.failures = static_cast<long long>(hc.failures);
-    stats.bp_fail = static_cast<long long>(hc.bp_fail);
-    stats.stab_success = static_cast<long long>(hc.stab_success);
-    stats.exact = static_cast<long long>(hc.exact);
-    stats.total_iters = static_cast<long long>(hc.total_iters);
-    stats.bp_trial_iterations = static_cast<long long>(hc.bp_trial_iterations);
+    fill_stats(hc, stats);
     stats.device_ms = ms;
     stats.kernel_launches = 1;
     stats.slots = grid;
@@ -695,22 +734,8 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     cudaEventDestroy(poll_ev[0]);
     cudaEventDestroy(poll_ev[1]);
     if (!err.empty()) return err;
-    stats.trials = static_cast<long long>(hc.done);
-    stats.failures = static_cast<long long>(hc.failures);
-    stats.bp_fail = static_cast<long long>(hc.bp_fail);
-    stats.pp_success = static_cast<long long>(hc.pp_success);
-    stats.flip_pp_success = static_cast<long long>(hc.flip_pp_success);
-    stats.osd_pp_success = static_cast<long long>(hc.osd_pp_success);
-    stats.stab_success = static_cast<long long>(hc.stab_success);
-    stats.ets_used = static_cast<long long>(hc.ets_used);
-    stats.ets_saved = static_cast<long long>(hc.ets_saved);
-    stats.ets6_used = static_cast<long long>(hc.ets6_used);
-    stats.ets6_saved = static_cast<long long>(hc.ets6_saved);
-    stats.ets12_used = static_cast<long long>(hc.ets12_used);
-    stats.ets12_saved = static_cast<long long>(hc.ets12_saved);
-    stats.exact = static_cast<long long>(hc.exact);
-    stats.total_iters = static_cast<long long>(hc.total_iters);
-    stats.bp_trial_iterations = static_cast<long long>(hc.bp_trial_iterations);
+    if (hc.bad_input) return "error vector has invalid value";
+    fill_stats(hc, stats);
     stats.device_ms = ms;
     stats.kernel_launches = launches;
     stats.check_ms = check_ms;

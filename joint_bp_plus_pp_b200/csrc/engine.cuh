@@ -85,6 +85,7 @@ struct DevCounters {
     unsigned long long ets_used, ets_saved, ets6_used, ets6_saved, ets12_used, ets12_saved;
     unsigned long long bp_trial_iterations;
     unsigned long long watchdog;
+    unsigned long long bad_input;   // error bytes outside 0..3 seen in a kSrcErrors source
 };
 
 struct DevRun {

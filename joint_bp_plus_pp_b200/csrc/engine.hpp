@@ -93,6 +93,8 @@ private:
     std::string res_code_why_;
     ResCode *rcode_ = nullptr;
     DevCounters *res_cnt_ = nullptr;
+    unsigned char *res_pp_scratch_ = nullptr;
+    size_t res_pp_bytes_ = 0;
     CodeModel model_;
     DevCode dcode_{};
     std::vector<void *> code_allocs_;

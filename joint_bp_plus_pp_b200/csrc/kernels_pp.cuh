@@ -103,6 +103,22 @@ __host__ __device__ inline size_t pp_smem_bytes(int n, int M, int mmax) {
            pp_align(8ull * CW);
 }
 
+// Carves the post-processing shared arrays from `base` (pp_smem_bytes(n, M, mmax) bytes).
+__device__ __forceinline__ PpShared pp_shared_carve(unsigned char *base, int n, int M, int mmax) {
+    const int MW = (mmax + 63) / 64;
+    PpShared sh;
+    size_t o = 0;
+    sh.est = base + o; o += pp_align(n);
+    sh.mark = base + o; o += pp_align(n);
+    sh.tgt = base + o; o += pp_align(M);
+    sh.diff = base + o; o += pp_align(mmax);
+    sh.touch = base + o; o += pp_align(mmax);
+    sh.ints = reinterpret_cast<int *>(base + o); o += pp_align(64 * 4);
+    sh.wv = reinterpret_cast<uint64_t *>(base + o); o += pp_align(8ull * MW);
+    sh.wc = reinterpret_cast<uint64_t *>(base + o);
+    return sh;
+}
+
 __device__ __forceinline__ int side_bit(int state, int side) { return (state >> side) & 1; }
 
 // Check (row of `side`) of a variable's k-th edge on that side.
@@ -169,22 +185,22 @@ static __device__ bool gf2_solve32(uint32_t *a, uint8_t *b, int m, int nv, uint3
 
 // One ETS table of one side (attempt_ets_fix_side).  diff / ints[7..9] hold the side's
 // syndrome difference.  Serial in thread 0: a few dozen entries of <= 32 variables.
-static __device__ bool blk_ets_table(const DevCode &code, const DevRun &run, const PpShared &sh, int side, int g) {
+static __device__ bool blk_ets_table(const DevCode &code, const DevEts &ets, const PpShared &sh, int side, int g) {
     if (threadIdx.x == 0) {
         sh.ints[10] = 0;
         const int c0 = sh.ints[8], c1 = sh.ints[9];
         const unsigned long long key = (static_cast<unsigned long long>(static_cast<unsigned>(c0)) << 32) |
                                        static_cast<unsigned>(c1);
-        const int nv = run.ets.size[g];
-        const int first = run.ets.first[g][side], count = run.ets.count[g][side];
+        const int nv = ets.size[g];
+        const int first = ets.first[g][side], count = ets.count[g][side];
         const int dv = code.s[side].dv, dc = code.s[side].dc;
         const int *chk_var = code.s[side].chk_var;
         int checks[32 * kMaxDv];
         uint32_t rows[32 * kMaxDv];
         uint8_t rhs[32 * kMaxDv];
         for (int e = first; e < first + count && nv > 0 && nv <= 32; ++e) {
-            if (run.ets.key[e] != key) continue;
-            const int *vars = run.ets.vars + run.ets.var_first[e];
+            if (ets.key[e] != key) continue;
+            const int *vars = ets.vars + ets.var_first[e];
             int nch = 0;
             for (int i = 0; i < nv; ++i)
                 for (int k = 0; k < dv; ++k) {
@@ -231,14 +247,14 @@ static __device__ bool blk_ets_table(const DevCode &code, const DevRun &run, con
 }
 
 // attempt_ets_fix_side_multi: the first group whose table applies; returns its index or -1.
-static __device__ int blk_ets_multi(const DevCode &code, const DevRun &run, const PpShared &sh, int side) {
+static __device__ int blk_ets_multi(const DevCode &code, const DevEts &ets, const PpShared &sh, int side) {
     bool any = false;
-    for (int g = 0; g < run.ets.ngroups; ++g) any |= run.ets.count[g][side] > 0;
+    for (int g = 0; g < ets.ngroups; ++g) any |= ets.count[g][side] > 0;
     if (!any) return -1;
     if (blk_side_diff(code, sh, side) != 2) return -1;
-    for (int g = 0; g < run.ets.ngroups; ++g) {
-        if (run.ets.count[g][side] == 0) continue;
-        if (blk_ets_table(code, run, sh, side, g)) return g;
+    for (int g = 0; g < ets.ngroups; ++g) {
+        if (ets.count[g][side] == 0) continue;
+        if (blk_ets_table(code, ets, sh, side, g)) return g;
     }
     return -1;
 }
@@ -247,7 +263,7 @@ static __device__ int blk_ets_multi(const DevCode &code, const DevRun &run, cons
 
 // Block exclusive scan of per-thread counts; returns this thread's offset, total in ints[20].
 static __device__ int blk_scan(const PpShared &sh, int cnt) {
-    __shared__ int part[kPpThreads / 32];
+    __shared__ int part[32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int incl = cnt;
     for (int d = 1; d < 32; d <<= 1) {
@@ -358,16 +374,36 @@ static __device__ bool blk_flip_attempt(const DevCode &code, const PpShared &sh,
     return true;
 }
 
-// Marks the flips of `side` between the slot's iterations j and j-1 (decision planes).
-static __device__ void blk_mark_flips(const DevCode &code, const DevRun &run, const PpShared &sh, int side, int slot,
-                               int k, int j, bool accumulate) {
+// Decision history of one trial for the flip window: bit `side` of the trial's decision of
+// variable v flipped between iterations j - 1 and j.
+// Slot engine: the ring of 32-slot bit planes (the trial's bit in each word).
+struct SlotHistory {
+    const DevRun *run;
+    int slot, k;   // k = the trial's current iteration (planes are indexed relative to it)
+    __device__ unsigned flip(int side, int j, int v, int n) const {
+        const size_t pa = plane_offset(*run, n, k - j), pb = plane_offset(*run, n, k - j + 1);
+        const unsigned *planes = side ? run->estz : run->estx;
+        const size_t row = static_cast<size_t>(slot / kGroup) * n;
+        return ((planes[pa + row + v] ^ planes[pb + row + v]) >> (slot % kGroup)) & 1u;
+    }
+};
+// Trial-resident engine: a ring of R per-iteration decision arrays (bytes 0..3).
+struct RingHistory {
+    const uint8_t *ring;
+    int R;
+    __device__ unsigned flip(int side, int j, int v, int n) const {
+        const uint8_t a = ring[static_cast<size_t>(j % R) * n + v], b = ring[static_cast<size_t>((j - 1) % R) * n + v];
+        return ((a ^ b) >> side) & 1u;
+    }
+};
+
+// Marks the flips of `side` between iterations j - 1 and j.
+template <class Hist>
+static __device__ void blk_mark_flips(const DevCode &code, const Hist &hist, const PpShared &sh, int side, int j,
+                                      bool accumulate) {
     const int n = code.n;
-    const size_t pa = plane_offset(run, n, k - j), pb = plane_offset(run, n, k - j + 1);
-    const unsigned *planes = side ? run.estz : run.estx;
-    const size_t row = static_cast<size_t>(slot / kGroup) * n;
-    const int b = slot % kGroup;
     for (int v = threadIdx.x; v < n; v += blockDim.x) {
-        const uint8_t f = static_cast<uint8_t>(((planes[pa + row + v] ^ planes[pb + row + v]) >> b) & 1u);
+        const uint8_t f = static_cast<uint8_t>(hist.flip(side, j, v, n));
         sh.mark[v] = accumulate ? static_cast<uint8_t>(sh.mark[v] | f) : f;
     }
     __syncthreads();
@@ -380,33 +416,34 @@ static __device__ bool blk_any_mark(const DevCode &code, const PpShared &sh) {
 }
 
 // build_flip_sets + the first set that applies (union, then the window newest to oldest,
-// or the last flips when there is neither window nor union).
-static __device__ bool blk_flip_side(const DevCode &code, const DevRun &run, const PpShared &sh, const PpScratch &sc,
-                              int side, int slot, int k) {
+// or the last flips when there is neither window nor union).  k = current iteration,
+// act = iteration the flip window started (0: none).
+template <class Hist>
+static __device__ bool blk_flip_side(const DevCode &code, const Hist &hist, int flip_hist, int act,
+                                     const PpShared &sh, const PpScratch &sc, int side, int k) {
     blk_side_diff(code, sh, side);
-    const int act = run.act_k[slot];
-    const bool window = act > 0 && run.flip_hist > 0;
+    const bool window = act > 0 && flip_hist > 0;
     int jlo = 0, wlen = 0;
     if (window) {
-        jlo = max(max(act, 2), k - run.flip_hist + 1);
+        jlo = max(max(act, 2), k - flip_hist + 1);
         wlen = k >= jlo ? k - jlo + 1 : 0;
     }
     bool have_union = false;
     if (window) {
         for (int v = threadIdx.x; v < code.n; v += blockDim.x) sh.mark[v] = 0;
         __syncthreads();
-        for (int j = jlo; j <= k; ++j) blk_mark_flips(code, run, sh, side, slot, k, j, true);
+        for (int j = jlo; j <= k; ++j) blk_mark_flips(code, hist, sh, side, j, true);
         have_union = blk_any_mark(code, sh);
         if (have_union && blk_flip_attempt(code, sh, sc, side)) return true;
     }
     if (wlen > 0) {
         for (int j = k; j >= jlo; --j) {
-            blk_mark_flips(code, run, sh, side, slot, k, j, false);
+            blk_mark_flips(code, hist, sh, side, j, false);
             if (!blk_any_mark(code, sh)) continue;
             if (blk_flip_attempt(code, sh, sc, side)) return true;
         }
     } else if (!have_union && k >= 2) {
-        blk_mark_flips(code, run, sh, side, slot, k, k, false);
+        blk_mark_flips(code, hist, sh, side, k, false);
         if (blk_any_mark(code, sh) && blk_flip_attempt(code, sh, sc, side)) return true;
     }
     return false;
@@ -436,14 +473,13 @@ static __device__ void blk_sort_pairs(unsigned long long *key, int *idx, int np2
 }
 
 // attempt_osd_pp_side restated as one incremental elimination (see the file comment).
-static __device__ bool blk_osd_side(const DevCode &code, const DevRun &run, const PpShared &sh, const PpScratch &sc,
-                             int side, int slot) {
+static __device__ bool blk_osd_side(const DevCode &code, const double *llr, const PpShared &sh, const PpScratch &sc,
+                                    int side) {
     const int n = code.n, m = code.s[side].m, dv = code.s[side].dv;
     const int MW = (m + 63) / 64, CW = (m + 2 + 63) / 64;
     const int np2 = pp_npow2(n);
     const int cnt = blk_side_diff(code, sh, side);
     if (cnt == 0) return false;  // "skipped (no syndrome diff)"
-    const double *llr = run.llr + (static_cast<size_t>(side) * run.S + slot) * n;
     for (int i = threadIdx.x; i < np2; i += blockDim.x) {
         sc.key[i] = i < n ? static_cast<unsigned long long>(__double_as_longlong(llr[i])) : ~0ull;
         sc.idx[i] = i < n ? i : 0x7fffffff;
@@ -544,6 +580,66 @@ static __device__ bool blk_osd_side(const DevCode &code, const DevRun &run, cons
 
 // ------------------------------------------------------------------ driver
 
+// Outcome of one post-processing pass.
+struct PpOutcome {
+    bool ets_used, e6, e12, ok, ets_ok, flip_ok, osd_ok;
+};
+
+// The stage sequence of an in-loop attempt or a post-BP pass on sh.est (in place): ETS on
+// both sides, then (if the syndromes do not both match) flip sets, then OSD when at most
+// 20 checks per side are unsatisfied (jointbp_ets.cpp:2736-3074, 6020-6197).  llr_x / llr_z
+// are the |LLR| keys of the OSD column order.
+template <class Hist>
+static __device__ PpOutcome blk_pp_stages(const DevCode &code, const DevEts &ets, const Hist &hist, int flip_hist,
+                                          int act, int k, const double *llr_x, const double *llr_z,
+                                          const PpShared &sh, const PpScratch &sc) {
+    PpOutcome r{};
+    const int gx = blk_ets_multi(code, ets, sh, 0);
+    const int gz = blk_ets_multi(code, ets, sh, 1);
+    r.ets_used = gx >= 0 || gz >= 0;
+    r.e6 = (gx >= 0 && ets.size[gx] == 6) || (gz >= 0 && ets.size[gz] == 6);
+    r.e12 = (gx >= 0 && ets.size[gx] == 12) || (gz >= 0 && ets.size[gz] == 12);
+    bool ok = false;
+    if (r.ets_used) {
+        ok = blk_side_diff(code, sh, 0) == 0;
+        ok = (blk_side_diff(code, sh, 1) == 0) && ok;
+        r.ets_ok = ok;
+    }
+    if (!ok) {
+        const bool fx = blk_flip_side(code, hist, flip_hist, act, sh, sc, 0, k);
+        const bool fz = blk_flip_side(code, hist, flip_hist, act, sh, sc, 1, k);
+        if (fx || fz) {
+            ok = blk_side_diff(code, sh, 0) == 0;
+            ok = (blk_side_diff(code, sh, 1) == 0) && ok;
+            r.flip_ok = ok;
+        }
+    }
+    if (!ok) {
+        const int ux = blk_side_diff(code, sh, 0), uz = blk_side_diff(code, sh, 1);
+        if ((ux > uz ? ux : uz) <= 20) {
+            const bool ox = blk_osd_side(code, llr_x, sh, sc, 0);
+            const bool oz = blk_osd_side(code, llr_z, sh, sc, 1);
+            if (ox || oz) {
+                ok = blk_side_diff(code, sh, 0) == 0;
+                ok = (blk_side_diff(code, sh, 1) == 0) && ok;
+                r.osd_ok = ok;
+            }
+        }
+    }
+    r.ok = ok;
+    return r;
+}
+
+// Result flags of a pass (ResultBit), for an in-loop success or a post-BP pass.
+__device__ __forceinline__ int pp_result_flags(const PpOutcome &o, bool in_loop_success) {
+    if (in_loop_success)
+        return kResSyndromeOk | kResPpInDecode | (o.ets_ok ? kResPpInEts : 0) | (o.flip_ok ? kResPpInFlip : 0) |
+               (o.ets_used ? kResUsedAny : 0) | (o.e6 ? kResUsed6 : 0) | (o.e12 ? kResUsed12 : 0);
+    return kResPostEntered | (o.ok ? kResSyndromeOk : 0) | (o.ets_used ? kResEtsPost : 0) | (o.e6 ? kResUsed6 : 0) |
+           (o.e12 ? kResUsed12 : 0) | (o.ets_ok ? kResEtsOk : 0) | (o.flip_ok ? kResFlipOk : 0) |
+           (o.osd_ok ? kResOsdOk : 0);
+}
+
 // Post-processing of the pending slots (in-loop attempt at iteration k, or post-BP on the
 // final estimate).  The stage sequence is the same in both; an in-loop attempt keeps the
 // corrected estimate only if both syndromes match, a post-BP run keeps whatever its stages
@@ -552,19 +648,7 @@ static __device__ bool blk_osd_side(const DevCode &code, const DevRun &run, cons
 static __global__ void __launch_bounds__(kPpThreads) k_postprocess(DevCode code, DevRun run) {
     extern __shared__ unsigned char pp_smem[];
     const int n = code.n, mx = code.s[0].m, mz = code.s[1].m, M = mx + mz, mmax = mx > mz ? mx : mz;
-    const int MW = (mmax + 63) / 64;
-    PpShared sh;
-    {
-        size_t o = 0;
-        sh.est = pp_smem + o; o += pp_align(n);
-        sh.mark = pp_smem + o; o += pp_align(n);
-        sh.tgt = pp_smem + o; o += pp_align(M);
-        sh.diff = pp_smem + o; o += pp_align(mmax);
-        sh.touch = pp_smem + o; o += pp_align(mmax);
-        sh.ints = reinterpret_cast<int *>(pp_smem + o); o += pp_align(64 * 4);
-        sh.wv = reinterpret_cast<uint64_t *>(pp_smem + o); o += pp_align(8ull * MW);
-        sh.wc = reinterpret_cast<uint64_t *>(pp_smem + o);
-    }
+    const PpShared sh = pp_shared_carve(pp_smem, n, M, mmax);
     const PpScratch sc = pp_scratch_carve(run.pp_scratch + run.pp_scratch_stride * blockIdx.x, n, mmax);
     const int npend = *run.n_pp;
     const int G = run.S / kGroup;
@@ -580,40 +664,11 @@ static __global__ void __launch_bounds__(kPpThreads) k_postprocess(DevCode code,
         for (int r = threadIdx.x; r < M; r += blockDim.x)
             sh.tgt[r] = static_cast<uint8_t>((run.synm[static_cast<size_t>(r) * G + group] >> b) & 1u);
         __syncthreads();
-        // ETS, both sides (X corrections flip x-bits, Z corrections z-bits)
-        const int gx = blk_ets_multi(code, run, sh, 0);
-        const int gz = blk_ets_multi(code, run, sh, 1);
-        const bool ets_used = gx >= 0 || gz >= 0;
-        const bool e6 = (gx >= 0 && run.ets.size[gx] == 6) || (gz >= 0 && run.ets.size[gz] == 6);
-        const bool e12 = (gx >= 0 && run.ets.size[gx] == 12) || (gz >= 0 && run.ets.size[gz] == 12);
-        bool ok = false, ets_ok = false, flip_ok = false, osd_ok = false;
-        if (ets_used) {
-            ok = blk_side_diff(code, sh, 0) == 0;
-            ok = (blk_side_diff(code, sh, 1) == 0) && ok;
-            ets_ok = ok;
-        }
-        if (!ok) {
-            const bool fx = blk_flip_side(code, run, sh, sc, 0, slot, k);
-            const bool fz = blk_flip_side(code, run, sh, sc, 1, slot, k);
-            if (fx || fz) {
-                ok = blk_side_diff(code, sh, 0) == 0;
-                ok = (blk_side_diff(code, sh, 1) == 0) && ok;
-                flip_ok = ok;
-            }
-        }
-        if (!ok) {
-            const int ux = blk_side_diff(code, sh, 0), uz = blk_side_diff(code, sh, 1);
-            if ((ux > uz ? ux : uz) <= 20) {
-                const bool ox = blk_osd_side(code, run, sh, sc, 0, slot);
-                const bool oz = blk_osd_side(code, run, sh, sc, 1, slot);
-                if (ox || oz) {
-                    ok = blk_side_diff(code, sh, 0) == 0;
-                    ok = (blk_side_diff(code, sh, 1) == 0) && ok;
-                    osd_ok = ok;
-                }
-            }
-        }
-        const bool in_loop_success = mode == kPpInLoop && ok;
+        const SlotHistory hist{&run, slot, k};
+        const double *llr = run.llr + static_cast<size_t>(slot) * n;
+        const PpOutcome o = blk_pp_stages(code, run.ets, hist, run.flip_hist, run.act_k[slot], k, llr,
+                                          llr + static_cast<size_t>(run.S) * n, sh, sc);
+        const bool in_loop_success = mode == kPpInLoop && o.ok;
         const bool post = !in_loop_success && (mode == kPpPost || k >= run.max_iter);
         if (in_loop_success || post) {
             // write the corrected decisions back into the slot's bits of the current planes
@@ -626,21 +681,13 @@ static __global__ void __launch_bounds__(kPpThreads) k_postprocess(DevCode code,
             }
         }
         if (threadIdx.x == 0) {
-            int rf = run.res_flags[slot];
+            if (in_loop_success || post) run.res_flags[slot] = pp_result_flags(o, in_loop_success);
             if (in_loop_success) {
-                rf = kResSyndromeOk | kResPpInDecode | (ets_ok ? kResPpInEts : 0) | (flip_ok ? kResPpInFlip : 0) |
-                     (ets_used ? kResUsedAny : 0) | (e6 ? kResUsed6 : 0) | (e12 ? kResUsed12 : 0);
-                run.res_flags[slot] = rf;
                 run.res_iters[slot] = k;
                 if (k < run.max_iter) {
                     run.flags[slot] = kFinished;
                     run.retired[atomicAdd(run.n_retired, 1)] = slot;
                 }
-            } else if (post) {
-                rf = kResPostEntered | (ok ? kResSyndromeOk : 0) | (ets_used ? kResEtsPost : 0) | (e6 ? kResUsed6 : 0) |
-                     (e12 ? kResUsed12 : 0) | (ets_ok ? kResEtsOk : 0) | (flip_ok ? kResFlipOk : 0) |
-                     (osd_ok ? kResOsdOk : 0);
-                run.res_flags[slot] = rf;
             }
         }
         __syncthreads();

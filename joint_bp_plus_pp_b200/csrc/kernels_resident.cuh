@@ -41,6 +41,7 @@
 
 #include "engine.cuh"
 #include "kernels_slots.cuh"
+#include "kernels_pp.cuh"
 
 namespace jbp {
 
@@ -74,7 +75,19 @@ struct ResRun {
     jbp_trial_result *res_out;
     unsigned long long *hist;
     DevCounters *cnt;
+    // post-processing (PP instantiations only)
+    int flip_hist;
+    DevCode dc;                    // table form of the code for the post-processing stages
+    DevEts ets;
+    unsigned char *pp_scratch;     // per block: PpScratch | decision ring [R][n] | |LLR| [2][n] doubles
+    size_t pp_scratch_stride;
 };
+
+// Per-block global scratch of a post-processing run: the GF(2) work areas, the ring of the
+// last R iterations' decisions and the |LLR| keys of the OSD order.
+__host__ __device__ inline size_t res_pp_scratch_bytes(int n, int mmax, int R) {
+    return pp_align(pp_scratch_bytes(n, mmax)) + pp_align(static_cast<size_t>(R) * n) + pp_align(16ull * n);
+}
 
 __device__ __forceinline__ unsigned res_mod(unsigned x, unsigned P, unsigned magic) {
     const unsigned q = __umulhi(x, magic);
@@ -116,12 +129,13 @@ __device__ __forceinline__ float with_bit(float a, unsigned b) {
 }
 
 // Shared-memory bytes of the resident kernel for a code.
-__host__ __device__ inline size_t res_smem_bytes(int n, int m, int L, size_t store_bytes) {
+__host__ __device__ inline size_t res_smem_bytes(int n, int m, int L, size_t store_bytes, bool pp) {
     const size_t c2v = (2ull * L * m * store_bytes + 15) / 16 * 16;
     const size_t A = 2ull * n * 4;
     const size_t err = (static_cast<size_t>(n) + 15) / 16 * 16;
     const size_t syn = (2ull * ((m + 31) / 32) + 3) / 4 * 4 * 4;
-    return c2v + A + err + syn + 64;
+    const size_t base = c2v + A + err + syn + 64;
+    return pp ? pp_align(base) + pp_smem_bytes(n, 2 * m, m) + 256 : base;
 }
 
 
@@ -184,17 +198,53 @@ __device__ __forceinline__ bool res_check_row(const ResCode &code, typename ST::
     return bad;
 }
 
+// Returns this thread's number of tested checks that failed.
 template <int P, int J, int L, class ST, int SIDE>
-__device__ __forceinline__ bool res_check_side(const ResCode &code, typename ST::T *c2v, const float *A,
-                                               const unsigned *syn, bool test) {
-    bool bad = false;
+__device__ __forceinline__ int res_check_side(const ResCode &code, typename ST::T *c2v, const float *A,
+                                              const unsigned *syn, bool test) {
+    int bad = 0;
     for (int x = threadIdx.x; x < P; x += blockDim.x) {
-        bad |= res_check_row<P, J, L, ST, SIDE, 0>(code, c2v, A, syn, x, test);
-        if (J > 1) bad |= res_check_row<P, J, L, ST, SIDE, (J > 1 ? 1 : 0)>(code, c2v, A, syn, x, test);
-        if (J > 2) bad |= res_check_row<P, J, L, ST, SIDE, (J > 2 ? 2 : 0)>(code, c2v, A, syn, x, test);
-        if (J > 3) bad |= res_check_row<P, J, L, ST, SIDE, (J > 3 ? 3 : 0)>(code, c2v, A, syn, x, test);
+        bad += res_check_row<P, J, L, ST, SIDE, 0>(code, c2v, A, syn, x, test);
+        if (J > 1) bad += res_check_row<P, J, L, ST, SIDE, (J > 1 ? 1 : 0)>(code, c2v, A, syn, x, test);
+        if (J > 2) bad += res_check_row<P, J, L, ST, SIDE, (J > 2 ? 2 : 0)>(code, c2v, A, syn, x, test);
+        if (J > 3) bad += res_check_row<P, J, L, ST, SIDE, (J > 3 ? 3 : 0)>(code, c2v, A, syn, x, test);
     }
     return bad;
+}
+
+// Syndrome test of the decisions in A's low bits: this thread's failing checks of one side.
+template <int P, int J, int L>
+__device__ __forceinline__ int res_test_side(const ResCode &code, const float *A_all, const unsigned *syn_all,
+                                             int side) {
+    constexpr int m = J * P, n = L * P, mw = (m + 31) / 32;
+    int bad = 0;
+    for (int c = threadIdx.x; c < m; c += blockDim.x) {
+        const int j = c / P, x = c - j * P;
+        unsigned par = 0;
+#pragma unroll
+        for (int l = 0; l < L; ++l) {
+            const unsigned y = (static_cast<unsigned>(code.fa[side][j][l]) * static_cast<unsigned>(x) +
+                                code.fb[side][j][l]) % static_cast<unsigned>(P);
+            par ^= __float_as_uint(A_all[side * n + l * P + y]);
+        }
+        bad += (par & 1u) != ((syn_all[side * mw + (c >> 5)] >> (c & 31)) & 1u);
+    }
+    return bad;
+}
+
+// Block sums of two per-thread counts through cnt[0..1] (zero on entry; left zero on return).
+__device__ __forceinline__ int2 res_block_sum2(int a, int b, int *cnt) {
+    a = __reduce_add_sync(0xffffffffu, a);
+    b = __reduce_add_sync(0xffffffffu, b);
+    if ((threadIdx.x & 31) == 0) {
+        if (a) atomicAdd(&cnt[0], a);
+        if (b) atomicAdd(&cnt[1], b);
+    }
+    __syncthreads();
+    const int2 r = make_int2(cnt[0], cnt[1]);
+    __syncthreads();
+    if (threadIdx.x == 0) { cnt[0] = 0; cnt[1] = 0; }
+    return r;
 }
 
 // log2((c0 + c1 2^-s) / (c2 + c3 2^-s)) for any sign of s, with one ex2 and two lg2:
@@ -258,7 +308,29 @@ __device__ __forceinline__ bool res_in_row_space(uint64_t *vec, int words, const
     return r;
 }
 
+// |LLR| of the x and z bits of every variable from the current c2v (the slot engine's FP32
+// keys, base 2), as doubles for the OSD column order.
 template <int P, int J, int L, class ST>
+__device__ void res_abs_llr(const ResCode &code, const typename ST::T *c2v, const float4 lp, double *llr) {
+    constexpr int m = J * P, n = L * P;
+    for (int v = threadIdx.x; v < n; v += blockDim.x) {
+        const int l = v / P, y = v - l * P;
+        float Lam = 0.0f, Mu = 0.0f;
+        for (int j = 0; j < J; ++j) {
+            const unsigned xx = (static_cast<unsigned>(code.ia[0][j][l]) * static_cast<unsigned>(y) + code.ib[0][j][l]) %
+                                static_cast<unsigned>(P);
+            const unsigned xz = (static_cast<unsigned>(code.ia[1][j][l]) * static_cast<unsigned>(y) + code.ib[1][j][l]) %
+                                static_cast<unsigned>(P);
+            Lam += ST::ld(c2v + l * m + j * P + xx);
+            Mu += ST::ld(c2v + (L + l) * m + j * P + xz);
+        }
+        const float w0 = lp.x, w1 = lp.y - Lam, w2 = lp.z - Mu, w3 = lp.w - Lam - Mu;
+        llr[v] = fabsf(res_lse2(w1, w3) - res_lse2(w0, w2));
+        llr[n + v] = fabsf(res_lse2(w2, w3) - res_lse2(w0, w1));
+    }
+}
+
+template <int P, int J, int L, class ST, bool PP>
 __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRun run) {
     extern __shared__ __align__(16) unsigned char res_smem[];
     using T = typename ST::T;
@@ -268,11 +340,30 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
     float *const A = reinterpret_cast<float *>(res_smem + c2v_bytes);
     uint8_t *const err = res_smem + c2v_bytes + 2ull * n * 4;
     unsigned *const syn = reinterpret_cast<unsigned *>(err + (n + 15) / 16 * 16);
-    int *const ints = reinterpret_cast<int *>(syn + (2 * mw + 3) / 4 * 4);
+    int *const ints = reinterpret_cast<int *>(syn + (2 * mw + 3) / 4 * 4);   // 16 ints
     __shared__ long long trial_sh;
     __shared__ float4 lp_sh, pr_sh;
     __shared__ float lpx_sh, lpz_sh;
+    __shared__ unsigned short us_hist[100];
+    __shared__ int pp_sh[4];   // mode, act_k, pstate
     const bool have_err = run.source != kSrcSyndromes;
+
+    // post-processing state (PP instantiations)
+    PpShared psh{};
+    PpScratch psc{};
+    uint8_t *ring = nullptr;
+    double *llr = nullptr;
+    const int R = PP ? max(run.flip_hist + 1, 3) : 1;
+    const int llr_from = min(100, run.max_iter);
+    const int slow_from = PP ? max(1, llr_from - 2) : 0x7fffffff;
+    if (PP) {
+        const size_t base = pp_align(c2v_bytes + 2ull * n * 4 + (n + 15) / 16 * 16 + (2 * mw + 3) / 4 * 4 * 4 + 64);
+        psh = pp_shared_carve(res_smem + base, n, 2 * m, m);
+        unsigned char *g = run.pp_scratch + run.pp_scratch_stride * blockIdx.x;
+        psc = pp_scratch_carve(g, n, m);
+        ring = g + pp_align(pp_scratch_bytes(n, m));
+        llr = reinterpret_cast<double *>(ring + pp_align(static_cast<size_t>(R) * n));
+    }
 
     // prior: FP64 as the slot engine's refill, then its log2 weights and probabilities in FP32
     if (threadIdx.x == 0) {
@@ -291,6 +382,7 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
                             static_cast<float>(q[3]));
         lpx_sh = static_cast<float>(log2((q[0] + q[2]) / (q[1] + q[3])));
         lpz_sh = static_cast<float>(log2((q[0] + q[1]) / (q[2] + q[3])));
+        for (int i = 0; i < 16; ++i) ints[i] = 0;
     }
     __syncthreads();
     const float4 lp = lp_sh, pr = pr_sh;
@@ -300,6 +392,8 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
         if (threadIdx.x == 0) {
             const unsigned long long k = atomicAdd(&run.cnt->next_trial, 1ull);
             trial_sh = k < static_cast<unsigned long long>(run.ntrials) ? static_cast<long long>(k) : -1;
+            pp_sh[1] = 0;   // act_k
+            pp_sh[2] = 0;   // pstate
         }
         __syncthreads();
         const long long k = trial_sh;
@@ -318,7 +412,25 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
             }
         } else if (run.source == kSrcErrors) {
             const uint8_t *src = run.src_err + local * n;
-            for (int v = threadIdx.x; v < n; v += blockDim.x) err[v] = src[v];
+            if ((n & 15) == 0 && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+                // 16-byte loads; a byte above 3 is reported and masked
+                const uint4 *s16 = reinterpret_cast<const uint4 *>(src);
+                uint4 *d16 = reinterpret_cast<uint4 *>(err);
+                unsigned badw = 0u;
+                for (int i = threadIdx.x; i < n / 16; i += blockDim.x) {
+                    uint4 w = s16[i];
+                    badw |= (w.x | w.y | w.z | w.w) & 0xFCFCFCFCu;
+                    w.x &= 0x03030303u; w.y &= 0x03030303u; w.z &= 0x03030303u; w.w &= 0x03030303u;
+                    d16[i] = w;
+                }
+                if (badw) atomicAdd(&run.cnt->bad_input, 1ull);
+            } else {
+                for (int v = threadIdx.x; v < n; v += blockDim.x) {
+                    const uint8_t e = src[v];
+                    if (e > 3) atomicAdd(&run.cnt->bad_input, 1ull);
+                    err[v] = e & 3;
+                }
+            }
         } else if (run.source == kSrcMt19937) {
             if (threadIdx.x < 32) warp_mt_trial(reinterpret_cast<unsigned long long *>(A), run.seed, t, run.p, n, err);
         }
@@ -351,38 +463,97 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
         }
         __syncthreads();
 
-        // ---- BP iterations (it = completed iterations); the check phase of iteration it+1
-        // also tests the decisions of iteration it
-        int it = 0;
-        bool ok = false;
+        // ---- BP iterations (it = completed iterations).  Until slow_from the check phase of
+        // iteration it+1 also tests the decisions of iteration it; from slow_from on (only with
+        // post-processing) each iteration is tested after its variable phase and feeds the stall
+        // triggers, the flip window and the post-processing attempts (jointbp_ets.cpp:2521-2633).
+        int it = 0, rf = 0, iters = run.max_iter;
         for (;;) {
-            const bool test = it >= 1 && (it >= run.max_iter ||
-                                          (it > run.check_warmup && (it - run.check_warmup) % run.check_interval == 0));
-            bool bad = false;
+            const bool fused = it >= 1 && it < slow_from &&
+                               (it >= run.max_iter ||
+                                (it > run.check_warmup && (it - run.check_warmup) % run.check_interval == 0));
+            int bx = 0, bz = 0;
             if (it < run.max_iter) {
-                bad = res_check_side<P, J, L, ST, 0>(code, c2v, A, syn, test);
-                bad |= res_check_side<P, J, L, ST, 1>(code, c2v, A, syn, test);
-            } else {
-                for (int r = threadIdx.x; r < 2 * m; r += blockDim.x) {
-                    const int side = r >= m, c = r - side * m, j = c / P, x = c - j * P;
-                    unsigned par = 0;
-#pragma unroll
-                    for (int l = 0; l < L; ++l) {
-                        const unsigned y = (static_cast<unsigned>(code.fa[side][j][l]) * static_cast<unsigned>(x) +
-                                            code.fb[side][j][l]) % static_cast<unsigned>(P);
-                        par ^= __float_as_uint(A[side * n + l * P + y]);
-                    }
-                    bad |= (par & 1u) != ((syn[side * mw + (c >> 5)] >> (c & 31)) & 1u);
-                }
+                bx = res_check_side<P, J, L, ST, 0>(code, c2v, A, syn, fused);
+                bz = res_check_side<P, J, L, ST, 1>(code, c2v, A, syn, fused);
+            } else if (fused) {
+                bx = res_test_side<P, J, L>(code, A, syn, 0);
+                bz = res_test_side<P, J, L>(code, A, syn, 1);
             }
-            bad = __syncthreads_or(bad);
-            if (test && !bad) { ok = true; break; }
+            int2 u = make_int2(0, 0);
+            if (PP) u = res_block_sum2(bx, bz, ints);
+            else u.x = __syncthreads_or(bx + bz);
+            if (fused) {
+                if (u.x + u.y == 0) { rf = kResSyndromeOk | kResBpOk; iters = it; break; }
+                if (PP && threadIdx.x == 0) us_hist[it % 100] = static_cast<unsigned short>(min(max(u.x, u.y), 65535));
+            }
             if (it >= run.max_iter) break;
             for (int y = threadIdx.x; y < P; y += blockDim.x) res_var_cols<P, J, L, ST, 0>(code, c2v, A, y, lp, pr);
             __syncthreads();
             ++it;
+            if (PP && it >= slow_from) {
+                const int2 us = res_block_sum2(res_test_side<P, J, L>(code, A, syn, 0),
+                                               res_test_side<P, J, L>(code, A, syn, 1), ints);
+                if (us.x + us.y == 0) { rf = kResSyndromeOk | kResBpOk; iters = it; break; }
+                uint8_t *cur = ring + static_cast<size_t>(it % R) * n;
+                for (int v = threadIdx.x; v < n; v += blockDim.x)
+                    cur[v] = static_cast<uint8_t>((__float_as_uint(A[v]) & 1u) | ((__float_as_uint(A[n + v]) & 1u) << 1));
+                __syncthreads();
+                // est == prev_est / prev_prev_est (jointbp_ets.cpp:2555-2556)
+                const uint8_t *p1 = ring + static_cast<size_t>((it - 1) % R) * n;
+                const uint8_t *p2 = ring + static_cast<size_t>((it - 2 + R) % R) * n;
+                bool s1 = it >= 2, s2 = it >= 3;
+                for (int v = threadIdx.x; v < n; v += blockDim.x) {
+                    if (s1) s1 = cur[v] == p1[v];
+                    if (s2) s2 = cur[v] == p2[v];
+                }
+                const bool same = __syncthreads_and(s1) != 0;
+                const bool pp2 = __syncthreads_and(s2) != 0;
+                if (threadIdx.x == 0) {
+                    const int sig = max(us.x, us.y);
+                    us_hist[it % 100] = static_cast<unsigned short>(min(sig, 65535));
+                    const bool osc = pp2 && !same;
+                    const bool allow = it >= 100 || it == run.max_iter;
+                    int st = pp_sh[2];
+                    bool act = false;
+                    if (!(st & 1) && (same || it == run.max_iter) && allow) { st |= 1; act = true; }
+                    if (!(st & 2) && osc && allow) { st |= 2; act = true; }
+                    if (!(st & 4) && allow && us_oscillation(us_hist, it)) { st |= 4; act = true; }
+                    pp_sh[2] = st;
+                    if (act && pp_sh[1] == 0 && run.flip_hist > 0) pp_sh[1] = it;
+                    pp_sh[0] = (st && sig <= 20) ? kPpInLoop : (it >= run.max_iter ? kPpPost : 0);
+                }
+                __syncthreads();
+                const int mode = pp_sh[0];
+                if (mode) {
+                    for (int v = threadIdx.x; v < n; v += blockDim.x) psh.est[v] = cur[v];
+                    for (int r = threadIdx.x; r < 2 * m; r += blockDim.x) {
+                        const int side = r >= m, c = r - side * m;
+                        psh.tgt[r] = static_cast<uint8_t>((syn[side * mw + (c >> 5)] >> (c & 31)) & 1u);
+                    }
+                    res_abs_llr<P, J, L, ST>(code, c2v, lp, llr);
+                    __syncthreads();
+                    const RingHistory hist{ring, R};
+                    const PpOutcome o = blk_pp_stages(run.dc, run.ets, hist, run.flip_hist, pp_sh[1], it, llr, llr + n,
+                                                      psh, psc);
+                    const bool in_loop_success = mode == kPpInLoop && o.ok;
+                    const bool post = !in_loop_success && (mode == kPpPost || it >= run.max_iter);
+                    if (in_loop_success || post) {
+                        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+                            A[v] = with_bit(A[v], psh.est[v] & 1u);
+                            A[n + v] = with_bit(A[n + v], (psh.est[v] >> 1) & 1u);
+                        }
+                        rf = pp_result_flags(o, in_loop_success);
+                        iters = it;
+                        __syncthreads();
+                        break;
+                    }
+                    __syncthreads();
+                }
+                if (it >= run.max_iter) { iters = it; break; }
+            }
         }
-        const int iters = ok ? it : run.max_iter;
+        const bool ok = (rf & kResSyndromeOk) != 0;
 
         // ---- classification (jointbp_ets.cpp:6199-6245): exact, stabilizer-equivalent residual
         const int words = (n + 63) / 64, w32 = 2 * words;
@@ -398,43 +569,24 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
             const unsigned tv = in && have_err ? err[v] : e;
             if (in && run.est_out) run.est_out[local * n + v] = static_cast<uint8_t>(e);
             exact &= tv == e;
-            const unsigned bx = __ballot_sync(0xffffffffu, ((tv ^ e) & 1u) != 0);
-            const unsigned bz = __ballot_sync(0xffffffffu, ((tv ^ e) & 2u) != 0);
-            if ((threadIdx.x & 31) == 0) { rx[base >> 5] = bx; rz[base >> 5] = bz; }
+            const unsigned bxm = __ballot_sync(0xffffffffu, ((tv ^ e) & 1u) != 0);
+            const unsigned bzm = __ballot_sync(0xffffffffu, ((tv ^ e) & 2u) != 0);
+            if ((threadIdx.x & 31) == 0) { rx[base >> 5] = bxm; rz[base >> 5] = bzm; }
         }
         exact = __syncthreads_and(exact) && have_err;
         bool stab = false;
         if (have_err && ok && !exact) {
-            stab = res_in_row_space(reinterpret_cast<uint64_t *>(rx), words, code.basis_rows[1], code.pivot_row[1], ints);
+            stab = res_in_row_space(reinterpret_cast<uint64_t *>(rx), words, code.basis_rows[1], code.pivot_row[1],
+                                    ints + 8);
             if (stab)
                 stab = res_in_row_space(reinterpret_cast<uint64_t *>(rz), words, code.basis_rows[0], code.pivot_row[0],
-                                        ints);
+                                        ints + 8);
         } else if (have_err && ok) {
             stab = true;   // exact: the residual is zero
         }
         const bool success = have_err ? (ok && stab) : ok;
-        if (threadIdx.x == 0) {
-            DevCounters *cn = run.cnt;
-            atomicAdd(&cn->done, 1ull);
-            atomicAdd(&cn->total_iters, static_cast<unsigned long long>(iters));
-            atomicAdd(&cn->bp_trial_iterations, static_cast<unsigned long long>(iters));
-            if (!success) atomicAdd(&cn->failures, 1ull);
-            if (!ok) atomicAdd(&cn->bp_fail, 1ull);
-            if (exact) atomicAdd(&cn->exact, 1ull);
-            if (ok) atomicAdd(&cn->syndrome_ok, 1ull);
-            if (success && !exact && stab) atomicAdd(&cn->stab_success, 1ull);
-            if (run.hist && iters >= 1 && iters <= run.max_iter) atomicAdd(&run.hist[iters], 1ull);
-            if (run.res_out) {
-                jbp_trial_result rec{};
-                rec.iterations = iters;
-                rec.syndrome_ok = ok;
-                rec.bp_ok = ok;
-                rec.success = success;
-                rec.exact = exact;
-                rec.stab_equiv = stab;
-                run.res_out[local] = rec;
-            }
-        }
+        if (threadIdx.x == 0)
+            account_trial(run.cnt, run.hist, run.res_out, run.max_iter, local, iters, rf, ok, success, exact, stab);
         __syncthreads();
     }
 }

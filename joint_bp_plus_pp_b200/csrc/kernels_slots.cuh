@@ -277,6 +277,67 @@ static __device__ bool warp_in_row_space(uint64_t *vec, int words, const uint64_
     return false;
 }
 
+// Run Summary counters exactly as the simulate loop derives them (jointbp_ets.cpp:6012-6019,
+// 6070-6080, 6199-6224), the iteration histogram and the per-trial record, from a trial's
+// iterations, result flags (ResultBit) and classification.  One thread per trial.
+__device__ __forceinline__ void account_trial(DevCounters *c, unsigned long long *hist, jbp_trial_result *res_out,
+                                              int max_iter, long long local, int iters, int rf, bool ok, bool success,
+                                              bool exact, bool stab) {
+    const bool in_dec = rf & kResPpInDecode;
+    const bool used_any = rf & kResUsedAny, used6 = rf & kResUsed6, used12 = rf & kResUsed12;
+    const bool post = rf & kResPostEntered;
+    const bool ets_ok = in_dec ? (rf & kResPpInEts) : (rf & kResEtsOk);
+    const bool flip_ok = in_dec ? (rf & kResPpInFlip) : (rf & kResFlipOk);
+    const bool osd_ok = rf & kResOsdOk;
+    const bool osd_success = osd_ok || (in_dec && !(rf & kResPpInEts) && !(rf & kResPpInFlip));
+    const bool pp_this = success && (in_dec || ets_ok || flip_ok || osd_ok);
+    atomicAdd(&c->done, 1ull);
+    atomicAdd(&c->total_iters, static_cast<unsigned long long>(iters));
+    atomicAdd(&c->bp_trial_iterations, static_cast<unsigned long long>(iters));
+    if (!success) atomicAdd(&c->failures, 1ull);
+    if (!(rf & kResBpOk)) atomicAdd(&c->bp_fail, 1ull);
+    if (exact) atomicAdd(&c->exact, 1ull);
+    if (ok) atomicAdd(&c->syndrome_ok, 1ull);
+    if (success && !exact && stab) atomicAdd(&c->stab_success, 1ull);
+    if (in_dec && used_any) {
+        atomicAdd(&c->ets_used, 1ull);
+        if (used6) atomicAdd(&c->ets6_used, 1ull);
+        if (used12) atomicAdd(&c->ets12_used, 1ull);
+    }
+    if (post) {
+        if (rf & kResEtsPost) atomicAdd(&c->ets_used, 1ull);
+        if (used6) atomicAdd(&c->ets6_used, 1ull);
+        if (used12) atomicAdd(&c->ets12_used, 1ull);
+    }
+    if (success && ets_ok) {
+        atomicAdd(&c->ets_saved, 1ull);
+        if (used6) atomicAdd(&c->ets6_saved, 1ull);
+        if (used12) atomicAdd(&c->ets12_saved, 1ull);
+    }
+    if (success && flip_ok) atomicAdd(&c->flip_pp_success, 1ull);
+    if (pp_this) atomicAdd(&c->pp_success, 1ull);
+    if (success && osd_success) atomicAdd(&c->osd_pp_success, 1ull);
+    if (hist && iters >= 1 && iters <= max_iter) atomicAdd(&hist[iters], 1ull);
+    if (res_out) {
+        jbp_trial_result rec;
+        rec.iterations = iters;
+        rec.syndrome_ok = ok;
+        rec.bp_ok = (rf & kResBpOk) ? 1 : 0;
+        rec.success = success;
+        rec.exact = exact;
+        rec.stab_equiv = stab;
+        rec.pp_success = pp_this;
+        rec.pp_ets = ets_ok;
+        rec.pp_flip = flip_ok;
+        rec.pp_osd = osd_success;
+        rec.ets_used_flags = static_cast<uint8_t>((used_any ? 1 : 0) | (used6 ? 2 : 0) | (used12 ? 4 : 0) |
+                                                  ((rf & kResEtsPost) ? 8 : 0) | (post ? 16 : 0));
+        rec.pp_in_decode = in_dec;
+        rec.reserved = osd_ok;
+        res_out[local] = rec;
+    }
+}
+
 // Classifies each retired trial (jointbp_ets.cpp:6199-6245): exact match, stabilizer
 // equivalence of the residual (x-part in rowspace(Hz), z-part in rowspace(Hx)), success;
 // writes the per-trial record and estimate and updates the run counters.
@@ -343,62 +404,7 @@ static __global__ void k_classify(DevCode code, DevRun run) {
         }
         const bool success = have_err ? (ok && stab) : ok;
         if (lane == 0) {
-            // Run Summary counters exactly as the simulate loop derives them
-            // (jointbp_ets.cpp:6012-6019, 6070-6080, 6199-6224)
-            const bool in_dec = rf & kResPpInDecode;
-            const bool used_any = rf & kResUsedAny, used6 = rf & kResUsed6, used12 = rf & kResUsed12;
-            const bool post = rf & kResPostEntered;
-            const bool ets_ok = in_dec ? (rf & kResPpInEts) : (rf & kResEtsOk);
-            const bool flip_ok = in_dec ? (rf & kResPpInFlip) : (rf & kResFlipOk);
-            const bool osd_ok = rf & kResOsdOk;
-            const bool osd_success = osd_ok || (in_dec && !(rf & kResPpInEts) && !(rf & kResPpInFlip));
-            const bool pp_this = success && (in_dec || ets_ok || flip_ok || osd_ok);
-            DevCounters *c = run.cnt;
-            atomicAdd(&c->done, 1ull);
-            atomicAdd(&c->total_iters, static_cast<unsigned long long>(iters));
-            atomicAdd(&c->bp_trial_iterations, static_cast<unsigned long long>(iters));
-            if (!success) atomicAdd(&c->failures, 1ull);
-            if (!(rf & kResBpOk)) atomicAdd(&c->bp_fail, 1ull);
-            if (exact) atomicAdd(&c->exact, 1ull);
-            if (ok) atomicAdd(&c->syndrome_ok, 1ull);
-            if (success && !exact && stab) atomicAdd(&c->stab_success, 1ull);
-            if (in_dec && used_any) {
-                atomicAdd(&c->ets_used, 1ull);
-                if (used6) atomicAdd(&c->ets6_used, 1ull);
-                if (used12) atomicAdd(&c->ets12_used, 1ull);
-            }
-            if (post) {
-                if (rf & kResEtsPost) atomicAdd(&c->ets_used, 1ull);
-                if (used6) atomicAdd(&c->ets6_used, 1ull);
-                if (used12) atomicAdd(&c->ets12_used, 1ull);
-            }
-            if (success && ets_ok) {
-                atomicAdd(&c->ets_saved, 1ull);
-                if (used6) atomicAdd(&c->ets6_saved, 1ull);
-                if (used12) atomicAdd(&c->ets12_saved, 1ull);
-            }
-            if (success && flip_ok) atomicAdd(&c->flip_pp_success, 1ull);
-            if (pp_this) atomicAdd(&c->pp_success, 1ull);
-            if (success && osd_success) atomicAdd(&c->osd_pp_success, 1ull);
-            if (run.hist && iters >= 1 && iters <= run.max_iter) atomicAdd(&run.hist[iters], 1ull);
-            if (run.res_out) {
-                jbp_trial_result rec;
-                rec.iterations = iters;
-                rec.syndrome_ok = ok;
-                rec.bp_ok = (rf & kResBpOk) ? 1 : 0;
-                rec.success = success;
-                rec.exact = exact;
-                rec.stab_equiv = stab;
-                rec.pp_success = pp_this;
-                rec.pp_ets = ets_ok;
-                rec.pp_flip = flip_ok;
-                rec.pp_osd = osd_success;
-                rec.ets_used_flags = static_cast<uint8_t>((used_any ? 1 : 0) | (used6 ? 2 : 0) | (used12 ? 4 : 0) |
-                                                          ((rf & kResEtsPost) ? 8 : 0) | (post ? 16 : 0));
-                rec.pp_in_decode = in_dec;
-                rec.reserved = osd_ok;
-                run.res_out[local] = rec;
-            }
+            account_trial(run.cnt, run.hist, run.res_out, run.max_iter, local, iters, rf, ok, success, exact, stab);
             run.flags[slot] = 0;
         }
         __syncwarp();
@@ -466,7 +472,10 @@ static __global__ void k_sample(DevCode code, DevRun run) {
         const long long t = run.trial[slot];
         uint8_t e = 0;
         if (run.source == kSrcPhilox) e = sample_philox(run.seed, t, v, run.p);
-        else if (run.source == kSrcErrors) e = run.src_err[(t - run.first_trial) * n + v];
+        else if (run.source == kSrcErrors) {
+            e = run.src_err[(t - run.first_trial) * n + v];
+            if (e > 3) { atomicAdd(&run.cnt->bad_input, 1ull); e &= 3; }
+        }
         run.err[static_cast<size_t>(slot) * n + v] = e;
     }
 }

@@ -107,3 +107,63 @@ def test_resident_refuses_what_it_does_not_run(decoder):
         with pytest.raises(JbpError) as e:
             decoder.simulate(1, 4, 0.05, ropts(max_iter=10, **bad))
         assert e.value.code == 4
+
+
+# ---------------------------------------------------------------- post-processing in the resident kernel
+
+def test_resident_pp_stage_trials(decoder, oracle):
+    """Errors that make each post-processing stage act (constructed trapping-set errors and
+    sampled trials), decoded with the stages inside the resident kernel: its flags agree with
+    the oracle's classification of its own estimates, and its outcomes agree with the
+    reference's FP64 records on nearly every case (the BP before the stages is FP32)."""
+    from test_gpu_pp import gpu_record, golden_record, load_stage_trials
+    total = same_est = same_rec = 0
+    for (p, mi, fh), cases in sorted(load_stage_trials(decoder.n).items()):
+        errs = np.stack([c[1] for c in cases])
+        st, res, est = decoder.decode_errors(errs, p, ropts(max_iter=mi, flip_hist=fh, enable_pp=True))
+        for (label, err, est_ref, rec), r, e in zip(cases, res, est):
+            ok, exact, stab, success = oracle.classify(err, e)
+            assert (r["syndrome_ok"], r["exact"], r["success"]) == (ok, exact, success), (label, mi)
+            total += 1
+            same_est += bool((e == est_ref).all())
+            same_rec += gpu_record(r) == golden_record(rec)
+    assert same_est >= 0.85 * total, (same_est, total)
+    assert same_rec >= 0.8 * total, (same_rec, total)
+
+
+@pytest.mark.parametrize("name", ["p050_mi200_pp_s305", "p060_mi120_pp_s7"])
+def test_resident_pp_ler_close_to_fp64(decoder, name):
+    from conftest import load_sim_case
+    from test_gpu_pp import opts_for
+    meta, errs, _ = load_sim_case(name)
+    st64, r64, _ = decoder.decode_errors(errs, meta["p"], opts_for(meta), want_est=False)
+    st, r, _ = decoder.decode_errors(errs, meta["p"], ropts(max_iter=meta["max_iter"], flip_hist=meta["flip_hist"],
+                                                            enable_pp=True), want_est=False)
+    assert st["trials"] == len(errs) and st["kernel_launches"] == 1
+    assert abs(st["failures"] - st64["failures"]) <= max(3, len(errs) // 4)
+    assert (r["success"] != r64["success"]).mean() <= 0.1
+
+
+def test_resident_pp_saves_trials(decoder):
+    """At p=0.06 with max-iter 120 many trials stall; the in-kernel stages save some of them
+    and the Run Summary counters stay consistent with the per-trial records."""
+    st, res = decoder.simulate(7, 600, 0.06, ropts(max_iter=120, enable_pp=True))
+    assert st["pp_success"] > 0
+    assert st["pp_success"] == int(res["pp_success"].sum())
+    assert st["failures"] == int((res["success"] == 0).sum())
+    assert st["bp_fail"] == int((res["bp_ok"] == 0).sum())
+    assert st["flip_pp_success"] == int((res["pp_flip"] & res["success"]).sum())
+
+
+@pytest.mark.parametrize("engine,prec", [("resident", "fp16"), ("slots", "fp32"), ("slots", "fp64")])
+def test_invalid_error_values_are_rejected(decoder, engine, prec):
+    """Error bytes outside 0..3 are found on the device while the errors are read."""
+    from joint_bp_plus_pp_b200 import JbpError, Options
+    err = np.zeros((3, decoder.n), np.uint8)
+    err[1, 4000] = 7
+    with pytest.raises(JbpError) as e:
+        decoder.decode_errors(err, 0.05, Options(precision=prec, engine=engine, max_iter=5, enable_pp=False))
+    assert e.value.code == 1 and "invalid value" in str(e.value)
+    st, res, _ = decoder.decode_errors(err[[0, 2]], 0.05, Options(precision=prec, engine=engine, max_iter=5,
+                                                                  enable_pp=False))
+    assert st["trials"] == 2 and res["success"].all()
