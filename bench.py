@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument("--e2e-batch", type=int, default=65536, help="trials per end-to-end step (0 = skip)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--slots", type=int, default=0)
+    ap.add_argument("--learned-from", type=int, default=6,
+                    help="stalled trials try the shipped learned flip proposal from this iteration (0 = off)")
     return ap.parse_args()
 
 
@@ -196,8 +198,10 @@ def run_reference(args, rank, world):
     return 0
 
 
-def workload_name(args, decoder):
+def workload_name(args, decoder, learned_from=0):
     pp = f"BP+PP (ETS, flip, OSD), flip-hist {args.flip_hist}" if not args.no_pp else "plain BP (--no-pp)"
+    if learned_from:
+        pp += f", learned flip proposal at stalls from iteration {learned_from}"
     return f"batched Monte Carlo, [[9216,4612]] APM code, p={args.p}, max-iter {args.max_iter}, {pp}, {decoder}"
 
 
@@ -224,8 +228,13 @@ def main():
 
     dec = Decoder.from_params(device=local)
     pp = not args.no_pp
+    from joint_bp_plus_pp_b200 import load_flip_model
+    model = load_flip_model() if (pp and args.learned_from > 0 and args.precision == "fp16") else None
+    learned_from = args.learned_from if model is not None else 0
+    if model is not None:
+        dec.set_flip_model(model)
     opts = Options(precision=args.precision, max_iter=args.max_iter, enable_pp=pp, flip_hist=args.flip_hist,
-                   slots=args.slots, profile=True, engine=args.engine)
+                   slots=args.slots, profile=True, engine=args.engine, learned_from=learned_from)
     B = args.batch
     stride = B * (args.warmup + args.steps + 2)
     base = 1 + rank * stride          # distinct trial ranges per rank
@@ -246,7 +255,8 @@ def main():
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record()
     agg = {"trials": 0, "failures": 0, "total_iters": 0, "check_ms": 0.0, "var_ms": 0.0, "kernel_launches": 0,
-           "bp_trial_iterations": 0, "profiled_iterations": 0, "device_ms": 0.0, "pp_success": 0}
+           "bp_trial_iterations": 0, "profiled_iterations": 0, "device_ms": 0.0, "pp_success": 0,
+           "learned_attempts": 0, "learned_success": 0}
     first_res = None
     for k in range(args.steps):
         st, res = dec.simulate(args.seed, B, args.p, opts, first_trial=base + (args.warmup + k) * B,
@@ -339,7 +349,7 @@ def main():
         host = torch.empty((E, N_QUBITS), dtype=torch.uint8, pin_memory=True).numpy()
         host[:] = sample_reference_errors(N_QUBITS, args.seed, base + 5 * 10 ** 8, E, args.p)
         oe = Options(precision=args.precision, max_iter=args.max_iter, enable_pp=pp, flip_hist=args.flip_hist,
-                     slots=args.slots, engine=args.engine)
+                     slots=args.slots, engine=args.engine, learned_from=learned_from)
         dec.decode_errors(host[: max(32, E // 8)], args.p, oe, want_est=False)
         torch.cuda.synchronize()
         barrier()
@@ -379,9 +389,12 @@ def main():
         "dtype": {"fp32": "f32", "fp16": "f32 arithmetic, f16 message storage", "fp64": "f64"}[args.precision],
         "data": "synthetic: Philox4x32-10 depolarizing noise keyed by (seed, trial index)",
         "config": {"workload": workload_name(args, {"fp16": "FP32 arithmetic with FP16 message storage",
-                                                    "fp32": "FP32 messages", "fp64": "FP64 messages"}[args.precision]),
+                                                    "fp32": "FP32 messages", "fp64": "FP64 messages"}[args.precision],
+                                             learned_from),
                    "p": args.p,
                    "max_iter": args.max_iter, "enable_pp": pp, "flip_hist": args.flip_hist,
+                   "learned_from": learned_from,
+                   "learned": {"attempts": agg["learned_attempts"], "saved": agg["learned_success"]},
                    "trials_per_step": B, "engine": "resident" if resident else "slots",
                    "l2": ("trial state in shared memory; no message traffic to HBM" if resident
                           else "message state (>= 7 GB) larger than L2"),

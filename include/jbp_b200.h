@@ -64,6 +64,9 @@ typedef struct {
     int use_prior;         /* 1: decode with `prior` below instead of normalize(1-p, p/3, p/3, p/3) */
     double prior[4];       /* probabilities of I, X, Z, Y (used as given, as cuda_bp_decode does) */
     int engine;            /* JBP_ENGINE_* (default AUTO) */
+    int learned_from;      /* > 0: from this iteration on, a stalled trial (decisions unchanged or
+                              oscillating) first tries the learned flip proposal set with
+                              jbp_set_flip_model (resident engine, post-processing on); 0 = off */
 } jbp_options;
 
 /* Per-trial outcome (16 bytes). */
@@ -78,7 +81,8 @@ typedef struct {
     uint8_t pp_ets;        /* ETS stage produced the final estimate */
     uint8_t pp_flip;       /* flip stage produced the final estimate */
     uint8_t pp_osd;        /* OSD counted (reference osd_success) */
-    uint8_t ets_used_flags;/* bit0 ETS used, bit1 size 6, bit2 size 12, bit3 post-BP ETS applied */
+    uint8_t ets_used_flags;/* bit0 ETS used, bit1 size 6, bit2 size 12, bit3 post-BP ETS applied,
+                              bit4 post-BP stages ran, bit5 a learned flip proposal was accepted */
     uint8_t pp_in_decode;  /* post-processing succeeded inside the BP loop */
     uint8_t reserved;
 } jbp_trial_result;
@@ -95,6 +99,8 @@ typedef struct {
     double var_ms;             /* with profile: device time of all variable-node kernel launches */
     long long profiled_iterations; /* with profile: BP iterations (launch pairs) timed */
     long long slots;           /* trials in flight used by the run */
+    long long learned_attempts;/* learned flip proposals evaluated */
+    long long learned_success; /* trials whose accepted learned proposal was a success */
 } jbp_stats;
 
 void jbp_default_options(jbp_options *opt);
@@ -147,6 +153,38 @@ int jbp_decode_errors_device(jbp_ctx *ctx, const jbp_options *opt, long long ntr
 int jbp_decode_syndromes_noalloc(jbp_ctx *ctx, const jbp_options *opt, int ntrials, const uint8_t *d_sx,
                                  const uint8_t *d_sz, double p, uint8_t *d_est_out, jbp_trial_result *d_res,
                                  void *stream);
+
+/* Learned flip proposal (no counterpart in the reference): a 3-layer MLP (8 -> 64 -> 64 -> 2,
+ * ReLU) over per-qubit features of a stalled BP state -- the four normalized log2 weights of
+ * I, X, Z, Y, the x-bit and z-bit flips over the last 5 iterations, and the unsatisfied X and
+ * Z checks at the qubit -- whose two logits propose flipping the qubit's x-bit and z-bit.  A
+ * proposal is applied only if both syndromes then match exactly.  Parameters: FP32, the
+ * layout W1[64][8], b1[64], W2[64][64], b2[64], W3[2][64], b3[2] (jbp_mlp_param_count()).
+ * Features x are nsamples x 8 floats, labels y nsamples x 2 floats (0/1), host buffers. */
+int jbp_mlp_param_count(void);
+/* Gradient of the mean loss (binary cross-entropy with logits, positives weighted by
+ * pos_weight, summed over the two outputs) on the GPU; grad_out has jbp_mlp_param_count()
+ * entries. */
+int jbp_mlp_grad(jbp_ctx *ctx, const float *params, long long nsamples, const float *x, const float *y,
+                 float pos_weight, float *grad_out, double *loss_out);
+/* Adam training on the GPU (minibatches of `batch`, reshuffled each epoch from `seed`);
+ * params is updated in place; epoch_loss (epochs entries, may be null) gets each epoch's
+ * mean loss. */
+int jbp_mlp_train(jbp_ctx *ctx, float *params, long long nsamples, const float *x, const float *y, int epochs,
+                  int batch, float lr, float pos_weight, uint64_t seed, double *epoch_loss);
+/* BF16 tensor-core inference (the kernel code the decoder runs after a stall): logits is
+ * nsamples x 2. */
+int jbp_mlp_infer(jbp_ctx *ctx, const float *params, long long nsamples, const float *x, float *logits);
+/* The model used when jbp_options.learned_from > 0 (params = NULL removes it). */
+int jbp_set_flip_model(jbp_ctx *ctx, const float *params);
+/* Training data: runs the Monte Carlo like jbp_simulate (resident engine, post-processing on,
+ * opt->learned_from > 0 gives the first stall iteration) and, at every stall where the learned
+ * proposal would run, records the features and labels (x-bit / z-bit of error xor estimate) of
+ * the qubits next to an unsatisfied check, the qubits whose estimate is wrong and 1 in 32 of
+ * the others, up to `capacity` samples.  Decoding itself is unchanged. */
+int jbp_collect_stall_states(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed, long long first_trial,
+                             long long ntrials, double p, int sampler, long long capacity, float *x_out, float *y_out,
+                             long long *count_out, jbp_stats *stats);
 
 /* Errors of trials first_trial.. drawn by a device sampler (JBP_SAMPLER_*), copied to the host
  * buffer err (ntrials x n).  The same streams jbp_simulate decodes. */

@@ -38,7 +38,8 @@ class COptions(ctypes.Structure):
                 ("flip_hist", ctypes.c_int), ("enable_pp", ctypes.c_int), ("freeze_syn", ctypes.c_int),
                 ("check_warmup", ctypes.c_int), ("check_interval", ctypes.c_int), ("slots", ctypes.c_int),
                 ("iters_per_launch", ctypes.c_int), ("watchdog_ms", ctypes.c_int), ("profile", ctypes.c_int),
-                ("use_prior", ctypes.c_int), ("prior", ctypes.c_double * 4), ("engine", ctypes.c_int)]
+                ("use_prior", ctypes.c_int), ("prior", ctypes.c_double * 4), ("engine", ctypes.c_int),
+                ("learned_from", ctypes.c_int)]
 
 
 TRIAL_DTYPE = np.dtype([("iterations", np.int32), ("syndrome_ok", np.uint8), ("bp_ok", np.uint8),
@@ -60,7 +61,9 @@ class CStats(ctypes.Structure):
                                                                 ("check_ms", ctypes.c_double),
                                                                 ("var_ms", ctypes.c_double),
                                                                 ("profiled_iterations", ctypes.c_longlong),
-                                                                ("slots", ctypes.c_longlong)]
+                                                                ("slots", ctypes.c_longlong),
+                                                                ("learned_attempts", ctypes.c_longlong),
+                                                                ("learned_success", ctypes.c_longlong)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -83,13 +86,14 @@ class Options:
     profile: bool = False
     prior: tuple = None    # (I, X, Z, Y) probabilities used as given instead of those of p
     engine: str = "auto"   # "auto", "resident" (shared-memory trial-resident tier) or "slots"
+    learned_from: int = 0  # > 0: stalled trials try the learned flip proposal from this iteration
 
     def to_c(self):
         pr = (ctypes.c_double * 4)(*(self.prior or (0.0, 0.0, 0.0, 0.0)))
         return COptions(PREC[self.precision], self.max_iter, self.damping, self.flip_hist, int(self.enable_pp),
                         int(self.freeze_syn), self.check_warmup, self.check_interval, self.slots,
                         self.iters_per_launch, self.watchdog_ms, int(self.profile), int(self.prior is not None), pr,
-                        ENGINE[self.engine])
+                        ENGINE[self.engine], int(self.learned_from))
 
 
 _lib = None
@@ -124,6 +128,14 @@ def load_library(path=None):
     lib.jbp_sample_reference_errors.argtypes = [i, ctypes.c_uint64, ll, ll, d, vp, i]
     lib.jbp_default_options.argtypes = [ctypes.POINTER(COptions)]
     lib.jbp_default_options.restype = None
+    fp = ctypes.c_float
+    lib.jbp_mlp_param_count.restype = i
+    lib.jbp_mlp_grad.argtypes = [vp, vp, ll, vp, vp, fp, vp, ctypes.POINTER(d)]
+    lib.jbp_mlp_train.argtypes = [vp, vp, ll, vp, vp, i, i, fp, fp, ctypes.c_uint64, vp]
+    lib.jbp_mlp_infer.argtypes = [vp, vp, ll, vp, vp]
+    lib.jbp_set_flip_model.argtypes = [vp, vp]
+    lib.jbp_collect_stall_states.argtypes = [vp, ctypes.POINTER(COptions), ctypes.c_uint64, ll, ll, d, i, ll, vp, vp,
+                                             ctypes.POINTER(ll), ctypes.POINTER(CStats)]
     if path is None:
         _lib = lib
     return lib
@@ -251,6 +263,79 @@ class Decoder:
                                                              ctypes.c_void_p(d_res_ptr), ctypes.byref(st),
                                                              ctypes.c_void_p(stream)))
         return st.as_dict()
+
+
+    # ------------------------------------------------------------ learned flip proposal
+
+    def set_flip_model(self, params):
+        """Model used when Options.learned_from > 0 (None removes it)."""
+        if params is None:
+            _check(self._lib, self._lib.jbp_set_flip_model(self._h, None))
+            return
+        prm = np.ascontiguousarray(params, np.float32)
+        assert prm.size == MLP_PARAMS
+        _check(self._lib, self._lib.jbp_set_flip_model(self._h, _ptr(prm)))
+
+    def mlp_grad(self, params, x, y, pos_weight=1.0):
+        """GPU gradient and mean loss of the flip-proposal MLP on samples (x: n x 8, y: n x 2)."""
+        prm = np.ascontiguousarray(params, np.float32)
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        g = np.zeros(MLP_PARAMS, np.float32)
+        loss = ctypes.c_double()
+        _check(self._lib, self._lib.jbp_mlp_grad(self._h, _ptr(prm), len(x), _ptr(x), _ptr(y), pos_weight, _ptr(g),
+                                                 ctypes.byref(loss)))
+        return g, loss.value
+
+    def mlp_train(self, params, x, y, epochs=10, batch=4096, lr=1e-3, pos_weight=1.0, seed=1):
+        """Adam training on the GPU; returns (params, per-epoch mean loss)."""
+        prm = np.array(params, np.float32)
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        hist = np.zeros(max(1, epochs), np.float64)
+        _check(self._lib, self._lib.jbp_mlp_train(self._h, _ptr(prm), len(x), _ptr(x), _ptr(y), epochs, batch, lr,
+                                                  pos_weight, seed, _ptr(hist)))
+        return prm, hist[:epochs]
+
+    def mlp_infer(self, params, x):
+        """BF16 tensor-core inference (the decoder's fused kernel code): logits n x 2."""
+        prm = np.ascontiguousarray(params, np.float32)
+        x = np.ascontiguousarray(x, np.float32)
+        out = np.zeros((len(x), 2), np.float32)
+        _check(self._lib, self._lib.jbp_mlp_infer(self._h, _ptr(prm), len(x), _ptr(x), _ptr(out)))
+        return out
+
+    def collect_stall_states(self, seed, ntrials, p, opts, capacity, first_trial=1, sampler="philox"):
+        """Features and labels of the qubits of stalled BP states (training data)."""
+        x = np.zeros((capacity, 8), np.float32)
+        y = np.zeros((capacity, 2), np.float32)
+        cnt = ctypes.c_longlong()
+        st = CStats()
+        co = opts.to_c()
+        _check(self._lib, self._lib.jbp_collect_stall_states(self._h, ctypes.byref(co), seed, first_trial, ntrials, p,
+                                                             SAMPLER[sampler], capacity, _ptr(x), _ptr(y),
+                                                             ctypes.byref(cnt), ctypes.byref(st)))
+        return x[:cnt.value], y[:cnt.value], st.as_dict()
+
+
+MLP_PARAMS = 4866
+FLIP_MODEL_PATH = DATA_DIR / "flip_mlp_params.npy"
+
+
+def mlp_init(seed=0):
+    """He-initialised parameters of the flip-proposal MLP (W1, b1, W2, b2, W3, b3)."""
+    rng = np.random.default_rng(seed)
+    w1 = rng.normal(0, (2 / 8) ** 0.5, (64, 8))
+    w2 = rng.normal(0, (2 / 64) ** 0.5, (64, 64))
+    w3 = rng.normal(0, (1 / 64) ** 0.5, (2, 64))
+    return np.concatenate([w1.ravel(), np.zeros(64), w2.ravel(), np.zeros(64), w3.ravel(), np.full(2, -3.0)]).astype(
+        np.float32)
+
+
+def load_flip_model(path=FLIP_MODEL_PATH):
+    """The trained flip-proposal parameters shipped with the package (None if absent)."""
+    p = Path(path)
+    return np.load(p).astype(np.float32) if p.exists() else None
 
 
 def wilson_interval(n, k, z=1.96):

@@ -240,8 +240,60 @@ static int decode_host(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, 
         total.var_ms += st.var_ms;
         total.profiled_iterations += st.profiled_iterations;
         total.slots = std::max(total.slots, st.slots);
+        total.learned_attempts += st.learned_attempts;
+        total.learned_success += st.learned_success;
     }
     if (stats) *stats = total;
+    return JBP_OK;
+}
+
+int jbp_collect_stall_states(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed, long long first_trial,
+                             long long ntrials, double p, int sampler, long long capacity, float *x_out, float *y_out,
+                             long long *count_out, jbp_stats *stats) {
+    if (!ctx || ntrials < 0 || capacity <= 0 || !x_out || !y_out || !count_out)
+        return fail(JBP_ERR_ARG, "invalid argument");
+    if (sampler != JBP_SAMPLER_PHILOX && sampler != JBP_SAMPLER_MT19937) return fail(JBP_ERR_ARG, "unknown sampler");
+    jbp::RunRequest rq;
+    rq.opt = normalized(opt);
+    if (rq.opt.learned_from <= 0) return fail(JBP_ERR_ARG, "learned_from must be > 0 to define the stalls");
+    rq.source = sampler == JBP_SAMPLER_PHILOX ? jbp::kSrcPhilox : jbp::kSrcMt19937;
+    rq.seed = seed;
+    rq.first_trial = first_trial;
+    rq.ntrials = ntrials;
+    rq.p = p;
+    rq.collect = true;
+    rq.col_cap = capacity;
+    cudaSetDevice(ctx->engine.device());
+    float *dx = nullptr, *dy = nullptr;
+    unsigned long long *dc = nullptr;
+    cudaError_t ce = cudaMalloc(&dx, sizeof(float) * 8 * capacity);
+    if (ce == cudaSuccess) ce = cudaMalloc(&dy, sizeof(float) * 2 * capacity);
+    if (ce == cudaSuccess) ce = cudaMalloc(&dc, sizeof(unsigned long long));
+    if (ce == cudaSuccess) ce = cudaMemset(dc, 0, sizeof(unsigned long long));
+    std::string e;
+    jbp_stats st;
+    std::memset(&st, 0, sizeof(st));
+    unsigned long long cnt = 0;
+    if (ce != cudaSuccess) e = jbp::cuda_err(ce, "cudaMalloc(collection)");
+    if (e.empty()) {
+        rq.d_col_x = dx;
+        rq.d_col_y = dy;
+        rq.d_col_count = dc;
+        e = ctx->engine.run(rq, st);
+    }
+    if (e.empty()) {
+        ce = cudaMemcpy(&cnt, dc, sizeof(cnt), cudaMemcpyDeviceToHost);
+        const long long keep = std::min<long long>(static_cast<long long>(cnt), capacity);
+        if (ce == cudaSuccess && keep > 0) ce = cudaMemcpy(x_out, dx, sizeof(float) * 8 * keep, cudaMemcpyDeviceToHost);
+        if (ce == cudaSuccess && keep > 0) ce = cudaMemcpy(y_out, dy, sizeof(float) * 2 * keep, cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) e = jbp::cuda_err(ce, "copy collection");
+        *count_out = keep;
+    }
+    cudaFree(dx);
+    cudaFree(dy);
+    cudaFree(dc);
+    if (!e.empty()) return engine_fail(e);
+    if (stats) *stats = st;
     return JBP_OK;
 }
 

@@ -11,6 +11,7 @@
 #include "kernels_slots.cuh"
 #include "kernels_pp.cuh"
 #include "kernels_resident.cuh"
+#include "mlp.cuh"
 
 namespace jbp {
 
@@ -104,6 +105,8 @@ void fill_stats(const DevCounters &hc, jbp_stats &stats) {
     stats.exact = static_cast<long long>(hc.exact);
     stats.total_iters = static_cast<long long>(hc.total_iters);
     stats.bp_trial_iterations = static_cast<long long>(hc.bp_trial_iterations);
+    stats.learned_attempts = static_cast<long long>(hc.learned_attempts);
+    stats.learned_success = static_cast<long long>(hc.learned_success);
 }
 
 }  // namespace
@@ -113,6 +116,7 @@ Engine::~Engine() {
     delete rcode_;
     cudaFree(res_cnt_);
     cudaFree(res_pp_scratch_);
+    cudaFree(mlp_dev_);
     for (void *p : code_allocs_) cudaFree(p);
     for (void *p : ets_allocs_) cudaFree(p);
 }
@@ -234,6 +238,21 @@ std::string Engine::build_res_code() {
     return "";
 }
 
+std::string Engine::set_flip_model(const float *params) {
+    if (!params) {
+        has_mlp_ = false;
+        return "";
+    }
+    JBP_CUDA_TRY(cudaSetDevice(device_), "cudaSetDevice");
+    if (!mlp_dev_) JBP_CUDA_TRY(cudaMalloc(&mlp_dev_, sizeof(uint32_t) * kMlpDevWords), "cudaMalloc(mlp)");
+    std::vector<uint32_t> packed(kMlpDevWords);
+    mlp_pack(params, packed.data());
+    JBP_CUDA_TRY(cudaMemcpy(mlp_dev_, packed.data(), sizeof(uint32_t) * kMlpDevWords, cudaMemcpyHostToDevice),
+                 "upload mlp");
+    has_mlp_ = true;
+    return "";
+}
+
 bool Engine::resident_applies(const jbp_options &o, std::string *why) const {
     auto no = [&](const std::string &w) {
         if (why) *why = w;
@@ -243,6 +262,7 @@ bool Engine::resident_applies(const jbp_options &o, std::string *why) const {
     if (o.precision != JBP_PREC_FP16) return no("the resident tier stores messages in FP16 (precision FP16)");
     if (o.enable_pp && (o.check_interval != 1 || o.check_warmup != 0))
         return no("post-processing needs a syndrome test every iteration");
+    if (o.learned_from > 0 && !o.enable_pp) return no("learned flip proposals need post-processing on");
     if (o.damping > 0.0) return no("damping runs on the slot tier");
     if (o.freeze_syn) return no("freeze-syn runs on the slot tier");
     return true;
@@ -265,7 +285,9 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     const long long want = std::max<long long>(1, std::min<long long>(rq.ntrials, 1LL << 30));
     const int grid = static_cast<int>(std::min<long long>(static_cast<long long>(per_sm) * sm_count_, want));
     const int H = std::max(0, o.flip_hist);
-    const int R = std::max(H + 1, 3);
+    const bool learned = pp && o.learned_from > 0;
+    if (learned && !rq.collect && !has_mlp_) return "learned flip proposals requested but no model is set";
+    const int R = std::max(H + 1, learned ? 6 : 3);   // the kernel's ring size
     size_t stride = 0;
     if (pp) {
         std::string ee = upload_ets();
@@ -304,6 +326,13 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     r.ets = dets_;
     r.pp_scratch = pp ? res_pp_scratch_ : nullptr;
     r.pp_scratch_stride = stride;
+    r.learned_from = learned ? o.learned_from : 0;
+    r.mlp.w = mlp_dev_;
+    r.collect = rq.collect ? 1 : 0;
+    r.col_x = rq.d_col_x;
+    r.col_y = rq.d_col_y;
+    r.col_count = rq.d_col_count;
+    r.col_cap = rq.col_cap;
     cudaStream_t st = rq.stream;
     cudaEvent_t ev0, ev1;
     JBP_CUDA_TRY(cudaEventCreate(&ev0), "cudaEventCreate");
@@ -470,8 +499,10 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     if (o.engine != JBP_ENGINE_SLOTS) {
         std::string why;
         if (resident_applies(o, &why)) return run_resident(rq, stats);
-        if (o.engine == JBP_ENGINE_RESIDENT) return "resident engine not available: " + why;
+        if (o.engine == JBP_ENGINE_RESIDENT || o.learned_from > 0 || rq.collect)
+            return "resident engine not available: " + why;
     }
+    if (o.learned_from > 0 || rq.collect) return "learned flip proposals are not available on the slot engine";
     const SideGraph &gx = model_.side[0], &gz = model_.side[1];
     if (!gx.regular || !gz.regular || gx.dc_max != gz.dc_max || gx.dv_max != gz.dv_max)
         return "the GPU kernels need a code with equal regular degrees on both sides";

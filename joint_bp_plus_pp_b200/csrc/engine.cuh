@@ -72,6 +72,7 @@ enum ResultBit : int {
     kResFlipOk = 1 << 10,
     kResOsdOk = 1 << 11,
     kResPostEntered = 1 << 12,   // post-BP stages ran
+    kResLearned = 1 << 13,       // a learned flip proposal produced the final estimate
 };
 
 // Post-processing request kinds (pp_mode).
@@ -86,6 +87,7 @@ struct DevCounters {
     unsigned long long bp_trial_iterations;
     unsigned long long watchdog;
     unsigned long long bad_input;   // error bytes outside 0..3 seen in a kSrcErrors source
+    unsigned long long learned_attempts, learned_success;   // learned flip proposals tried / saves
 };
 
 struct DevRun {

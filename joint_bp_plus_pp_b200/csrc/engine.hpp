@@ -27,6 +27,11 @@ struct RunRequest {
     jbp_trial_result *d_res_out = nullptr;
     unsigned long long *d_hist = nullptr;
     cudaStream_t stream = nullptr;
+    // stall-state collection for training the learned proposal (device buffers)
+    bool collect = false;
+    float *d_col_x = nullptr, *d_col_y = nullptr;
+    unsigned long long *d_col_count = nullptr;
+    long long col_cap = 0;
 };
 
 class Engine {
@@ -44,6 +49,8 @@ public:
     std::string sample_errors(unsigned long long seed, long long first, long long count, double p, int source,
                               uint8_t *d_out);
     const DevCode &dev_code() const { return dcode_; }
+    // Learned flip proposal parameters (FP32, mlp.cuh layout); null removes the model.
+    std::string set_flip_model(const float *params);
     int sm_count() const { return sm_count_; }
 
 private:
@@ -95,6 +102,8 @@ private:
     DevCounters *res_cnt_ = nullptr;
     unsigned char *res_pp_scratch_ = nullptr;
     size_t res_pp_bytes_ = 0;
+    uint32_t *mlp_dev_ = nullptr;
+    bool has_mlp_ = false;
     CodeModel model_;
     DevCode dcode_{};
     std::vector<void *> code_allocs_;

@@ -42,6 +42,7 @@
 #include "engine.cuh"
 #include "kernels_slots.cuh"
 #include "kernels_pp.cuh"
+#include "mlp.cuh"
 
 namespace jbp {
 
@@ -79,14 +80,26 @@ struct ResRun {
     int flip_hist;
     DevCode dc;                    // table form of the code for the post-processing stages
     DevEts ets;
-    unsigned char *pp_scratch;     // per block: PpScratch | decision ring [R][n] | |LLR| [2][n] doubles
+    unsigned char *pp_scratch;     // per block: PpScratch | decision ring [R][n] | |LLR| [2][n] doubles |
+                                   // features [n][8]
     size_t pp_scratch_stride;
+    // learned flip proposal (mlp.cuh): tried at stalls from iteration learned_from (0 = off)
+    int learned_from;
+    MlpDev mlp;
+    int collect;                   // 1: record stall-state samples instead of proposing
+    float *col_x, *col_y;          // [col_cap][8], [col_cap][2]
+    unsigned long long *col_count;
+    long long col_cap;
 };
+
+constexpr int kLearnedTries = 3;   // learned proposals per trial at most
+constexpr int kLearnedMaxUnsat = 30;   // ... and only while max(us_x, us_z) is at most this
 
 // Per-block global scratch of a post-processing run: the GF(2) work areas, the ring of the
 // last R iterations' decisions and the |LLR| keys of the OSD order.
 __host__ __device__ inline size_t res_pp_scratch_bytes(int n, int mmax, int R) {
-    return pp_align(pp_scratch_bytes(n, mmax)) + pp_align(static_cast<size_t>(R) * n) + pp_align(16ull * n);
+    return pp_align(pp_scratch_bytes(n, mmax)) + pp_align(static_cast<size_t>(R) * n) + pp_align(16ull * n) +
+           pp_align(32ull * n);
 }
 
 __device__ __forceinline__ unsigned res_mod(unsigned x, unsigned P, unsigned magic) {
@@ -259,9 +272,14 @@ __device__ __forceinline__ float res_couple(float s, float c0, float c1, float c
 }
 
 // Variable phase for block column LL, variable offset y: sums, hard decision, new A.
-template <int P, int J, int L, class ST, int LL>
+// With HIST the low 6 mantissa bits of A keep the side's decision bits of the last 6
+// iterations (bit 0 = this one), and ch1 / ch2 collect whether any decision differs from the
+// previous iteration / the one before (the stall and oscillation tests of the learned
+// proposal).  The perturbation is below 2^-17 of |A|, far under the FP16 message precision.
+template <int P, int J, int L, class ST, int LL, bool HIST>
 __device__ __forceinline__ void res_var_col(const ResCode &code, const typename ST::T *c2v, float *A, int y,
-                                            const float4 lp, const float4 pr) {
+                                            const float4 *lps, const float4 *prs, unsigned &ch1, unsigned &ch2) {
+    const float4 lp = *lps, pr = *prs;   // block constants, re-read from shared memory
     constexpr int m = J * P, n = L * P;
     float Lam = 0.0f, Mu = 0.0f;
 #pragma unroll
@@ -282,15 +300,24 @@ __device__ __forceinline__ void res_var_col(const ResCode &code, const typename 
     const float Gx = res_couple(Mu, pr.x, pr.z, pr.y, pr.w);
     const float Hz = res_couple(Lam, pr.x, pr.y, pr.z, pr.w);
     const int v = LL * P + y;
-    A[v] = with_bit(Lam + Gx, best & 1u);
-    A[n + v] = with_bit(Mu + Hz, best >> 1);
+    if (HIST) {
+        const unsigned hx = ((__float_as_uint(A[v]) << 1) | (best & 1u)) & 0x3Fu;
+        const unsigned hz = ((__float_as_uint(A[n + v]) << 1) | (best >> 1)) & 0x3Fu;
+        ch1 |= (hx ^ (hx >> 1)) | (hz ^ (hz >> 1));
+        ch2 |= (hx ^ (hx >> 2)) | (hz ^ (hz >> 2));
+        A[v] = __uint_as_float((__float_as_uint(Lam + Gx) & ~0x3Fu) | hx);
+        A[n + v] = __uint_as_float((__float_as_uint(Mu + Hz) & ~0x3Fu) | hz);
+    } else {
+        A[v] = with_bit(Lam + Gx, best & 1u);
+        A[n + v] = with_bit(Mu + Hz, best >> 1);
+    }
 }
 
-template <int P, int J, int L, class ST, int LL>
+template <int P, int J, int L, class ST, int LL, bool HIST>
 __device__ __forceinline__ void res_var_cols(const ResCode &code, const typename ST::T *c2v, float *A, int y,
-                                             const float4 lp, const float4 pr) {
-    res_var_col<P, J, L, ST, LL>(code, c2v, A, y, lp, pr);
-    if constexpr (LL + 1 < L) res_var_cols<P, J, L, ST, LL + 1>(code, c2v, A, y, lp, pr);
+                                             const float4 *lps, const float4 *prs, unsigned &ch1, unsigned &ch2) {
+    res_var_col<P, J, L, ST, LL, HIST>(code, c2v, A, y, lps, prs, ch1, ch2);
+    if constexpr (LL + 1 < L) res_var_cols<P, J, L, ST, LL + 1, HIST>(code, c2v, A, y, lps, prs, ch1, ch2);
 }
 
 // Block-wide membership test of vec (shared memory, `words` 64-bit words) in a row space
@@ -330,6 +357,259 @@ __device__ void res_abs_llr(const ResCode &code, const typename ST::T *c2v, cons
     }
 }
 
+// Per-qubit features of the stalled state at iteration `it` (mlp.cuh, include/jbp_b200.h):
+// the normalized log2 weights of I, X, Z, Y from the current c2v (w - max w, / 16, >= -4), the
+// x-bit and z-bit flips over the last 5 iterations (decision history in A's low bits, / 5),
+// and the unsatisfied X and Z checks at the qubit (/ 3, from psh.est against psh.tgt).
+template <int P, int J, int L, class ST>
+__device__ void res_features(const ResCode &code, const DevCode &dc, const typename ST::T *c2v, const float *A,
+                             const float4 lp, int it, const PpShared &psh, float *feat) {
+    constexpr int m = J * P, n = L * P;
+    for (int v = threadIdx.x; v < n; v += blockDim.x) {
+        const int l = v / P, y = v - l * P;
+        float Lam = 0.0f, Mu = 0.0f;
+        for (int j = 0; j < J; ++j) {
+            const unsigned xx = (static_cast<unsigned>(code.ia[0][j][l]) * static_cast<unsigned>(y) + code.ib[0][j][l]) %
+                                static_cast<unsigned>(P);
+            const unsigned xz = (static_cast<unsigned>(code.ia[1][j][l]) * static_cast<unsigned>(y) + code.ib[1][j][l]) %
+                                static_cast<unsigned>(P);
+            Lam += ST::ld(c2v + l * m + j * P + xx);
+            Mu += ST::ld(c2v + (L + l) * m + j * P + xz);
+        }
+        const float w0 = lp.x, w1 = lp.y - Lam, w2 = lp.z - Mu, w3 = lp.w - Lam - Mu;
+        const float mx = fmaxf(fmaxf(w0, w1), fmaxf(w2, w3));
+        float *f = feat + static_cast<size_t>(v) * kMlpIn;
+        f[0] = fmaxf((w0 - mx) * 0.0625f, -4.0f);
+        f[1] = fmaxf((w1 - mx) * 0.0625f, -4.0f);
+        f[2] = fmaxf((w2 - mx) * 0.0625f, -4.0f);
+        f[3] = fmaxf((w3 - mx) * 0.0625f, -4.0f);
+        // flips over the last 5 iterations, from the decision history in A's low bits
+        const unsigned hx = __float_as_uint(A[v]) & 0x3Fu, hz = __float_as_uint(A[n + v]) & 0x3Fu;
+        const int span = min(5, it - 1);
+        const unsigned msk = (1u << max(span, 0)) - 1u;
+        f[4] = __popc((hx ^ (hx >> 1)) & msk) * 0.2f;
+        f[5] = __popc((hz ^ (hz >> 1)) & msk) * 0.2f;
+    }
+    for (int side = 0; side < 2; ++side) {
+        blk_side_diff(dc, psh, side);
+        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+            int u = 0;
+            for (int k = 0; k < dc.s[side].dv; ++k) u += psh.diff[var_check(dc, side, v, k)];
+            feat[static_cast<size_t>(v) * kMlpIn + 6 + side] = u * (1.0f / 3.0f);
+        }
+        __syncthreads();
+    }
+}
+
+// Post-processing working areas of this block: shared arrays after the trial state, and the
+// per-block global scratch (recomputed where needed so that the BP loop keeps no pointers).
+struct ResPpPtrs {
+    PpShared psh;
+    PpScratch psc;
+    uint8_t *ring;
+    double *llr;
+    float *feat;
+    int R;
+};
+
+template <int P, int J, int L, class ST>
+__device__ __forceinline__ ResPpPtrs res_pp_ptrs(const ResRun &run, unsigned char *smem) {
+    constexpr int m = J * P, n = L * P, mw = (m + 31) / 32;
+    constexpr size_t c2v_bytes = (2ull * L * m * sizeof(typename ST::T) + 15) / 16 * 16;
+    ResPpPtrs q;
+    q.R = max(run.flip_hist + 1, run.learned_from > 0 ? 6 : 3);
+    const size_t base = pp_align(c2v_bytes + 2ull * n * 4 + (n + 15) / 16 * 16 + (2 * mw + 3) / 4 * 4 * 4 + 64);
+    q.psh = pp_shared_carve(smem + base, n, 2 * m, m);
+    unsigned char *g = run.pp_scratch + run.pp_scratch_stride * blockIdx.x;
+    q.psc = pp_scratch_carve(g, n, m);
+    q.ring = g + pp_align(pp_scratch_bytes(n, m));
+    q.llr = reinterpret_cast<double *>(q.ring + pp_align(static_cast<size_t>(q.R) * n));
+    q.feat = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(q.llr) + pp_align(16ull * n));
+    return q;
+}
+
+// The learned flip proposal on the stalled state of iteration `it` (rare path, kept out of
+// line so that the BP loop's registers are not shaped by it).  In collection mode it records
+// the samples and returns false; otherwise it solves the proposed flip sets and returns true,
+// with the corrected decisions in A's low bits, only if both syndromes then match exactly.
+template <int P, int J, int L, class ST>
+__device__ __noinline__ bool res_learned_attempt(const ResCode &code, const ResRun &run, unsigned char *smem,
+                                                 typename ST::T *c2v, float *A, const unsigned *syn, const uint8_t *err,
+                                                 bool have_err, int it, long long t, const float4 lp) {
+    constexpr int m = J * P, n = L * P, mw = (m + 31) / 32;
+    const ResPpPtrs q = res_pp_ptrs<P, J, L, ST>(run, smem);
+    const PpShared &psh = q.psh;
+    const PpScratch &psc = q.psc;
+    float *feat = q.feat;
+    double *llr_scratch = q.llr;
+    for (int v = threadIdx.x; v < n; v += blockDim.x)
+        psh.est[v] = static_cast<uint8_t>((__float_as_uint(A[v]) & 1u) | ((__float_as_uint(A[n + v]) & 1u) << 1));
+    for (int r = threadIdx.x; r < 2 * m; r += blockDim.x) {
+        const int side = r >= m, c = r - side * m;
+        psh.tgt[r] = static_cast<uint8_t>((syn[side * mw + (c >> 5)] >> (c & 31)) & 1u);
+    }
+    __syncthreads();
+    res_features<P, J, L, ST>(code, run.dc, c2v, A, lp, it, psh, feat);
+    if (run.collect) {
+        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+            const float *f = feat + static_cast<size_t>(v) * kMlpIn;
+            const unsigned lab = have_err ? (err[v] ^ psh.est[v]) : 0u;
+            const unsigned h = static_cast<unsigned>(splitmix64(static_cast<unsigned long long>(t) * 1315423911ull +
+                                                                static_cast<unsigned long long>(it) * 9216ull + v));
+            if (!(lab || f[6] + f[7] > 0.0f || (h & 31u) == 0u)) continue;
+            const unsigned long long q = atomicAdd(run.col_count, 1ull);
+            if (q >= static_cast<unsigned long long>(run.col_cap)) continue;
+            for (int kk = 0; kk < kMlpIn; ++kk) run.col_x[q * kMlpIn + kk] = f[kk];
+            run.col_y[q * 2] = static_cast<float>(lab & 1u);
+            run.col_y[q * 2 + 1] = static_cast<float>((lab >> 1) & 1u);
+        }
+        __syncthreads();
+        return false;
+    }
+    if (threadIdx.x == 0) atomicAdd(&run.cnt->learned_attempts, 1ull);
+    // logits of every qubit (x-flip, z-flip) into the |LLR| scratch, which is free here
+    float *logit = reinterpret_cast<float *>(llr_scratch);
+    const int wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5, lane = threadIdx.x & 31;
+    for (int tile = wid; tile * 16 < n; tile += nwarps) {
+        auto fget = [&](int row, int kk) -> float {
+            const int v = tile * 16 + row;
+            return v < n ? feat[static_cast<size_t>(v) * kMlpIn + kk] : 0.0f;
+        };
+        float o[4];
+        mlp_tile(run.mlp, fget, o);
+        if ((lane & 3) == 0) {
+            const int v0 = tile * 16 + (lane >> 2), v1 = v0 + 8;
+            if (v0 < n) { logit[2 * v0] = o[0]; logit[2 * v0 + 1] = o[1]; }
+            if (v1 < n) { logit[2 * v1] = o[2]; logit[2 * v1 + 1] = o[3]; }
+        }
+    }
+    __syncthreads();
+    // The proposal per side: the qubits in the order of their learned score (most likely wrong
+    // first) enter the incremental GF(2) elimination of the OSD stage (blk_osd_side); the first
+    // prefix whose span holds the side's syndrome difference gives the flips, kept only if the
+    // solution is unique and of weight <= 30 (the reference's OSD acceptance), so that the side's
+    // syndrome then matches.  Keys: 1 - sigmoid(logit) > 0, ascending = most likely wrong first.
+    double *key = reinterpret_cast<double *>(feat);   // the features are no longer needed
+    for (int v = threadIdx.x; v < n; v += blockDim.x) {
+        key[v] = 1.0 / (1.0 + exp(static_cast<double>(logit[2 * v])));
+        key[n + v] = 1.0 / (1.0 + exp(static_cast<double>(logit[2 * v + 1])));
+    }
+    __syncthreads();
+    int left = 0;
+    for (int side = 0; side < 2; ++side) {
+        if (blk_side_diff(run.dc, psh, side) == 0) continue;
+        if (!blk_osd_side(run.dc, key + static_cast<size_t>(side) * n, psh, psc, side)) ++left;
+    }
+    const bool accepted = left == 0;
+    if (accepted)
+        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+            A[v] = with_bit(A[v], psh.est[v] & 1u);
+            A[n + v] = with_bit(A[n + v], (psh.est[v] >> 1) & 1u);
+        }
+    // a rejected proposal leaves nothing behind: later stages reload the estimate from the ring
+    __syncthreads();
+    return accepted;
+}
+
+// One post-processing pass (in-loop attempt or post-BP) on the decisions of iteration `it`
+// (rare path, out of line).  Returns the trial's result flags when the pass ends the trial
+// (in-loop success, or the post-BP pass), with the corrected decisions in A's low bits;
+// 0 when BP continues.
+template <int P, int J, int L, class ST>
+__device__ __forceinline__ int res_pp_attempt(const ResCode &code, const ResRun &run, const ResPpPtrs &q,
+                                              const typename ST::T *c2v, float *A, const unsigned *syn,
+                                              const uint8_t *cur, int it, int mode, int act_k, const float4 lp) {
+    constexpr int m = J * P, n = L * P, mw = (m + 31) / 32;
+    const PpShared &psh = q.psh;
+    const PpScratch &psc = q.psc;
+    const uint8_t *ring = q.ring;
+    const int R = q.R;
+    double *llr = q.llr;
+    for (int v = threadIdx.x; v < n; v += blockDim.x) psh.est[v] = cur[v];
+    for (int r = threadIdx.x; r < 2 * m; r += blockDim.x) {
+        const int side = r >= m, c = r - side * m;
+        psh.tgt[r] = static_cast<uint8_t>((syn[side * mw + (c >> 5)] >> (c & 31)) & 1u);
+    }
+    res_abs_llr<P, J, L, ST>(code, c2v, lp, llr);
+    __syncthreads();
+    const RingHistory hist{ring, R};
+    const PpOutcome o = blk_pp_stages(run.dc, run.ets, hist, run.flip_hist, act_k, it, llr, llr + n, psh, psc);
+    const bool in_loop_success = mode == kPpInLoop && o.ok;
+    const bool post = !in_loop_success && (mode == kPpPost || it >= run.max_iter);
+    int rf = 0;
+    if (in_loop_success || post) {
+        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+            A[v] = with_bit(A[v], psh.est[v] & 1u);
+            A[n + v] = with_bit(A[n + v], (psh.est[v] >> 1) & 1u);
+        }
+        rf = pp_result_flags(o, in_loop_success);
+    }
+    __syncthreads();
+    return rf;
+}
+
+// One iteration from `slow_from` on (post-processing instantiations; rare path, out of line):
+// syndrome test after the variable phase, the decision ring, the stall / oscillation /
+// us-signal triggers (jointbp_ets.cpp:2521-2633), the learned proposal and the
+// post-processing pass.  Returns 0 to continue BP, else the trial's result flags (-1 for
+// a finished trial without any flag: not converged, no stage succeeded).
+template <int P, int J, int L, class ST>
+__device__ __noinline__ int res_slow_step(const ResCode &code, const ResRun &run, unsigned char *smem,
+                                          typename ST::T *c2v, float *A, const unsigned *syn, const uint8_t *err,
+                                          bool have_err, int it, long long t, const float4 lp,
+                                          unsigned short *us_hist, int *pp_sh, int *ints) {
+    constexpr int n = L * P;
+    const ResPpPtrs q = res_pp_ptrs<P, J, L, ST>(run, smem);
+    const uint8_t *ring = q.ring;
+    const int R = q.R;
+    const int2 us = res_block_sum2(res_test_side<P, J, L>(code, A, syn, 0), res_test_side<P, J, L>(code, A, syn, 1),
+                                   ints);
+    if (us.x + us.y == 0) return kResSyndromeOk | kResBpOk;
+    uint8_t *cur = q.ring + static_cast<size_t>(it % R) * n;
+    for (int v = threadIdx.x; v < n; v += blockDim.x)
+        cur[v] = static_cast<uint8_t>((__float_as_uint(A[v]) & 1u) | ((__float_as_uint(A[n + v]) & 1u) << 1));
+    __syncthreads();
+    // est == prev_est / prev_prev_est (jointbp_ets.cpp:2555-2556)
+    const uint8_t *p1 = ring + static_cast<size_t>((it - 1) % R) * n;
+    const uint8_t *p2 = ring + static_cast<size_t>((it - 2 + R) % R) * n;
+    bool s1 = it >= 2, s2 = it >= 3;
+    for (int v = threadIdx.x; v < n; v += blockDim.x) {
+        if (s1) s1 = cur[v] == p1[v];
+        if (s2) s2 = cur[v] == p2[v];
+    }
+    const bool same = __syncthreads_and(s1) != 0;
+    const bool pp2 = __syncthreads_and(s2) != 0;
+    if (threadIdx.x == 0) {
+        const int sig = max(us.x, us.y);
+        us_hist[it % 100] = static_cast<unsigned short>(min(sig, 65535));
+        const bool osc = pp2 && !same;
+        const bool allow = it >= 100 || it == run.max_iter;
+        int st = pp_sh[2];
+        bool act = false;
+        if (!(st & 1) && (same || it == run.max_iter) && allow) { st |= 1; act = true; }
+        if (!(st & 2) && osc && allow) { st |= 2; act = true; }
+        if (!(st & 4) && allow && us_oscillation(us_hist, it)) { st |= 4; act = true; }
+        pp_sh[2] = st;
+        if (act && pp_sh[1] == 0 && run.flip_hist > 0) pp_sh[1] = it;
+        pp_sh[0] = (st && sig <= 20) ? kPpInLoop : (it >= run.max_iter ? kPpPost : 0);
+    }
+    __syncthreads();
+    // learned flip proposal at a stall (decisions unchanged or oscillating)
+    if (run.learned_from > 0 && it >= run.learned_from && (same || (pp2 && !same)) && pp_sh[3] < kLearnedTries &&
+        max(us.x, us.y) <= kLearnedMaxUnsat) {
+        __syncthreads();
+        if (threadIdx.x == 0) pp_sh[3] += 1;
+        if (res_learned_attempt<P, J, L, ST>(code, run, smem, c2v, A, syn, err, have_err, it, t, lp))
+            return kResSyndromeOk | kResLearned;
+    }
+    const int mode = pp_sh[0];
+    if (mode) {
+        const int r2 = res_pp_attempt<P, J, L, ST>(code, run, q, c2v, A, syn, cur, it, mode, pp_sh[1], lp);
+        if (r2) return r2;
+    }
+    return it >= run.max_iter ? -1 : 0;
+}
+
 template <int P, int J, int L, class ST, bool PP>
 __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRun run) {
     extern __shared__ __align__(16) unsigned char res_smem[];
@@ -349,21 +629,9 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
     const bool have_err = run.source != kSrcSyndromes;
 
     // post-processing state (PP instantiations)
-    PpShared psh{};
-    PpScratch psc{};
-    uint8_t *ring = nullptr;
-    double *llr = nullptr;
-    const int R = PP ? max(run.flip_hist + 1, 3) : 1;
+    const bool learned = PP && run.learned_from > 0;
     const int llr_from = min(100, run.max_iter);
     const int slow_from = PP ? max(1, llr_from - 2) : 0x7fffffff;
-    if (PP) {
-        const size_t base = pp_align(c2v_bytes + 2ull * n * 4 + (n + 15) / 16 * 16 + (2 * mw + 3) / 4 * 4 * 4 + 64);
-        psh = pp_shared_carve(res_smem + base, n, 2 * m, m);
-        unsigned char *g = run.pp_scratch + run.pp_scratch_stride * blockIdx.x;
-        psc = pp_scratch_carve(g, n, m);
-        ring = g + pp_align(pp_scratch_bytes(n, m));
-        llr = reinterpret_cast<double *>(ring + pp_align(static_cast<size_t>(R) * n));
-    }
 
     // prior: FP64 as the slot engine's refill, then its log2 weights and probabilities in FP32
     if (threadIdx.x == 0) {
@@ -385,8 +653,6 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
         for (int i = 0; i < 16; ++i) ints[i] = 0;
     }
     __syncthreads();
-    const float4 lp = lp_sh, pr = pr_sh;
-    const float lpx = lpx_sh, lpz = lpz_sh;
 
     for (;;) {
         if (threadIdx.x == 0) {
@@ -394,6 +660,7 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
             trial_sh = k < static_cast<unsigned long long>(run.ntrials) ? static_cast<long long>(k) : -1;
             pp_sh[1] = 0;   // act_k
             pp_sh[2] = 0;   // pstate
+            pp_sh[3] = 0;   // learned proposals tried
         }
         __syncthreads();
         const long long k = trial_sh;
@@ -458,7 +725,7 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
             uint4 *z = reinterpret_cast<uint4 *>(c2v);
             constexpr int nz = static_cast<int>(c2v_bytes / 16);
             for (int i = threadIdx.x; i < nz; i += blockDim.x) z[i] = make_uint4(0u, 0u, 0u, 0u);
-            const float ax = with_bit(lpx, 0u), az = with_bit(lpz, 0u);
+            const float ax = with_bit(lpx_sh, 0u), az = with_bit(lpz_sh, 0u);
             for (int v = threadIdx.x; v < n; v += blockDim.x) { A[v] = ax; A[n + v] = az; }
         }
         __syncthreads();
@@ -468,6 +735,7 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
         // post-processing) each iteration is tested after its variable phase and feeds the stall
         // triggers, the flip window and the post-processing attempts (jointbp_ets.cpp:2521-2633).
         int it = 0, rf = 0, iters = run.max_iter;
+        bool stall = false;   // (learned) decisions of iteration `it` equal those of it-1, or of it-2
         for (;;) {
             const bool fused = it >= 1 && it < slow_from &&
                                (it >= run.max_iter ||
@@ -486,71 +754,42 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
             if (fused) {
                 if (u.x + u.y == 0) { rf = kResSyndromeOk | kResBpOk; iters = it; break; }
                 if (PP && threadIdx.x == 0) us_hist[it % 100] = static_cast<unsigned short>(min(max(u.x, u.y), 65535));
-            }
-            if (it >= run.max_iter) break;
-            for (int y = threadIdx.x; y < P; y += blockDim.x) res_var_cols<P, J, L, ST, 0>(code, c2v, A, y, lp, pr);
-            __syncthreads();
-            ++it;
-            if (PP && it >= slow_from) {
-                const int2 us = res_block_sum2(res_test_side<P, J, L>(code, A, syn, 0),
-                                               res_test_side<P, J, L>(code, A, syn, 1), ints);
-                if (us.x + us.y == 0) { rf = kResSyndromeOk | kResBpOk; iters = it; break; }
-                uint8_t *cur = ring + static_cast<size_t>(it % R) * n;
-                for (int v = threadIdx.x; v < n; v += blockDim.x)
-                    cur[v] = static_cast<uint8_t>((__float_as_uint(A[v]) & 1u) | ((__float_as_uint(A[n + v]) & 1u) << 1));
-                __syncthreads();
-                // est == prev_est / prev_prev_est (jointbp_ets.cpp:2555-2556)
-                const uint8_t *p1 = ring + static_cast<size_t>((it - 1) % R) * n;
-                const uint8_t *p2 = ring + static_cast<size_t>((it - 2 + R) % R) * n;
-                bool s1 = it >= 2, s2 = it >= 3;
-                for (int v = threadIdx.x; v < n; v += blockDim.x) {
-                    if (s1) s1 = cur[v] == p1[v];
-                    if (s2) s2 = cur[v] == p2[v];
-                }
-                const bool same = __syncthreads_and(s1) != 0;
-                const bool pp2 = __syncthreads_and(s2) != 0;
-                if (threadIdx.x == 0) {
-                    const int sig = max(us.x, us.y);
-                    us_hist[it % 100] = static_cast<unsigned short>(min(sig, 65535));
-                    const bool osc = pp2 && !same;
-                    const bool allow = it >= 100 || it == run.max_iter;
-                    int st = pp_sh[2];
-                    bool act = false;
-                    if (!(st & 1) && (same || it == run.max_iter) && allow) { st |= 1; act = true; }
-                    if (!(st & 2) && osc && allow) { st |= 2; act = true; }
-                    if (!(st & 4) && allow && us_oscillation(us_hist, it)) { st |= 4; act = true; }
-                    pp_sh[2] = st;
-                    if (act && pp_sh[1] == 0 && run.flip_hist > 0) pp_sh[1] = it;
-                    pp_sh[0] = (st && sig <= 20) ? kPpInLoop : (it >= run.max_iter ? kPpPost : 0);
-                }
-                __syncthreads();
-                const int mode = pp_sh[0];
-                if (mode) {
-                    for (int v = threadIdx.x; v < n; v += blockDim.x) psh.est[v] = cur[v];
-                    for (int r = threadIdx.x; r < 2 * m; r += blockDim.x) {
-                        const int side = r >= m, c = r - side * m;
-                        psh.tgt[r] = static_cast<uint8_t>((syn[side * mw + (c >> 5)] >> (c & 31)) & 1u);
-                    }
-                    res_abs_llr<P, J, L, ST>(code, c2v, lp, llr);
+                // learned flip proposal at a stall of iteration `it` (its decisions are in A's low
+                // bits; the c2v already hold the next check update, which is the state it reads)
+                if (learned && stall && it >= run.learned_from && pp_sh[3] < kLearnedTries &&
+                    max(u.x, u.y) <= kLearnedMaxUnsat) {
                     __syncthreads();
-                    const RingHistory hist{ring, R};
-                    const PpOutcome o = blk_pp_stages(run.dc, run.ets, hist, run.flip_hist, pp_sh[1], it, llr, llr + n,
-                                                      psh, psc);
-                    const bool in_loop_success = mode == kPpInLoop && o.ok;
-                    const bool post = !in_loop_success && (mode == kPpPost || it >= run.max_iter);
-                    if (in_loop_success || post) {
-                        for (int v = threadIdx.x; v < n; v += blockDim.x) {
-                            A[v] = with_bit(A[v], psh.est[v] & 1u);
-                            A[n + v] = with_bit(A[n + v], (psh.est[v] >> 1) & 1u);
-                        }
-                        rf = pp_result_flags(o, in_loop_success);
+                    if (threadIdx.x == 0) pp_sh[3] += 1;
+                    if (res_learned_attempt<P, J, L, ST>(code, run, res_smem, c2v, A, syn, err, have_err, it, t, lp_sh)) {
+                        rf = kResSyndromeOk | kResLearned;
                         iters = it;
-                        __syncthreads();
                         break;
                     }
-                    __syncthreads();
                 }
-                if (it >= run.max_iter) { iters = it; break; }
+            }
+            if (it >= run.max_iter) break;
+            if (learned) {
+                unsigned ch1 = 0u, ch2 = 0u;
+                for (int y = threadIdx.x; y < P; y += blockDim.x)
+                    res_var_cols<P, J, L, ST, 0, true>(code, c2v, A, y, &lp_sh, &pr_sh, ch1, ch2);
+                const bool d1 = __syncthreads_or(ch1 & 1u) != 0;
+                const bool d2 = __syncthreads_or(ch2 & 1u) != 0;
+                stall = it + 1 >= 3 && (!d1 || !d2);
+            } else {
+                unsigned ch1 = 0u, ch2 = 0u;
+                for (int y = threadIdx.x; y < P; y += blockDim.x)
+                    res_var_cols<P, J, L, ST, 0, false>(code, c2v, A, y, &lp_sh, &pr_sh, ch1, ch2);
+                __syncthreads();
+            }
+            ++it;
+            if (PP && it >= slow_from) {
+                const int r3 = res_slow_step<P, J, L, ST>(code, run, res_smem, c2v, A, syn, err, have_err, it, t, lp_sh,
+                                                         us_hist, pp_sh, ints);
+                if (r3 != 0) {
+                    rf = r3 < 0 ? 0 : r3;
+                    iters = it;
+                    break;
+                }
             }
         }
         const bool ok = (rf & kResSyndromeOk) != 0;

@@ -317,6 +317,8 @@ __device__ __forceinline__ void account_trial(DevCounters *c, unsigned long long
     if (success && flip_ok) atomicAdd(&c->flip_pp_success, 1ull);
     if (pp_this) atomicAdd(&c->pp_success, 1ull);
     if (success && osd_success) atomicAdd(&c->osd_pp_success, 1ull);
+    const bool learned = rf & kResLearned;
+    if (success && learned) atomicAdd(&c->learned_success, 1ull);
     if (hist && iters >= 1 && iters <= max_iter) atomicAdd(&hist[iters], 1ull);
     if (res_out) {
         jbp_trial_result rec;
@@ -331,7 +333,8 @@ __device__ __forceinline__ void account_trial(DevCounters *c, unsigned long long
         rec.pp_flip = flip_ok;
         rec.pp_osd = osd_success;
         rec.ets_used_flags = static_cast<uint8_t>((used_any ? 1 : 0) | (used6 ? 2 : 0) | (used12 ? 4 : 0) |
-                                                  ((rf & kResEtsPost) ? 8 : 0) | (post ? 16 : 0));
+                                                  ((rf & kResEtsPost) ? 8 : 0) | (post ? 16 : 0) |
+                                                  (learned ? 32 : 0));
         rec.pp_in_decode = in_dec;
         rec.reserved = osd_ok;
         res_out[local] = rec;

@@ -1,0 +1,71 @@
+"""Training recipe of the learned flip proposal (the decoder's own stalled states -> GPU training).
+
+The decoder (resident engine, post-processing on) records, at every stall from iteration
+`learned_from` on, the features and labels of the qubits next to an unsatisfied check, of the
+qubits whose estimate is wrong and of 1 in 32 of the others (jbp_collect_stall_states).  The
+MLP is then trained on the GPU by the library's own forward/backward kernels with Adam
+(jbp_mlp_train) and saved as FP32 parameters.
+
+    python -m joint_bp_plus_pp_b200.learned --out data/flip_mlp_params.npy
+
+The default recipe decodes 100,000 seeded depolarizing trials at each p in {0.04, 0.045, 0.05,
+0.055} on the shipped [[9216,4612]] code (max-iter 100, flip-hist 5) and records the stalls from
+iteration 6 on with at most 30 unsatisfied checks per side -- the states the decoder will
+propose on.
+"""
+import argparse
+import json
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+from . import Decoder, Options, mlp_init, FLIP_MODEL_PATH
+
+
+def collect(dec, ps=(0.04, 0.045, 0.05, 0.055), trials_per_p=100000, max_iter=100, learned_from=6,
+            capacity=2_000_000, seed=20240, flip_hist=5):
+    xs, ys, info = [], [], []
+    o = Options(precision="fp16", engine="resident", max_iter=max_iter, enable_pp=True, flip_hist=flip_hist,
+                learned_from=learned_from)
+    for i, p in enumerate(ps):
+        x, y, st = dec.collect_stall_states(seed + i, trials_per_p, p, o, capacity, first_trial=1)
+        xs.append(x)
+        ys.append(y)
+        info.append({"p": p, "trials": st["trials"], "samples": len(x), "failures": st["failures"]})
+    return np.concatenate(xs), np.concatenate(ys), info
+
+
+def train(dec, x, y, epochs=12, batch=8192, lr=2e-3, pos_weight=4.0, seed=7):
+    params = mlp_init(seed)
+    params, hist = dec.mlp_train(params, x, y, epochs=epochs, batch=batch, lr=lr, pos_weight=pos_weight, seed=seed)
+    return params, hist
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=str(FLIP_MODEL_PATH))
+    ap.add_argument("--trials-per-p", type=int, default=100000)
+    ap.add_argument("--epochs", type=int, default=12)
+    ap.add_argument("--learned-from", type=int, default=6)
+    ap.add_argument("--report", default=None, help="JSON summary of the run")
+    a = ap.parse_args(argv)
+    dec = Decoder.from_params()
+    t0 = time.time()
+    x, y, info = collect(dec, trials_per_p=a.trials_per_p, learned_from=a.learned_from)
+    t1 = time.time()
+    params, hist = train(dec, x, y, epochs=a.epochs)
+    t2 = time.time()
+    np.save(a.out, params)
+    rep = {"samples": int(len(x)), "positives_x": int(y[:, 0].sum()), "positives_z": int(y[:, 1].sum()),
+           "collect": info, "collect_s": t1 - t0, "train_s": t2 - t1, "epoch_loss": [float(v) for v in hist],
+           "learned_from": a.learned_from}
+    print(json.dumps(rep))
+    if a.report:
+        Path(a.report).write_text(json.dumps(rep, indent=1))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
