@@ -275,7 +275,9 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     if (!res_cnt_) JBP_CUDA_TRY(cudaMalloc(&res_cnt_, sizeof(DevCounters)), "cudaMalloc(counters)");
     const ResCode &rc = *rcode_;
     const bool pp = o.enable_pp != 0;
-    auto kern = pp ? k_resident<768, 3, 12, StoreHalf, true> : k_resident<768, 3, 12, StoreHalf, false>;
+    auto kern = !pp ? k_resident<768, 3, 12, StoreHalf, false, false>
+                    : (o.learned_from > 0 ? k_resident<768, 3, 12, StoreHalf, true, true>
+                                          : k_resident<768, 3, 12, StoreHalf, true, false>);
     const size_t smem = res_smem_bytes(rc.n, rc.m, rc.L, sizeof(__half), pp);
     JBP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
                  "smem attribute");

@@ -557,7 +557,7 @@ template <int P, int J, int L, class ST>
 __device__ __noinline__ int res_slow_step(const ResCode &code, const ResRun &run, unsigned char *smem,
                                           typename ST::T *c2v, float *A, const unsigned *syn, const uint8_t *err,
                                           bool have_err, int it, long long t, const float4 lp,
-                                          unsigned short *us_hist, int *pp_sh, int *ints) {
+                                          unsigned short *us_hist, int *pp_sh, int *ints, bool slow) {
     constexpr int n = L * P;
     const ResPpPtrs q = res_pp_ptrs<P, J, L, ST>(run, smem);
     const uint8_t *ring = q.ring;
@@ -565,6 +565,15 @@ __device__ __noinline__ int res_slow_step(const ResCode &code, const ResRun &run
     const int2 us = res_block_sum2(res_test_side<P, J, L>(code, A, syn, 0), res_test_side<P, J, L>(code, A, syn, 1),
                                    ints);
     if (us.x + us.y == 0) return kResSyndromeOk | kResBpOk;
+    if (!slow) {
+        // a stall before slow_from: only the learned proposal (the fused test of the next check
+        // phase records this iteration's us signal)
+        if (max(us.x, us.y) > kLearnedMaxUnsat) return 0;
+        __syncthreads();
+        if (threadIdx.x == 0) pp_sh[3] += 1;
+        return res_learned_attempt<P, J, L, ST>(code, run, smem, c2v, A, syn, err, have_err, it, t, lp)
+                   ? (kResSyndromeOk | kResLearned) : 0;
+    }
     uint8_t *cur = q.ring + static_cast<size_t>(it % R) * n;
     for (int v = threadIdx.x; v < n; v += blockDim.x)
         cur[v] = static_cast<uint8_t>((__float_as_uint(A[v]) & 1u) | ((__float_as_uint(A[n + v]) & 1u) << 1));
@@ -610,7 +619,7 @@ __device__ __noinline__ int res_slow_step(const ResCode &code, const ResRun &run
     return it >= run.max_iter ? -1 : 0;
 }
 
-template <int P, int J, int L, class ST, bool PP>
+template <int P, int J, int L, class ST, bool PP, bool LEARNED>
 __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRun run) {
     extern __shared__ __align__(16) unsigned char res_smem[];
     using T = typename ST::T;
@@ -625,11 +634,12 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
     __shared__ float4 lp_sh, pr_sh;
     __shared__ float lpx_sh, lpz_sh;
     __shared__ unsigned short us_hist[100];
+    __shared__ int us_cnt[2][2];   // unsatisfied checks per side of the tested iteration, by its parity
     __shared__ int pp_sh[4];   // mode, act_k, pstate
     const bool have_err = run.source != kSrcSyndromes;
 
     // post-processing state (PP instantiations)
-    const bool learned = PP && run.learned_from > 0;
+    constexpr bool learned = LEARNED && PP;   // the host launches this instantiation only with a model
     const int llr_from = min(100, run.max_iter);
     const int slow_from = PP ? max(1, llr_from - 2) : 0x7fffffff;
 
@@ -661,6 +671,7 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
             pp_sh[1] = 0;   // act_k
             pp_sh[2] = 0;   // pstate
             pp_sh[3] = 0;   // learned proposals tried
+            us_cnt[0][0] = us_cnt[0][1] = us_cnt[1][0] = us_cnt[1][1] = 0;
         }
         __syncthreads();
         const long long k = trial_sh;
@@ -748,27 +759,24 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
                 bx = res_test_side<P, J, L>(code, A, syn, 0);
                 bz = res_test_side<P, J, L>(code, A, syn, 1);
             }
-            int2 u = make_int2(0, 0);
-            if (PP) u = res_block_sum2(bx, bz, ints);
-            else u.x = __syncthreads_or(bx + bz);
-            if (fused) {
-                if (u.x + u.y == 0) { rf = kResSyndromeOk | kResBpOk; iters = it; break; }
-                if (PP && threadIdx.x == 0) us_hist[it % 100] = static_cast<unsigned short>(min(max(u.x, u.y), 65535));
-                // learned flip proposal at a stall of iteration `it` (its decisions are in A's low
-                // bits; the c2v already hold the next check update, which is the state it reads)
-                if (learned && stall && it >= run.learned_from && pp_sh[3] < kLearnedTries &&
-                    max(u.x, u.y) <= kLearnedMaxUnsat) {
-                    __syncthreads();
-                    if (threadIdx.x == 0) pp_sh[3] += 1;
-                    if (res_learned_attempt<P, J, L, ST>(code, run, res_smem, c2v, A, syn, err, have_err, it, t, lp_sh)) {
-                        rf = kResSyndromeOk | kResLearned;
-                        iters = it;
-                        break;
-                    }
+            if (PP && fused) {
+                // per-side counts of the tested iteration (the us signal): one atomic per warp
+                const int wx = __reduce_add_sync(0xffffffffu, bx), wz = __reduce_add_sync(0xffffffffu, bz);
+                if ((threadIdx.x & 31) == 0) {
+                    if (wx) atomicAdd(&us_cnt[it & 1][0], wx);
+                    if (wz) atomicAdd(&us_cnt[it & 1][1], wz);
                 }
             }
+            const bool bad = __syncthreads_or(bx + bz) != 0;
+            if (fused) {
+                if (!bad) { rf = kResSyndromeOk | kResBpOk; iters = it; break; }
+                if (PP && threadIdx.x == 0)
+                    us_hist[it % 100] =
+                        static_cast<unsigned short>(min(max(us_cnt[it & 1][0], us_cnt[it & 1][1]), 65535));
+            }
             if (it >= run.max_iter) break;
-            if (learned) {
+            if (PP && threadIdx.x == 0) us_cnt[(it + 1) & 1][0] = us_cnt[(it + 1) & 1][1] = 0;   // next test's slot
+            if constexpr (learned) {
                 unsigned ch1 = 0u, ch2 = 0u;
                 for (int y = threadIdx.x; y < P; y += blockDim.x)
                     res_var_cols<P, J, L, ST, 0, true>(code, c2v, A, y, &lp_sh, &pr_sh, ch1, ch2);
@@ -782,9 +790,12 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
                 __syncthreads();
             }
             ++it;
-            if (PP && it >= slow_from) {
+            // rare paths, one out-of-line call site: iterations from slow_from on, and (learned)
+            // a stall of this iteration, whose c2v are still those its decisions came from
+            const bool slow = PP && it >= slow_from;
+            if (slow || (learned && stall && it >= run.learned_from && pp_sh[3] < kLearnedTries)) {
                 const int r3 = res_slow_step<P, J, L, ST>(code, run, res_smem, c2v, A, syn, err, have_err, it, t, lp_sh,
-                                                         us_hist, pp_sh, ints);
+                                                         us_hist, pp_sh, ints, slow);
                 if (r3 != 0) {
                     rf = r3 < 0 ? 0 : r3;
                     iters = it;
