@@ -41,6 +41,8 @@ struct Args {
     long long trials = 1, min_fails = 0, report_every = 100, progress_every = 100, trial_index = -1;
     int precision = JBP_PREC_FP64, sampler = JBP_SAMPLER_MT19937, slots = 0;
     long long batch = 1 << 18;
+    int engine = JBP_ENGINE_AUTO, learned_from = 0;
+    std::string flip_model;
 };
 
 void usage(const char *prog) {
@@ -59,7 +61,10 @@ void usage(const char *prog) {
               << "Extra options:\n"
               << "  --precision fp64|fp32|fp16 (fp64)  --sampler mt19937|philox (mt19937)\n"
               << "  --slots N (trials in flight, 0 = auto)  --batch N (trials per GPU call, 262144)\n"
-              << "  --ets-dir DIR (default: the params path without extension)\n";
+              << "  --ets-dir DIR (default: the params path without extension)\n"
+              << "  --engine auto|resident|slots (auto)  --learned-from N (0 = off; learned flip proposal at\n"
+              << "  stalls from iteration N, FP16 resident engine)  --flip-model FILE.npy (default: the\n"
+              << "  shipped data/flip_mlp_params.npy next to the library)\n";
 }
 
 // format_scaled_unit / format_latency (jointbp_ets.cpp:203-237)
@@ -180,7 +185,16 @@ int parse(int argc, char **argv, Args &a) {
                 if (s == "mt19937") a.sampler = JBP_SAMPLER_MT19937;
                 else if (s == "philox") a.sampler = JBP_SAMPLER_PHILOX;
                 else { std::cerr << "--sampler must be mt19937 or philox\n"; return 1; }
-            } else if (f == "--slots") { VAL(); a.slots = std::stoi(v); }
+            } else if (f == "--engine") {
+                VAL();
+                const std::string s = v;
+                if (s == "auto") a.engine = JBP_ENGINE_AUTO;
+                else if (s == "resident") a.engine = JBP_ENGINE_RESIDENT;
+                else if (s == "slots") a.engine = JBP_ENGINE_SLOTS;
+                else { std::cerr << "--engine must be auto, resident or slots\n"; return 1; }
+            } else if (f == "--learned-from") { VAL(); a.learned_from = std::max(0, std::stoi(v)); }
+            else if (f == "--flip-model") { VAL(); a.flip_model = v; }
+            else if (f == "--slots") { VAL(); a.slots = std::stoi(v); }
             else if (f == "--batch") { VAL(); a.batch = std::max(1LL, std::stoll(v)); }
             else if (f == "--ets-dir") { VAL(); a.ets_dir = v; }
             else {
@@ -233,7 +247,59 @@ jbp_options options(const Args &a) {
     o.check_warmup = a.check_warmup;
     o.check_interval = a.check_interval;
     o.slots = a.slots;
+    o.engine = a.engine;
+    o.learned_from = a.learned_from;
     return o;
+}
+
+// Learned flip-proposal parameters from a NumPy .npy file (format 1.0/2.0, little-endian
+// float32 '<f4', C order, jbp_mlp_param_count() values).  Returns an error or "".
+std::string load_npy_f32(const std::string &path, std::vector<float> &out, size_t count) {
+    std::ifstream in(path, std::ios::binary);
+    if (!in) return "cannot open " + path;
+    char magic[8];
+    if (!in.read(magic, 8) || std::memcmp(magic, "\x93NUMPY", 6) != 0) return path + ": not a .npy file";
+    size_t hlen = 0;
+    if (magic[6] == 1) {
+        unsigned char b[2];
+        if (!in.read(reinterpret_cast<char *>(b), 2)) return path + ": truncated header";
+        hlen = b[0] | (b[1] << 8);
+    } else {
+        unsigned char b[4];
+        if (!in.read(reinterpret_cast<char *>(b), 4)) return path + ": truncated header";
+        hlen = b[0] | (b[1] << 8) | (b[2] << 16) | (static_cast<size_t>(b[3]) << 24);
+    }
+    std::string hdr(hlen, '\0');
+    if (!in.read(&hdr[0], static_cast<std::streamsize>(hlen))) return path + ": truncated header";
+    if (hdr.find("'<f4'") == std::string::npos || hdr.find("True") != std::string::npos)
+        return path + ": expected little-endian float32 in C order";
+    out.resize(count);
+    if (!in.read(reinterpret_cast<char *>(out.data()), static_cast<std::streamsize>(count * sizeof(float))))
+        return path + ": fewer than " + std::to_string(count) + " values";
+    return "";
+}
+
+// Sets the learned flip model when --learned-from is given (the shipped model by default).
+int setup_flip_model(jbp_ctx *ctx, const Args &a, const char *argv0) {
+    if (a.learned_from <= 0) return 0;
+    std::string path = a.flip_model;
+    if (path.empty()) {
+        // <repo>/joint_bp_plus_pp_b200/bin/jointbp_b200 -> ../data/flip_mlp_params.npy
+        std::string self = argv0;
+        const size_t sl = self.find_last_of('/');
+        path = (sl == std::string::npos ? std::string(".") : self.substr(0, sl)) + "/../data/flip_mlp_params.npy";
+    }
+    std::vector<float> prm;
+    const std::string e = load_npy_f32(path, prm, static_cast<size_t>(jbp_mlp_param_count()));
+    if (!e.empty()) {
+        std::cerr << e << "\n";
+        return 1;
+    }
+    if (jbp_set_flip_model(ctx, prm.data()) != JBP_OK) {
+        std::cerr << jbp_last_error() << "\n";
+        return 1;
+    }
+    return 0;
 }
 
 void add_stats(jbp_stats &acc, const jbp_stats &s) {
@@ -505,6 +571,10 @@ int main(int argc, char **argv) {
     }
     if (a.enable_pp && load_ets(ctx, a)) {
         std::cerr << "ETS load failed: " << jbp_last_error() << "\n";
+        jbp_destroy(ctx);
+        return 1;
+    }
+    if (setup_flip_model(ctx, a, argv[0])) {
         jbp_destroy(ctx);
         return 1;
     }

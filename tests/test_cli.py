@@ -110,3 +110,22 @@ def test_trial_index_with_post_processing():
                 "--trials", "1", "--trial-index", "19", "--est", "/dev/stdout"])
     assert r.returncode == 0, r.stderr
     assert int(s["pp_success"]) == 1 and int(s["flip_pp_success"]) == 1 and int(s["iters"]) == rec["iterations"]
+
+
+@pytest.mark.gpu
+def test_resident_engine_and_learned_proposal_from_the_cli(tmp_path):
+    """--engine resident with post-processing and the shipped learned model (--learned-from)."""
+    base = ["--simulate", "--p", "0.045", "--trials", "8000", "--max-iter", "300", "--flip-hist", "5",
+            "--precision", "fp16", "--sampler", "philox", "--seed", "606", "--report-every", "0"]
+    r0, s0 = run(base + ["--engine", "resident"])
+    assert r0.returncode == 0, r0.stderr
+    r1, s1 = run(base + ["--engine", "resident", "--learned-from", "6"])
+    assert r1.returncode == 0, r1.stderr
+    assert s0["trials"] == s1["trials"] == "8000"
+    assert int(s1["failures"]) <= int(s0["failures"]) + 2
+    bad = tmp_path / "bad.npy"
+    bad.write_bytes(b"not numpy")
+    r2, _ = run(base + ["--learned-from", "6", "--flip-model", str(bad)])
+    assert r2.returncode != 0 and "npy" in r2.stderr
+    r3, _ = run(base + ["--engine", "bogus"])
+    assert r3.returncode != 0
