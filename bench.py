@@ -61,6 +61,26 @@ def parse_args():
 
 # ----------------------------------------------------------------------------- helpers
 
+def rank_first_trial(rank, batch, warmup, steps):
+    """First trial index of a rank's range: ranks decode disjoint contiguous ranges of
+    batch * (warmup + steps + 2) trials (warm-up, timed steps, comparison steps)."""
+    return 1 + rank * batch * (warmup + steps + 2)
+
+
+def reduce_over_ranks(dist, ms, counts, device):
+    """Max of the device time over ranks and the sum of integer counters (dict), the only
+    cross-rank operations of the bench (no collective on the data path)."""
+    import torch
+    if dist is None:
+        return ms, dict(counts)
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    keys = sorted(counts)
+    c = torch.tensor([float(counts[k]) for k in keys], device=device, dtype=torch.float64)
+    dist.all_reduce(c)
+    return float(t.item()), {k: int(round(v)) for k, v in zip(keys, c.tolist())}
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -236,8 +256,7 @@ def main():
     opts = Options(precision=args.precision, max_iter=args.max_iter, enable_pp=pp, flip_hist=args.flip_hist,
                    slots=args.slots, profile=True, engine=args.engine, learned_from=learned_from)
     B = args.batch
-    stride = B * (args.warmup + args.steps + 2)
-    base = 1 + rank * stride          # distinct trial ranges per rank
+    base = rank_first_trial(rank, B, args.warmup, args.steps)   # distinct trial ranges per rank
 
     def barrier():
         if dist is not None:
@@ -269,16 +288,9 @@ def main():
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        tr = torch.tensor([agg["trials"]], device=dev, dtype=torch.float64)
-        dist.all_reduce(tr)
-        total_trials = float(tr.item())
-    else:
-        total_trials = float(agg["trials"])
+    ms, tot = reduce_over_ranks(dist, ev0.elapsed_time(ev1), {"trials": agg["trials"], "failures": agg["failures"]},
+                                dev)
+    total_trials = float(tot["trials"])
     value = total_trials / (ms / 1000.0)
 
     peak, peak_kind = measured_peaks()
@@ -364,12 +376,8 @@ def main():
             agg["kernel_launches"] += st["kernel_launches"]
         b.record()
         torch.cuda.synchronize()
-        ems = a.elapsed_time(b)
-        if dist is not None:
-            t = torch.tensor([ems], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
-            done *= world
+        ems, tot_e = reduce_over_ranks(dist, a.elapsed_time(b), {"trials": done}, dev)
+        done = tot_e["trials"]
         e2e = {"value": done / (ems / 1000.0), "unit": UNIT, "h2d_bytes_per_step": E * N_QUBITS,
                "d2h_bytes_per_step": E * 16, "path": "jbp_decode_errors (host errors, pinned) -> results to host"}
 

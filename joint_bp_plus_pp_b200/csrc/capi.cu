@@ -189,8 +189,24 @@ static int decode_host(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, 
     cudaSetDevice(ctx->engine.device());
     jbp_stats total;
     std::memset(&total, 0, sizeof(total));
+    // Inputs in pinned host memory the device can address (cudaHostAlloc / cudaHostRegister)
+    // are read by the kernels in place: each trial's data crosses PCIe when a block starts the
+    // trial, overlapping the decoding of the others, and no staging copy is made.
+    auto mapped = [](const void *h) -> const uint8_t * {
+        if (!h) return nullptr;
+        cudaPointerAttributes at;
+        if (cudaPointerGetAttributes(&at, h) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        return at.type == cudaMemoryTypeHost && at.devicePointer ? static_cast<const uint8_t *>(at.devicePointer)
+                                                                 : nullptr;
+    };
+    const uint8_t *m_err = mapped(err), *m_sx = mapped(sx), *m_sz = mapped(sz);
     // chunks bound the staging memory; each chunk is one engine run
-    const long long chunk = std::max<long long>(1, std::min<long long>(ntrials, 1LL << 17));
+    const bool in_place = (err && m_err) || (!err && m_sx && m_sz);
+    const long long chunk =
+        std::max<long long>(1, std::min<long long>(ntrials, in_place && !est_out ? 1LL << 20 : 1LL << 17));
     for (long long base = 0; base < ntrials; base += chunk) {
         const long long cnt = std::min(chunk, ntrials - base);
         jbp::RunRequest rq;
@@ -199,12 +215,19 @@ static int decode_host(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, 
         rq.first_trial = 0;
         rq.ntrials = cnt;
         cudaError_t ce;
-        if (err) {
+        if (err && m_err) {
+            rq.source = jbp::kSrcErrors;
+            rq.d_err = m_err + base * n;
+        } else if (err) {
             if (int rc = grow(&ctx->d_in, &ctx->in_bytes, static_cast<size_t>(cnt * n))) return rc;
             ce = cudaMemcpy(ctx->d_in, err + base * n, static_cast<size_t>(cnt * n), cudaMemcpyHostToDevice);
             if (ce != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(ce, "copy errors"));
             rq.source = jbp::kSrcErrors;
             rq.d_err = ctx->d_in;
+        } else if (m_sx && m_sz) {
+            rq.source = jbp::kSrcSyndromes;
+            rq.d_sx = m_sx + base * mx;
+            rq.d_sz = m_sz + base * mz;
         } else {
             if (!sx || !sz) return fail(JBP_ERR_ARG, "null syndrome");
             if (int rc = grow(&ctx->d_in, &ctx->in_bytes, static_cast<size_t>(cnt * mx))) return rc;

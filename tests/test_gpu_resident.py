@@ -167,3 +167,34 @@ def test_invalid_error_values_are_rejected(decoder, engine, prec):
     st, res, _ = decoder.decode_errors(err[[0, 2]], 0.05, Options(precision=prec, engine=engine, max_iter=5,
                                                                   enable_pp=False))
     assert st["trials"] == 2 and res["success"].all()
+
+
+@pytest.mark.parametrize("engine,prec", [("resident", "fp16"), ("slots", "fp64")])
+def test_pinned_host_inputs_are_read_in_place(decoder, oracle, engine, prec):
+    """Errors and syndromes in pinned, device-addressable host memory are read by the kernels
+    in place (no staging copy); the results equal those from pageable buffers."""
+    import torch
+    from joint_bp_plus_pp_b200 import Options
+    o = Options(precision=prec, engine=engine, max_iter=60, enable_pp=False)
+    err = decoder.sample_errors(515, 1, 300, 0.05, sampler="philox")
+    pinned = torch.empty(err.shape, dtype=torch.uint8, pin_memory=True).numpy()
+    pinned[:] = err
+    s1, r1, e1 = decoder.decode_errors(err, 0.05, o)
+    s2, r2, e2 = decoder.decode_errors(pinned, 0.05, o)
+    assert (r1 == r2).all() and (e1 == e2).all()
+    sx = np.stack([oracle.syndrome(e)[0] for e in err[:64]])
+    sz = np.stack([oracle.syndrome(e)[1] for e in err[:64]])
+    psx = torch.empty(sx.shape, dtype=torch.uint8, pin_memory=True).numpy()
+    psz = torch.empty(sz.shape, dtype=torch.uint8, pin_memory=True).numpy()
+    psx[:] = sx
+    psz[:] = sz
+    _, q1, f1 = decoder.decode_syndromes(sx, sz, 0.05, o)
+    _, q2, f2 = decoder.decode_syndromes(psx, psz, 0.05, o)
+    assert (q1 == q2).all() and (f1 == f2).all()
+    bad = pinned.copy()
+    bad_p = torch.empty(err.shape, dtype=torch.uint8, pin_memory=True).numpy()
+    bad_p[:] = err
+    bad_p[7, 100] = 9
+    from joint_bp_plus_pp_b200 import JbpError
+    with pytest.raises(JbpError):
+        decoder.decode_errors(bad_p, 0.05, o)
