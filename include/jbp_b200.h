@@ -64,6 +64,8 @@ typedef struct {
     int use_prior;         /* 1: decode with `prior` below instead of normalize(1-p, p/3, p/3, p/3) */
     double prior[4];       /* probabilities of I, X, Z, Y (used as given, as cuda_bp_decode does) */
     int engine;            /* JBP_ENGINE_* (default AUTO) */
+    double p_max;          /* > p: each trial's error rate is drawn uniformly from [p, p_max), keyed by
+                              (seed, trial index); jbp_simulate only; 0 = every trial at p */
     int learned_from;      /* > 0: from this iteration on, a stalled trial (decisions unchanged or
                               oscillating) first tries the learned flip proposal set with
                               jbp_set_flip_model (resident engine, post-processing on); 0 = off */

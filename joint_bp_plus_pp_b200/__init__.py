@@ -39,7 +39,7 @@ class COptions(ctypes.Structure):
                 ("check_warmup", ctypes.c_int), ("check_interval", ctypes.c_int), ("slots", ctypes.c_int),
                 ("iters_per_launch", ctypes.c_int), ("watchdog_ms", ctypes.c_int), ("profile", ctypes.c_int),
                 ("use_prior", ctypes.c_int), ("prior", ctypes.c_double * 4), ("engine", ctypes.c_int),
-                ("learned_from", ctypes.c_int)]
+                ("p_max", ctypes.c_double), ("learned_from", ctypes.c_int)]
 
 
 TRIAL_DTYPE = np.dtype([("iterations", np.int32), ("syndrome_ok", np.uint8), ("bp_ok", np.uint8),
@@ -87,13 +87,14 @@ class Options:
     prior: tuple = None    # (I, X, Z, Y) probabilities used as given instead of those of p
     engine: str = "auto"   # "auto", "resident" (shared-memory trial-resident tier) or "slots"
     learned_from: int = 0  # > 0: stalled trials try the learned flip proposal from this iteration
+    p_max: float = 0.0     # > p: per-trial error rate uniform in [p, p_max) (simulate)
 
     def to_c(self):
         pr = (ctypes.c_double * 4)(*(self.prior or (0.0, 0.0, 0.0, 0.0)))
         return COptions(PREC[self.precision], self.max_iter, self.damping, self.flip_hist, int(self.enable_pp),
                         int(self.freeze_syn), self.check_warmup, self.check_interval, self.slots,
                         self.iters_per_launch, self.watchdog_ms, int(self.profile), int(self.prior is not None), pr,
-                        ENGINE[self.engine], int(self.learned_from))
+                        ENGINE[self.engine], float(self.p_max), int(self.learned_from))
 
 
 _lib = None

@@ -51,6 +51,29 @@ def host_cxx():
     raise RuntimeError("g++ not found")
 
 
+# Register spills of the trial-resident kernels above this (bytes of spill stores) fail the
+# build: their 768-thread blocks run at 80 registers per thread, and spills in the BP loop
+# have cost more than half of the throughput before.
+RESIDENT_SPILL_LIMIT = 512
+
+
+def check_resident_spills(log):
+    """Raises if a k_resident instantiation reports more spill stores than the limit."""
+    import re
+    cur = None
+    for line in log.splitlines():
+        m = re.search(r"Function properties for (\S*k_resident\S*)", line)
+        if m:
+            cur = m.group(1)
+            continue
+        m = re.search(r"(\d+) bytes spill stores", line)
+        if cur and m:
+            if int(m.group(1)) > RESIDENT_SPILL_LIMIT:
+                raise RuntimeError(f"{cur}: {m.group(1)} bytes of register spill stores "
+                                   f"(limit {RESIDENT_SPILL_LIMIT})")
+            cur = None
+
+
 def _compile(src, force):
     out = OBJ / (Path(src).name + ".o")
     srcp = CSRC / src
@@ -58,12 +81,18 @@ def _compile(src, force):
     if not force and out.exists() and all(out.stat().st_mtime >= d.stat().st_mtime for d in deps):
         return out, None
     if src.endswith(".cu"):
-        cmd = [nvcc()] + NVFLAGS + ["-c", str(srcp), "-o", str(out)]
+        cmd = [nvcc()] + NVFLAGS + (["-Xptxas", "-v"] if src == "engine.cu" else []) + ["-c", str(srcp), "-o", str(out)]
     else:
         cmd = [host_cxx()] + HOSTFLAGS + [f"-I{cuda_home()}/include", "-c", str(srcp), "-o", str(out)]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"compile failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    if src == "engine.cu":
+        try:
+            check_resident_spills(r.stdout + r.stderr)
+        except RuntimeError:
+            out.unlink(missing_ok=True)
+            raise
     return out, (r.stdout + r.stderr).strip() or None
 
 

@@ -59,6 +59,8 @@ int finish_create(jbp::CodeModel &&m, const std::string &ets_dir, int device, jb
     auto ctx = std::make_unique<jbp_ctx>();
     std::string e = ctx->engine.init(std::move(m), device);
     if (!e.empty()) return fail(JBP_ERR_CUDA, e);
+    cudaError_t ce = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(ce, "cudaStreamCreate"));
     *out = ctx.release();
     return JBP_OK;
 }
@@ -153,6 +155,7 @@ int jbp_simulate(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed, long long 
     rq.first_trial = first_trial;
     rq.ntrials = ntrials;
     rq.p = p;
+    rq.stream = ctx->stream;
     cudaSetDevice(ctx->engine.device());
     if (per_trial) {
         if (int rc = grow(&ctx->d_res, &ctx->res_count, static_cast<size_t>(ntrials))) return rc;
@@ -161,7 +164,7 @@ int jbp_simulate(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed, long long 
     if (iter_hist) {
         if (rq.opt.max_iter < 1) return fail(JBP_ERR_ARG, "max_iter must be >= 1");
         if (int rc = grow(&ctx->d_hist, &ctx->hist_count, static_cast<size_t>(rq.opt.max_iter) + 1)) return rc;
-        cudaMemset(ctx->d_hist, 0, sizeof(unsigned long long) * (rq.opt.max_iter + 1));
+        cudaMemsetAsync(ctx->d_hist, 0, sizeof(unsigned long long) * (rq.opt.max_iter + 1), ctx->stream);
         rq.d_hist = ctx->d_hist;
     }
     jbp_stats st;
@@ -211,7 +214,9 @@ static int decode_host(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, 
         const long long cnt = std::min(chunk, ntrials - base);
         jbp::RunRequest rq;
         rq.opt = normalized(opt);
+        rq.opt.p_max = 0.0;   // known inputs: every trial decodes with the given p
         rq.p = p;
+        rq.stream = ctx->stream;
         rq.first_trial = 0;
         rq.ntrials = cnt;
         cudaError_t ce;
@@ -284,6 +289,7 @@ int jbp_collect_stall_states(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed
     rq.first_trial = first_trial;
     rq.ntrials = ntrials;
     rq.p = p;
+    rq.stream = ctx->stream;
     rq.collect = true;
     rq.col_cap = capacity;
     cudaSetDevice(ctx->engine.device());
@@ -292,7 +298,7 @@ int jbp_collect_stall_states(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed
     cudaError_t ce = cudaMalloc(&dx, sizeof(float) * 8 * capacity);
     if (ce == cudaSuccess) ce = cudaMalloc(&dy, sizeof(float) * 2 * capacity);
     if (ce == cudaSuccess) ce = cudaMalloc(&dc, sizeof(unsigned long long));
-    if (ce == cudaSuccess) ce = cudaMemset(dc, 0, sizeof(unsigned long long));
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(dc, 0, sizeof(unsigned long long), ctx->stream);
     std::string e;
     jbp_stats st;
     std::memset(&st, 0, sizeof(st));
@@ -337,6 +343,7 @@ int jbp_decode_errors_device(jbp_ctx *ctx, const jbp_options *opt, long long ntr
     if (!ctx || !d_err || !d_res || ntrials < 0) return fail(JBP_ERR_ARG, "invalid argument");
     jbp::RunRequest rq;
     rq.opt = normalized(opt);
+    rq.opt.p_max = 0.0;
     rq.source = jbp::kSrcErrors;
     rq.first_trial = 0;
     rq.ntrials = ntrials;

@@ -53,8 +53,9 @@ void finish_side(SideGraph &g, int n) {
     for (int c = 0; c < g.m; ++c) g.dc_max = std::max(g.dc_max, g.chk_off[c + 1] - g.chk_off[c]);
     g.dv_max = 0;
     for (int v = 0; v < n; ++v) g.dv_max = std::max(g.dv_max, deg[v]);
-    g.regular = true;
-    for (int c = 0; c < g.m && g.regular; ++c) g.regular = (g.chk_off[c + 1] - g.chk_off[c]) == g.dc_max;
+    g.checks_regular = true;
+    for (int c = 0; c < g.m && g.checks_regular; ++c) g.checks_regular = (g.chk_off[c + 1] - g.chk_off[c]) == g.dc_max;
+    g.regular = g.checks_regular;
     for (int v = 0; v < n && g.regular; ++v) g.regular = deg[v] == g.dv_max;
 }
 

@@ -22,6 +22,7 @@ struct SideGraph {
     std::vector<int> var_edge;    // edges of each variable, ascending check index
     int dc_max = 0, dv_max = 0;
     bool regular = false;         // every check has dc_max edges and every variable dv_max
+    bool checks_regular = false;  // every check has dc_max edges (variables may have fewer than dv_max)
 };
 
 // GF(2) basis of a check matrix's row space: rows reduced at their highest bit.

@@ -11,6 +11,9 @@
 
 struct jbp_ctx {
     jbp::Engine engine;
+    // the context's own non-blocking stream for the host-buffer calls, so that contexts used
+    // from different host threads decode concurrently on one device
+    cudaStream_t stream = nullptr;
     // cached device staging for host-buffer calls
     uint8_t *d_in = nullptr, *d_in2 = nullptr, *d_est = nullptr;
     size_t in_bytes = 0, in2_bytes = 0, est_bytes = 0;
@@ -19,6 +22,7 @@ struct jbp_ctx {
     unsigned long long *d_hist = nullptr;
     size_t hist_count = 0;
     ~jbp_ctx() {
+        if (stream) cudaStreamDestroy(stream);
         cudaFree(d_in);
         cudaFree(d_in2);
         cudaFree(d_est);

@@ -72,6 +72,7 @@ bool select_kernels(int dc, int dv, int precision, bool damp, KernelSet &k) {
 #define JBP_CASE(DC, DV) \
     if (dc == DC && dv == DV) { k = kernels_for<DC, DV>(precision, damp); return true; }
     JBP_CASE(12, 3)
+    JBP_CASE(7, 4)
     JBP_CASE(8, 3)
     JBP_CASE(6, 3)
     JBP_CASE(4, 2)
@@ -144,7 +145,12 @@ std::string Engine::init(CodeModel model, int device) {
         std::string e = dev_upload(code_allocs_, g.chk_var, &p);
         if (!e.empty()) return e;
         d.chk_var = p;
-        e = dev_upload(code_allocs_, g.var_edge, &p);
+        // per-variable edge lists padded to dv_max with -1 (variables of lower degree)
+        std::vector<int> ve(static_cast<size_t>(model_.n) * std::max(1, g.dv_max), -1);
+        for (int v = 0; v < model_.n; ++v)
+            for (int k = g.var_off[v]; k < g.var_off[v + 1]; ++k)
+                ve[static_cast<size_t>(v) * g.dv_max + (k - g.var_off[v])] = g.var_edge[k];
+        e = dev_upload(code_allocs_, ve, &p);
         if (!e.empty()) return e;
         d.var_edge = p;
         uint64_t *rows = nullptr;
@@ -310,6 +316,7 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     r.check_interval = std::max(1, o.check_interval);
     r.source = rq.source;
     r.p = rq.p;
+    r.p_max = o.p_max;
     r.use_prior = o.use_prior ? 1 : 0;
     for (int i = 0; i < 4; ++i) r.prior4[i] = o.prior[i];
     r.seed = rq.seed;
@@ -367,7 +374,7 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
 void Engine::free_buffers() {
     for (void *&p : buf_.msg) { cudaFree(p); p = nullptr; }
     cudaFree(buf_.trial); cudaFree(buf_.iter); cudaFree(buf_.flags); cudaFree(buf_.frz); cudaFree(buf_.unsat);
-    cudaFree(buf_.prior); cudaFree(buf_.lprior); cudaFree(buf_.err);
+    cudaFree(buf_.prior); cudaFree(buf_.lprior); cudaFree(buf_.err); cudaFree(buf_.slot_p);
     cudaFree(buf_.unsat_mask); cudaFree(buf_.estx); cudaFree(buf_.estz); cudaFree(buf_.synm);
     cudaFree(buf_.res_iters); cudaFree(buf_.res_flags); cudaFree(buf_.lists); cudaFree(buf_.counts);
     cudaFree(buf_.cnt);
@@ -417,7 +424,7 @@ std::string Engine::upload_ets() {
     return "";
 }
 
-std::string Engine::ensure_buffers(int S, int precision, bool damp, bool pp, int R) {
+std::string Engine::ensure_buffers(int S, int precision, bool damp, bool pp, int R, cudaStream_t st) {
     if (buf_.S == S && buf_.precision == precision && buf_.damp == damp && buf_.pp == pp && buf_.R == R) return "";
     free_buffers();
     const int n = model_.n, M = model_.side[0].m + model_.side[1].m;
@@ -435,6 +442,7 @@ std::string Engine::ensure_buffers(int S, int precision, bool damp, bool pp, int
     JBP_CUDA_TRY(cudaMalloc(&buf_.frz, sizeof(int) * S), "cudaMalloc(slots)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.unsat, sizeof(int) * 2 * S), "cudaMalloc(slots)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.prior, sizeof(double) * 4 * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(cudaMalloc(&buf_.slot_p, sizeof(double) * S), "cudaMalloc(slots)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.lprior, sizeof(float) * 8 * S), "cudaMalloc(slots)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.err, static_cast<size_t>(n) * S), "cudaMalloc(err)");
     const size_t G = static_cast<size_t>(S) / kGroup;
@@ -452,14 +460,14 @@ std::string Engine::ensure_buffers(int S, int precision, bool damp, bool pp, int
         JBP_CUDA_TRY(cudaMalloc(&buf_.us_hist, sizeof(unsigned short) * 100 * S), "cudaMalloc(pp)");
         JBP_CUDA_TRY(cudaMalloc(&buf_.dprev, sizeof(unsigned) * G), "cudaMalloc(pp)");
         JBP_CUDA_TRY(cudaMalloc(&buf_.dpprev, sizeof(unsigned) * G), "cudaMalloc(pp)");
-        JBP_CUDA_TRY(cudaMemset(buf_.dprev, 0, sizeof(unsigned) * G), "memset(pp)");
-        JBP_CUDA_TRY(cudaMemset(buf_.dpprev, 0, sizeof(unsigned) * G), "memset(pp)");
+        JBP_CUDA_TRY(cudaMemsetAsync(buf_.dprev, 0, sizeof(unsigned) * G, st), "memset(pp)");
+        JBP_CUDA_TRY(cudaMemsetAsync(buf_.dpprev, 0, sizeof(unsigned) * G, st), "memset(pp)");
         buf_.pp_stride = pp_scratch_bytes(n, mmax);
         buf_.pp_blocks = std::min(sm_count_, static_cast<int>(S));
         JBP_CUDA_TRY(cudaMalloc(&buf_.pp_scratch, buf_.pp_stride * buf_.pp_blocks), "cudaMalloc(pp scratch)");
     }
     JBP_CUDA_TRY(cudaMalloc(&buf_.synm, sizeof(unsigned) * G * M), "cudaMalloc(syn)");
-    JBP_CUDA_TRY(cudaMemset(buf_.synm, 0, sizeof(unsigned) * G * M), "memset(syn)");
+    JBP_CUDA_TRY(cudaMemsetAsync(buf_.synm, 0, sizeof(unsigned) * G * M, st), "memset(syn)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.unsat_mask, sizeof(unsigned) * 2 * G), "cudaMalloc(unsat)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.res_iters, sizeof(int) * S), "cudaMalloc(slots)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.res_flags, sizeof(int) * S), "cudaMalloc(slots)");
@@ -467,6 +475,8 @@ std::string Engine::ensure_buffers(int S, int precision, bool damp, bool pp, int
     JBP_CUDA_TRY(cudaMalloc(&buf_.counts, sizeof(int) * 4), "cudaMalloc(lists)");
     JBP_CUDA_TRY(cudaMalloc(&buf_.cnt, sizeof(DevCounters)), "cudaMalloc(counters)");
     JBP_CUDA_TRY(cudaMallocHost(&buf_.h_done, sizeof(unsigned long long) * 2), "cudaMallocHost");
+    // the memsets above are ordered on the run's stream (no device-wide synchronization: another
+    // context may be capturing a graph on another host thread)
     buf_.S = S;
     buf_.precision = precision;
     buf_.damp = damp;
@@ -497,6 +507,7 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
         return "p must be in (0, 1)";
     }
     if (o.damping < 0.0 || o.damping > 1.0) return "damping must be in [0, 1]";
+    if (o.p_max > rq.p && !(o.p_max < 1.0)) return "p_max must be below 1";
     if (o.engine < JBP_ENGINE_AUTO || o.engine > JBP_ENGINE_SLOTS) return "unknown engine";
     if (o.engine != JBP_ENGINE_SLOTS) {
         std::string why;
@@ -506,8 +517,8 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     }
     if (o.learned_from > 0 || rq.collect) return "learned flip proposals are not available on the slot engine";
     const SideGraph &gx = model_.side[0], &gz = model_.side[1];
-    if (!gx.regular || !gz.regular || gx.dc_max != gz.dc_max || gx.dv_max != gz.dv_max)
-        return "the GPU kernels need a code with equal regular degrees on both sides";
+    if (!gx.checks_regular || !gz.checks_regular || gx.dc_max != gz.dc_max || gx.dv_max != gz.dv_max)
+        return "the GPU kernels need a code whose checks all have one degree and whose sides have equal degrees";
     const bool pp = o.enable_pp != 0;
     if (pp && (o.check_interval != 1 || o.check_warmup != 0))
         return "post-processing needs a syndrome test every iteration (check interval 1, warmup 0)";
@@ -529,7 +540,7 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
         std::string ee = upload_ets();
         if (!ee.empty()) return ee;
     }
-    std::string e = ensure_buffers(S, o.precision, damp, pp, R);
+    std::string e = ensure_buffers(S, o.precision, damp, pp, R, rq.stream);
     if (!e.empty()) return e;
 
     cudaStream_t st = rq.stream;
@@ -541,6 +552,8 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     r.check_interval = std::max(1, o.check_interval);
     r.source = rq.source;
     r.p = rq.p;
+    r.p_max = o.p_max;
+    r.slot_p = buf_.slot_p;
     r.seed = rq.seed;
     r.first_trial = rq.first_trial;
     r.ntrials = rq.ntrials;
@@ -787,7 +800,7 @@ std::string Engine::sample_errors(unsigned long long seed, long long first, long
     JBP_CUDA_TRY(cudaSetDevice(device_), "cudaSetDevice");
     k_sample_out<<<sm_count_ * 4, 256>>>(model_.n, seed, first, count, p, source, d_out);
     JBP_CUDA_TRY(cudaGetLastError(), "sample launch");
-    JBP_CUDA_TRY(cudaDeviceSynchronize(), "sample");
+    JBP_CUDA_TRY(cudaStreamSynchronize(nullptr), "sample");
     return "";
 }
 

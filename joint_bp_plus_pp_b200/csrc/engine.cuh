@@ -33,7 +33,7 @@ enum SourceKind : int {
 struct DevSide {
     int m, edges, dc, dv;
     const int *chk_var;             // [edges], edge = c * dc + position
-    const int *var_edge;            // [n * dv], ascending check
+    const int *var_edge;            // [n * dv], ascending check; -1 pads variables of lower degree
 };
 
 struct DevCode {
@@ -95,7 +95,7 @@ struct DevRun {
     int S;                          // slots
     int max_iter, check_warmup, check_interval;
     int source;
-    double p;
+    double p, p_max;                // p_max > p: per-trial p uniform in [p, p_max) (trial_p)
     unsigned long long seed;
     long long first_trial, ntrials;
     const uint8_t *src_err;         // [ntrials][n]
@@ -110,6 +110,7 @@ struct DevRun {
     int *unsat;                     // [2][S] unsatisfied-check counts (kept when PP needs them)
     unsigned *unsat_mask;           // [2][G] slots of a group with an unsatisfied check, per side
     double *prior;                  // [S][4] normalized prior (FP64 path)
+    double *slot_p;                 // [S] error rate of the slot's trial
     float *lprior;                  // [S][8] log prior x4, prior LLR x/z (FP32 path)
     uint8_t *err;                   // [S][n] true error of the slot's trial
     // Hard decisions as bit planes: bit (slot % 32) of plane[g * n + v] is the x-bit (estx)

@@ -62,7 +62,7 @@ private:
         long long *trial = nullptr;
         int *iter = nullptr, *flags = nullptr, *frz = nullptr, *unsat = nullptr;
         unsigned *unsat_mask = nullptr, *estx = nullptr, *estz = nullptr, *synm = nullptr;
-        double *prior = nullptr;
+        double *prior = nullptr, *slot_p = nullptr;
         float *lprior = nullptr;
         uint8_t *err = nullptr;
         int *res_iters = nullptr, *res_flags = nullptr;
@@ -88,7 +88,7 @@ private:
     std::string run_resident(const RunRequest &rq, jbp_stats &stats);
     std::string build_res_code();
 
-    std::string ensure_buffers(int S, int precision, bool damp, bool pp, int R);
+    std::string ensure_buffers(int S, int precision, bool damp, bool pp, int R, cudaStream_t st);
     std::string upload_ets();
     void free_buffers();
     int choose_slots(const jbp_options &opt, long long ntrials) const;

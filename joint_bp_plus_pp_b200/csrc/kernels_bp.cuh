@@ -225,16 +225,21 @@ __global__ void __launch_bounds__(256) k_var_f64(DevCode code, DevRun run, DevMs
             const double *pr = run.prior + 4 * slot;
             const double p0 = pr[0], p1 = pr[1], p2 = pr[2], p3 = pr[3];
             size_t ox[DV], oz[DV];
+            bool vx[DV], vz[DV];   // edge present (a variable of lower degree is padded with -1)
             double ax[DV], bx[DV], az[DV], bz[DV];
 #pragma unroll
             for (int k = 0; k < DV; ++k) {
-                ox[k] = msg_off<DC>(__ldg(code.s[0].var_edge + v * DV + k), G, group, lane);
-                oz[k] = msg_off<DC>(__ldg(code.s[1].var_edge + v * DV + k), G, group, lane);
+                const int ex = __ldg(code.s[0].var_edge + v * DV + k), ez = __ldg(code.s[1].var_edge + v * DV + k);
+                vx[k] = ex >= 0;
+                vz[k] = ez >= 0;
+                ox[k] = vx[k] ? msg_off<DC>(ex, G, group, lane) : 0;
+                oz[k] = vz[k] ? msg_off<DC>(ez, G, group, lane) : 0;
             }
+            // a padded edge is the identity message (1, 1, 1, 1): products are unchanged exactly
 #pragma unroll
             for (int k = 0; k < DV; ++k) {
-                const double2 cx = c2vx[ox[k]];
-                const double2 cz = c2vz[oz[k]];
+                const double2 cx = vx[k] ? c2vx[ox[k]] : make_double2(1.0, 1.0);
+                const double2 cz = vz[k] ? c2vz[oz[k]] : make_double2(1.0, 1.0);
                 ax[k] = cx.x; bx[k] = cx.y; az[k] = cz.x; bz[k] = cz.y;
             }
             // prefix / suffix products of the X messages (a, b, a, b) and Z messages (a, a, b, b)
@@ -278,6 +283,7 @@ __global__ void __launch_bounds__(256) k_var_f64(DevCode code, DevRun run, DevMs
 #pragma unroll
             for (int k = 0; k < DV; ++k) {
                 if (frz & 1) break;
+                if (!vx[k]) continue;
                 const double EA = dmul(PA[k], SA[k + 1]), EB = dmul(PB[k], SB[k + 1]);
                 double n0 = dmul(dmul(p0, EA), ZA), n1 = dmul(dmul(p1, EB), ZA);
                 double n2 = dmul(dmul(p2, EA), ZB), n3 = dmul(dmul(p3, EB), ZB);
@@ -287,6 +293,7 @@ __global__ void __launch_bounds__(256) k_var_f64(DevCode code, DevRun run, DevMs
 #pragma unroll
             for (int k = 0; k < DV; ++k) {
                 if (frz & 2) break;
+                if (!vz[k]) continue;
                 const double FA = dmul(QA[k], TA[k + 1]), FB = dmul(QB[k], TB[k + 1]);
                 double n0 = dmul(dmul(p0, XA), FA), n1 = dmul(dmul(p1, XB), FA);
                 double n2 = dmul(dmul(p2, XA), FB), n3 = dmul(dmul(p3, XB), FB);
@@ -421,16 +428,20 @@ __device__ __forceinline__ int var_llr_one(const DevCode &code, const DevRun &ru
     T *v2cx = static_cast<T *>(msg.v2c[0]);
     T *v2cz = static_cast<T *>(msg.v2c[1]);
     size_t ox[DV], oz[DV];
+    bool vx[DV], vz[DV];   // edge present (a variable of lower degree is padded with -1)
     float lx[DV], lz[DV];
 #pragma unroll
     for (int k = 0; k < DV; ++k) {
-        ox[k] = msg_off<DC>(__ldg(code.s[0].var_edge + v * DV + k), G, group, lane);
-        oz[k] = msg_off<DC>(__ldg(code.s[1].var_edge + v * DV + k), G, group, lane);
+        const int ex = __ldg(code.s[0].var_edge + v * DV + k), ez = __ldg(code.s[1].var_edge + v * DV + k);
+        vx[k] = ex >= 0;
+        vz[k] = ez >= 0;
+        ox[k] = vx[k] ? msg_off<DC>(ex, G, group, lane) : 0;
+        oz[k] = vz[k] ? msg_off<DC>(ez, G, group, lane) : 0;
     }
 #pragma unroll
     for (int k = 0; k < DV; ++k) {
-        lx[k] = ld_msg<T>(c2vx + ox[k]);
-        lz[k] = ld_msg<T>(c2vz + oz[k]);
+        lx[k] = vx[k] ? ld_msg<T>(c2vx + ox[k]) : 0.0f;
+        lz[k] = vz[k] ? ld_msg<T>(c2vz + oz[k]) : 0.0f;
     }
     float Lam = 0.0f, Mu = 0.0f;
 #pragma unroll
@@ -467,8 +478,8 @@ __device__ __forceinline__ int var_llr_one(const DevCode &code, const DevRun &ru
             ox_v = clamp_llr(lg2_approx(fmaxf(qx0, 1e-30f)) - lg2_approx(fmaxf(qx1, 1e-30f)));
             oz_v = clamp_llr(lg2_approx(fmaxf(qz0, 1e-30f)) - lg2_approx(fmaxf(qz1, 1e-30f)));
         }
-        if (!(frz & 1)) st_msg<T>(v2cx + ox[k], ox_v);
-        if (!(frz & 2)) st_msg<T>(v2cz + oz[k], oz_v);
+        if (!(frz & 1) && vx[k]) st_msg<T>(v2cx + ox[k], ox_v);
+        if (!(frz & 2) && vz[k]) st_msg<T>(v2cz + oz[k], oz_v);
     }
     return best;
 }

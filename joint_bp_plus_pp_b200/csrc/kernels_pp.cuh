@@ -121,10 +121,11 @@ __device__ __forceinline__ PpShared pp_shared_carve(unsigned char *base, int n, 
 
 __device__ __forceinline__ int side_bit(int state, int side) { return (state >> side) & 1; }
 
-// Check (row of `side`) of a variable's k-th edge on that side.
+// Check (row of `side`) of a variable's k-th edge on that side, or -1 past its degree.
 __device__ __forceinline__ int var_check(const DevCode &code, int side, int v, int k) {
     const DevSide &g = code.s[side];
-    return __ldg(g.var_edge + v * g.dv + k) / g.dc;
+    const int e = __ldg(g.var_edge + v * g.dv + k);
+    return e >= 0 ? e / g.dc : -1;
 }
 
 // diff = side syndrome of est xor target; returns the number of unsatisfied checks and
@@ -205,6 +206,7 @@ static __device__ bool blk_ets_table(const DevCode &code, const DevEts &ets, con
             for (int i = 0; i < nv; ++i)
                 for (int k = 0; k < dv; ++k) {
                     const int c = var_check(code, side, vars[i], k);
+                    if (c < 0) continue;
                     bool seen = false;
                     for (int j = 0; j < nch; ++j) seen |= checks[j] == c;
                     if (!seen) checks[nch++] = c;
@@ -303,7 +305,10 @@ static __device__ bool blk_flip_attempt(const DevCode &code, const PpShared &sh,
     __syncthreads();
     if (nv == 0) return false;
     for (int i = threadIdx.x; i < nv; i += blockDim.x)
-        for (int k = 0; k < dv; ++k) sh.touch[var_check(code, side, sc.list[i], k)] = 1;
+        for (int k = 0; k < dv; ++k) {
+            const int c = var_check(code, side, sc.list[i], k);
+            if (c >= 0) sh.touch[c] = 1;
+        }
     __syncthreads();
     // every unsatisfied check must be covered; covered checks become rows
     const int cper = (m + blockDim.x - 1) / blockDim.x;
@@ -505,14 +510,14 @@ static __device__ bool blk_osd_side(const DevCode &code, const double *llr, cons
         if (threadIdx.x == 0) {
             for (int k = 0; k < dv; ++k) {
                 const int c = var_check(code, side, var, k);
-                sh.wv[c >> 6] ^= 1ull << (c & 63);
+                if (c >= 0) sh.wv[c >> 6] ^= 1ull << (c & 63);
             }
             sh.wc[j >> 6] |= 1ull << (j & 63);
         }
         __syncthreads();
         for (int k = 0; k < dv; ++k) {
             const int c = var_check(code, side, var, k);
-            const int b = sc.piv[c];
+            const int b = c >= 0 ? sc.piv[c] : -1;
             if (b >= 0) {
                 const uint64_t *bv = sc.vec + static_cast<size_t>(b) * MW, *bc = sc.comb + static_cast<size_t>(b) * CW;
                 for (int w = threadIdx.x; w < MW; w += blockDim.x) sh.wv[w] ^= bv[w];

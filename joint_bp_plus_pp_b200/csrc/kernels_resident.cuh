@@ -64,7 +64,7 @@ struct ResCode {
 struct ResRun {
     int max_iter, check_warmup, check_interval;
     int source;
-    double p;
+    double p, p_max;               // p_max > p: per-trial p uniform in [p, p_max) (trial_p)
     int use_prior;
     double prior4[4];
     unsigned long long seed;
@@ -394,7 +394,10 @@ __device__ void res_features(const ResCode &code, const DevCode &dc, const typen
         blk_side_diff(dc, psh, side);
         for (int v = threadIdx.x; v < n; v += blockDim.x) {
             int u = 0;
-            for (int k = 0; k < dc.s[side].dv; ++k) u += psh.diff[var_check(dc, side, v, k)];
+            for (int k = 0; k < dc.s[side].dv; ++k) {
+                const int c = var_check(dc, side, v, k);
+                if (c >= 0) u += psh.diff[c];
+            }
             feat[static_cast<size_t>(v) * kMlpIn + 6 + side] = u * (1.0f / 3.0f);
         }
         __syncthreads();
@@ -619,6 +622,27 @@ __device__ __noinline__ int res_slow_step(const ResCode &code, const ResRun &run
     return it >= run.max_iter ? -1 : 0;
 }
 
+// Prior of a trial (error rate pt; thread 0, once per run or per trial; out of line): FP64 as
+// the slot engine's refill, then its log2 weights and probabilities in FP32.
+__device__ __noinline__ void res_set_prior(const ResRun &run, double pt, float4 *lp, float4 *pr, float *lpx,
+                                           float *lpz) {
+    double q[4];
+    if (run.use_prior) {
+        for (int i = 0; i < 4; ++i) q[i] = run.prior4[i];
+    } else {
+        q[0] = 1.0 - pt; q[1] = pt / 3.0; q[2] = q[1]; q[3] = q[1];
+        const double s = ((q[0] + q[1]) + q[2]) + q[3];
+        for (int i = 0; i < 4; ++i) q[i] = s > 0.0 ? q[i] / s : 0.25;
+    }
+    for (int i = 0; i < 4; ++i) q[i] = fmax(q[i], 1e-30);
+    *lp = make_float4(static_cast<float>(log2(q[0])), static_cast<float>(log2(q[1])), static_cast<float>(log2(q[2])),
+                      static_cast<float>(log2(q[3])));
+    *pr = make_float4(static_cast<float>(q[0]), static_cast<float>(q[1]), static_cast<float>(q[2]),
+                      static_cast<float>(q[3]));
+    *lpx = static_cast<float>(log2((q[0] + q[2]) / (q[1] + q[3])));
+    *lpz = static_cast<float>(log2((q[0] + q[1]) / (q[2] + q[3])));
+}
+
 template <int P, int J, int L, class ST, bool PP, bool LEARNED>
 __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRun run) {
     extern __shared__ __align__(16) unsigned char res_smem[];
@@ -643,23 +667,9 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
     const int llr_from = min(100, run.max_iter);
     const int slow_from = PP ? max(1, llr_from - 2) : 0x7fffffff;
 
-    // prior: FP64 as the slot engine's refill, then its log2 weights and probabilities in FP32
+    __shared__ double pt_sh;
     if (threadIdx.x == 0) {
-        double q[4];
-        if (run.use_prior) {
-            for (int i = 0; i < 4; ++i) q[i] = run.prior4[i];
-        } else {
-            q[0] = 1.0 - run.p; q[1] = run.p / 3.0; q[2] = q[1]; q[3] = q[1];
-            const double s = ((q[0] + q[1]) + q[2]) + q[3];
-            for (int i = 0; i < 4; ++i) q[i] = s > 0.0 ? q[i] / s : 0.25;
-        }
-        for (int i = 0; i < 4; ++i) q[i] = fmax(q[i], 1e-30);
-        lp_sh = make_float4(static_cast<float>(log2(q[0])), static_cast<float>(log2(q[1])),
-                            static_cast<float>(log2(q[2])), static_cast<float>(log2(q[3])));
-        pr_sh = make_float4(static_cast<float>(q[0]), static_cast<float>(q[1]), static_cast<float>(q[2]),
-                            static_cast<float>(q[3]));
-        lpx_sh = static_cast<float>(log2((q[0] + q[2]) / (q[1] + q[3])));
-        lpz_sh = static_cast<float>(log2((q[0] + q[1]) / (q[2] + q[3])));
+        res_set_prior(run, run.p, &lp_sh, &pr_sh, &lpx_sh, &lpz_sh);
         for (int i = 0; i < 16; ++i) ints[i] = 0;
     }
     __syncthreads();
@@ -678,13 +688,23 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
         if (k < 0) break;
         const long long t = run.trial_list ? run.trial_list[k] : run.first_trial + k;
         const long long local = t - run.first_trial;
+        if (run.p_max > run.p) {
+            if (threadIdx.x == 0) {
+                pt_sh = trial_p(run.p, run.p_max, run.seed, t);
+                res_set_prior(run, pt_sh, &lp_sh, &pr_sh, &lpx_sh, &lpz_sh);
+            }
+            __syncthreads();
+        } else if (threadIdx.x == 0) {
+            pt_sh = run.p;
+        }
+        const double pt = run.p_max > run.p ? pt_sh : run.p;
 
         // ---- error and target syndrome
         for (int w = threadIdx.x; w < 2 * mw; w += blockDim.x) syn[w] = 0u;
         if (run.source == kSrcPhilox) {
             for (int v2 = threadIdx.x; 2 * v2 < n; v2 += blockDim.x) {
                 uint8_t e0, e1;
-                sample_philox_pair(run.seed, t, v2, run.p, e0, e1);
+                sample_philox_pair(run.seed, t, v2, pt, e0, e1);
                 err[2 * v2] = e0;
                 if (2 * v2 + 1 < n) err[2 * v2 + 1] = e1;
             }
@@ -710,7 +730,7 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
                 }
             }
         } else if (run.source == kSrcMt19937) {
-            if (threadIdx.x < 32) warp_mt_trial(reinterpret_cast<unsigned long long *>(A), run.seed, t, run.p, n, err);
+            if (threadIdx.x < 32) warp_mt_trial(reinterpret_cast<unsigned long long *>(A), run.seed, t, pt, n, err);
         }
         __syncthreads();
         if (run.source == kSrcSyndromes) {

@@ -58,6 +58,18 @@ __device__ __forceinline__ void sample_philox_pair(unsigned long long seed, long
     e1 = pauli_from_uniform(static_cast<double>(x1 >> 11) * 0x1.0p-53, p);
 }
 
+// Error rate of trial t: p, or with p_max > p a uniform draw from [p, p_max) keyed by
+// (seed, t) (its own Philox stream, independent of the error samples).
+__device__ __forceinline__ double trial_p(double p, double p_max, unsigned long long seed, long long t) {
+    if (!(p_max > p)) return p;
+    const uint4 r = philox4x32_10(make_uint4(0xFFFFFFFFu, static_cast<uint32_t>(t),
+                                             static_cast<uint32_t>(static_cast<unsigned long long>(t) >> 32),
+                                             0x50524154u),
+                                  make_uint2(static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32)));
+    const double u = static_cast<double>((static_cast<unsigned long long>(r.y) << 32 | r.x) >> 11) * 0x1.0p-53;
+    return p + (p_max - p) * u;
+}
+
 // ------------------------------------------------------------------ per-iteration kernels
 
 // Whether iteration k1 (1-based) of a slot ends with a syndrome test: always at max_iter,
@@ -435,7 +447,9 @@ static __global__ void k_refill(DevRun run, int precision) {
             if (run.use_prior) {
                 p0 = run.prior4[0]; p1 = run.prior4[1]; p2 = run.prior4[2]; p3 = run.prior4[3];
             } else {
-                p0 = __dsub_rn(1.0, run.p); p1 = __ddiv_rn(run.p, 3.0); p2 = p1; p3 = p1;
+                const double pt = trial_p(run.p, run.p_max, run.seed, run.trial[slot]);
+                run.slot_p[slot] = pt;
+                p0 = __dsub_rn(1.0, pt); p1 = __ddiv_rn(pt, 3.0); p2 = p1; p3 = p1;
                 const double s = __dadd_rn(__dadd_rn(__dadd_rn(p0, p1), p2), p3);
                 if (s <= 0.0) { p0 = p1 = p2 = p3 = 0.25; }
                 else { p0 = __ddiv_rn(p0, s); p1 = __ddiv_rn(p1, s); p2 = __ddiv_rn(p2, s); p3 = __ddiv_rn(p3, s); }
@@ -474,7 +488,7 @@ static __global__ void k_sample(DevCode code, DevRun run) {
         const int slot = run.fresh[f];
         const long long t = run.trial[slot];
         uint8_t e = 0;
-        if (run.source == kSrcPhilox) e = sample_philox(run.seed, t, v, run.p);
+        if (run.source == kSrcPhilox) e = sample_philox(run.seed, t, v, run.slot_p[slot]);
         else if (run.source == kSrcErrors) {
             e = run.src_err[(t - run.first_trial) * n + v];
             if (e > 3) { atomicAdd(&run.cnt->bad_input, 1ull); e &= 3; }
@@ -547,7 +561,8 @@ static __global__ void k_sample_mt(DevCode code, DevRun run) {
     const int nf = *run.n_fresh;
     for (int f = blockIdx.x * 8 + wib; f < nf; f += gridDim.x * 8) {
         const int slot = run.fresh[f];
-        warp_mt_trial(st[wib], run.seed, run.trial[slot], run.p, code.n, run.err + static_cast<size_t>(slot) * code.n);
+        warp_mt_trial(st[wib], run.seed, run.trial[slot], run.slot_p[slot], code.n,
+                      run.err + static_cast<size_t>(slot) * code.n);
     }
 }
 

@@ -104,6 +104,7 @@ size_t layout(const jbp::DevCode &code, int S, int precision, unsigned char *bas
     r.unsat = cv.take<int>(2 * S);
     r.unsat_mask = cv.take<unsigned>(2 * G);
     r.prior = cv.take<double>(4 * S);
+    r.slot_p = cv.take<double>(S);
     r.lprior = cv.take<float>(8 * S);
     r.err = cv.take<uint8_t>(static_cast<size_t>(S) * n);
     r.estx = cv.take<unsigned>(static_cast<size_t>(G) * n);

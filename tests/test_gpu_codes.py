@@ -1,0 +1,74 @@
+"""GPU decoding of codes given as check lists with mixed variable degrees (hypergraph products
+of random (3,4)-regular classical codes), per-trial error rates, and the mixed-size batch."""
+import numpy as np
+import pytest
+
+from joint_bp_plus_pp_b200.codes import hgp_code
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def hgp():
+    from joint_bp_plus_pp_b200 import Decoder
+    from oracle_bind import Oracle
+    n, xo, xv, zo, zv = hgp_code(32, 1)
+    return Decoder.from_checks(n, xo, xv, zo, zv), Oracle.from_checks(n, xo, xv, zo, zv)
+
+
+@pytest.mark.parametrize("pp", [False, True])
+def test_fp64_hgp_bit_exact_vs_oracle(hgp, pp):
+    """FP64 on an irregular code (degree-3 and degree-4 variables padded to 4): estimates,
+    iteration counts and outcomes equal the oracle's, with and without post-processing."""
+    from joint_bp_plus_pp_b200 import Options
+    dec, orc = hgp
+    p, mi, k = 0.06, 40, 48
+    rng = np.random.default_rng(9)
+    u = rng.random((k, dec.n))
+    err = np.where(u < 1 - p, 0, 1 + ((u - (1 - p)) / p * 3).astype(int).clip(0, 2)).astype(np.uint8)
+    st, res, est = dec.decode_errors(err, p, Options(precision="fp64", max_iter=mi, enable_pp=pp))
+    assert 0 < int(res["syndrome_ok"].sum()) < k
+    for t in range(k):
+        o = orc.error_trial(err[t], p, mi, enable_pp=pp)
+        assert (o["est"] == est[t]).all(), t
+        assert (o["iterations"], o["syndrome_ok"], o["success"]) == \
+               (res["iterations"][t], res["syndrome_ok"][t], res["success"][t]), t
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+def test_llr_hgp_agrees_with_fp64(hgp, prec):
+    from joint_bp_plus_pp_b200 import Options
+    dec, _ = hgp
+    err = dec.sample_errors(3, 1, 2000, 0.03, sampler="philox")
+    _, r64, e64 = dec.decode_errors(err, 0.03, Options(precision="fp64", max_iter=100, enable_pp=False))
+    _, rlo, elo = dec.decode_errors(err, 0.03, Options(precision=prec, max_iter=100, enable_pp=False))
+    assert (e64 == elo).all(axis=1).mean() >= 0.98
+    assert abs(int(r64["success"].sum()) - int(rlo["success"].sum())) <= 10
+
+
+def test_per_trial_error_rate_range(hgp):
+    """p drawn per trial from [0.01, 0.06): the failure rate lies between those of fixed 0.01
+    and 0.06, and the draw is a function of (seed, trial)."""
+    from joint_bp_plus_pp_b200 import Options
+    dec, _ = hgp
+    o = dict(precision="fp32", max_iter=100, enable_pp=False)
+    lo, _ = dec.simulate(5, 3000, 0.01, Options(**o), per_trial=False)
+    hi, _ = dec.simulate(5, 3000, 0.06, Options(**o), per_trial=False)
+    mix, r1 = dec.simulate(5, 3000, 0.01, Options(p_max=0.06, **o))
+    _, r2 = dec.simulate(5, 3000, 0.01, Options(p_max=0.06, slots=512, **o))
+    assert lo["failures"] <= mix["failures"] <= hi["failures"] and lo["failures"] < hi["failures"]
+    assert (r1 == r2).all()
+
+
+def test_mixed_size_batch_concurrently():
+    """The four hypergraph-product codes (n = 1,600 ... 14,400) decoded at once from four host
+    threads, each context on its own stream."""
+    from joint_bp_plus_pp_b200 import Options
+    from joint_bp_plus_pp_b200.mixed import build, simulate_mixed
+    decs = build()
+    assert [d.n for d in decs] == [1600, 3600, 6400, 14400]
+    opts = Options(precision="fp32", max_iter=200, enable_pp=False, p_max=0.06)
+    stats, wall = simulate_mixed(decs, 1000, opts)
+    assert all(s["trials"] == 1000 for s in stats) and wall > 0
+    solo, _ = decs[0].simulate(11, 1000, 0.01, opts, per_trial=False)
+    assert (solo["failures"], solo["total_iters"]) == (stats[0]["failures"], stats[0]["total_iters"])
