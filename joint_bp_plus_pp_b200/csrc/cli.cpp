@@ -42,7 +42,8 @@ struct Args {
     int precision = JBP_PREC_FP64, sampler = JBP_SAMPLER_MT19937, slots = 0;
     long long batch = 1 << 18;
     int engine = JBP_ENGINE_AUTO, learned_from = 0;
-    std::string flip_model;
+    std::string flip_model, checks;
+    double p_max = 0.0;
 };
 
 void usage(const char *prog) {
@@ -64,7 +65,9 @@ void usage(const char *prog) {
               << "  --ets-dir DIR (default: the params path without extension)\n"
               << "  --engine auto|resident|slots (auto)  --learned-from N (0 = off; learned flip proposal at\n"
               << "  stalls from iteration N, FP16 resident engine)  --flip-model FILE.npy (default: the\n"
-              << "  shipped data/flip_mlp_params.npy next to the library)\n";
+              << "  shipped data/flip_mlp_params.npy next to the library)\n"
+              << "  --checks FILE (a code as check lists instead of --params: 'n mx mz', then one line of\n"
+              << "  variables per X check and per Z check)  --p-max P (per-trial p uniform in [p, P))\n";
 }
 
 // format_scaled_unit / format_latency (jointbp_ets.cpp:203-237)
@@ -194,6 +197,8 @@ int parse(int argc, char **argv, Args &a) {
                 else { std::cerr << "--engine must be auto, resident or slots\n"; return 1; }
             } else if (f == "--learned-from") { VAL(); a.learned_from = std::max(0, std::stoi(v)); }
             else if (f == "--flip-model") { VAL(); a.flip_model = v; }
+            else if (f == "--checks") { VAL(); a.checks = v; }
+            else if (f == "--p-max") { VAL(); a.p_max = std::stod(v); }
             else if (f == "--slots") { VAL(); a.slots = std::stoi(v); }
             else if (f == "--batch") { VAL(); a.batch = std::max(1LL, std::stoll(v)); }
             else if (f == "--ets-dir") { VAL(); a.ets_dir = v; }
@@ -249,6 +254,7 @@ jbp_options options(const Args &a) {
     o.slots = a.slots;
     o.engine = a.engine;
     o.learned_from = a.learned_from;
+    o.p_max = a.p_max;
     return o;
 }
 
@@ -538,7 +544,7 @@ int main(int argc, char **argv) {
                                                      std::chrono::system_clock::now().time_since_epoch())
                                                      .count());
     }
-    if (a.params.empty()) {
+    if (a.params.empty() && a.checks.empty()) {
         std::cerr << "--params is required\n";
         return 1;
     }
@@ -560,16 +566,47 @@ int main(int argc, char **argv) {
             return 1;
         }
     }
-    if (!exists(a.params)) {
-        std::cerr << "Failed to read params: " << a.params << "\n";
-        return 1;
-    }
     jbp_ctx *ctx = nullptr;
-    if (jbp_create_from_params(a.params.c_str(), nullptr, a.device, &ctx) != JBP_OK) {
-        std::cerr << "init failed: " << jbp_last_error() << "\n";
-        return 1;
+    if (!a.checks.empty()) {
+        // a code given as check lists (no ETS tables)
+        std::ifstream in(a.checks);
+        int n = 0, m[2] = {0, 0};
+        if (!in || !(in >> n >> m[0] >> m[1]) || n <= 0 || m[0] <= 0 || m[1] <= 0) {
+            std::cerr << "Failed to read checks: " << a.checks << "\n";
+            return 1;
+        }
+        std::string line;
+        std::getline(in, line);
+        std::vector<int> off[2], var[2];
+        for (int s = 0; s < 2; ++s) {
+            off[s].push_back(0);
+            for (int c = 0; c < m[s]; ++c) {
+                if (!std::getline(in, line)) {
+                    std::cerr << "Failed to read checks: " << a.checks << " (too few lines)\n";
+                    return 1;
+                }
+                std::istringstream ls(line);
+                int v;
+                while (ls >> v) var[s].push_back(v);
+                off[s].push_back(static_cast<int>(var[s].size()));
+            }
+        }
+        if (jbp_create_from_checks(n, m[0], off[0].data(), var[0].data(), m[1], off[1].data(), var[1].data(),
+                                   a.device, &ctx) != JBP_OK) {
+            std::cerr << "init failed: " << jbp_last_error() << "\n";
+            return 1;
+        }
+    } else {
+        if (!exists(a.params)) {
+            std::cerr << "Failed to read params: " << a.params << "\n";
+            return 1;
+        }
+        if (jbp_create_from_params(a.params.c_str(), nullptr, a.device, &ctx) != JBP_OK) {
+            std::cerr << "init failed: " << jbp_last_error() << "\n";
+            return 1;
+        }
     }
-    if (a.enable_pp && load_ets(ctx, a)) {
+    if (a.enable_pp && a.checks.empty() && load_ets(ctx, a)) {
         std::cerr << "ETS load failed: " << jbp_last_error() << "\n";
         jbp_destroy(ctx);
         return 1;

@@ -72,3 +72,20 @@ def test_mixed_size_batch_concurrently():
     assert all(s["trials"] == 1000 for s in stats) and wall > 0
     solo, _ = decs[0].simulate(11, 1000, 0.01, opts, per_trial=False)
     assert (solo["failures"], solo["total_iters"]) == (stats[0]["failures"], stats[0]["total_iters"])
+
+
+def test_cli_decodes_a_check_list_code(tmp_path):
+    """bin/jointbp_b200 --checks: a hypergraph-product code from a check-list file, per-trial p."""
+    import re
+    import subprocess
+    from pathlib import Path
+    from joint_bp_plus_pp_b200.codes import write_checks
+    cli = Path(__file__).resolve().parents[1] / "joint_bp_plus_pp_b200" / "bin" / "jointbp_b200"
+    f = tmp_path / "hgp32.checks"
+    write_checks(f, *hgp_code(32, 1))
+    r = subprocess.run([str(cli), "--checks", str(f), "--simulate", "--p", "0.01", "--p-max", "0.06",
+                        "--trials", "2000", "--max-iter", "100", "--precision", "fp32", "--sampler", "philox",
+                        "--seed", "3", "--report-every", "0"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    s = dict(re.findall(r"(\w+)=(\S+)", [l for l in r.stdout.splitlines() if l.startswith("trials=")][-1]))
+    assert s["trials"] == "2000" and 0 < int(s["failures"]) < 2000
