@@ -217,10 +217,24 @@ std::string Engine::build_res_code() {
                     if (var_at(x) != l * P + host_mod(a * x + b, P)) return "a block is not an affine permutation";
                 long long ia = 0;
                 if (!host_inverse(a, P, ia)) return "a block multiplier has no inverse";
-                rc->fa[s][j][l] = static_cast<unsigned short>(a);
-                rc->fb[s][j][l] = static_cast<unsigned short>(b);
-                rc->ia[s][j][l] = static_cast<unsigned short>(ia);
-                rc->ib[s][j][l] = static_cast<unsigned short>(host_mod(-ia * b, P));
+                const long long ib = host_mod(-ia * b, P);
+                auto fx = [&](long long c) {   // ceil(c 2^32 / P)
+                    return static_cast<unsigned>(((static_cast<unsigned long long>(c) << 32) + P - 1) / P);
+                };
+                rc->fF[s][j][l] = fx(a);
+                rc->fG[s][j][l] = fx(b);
+                rc->iF[s][j][l] = fx(ia);
+                rc->iG[s][j][l] = fx(ib);
+                // the fixed-point maps must reproduce both permutations exactly
+                for (unsigned x = 0; x < static_cast<unsigned>(P); ++x) {
+                    const unsigned y = static_cast<unsigned>(
+                        (static_cast<unsigned long long>(x * rc->fF[s][j][l] + rc->fG[s][j][l]) * P) >> 32);
+                    const unsigned xb = static_cast<unsigned>(
+                        (static_cast<unsigned long long>(x * rc->iF[s][j][l] + rc->iG[s][j][l]) * P) >> 32);
+                    if (y != static_cast<unsigned>(host_mod(a * x + b, P)) ||
+                        xb != static_cast<unsigned>(host_mod(ia * x + ib, P)))
+                        return "fixed-point block map check failed";
+                }
             }
     }
     // the device modulo: x - umulhi(x, magic) * P, corrected once, for every x the kernels form

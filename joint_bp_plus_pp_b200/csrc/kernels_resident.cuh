@@ -53,8 +53,10 @@ constexpr int kResThreads = 768;
 struct ResCode {
     int P, J, L, n, m;             // n = L*P, m = J*P checks per side
     unsigned magic;                // ceil(2^32 / P): x mod P for x < 2^32
-    unsigned short fa[2][kResMaxJ][kResMaxL], fb[2][kResMaxJ][kResMaxL];  // check -> variable
-    unsigned short ia[2][kResMaxJ][kResMaxL], ib[2][kResMaxJ][kResMaxL];  // variable -> check
+    // affine maps in fixed point: y = (a x + b) mod P is __umulhi(x F + G, P) with
+    // F = ceil(a 2^32 / P), G = ceil(b 2^32 / P) (exact for x < P, checked at start-up)
+    unsigned fF[2][kResMaxJ][kResMaxL], fG[2][kResMaxJ][kResMaxL];   // check -> variable
+    unsigned iF[2][kResMaxJ][kResMaxL], iG[2][kResMaxJ][kResMaxL];   // variable -> check
     int words;
     const uint64_t *basis_rows[2];
     const int *pivot_row[2];
@@ -100,6 +102,13 @@ constexpr int kLearnedMaxUnsat = 30;   // ... and only while max(us_x, us_z) is 
 __host__ __device__ inline size_t res_pp_scratch_bytes(int n, int mmax, int R) {
     return pp_align(pp_scratch_bytes(n, mmax)) + pp_align(static_cast<size_t>(R) * n) + pp_align(16ull * n) +
            pp_align(32ull * n);
+}
+
+// (a x + b) mod P from the fixed-point constants of the map: one multiply-add and one
+// high-half multiply.
+template <int P>
+__device__ __forceinline__ unsigned res_map(unsigned F, unsigned G, unsigned x) {
+    return __umulhi(x * F + G, static_cast<unsigned>(P));
 }
 
 __device__ __forceinline__ unsigned res_mod(unsigned x, unsigned P, unsigned magic) {
@@ -174,8 +183,7 @@ __device__ __forceinline__ bool res_check_row(const ResCode &code, typename ST::
     unsigned sgn = 0u, par = 0u;
 #pragma unroll
     for (int l = 0; l < L; ++l) {
-        const unsigned y = (static_cast<unsigned>(code.fa[SIDE][JJ][l]) * static_cast<unsigned>(x) +
-                            code.fb[SIDE][JJ][l]) % static_cast<unsigned>(P);
+        const unsigned y = res_map<P>(code.fF[SIDE][JJ][l], code.fG[SIDE][JJ][l], static_cast<unsigned>(x));
         const float a = A[l * P + y];
         par ^= __float_as_uint(a);
         const float v = a - ST::ld(c2v + l * m);
@@ -236,8 +244,7 @@ __device__ __forceinline__ int res_test_side(const ResCode &code, const float *A
         unsigned par = 0;
 #pragma unroll
         for (int l = 0; l < L; ++l) {
-            const unsigned y = (static_cast<unsigned>(code.fa[side][j][l]) * static_cast<unsigned>(x) +
-                                code.fb[side][j][l]) % static_cast<unsigned>(P);
+            const unsigned y = res_map<P>(code.fF[side][j][l], code.fG[side][j][l], static_cast<unsigned>(x));
             par ^= __float_as_uint(A_all[side * n + l * P + y]);
         }
         bad += (par & 1u) != ((syn_all[side * mw + (c >> 5)] >> (c & 31)) & 1u);
@@ -284,10 +291,8 @@ __device__ __forceinline__ void res_var_col(const ResCode &code, const typename 
     float Lam = 0.0f, Mu = 0.0f;
 #pragma unroll
     for (int j = 0; j < J; ++j) {
-        const unsigned xx = (static_cast<unsigned>(code.ia[0][j][LL]) * static_cast<unsigned>(y) + code.ib[0][j][LL]) %
-                            static_cast<unsigned>(P);
-        const unsigned xz = (static_cast<unsigned>(code.ia[1][j][LL]) * static_cast<unsigned>(y) + code.ib[1][j][LL]) %
-                            static_cast<unsigned>(P);
+        const unsigned xx = res_map<P>(code.iF[0][j][LL], code.iG[0][j][LL], static_cast<unsigned>(y));
+        const unsigned xz = res_map<P>(code.iF[1][j][LL], code.iG[1][j][LL], static_cast<unsigned>(y));
         Lam += ST::ld(c2v + LL * m + j * P + xx);
         Mu += ST::ld(c2v + (L + LL) * m + j * P + xz);
     }
@@ -344,10 +349,8 @@ __device__ void res_abs_llr(const ResCode &code, const typename ST::T *c2v, cons
         const int l = v / P, y = v - l * P;
         float Lam = 0.0f, Mu = 0.0f;
         for (int j = 0; j < J; ++j) {
-            const unsigned xx = (static_cast<unsigned>(code.ia[0][j][l]) * static_cast<unsigned>(y) + code.ib[0][j][l]) %
-                                static_cast<unsigned>(P);
-            const unsigned xz = (static_cast<unsigned>(code.ia[1][j][l]) * static_cast<unsigned>(y) + code.ib[1][j][l]) %
-                                static_cast<unsigned>(P);
+            const unsigned xx = res_map<P>(code.iF[0][j][l], code.iG[0][j][l], static_cast<unsigned>(y));
+            const unsigned xz = res_map<P>(code.iF[1][j][l], code.iG[1][j][l], static_cast<unsigned>(y));
             Lam += ST::ld(c2v + l * m + j * P + xx);
             Mu += ST::ld(c2v + (L + l) * m + j * P + xz);
         }
@@ -369,10 +372,8 @@ __device__ void res_features(const ResCode &code, const DevCode &dc, const typen
         const int l = v / P, y = v - l * P;
         float Lam = 0.0f, Mu = 0.0f;
         for (int j = 0; j < J; ++j) {
-            const unsigned xx = (static_cast<unsigned>(code.ia[0][j][l]) * static_cast<unsigned>(y) + code.ib[0][j][l]) %
-                                static_cast<unsigned>(P);
-            const unsigned xz = (static_cast<unsigned>(code.ia[1][j][l]) * static_cast<unsigned>(y) + code.ib[1][j][l]) %
-                                static_cast<unsigned>(P);
+            const unsigned xx = res_map<P>(code.iF[0][j][l], code.iG[0][j][l], static_cast<unsigned>(y));
+            const unsigned xz = res_map<P>(code.iF[1][j][l], code.iG[1][j][l], static_cast<unsigned>(y));
             Lam += ST::ld(c2v + l * m + j * P + xx);
             Mu += ST::ld(c2v + (L + l) * m + j * P + xz);
         }
@@ -744,8 +745,7 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
                 unsigned par = 0;
 #pragma unroll
                 for (int l = 0; l < L; ++l) {
-                    const unsigned y = (static_cast<unsigned>(code.fa[side][j][l]) * static_cast<unsigned>(x) +
-                                        code.fb[side][j][l]) % static_cast<unsigned>(P);
+                    const unsigned y = res_map<P>(code.fF[side][j][l], code.fG[side][j][l], static_cast<unsigned>(x));
                     par ^= (err[l * P + y] >> side) & 1u;
                 }
                 if (par) atomicOr(&syn[side * mw + (c >> 5)], 1u << (c & 31));
