@@ -354,6 +354,23 @@ def main():
                                 "iteration_disagreements": int((rlo["iterations"] != r64["iterations"]).sum()),
                                 "ler_difference": (flo - f64) / F}}
 
+    # precision report: final LLRs against FP64 on identical trials with a fixed iteration count
+    precision = None
+    if args.fp64_batch > 0 and rank == 0 and args.precision != "fp64":
+        it = 12
+        perr = dec.sample_errors(args.seed, base + 7 * 10 ** 8, 256, args.p, sampler="philox")
+        base_o = dict(max_iter=it, check_warmup=it, enable_pp=False)
+        _, r64p, l64 = dec.decode_errors_llr(perr, args.p, Options(precision="fp64", **base_o))
+        _, rlop, llo = dec.decode_errors_llr(perr, args.p, Options(precision=args.precision, engine=args.engine,
+                                                                   **base_o))
+        inside = np.abs(l64) <= 50
+        dev = np.abs(llo - l64)
+        precision = {"trials": 256, "iterations": it, "llr_entries": int(l64.size),
+                     "max_abs_llr_dev_nat": float(dev[inside].max()),
+                     "max_rel_llr_dev": float((dev[inside] / np.maximum(np.abs(l64[inside]), 1.0)).max()),
+                     "range": "|LLR_fp64| <= 50 nat (messages saturate at 110 bits = 76 nat)",
+                     "sign_disagreements": int(((llo > 0) != (l64 > 0)).sum())}
+
     # end to end through the C ABI with host buffers (reference-sampled errors in pinned memory)
     e2e = None
     if args.e2e_batch > 0:
@@ -412,6 +429,7 @@ def main():
         "ler": {"trials": agg["trials"], "failures": agg["failures"], "ci95": [lo, hi],
                 "avg_iter": agg["total_iters"] / max(1, agg["trials"])},
         "fp64": fp64,
+        "precision": precision,
         "clocks": clk,
         "e2e": e2e,
         "cpu_baseline": cpu,

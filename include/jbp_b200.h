@@ -135,6 +135,13 @@ int jbp_decode_errors(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, c
 int jbp_decode_syndromes(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *sx,
                          const uint8_t *sz, double p, uint8_t *est_out, jbp_trial_result *res, jbp_stats *stats);
 
+/* jbp_decode_errors with the final LLRs of every trial (precision diagnostics): llr_out is
+ * ntrials x n x 2 floats, the natural log of P(bit = 1) / P(bit = 0) of each qubit's x bit and
+ * z bit from the check-to-variable messages when the trial ends -- those of its last variable
+ * update when the syndrome is tested only at max_iter (check_warmup >= max_iter). */
+int jbp_decode_errors_llr(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *err, double p,
+                          float *llr_out, jbp_trial_result *res, jbp_stats *stats);
+
 /* Device-resident variants: every pointer is device memory of the context's device and
  * the call is ordered on `stream` (a cudaStream_t, 0 = legacy default stream). */
 int jbp_decode_errors_device(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *d_err,
@@ -187,6 +194,15 @@ int jbp_set_flip_model(jbp_ctx *ctx, const float *params);
 int jbp_collect_stall_states(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed, long long first_trial,
                              long long ntrials, double p, int sampler, long long capacity, float *x_out, float *y_out,
                              long long *count_out, jbp_stats *stats);
+
+/* Autotuner: times short Monte-Carlo probes (probe_trials trials of seed 1 at error rate p, the
+ * options in *opt) over the launch choices that do not change any decoding result -- the
+ * engine (resident where it applies, else slots), the slot engine's trials in flight (4096 ..
+ * 32768) and its BP iterations per CUDA-graph launch (2, 4, 8) -- and writes the fastest into
+ * *best (a copy of *opt with engine, slots and iters_per_launch set).  best_trials_per_s may
+ * be null. */
+int jbp_autotune(jbp_ctx *ctx, const jbp_options *opt, double p, long long probe_trials, jbp_options *best,
+                 double *best_trials_per_s);
 
 /* Errors of trials first_trial.. drawn by a device sampler (JBP_SAMPLER_*), copied to the host
  * buffer err (ntrials x n).  The same streams jbp_simulate decodes. */

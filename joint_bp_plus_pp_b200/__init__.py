@@ -123,6 +123,8 @@ def load_library(path=None):
                                  vp, vp]
     lib.jbp_decode_errors.argtypes = [vp, ctypes.POINTER(COptions), ll, vp, d, vp, vp, ctypes.POINTER(CStats)]
     lib.jbp_decode_syndromes.argtypes = [vp, ctypes.POINTER(COptions), ll, vp, vp, d, vp, vp, ctypes.POINTER(CStats)]
+    lib.jbp_decode_errors_llr.argtypes = [vp, ctypes.POINTER(COptions), ll, vp, d, vp, vp, ctypes.POINTER(CStats)]
+    lib.jbp_autotune.argtypes = [vp, ctypes.POINTER(COptions), d, ll, ctypes.POINTER(COptions), ctypes.POINTER(d)]
     lib.jbp_decode_errors_device.argtypes = [vp, ctypes.POINTER(COptions), ll, vp, d, vp, vp, ctypes.POINTER(CStats),
                                              vp]
     lib.jbp_sample_errors.argtypes = [vp, ctypes.c_uint64, ll, ll, d, i, vp]
@@ -239,6 +241,34 @@ class Decoder:
         _check(self._lib, self._lib.jbp_decode_errors(self._h, ctypes.byref(co), t, _ptr(err), p, _ptr(est),
                                                       _ptr(res), ctypes.byref(st)))
         return st.as_dict(), res, est
+
+    def autotune(self, p, opts=None, probe_trials=16384):
+        """Fastest launch configuration (engine, slots, iterations per graph) for these options:
+        returns (Options, trials/s of the probe)."""
+        opts = opts or Options()
+        co = opts.to_c()
+        best = COptions()
+        rate = ctypes.c_double()
+        _check(self._lib, self._lib.jbp_autotune(self._h, ctypes.byref(co), p, probe_trials, ctypes.byref(best),
+                                                 ctypes.byref(rate)))
+        inv = {v: k for k, v in ENGINE.items()}
+        from dataclasses import replace
+        return replace(opts, engine=inv[best.engine], slots=best.slots, iters_per_launch=best.iters_per_launch), \
+            rate.value
+
+    def decode_errors_llr(self, err, p, opts=None):
+        """decode_errors plus the final LLRs (trials x n x 2: x bit, z bit; natural log of
+        P(1)/P(0)) -- those of the last variable update when opts.check_warmup >= max_iter."""
+        err = np.ascontiguousarray(err, np.uint8).reshape(-1, self.n)
+        opts = opts or Options()
+        t = err.shape[0]
+        llr = np.zeros((t, self.n, 2), np.float32)
+        res = np.zeros(t, TRIAL_DTYPE)
+        st = CStats()
+        co = opts.to_c()
+        _check(self._lib, self._lib.jbp_decode_errors_llr(self._h, ctypes.byref(co), t, _ptr(err), p, _ptr(llr),
+                                                          _ptr(res), ctypes.byref(st)))
+        return st.as_dict(), res, llr
 
     def decode_syndromes(self, sx, sz, p, opts=None, want_est=True):
         sx = np.ascontiguousarray(sx, np.uint8).reshape(-1, self.mx)

@@ -185,7 +185,8 @@ int jbp_simulate(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed, long long 
 }
 
 static int decode_host(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *err, const uint8_t *sx,
-                       const uint8_t *sz, double p, uint8_t *est_out, jbp_trial_result *res, jbp_stats *stats) {
+                       const uint8_t *sz, double p, uint8_t *est_out, jbp_trial_result *res, jbp_stats *stats,
+                       float *llr_out = nullptr) {
     if (!ctx || ntrials < 0 || !res) return fail(JBP_ERR_ARG, "invalid argument");
     const auto &m = ctx->engine.model();
     const long long n = m.n, mx = m.side[0].m, mz = m.side[1].m;
@@ -208,8 +209,8 @@ static int decode_host(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, 
     const uint8_t *m_err = mapped(err), *m_sx = mapped(sx), *m_sz = mapped(sz);
     // chunks bound the staging memory; each chunk is one engine run
     const bool in_place = (err && m_err) || (!err && m_sx && m_sz);
-    const long long chunk =
-        std::max<long long>(1, std::min<long long>(ntrials, in_place && !est_out ? 1LL << 20 : 1LL << 17));
+    const long long chunk = std::max<long long>(
+        1, std::min<long long>(ntrials, llr_out ? 4096 : (in_place && !est_out ? 1LL << 20 : 1LL << 17)));
     for (long long base = 0; base < ntrials; base += chunk) {
         const long long cnt = std::min(chunk, ntrials - base);
         jbp::RunRequest rq;
@@ -251,12 +252,18 @@ static int decode_host(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, 
         }
         if (int rc = grow(&ctx->d_res, &ctx->res_count, static_cast<size_t>(cnt))) return rc;
         rq.d_res_out = ctx->d_res;
+        if (llr_out) {
+            if (int rc = grow(&ctx->d_llr, &ctx->llr_count, static_cast<size_t>(cnt * n * 2))) return rc;
+            rq.d_llr_out = ctx->d_llr;
+        }
         jbp_stats st;
         std::string e = ctx->engine.run(rq, st);
         if (!e.empty()) return engine_fail(e);
         ce = cudaMemcpy(res + base, ctx->d_res, sizeof(jbp_trial_result) * cnt, cudaMemcpyDeviceToHost);
         if (ce == cudaSuccess && est_out)
             ce = cudaMemcpy(est_out + base * n, ctx->d_est, static_cast<size_t>(cnt * n), cudaMemcpyDeviceToHost);
+        if (ce == cudaSuccess && llr_out)
+            ce = cudaMemcpy(llr_out + base * n * 2, ctx->d_llr, sizeof(float) * cnt * n * 2, cudaMemcpyDeviceToHost);
         if (ce != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(ce, "copy results"));
         long long *a = &total.trials;
         const long long *b = &st.trials;
@@ -333,6 +340,12 @@ int jbp_decode_errors(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, c
     return decode_host(ctx, opt, ntrials, err, nullptr, nullptr, p, est_out, res, stats);
 }
 
+int jbp_decode_errors_llr(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *err, double p,
+                          float *llr_out, jbp_trial_result *res, jbp_stats *stats) {
+    if (!err || !llr_out) return fail(JBP_ERR_ARG, "null buffer");
+    return decode_host(ctx, opt, ntrials, err, nullptr, nullptr, p, nullptr, res, stats, llr_out);
+}
+
 int jbp_decode_syndromes(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *sx,
                          const uint8_t *sz, double p, uint8_t *est_out, jbp_trial_result *res, jbp_stats *stats) {
     return decode_host(ctx, opt, ntrials, nullptr, sx, sz, p, est_out, res, stats);
@@ -357,6 +370,43 @@ int jbp_decode_errors_device(jbp_ctx *ctx, const jbp_options *opt, long long ntr
     std::string e = ctx->engine.run(rq, st);
     if (!e.empty()) return engine_fail(e);
     if (stats) *stats = st;
+    return JBP_OK;
+}
+
+int jbp_autotune(jbp_ctx *ctx, const jbp_options *opt, double p, long long probe_trials, jbp_options *best,
+                 double *best_trials_per_s) {
+    if (!ctx || !best || probe_trials <= 0) return fail(JBP_ERR_ARG, "invalid argument");
+    const jbp_options base = normalized(opt);
+    std::vector<jbp_options> cand;
+    jbp_options c = base;
+    c.engine = JBP_ENGINE_RESIDENT;
+    cand.push_back(c);
+    for (int S : {4096, 8192, 16384, 32768})
+        for (int gi : {2, 4, 8}) {
+            c = base;
+            c.engine = JBP_ENGINE_SLOTS;
+            c.slots = S;
+            c.iters_per_launch = gi;
+            cand.push_back(c);
+        }
+    double best_rate = -1.0;
+    for (const jbp_options &o : cand) {
+        jbp_stats st;
+        // a short run first (buffers, graphs), then the timed probe
+        int rc = jbp_simulate(ctx, &o, 1, 1, std::max<long long>(64, probe_trials / 8), p, JBP_SAMPLER_PHILOX, &st,
+                              nullptr, nullptr);
+        if (rc == JBP_ERR_UNSUPPORTED) continue;   // e.g. the resident engine does not apply
+        if (rc != JBP_OK) return rc;
+        rc = jbp_simulate(ctx, &o, 1, 1, probe_trials, p, JBP_SAMPLER_PHILOX, &st, nullptr, nullptr);
+        if (rc != JBP_OK) return rc;
+        const double rate = st.device_ms > 0.0 ? st.trials / (st.device_ms / 1000.0) : 0.0;
+        if (rate > best_rate) {
+            best_rate = rate;
+            *best = o;
+        }
+    }
+    if (best_rate < 0.0) return fail(JBP_ERR_UNSUPPORTED, "no engine configuration applies");
+    if (best_trials_per_s) *best_trials_per_s = best_rate;
     return JBP_OK;
 }
 

@@ -44,6 +44,7 @@ struct Args {
     int engine = JBP_ENGINE_AUTO, learned_from = 0;
     std::string flip_model, checks;
     double p_max = 0.0;
+    bool autotune = false;
 };
 
 void usage(const char *prog) {
@@ -67,7 +68,8 @@ void usage(const char *prog) {
               << "  stalls from iteration N, FP16 resident engine)  --flip-model FILE.npy (default: the\n"
               << "  shipped data/flip_mlp_params.npy next to the library)\n"
               << "  --checks FILE (a code as check lists instead of --params: 'n mx mz', then one line of\n"
-              << "  variables per X check and per Z check)  --p-max P (per-trial p uniform in [p, P))\n";
+              << "  variables per X check and per Z check)  --p-max P (per-trial p uniform in [p, P))\n"
+              << "  --autotune (time short probes and keep the fastest engine / slots / graph length)\n";
 }
 
 // format_scaled_unit / format_latency (jointbp_ets.cpp:203-237)
@@ -198,6 +200,7 @@ int parse(int argc, char **argv, Args &a) {
             } else if (f == "--learned-from") { VAL(); a.learned_from = std::max(0, std::stoi(v)); }
             else if (f == "--flip-model") { VAL(); a.flip_model = v; }
             else if (f == "--checks") { VAL(); a.checks = v; }
+            else if (f == "--autotune") a.autotune = true;
             else if (f == "--p-max") { VAL(); a.p_max = std::stod(v); }
             else if (f == "--slots") { VAL(); a.slots = std::stoi(v); }
             else if (f == "--batch") { VAL(); a.batch = std::max(1LL, std::stoll(v)); }
@@ -429,7 +432,20 @@ int simulate(jbp_ctx *ctx, const Args &a, int n) {
         std::cerr << "--est is only supported with --trials 1\n";
         return 1;
     }
-    const jbp_options o = options(a);
+    jbp_options o = options(a);
+    if (a.autotune) {
+        jbp_options best;
+        double rate = 0.0;
+        if (jbp_autotune(ctx, &o, a.p, std::min<long long>(16384, std::max<long long>(1024, a.trials)), &best, &rate) !=
+            JBP_OK) {
+            std::cerr << "autotune failed: " << jbp_last_error() << "\n";
+            return 1;
+        }
+        o = best;
+        std::cout << "autotune: engine=" << (o.engine == JBP_ENGINE_RESIDENT ? "resident" : "slots")
+                  << " slots=" << o.slots << " iters_per_launch=" << o.iters_per_launch << " probe_trials_per_s="
+                  << std::fixed << std::setprecision(0) << rate << "\n";
+    }
     const long long first = a.trial_index >= 0 ? a.trial_index : 1;
     std::vector<long long> hist(static_cast<size_t>(a.max_iter) + 1, 0), chunk_hist(hist.size());
     std::vector<jbp_trial_result> per;

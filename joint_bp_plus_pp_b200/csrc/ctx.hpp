@@ -21,6 +21,8 @@ struct jbp_ctx {
     size_t res_count = 0;
     unsigned long long *d_hist = nullptr;
     size_t hist_count = 0;
+    float *d_llr = nullptr;
+    size_t llr_count = 0;
     ~jbp_ctx() {
         if (stream) cudaStreamDestroy(stream);
         cudaFree(d_in);
@@ -28,6 +30,7 @@ struct jbp_ctx {
         cudaFree(d_est);
         cudaFree(d_res);
         cudaFree(d_hist);
+        cudaFree(d_llr);
     }
 };
 

@@ -203,7 +203,6 @@ std::string Engine::build_res_code() {
     auto rc = std::make_unique<ResCode>();
     std::memset(rc.get(), 0, sizeof(ResCode));
     rc->P = P; rc->J = J; rc->L = L; rc->n = n; rc->m = m;
-    rc->magic = static_cast<unsigned>(((1ull << 32) + P - 1) / P);
     for (int s = 0; s < 2; ++s) {
         const SideGraph &g = model_.side[s];
         if (!g.regular || g.dc_max != L || g.dv_max != J) return "side degrees do not match the block structure";
@@ -236,13 +235,6 @@ std::string Engine::build_res_code() {
                         return "fixed-point block map check failed";
                 }
             }
-    }
-    // the device modulo: x - umulhi(x, magic) * P, corrected once, for every x the kernels form
-    for (unsigned long long x = 0; x < static_cast<unsigned long long>(P) * P; ++x) {
-        const unsigned q = static_cast<unsigned>((x * rc->magic) >> 32);
-        long long r = static_cast<long long>(x) - static_cast<long long>(q) * P;
-        if (r < 0) r += P;
-        if (r != static_cast<long long>(x % P)) return "modular reduction check failed";
     }
     rc->words = dcode_.words;
     for (int s = 0; s < 2; ++s) {
@@ -341,6 +333,7 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     r.src_sx = rq.d_sx;
     r.src_sz = rq.d_sz;
     r.est_out = rq.d_est_out;
+    r.llr_out = rq.d_llr_out;
     r.res_out = rq.d_res_out;
     r.hist = rq.d_hist;
     r.cnt = res_cnt_;
@@ -575,6 +568,7 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     r.src_sx = rq.d_sx;
     r.src_sz = rq.d_sz;
     r.est_out = rq.d_est_out;
+    r.llr_out = rq.d_llr_out;
     r.res_out = rq.d_res_out;
     r.hist = rq.d_hist;
     r.trial = buf_.trial;
@@ -677,6 +671,12 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
         if (pp) {
             k_postprocess<<<buf_.pp_blocks, kPpThreads,
                             pp_smem_bytes(n, M, std::max(gx.m, gz.m)), s>>>(dcode_, r);
+            launches += 1;
+        }
+        if (rq.d_llr_out) {
+            if (o.precision == JBP_PREC_FP64) k_llr_out<double2><<<sm_count_ * 2, 256, 0, s>>>(dcode_, r, msg);
+            else if (o.precision == JBP_PREC_FP32) k_llr_out<float><<<sm_count_ * 2, 256, 0, s>>>(dcode_, r, msg);
+            else k_llr_out<__half><<<sm_count_ * 2, 256, 0, s>>>(dcode_, r, msg);
             launches += 1;
         }
         k_classify<<<sm_count_ * 2, classify_tpb, classify_smem, s>>>(dcode_, r);

@@ -101,6 +101,7 @@ struct DevRun {
     const uint8_t *src_err;         // [ntrials][n]
     const uint8_t *src_sx, *src_sz; // [ntrials][m]
     uint8_t *est_out;               // [ntrials][n] or null
+    float *llr_out;                 // [ntrials][n][2] final LLRs (x, z) or null
     jbp_trial_result *res_out;      // [ntrials] or null
     unsigned long long *hist;       // [max_iter + 1] or null
     // slot state

@@ -24,6 +24,7 @@ struct RunRequest {
     const uint8_t *d_sx = nullptr;
     const uint8_t *d_sz = nullptr;
     uint8_t *d_est_out = nullptr;       // outputs (device, optional)
+    float *d_llr_out = nullptr;         // [ntrials][n][2] final LLRs (diagnostics)
     jbp_trial_result *d_res_out = nullptr;
     unsigned long long *d_hist = nullptr;
     cudaStream_t stream = nullptr;

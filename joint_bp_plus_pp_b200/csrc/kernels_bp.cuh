@@ -510,4 +510,55 @@ __global__ void __launch_bounds__(256) k_var_llr(DevCode code, DevRun run, DevMs
     }
 }
 
+// Final LLRs of retired trials (diagnostics of the precision report): per variable, natural
+// log of P(bit = 1) / P(bit = 0) of the x and z bits, from the c2v in memory when the trial
+// retires (those of its last variable update when the syndrome is tested only at max_iter).
+template <typename T>
+__global__ void k_llr_out(DevCode code, DevRun run, DevMsgs msg) {
+    const int nret = *run.n_retired;
+    const int n = code.n, G = run.S / kGroup, dc = code.s[0].dc, dv = code.s[0].dv;
+    const long long total = static_cast<long long>(nret) * n;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int r = static_cast<int>(i / n), v = static_cast<int>(i - static_cast<long long>(r) * n);
+        const int slot = run.retired[r];
+        const long long local = run.trial[slot] - run.first_trial;
+        const int g = slot / kGroup, lane = slot % kGroup;
+        float lx, lz;
+        if constexpr (sizeof(T) == sizeof(double2)) {
+            const double *pr = run.prior + 4 * slot;
+            double XA = 1.0, XB = 1.0, ZA = 1.0, ZB = 1.0;
+            for (int side = 0; side < 2; ++side)
+                for (int k = 0; k < dv; ++k) {
+                    const int e = __ldg(code.s[side].var_edge + v * dv + k);
+                    if (e < 0) continue;
+                    const int c = e / dc, pos = e - c * dc;
+                    const double2 m = static_cast<const double2 *>(msg.c2v[side])
+                        [((static_cast<size_t>(c) * G + g) * dc + pos) * kGroup + lane];
+                    if (side == 0) { XA *= m.x; XB *= m.y; } else { ZA *= m.x; ZB *= m.y; }
+                }
+            const double t0 = pr[0] * XA * ZA, t1 = pr[1] * XB * ZA, t2 = pr[2] * XA * ZB, t3 = pr[3] * XB * ZB;
+            lx = static_cast<float>(log(fmax(t1 + t3, 1e-300)) - log(fmax(t0 + t2, 1e-300)));
+            lz = static_cast<float>(log(fmax(t2 + t3, 1e-300)) - log(fmax(t0 + t1, 1e-300)));
+        } else {
+            float Lam = 0.0f, Mu = 0.0f;
+            for (int side = 0; side < 2; ++side)
+                for (int k = 0; k < dv; ++k) {
+                    const int e = __ldg(code.s[side].var_edge + v * dv + k);
+                    if (e < 0) continue;
+                    const int c = e / dc, pos = e - c * dc;
+                    const float m = ld_msg<T>(static_cast<const T *>(msg.c2v[side]) +
+                                              ((static_cast<size_t>(c) * G + g) * dc + pos) * kGroup + lane);
+                    if (side == 0) Lam += m; else Mu += m;
+                }
+            const float *lp = run.lprior + 8 * slot;
+            const float w0 = lp[0], w1 = lp[1] - Lam, w2 = lp[2] - Mu, w3 = lp[3] - Lam - Mu;
+            lx = (lse2(w1, w3) - lse2(w0, w2)) * 0.69314718f;
+            lz = (lse2(w2, w3) - lse2(w0, w1)) * 0.69314718f;
+        }
+        run.llr_out[(local * n + v) * 2] = lx;
+        run.llr_out[(local * n + v) * 2 + 1] = lz;
+    }
+}
+
 }  // namespace jbp

@@ -52,7 +52,6 @@ constexpr int kResThreads = 768;
 
 struct ResCode {
     int P, J, L, n, m;             // n = L*P, m = J*P checks per side
-    unsigned magic;                // ceil(2^32 / P): x mod P for x < 2^32
     // affine maps in fixed point: y = (a x + b) mod P is __umulhi(x F + G, P) with
     // F = ceil(a 2^32 / P), G = ceil(b 2^32 / P) (exact for x < P, checked at start-up)
     unsigned fF[2][kResMaxJ][kResMaxL], fG[2][kResMaxJ][kResMaxL];   // check -> variable
@@ -75,6 +74,7 @@ struct ResRun {
     const uint8_t *src_err;        // [ntrials][n]
     const uint8_t *src_sx, *src_sz;
     uint8_t *est_out;
+    float *llr_out;                // [ntrials][n][2] final LLRs (x, z), natural units, or null
     jbp_trial_result *res_out;
     unsigned long long *hist;
     DevCounters *cnt;
@@ -111,11 +111,6 @@ __device__ __forceinline__ unsigned res_map(unsigned F, unsigned G, unsigned x) 
     return __umulhi(x * F + G, static_cast<unsigned>(P));
 }
 
-__device__ __forceinline__ unsigned res_mod(unsigned x, unsigned P, unsigned magic) {
-    const unsigned q = __umulhi(x, magic);
-    int r = static_cast<int>(x - q * P);
-    return static_cast<unsigned>(r < 0 ? r + static_cast<int>(P) : r);
-}
 
 // 16-bit message storage: IEEE half.
 struct StoreHalf {
@@ -623,6 +618,26 @@ __device__ __noinline__ int res_slow_step(const ResCode &code, const ResRun &run
     return it >= run.max_iter ? -1 : 0;
 }
 
+// Final LLRs of a trial (diagnostics of the precision report; out of line): natural log of
+// P(bit = 1) / P(bit = 0) of the x and z bits from the c2v in shared memory when the trial
+// ends (those of its last variable update when the syndrome is tested only at max_iter).
+template <int P, int J, int L, class ST>
+__device__ __noinline__ void res_write_llr(const ResCode &code, const typename ST::T *c2v, const float4 lp,
+                                           float *out) {
+    constexpr int m = J * P, n = L * P;
+    for (int v = threadIdx.x; v < n; v += blockDim.x) {
+        const int l = v / P, y = v - l * P;
+        float Lam = 0.0f, Mu = 0.0f;
+        for (int j = 0; j < J; ++j) {
+            Lam += ST::ld(c2v + l * m + j * P + res_map<P>(code.iF[0][j][l], code.iG[0][j][l], y));
+            Mu += ST::ld(c2v + (L + l) * m + j * P + res_map<P>(code.iF[1][j][l], code.iG[1][j][l], y));
+        }
+        const float w0 = lp.x, w1 = lp.y - Lam, w2 = lp.z - Mu, w3 = lp.w - Lam - Mu;
+        out[2 * v] = (res_lse2(w1, w3) - res_lse2(w0, w2)) * 0.69314718f;
+        out[2 * v + 1] = (res_lse2(w2, w3) - res_lse2(w0, w1)) * 0.69314718f;
+    }
+}
+
 // Prior of a trial (error rate pt; thread 0, once per run or per trial; out of line): FP64 as
 // the slot engine's refill, then its log2 weights and probabilities in FP32.
 __device__ __noinline__ void res_set_prior(const ResRun &run, double pt, float4 *lp, float4 *pr, float *lpx,
@@ -645,7 +660,8 @@ __device__ __noinline__ void res_set_prior(const ResRun &run, double pt, float4 
 }
 
 template <int P, int J, int L, class ST, bool PP, bool LEARNED>
-__global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRun run) {
+__global__ void __launch_bounds__(kResThreads, 1)
+    k_resident(const __grid_constant__ ResCode code, const __grid_constant__ ResRun run) {
     extern __shared__ __align__(16) unsigned char res_smem[];
     using T = typename ST::T;
     constexpr int m = J * P, n = L * P, mw = (m + 31) / 32;
@@ -824,6 +840,7 @@ __global__ void __launch_bounds__(kResThreads, 1) k_resident(ResCode code, ResRu
             }
         }
         const bool ok = (rf & kResSyndromeOk) != 0;
+        if (run.llr_out) res_write_llr<P, J, L, ST>(code, c2v, lp_sh, run.llr_out + local * n * 2);
 
         // ---- classification (jointbp_ets.cpp:6199-6245): exact, stabilizer-equivalent residual
         const int words = (n + 63) / 64, w32 = 2 * words;

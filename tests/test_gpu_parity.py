@@ -208,3 +208,19 @@ def test_simulate_counts_and_hist(decoder):
     assert int(st["hist"].sum()) == 2000
     assert 7.0 < st["total_iters"] / 2000 < 12.0
     assert st["failures"] <= 2
+
+
+@pytest.mark.parametrize("prec,engine,tol", [("fp32", "slots", 0.01), ("fp16", "slots", 0.3), ("fp16", "resident", 0.3)])
+def test_final_llr_deviation_vs_fp64(decoder, prec, engine, tol):
+    """Max |LLR| deviation against FP64 (natural units) after 12 iterations on 256 identical
+    trials at p=0.04, over the LLRs inside the LLR decoders' range (|LLR_fp64| <= 50; their
+    messages saturate at 110 bits = 76 nat by design), and sign agreement."""
+    err = decoder.sample_errors(77, 1, 256, 0.04, sampler="philox")
+    it = 12
+    _, _, l64 = decoder.decode_errors_llr(err, 0.04, opts(max_iter=it, check_warmup=it))
+    _, _, llo = decoder.decode_errors_llr(err, 0.04, opts(max_iter=it, check_warmup=it, precision=prec,
+                                                          engine=engine))
+    assert np.isfinite(llo).all()
+    inside = np.abs(l64) <= 50
+    assert np.abs(llo - l64)[inside].max() <= tol
+    assert ((llo > 0) != (l64 > 0)).mean() <= 1e-4

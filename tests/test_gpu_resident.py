@@ -198,3 +198,14 @@ def test_pinned_host_inputs_are_read_in_place(decoder, oracle, engine, prec):
     from joint_bp_plus_pp_b200 import JbpError
     with pytest.raises(JbpError):
         decoder.decode_errors(bad_p, 0.05, o)
+
+
+def test_autotune_picks_a_configuration_that_decodes_identically(decoder):
+    from joint_bp_plus_pp_b200 import Options
+    for prec, want in (("fp16", "resident"), ("fp64", "slots")):
+        o = Options(precision=prec, max_iter=200, enable_pp=False)
+        best, rate = decoder.autotune(0.04, o, probe_trials=2048)
+        assert rate > 0 and best.engine == want
+        s1, r1 = decoder.simulate(9, 512, 0.04, o)
+        s2, r2 = decoder.simulate(9, 512, 0.04, best)
+        assert (r1["iterations"] == r2["iterations"]).all() and (r1["success"] == r2["success"]).all()
