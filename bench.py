@@ -106,6 +106,12 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.lines = []
+        self.first = 0
+
+    def mark(self):
+        """Start of the timed region: later samples only (the sampler is started before the
+        warm-up so that nvidia-smi's own start-up does not fall into the timed region)."""
+        self.first = len(self.lines)
 
     def start(self):
         try:
@@ -131,7 +137,8 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        lines = self.lines[self.first:] or self.lines[-2:]
+        for line in lines:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -262,14 +269,13 @@ def main():
         if dist is not None:
             dist.barrier()
 
+    clocks = ClockSampler(local)
+    clocks.start()
     for w in range(args.warmup):
         dec.simulate(args.seed, B, args.p, opts, first_trial=base + w * B, per_trial=False)
     torch.cuda.synchronize()
     barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
-    torch.cuda.synchronize()
-    barrier()
+    clocks.mark()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record()
@@ -277,9 +283,13 @@ def main():
            "bp_trial_iterations": 0, "profiled_iterations": 0, "device_ms": 0.0, "pp_success": 0,
            "learned_attempts": 0, "learned_success": 0}
     first_res = None
+    step_wall, step_kernel = [], []
     for k in range(args.steps):
+        t0 = time.perf_counter()
         st, res = dec.simulate(args.seed, B, args.p, opts, first_trial=base + (args.warmup + k) * B,
                                per_trial=(k == 0))
+        step_wall.append(round((time.perf_counter() - t0) * 1e3, 2))
+        step_kernel.append(round(st["device_ms"], 2))
         if k == 0:
             first_res = res
         for key in agg:
@@ -431,6 +441,7 @@ def main():
         "fp64": fp64,
         "precision": precision,
         "clocks": clk,
+        "step_ms": {"host_wall": step_wall, "kernel": step_kernel},
         "e2e": e2e,
         "cpu_baseline": cpu,
     }

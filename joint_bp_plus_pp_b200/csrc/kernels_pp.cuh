@@ -478,8 +478,14 @@ static __device__ void blk_sort_pairs(unsigned long long *key, int *idx, int np2
 }
 
 // attempt_osd_pp_side restated as one incremental elimination (see the file comment).
+// The basis is kept fully reduced (no basis vector has a bit at another one's pivot), so a new
+// column is reduced by the basis vectors pivoted at its own checks alone.  Per column, warp 0
+// builds the reduced column and its lowest set bit; after one barrier every warp clears the
+// new pivot from its share of the basis, testing 32 basis vectors per load and ballot; warp 0
+// appends the column and updates the residual of the syndrome difference; a second barrier
+// ends the column.  `max_cols` limits the columns taken (the whole order by default).
 static __device__ bool blk_osd_side(const DevCode &code, const double *llr, const PpShared &sh, const PpScratch &sc,
-                                    int side) {
+                                    int side, int max_cols = 0x7fffffff) {
     const int n = code.n, m = code.s[side].m, dv = code.s[side].dv;
     const int MW = (m + 63) / 64, CW = (m + 2 + 63) / 64;
     const int np2 = pp_npow2(n);
@@ -500,73 +506,98 @@ static __device__ bool blk_osd_side(const DevCode &code, const double *llr, cons
     __syncthreads();
     blk_sort_pairs(sc.key, sc.idx, np2);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    for (int j = 0; j < n; ++j) {
-        const int var = sc.idx[j];
+    const int ncols = min(n, max_cols);
+    for (int j = 0; j < ncols; ++j) {
         const int rank = sh.ints[30];
-        // the column: the variable's checks, reduced by the basis vectors pivoted there
-        for (int w = threadIdx.x; w < MW; w += blockDim.x) sh.wv[w] = 0;
-        for (int w = threadIdx.x; w < CW; w += blockDim.x) sh.wc[w] = 0;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int k = 0; k < dv; ++k) {
-                const int c = var_check(code, side, var, k);
-                if (c >= 0) sh.wv[c >> 6] ^= 1ull << (c & 63);
+        if (warp == 0) {
+            // the column: the variable's checks, reduced by the basis vectors pivoted there.
+            // Lane k fetches check k and its pivot; the basis words are gathered in registers,
+            // 4 words per lane per pass, so the loads of the different checks overlap.
+            const int var = sc.idx[j];
+            for (int w0 = 0; w0 < MW || w0 < CW; w0 += 128) {
+                uint64_t av[4] = {0ull, 0ull, 0ull, 0ull}, ac[4] = {0ull, 0ull, 0ull, 0ull};
+                for (int k0 = 0; k0 < dv; k0 += 32) {
+                    int ck = -1, bk = -1;
+                    if (k0 + lane < dv) {
+                        ck = var_check(code, side, var, k0 + lane);
+                        bk = ck >= 0 ? sc.piv[ck] : -1;
+                    }
+                    const int kn = min(32, dv - k0);
+#pragma unroll 4
+                    for (int k = 0; k < kn; ++k) {
+                        const int c = __shfl_sync(0xffffffffu, ck, k), b = __shfl_sync(0xffffffffu, bk, k);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const int w = w0 + q * 32 + lane;
+                            if (c >= 0 && (c >> 6) == w) av[q] ^= 1ull << (c & 63);
+                            if (b >= 0) {
+                                if (w < MW) av[q] ^= sc.vec[static_cast<size_t>(b) * MW + w];
+                                if (w < CW) ac[q] ^= sc.comb[static_cast<size_t>(b) * CW + w];
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int w = w0 + q * 32 + lane;
+                    if (w < MW) sh.wv[w] = av[q];
+                    if (w < CW) sh.wc[w] = ac[q] ^ (w == (j >> 6) ? 1ull << (j & 63) : 0ull);
+                }
             }
-            sh.wc[j >> 6] |= 1ull << (j & 63);
-        }
-        __syncthreads();
-        for (int k = 0; k < dv; ++k) {
-            const int c = var_check(code, side, var, k);
-            const int b = c >= 0 ? sc.piv[c] : -1;
-            if (b >= 0) {
-                const uint64_t *bv = sc.vec + static_cast<size_t>(b) * MW, *bc = sc.comb + static_cast<size_t>(b) * CW;
-                for (int w = threadIdx.x; w < MW; w += blockDim.x) sh.wv[w] ^= bv[w];
-                for (int w = threadIdx.x; w < CW; w += blockDim.x) sh.wc[w] ^= bc[w];
+            __syncwarp();
+            // lowest set bit of the reduced column, or none (first dependent column)
+            unsigned lo = 0x7fffffffu;
+            for (int w = lane; w < MW; w += 32) {
+                const uint64_t x = sh.wv[w];
+                if (x) lo = min(lo, static_cast<unsigned>(w * 64 + __ffsll(static_cast<long long>(x)) - 1));
             }
-            __syncthreads();
+            lo = __reduce_min_sync(0xffffffffu, lo);
+            if (lane == 0) sh.ints[32] = static_cast<int>(lo);
         }
-        // lowest set bit of the reduced column, or none (first dependent column)
-        if (threadIdx.x == 0) sh.ints[32] = 0x7fffffff;
-        __syncthreads();
-        for (int w = threadIdx.x; w < MW; w += blockDim.x)
-            if (sh.wv[w]) atomicMin(&sh.ints[32], w * 64 + __ffsll(static_cast<long long>(sh.wv[w])) - 1);
         __syncthreads();
         const int p = sh.ints[32];
         if (p == 0x7fffffff) break;
-        // eliminate the new pivot row from the basis, one basis vector per warp
+        // clear the new pivot row from the basis
         const int pw = p >> 6;
         const uint64_t pb = 1ull << (p & 63);
-        for (int b = warp; b < rank; b += nwarps) {
-            uint64_t *bv = sc.vec + static_cast<size_t>(b) * MW;
-            if (!(bv[pw] & pb)) continue;
-            uint64_t *bc = sc.comb + static_cast<size_t>(b) * CW;
-            for (int w = lane; w < MW; w += 32) bv[w] ^= sh.wv[w];
-            for (int w = lane; w < CW; w += 32) bc[w] ^= sh.wc[w];
-        }
-        // append; update the residual of the syndrome difference
-        {
-            uint64_t *nvp = sc.vec + static_cast<size_t>(rank) * MW, *ncp = sc.comb + static_cast<size_t>(rank) * CW;
-            for (int w = threadIdx.x; w < MW; w += blockDim.x) nvp[w] = sh.wv[w];
-            for (int w = threadIdx.x; w < CW; w += blockDim.x) ncp[w] = sh.wc[w];
-        }
-        const bool hit = (sc.rvec[pw] & pb) != 0;
-        __syncthreads();
-        if (hit) {
-            for (int w = threadIdx.x; w < MW; w += blockDim.x) sc.rvec[w] ^= sh.wv[w];
-            for (int w = threadIdx.x; w < CW; w += blockDim.x) sc.rcomb[w] ^= sh.wc[w];
-        }
-        if (threadIdx.x == 0) { sc.piv[p] = rank; sh.ints[30] = rank + 1; }
-        __syncthreads();
-        if (hit) {
-            bool nz = false;
-            for (int w = threadIdx.x; w < MW; w += blockDim.x) nz |= sc.rvec[w] != 0;
-            if (!__syncthreads_or(nz)) {
-                for (int w = threadIdx.x; w < CW; w += blockDim.x) sc.delta[w] = sc.rcomb[w];
-                if (threadIdx.x == 0) sh.ints[31] = j + 1;
-                __syncthreads();
-                break;  // solution found; it is the unique one for every K up to the first dependent column
+        for (int b0 = warp * 32; b0 < rank; b0 += nwarps * 32) {
+            const int b = b0 + lane;
+            unsigned hits = __ballot_sync(0xffffffffu, b < rank && (sc.vec[static_cast<size_t>(b) * MW + pw] & pb));
+            while (hits) {
+                const int bb = b0 + __ffs(hits) - 1;
+                hits &= hits - 1;
+                uint64_t *bv = sc.vec + static_cast<size_t>(bb) * MW;
+                uint64_t *bc = sc.comb + static_cast<size_t>(bb) * CW;
+                for (int w = lane; w < MW; w += 32) bv[w] ^= sh.wv[w];
+                for (int w = lane; w < CW; w += 32) bc[w] ^= sh.wc[w];
             }
         }
+        if (warp == 0) {
+            // append; update the residual of the syndrome difference
+            uint64_t *nvp = sc.vec + static_cast<size_t>(rank) * MW, *ncp = sc.comb + static_cast<size_t>(rank) * CW;
+            for (int w = lane; w < MW; w += 32) nvp[w] = sh.wv[w];
+            for (int w = lane; w < CW; w += 32) ncp[w] = sh.wc[w];
+            const bool hit = (sc.rvec[pw] & pb) != 0;
+            __syncwarp();
+            bool nz = false;
+            if (hit) {
+                for (int w = lane; w < MW; w += 32) nz |= (sc.rvec[w] ^= sh.wv[w]) != 0;
+                for (int w = lane; w < CW; w += 32) sc.rcomb[w] ^= sh.wc[w];
+            }
+            const bool solved = hit && !__any_sync(0xffffffffu, nz);
+            __syncwarp();
+            if (solved) {
+                // the unique solution for every K up to the first dependent column
+                for (int w = lane; w < CW; w += 32) sc.delta[w] = sc.rcomb[w];
+            }
+            if (lane == 0) {
+                sc.piv[p] = rank;
+                sh.ints[30] = rank + 1;
+                if (solved) sh.ints[31] = j + 1;
+            }
+        }
+        __syncthreads();
+        if (sh.ints[31] >= 0) break;
     }
     __syncthreads();
     if (sh.ints[31] < 0) return false;

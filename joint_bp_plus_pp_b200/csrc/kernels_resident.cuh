@@ -96,6 +96,7 @@ struct ResRun {
 
 constexpr int kLearnedTries = 3;   // learned proposals per trial at most
 constexpr int kLearnedMaxUnsat = 30;   // ... and only while max(us_x, us_z) is at most this
+constexpr int kLearnedMaxCols = 512;   // ... solved from at most this many of the best-scored qubits
 
 // Per-block global scratch of a post-processing run: the GF(2) work areas, the ring of the
 // last R iterations' decisions and the |LLR| keys of the OSD order.
@@ -138,8 +139,8 @@ __device__ __forceinline__ float res_lse2(float a, float b) {
     return fmaxf(a, b) + res_lg2(1.0f + res_ex2(-fabsf(a - b)));
 }
 
-constexpr float kResVinMax = 120.0f;   // variable-to-check magnitude clamp (2^-120 is a normal float)
 constexpr float kResCmax = 110.0f;     // check-to-variable magnitude clamp (exact in FP16 storage)
+constexpr int kResSepTest = 24;        // test on its own when at most this many threads failed the last test
 
 __device__ __forceinline__ float with_bit(float a, unsigned b) {
     return __uint_as_float((__float_as_uint(a) & ~1u) | b);
@@ -161,11 +162,15 @@ __host__ __device__ inline size_t res_smem_bytes(int n, int m, int L, size_t sto
 // target.  Returns whether the tested check failed.
 //
 // Stable tanh rule.  Per edge u = 2^-|y|, N = 1 - u, D = 1 + u, t = N / D.  A set of edges is
-// carried as (PN, Q) with PN = prod N and Q = prod D - prod N, so prod D = PN + Q and
-// 1 - T = Q / prod D; joining two sets, Q = PD_a * Q_b + PN_b * Q_a, is a sum of positive terms
-// and keeps full relative precision however close T is to 1.  A single edge has Q = 2u exactly.
-// The output magnitude log2((1 + T) / (1 - T)) = log2((2 PN + Q) / Q) over the other edges
-// therefore grows like min |y| instead of saturating where 1 - T rounds to zero.
+// carried as (PN, H) with PN = prod N and H = (prod D - prod N) / 2, so prod D = PN + 2H and
+// 1 - T = 2H / prod D.  Joining a set with one edge, H' = D H + u PN = H + u (H + PN) and
+// PN' = PN - u PN: sums of positive terms and one rounding each, which keep full relative
+// precision however close T is to 1.  A single edge has H = u exactly, and H of any set is at
+// least the largest u in it; joining two sets a, b: H = PD_a H_b + PN_b H_a.  The output
+// magnitude log2((1 + T) / (1 - T)) over the other edges is log2(1 + PN / H): it grows like
+// min |y| instead of saturating where 1 - T rounds to zero.  H is zero only when every other
+// edge has u = 0 (|y| above 126), and then PN = 1: the output is +inf before the clamp to
+// kResCmax, as it is whenever all other edges are that reliable, so no input clamp is needed.
 template <int P, int J, int L, class ST, int SIDE, int JJ>
 __device__ __forceinline__ bool res_check_row(const ResCode &code, typename ST::T *c2v_all, const float *A_all,
                                               const unsigned *syn_all, int x, bool test) {
@@ -184,32 +189,32 @@ __device__ __forceinline__ bool res_check_row(const ResCode &code, typename ST::
         const float v = a - ST::ld(c2v + l * m);
         const unsigned sv = __float_as_uint(v) & 0x80000000u;
         sgn ^= sv;
-        // sign of the edge kept in u's sign bit, |u| = 2^-min(|v|, kResVinMax)
-        u[l] = __uint_as_float(__float_as_uint(res_ex2(-fminf(fabsf(v), kResVinMax))) | sv);
+        // sign of the edge kept in u's sign bit, |u| = 2^-|v| (flushed to zero above |v| = 126)
+        u[l] = __uint_as_float(__float_as_uint(res_ex2(-fabsf(v))) | sv);
     }
     const bool bad = test && ((par & 1u) != sbit);
-    float sPN[L + 1], sQ[L + 1];
+    // suffix sets {l, .., L-1}
+    float sPN[L + 1], sH[L + 1];
     sPN[L] = 1.0f;
-    sQ[L] = 0.0f;
+    sH[L] = 0.0f;
 #pragma unroll
     for (int l = L - 1; l >= 0; --l) {
         const float au = fabsf(u[l]);
-        const float N = 1.0f - au, D = 1.0f + au, Q = au + au;
-        sQ[l] = fmaf(D, sQ[l + 1], sPN[l + 1] * Q);
-        sPN[l] = N * sPN[l + 1];
+        sH[l] = fmaf(au, sH[l + 1] + sPN[l + 1], sH[l + 1]);
+        sPN[l] = fmaf(-au, sPN[l + 1], sPN[l + 1]);
     }
     sgn ^= sbit << 31;
-    float pPN = 1.0f, pQ = 0.0f;
+    // prefix set {0, .., l-1} joined with the suffix {l+1, .., L-1}
+    float pPN = 1.0f, pH = 0.0f;
 #pragma unroll
     for (int l = 0; l < L; ++l) {
         const float ePN = pPN * sPN[l + 1];
-        const float eQ = fmaf(pPN + pQ, sQ[l + 1], sPN[l + 1] * pQ);
-        const float mag = fminf(res_lg2(fmaf(2.0f, ePN, eQ) * res_rcp(eQ)), kResCmax);
+        const float eH = fmaf(fmaf(2.0f, pH, pPN), sH[l + 1], sPN[l + 1] * pH);
+        const float mag = fminf(res_lg2(fmaf(ePN, res_rcp(eH), 1.0f)), kResCmax);
         ST::st(c2v + l * m, __uint_as_float(__float_as_uint(mag) ^ ((sgn ^ __float_as_uint(u[l])) & 0x80000000u)));
         const float au = fabsf(u[l]);
-        const float N = 1.0f - au, Q = au + au;
-        pQ = fmaf(pPN + pQ, Q, N * pQ);
-        pPN *= N;
+        pH = fmaf(au, pH + pPN, pH);
+        pPN = fmaf(-au, pPN, pPN);
     }
     return bad;
 }
@@ -497,7 +502,7 @@ __device__ __noinline__ bool res_learned_attempt(const ResCode &code, const ResR
     int left = 0;
     for (int side = 0; side < 2; ++side) {
         if (blk_side_diff(run.dc, psh, side) == 0) continue;
-        if (!blk_osd_side(run.dc, key + static_cast<size_t>(side) * n, psh, psc, side)) ++left;
+        if (!blk_osd_side(run.dc, key + static_cast<size_t>(side) * n, psh, psc, side, kLearnedMaxCols)) ++left;
     }
     const bool accepted = left == 0;
     if (accepted)
@@ -717,7 +722,8 @@ __global__ void __launch_bounds__(kResThreads, 1)
         const double pt = run.p_max > run.p ? pt_sh : run.p;
 
         // ---- error and target syndrome
-        for (int w = threadIdx.x; w < 2 * mw; w += blockDim.x) syn[w] = 0u;
+        if (!have_err)
+            for (int w = threadIdx.x; w < 2 * mw; w += blockDim.x) syn[w] = 0u;
         if (run.source == kSrcPhilox) {
             for (int v2 = threadIdx.x; 2 * v2 < n; v2 += blockDim.x) {
                 uint8_t e0, e1;
@@ -756,15 +762,20 @@ __global__ void __launch_bounds__(kResThreads, 1)
                 if (run.src_sz[local * m + c] & 1) atomicOr(&syn[mw + (c >> 5)], 1u << (c & 31));
             }
         } else {
-            for (int r = threadIdx.x; r < 2 * m; r += blockDim.x) {
+            // one syndrome word per warp and step: the 32 lanes take 32 consecutive checks of
+            // one side (m is a multiple of 32), so row r0 / 32 is word side * mw + c / 32
+            static_assert(m % 32 == 0 && kResThreads % 32 == 0, "warp-aligned syndrome words");
+            for (int r0 = threadIdx.x & ~31; r0 < 2 * m; r0 += blockDim.x) {
+                const int r = r0 + (threadIdx.x & 31);
                 const int side = r >= m, c = r - side * m, j = c / P, x = c - j * P;
                 unsigned par = 0;
 #pragma unroll
                 for (int l = 0; l < L; ++l) {
                     const unsigned y = res_map<P>(code.fF[side][j][l], code.fG[side][j][l], static_cast<unsigned>(x));
-                    par ^= (err[l * P + y] >> side) & 1u;
+                    par ^= err[l * P + y];
                 }
-                if (par) atomicOr(&syn[side * mw + (c >> 5)], 1u << (c & 31));
+                const unsigned word = __ballot_sync(0xffffffffu, (par >> side) & 1u);
+                if ((threadIdx.x & 31) == 0) syn[r0 >> 5] = word;
             }
         }
         // ---- BP state: c2v = 0, A = prior LLR of each side's bit
@@ -783,12 +794,17 @@ __global__ void __launch_bounds__(kResThreads, 1)
         // triggers, the flip window and the post-processing attempts (jointbp_ets.cpp:2521-2633).
         int it = 0, rf = 0, iters = run.max_iter;
         bool stall = false;   // (learned) decisions of iteration `it` equal those of it-1, or of it-2
+        int near = 0x7fffffff;   // threads with a failing check at the last test
         for (;;) {
             const bool fused = it >= 1 && it < slow_from &&
                                (it >= run.max_iter ||
                                 (it > run.check_warmup && (it - run.check_warmup) % run.check_interval == 0));
+            // Close to convergence the test runs on its own first: when it passes, the check
+            // phase it would have been fused into is not computed (the same decisions and
+            // iteration counts either way; only the c2v left behind differ).
+            const bool sep = fused && it < run.max_iter && near <= kResSepTest;
             int bx = 0, bz = 0;
-            if (it < run.max_iter) {
+            if (it < run.max_iter && !sep) {
                 bx = res_check_side<P, J, L, ST, 0>(code, c2v, A, syn, fused);
                 bz = res_check_side<P, J, L, ST, 1>(code, c2v, A, syn, fused);
             } else if (fused) {
@@ -803,14 +819,20 @@ __global__ void __launch_bounds__(kResThreads, 1)
                     if (wz) atomicAdd(&us_cnt[it & 1][1], wz);
                 }
             }
-            const bool bad = __syncthreads_or(bx + bz) != 0;
+            const int nbad = __syncthreads_count(bx + bz != 0);
             if (fused) {
-                if (!bad) { rf = kResSyndromeOk | kResBpOk; iters = it; break; }
+                if (nbad == 0) { rf = kResSyndromeOk | kResBpOk; iters = it; break; }
+                near = nbad;
                 if (PP && threadIdx.x == 0)
                     us_hist[it % 100] =
                         static_cast<unsigned short>(min(max(us_cnt[it & 1][0], us_cnt[it & 1][1]), 65535));
             }
             if (it >= run.max_iter) break;
+            if (sep) {
+                res_check_side<P, J, L, ST, 0>(code, c2v, A, syn, false);
+                res_check_side<P, J, L, ST, 1>(code, c2v, A, syn, false);
+                __syncthreads();
+            }
             if (PP && threadIdx.x == 0) us_cnt[(it + 1) & 1][0] = us_cnt[(it + 1) & 1][1] = 0;   // next test's slot
             if constexpr (learned) {
                 unsigned ch1 = 0u, ch2 = 0u;
