@@ -137,8 +137,9 @@ int jbp_decode_syndromes(jbp_ctx *ctx, const jbp_options *opt, long long ntrials
 
 /* jbp_decode_errors with the final LLRs of every trial (precision diagnostics): llr_out is
  * ntrials x n x 2 floats, the natural log of P(bit = 1) / P(bit = 0) of each qubit's x bit and
- * z bit from the check-to-variable messages when the trial ends -- those of its last variable
- * update when the syndrome is tested only at max_iter (check_warmup >= max_iter). */
+ * z bit from the check-to-variable messages the trial ends with.  With the syndrome tested only
+ * at max_iter (check_warmup >= max_iter) these are the messages of its last iteration for every
+ * trial; a trial that stops earlier may end with one more check update. */
 int jbp_decode_errors_llr(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *err, double p,
                           float *llr_out, jbp_trial_result *res, jbp_stats *stats);
 
