@@ -205,6 +205,19 @@ int jbp_collect_stall_states(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed
 int jbp_autotune(jbp_ctx *ctx, const jbp_options *opt, double p, long long probe_trials, jbp_options *best,
                  double *best_trials_per_s);
 
+/* Mixed-size Monte Carlo in one kernel launch (no counterpart in the reference): the trials of
+ * the codes of nctx contexts on one device -- code i decodes trials first_trial[i] ..
+ * first_trial[i] + ntrials[i] - 1 of seed seeds[i] (Philox noise, per-trial p uniform in
+ * [p, opt->p_max) when p_max > p) -- taken by one persistent kernel from one work queue, largest
+ * code first.  Plain BP (opt->enable_pp = 0), FP32 arithmetic with FP32 (JBP_PREC_FP32) or FP16
+ * (JBP_PREC_FP16) message storage; the codes' checks must all have one degree (6, 7 or 8), the
+ * same for every code.  first_trial may be null (every code from trial 1); stats receives one
+ * entry per code; per_trial, if not null, holds nctx host arrays (each null or ntrials[i]
+ * records).  Runs on the first context's stream. */
+int jbp_simulate_mixed(jbp_ctx *const *ctxs, int nctx, const jbp_options *opt, const uint64_t *seeds,
+                       const long long *first_trial, const long long *ntrials, double p, jbp_stats *stats,
+                       jbp_trial_result *const *per_trial);
+
 /* Errors of trials first_trial.. drawn by a device sampler (JBP_SAMPLER_*), copied to the host
  * buffer err (ntrials x n).  The same streams jbp_simulate decodes. */
 int jbp_sample_errors(jbp_ctx *ctx, uint64_t seed, long long first_trial, long long ntrials, double p, int sampler,

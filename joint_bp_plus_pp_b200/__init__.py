@@ -125,6 +125,7 @@ def load_library(path=None):
     lib.jbp_decode_syndromes.argtypes = [vp, ctypes.POINTER(COptions), ll, vp, vp, d, vp, vp, ctypes.POINTER(CStats)]
     lib.jbp_decode_errors_llr.argtypes = [vp, ctypes.POINTER(COptions), ll, vp, d, vp, vp, ctypes.POINTER(CStats)]
     lib.jbp_autotune.argtypes = [vp, ctypes.POINTER(COptions), d, ll, ctypes.POINTER(COptions), ctypes.POINTER(d)]
+    lib.jbp_simulate_mixed.argtypes = [vp, i, ctypes.POINTER(COptions), vp, vp, vp, d, ctypes.POINTER(CStats), vp]
     lib.jbp_decode_errors_device.argtypes = [vp, ctypes.POINTER(COptions), ll, vp, d, vp, vp, ctypes.POINTER(CStats),
                                              vp]
     lib.jbp_sample_errors.argtypes = [vp, ctypes.c_uint64, ll, ll, d, i, vp]
@@ -347,6 +348,30 @@ class Decoder:
                                                              SAMPLER[sampler], capacity, _ptr(x), _ptr(y),
                                                              ctypes.byref(cnt), ctypes.byref(st)))
         return x[:cnt.value], y[:cnt.value], st.as_dict()
+
+
+def simulate_mixed(decoders, ntrials, p, opts=None, seeds=None, first_trial=None, per_trial=False):
+    """Mixed-size Monte Carlo in one kernel launch over the codes of several decoders on one
+    device (jbp_simulate_mixed): code i decodes ntrials[i] Philox trials of seeds[i] from
+    first_trial[i].  Plain BP in FP32 (opts.precision "fp32", or "fp16" message storage).
+    Returns (list of stats, list of per-trial records or None)."""
+    k = len(decoders)
+    lib = decoders[0]._lib
+    opts = opts or Options(precision="fp32", enable_pp=False)
+    ntrials = [int(t) for t in (ntrials if hasattr(ntrials, "__len__") else [ntrials] * k)]
+    seeds = np.asarray(seeds if seeds is not None else [11 + i for i in range(k)], np.uint64)
+    first = np.asarray(first_trial if first_trial is not None else [1] * k, np.int64)
+    ntr = np.asarray(ntrials, np.int64)
+    if len(seeds) != k or len(first) != k or len(ntr) != k:
+        raise ValueError("one seed, first trial and trial count per decoder")
+    ctxs = (ctypes.c_void_p * k)(*[d._h for d in decoders])
+    stats = (CStats * k)()
+    res = [np.zeros(t, TRIAL_DTYPE) for t in ntrials] if per_trial else None
+    ptrs = (ctypes.c_void_p * k)(*[r.ctypes.data for r in res]) if per_trial else None
+    co = opts.to_c()
+    _check(lib, lib.jbp_simulate_mixed(ctxs, k, ctypes.byref(co), _ptr(seeds), _ptr(first), _ptr(ntr), p, stats,
+                                       ptrs))
+    return [s.as_dict() for s in stats], res
 
 
 MLP_PARAMS = 4866

@@ -184,6 +184,43 @@ int jbp_simulate(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed, long long 
     return JBP_OK;
 }
 
+int jbp_simulate_mixed(jbp_ctx *const *ctxs, int nctx, const jbp_options *opt, const uint64_t *seeds,
+                       const long long *first_trial, const long long *ntrials, double p, jbp_stats *stats,
+                       jbp_trial_result *const *per_trial) {
+    if (!ctxs || nctx < 1 || !seeds || !ntrials || !stats) return fail(JBP_ERR_ARG, "invalid argument");
+    jbp::MixedRequest rq;
+    rq.opt = normalized(opt);
+    rq.p = p;
+    for (int i = 0; i < nctx; ++i) {
+        if (!ctxs[i] || ntrials[i] < 0) return fail(JBP_ERR_ARG, "invalid argument");
+        rq.engines.push_back(&ctxs[i]->engine);
+        rq.seeds.push_back(seeds[i]);
+        rq.first_trial.push_back(first_trial ? first_trial[i] : 1);
+        rq.ntrials.push_back(ntrials[i]);
+    }
+    cudaSetDevice(ctxs[0]->engine.device());
+    rq.stream = ctxs[0]->stream;
+    rq.d_res.assign(static_cast<size_t>(nctx), nullptr);
+    if (per_trial)
+        for (int i = 0; i < nctx; ++i)
+            if (per_trial[i] && ntrials[i] > 0) {
+                if (int rc = grow(&ctxs[i]->d_res, &ctxs[i]->res_count, static_cast<size_t>(ntrials[i]))) return rc;
+                rq.d_res[i] = ctxs[i]->d_res;
+            }
+    std::vector<jbp_stats> st;
+    std::string e = jbp::Engine::run_mixed(rq, st);
+    if (!e.empty()) return engine_fail(e);
+    for (int i = 0; i < nctx; ++i) {
+        if (rq.d_res[i]) {
+            cudaError_t ce = cudaMemcpy(per_trial[i], rq.d_res[i], sizeof(jbp_trial_result) * ntrials[i],
+                                        cudaMemcpyDeviceToHost);
+            if (ce != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(ce, "copy results"));
+        }
+        stats[i] = st[i];
+    }
+    return JBP_OK;
+}
+
 static int decode_host(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *err, const uint8_t *sx,
                        const uint8_t *sz, double p, uint8_t *est_out, jbp_trial_result *res, jbp_stats *stats,
                        float *llr_out = nullptr) {

@@ -11,6 +11,7 @@
 #include "kernels_slots.cuh"
 #include "kernels_pp.cuh"
 #include "kernels_resident.cuh"
+#include "kernels_mixed.cuh"
 #include "mlp.cuh"
 
 namespace jbp {
@@ -113,6 +114,8 @@ void fill_stats(const DevCounters &hc, jbp_stats &stats) {
 }  // namespace
 
 Engine::~Engine() {
+    cudaFree(mix_scratch_);
+    cudaFree(mix_cnt_);
     free_buffers();
     delete rcode_;
     cudaFree(res_cnt_);
@@ -815,6 +818,176 @@ std::string Engine::sample_errors(unsigned long long seed, long long first, long
     k_sample_out<<<sm_count_ * 4, 256>>>(model_.n, seed, first, count, p, source, d_out);
     JBP_CUDA_TRY(cudaGetLastError(), "sample launch");
     JBP_CUDA_TRY(cudaStreamSynchronize(nullptr), "sample");
+    return "";
+}
+
+
+// ---------------------------------------------------------------- mixed-size launch
+
+std::string Engine::mixed_slots() {
+    if (mix_slot_[0]) return "";
+    for (int s = 0; s < 2; ++s) {
+        const SideGraph &g = model_.side[s];
+        const int dv = std::max(1, g.dv_max);
+        std::vector<int> sl(static_cast<size_t>(model_.n) * dv, -1);
+        for (int v = 0; v < model_.n; ++v)
+            for (int k = g.var_off[v]; k < g.var_off[v + 1]; ++k) {
+                const int e = g.var_edge[k], c = e / g.dc_max, pos = e - c * g.dc_max;
+                sl[static_cast<size_t>(v) * dv + (k - g.var_off[v])] = pos * g.m + c;
+            }
+        int *p = nullptr;
+        std::string e = dev_upload(code_allocs_, sl, &p);
+        if (!e.empty()) return e;
+        mix_slot_[s] = p;
+    }
+    return "";
+}
+
+namespace {
+template <int DC>
+void *mixed_kernel(int precision) {
+    return precision == JBP_PREC_FP16 ? reinterpret_cast<void *>(k_mixed<DC, StoreHalf>)
+                                      : reinterpret_cast<void *>(k_mixed<DC, StoreFloat>);
+}
+}  // namespace
+
+std::string Engine::run_mixed(const MixedRequest &rq, std::vector<jbp_stats> &stats) {
+    const int nc = static_cast<int>(rq.engines.size());
+    stats.assign(static_cast<size_t>(std::max(nc, 0)), jbp_stats{});
+    for (jbp_stats &s : stats) std::memset(&s, 0, sizeof(s));
+    if (nc < 1 || nc > kMixMaxCodes) return "the mixed launch takes 1 to 8 codes";
+    if (rq.seeds.size() != static_cast<size_t>(nc) || rq.ntrials.size() != static_cast<size_t>(nc) ||
+        rq.first_trial.size() != static_cast<size_t>(nc))
+        return "one seed, first trial and trial count per code";
+    const jbp_options &o = rq.opt;
+    if (o.precision != JBP_PREC_FP32 && o.precision != JBP_PREC_FP16)
+        return "FP64 is not available in the mixed launch (FP32 arithmetic: precision FP32, or FP16 storage)";
+    if (o.enable_pp) return "post-processing is not available in the mixed launch (plain BP)";
+    if (o.damping > 0.0 || o.freeze_syn || o.learned_from > 0)
+        return "damping, freeze-syn and the learned proposal are not available in the mixed launch";
+    if (o.max_iter < 1) return "max_iter must be >= 1";
+    if (o.use_prior) {
+        for (int i = 0; i < 4; ++i)
+            if (!(o.prior[i] >= 0.0 && o.prior[i] <= 1.0)) return "prior entries must be in [0, 1]";
+    } else if (!(rq.p > 0.0 && rq.p < 1.0)) {
+        return "p must be in (0, 1)";
+    }
+    if (o.p_max > rq.p && !(o.p_max < 1.0)) return "p_max must be below 1";
+    Engine &e0 = *rq.engines[0];
+    const int DC = e0.model_.side[0].dc_max;
+    for (Engine *e : rq.engines) {
+        if (!e || e->device_ != e0.device_) return "the codes of a mixed launch must be on one device";
+        for (int s = 0; s < 2; ++s)
+            if (!e->model_.side[s].checks_regular || e->model_.side[s].dc_max != DC)
+                return "the codes of a mixed launch need a code-wide check degree, the same for every code";
+    }
+    void *kern = DC == 6 ? mixed_kernel<6>(o.precision)
+                         : DC == 7 ? mixed_kernel<7>(o.precision) : DC == 8 ? mixed_kernel<8>(o.precision) : nullptr;
+    if (!kern) return "check degrees other than 6, 7 and 8 are not available in the mixed launch";
+    JBP_CUDA_TRY(cudaSetDevice(e0.device_), "cudaSetDevice");
+    cudaFuncAttributes fa{};
+    JBP_CUDA_TRY(cudaFuncGetAttributes(&fa, kern), "kernel attributes");
+    const size_t limit = static_cast<size_t>(e0.smem_optin_) - fa.sharedSizeBytes;
+    const size_t es = o.precision == JBP_PREC_FP16 ? 2 : 4;
+    // largest codes first: the launch's tail is made of the shortest trials
+    std::vector<int> order(nc);
+    for (int i = 0; i < nc; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return rq.engines[a]->model_.n > rq.engines[b]->model_.n; });
+    size_t smem = 0, scratch = 0;
+    std::vector<size_t> base(nc), full(nc);
+    for (int i = 0; i < nc; ++i) {
+        const CodeModel &m = rq.engines[i]->model_;
+        base[i] = mix_state_bytes(m.n, m.side[0].m, m.side[1].m);
+        full[i] = base[i] + mix_c2v_bytes(m.side[0].m, m.side[1].m, DC, es);
+        if (base[i] > limit) return "a code of the mixed launch is too large for one block's shared memory";
+        if (full[i] - base[i] < 16ull * ((m.n + 63) / 64))
+            return "codes with fewer check edges than 2 bits per variable are not available in the mixed launch";
+        smem = std::max(smem, full[i] <= limit ? full[i] : base[i]);
+    }
+    for (int i = 0; i < nc; ++i)
+        if (full[i] > smem) scratch = std::max(scratch, (full[i] - base[i] + 255) / 256 * 256);
+    JBP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+                 "smem attribute");
+    int per_sm = 0;
+    JBP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kMixThreads, smem), "occupancy");
+    if (per_sm < 1) return "the mixed kernel does not fit on an SM";
+    long long total = 0;
+    for (int i = 0; i < nc; ++i) {
+        if (rq.ntrials[i] < 0) return "invalid trial count";
+        total += rq.ntrials[i];
+    }
+    if (total == 0) return "";
+    const int grid = static_cast<int>(std::min<long long>(static_cast<long long>(per_sm) * e0.sm_count_, total));
+    if (scratch * grid > e0.mix_scratch_bytes_) {
+        cudaFree(e0.mix_scratch_);
+        e0.mix_scratch_ = nullptr;
+        e0.mix_scratch_bytes_ = 0;
+        JBP_CUDA_TRY(cudaMalloc(&e0.mix_scratch_, scratch * grid), "cudaMalloc(mixed scratch)");
+        e0.mix_scratch_bytes_ = scratch * grid;
+    }
+    if (!e0.mix_cnt_) JBP_CUDA_TRY(cudaMalloc(&e0.mix_cnt_, sizeof(DevCounters) * (kMixMaxCodes + 1)),
+                                   "cudaMalloc(mixed counters)");
+    MixRun r{};
+    r.ncodes = nc;
+    r.next = reinterpret_cast<unsigned long long *>(e0.mix_cnt_ + kMixMaxCodes);
+    r.max_iter = o.max_iter;
+    r.check_warmup = std::max(0, o.check_warmup);
+    r.check_interval = std::max(1, o.check_interval);
+    r.p = rq.p;
+    r.p_max = o.p_max;
+    r.use_prior = o.use_prior ? 1 : 0;
+    for (int i = 0; i < 4; ++i) r.prior4[i] = o.prior[i];
+    r.scratch = e0.mix_scratch_;
+    r.scratch_stride = scratch;
+    long long end = 0;
+    for (int k = 0; k < nc; ++k) {
+        const int i = order[k];
+        Engine &e = *rq.engines[i];
+        std::string err = e.mixed_slots();
+        if (!err.empty()) return err;
+        MixCode &mc = r.code[k];
+        mc.dc = e.dcode_;
+        mc.slot[0] = e.mix_slot_[0];
+        mc.slot[1] = e.mix_slot_[1];
+        mc.seed = rq.seeds[i];
+        mc.first_trial = rq.first_trial[i];
+        mc.ntrials = rq.ntrials[i];
+        end += rq.ntrials[i];
+        mc.item_end = end;
+        mc.cnt = e0.mix_cnt_ + k;
+        mc.res_out = i < static_cast<int>(rq.d_res.size()) ? rq.d_res[i] : nullptr;
+        mc.c2v_in_smem = full[i] <= smem ? 1 : 0;
+    }
+    cudaStream_t st = rq.stream;
+    cudaEvent_t ev0, ev1;
+    JBP_CUDA_TRY(cudaEventCreate(&ev0), "cudaEventCreate");
+    JBP_CUDA_TRY(cudaEventCreate(&ev1), "cudaEventCreate");
+    cudaError_t ce = cudaEventRecord(ev0, st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(e0.mix_cnt_, 0, sizeof(DevCounters) * (kMixMaxCodes + 1), st);
+    if (ce == cudaSuccess) {
+        void *args[] = {&r};
+        ce = cudaLaunchKernel(kern, dim3(grid), dim3(kMixThreads), args, smem, st);
+    }
+    if (ce == cudaSuccess) ce = cudaEventRecord(ev1, st);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(ev1);
+    std::vector<DevCounters> hc(kMixMaxCodes);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpy(hc.data(), e0.mix_cnt_, sizeof(DevCounters) * kMixMaxCodes, cudaMemcpyDeviceToHost);
+    float ms = 0.0f;
+    if (ce == cudaSuccess) cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    if (ce != cudaSuccess) return cuda_err(ce, "mixed run");
+    for (int k = 0; k < nc; ++k) {
+        const int i = order[k];
+        if (hc[k].done != static_cast<unsigned long long>(rq.ntrials[i]))
+            return "mixed run finished an unexpected number of trials";
+        fill_stats(hc[k], stats[i]);
+        stats[i].device_ms = ms;
+        stats[i].kernel_launches = 1;
+        stats[i].slots = grid;
+    }
     return "";
 }
 

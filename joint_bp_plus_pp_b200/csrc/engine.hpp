@@ -35,6 +35,20 @@ struct RunRequest {
     long long col_cap = 0;
 };
 
+class Engine;
+
+// Mixed-size Monte Carlo in one launch (kernels_mixed.cuh): the codes of several engines on
+// one device, trials first_trial[i] .. of code i with seed seeds[i].
+struct MixedRequest {
+    std::vector<Engine *> engines;
+    jbp_options opt{};
+    std::vector<unsigned long long> seeds;
+    std::vector<long long> first_trial, ntrials;
+    double p = 0.05;
+    std::vector<jbp_trial_result *> d_res;   // per code, optional device buffers
+    cudaStream_t stream = nullptr;
+};
+
 class Engine {
 public:
     Engine() = default;
@@ -53,6 +67,8 @@ public:
     // Learned flip proposal parameters (FP32, mlp.cuh layout); null removes the model.
     std::string set_flip_model(const float *params);
     int sm_count() const { return sm_count_; }
+    // One launch over the codes of rq.engines; stats[i] for code i.
+    static std::string run_mixed(const MixedRequest &rq, std::vector<jbp_stats> &stats);
 
 private:
     struct Buffers {
@@ -94,8 +110,15 @@ private:
     void free_buffers();
     int choose_slots(const jbp_options &opt, long long ntrials) const;
 
+    // the variables' c2v slot tables of the mixed launch, built on first use
+    std::string mixed_slots();
+
     int device_ = 0;
     int sm_count_ = 0;
+    const int *mix_slot_[2] = {nullptr, nullptr};
+    unsigned char *mix_scratch_ = nullptr;   // per-block c2v of the codes that do not fit shared memory
+    size_t mix_scratch_bytes_ = 0;
+    DevCounters *mix_cnt_ = nullptr;         // kMixMaxCodes counters + the work counter
     int smem_optin_ = 0;
     bool res_code_ok_ = false;
     std::string res_code_why_;

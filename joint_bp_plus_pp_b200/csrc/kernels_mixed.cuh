@@ -1,0 +1,289 @@
+// Mixed-size Monte Carlo in one launch: the trials of several codes (any check-regular CSS
+// codes with the same check degree DC, e.g. hypergraph products of (3,4)-regular classical
+// codes, n = 1,600 ... 14,400, variable degrees 3 and 4) decoded by one persistent kernel.
+// One block of 768 threads per SM takes work items -- (code, trial) pairs, the codes in the
+// host's order, largest first -- from one atomic counter, so trials of all sizes share the
+// SMs with no partition to tune and the tail of the launch is made of the smallest trials.
+//
+// Per trial, in shared memory: A [side][v] (FP32 variable totals, decision bit in the lowest
+// mantissa bit, as in kernels_resident.cuh), the error [v] and the target syndrome bits; the
+// check-to-variable messages c2v [side][i][c] (edge i of check c) stay in shared memory when
+// the code's trial fits beside them (the launch's shared size is the largest such trial), and
+// otherwise in a per-block global scratch that stays in L2.  Neighbours come from tables:
+// check c's variables chk_var[c*DC + i] (the code's own table) and each variable's c2v slots
+// slot[v*dv + k] = i*m + c (-1 for the missing edges of lower-degree variables), built on the
+// host.  The check phase reads its c2v row by row (lanes take consecutive checks: coalesced or
+// conflict-free), the variable phase gathers.
+//
+// Arithmetic per edge and per variable is the resident engine's (the stable tanh rule in
+// (PN, H) form, the exact 4-ary coupling, the flooding schedule with early exit and the
+// syndrome test fused into the next check phase, jointbp_ets.cpp:1943-2535); classification
+// as jointbp_ets.cpp:6199-6211.  No post-processing: the mixed workload decodes with plain BP.
+#pragma once
+
+#include "kernels_resident.cuh"
+
+namespace jbp {
+
+constexpr int kMixThreads = 768;
+constexpr int kMixMaxCodes = 8;
+
+struct MixCode {
+    DevCode dc;                    // n, per-side m / dc / dv, chk_var, basis rows (classification)
+    const int *slot[2];            // [n][dv] c2v slot of each variable's edges, -1 pads
+    unsigned long long seed;
+    long long first_trial, ntrials;
+    long long item_end;            // work items of codes 0..this one
+    DevCounters *cnt;
+    jbp_trial_result *res_out;     // optional, [ntrials]
+    int c2v_in_smem;
+};
+
+struct MixRun {
+    MixCode code[kMixMaxCodes];
+    int ncodes;
+    unsigned long long *next;      // work counter
+    int max_iter, check_warmup, check_interval;
+    double p, p_max;
+    int use_prior;
+    double prior4[4];
+    unsigned char *scratch;        // per block, scratch_stride bytes (c2v of the codes that do not fit)
+    size_t scratch_stride;
+    unsigned long long *bad_input;
+};
+
+__host__ __device__ inline size_t mix_align(size_t b) { return (b + 15) / 16 * 16; }
+
+// Shared bytes of a trial of a code without and with its c2v.
+__host__ __device__ inline size_t mix_state_bytes(int n, int mx, int mz) {
+    const int mw = (mx > mz ? mx : mz) / 32 + 1;
+    return mix_align(8ull * n) + mix_align(static_cast<size_t>(n)) + mix_align(8ull * mw);
+}
+__host__ __device__ inline size_t mix_c2v_bytes(int mx, int mz, int dc, size_t store_bytes) {
+    return mix_align(store_bytes * dc * (static_cast<size_t>(mx) + mz));
+}
+
+// New c2v of check c of one side (its DC edges at c2v[i*m + c]); with `test`, also whether
+// the decisions in A's low bits fail the check.  The stable tanh rule of res_check_row.
+template <int DC, class ST>
+__device__ __forceinline__ bool mix_check_row(const int *__restrict__ chk_var, typename ST::T *c2v, int m,
+                                              const float *A, int c, unsigned sbit, bool test) {
+    int vv[DC];
+#pragma unroll
+    for (int i = 0; i < DC; ++i) vv[i] = __ldg(chk_var + static_cast<size_t>(c) * DC + i);
+    float u[DC];
+    unsigned sgn = 0u, par = 0u;
+#pragma unroll
+    for (int i = 0; i < DC; ++i) {
+        const float a = A[vv[i]];
+        par ^= __float_as_uint(a);
+        const float v = a - ST::ld(c2v + static_cast<size_t>(i) * m + c);
+        const unsigned sv = __float_as_uint(v) & 0x80000000u;
+        sgn ^= sv;
+        u[i] = __uint_as_float(__float_as_uint(res_ex2(-fabsf(v))) | sv);
+    }
+    const bool bad = test && ((par & 1u) != sbit);
+    float sPN[DC + 1], sH[DC + 1];
+    sPN[DC] = 1.0f;
+    sH[DC] = 0.0f;
+#pragma unroll
+    for (int i = DC - 1; i >= 0; --i) {
+        const float au = fabsf(u[i]);
+        sH[i] = fmaf(au, sH[i + 1] + sPN[i + 1], sH[i + 1]);
+        sPN[i] = fmaf(-au, sPN[i + 1], sPN[i + 1]);
+    }
+    sgn ^= sbit << 31;
+    float pPN = 1.0f, pH = 0.0f;
+#pragma unroll
+    for (int i = 0; i < DC; ++i) {
+        const float ePN = pPN * sPN[i + 1];
+        const float eH = fmaf(fmaf(2.0f, pH, pPN), sH[i + 1], sPN[i + 1] * pH);
+        const float mag = fminf(res_lg2(fmaf(ePN, res_rcp(eH), 1.0f)), kResCmax);
+        ST::st(c2v + static_cast<size_t>(i) * m + c,
+               __uint_as_float(__float_as_uint(mag) ^ ((sgn ^ __float_as_uint(u[i])) & 0x80000000u)));
+        const float au = fabsf(u[i]);
+        pH = fmaf(au, pH + pPN, pH);
+        pPN = fmaf(-au, pPN, pPN);
+    }
+    return bad;
+}
+
+// Syndrome test alone (the decisions in A's low bits against the target): failing checks of
+// this thread on one side.
+template <int DC>
+__device__ __forceinline__ int mix_test_side(const int *__restrict__ chk_var, int m, const float *A,
+                                             const unsigned *syn) {
+    int bad = 0;
+    for (int c = threadIdx.x; c < m; c += blockDim.x) {
+        unsigned par = 0;
+#pragma unroll
+        for (int i = 0; i < DC; ++i) par ^= __float_as_uint(A[__ldg(chk_var + static_cast<size_t>(c) * DC + i)]);
+        bad += (par & 1u) != ((syn[c >> 5] >> (c & 31)) & 1u);
+    }
+    return bad;
+}
+
+// Variable v: sums of its X and Z c2v, hard decision, new totals (res_var_col without the
+// decision history).
+template <class ST>
+__device__ __forceinline__ void mix_var(const int *__restrict__ slot_x, int dvx, const int *__restrict__ slot_z,
+                                        int dvz, const typename ST::T *c2v_x, const typename ST::T *c2v_z, float *A,
+                                        int n, int v, const float4 lp, const float4 pr) {
+    float Lam = 0.0f, Mu = 0.0f;
+    for (int k = 0; k < dvx; ++k) {
+        const int s = __ldg(slot_x + static_cast<size_t>(v) * dvx + k);
+        if (s >= 0) Lam += ST::ld(c2v_x + s);
+    }
+    for (int k = 0; k < dvz; ++k) {
+        const int s = __ldg(slot_z + static_cast<size_t>(v) * dvz + k);
+        if (s >= 0) Mu += ST::ld(c2v_z + s);
+    }
+    const float w0 = lp.x, w1 = lp.y - Lam, w2 = lp.z - Mu, w3 = lp.w - Lam - Mu;
+    unsigned best = 0;
+    float bv = w0;
+    if (w1 > bv) { best = 1; bv = w1; }
+    if (w2 > bv) { best = 2; bv = w2; }
+    if (w3 > bv) { best = 3; }
+    const float Gx = res_couple(Mu, pr.x, pr.z, pr.y, pr.w);
+    const float Hz = res_couple(Lam, pr.x, pr.y, pr.z, pr.w);
+    A[v] = with_bit(Lam + Gx, best & 1u);
+    A[n + v] = with_bit(Mu + Hz, best >> 1);
+}
+
+template <int DC, class ST>
+__global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant__ MixRun run) {
+    extern __shared__ __align__(16) unsigned char mix_smem[];
+    using T = typename ST::T;
+    __shared__ long long item_sh;
+    __shared__ int code_sh;
+    __shared__ float4 lp_sh, pr_sh;
+    __shared__ float lpx_sh, lpz_sh;
+    __shared__ int ints[16];
+    if (threadIdx.x < 16) ints[threadIdx.x] = 0;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const unsigned long long k = atomicAdd(run.next, 1ull);
+            const long long total = run.code[run.ncodes - 1].item_end;
+            long long item = k < static_cast<unsigned long long>(total) ? static_cast<long long>(k) : -1;
+            int ci = 0;
+            if (item >= 0) {
+                while (item >= run.code[ci].item_end) ++ci;
+                item -= ci > 0 ? run.code[ci - 1].item_end : 0;
+            }
+            item_sh = item;
+            code_sh = ci;
+            if (item >= 0) {
+                const double pt = run.p_max > run.p
+                                      ? trial_p(run.p, run.p_max, run.code[ci].seed, run.code[ci].first_trial + item)
+                                      : run.p;
+                res_set_prior(run.use_prior, run.prior4, pt, &lp_sh, &pr_sh, &lpx_sh, &lpz_sh);
+            }
+        }
+        __syncthreads();
+        const long long local = item_sh;
+        if (local < 0) break;
+        const MixCode &mc = run.code[code_sh];
+        const int n = mc.dc.n, mx = mc.dc.s[0].m, mz = mc.dc.s[1].m;
+        const int mwx = (mx + 31) / 32, mwz = (mz + 31) / 32;
+        const long long t = mc.first_trial + local;
+        const double pt = run.p_max > run.p ? trial_p(run.p, run.p_max, mc.seed, t) : run.p;
+        float *const A = reinterpret_cast<float *>(mix_smem);
+        uint8_t *const err = mix_smem + mix_align(8ull * n);
+        unsigned *const syn = reinterpret_cast<unsigned *>(err + mix_align(static_cast<size_t>(n)));
+        unsigned *const synz = syn + mwx;
+        T *const c2v = mc.c2v_in_smem
+                           ? reinterpret_cast<T *>(mix_smem + mix_state_bytes(n, mx, mz))
+                           : reinterpret_cast<T *>(run.scratch + run.scratch_stride * blockIdx.x);
+        T *const c2vz = c2v + static_cast<size_t>(DC) * mx;
+        const int dvx = mc.dc.s[0].dv, dvz = mc.dc.s[1].dv;
+
+        // ---- error (Philox, the stream of the other engines), target syndrome, BP state
+        for (int w = threadIdx.x; w < mwx + mwz; w += blockDim.x) syn[w] = 0u;
+        for (int v2 = threadIdx.x; 2 * v2 < n; v2 += blockDim.x) {
+            uint8_t e0, e1;
+            sample_philox_pair(mc.seed, t, v2, pt, e0, e1);
+            err[2 * v2] = e0;
+            if (2 * v2 + 1 < n) err[2 * v2 + 1] = e1;
+        }
+        __syncthreads();
+        for (int r = threadIdx.x; r < mx + mz; r += blockDim.x) {
+            const int side = r >= mx, c = r - side * mx;
+            const int *cv = mc.dc.s[side].chk_var + static_cast<size_t>(c) * DC;
+            unsigned par = 0;
+#pragma unroll
+            for (int i = 0; i < DC; ++i) par ^= err[__ldg(cv + i)];
+            if ((par >> side) & 1u) atomicOr(&(side ? synz : syn)[c >> 5], 1u << (c & 31));
+        }
+        {
+            const size_t nmsg = static_cast<size_t>(DC) * (mx + mz);
+            for (size_t i = threadIdx.x; i < nmsg; i += blockDim.x) c2v[i] = T(0.0f);
+            const float ax = with_bit(lpx_sh, 0u), az = with_bit(lpz_sh, 0u);
+            for (int v = threadIdx.x; v < n; v += blockDim.x) { A[v] = ax; A[n + v] = az; }
+        }
+        __syncthreads();
+
+        // ---- BP iterations (it = completed iterations; the test of iteration it rides in the
+        // check phase of iteration it + 1)
+        int it = 0, rf = 0, iters = run.max_iter;
+        const float4 lp = lp_sh, pr = pr_sh;
+        for (;;) {
+            const bool fused = it >= 1 && (it >= run.max_iter ||
+                                           (it > run.check_warmup && (it - run.check_warmup) % run.check_interval == 0));
+            int bad = 0;
+            if (it < run.max_iter) {
+                for (int c = threadIdx.x; c < mx; c += blockDim.x)
+                    bad += mix_check_row<DC, ST>(mc.dc.s[0].chk_var, c2v, mx, A, c, (syn[c >> 5] >> (c & 31)) & 1u,
+                                                 fused);
+                for (int c = threadIdx.x; c < mz; c += blockDim.x)
+                    bad += mix_check_row<DC, ST>(mc.dc.s[1].chk_var, c2vz, mz, A + n, c,
+                                                 (synz[c >> 5] >> (c & 31)) & 1u, fused);
+            } else if (fused) {
+                bad = mix_test_side<DC>(mc.dc.s[0].chk_var, mx, A, syn) +
+                      mix_test_side<DC>(mc.dc.s[1].chk_var, mz, A + n, synz);
+            }
+            const bool any = __syncthreads_or(bad) != 0;
+            if (fused && !any) { rf = kResSyndromeOk | kResBpOk; iters = it; break; }
+            if (it >= run.max_iter) break;
+            for (int v = threadIdx.x; v < n; v += blockDim.x)
+                mix_var<ST>(mc.slot[0], dvx, mc.slot[1], dvz, c2v, c2vz, A, n, v, lp, pr);
+            __syncthreads();
+            ++it;
+        }
+        const bool ok = (rf & kResSyndromeOk) != 0;
+
+        // ---- classification (jointbp_ets.cpp:6199-6211): exact, stabilizer-equivalent residual
+        const int words = (n + 63) / 64, w32 = 2 * words;
+        unsigned *rx = reinterpret_cast<unsigned *>(c2v);     // the messages are no longer needed
+        unsigned *rz = rx + w32;
+        for (int w = threadIdx.x; w < 2 * w32; w += blockDim.x) rx[w] = 0u;
+        __syncthreads();
+        bool exact = true;
+        for (int base = (threadIdx.x >> 5) * 32; base < n; base += blockDim.x) {
+            const int v = base + (threadIdx.x & 31);
+            const bool in = v < n;
+            const unsigned e = in ? ((__float_as_uint(A[v]) & 1u) | ((__float_as_uint(A[n + v]) & 1u) << 1)) : 0u;
+            const unsigned tv = in ? err[v] : e;
+            exact &= tv == e;
+            const unsigned bxm = __ballot_sync(0xffffffffu, ((tv ^ e) & 1u) != 0);
+            const unsigned bzm = __ballot_sync(0xffffffffu, ((tv ^ e) & 2u) != 0);
+            if ((threadIdx.x & 31) == 0) { rx[base >> 5] = bxm; rz[base >> 5] = bzm; }
+        }
+        exact = __syncthreads_and(exact) != 0;
+        bool stab = false;
+        if (ok && !exact) {
+            stab = res_in_row_space(reinterpret_cast<uint64_t *>(rx), words, mc.dc.basis_rows[1], mc.dc.pivot_row[1],
+                                    ints + 8);
+            if (stab)
+                stab = res_in_row_space(reinterpret_cast<uint64_t *>(rz), words, mc.dc.basis_rows[0],
+                                        mc.dc.pivot_row[0], ints + 8);
+        } else if (ok) {
+            stab = true;
+        }
+        const bool success = ok && stab;
+        if (threadIdx.x == 0)
+            account_trial(mc.cnt, nullptr, mc.res_out, run.max_iter, local, iters, rf, ok, success, exact, stab);
+        __syncthreads();
+    }
+}
+
+}  // namespace jbp

@@ -120,6 +120,13 @@ struct StoreHalf {
     static __device__ __forceinline__ void st(T *p, float v) { *p = __float2half_rn(v); }
 };
 
+// 32-bit message storage.
+struct StoreFloat {
+    using T = float;
+    static __device__ __forceinline__ float ld(const T *p) { return *p; }
+    static __device__ __forceinline__ void st(T *p, float v) { *p = v; }
+};
+
 __device__ __forceinline__ float res_ex2(float x) {
     float y;
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -645,11 +652,11 @@ __device__ __noinline__ void res_write_llr(const ResCode &code, const typename S
 
 // Prior of a trial (error rate pt; thread 0, once per run or per trial; out of line): FP64 as
 // the slot engine's refill, then its log2 weights and probabilities in FP32.
-__device__ __noinline__ void res_set_prior(const ResRun &run, double pt, float4 *lp, float4 *pr, float *lpx,
-                                           float *lpz) {
+__device__ __noinline__ void res_set_prior(int use_prior, const double *prior4, double pt, float4 *lp, float4 *pr,
+                                           float *lpx, float *lpz) {
     double q[4];
-    if (run.use_prior) {
-        for (int i = 0; i < 4; ++i) q[i] = run.prior4[i];
+    if (use_prior) {
+        for (int i = 0; i < 4; ++i) q[i] = prior4[i];
     } else {
         q[0] = 1.0 - pt; q[1] = pt / 3.0; q[2] = q[1]; q[3] = q[1];
         const double s = ((q[0] + q[1]) + q[2]) + q[3];
@@ -691,7 +698,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
 
     __shared__ double pt_sh;
     if (threadIdx.x == 0) {
-        res_set_prior(run, run.p, &lp_sh, &pr_sh, &lpx_sh, &lpz_sh);
+        res_set_prior(run.use_prior, run.prior4, run.p, &lp_sh, &pr_sh, &lpx_sh, &lpz_sh);
         for (int i = 0; i < 16; ++i) ints[i] = 0;
     }
     __syncthreads();
@@ -713,7 +720,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
         if (run.p_max > run.p) {
             if (threadIdx.x == 0) {
                 pt_sh = trial_p(run.p, run.p_max, run.seed, t);
-                res_set_prior(run, pt_sh, &lp_sh, &pr_sh, &lpx_sh, &lpz_sh);
+                res_set_prior(run.use_prior, run.prior4, pt_sh, &lp_sh, &pr_sh, &lpx_sh, &lpz_sh);
             }
             __syncthreads();
         } else if (threadIdx.x == 0) {

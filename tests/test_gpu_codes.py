@@ -64,14 +64,69 @@ def test_mixed_size_batch_concurrently():
     """The four hypergraph-product codes (n = 1,600 ... 14,400) decoded at once from four host
     threads, each context on its own stream."""
     from joint_bp_plus_pp_b200 import Options
-    from joint_bp_plus_pp_b200.mixed import build, simulate_mixed
+    from joint_bp_plus_pp_b200.mixed import build, simulate_concurrent
     decs = build()
     assert [d.n for d in decs] == [1600, 3600, 6400, 14400]
     opts = Options(precision="fp32", max_iter=200, enable_pp=False, p_max=0.06)
-    stats, wall = simulate_mixed(decs, 1000, opts)
+    stats, wall = simulate_concurrent(decs, 1000, opts)
     assert all(s["trials"] == 1000 for s in stats) and wall > 0
     solo, _ = decs[0].simulate(11, 1000, 0.01, opts, per_trial=False)
     assert (solo["failures"], solo["total_iters"]) == (stats[0]["failures"], stats[0]["total_iters"])
+
+
+@pytest.fixture(scope="module")
+def mixed_codes():
+    from joint_bp_plus_pp_b200.mixed import build
+    return build()
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+def test_mixed_one_launch_agrees_with_fp64(mixed_codes, prec):
+    """The four codes (n = 1,600 ... 14,400; the largest keeps its messages in global memory,
+    the others in shared memory) in one launch: every code's records are consistent with its
+    counters, and its outcomes and iteration counts agree with FP64 BP (slot engine) on the
+    same Philox trials with the same per-trial p."""
+    from joint_bp_plus_pp_b200 import Options, simulate_mixed
+    T, seeds = 600, [21, 22, 23, 24]
+    base = dict(max_iter=200, enable_pp=False, p_max=0.04)
+    stats, res = simulate_mixed(mixed_codes, [T] * 4, 0.01, Options(precision=prec, **base), seeds=seeds,
+                                per_trial=True)
+    for d, s, r, seed in zip(mixed_codes, stats, res, seeds):
+        assert s["trials"] == T and s["kernel_launches"] == 1
+        assert s["failures"] == int((r["success"] == 0).sum())
+        assert s["total_iters"] == int(r["iterations"].sum())
+        assert s["exact"] == int(r["exact"].sum())
+        assert (r["success"] <= r["syndrome_ok"]).all() and (r["exact"] <= r["success"]).all()
+        _, r64 = d.simulate(seed, T, 0.01, Options(precision="fp64", **base))
+        assert abs(int(r["success"].sum()) - int(r64["success"].sum())) <= max(4, T // 50), d.n
+        assert (r["success"] == r64["success"]).mean() >= 0.97, d.n
+        assert (r["iterations"] == r64["iterations"]).mean() >= 0.85, d.n
+
+
+def test_mixed_one_launch_is_per_trial_deterministic(mixed_codes):
+    """A code's trials decode the same whatever else shares the launch and in whatever order."""
+    from joint_bp_plus_pp_b200 import Options, simulate_mixed
+    o = Options(precision="fp32", max_iter=200, enable_pp=False, p_max=0.06)
+    _, all4 = simulate_mixed(mixed_codes, [300] * 4, 0.01, o, seeds=[5, 6, 7, 8], per_trial=True)
+    _, rev = simulate_mixed(mixed_codes[::-1], [300] * 4, 0.01, o, seeds=[8, 7, 6, 5], per_trial=True)
+    _, one = simulate_mixed([mixed_codes[2]], [300], 0.01, o, seeds=[7], per_trial=True)
+    for i in range(4):
+        assert (all4[i] == rev[3 - i]).all()
+    assert (all4[2] == one[0]).all()
+
+
+def test_mixed_one_launch_refuses_what_it_does_not_run(mixed_codes):
+    from joint_bp_plus_pp_b200 import Decoder, JbpError, Options, simulate_mixed
+    n, xo, xv, zo, zv = hgp_code(32, 3, dv=3, dc=3)      # checks of weight 6 beside weight 7
+    other = Decoder.from_checks(n, xo, xv, zo, zv)
+    for decs, o in ((mixed_codes[:2], Options(precision="fp64", enable_pp=False)),
+                    (mixed_codes[:2], Options(precision="fp32", enable_pp=True)),
+                    ([mixed_codes[0], other], Options(precision="fp32", enable_pp=False))):
+        with pytest.raises(JbpError) as e:
+            simulate_mixed(decs, [8] * len(decs), 0.02, o)
+        assert e.value.code == 4, str(e.value)
+    st, _ = simulate_mixed([other], [64], 0.02, Options(precision="fp32", enable_pp=False, max_iter=50))
+    assert st[0]["trials"] == 64
 
 
 def test_cli_decodes_a_check_list_code(tmp_path):
