@@ -828,17 +828,22 @@ std::string Engine::mixed_slots() {
     if (mix_slot_[0]) return "";
     for (int s = 0; s < 2; ++s) {
         const SideGraph &g = model_.side[s];
-        const int dv = std::max(1, g.dv_max);
-        std::vector<int> sl(static_cast<size_t>(model_.n) * dv, -1);
-        for (int v = 0; v < model_.n; ++v)
+        const int dv = std::max(1, g.dv_max), dc = g.dc_max, m = g.m, n = model_.n;
+        // variable -> c2v slot, k-major; check -> variable, i-major (both read coalesced)
+        std::vector<int> sl(static_cast<size_t>(n) * dv, -1), ck(static_cast<size_t>(m) * dc);
+        for (int v = 0; v < n; ++v)
             for (int k = g.var_off[v]; k < g.var_off[v + 1]; ++k) {
-                const int e = g.var_edge[k], c = e / g.dc_max, pos = e - c * g.dc_max;
-                sl[static_cast<size_t>(v) * dv + (k - g.var_off[v])] = pos * g.m + c;
+                const int e = g.var_edge[k], c = e / dc, pos = e - c * dc;
+                sl[static_cast<size_t>(k - g.var_off[v]) * n + v] = pos * m + c;
             }
-        int *p = nullptr;
+        for (int c = 0; c < m; ++c)
+            for (int i = 0; i < dc; ++i) ck[static_cast<size_t>(i) * m + c] = g.chk_var[static_cast<size_t>(c) * dc + i];
+        int *p = nullptr, *q = nullptr;
         std::string e = dev_upload(code_allocs_, sl, &p);
+        if (e.empty()) e = dev_upload(code_allocs_, ck, &q);
         if (!e.empty()) return e;
         mix_slot_[s] = p;
+        mix_chk_[s] = q;
     }
     return "";
 }
@@ -877,9 +882,12 @@ std::string Engine::run_mixed(const MixedRequest &rq, std::vector<jbp_stats> &st
     const int DC = e0.model_.side[0].dc_max;
     for (Engine *e : rq.engines) {
         if (!e || e->device_ != e0.device_) return "the codes of a mixed launch must be on one device";
-        for (int s = 0; s < 2; ++s)
+        for (int s = 0; s < 2; ++s) {
             if (!e->model_.side[s].checks_regular || e->model_.side[s].dc_max != DC)
                 return "the codes of a mixed launch need a code-wide check degree, the same for every code";
+            if (e->model_.side[s].dv_max > kMixMaxDv)
+                return "variable degrees above 4 are not available in the mixed launch";
+        }
     }
     void *kern = DC == 6 ? mixed_kernel<6>(o.precision)
                          : DC == 7 ? mixed_kernel<7>(o.precision) : DC == 8 ? mixed_kernel<8>(o.precision) : nullptr;
@@ -950,6 +958,8 @@ std::string Engine::run_mixed(const MixedRequest &rq, std::vector<jbp_stats> &st
         mc.dc = e.dcode_;
         mc.slot[0] = e.mix_slot_[0];
         mc.slot[1] = e.mix_slot_[1];
+        mc.chk[0] = e.mix_chk_[0];
+        mc.chk[1] = e.mix_chk_[1];
         mc.seed = rq.seeds[i];
         mc.first_trial = rq.first_trial[i];
         mc.ntrials = rq.ntrials[i];

@@ -110,12 +110,13 @@ private:
     void free_buffers();
     int choose_slots(const jbp_options &opt, long long ntrials) const;
 
-    // the variables' c2v slot tables of the mixed launch, built on first use
+    // the neighbour tables of the mixed launch, built on first use
     std::string mixed_slots();
 
     int device_ = 0;
     int sm_count_ = 0;
-    const int *mix_slot_[2] = {nullptr, nullptr};
+    const int *mix_slot_[2] = {nullptr, nullptr};   // [dv][n] message slot of each variable's edges
+    const int *mix_chk_[2] = {nullptr, nullptr};    // [dc][m] variable of each check's edges
     unsigned char *mix_scratch_ = nullptr;   // per-block c2v of the codes that do not fit shared memory
     size_t mix_scratch_bytes_ = 0;
     DevCounters *mix_cnt_ = nullptr;         // kMixMaxCodes counters + the work counter

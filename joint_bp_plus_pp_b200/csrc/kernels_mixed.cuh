@@ -9,11 +9,13 @@
 // mantissa bit, as in kernels_resident.cuh), the error [v] and the target syndrome bits; the
 // check-to-variable messages c2v [side][i][c] (edge i of check c) stay in shared memory when
 // the code's trial fits beside them (the launch's shared size is the largest such trial), and
-// otherwise in a per-block global scratch that stays in L2.  Neighbours come from tables:
-// check c's variables chk_var[c*DC + i] (the code's own table) and each variable's c2v slots
-// slot[v*dv + k] = i*m + c (-1 for the missing edges of lower-degree variables), built on the
-// host.  The check phase reads its c2v row by row (lanes take consecutive checks: coalesced or
-// conflict-free), the variable phase gathers.
+// otherwise in a per-block global scratch that stays in L2.  Neighbours come from tables built
+// on the host: the variable of edge i of check c, chk[i*m + c], and the c2v slot i*m + c of
+// edge k of variable v, slot[k*n + v] (-1 for the missing edges of lower-degree variables).
+// Both are index-major so that a warp's lanes, which take consecutive checks or variables,
+// read them coalesced; the check phase
+// reads its c2v row by row the same way, the variable phase gathers, with all of a variable's
+// slot loads issued before its message loads (variable degree at most kMixMaxDv).
 //
 // Arithmetic per edge and per variable is the resident engine's (the stable tanh rule in
 // (PN, H) form, the exact 4-ary coupling, the flooding schedule with early exit and the
@@ -27,10 +29,12 @@ namespace jbp {
 
 constexpr int kMixThreads = 768;
 constexpr int kMixMaxCodes = 8;
+constexpr int kMixMaxDv = 4;
 
 struct MixCode {
-    DevCode dc;                    // n, per-side m / dc / dv, chk_var, basis rows (classification)
-    const int *slot[2];            // [n][dv] c2v slot of each variable's edges, -1 pads
+    DevCode dc;                    // n, per-side m / dc / dv, basis rows (classification)
+    const int *chk[2];             // [DC][m] variable of edge i of check c
+    const int *slot[2];            // [dv][n] c2v slot (i*m + c) of each variable's edges, -1 pads
     unsigned long long seed;
     long long first_trial, ntrials;
     long long item_end;            // work items of codes 0..this one
@@ -66,11 +70,11 @@ __host__ __device__ inline size_t mix_c2v_bytes(int mx, int mz, int dc, size_t s
 // New c2v of check c of one side (its DC edges at c2v[i*m + c]); with `test`, also whether
 // the decisions in A's low bits fail the check.  The stable tanh rule of res_check_row.
 template <int DC, class ST>
-__device__ __forceinline__ bool mix_check_row(const int *__restrict__ chk_var, typename ST::T *c2v, int m,
+__device__ __forceinline__ bool mix_check_row(const int *__restrict__ chk, typename ST::T *c2v, int m,
                                               const float *A, int c, unsigned sbit, bool test) {
     int vv[DC];
 #pragma unroll
-    for (int i = 0; i < DC; ++i) vv[i] = __ldg(chk_var + static_cast<size_t>(c) * DC + i);
+    for (int i = 0; i < DC; ++i) vv[i] = __ldg(chk + static_cast<size_t>(i) * m + c);
     float u[DC];
     unsigned sgn = 0u, par = 0u;
 #pragma unroll
@@ -111,13 +115,13 @@ __device__ __forceinline__ bool mix_check_row(const int *__restrict__ chk_var, t
 // Syndrome test alone (the decisions in A's low bits against the target): failing checks of
 // this thread on one side.
 template <int DC>
-__device__ __forceinline__ int mix_test_side(const int *__restrict__ chk_var, int m, const float *A,
+__device__ __forceinline__ int mix_test_side(const int *__restrict__ chk, int m, const float *A,
                                              const unsigned *syn) {
     int bad = 0;
     for (int c = threadIdx.x; c < m; c += blockDim.x) {
         unsigned par = 0;
 #pragma unroll
-        for (int i = 0; i < DC; ++i) par ^= __float_as_uint(A[__ldg(chk_var + static_cast<size_t>(c) * DC + i)]);
+        for (int i = 0; i < DC; ++i) par ^= __float_as_uint(A[__ldg(chk + static_cast<size_t>(i) * m + c)]);
         bad += (par & 1u) != ((syn[c >> 5] >> (c & 31)) & 1u);
     }
     return bad;
@@ -129,14 +133,17 @@ template <class ST>
 __device__ __forceinline__ void mix_var(const int *__restrict__ slot_x, int dvx, const int *__restrict__ slot_z,
                                         int dvz, const typename ST::T *c2v_x, const typename ST::T *c2v_z, float *A,
                                         int n, int v, const float4 lp, const float4 pr) {
-    float Lam = 0.0f, Mu = 0.0f;
-    for (int k = 0; k < dvx; ++k) {
-        const int s = __ldg(slot_x + static_cast<size_t>(v) * dvx + k);
-        if (s >= 0) Lam += ST::ld(c2v_x + s);
+    int sx[kMixMaxDv], sz[kMixMaxDv];
+#pragma unroll
+    for (int k = 0; k < kMixMaxDv; ++k) {
+        sx[k] = k < dvx ? __ldg(slot_x + static_cast<size_t>(k) * n + v) : -1;
+        sz[k] = k < dvz ? __ldg(slot_z + static_cast<size_t>(k) * n + v) : -1;
     }
-    for (int k = 0; k < dvz; ++k) {
-        const int s = __ldg(slot_z + static_cast<size_t>(v) * dvz + k);
-        if (s >= 0) Mu += ST::ld(c2v_z + s);
+    float Lam = 0.0f, Mu = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kMixMaxDv; ++k) {
+        if (sx[k] >= 0) Lam += ST::ld(c2v_x + sx[k]);
+        if (sz[k] >= 0) Mu += ST::ld(c2v_z + sz[k]);
     }
     const float w0 = lp.x, w1 = lp.y - Lam, w2 = lp.z - Mu, w3 = lp.w - Lam - Mu;
     unsigned best = 0;
@@ -208,10 +215,10 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant_
         __syncthreads();
         for (int r = threadIdx.x; r < mx + mz; r += blockDim.x) {
             const int side = r >= mx, c = r - side * mx;
-            const int *cv = mc.dc.s[side].chk_var + static_cast<size_t>(c) * DC;
+            const int *ck = mc.chk[side], ms = side ? mz : mx;
             unsigned par = 0;
 #pragma unroll
-            for (int i = 0; i < DC; ++i) par ^= err[__ldg(cv + i)];
+            for (int i = 0; i < DC; ++i) par ^= err[__ldg(ck + static_cast<size_t>(i) * ms + c)];
             if ((par >> side) & 1u) atomicOr(&(side ? synz : syn)[c >> 5], 1u << (c & 31));
         }
         {
@@ -232,14 +239,12 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant_
             int bad = 0;
             if (it < run.max_iter) {
                 for (int c = threadIdx.x; c < mx; c += blockDim.x)
-                    bad += mix_check_row<DC, ST>(mc.dc.s[0].chk_var, c2v, mx, A, c, (syn[c >> 5] >> (c & 31)) & 1u,
-                                                 fused);
+                    bad += mix_check_row<DC, ST>(mc.chk[0], c2v, mx, A, c, (syn[c >> 5] >> (c & 31)) & 1u, fused);
                 for (int c = threadIdx.x; c < mz; c += blockDim.x)
-                    bad += mix_check_row<DC, ST>(mc.dc.s[1].chk_var, c2vz, mz, A + n, c,
-                                                 (synz[c >> 5] >> (c & 31)) & 1u, fused);
+                    bad += mix_check_row<DC, ST>(mc.chk[1], c2vz, mz, A + n, c, (synz[c >> 5] >> (c & 31)) & 1u,
+                                                 fused);
             } else if (fused) {
-                bad = mix_test_side<DC>(mc.dc.s[0].chk_var, mx, A, syn) +
-                      mix_test_side<DC>(mc.dc.s[1].chk_var, mz, A + n, synz);
+                bad = mix_test_side<DC>(mc.chk[0], mx, A, syn) + mix_test_side<DC>(mc.chk[1], mz, A + n, synz);
             }
             const bool any = __syncthreads_or(bad) != 0;
             if (fused && !any) { rf = kResSyndromeOk | kResBpOk; iters = it; break; }
