@@ -43,7 +43,7 @@ def parse_args():
     ap.add_argument("--batch", type=int, default=131072, help="trials per step")
     ap.add_argument("--precision", default="fp16", choices=["fp32", "fp16", "fp64"],
                     help="fp16 = FP32 arithmetic with FP16 message storage (the trial-resident engine)")
-    ap.add_argument("--engine", default="auto", choices=["auto", "resident", "slots"])
+    ap.add_argument("--engine", default="auto", choices=["auto", "resident", "slots", "table"])
     ap.add_argument("--p", type=float, default=0.04)
     ap.add_argument("--max-iter", type=int, default=1000)
     ap.add_argument("--seed", type=int, default=106)
@@ -272,7 +272,8 @@ def main():
     clocks = ClockSampler(local)
     clocks.start()
     for w in range(args.warmup):
-        dec.simulate(args.seed, B, args.p, opts, first_trial=base + w * B, per_trial=False)
+        # the last warm-up step also sizes the per-trial result buffers the first timed step uses
+        dec.simulate(args.seed, B, args.p, opts, first_trial=base + w * B, per_trial=(w == args.warmup - 1))
     torch.cuda.synchronize()
     barrier()
     clocks.mark()
@@ -315,8 +316,11 @@ def main():
         n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
         sfu_peak = 16 * n_sm * sm_mhz / 1e3          # Gop/s: 16 MUFU results / clk / SM
         achieved = agg["bp_trial_iterations"] * mufu_per_ti / (kms / 1000.0) / 1e9 if kms > 0 else None
-        tr = traffic_tab.get("resident_dram_bytes_per_trial")
-        roofline = {"bound": "sfu", "kernel": "k_resident (trial in shared memory, FP16 c2v)", "achieved": achieved,
+        table = args.engine == "table"
+        tr = None if table else traffic_tab.get("resident_dram_bytes_per_trial")
+        kname = ("k_mixed (table-driven neighbours, one code, " + args.precision.upper() + " c2v)" if table
+                 else "k_resident (trial in shared memory, FP16 c2v)")
+        roofline = {"bound": "sfu", "kernel": kname, "achieved": achieved,
                     "peak": sfu_peak, "unit": "Gop/s", "frac": achieved / sfu_peak if achieved else None,
                     "traffic": tr * agg["trials"] / args.steps if tr is not None else None,
                     "peak_kind": f"derived: 16 MUFU results/clk/SM x {n_sm} SMs x median SM clock {sm_mhz:.0f} MHz",
@@ -430,8 +434,11 @@ def main():
                    "max_iter": args.max_iter, "enable_pp": pp, "flip_hist": args.flip_hist,
                    "learned_from": learned_from,
                    "learned": {"attempts": agg["learned_attempts"], "saved": agg["learned_success"]},
-                   "trials_per_step": B, "engine": "resident" if resident else "slots",
-                   "l2": ("trial state in shared memory; no message traffic to HBM" if resident
+                   "trials_per_step": B,
+                   "engine": "table" if args.engine == "table" else ("resident" if resident else "slots"),
+                   "l2": ("messages in a per-block scratch of 32 MB in all (FP32), L2-resident; variable totals "
+                          "in shared memory" if args.engine == "table" and args.precision == "fp32"
+                          else "trial state in shared memory; no message traffic to HBM" if resident
                           else "message state (>= 7 GB) larger than L2"),
                    "parallelism": f"replica trial ranges x{world}"},
         "gpu_launches": agg["kernel_launches"],

@@ -38,10 +38,15 @@ extern "C" {
 /* Decoding engines.  RESIDENT: one persistent thread block per SM keeps a whole trial's BP
  * state in shared memory (FP16 precision on quasi-cyclic affine codes such as the shipped APM
  * code).  SLOTS: trials in HBM-resident slots, one kernel per BP phase (every precision and
- * option).  AUTO picks RESIDENT where it applies, else SLOTS. */
+ * option).  AUTO picks RESIDENT where it applies, else SLOTS.  TABLE (explicit only): the
+ * table-driven persistent kernel of jbp_simulate_mixed on this one code -- plain BP on Philox
+ * noise or given errors (not syndromes), FP32 arithmetic with FP32 or FP16 message storage, any
+ * code whose checks have one degree (6, 7, 8 or 12) and whose variables have degree <= 4 per
+ * side. */
 #define JBP_ENGINE_AUTO 0
 #define JBP_ENGINE_RESIDENT 1
 #define JBP_ENGINE_SLOTS 2
+#define JBP_ENGINE_TABLE 3
 
 #define JBP_SAMPLER_PHILOX 0   /* counter-based Philox4x32-10 keyed by (seed, trial index) */
 #define JBP_SAMPLER_MT19937 1  /* the reference stream: splitmix64 seed -> mt19937_64 per trial */
@@ -210,8 +215,8 @@ int jbp_autotune(jbp_ctx *ctx, const jbp_options *opt, double p, long long probe
  * first_trial[i] + ntrials[i] - 1 of seed seeds[i] (Philox noise, per-trial p uniform in
  * [p, opt->p_max) when p_max > p) -- taken by one persistent kernel from one work queue, largest
  * code first.  Plain BP (opt->enable_pp = 0), FP32 arithmetic with FP32 (JBP_PREC_FP32) or FP16
- * (JBP_PREC_FP16) message storage; the codes' checks must all have one degree (6, 7 or 8), the
- * same for every code.  first_trial may be null (every code from trial 1); stats receives one
+ * (JBP_PREC_FP16) message storage; the codes' checks must all have one degree (6, 7, 8 or 12), the
+ * same for every code; variables of degree <= 4 per side.  first_trial may be null (every code from trial 1); stats receives one
  * entry per code; per_trial, if not null, holds nctx host arrays (each null or ntrials[i]
  * records).  Runs on the first context's stream. */
 int jbp_simulate_mixed(jbp_ctx *const *ctxs, int nctx, const jbp_options *opt, const uint64_t *seeds,

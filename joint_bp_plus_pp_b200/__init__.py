@@ -23,7 +23,7 @@ DEFAULT_PARAMS = DATA_DIR / "H_P768_J3_L12_dmax3_nc0-3_1-2_seed11579811919164041
 
 PREC = {"fp64": 0, "fp32": 1, "fp16": 2}
 SAMPLER = {"philox": 0, "mt19937": 1}
-ENGINE = {"auto": 0, "resident": 1, "slots": 2}
+ENGINE = {"auto": 0, "resident": 1, "slots": 2, "table": 3}
 ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "I/O error", 4: "unsupported", 5: "timeout"}
 
 

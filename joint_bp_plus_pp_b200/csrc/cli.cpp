@@ -64,7 +64,7 @@ void usage(const char *prog) {
               << "  --precision fp64|fp32|fp16 (fp64)  --sampler mt19937|philox (mt19937)\n"
               << "  --slots N (trials in flight, 0 = auto)  --batch N (trials per GPU call, 262144)\n"
               << "  --ets-dir DIR (default: the params path without extension)\n"
-              << "  --engine auto|resident|slots (auto)  --learned-from N (0 = off; learned flip proposal at\n"
+              << "  --engine auto|resident|slots|table (auto)  --learned-from N (0 = off; learned flip proposal at\n"
               << "  stalls from iteration N, FP16 resident engine)  --flip-model FILE.npy (default: the\n"
               << "  shipped data/flip_mlp_params.npy next to the library)\n"
               << "  --checks FILE (a code as check lists instead of --params: 'n mx mz', then one line of\n"
@@ -196,7 +196,8 @@ int parse(int argc, char **argv, Args &a) {
                 if (s == "auto") a.engine = JBP_ENGINE_AUTO;
                 else if (s == "resident") a.engine = JBP_ENGINE_RESIDENT;
                 else if (s == "slots") a.engine = JBP_ENGINE_SLOTS;
-                else { std::cerr << "--engine must be auto, resident or slots\n"; return 1; }
+                else if (s == "table") a.engine = JBP_ENGINE_TABLE;
+                else { std::cerr << "--engine must be auto, resident, slots or table\n"; return 1; }
             } else if (f == "--learned-from") { VAL(); a.learned_from = std::max(0, std::stoi(v)); }
             else if (f == "--flip-model") { VAL(); a.flip_model = v; }
             else if (f == "--checks") { VAL(); a.checks = v; }

@@ -518,7 +518,30 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     }
     if (o.damping < 0.0 || o.damping > 1.0) return "damping must be in [0, 1]";
     if (o.p_max > rq.p && !(o.p_max < 1.0)) return "p_max must be below 1";
-    if (o.engine < JBP_ENGINE_AUTO || o.engine > JBP_ENGINE_SLOTS) return "unknown engine";
+    if (o.engine < JBP_ENGINE_AUTO || o.engine > JBP_ENGINE_TABLE) return "unknown engine";
+    if (o.engine == JBP_ENGINE_TABLE) {
+        if ((rq.source != kSrcPhilox && rq.source != kSrcErrors) || rq.collect)
+            return "the table engine is not available for syndrome inputs or the mt19937 sampler "
+                   "(it decodes Philox Monte Carlo and given errors)";
+        MixedRequest mr;
+        mr.engines = {this};
+        mr.opt = o;
+        mr.seeds = {rq.seed};
+        mr.first_trial = {rq.first_trial};
+        mr.ntrials = {rq.ntrials};
+        mr.p = rq.p;
+        mr.d_res = {rq.d_res_out};
+        mr.d_hist = {rq.d_hist};
+        mr.d_err = {rq.source == kSrcErrors ? rq.d_err : nullptr};
+        mr.d_est = {rq.d_est_out};
+        mr.d_llr = {rq.d_llr_out};
+        mr.stream = rq.stream;
+        std::vector<jbp_stats> st;
+        std::string e = run_mixed(mr, st);
+        if (!e.empty()) return e;
+        stats = st[0];
+        return "";
+    }
     if (o.engine != JBP_ENGINE_SLOTS) {
         std::string why;
         if (resident_applies(o, &why)) return run_resident(rq, stats);
@@ -889,9 +912,12 @@ std::string Engine::run_mixed(const MixedRequest &rq, std::vector<jbp_stats> &st
                 return "variable degrees above 4 are not available in the mixed launch";
         }
     }
-    void *kern = DC == 6 ? mixed_kernel<6>(o.precision)
-                         : DC == 7 ? mixed_kernel<7>(o.precision) : DC == 8 ? mixed_kernel<8>(o.precision) : nullptr;
-    if (!kern) return "check degrees other than 6, 7 and 8 are not available in the mixed launch";
+    void *kern = DC == 6    ? mixed_kernel<6>(o.precision)
+                 : DC == 7  ? mixed_kernel<7>(o.precision)
+                 : DC == 8  ? mixed_kernel<8>(o.precision)
+                 : DC == 12 ? mixed_kernel<12>(o.precision)
+                            : nullptr;
+    if (!kern) return "check degrees other than 6, 7, 8 and 12 are not available in the mixed launch";
     JBP_CUDA_TRY(cudaSetDevice(e0.device_), "cudaSetDevice");
     cudaFuncAttributes fa{};
     JBP_CUDA_TRY(cudaFuncGetAttributes(&fa, kern), "kernel attributes");
@@ -967,6 +993,10 @@ std::string Engine::run_mixed(const MixedRequest &rq, std::vector<jbp_stats> &st
         mc.item_end = end;
         mc.cnt = e0.mix_cnt_ + k;
         mc.res_out = i < static_cast<int>(rq.d_res.size()) ? rq.d_res[i] : nullptr;
+        mc.hist = i < static_cast<int>(rq.d_hist.size()) ? rq.d_hist[i] : nullptr;
+        mc.src_err = i < static_cast<int>(rq.d_err.size()) ? rq.d_err[i] : nullptr;
+        mc.est_out = i < static_cast<int>(rq.d_est.size()) ? rq.d_est[i] : nullptr;
+        mc.llr_out = i < static_cast<int>(rq.d_llr.size()) ? rq.d_llr[i] : nullptr;
         mc.c2v_in_smem = full[i] <= smem ? 1 : 0;
     }
     cudaStream_t st = rq.stream;
@@ -989,6 +1019,8 @@ std::string Engine::run_mixed(const MixedRequest &rq, std::vector<jbp_stats> &st
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
     if (ce != cudaSuccess) return cuda_err(ce, "mixed run");
+    for (int k = 0; k < nc; ++k)
+        if (hc[k].bad_input) return "error vector has invalid value";
     for (int k = 0; k < nc; ++k) {
         const int i = order[k];
         if (hc[k].done != static_cast<unsigned long long>(rq.ntrials[i]))

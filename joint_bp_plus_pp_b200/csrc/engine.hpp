@@ -46,6 +46,10 @@ struct MixedRequest {
     std::vector<long long> first_trial, ntrials;
     double p = 0.05;
     std::vector<jbp_trial_result *> d_res;   // per code, optional device buffers
+    std::vector<unsigned long long *> d_hist;  // per code, optional iteration histograms [max_iter + 1]
+    std::vector<const uint8_t *> d_err;        // per code, optional given errors instead of Philox noise
+    std::vector<uint8_t *> d_est;              // per code, optional estimates
+    std::vector<float *> d_llr;                // per code, optional final LLRs
     cudaStream_t stream = nullptr;
 };
 

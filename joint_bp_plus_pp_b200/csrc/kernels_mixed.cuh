@@ -40,6 +40,10 @@ struct MixCode {
     long long item_end;            // work items of codes 0..this one
     DevCounters *cnt;
     jbp_trial_result *res_out;     // optional, [ntrials]
+    unsigned long long *hist;      // optional iteration histogram [max_iter + 1]
+    const uint8_t *src_err;        // optional [ntrials][n] errors (0..3) instead of Philox noise
+    uint8_t *est_out;              // optional [ntrials][n] final estimates
+    float *llr_out;                // optional [ntrials][n][2] final LLRs (natural log of P(1)/P(0))
     int c2v_in_smem;
 };
 
@@ -157,6 +161,27 @@ __device__ __forceinline__ void mix_var(const int *__restrict__ slot_x, int dvx,
     A[n + v] = with_bit(Mu + Hz, best >> 1);
 }
 
+// Final LLRs of a trial from its c2v (res_write_llr with table neighbours; out of line).
+template <class ST>
+__device__ __noinline__ void mix_write_llr(const int *__restrict__ slot_x, int dvx, const int *__restrict__ slot_z,
+                                           int dvz, const typename ST::T *c2v_x, const typename ST::T *c2v_z, int n,
+                                           const float4 lp, float *out) {
+    for (int v = threadIdx.x; v < n; v += blockDim.x) {
+        float Lam = 0.0f, Mu = 0.0f;
+        for (int k = 0; k < dvx; ++k) {
+            const int s = __ldg(slot_x + static_cast<size_t>(k) * n + v);
+            if (s >= 0) Lam += ST::ld(c2v_x + s);
+        }
+        for (int k = 0; k < dvz; ++k) {
+            const int s = __ldg(slot_z + static_cast<size_t>(k) * n + v);
+            if (s >= 0) Mu += ST::ld(c2v_z + s);
+        }
+        const float w0 = lp.x, w1 = lp.y - Lam, w2 = lp.z - Mu, w3 = lp.w - Lam - Mu;
+        out[2 * v] = (res_lse2(w1, w3) - res_lse2(w0, w2)) * 0.69314718f;
+        out[2 * v + 1] = (res_lse2(w2, w3) - res_lse2(w0, w1)) * 0.69314718f;
+    }
+}
+
 template <int DC, class ST>
 __global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant__ MixRun run) {
     extern __shared__ __align__(16) unsigned char mix_smem[];
@@ -206,11 +231,35 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant_
 
         // ---- error (Philox, the stream of the other engines), target syndrome, BP state
         for (int w = threadIdx.x; w < mwx + mwz; w += blockDim.x) syn[w] = 0u;
-        for (int v2 = threadIdx.x; 2 * v2 < n; v2 += blockDim.x) {
-            uint8_t e0, e1;
-            sample_philox_pair(mc.seed, t, v2, pt, e0, e1);
-            err[2 * v2] = e0;
-            if (2 * v2 + 1 < n) err[2 * v2 + 1] = e1;
+        if (mc.src_err) {
+            // given errors (device memory or mapped pinned host memory); a byte above 3 is
+            // reported and masked
+            const uint8_t *src = mc.src_err + local * n;
+            if ((n & 15) == 0 && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+                const uint4 *s16 = reinterpret_cast<const uint4 *>(src);
+                uint4 *d16 = reinterpret_cast<uint4 *>(err);
+                unsigned badw = 0u;
+                for (int i = threadIdx.x; i < n / 16; i += blockDim.x) {
+                    uint4 w = s16[i];
+                    badw |= (w.x | w.y | w.z | w.w) & 0xFCFCFCFCu;
+                    w.x &= 0x03030303u; w.y &= 0x03030303u; w.z &= 0x03030303u; w.w &= 0x03030303u;
+                    d16[i] = w;
+                }
+                if (badw) atomicAdd(&mc.cnt->bad_input, 1ull);
+            } else {
+                for (int v = threadIdx.x; v < n; v += blockDim.x) {
+                    const uint8_t e = src[v];
+                    if (e > 3) atomicAdd(&mc.cnt->bad_input, 1ull);
+                    err[v] = e & 3;
+                }
+            }
+        } else {
+            for (int v2 = threadIdx.x; 2 * v2 < n; v2 += blockDim.x) {
+                uint8_t e0, e1;
+                sample_philox_pair(mc.seed, t, v2, pt, e0, e1);
+                err[2 * v2] = e0;
+                if (2 * v2 + 1 < n) err[2 * v2 + 1] = e1;
+            }
         }
         __syncthreads();
         for (int r = threadIdx.x; r < mx + mz; r += blockDim.x) {
@@ -255,6 +304,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant_
             ++it;
         }
         const bool ok = (rf & kResSyndromeOk) != 0;
+        if (mc.llr_out) mix_write_llr<ST>(mc.slot[0], dvx, mc.slot[1], dvz, c2v, c2vz, n, lp, mc.llr_out + local * n * 2);
 
         // ---- classification (jointbp_ets.cpp:6199-6211): exact, stabilizer-equivalent residual
         const int words = (n + 63) / 64, w32 = 2 * words;
@@ -268,6 +318,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant_
             const bool in = v < n;
             const unsigned e = in ? ((__float_as_uint(A[v]) & 1u) | ((__float_as_uint(A[n + v]) & 1u) << 1)) : 0u;
             const unsigned tv = in ? err[v] : e;
+            if (in && mc.est_out) mc.est_out[local * n + v] = static_cast<uint8_t>(e);
             exact &= tv == e;
             const unsigned bxm = __ballot_sync(0xffffffffu, ((tv ^ e) & 1u) != 0);
             const unsigned bzm = __ballot_sync(0xffffffffu, ((tv ^ e) & 2u) != 0);
@@ -286,7 +337,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant_
         }
         const bool success = ok && stab;
         if (threadIdx.x == 0)
-            account_trial(mc.cnt, nullptr, mc.res_out, run.max_iter, local, iters, rf, ok, success, exact, stab);
+            account_trial(mc.cnt, mc.hist, mc.res_out, run.max_iter, local, iters, rf, ok, success, exact, stab);
         __syncthreads();
     }
 }

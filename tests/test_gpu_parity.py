@@ -224,3 +224,50 @@ def test_final_llr_deviation_vs_fp64(decoder, prec, engine, tol):
     inside = np.abs(l64) <= 50
     assert np.abs(llo - l64)[inside].max() <= tol
     assert ((llo > 0) != (l64 > 0)).mean() <= 1e-4
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16"])
+def test_table_engine_agrees_with_fp64(decoder, prec):
+    """The table-driven engine (the mixed-size launch's kernel on this one code) on the shipped
+    code: plain BP Philox Monte Carlo in one launch, counters consistent with the records,
+    outcomes and iteration counts against FP64 on the same trials."""
+    from joint_bp_plus_pp_b200 import Options
+    T = 4096
+    base = dict(max_iter=200, enable_pp=False)
+    st, r = decoder.simulate(606, T, 0.05, Options(precision=prec, engine="table", **base), hist=True)
+    assert st["trials"] == T and st["kernel_launches"] == 1
+    assert st["failures"] == int((r["success"] == 0).sum()) and st["total_iters"] == int(r["iterations"].sum())
+    assert int(st["hist"].sum()) == T
+    _, r64 = decoder.simulate(606, T, 0.05, Options(precision="fp64", **base))
+    assert (r["success"] == r64["success"]).mean() >= 0.995
+    assert (r["iterations"] == r64["iterations"]).mean() >= 0.95
+    assert abs(int(r["success"].sum()) - int(r64["success"].sum())) <= 8
+
+
+def test_table_engine_entry_points_agree(decoder, oracle):
+    """Philox Monte Carlo and the same errors given from the host decode identically through
+    the table engine; the returned estimates reproduce the reported flags (oracle)."""
+    from joint_bp_plus_pp_b200 import Options
+    o = Options(precision="fp32", engine="table", max_iter=60, enable_pp=False)
+    err = decoder.sample_errors(4242, 11, 64, 0.055, sampler="philox")
+    _, r1 = decoder.simulate(4242, 64, 0.055, o, first_trial=11)
+    _, r2, est = decoder.decode_errors(err, 0.055, o)
+    assert (r1 == r2).all()
+    assert 0 < int(r2["syndrome_ok"].sum()) < 64
+    for t in range(64):
+        ok, exact, stab, success = oracle.classify(err[t], est[t])
+        assert (r2["syndrome_ok"][t], r2["exact"][t], r2["success"][t]) == (ok, exact, success), t
+
+
+def test_table_engine_refuses_other_sources(decoder, oracle):
+    from joint_bp_plus_pp_b200 import JbpError, Options
+    o = Options(precision="fp32", engine="table", max_iter=20, enable_pp=False)
+    err = decoder.sample_errors(1, 1, 4, 0.05)
+    sx = np.stack([oracle.syndrome(e)[0] for e in err])
+    sz = np.stack([oracle.syndrome(e)[1] for e in err])
+    for call in (lambda: decoder.decode_syndromes(sx, sz, 0.05, o),
+                 lambda: decoder.simulate(1, 4, 0.05, o, sampler="mt19937"),
+                 lambda: decoder.simulate(1, 4, 0.05, Options(precision="fp32", engine="table", enable_pp=True))):
+        with pytest.raises(JbpError) as e:
+            call()
+        assert e.value.code == 4, str(e.value)

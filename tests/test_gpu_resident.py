@@ -155,7 +155,7 @@ def test_resident_pp_saves_trials(decoder):
     assert st["flip_pp_success"] == int((res["pp_flip"] & res["success"]).sum())
 
 
-@pytest.mark.parametrize("engine,prec", [("resident", "fp16"), ("slots", "fp32"), ("slots", "fp64")])
+@pytest.mark.parametrize("engine,prec", [("resident", "fp16"), ("slots", "fp32"), ("slots", "fp64"), ("table", "fp32")])
 def test_invalid_error_values_are_rejected(decoder, engine, prec):
     """Error bytes outside 0..3 are found on the device while the errors are read."""
     from joint_bp_plus_pp_b200 import JbpError, Options
