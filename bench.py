@@ -379,9 +379,12 @@ def main():
                                                                    **base_o))
         inside = np.abs(l64) <= 50
         dev = np.abs(llo - l64)
+        anyin = bool(inside.any())   # at low p every LLR can have grown past the range in 12 iterations
         precision = {"trials": 256, "iterations": it, "llr_entries": int(l64.size),
-                     "max_abs_llr_dev_nat": float(dev[inside].max()),
-                     "max_rel_llr_dev": float((dev[inside] / np.maximum(np.abs(l64[inside]), 1.0)).max()),
+                     "llr_entries_compared": int(inside.sum()),
+                     "max_abs_llr_dev_nat": float(dev[inside].max()) if anyin else None,
+                     "max_rel_llr_dev": float((dev[inside] / np.maximum(np.abs(l64[inside]), 1.0)).max())
+                     if anyin else None,
                      "range": "|LLR_fp64| <= 50 nat (messages saturate at 110 bits = 76 nat)",
                      "sign_disagreements": int(((llo > 0) != (l64 > 0)).sum())}
 
