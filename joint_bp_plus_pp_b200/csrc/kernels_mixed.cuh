@@ -76,44 +76,22 @@ __host__ __device__ inline size_t mix_c2v_bytes(int mx, int mz, int dc, size_t s
 template <int DC, class ST>
 __device__ __forceinline__ bool mix_check_row(const int *__restrict__ chk, typename ST::T *c2v, int m,
                                               const float *A, int c, unsigned sbit, bool test) {
-    int vv[DC];
+    // the row's variable indices, loaded together up front where the registers allow it
+    constexpr bool kPre = DC <= 8;
+    int vv[kPre ? DC : 1];
+    if constexpr (kPre) {
 #pragma unroll
-    for (int i = 0; i < DC; ++i) vv[i] = __ldg(chk + static_cast<size_t>(i) * m + c);
-    float u[DC];
-    unsigned sgn = 0u, par = 0u;
-#pragma unroll
-    for (int i = 0; i < DC; ++i) {
-        const float a = A[vv[i]];
-        par ^= __float_as_uint(a);
-        const float v = a - ST::ld(c2v + static_cast<size_t>(i) * m + c);
-        const unsigned sv = __float_as_uint(v) & 0x80000000u;
-        sgn ^= sv;
-        u[i] = __uint_as_float(__float_as_uint(res_ex2(-fabsf(v))) | sv);
+        for (int i = 0; i < DC; ++i) vv[i] = __ldg(chk + static_cast<size_t>(i) * m + c);
     }
-    const bool bad = test && ((par & 1u) != sbit);
-    float sPN[DC + 1], sH[DC + 1];
-    sPN[DC] = 1.0f;
-    sH[DC] = 0.0f;
-#pragma unroll
-    for (int i = DC - 1; i >= 0; --i) {
-        const float au = fabsf(u[i]);
-        sH[i] = fmaf(au, sH[i + 1] + sPN[i + 1], sH[i + 1]);
-        sPN[i] = fmaf(-au, sPN[i + 1], sPN[i + 1]);
-    }
-    sgn ^= sbit << 31;
-    float pPN = 1.0f, pH = 0.0f;
-#pragma unroll
-    for (int i = 0; i < DC; ++i) {
-        const float ePN = pPN * sPN[i + 1];
-        const float eH = fmaf(fmaf(2.0f, pH, pPN), sH[i + 1], sPN[i + 1] * pH);
-        const float mag = fminf(res_lg2(fmaf(ePN, res_rcp(eH), 1.0f)), kResCmax);
-        ST::st(c2v + static_cast<size_t>(i) * m + c,
-               __uint_as_float(__float_as_uint(mag) ^ ((sgn ^ __float_as_uint(u[i])) & 0x80000000u)));
-        const float au = fabsf(u[i]);
-        pH = fmaf(au, pH + pPN, pH);
-        pPN = fmaf(-au, pPN, pPN);
-    }
-    return bad;
+    unsigned par = 0u;
+    res_row_rule<DC>(
+        [&](int i) {
+            const float a = A[kPre ? vv[i] : __ldg(chk + static_cast<size_t>(i) * m + c)];
+            par ^= __float_as_uint(a);
+            return a - ST::ld(c2v + static_cast<size_t>(i) * m + c);
+        },
+        sbit, [&](int i, float y) { ST::st(c2v + static_cast<size_t>(i) * m + c, y); });
+    return test && ((par & 1u) != sbit);
 }
 
 // Syndrome test alone (the decisions in A's low bits against the target): failing checks of
@@ -190,6 +168,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant_
     __shared__ int code_sh;
     __shared__ float4 lp_sh, pr_sh;
     __shared__ float lpx_sh, lpz_sh;
+    __shared__ float first_sh[2][DC];   // first-iteration c2v of each position (syndrome bit 0)
     __shared__ int ints[16];
     if (threadIdx.x < 16) ints[threadIdx.x] = 0;
     for (;;) {
@@ -271,10 +250,21 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant_
             if ((par >> side) & 1u) atomicOr(&(side ? synz : syn)[c >> 5], 1u << (c & 31));
         }
         {
-            const size_t nmsg = static_cast<size_t>(DC) * (mx + mz);
-            for (size_t i = threadIdx.x; i < nmsg; i += blockDim.x) c2v[i] = T(0.0f);
             const float ax = with_bit(lpx_sh, 0u), az = with_bit(lpz_sh, 0u);
             for (int v = threadIdx.x; v < n; v += blockDim.x) { A[v] = ax; A[n + v] = az; }
+            if (threadIdx.x < 2) res_first_row<DC>(threadIdx.x ? az : ax, first_sh[threadIdx.x]);
+        }
+        __syncthreads();
+        {
+            // the first iteration's c2v in closed form (res_first_row)
+            for (int r = threadIdx.x; r < mx + mz; r += blockDim.x) {
+                const int side = r >= mx, c = r - side * mx, ms = side ? mz : mx;
+                const bool neg = ((side ? synz : syn)[c >> 5] >> (c & 31)) & 1u;
+                T *row = (side ? c2vz : c2v) + c;
+#pragma unroll
+                for (int i = 0; i < DC; ++i)
+                    ST::st(row + static_cast<size_t>(i) * ms, neg ? -first_sh[side][i] : first_sh[side][i]);
+            }
         }
         __syncthreads();
 
@@ -286,7 +276,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant_
             const bool fused = it >= 1 && (it >= run.max_iter ||
                                            (it > run.check_warmup && (it - run.check_warmup) % run.check_interval == 0));
             int bad = 0;
-            if (it < run.max_iter) {
+            if (it < run.max_iter && it > 0) {   // iteration 1's check phase is the closed form above
                 for (int c = threadIdx.x; c < mx; c += blockDim.x)
                     bad += mix_check_row<DC, ST>(mc.chk[0], c2v, mx, A, c, (syn[c >> 5] >> (c & 31)) & 1u, fused);
                 for (int c = threadIdx.x; c < mz; c += blockDim.x)

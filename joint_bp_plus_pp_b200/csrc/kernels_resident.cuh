@@ -164,9 +164,8 @@ __host__ __device__ inline size_t res_smem_bytes(int n, int m, int L, size_t sto
 }
 
 
-// Check phase, one block row JJ of side SIDE, check offset x: new c2v of the row's L edges
-// from A and the old c2v; with `test`, also the parity of the decision bits against the
-// target.  Returns whether the tested check failed.
+// The check rule on one check of L edges: from the edges' variable-to-check inputs in(l) and
+// the check's syndrome bit, out(l, c2v of edge l) for l = 0 .. L-1.
 //
 // Stable tanh rule.  Per edge u = 2^-|y|, N = 1 - u, D = 1 + u, t = N / D.  A set of edges is
 // carried as (PN, H) with PN = prod N and H = (prod D - prod N) / 2, so prod D = PN + 2H and
@@ -178,28 +177,18 @@ __host__ __device__ inline size_t res_smem_bytes(int n, int m, int L, size_t sto
 // min |y| instead of saturating where 1 - T rounds to zero.  H is zero only when every other
 // edge has u = 0 (|y| above 126), and then PN = 1: the output is +inf before the clamp to
 // kResCmax, as it is whenever all other edges are that reliable, so no input clamp is needed.
-template <int P, int J, int L, class ST, int SIDE, int JJ>
-__device__ __forceinline__ bool res_check_row(const ResCode &code, typename ST::T *c2v_all, const float *A_all,
-                                              const unsigned *syn_all, int x, bool test) {
-    constexpr int m = J * P, n = L * P, mw = (m + 31) / 32;
-    typename ST::T *c2v = c2v_all + SIDE * L * m + JJ * P + x;
-    const float *A = A_all + SIDE * n;
-    const int c = JJ * P + x;
-    const unsigned sbit = (syn_all[SIDE * mw + (c >> 5)] >> (c & 31)) & 1u;
+template <int L, class In, class Out>
+__device__ __forceinline__ void res_row_rule(In in, unsigned sbit, Out out) {
     float u[L];
-    unsigned sgn = 0u, par = 0u;
+    unsigned sgn = 0u;
 #pragma unroll
     for (int l = 0; l < L; ++l) {
-        const unsigned y = res_map<P>(code.fF[SIDE][JJ][l], code.fG[SIDE][JJ][l], static_cast<unsigned>(x));
-        const float a = A[l * P + y];
-        par ^= __float_as_uint(a);
-        const float v = a - ST::ld(c2v + l * m);
+        const float v = in(l);
         const unsigned sv = __float_as_uint(v) & 0x80000000u;
         sgn ^= sv;
         // sign of the edge kept in u's sign bit, |u| = 2^-|v| (flushed to zero above |v| = 126)
         u[l] = __uint_as_float(__float_as_uint(res_ex2(-fabsf(v))) | sv);
     }
-    const bool bad = test && ((par & 1u) != sbit);
     // suffix sets {l, .., L-1}
     float sPN[L + 1], sH[L + 1];
     sPN[L] = 1.0f;
@@ -218,12 +207,44 @@ __device__ __forceinline__ bool res_check_row(const ResCode &code, typename ST::
         const float ePN = pPN * sPN[l + 1];
         const float eH = fmaf(fmaf(2.0f, pH, pPN), sH[l + 1], sPN[l + 1] * pH);
         const float mag = fminf(res_lg2(fmaf(ePN, res_rcp(eH), 1.0f)), kResCmax);
-        ST::st(c2v + l * m, __uint_as_float(__float_as_uint(mag) ^ ((sgn ^ __float_as_uint(u[l])) & 0x80000000u)));
+        out(l, __uint_as_float(__float_as_uint(mag) ^ ((sgn ^ __float_as_uint(u[l])) & 0x80000000u)));
         const float au = fabsf(u[l]);
         pH = fmaf(au, pH + pPN, pH);
         pPN = fmaf(-au, pPN, pPN);
     }
-    return bad;
+}
+
+// The first iteration in closed form: every variable starts at the prior and every c2v at 0,
+// so every edge of a side has the same input v0 and a check's outputs depend only on the
+// position l and the check's syndrome bit (bit 1 negates them).  out[l] = the output for
+// syndrome bit 0, by the same rule (and so the same bits) as res_row_rule on such a row; out of
+// line, as it runs once per trial on two threads.
+template <int L>
+__device__ __noinline__ void res_first_row(float v0, float *out) {
+    res_row_rule<L>([&](int) { return v0; }, 0u, [&](int l, float x) { out[l] = x; });
+}
+
+// Check phase, one block row JJ of side SIDE, check offset x: new c2v of the row's L edges
+// from A and the old c2v; with `test`, also the parity of the decision bits against the
+// target.  Returns whether the tested check failed.
+template <int P, int J, int L, class ST, int SIDE, int JJ>
+__device__ __forceinline__ bool res_check_row(const ResCode &code, typename ST::T *c2v_all, const float *A_all,
+                                              const unsigned *syn_all, int x, bool test) {
+    constexpr int m = J * P, n = L * P, mw = (m + 31) / 32;
+    typename ST::T *c2v = c2v_all + SIDE * L * m + JJ * P + x;
+    const float *A = A_all + SIDE * n;
+    const int c = JJ * P + x;
+    const unsigned sbit = (syn_all[SIDE * mw + (c >> 5)] >> (c & 31)) & 1u;
+    unsigned par = 0u;
+    res_row_rule<L>(
+        [&](int l) {
+            const unsigned y = res_map<P>(code.fF[SIDE][JJ][l], code.fG[SIDE][JJ][l], static_cast<unsigned>(x));
+            const float a = A[l * P + y];
+            par ^= __float_as_uint(a);
+            return a - ST::ld(c2v + l * m);
+        },
+        sbit, [&](int l, float y) { ST::st(c2v + l * m, y); });
+    return test && ((par & 1u) != sbit);
 }
 
 // Returns this thread's number of tested checks that failed.
@@ -686,6 +707,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
     __shared__ long long trial_sh;
     __shared__ float4 lp_sh, pr_sh;
     __shared__ float lpx_sh, lpz_sh;
+    __shared__ float first_sh[2][L];   // first-iteration c2v of each position (syndrome bit 0)
     __shared__ unsigned short us_hist[100];
     __shared__ int us_cnt[2][2];   // unsatisfied checks per side of the tested iteration, by its parity
     __shared__ int pp_sh[4];   // mode, act_k, pstate
@@ -785,13 +807,19 @@ __global__ void __launch_bounds__(kResThreads, 1)
                 if ((threadIdx.x & 31) == 0) syn[r0 >> 5] = word;
             }
         }
-        // ---- BP state: c2v = 0, A = prior LLR of each side's bit
+        // ---- BP state: A = prior LLR of each side's bit, and the c2v of the first iteration in
+        // closed form (res_first_row): every edge of a side starts from the same input
         {
-            uint4 *z = reinterpret_cast<uint4 *>(c2v);
-            constexpr int nz = static_cast<int>(c2v_bytes / 16);
-            for (int i = threadIdx.x; i < nz; i += blockDim.x) z[i] = make_uint4(0u, 0u, 0u, 0u);
             const float ax = with_bit(lpx_sh, 0u), az = with_bit(lpz_sh, 0u);
             for (int v = threadIdx.x; v < n; v += blockDim.x) { A[v] = ax; A[n + v] = az; }
+            if (threadIdx.x < 2) res_first_row<L>(threadIdx.x ? az : ax, first_sh[threadIdx.x]);
+        }
+        __syncthreads();
+        for (int r = threadIdx.x; r < 2 * m; r += blockDim.x) {
+            const int side = r >= m, c = r - side * m;
+            const bool neg = (syn[side * mw + (c >> 5)] >> (c & 31)) & 1u;
+#pragma unroll
+            for (int l = 0; l < L; ++l) ST::st(c2v + (side * L + l) * m + c, neg ? -first_sh[side][l] : first_sh[side][l]);
         }
         __syncthreads();
 
@@ -811,7 +839,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
             // iteration counts either way; only the c2v left behind differ).
             const bool sep = fused && it < run.max_iter && near <= kResSepTest;
             int bx = 0, bz = 0;
-            if (it < run.max_iter && !sep) {
+            if (it < run.max_iter && !sep && it > 0) {   // iteration 1's check phase is the closed form above
                 bx = res_check_side<P, J, L, ST, 0>(code, c2v, A, syn, fused);
                 bz = res_check_side<P, J, L, ST, 1>(code, c2v, A, syn, fused);
             } else if (fused) {
