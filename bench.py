@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument("--e2e-batch", type=int, default=65536, help="trials per end-to-end step (0 = skip)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--slots", type=int, default=0)
+    ap.add_argument("--mixed-trials", type=int, default=20000,
+                    help="trials per code of the mixed-size one-launch run reported beside (0 = skip)")
     ap.add_argument("--learned-from", type=int, default=6,
                     help="stalled trials try the shipped learned flip proposal from this iteration (0 = off)")
     return ap.parse_args()
@@ -388,6 +390,27 @@ def main():
                      "range": "|LLR_fp64| <= 50 nat (messages saturate at 110 bits = 76 nat)",
                      "sign_disagreements": int(((llo > 0) != (l64 > 0)).sum())}
 
+    # config 3 beside the headline: the mixed-size workload in one launch (rank 0)
+    mixed = None
+    if args.mixed_trials > 0 and rank == 0:
+        try:
+            from joint_bp_plus_pp_b200.mixed import build as build_mixed, simulate_one_launch
+            mdecs = build_mixed(device=local)
+            mo = Options(precision="fp32", max_iter=200, enable_pp=False, p_max=0.06)
+            simulate_one_launch(mdecs, max(64, args.mixed_trials // 16), mo, seed=1000)   # warm-up
+            mst, mwall, _ = simulate_one_launch(mdecs, args.mixed_trials, mo)
+            mtot = sum(x["trials"] for x in mst)
+            mixed = {"workload": "hypergraph-product codes of seeded random (3,4)-regular classical codes, classical "
+                                 "n 32/48/64/96 (n 1,600-14,400), p uniform in [0.01, 0.06) per trial, max-iter 200, "
+                                 "plain BP, FP32 messages, all codes in one kernel launch",
+                     "trials_per_s": mtot / mwall, "device_trials_per_s": mtot / (mst[0]["device_ms"] / 1000.0),
+                     "launches": mst[0]["kernel_launches"],
+                     "per_code": [{"n": d.n, "trials": x["trials"], "failures": x["failures"],
+                                   "avg_iter": x["total_iters"] / max(1, x["trials"])} for d, x in zip(mdecs, mst)]}
+            del mdecs
+        except Exception as e:   # reported, the headline line still prints
+            mixed = {"error": str(e)}
+
     # end to end through the C ABI with host buffers (reference-sampled errors in pinned memory)
     e2e = None
     if args.e2e_batch > 0:
@@ -403,17 +426,18 @@ def main():
         b = torch.cuda.Event(enable_timing=True)
         a.record()
         nsteps = max(1, min(args.steps, 3))
-        done = 0
+        done = e2e_launches = 0
         for _ in range(nsteps):
             st, res, _ = dec.decode_errors(host, args.p, oe, want_est=False)
             done += st["trials"]
-            agg["kernel_launches"] += st["kernel_launches"]
+            e2e_launches += st["kernel_launches"]
         b.record()
         torch.cuda.synchronize()
         ems, tot_e = reduce_over_ranks(dist, a.elapsed_time(b), {"trials": done}, dev)
         done = tot_e["trials"]
         e2e = {"value": done / (ems / 1000.0), "unit": UNIT, "h2d_bytes_per_step": E * N_QUBITS,
-               "d2h_bytes_per_step": E * 16, "path": "jbp_decode_errors (host errors, pinned) -> results to host"}
+               "d2h_bytes_per_step": E * 16, "path": "jbp_decode_errors (host errors, pinned) -> results to host",
+               "steps": nsteps, "gpu_launches": e2e_launches}
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_seconds > 0:
@@ -450,6 +474,7 @@ def main():
                 "avg_iter": agg["total_iters"] / max(1, agg["trials"])},
         "fp64": fp64,
         "precision": precision,
+        "mixed_sizes_one_launch": mixed,
         "clocks": clk,
         "step_ms": {"host_wall": step_wall, "kernel": step_kernel},
         "e2e": e2e,
