@@ -258,7 +258,8 @@ def main():
     dec = Decoder.from_params(device=local)
     pp = not args.no_pp
     from joint_bp_plus_pp_b200 import load_flip_model
-    model = load_flip_model() if (pp and args.learned_from > 0 and args.precision == "fp16") else None
+    resident_tier = args.precision == "fp16" or (args.precision == "fp32" and args.engine == "resident")
+    model = load_flip_model() if (pp and args.learned_from > 0 and resident_tier) else None
     learned_from = args.learned_from if model is not None else 0
     if model is not None:
         dec.set_flip_model(model)
@@ -321,7 +322,8 @@ def main():
         table = args.engine == "table"
         tr = None if table else traffic_tab.get("resident_dram_bytes_per_trial")
         kname = ("k_mixed (table-driven neighbours, one code, " + args.precision.upper() + " c2v)" if table
-                 else "k_resident (trial in shared memory, FP16 c2v)")
+                 else "k_resident (trial in shared memory, FP16 c2v)" if args.precision == "fp16"
+                 else "k_resident (FP32 c2v in a per-block L2-resident scratch, the rest in shared memory)")
         roofline = {"bound": "sfu", "kernel": kname, "achieved": achieved,
                     "peak": sfu_peak, "unit": "Gop/s", "frac": achieved / sfu_peak if achieved else None,
                     "traffic": tr * agg["trials"] / args.steps if tr is not None else None,

@@ -114,6 +114,7 @@ void fill_stats(const DevCounters &hc, jbp_stats &stats) {
 }  // namespace
 
 Engine::~Engine() {
+    cudaFree(res_c2v_scratch_);
     cudaFree(mix_scratch_);
     cudaFree(mix_cnt_);
     free_buffers();
@@ -274,7 +275,9 @@ bool Engine::resident_applies(const jbp_options &o, std::string *why) const {
         return false;
     };
     if (!res_code_ok_) return no(res_code_why_);
-    if (o.precision != JBP_PREC_FP16) return no("the resident tier stores messages in FP16 (precision FP16)");
+    if (o.precision == JBP_PREC_FP64) return no("the resident tier computes in FP32 (precision FP16 or FP32)");
+    if (o.precision == JBP_PREC_FP32 && o.engine != JBP_ENGINE_RESIDENT)
+        return no("FP32 messages run on the resident tier only when it is asked for (engine RESIDENT)");
     if (o.enable_pp && (o.check_interval != 1 || o.check_warmup != 0))
         return no("post-processing needs a syndrome test every iteration");
     if (o.learned_from > 0 && !o.enable_pp) return no("learned flip proposals need post-processing on");
@@ -290,10 +293,16 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     if (!res_cnt_) JBP_CUDA_TRY(cudaMalloc(&res_cnt_, sizeof(DevCounters)), "cudaMalloc(counters)");
     const ResCode &rc = *rcode_;
     const bool pp = o.enable_pp != 0;
-    auto kern = !pp ? k_resident<768, 3, 12, StoreHalf, false, false>
-                    : (o.learned_from > 0 ? k_resident<768, 3, 12, StoreHalf, true, true>
-                                          : k_resident<768, 3, 12, StoreHalf, true, false>);
-    const size_t smem = res_smem_bytes(rc.n, rc.m, rc.L, sizeof(__half), pp);
+    // FP16 messages in shared memory; FP32 messages in a per-block global scratch (L2)
+    const bool f32 = o.precision == JBP_PREC_FP32;
+    auto kern = f32 ? (!pp ? k_resident<768, 3, 12, StoreFloat, false, false, true>
+                           : (o.learned_from > 0 ? k_resident<768, 3, 12, StoreFloat, true, true, true>
+                                                 : k_resident<768, 3, 12, StoreFloat, true, false, true>))
+                    : (!pp ? k_resident<768, 3, 12, StoreHalf, false, false>
+                           : (o.learned_from > 0 ? k_resident<768, 3, 12, StoreHalf, true, true>
+                                                 : k_resident<768, 3, 12, StoreHalf, true, false>));
+    const size_t store = f32 ? sizeof(float) : sizeof(__half);
+    const size_t smem = res_smem_bytes(rc.n, rc.m, rc.L, store, pp, !f32);
     JBP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
                  "smem attribute");
     int per_sm = 0;
@@ -317,6 +326,17 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
             res_pp_bytes_ = 0;
             JBP_CUDA_TRY(cudaMalloc(&res_pp_scratch_, need), "cudaMalloc(post-processing scratch)");
             res_pp_bytes_ = need;
+        }
+    }
+    size_t c2v_stride = 0;
+    if (f32) {
+        c2v_stride = (2ull * rc.L * rc.m * sizeof(float) + 255) / 256 * 256;
+        if (res_c2v_bytes_ < c2v_stride * grid) {
+            cudaFree(res_c2v_scratch_);
+            res_c2v_scratch_ = nullptr;
+            res_c2v_bytes_ = 0;
+            JBP_CUDA_TRY(cudaMalloc(&res_c2v_scratch_, c2v_stride * grid), "cudaMalloc(message scratch)");
+            res_c2v_bytes_ = c2v_stride * grid;
         }
     }
     ResRun r{};
@@ -345,6 +365,9 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     r.ets = dets_;
     r.pp_scratch = pp ? res_pp_scratch_ : nullptr;
     r.pp_scratch_stride = stride;
+    r.pp_smem_base = pp_align(res_base_bytes(rc.n, rc.m, rc.L, store, !f32));
+    r.c2v_scratch = f32 ? res_c2v_scratch_ : nullptr;
+    r.c2v_stride = c2v_stride;
     r.learned_from = learned ? o.learned_from : 0;
     r.mlp.w = mlp_dev_;
     r.collect = rq.collect ? 1 : 0;

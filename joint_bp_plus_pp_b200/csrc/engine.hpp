@@ -131,6 +131,8 @@ private:
     DevCounters *res_cnt_ = nullptr;
     unsigned char *res_pp_scratch_ = nullptr;
     size_t res_pp_bytes_ = 0;
+    unsigned char *res_c2v_scratch_ = nullptr;   // FP32 messages of the resident tier, per block
+    size_t res_c2v_bytes_ = 0;
     uint32_t *mlp_dev_ = nullptr;
     bool has_mlp_ = false;
     CodeModel model_;

@@ -85,6 +85,10 @@ struct ResRun {
     unsigned char *pp_scratch;     // per block: PpScratch | decision ring [R][n] | |LLR| [2][n] doubles |
                                    // features [n][8]
     size_t pp_scratch_stride;
+    size_t pp_smem_base;           // offset of the post-processing arrays in shared memory
+    // FP32 messages (the instantiation with GC): c2v of each block in global memory, L2-resident
+    unsigned char *c2v_scratch;
+    size_t c2v_stride;
     // learned flip proposal (mlp.cuh): tried at stalls from iteration learned_from (0 = off)
     int learned_from;
     MlpDev mlp;
@@ -153,13 +157,18 @@ __device__ __forceinline__ float with_bit(float a, unsigned b) {
     return __uint_as_float((__float_as_uint(a) & ~1u) | b);
 }
 
-// Shared-memory bytes of the resident kernel for a code.
-__host__ __device__ inline size_t res_smem_bytes(int n, int m, int L, size_t store_bytes, bool pp) {
-    const size_t c2v = (2ull * L * m * store_bytes + 15) / 16 * 16;
+// Shared-memory bytes of the resident kernel for a code: the trial state (c2v when it is kept
+// in shared memory, A, err, syn, 16 ints), then the post-processing arrays at pp_align(base).
+__host__ __device__ inline size_t res_base_bytes(int n, int m, int L, size_t store_bytes, bool c2v_in_smem) {
+    const size_t c2v = c2v_in_smem ? (2ull * L * m * store_bytes + 15) / 16 * 16 : 0;
     const size_t A = 2ull * n * 4;
     const size_t err = (static_cast<size_t>(n) + 15) / 16 * 16;
     const size_t syn = (2ull * ((m + 31) / 32) + 3) / 4 * 4 * 4;
-    const size_t base = c2v + A + err + syn + 64;
+    return c2v + A + err + syn + 64;
+}
+__host__ __device__ inline size_t res_smem_bytes(int n, int m, int L, size_t store_bytes, bool pp,
+                                                 bool c2v_in_smem = true) {
+    const size_t base = res_base_bytes(n, m, L, store_bytes, c2v_in_smem);
     return pp ? pp_align(base) + pp_smem_bytes(n, 2 * m, m) + 256 : base;
 }
 
@@ -446,12 +455,10 @@ struct ResPpPtrs {
 
 template <int P, int J, int L, class ST>
 __device__ __forceinline__ ResPpPtrs res_pp_ptrs(const ResRun &run, unsigned char *smem) {
-    constexpr int m = J * P, n = L * P, mw = (m + 31) / 32;
-    constexpr size_t c2v_bytes = (2ull * L * m * sizeof(typename ST::T) + 15) / 16 * 16;
+    constexpr int m = J * P, n = L * P;
     ResPpPtrs q;
     q.R = max(run.flip_hist + 1, run.learned_from > 0 ? 6 : 3);
-    const size_t base = pp_align(c2v_bytes + 2ull * n * 4 + (n + 15) / 16 * 16 + (2 * mw + 3) / 4 * 4 * 4 + 64);
-    q.psh = pp_shared_carve(smem + base, n, 2 * m, m);
+    q.psh = pp_shared_carve(smem + run.pp_smem_base, n, 2 * m, m);
     unsigned char *g = run.pp_scratch + run.pp_scratch_stride * blockIdx.x;
     q.psc = pp_scratch_carve(g, n, m);
     q.ring = g + pp_align(pp_scratch_bytes(n, m));
@@ -692,14 +699,17 @@ __device__ __noinline__ void res_set_prior(int use_prior, const double *prior4, 
     *lpz = static_cast<float>(log2((q[0] + q[1]) / (q[2] + q[3])));
 }
 
-template <int P, int J, int L, class ST, bool PP, bool LEARNED>
+// GC: the c2v live in a per-block global scratch (L2-resident) instead of shared memory -- the
+// FP32-message instantiation, whose 221 KB of c2v per trial do not fit beside the rest.
+template <int P, int J, int L, class ST, bool PP, bool LEARNED, bool GC = false>
 __global__ void __launch_bounds__(kResThreads, 1)
     k_resident(const __grid_constant__ ResCode code, const __grid_constant__ ResRun run) {
     extern __shared__ __align__(16) unsigned char res_smem[];
     using T = typename ST::T;
     constexpr int m = J * P, n = L * P, mw = (m + 31) / 32;
-    T *const c2v = reinterpret_cast<T *>(res_smem);
-    constexpr size_t c2v_bytes = (2ull * L * m * sizeof(T) + 15) / 16 * 16;
+    T *const c2v = GC ? reinterpret_cast<T *>(run.c2v_scratch + run.c2v_stride * blockIdx.x)
+                      : reinterpret_cast<T *>(res_smem);
+    constexpr size_t c2v_bytes = GC ? 0 : (2ull * L * m * sizeof(T) + 15) / 16 * 16;
     float *const A = reinterpret_cast<float *>(res_smem + c2v_bytes);
     uint8_t *const err = res_smem + c2v_bytes + 2ull * n * 4;
     unsigned *const syn = reinterpret_cast<unsigned *>(err + (n + 15) / 16 * 16);

@@ -103,7 +103,7 @@ def test_resident_explicit_prior_equals_p(decoder):
 
 def test_resident_refuses_what_it_does_not_run(decoder):
     from joint_bp_plus_pp_b200 import JbpError
-    for bad in (dict(damping=0.2), dict(freeze_syn=True), dict(precision="fp32")):
+    for bad in (dict(damping=0.2), dict(freeze_syn=True), dict(precision="fp64")):
         with pytest.raises(JbpError) as e:
             decoder.simulate(1, 4, 0.05, ropts(max_iter=10, **bad))
         assert e.value.code == 4
@@ -209,3 +209,24 @@ def test_autotune_picks_a_configuration_that_decodes_identically(decoder):
         s1, r1 = decoder.simulate(9, 512, 0.04, o)
         s2, r2 = decoder.simulate(9, 512, 0.04, best)
         assert (r1["iterations"] == r2["iterations"]).all() and (r1["success"] == r2["success"]).all()
+
+
+@pytest.mark.parametrize("pp", [False, True])
+def test_resident_fp32_messages(decoder, oracle, pp):
+    """FP32 messages on the resident tier (asked for explicitly; the messages live in a per-block
+    L2-resident scratch): one launch, flags recomputed by the oracle from the returned
+    estimates, outcomes against FP64 on the same trials, and AUTO keeps FP32 on the slot engine."""
+    from joint_bp_plus_pp_b200 import Options, sample_reference_errors
+    p, k = 0.055, 400
+    err = sample_reference_errors(decoder.n, 31, 1, k, p)
+    o = Options(precision="fp32", engine="resident", max_iter=200, enable_pp=pp)
+    st, res, est = decoder.decode_errors(err, p, o)
+    assert st["trials"] == k and st["kernel_launches"] == 1
+    for t in range(0, k, 5):
+        ok, exact, stab, success = oracle.classify(err[t], est[t])
+        assert (res["syndrome_ok"][t], res["exact"][t], res["success"][t]) == (ok, exact, success), t
+    _, r64, _ = decoder.decode_errors(err, p, Options(precision="fp64", max_iter=200, enable_pp=pp), want_est=False)
+    assert (res["success"] == r64["success"]).mean() >= 0.98
+    assert abs(int(res["success"].sum()) - int(r64["success"].sum())) <= 4
+    s_auto, _, _ = decoder.decode_errors(err[:8], p, Options(precision="fp32", max_iter=200, enable_pp=pp))
+    assert s_auto["kernel_launches"] > 1          # the slot engine: several launches per run
