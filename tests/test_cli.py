@@ -45,6 +45,16 @@ def test_help_and_usage_errors():
     assert r.returncode == 1 and "only valid with --simulate" in r.stderr
 
 
+def test_engine_and_autotune_flags_parse():
+    """--engine takes auto / resident / slots / table, --autotune is a flag; a bad engine name is
+    a usage error before any GPU work."""
+    r = subprocess.run([str(CLI), "--params", str(PARAMS), "--simulate", "--engine", "bogus"], capture_output=True,
+                       text=True)
+    assert r.returncode == 1 and "--engine must be auto, resident, slots or table" in r.stderr
+    r = subprocess.run([str(CLI), "--help"], capture_output=True, text=True)
+    assert "--engine auto|resident|slots|table" in r.stdout and "--autotune" in r.stdout
+
+
 def test_without_gpu_fails_loudly():
     import torch
     if torch.cuda.is_available():
