@@ -41,9 +41,11 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--batch", type=int, default=131072, help="trials per step")
-    ap.add_argument("--precision", default="fp16", choices=["fp32", "fp16", "fp64"],
-                    help="fp16 = FP32 arithmetic with FP16 message storage (the trial-resident engine)")
-    ap.add_argument("--engine", default="auto", choices=["auto", "resident", "slots", "table"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16", "fp64"],
+                    help="message storage: fp32 (FP32 arithmetic and messages), fp16 (FP32 arithmetic with FP16 "
+                         "message storage), fp64")
+    ap.add_argument("--engine", default=None, choices=["auto", "resident", "slots", "table"],
+                    help="default: the trial-resident engine for fp32 / fp16, the slot engine for fp64")
     ap.add_argument("--p", type=float, default=0.04)
     ap.add_argument("--max-iter", type=int, default=1000)
     ap.add_argument("--seed", type=int, default=106)
@@ -58,7 +60,10 @@ def parse_args():
                     help="trials per code of the mixed-size one-launch run reported beside (0 = skip)")
     ap.add_argument("--learned-from", type=int, default=6,
                     help="stalled trials try the shipped learned flip proposal from this iteration (0 = off)")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.engine is None:
+        a.engine = "slots" if a.precision == "fp64" else "resident"
+    return a
 
 
 # ----------------------------------------------------------------------------- helpers
@@ -320,10 +325,11 @@ def main():
         sfu_peak = 16 * n_sm * sm_mhz / 1e3          # Gop/s: 16 MUFU results / clk / SM
         achieved = agg["bp_trial_iterations"] * mufu_per_ti / (kms / 1000.0) / 1e9 if kms > 0 else None
         table = args.engine == "table"
-        tr = None if table else traffic_tab.get("resident_dram_bytes_per_trial")
+        tr = None if table else traffic_tab.get("resident_dram_bytes_per_trial" if args.precision == "fp16"
+                                                else "resident_fp32_dram_bytes_per_trial")
         kname = ("k_mixed (table-driven neighbours, one code, " + args.precision.upper() + " c2v)" if table
                  else "k_resident (trial in shared memory, FP16 c2v)" if args.precision == "fp16"
-                 else "k_resident (FP32 c2v in a per-block L2-resident scratch, the rest in shared memory)")
+                 else "k_resident (FP32 c2v: X side in shared memory, Z side in a per-block L2-resident scratch)")
         roofline = {"bound": "sfu", "kernel": kname, "achieved": achieved,
                     "peak": sfu_peak, "unit": "Gop/s", "frac": achieved / sfu_peak if achieved else None,
                     "traffic": tr * agg["trials"] / args.steps if tr is not None else None,
@@ -467,6 +473,8 @@ def main():
                    "engine": "table" if args.engine == "table" else ("resident" if resident else "slots"),
                    "l2": ("messages in a per-block scratch of 32 MB in all (FP32), L2-resident; variable totals "
                           "in shared memory" if args.engine == "table" and args.precision == "fp32"
+                          else "X-side FP32 messages and the rest of the trial in shared memory, Z-side FP32 messages "
+                               "in a per-block scratch of 16 MB in all, L2-resident" if resident and args.precision == "fp32"
                           else "trial state in shared memory; no message traffic to HBM" if resident
                           else "message state (>= 7 GB) larger than L2"),
                    "parallelism": f"replica trial ranges x{world}"},

@@ -302,7 +302,8 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
                            : (o.learned_from > 0 ? k_resident<768, 3, 12, StoreHalf, true, true>
                                                  : k_resident<768, 3, 12, StoreHalf, true, false>));
     const size_t store = f32 ? sizeof(float) : sizeof(__half);
-    const size_t smem = res_smem_bytes(rc.n, rc.m, rc.L, store, pp, !f32);
+    const int c2v_sides = f32 ? 1 : 2;   // sides whose c2v live in shared memory
+    const size_t smem = res_smem_bytes(rc.n, rc.m, rc.L, store, pp, c2v_sides);
     JBP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
                  "smem attribute");
     int per_sm = 0;
@@ -330,7 +331,7 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     }
     size_t c2v_stride = 0;
     if (f32) {
-        c2v_stride = (2ull * rc.L * rc.m * sizeof(float) + 255) / 256 * 256;
+        c2v_stride = (1ull * rc.L * rc.m * sizeof(float) + 255) / 256 * 256;   // the Z side
         if (res_c2v_bytes_ < c2v_stride * grid) {
             cudaFree(res_c2v_scratch_);
             res_c2v_scratch_ = nullptr;
@@ -365,7 +366,7 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     r.ets = dets_;
     r.pp_scratch = pp ? res_pp_scratch_ : nullptr;
     r.pp_scratch_stride = stride;
-    r.pp_smem_base = pp_align(res_base_bytes(rc.n, rc.m, rc.L, store, !f32));
+    r.pp_smem_base = pp_align(res_base_bytes(rc.n, rc.m, rc.L, store, c2v_sides));
     r.c2v_scratch = f32 ? res_c2v_scratch_ : nullptr;
     r.c2v_stride = c2v_stride;
     r.learned_from = learned ? o.learned_from : 0;

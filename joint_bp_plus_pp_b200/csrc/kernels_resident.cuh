@@ -86,7 +86,8 @@ struct ResRun {
                                    // features [n][8]
     size_t pp_scratch_stride;
     size_t pp_smem_base;           // offset of the post-processing arrays in shared memory
-    // FP32 messages (the instantiation with GC): c2v of each block in global memory, L2-resident
+    // FP32 messages (the instantiation with GC): the Z side's c2v of each block in global memory,
+    // L2-resident (the X side's stay in shared memory)
     unsigned char *c2v_scratch;
     size_t c2v_stride;
     // learned flip proposal (mlp.cuh): tried at stalls from iteration learned_from (0 = off)
@@ -157,18 +158,18 @@ __device__ __forceinline__ float with_bit(float a, unsigned b) {
     return __uint_as_float((__float_as_uint(a) & ~1u) | b);
 }
 
-// Shared-memory bytes of the resident kernel for a code: the trial state (c2v when it is kept
-// in shared memory, A, err, syn, 16 ints), then the post-processing arrays at pp_align(base).
-__host__ __device__ inline size_t res_base_bytes(int n, int m, int L, size_t store_bytes, bool c2v_in_smem) {
-    const size_t c2v = c2v_in_smem ? (2ull * L * m * store_bytes + 15) / 16 * 16 : 0;
+// Shared-memory bytes of the resident kernel for a code: the trial state (the c2v of the sides
+// kept in shared memory, A, err, syn, 16 ints), then the post-processing arrays at pp_align(base).
+__host__ __device__ inline size_t res_base_bytes(int n, int m, int L, size_t store_bytes, int c2v_sides_in_smem) {
+    const size_t c2v = (static_cast<size_t>(c2v_sides_in_smem) * L * m * store_bytes + 15) / 16 * 16;
     const size_t A = 2ull * n * 4;
     const size_t err = (static_cast<size_t>(n) + 15) / 16 * 16;
     const size_t syn = (2ull * ((m + 31) / 32) + 3) / 4 * 4 * 4;
     return c2v + A + err + syn + 64;
 }
 __host__ __device__ inline size_t res_smem_bytes(int n, int m, int L, size_t store_bytes, bool pp,
-                                                 bool c2v_in_smem = true) {
-    const size_t base = res_base_bytes(n, m, L, store_bytes, c2v_in_smem);
+                                                 int c2v_sides_in_smem = 2) {
+    const size_t base = res_base_bytes(n, m, L, store_bytes, c2v_sides_in_smem);
     return pp ? pp_align(base) + pp_smem_bytes(n, 2 * m, m) + 256 : base;
 }
 
@@ -237,10 +238,10 @@ __device__ __noinline__ void res_first_row(float v0, float *out) {
 // from A and the old c2v; with `test`, also the parity of the decision bits against the
 // target.  Returns whether the tested check failed.
 template <int P, int J, int L, class ST, int SIDE, int JJ>
-__device__ __forceinline__ bool res_check_row(const ResCode &code, typename ST::T *c2v_all, const float *A_all,
+__device__ __forceinline__ bool res_check_row(const ResCode &code, typename ST::T *c2v_side, const float *A_all,
                                               const unsigned *syn_all, int x, bool test) {
     constexpr int m = J * P, n = L * P, mw = (m + 31) / 32;
-    typename ST::T *c2v = c2v_all + SIDE * L * m + JJ * P + x;
+    typename ST::T *c2v = c2v_side + JJ * P + x;
     const float *A = A_all + SIDE * n;
     const int c = JJ * P + x;
     const unsigned sbit = (syn_all[SIDE * mw + (c >> 5)] >> (c & 31)) & 1u;
@@ -256,7 +257,7 @@ __device__ __forceinline__ bool res_check_row(const ResCode &code, typename ST::
     return test && ((par & 1u) != sbit);
 }
 
-// Returns this thread's number of tested checks that failed.
+// Returns this thread's number of tested checks that failed (c2v: the side's [l][c] messages).
 template <int P, int J, int L, class ST, int SIDE>
 __device__ __forceinline__ int res_check_side(const ResCode &code, typename ST::T *c2v, const float *A,
                                               const unsigned *syn, bool test) {
@@ -321,7 +322,8 @@ __device__ __forceinline__ float res_couple(float s, float c0, float c1, float c
 // previous iteration / the one before (the stall and oscillation tests of the learned
 // proposal).  The perturbation is below 2^-17 of |A|, far under the FP16 message precision.
 template <int P, int J, int L, class ST, int LL, bool HIST>
-__device__ __forceinline__ void res_var_col(const ResCode &code, const typename ST::T *c2v, float *A, int y,
+__device__ __forceinline__ void res_var_col(const ResCode &code, const typename ST::T *c2v,
+                                            const typename ST::T *c2vz, float *A, int y,
                                             const float4 *lps, const float4 *prs, unsigned &ch1, unsigned &ch2) {
     const float4 lp = *lps, pr = *prs;   // block constants, re-read from shared memory
     constexpr int m = J * P, n = L * P;
@@ -331,7 +333,7 @@ __device__ __forceinline__ void res_var_col(const ResCode &code, const typename 
         const unsigned xx = res_map<P>(code.iF[0][j][LL], code.iG[0][j][LL], static_cast<unsigned>(y));
         const unsigned xz = res_map<P>(code.iF[1][j][LL], code.iG[1][j][LL], static_cast<unsigned>(y));
         Lam += ST::ld(c2v + LL * m + j * P + xx);
-        Mu += ST::ld(c2v + (L + LL) * m + j * P + xz);
+        Mu += ST::ld(c2vz + LL * m + j * P + xz);
     }
     const float w0 = lp.x, w1 = lp.y - Lam, w2 = lp.z - Mu, w3 = lp.w - Lam - Mu;
     unsigned best = 0;
@@ -356,10 +358,11 @@ __device__ __forceinline__ void res_var_col(const ResCode &code, const typename 
 }
 
 template <int P, int J, int L, class ST, int LL, bool HIST>
-__device__ __forceinline__ void res_var_cols(const ResCode &code, const typename ST::T *c2v, float *A, int y,
+__device__ __forceinline__ void res_var_cols(const ResCode &code, const typename ST::T *c2v,
+                                             const typename ST::T *c2vz, float *A, int y,
                                              const float4 *lps, const float4 *prs, unsigned &ch1, unsigned &ch2) {
-    res_var_col<P, J, L, ST, LL, HIST>(code, c2v, A, y, lps, prs, ch1, ch2);
-    if constexpr (LL + 1 < L) res_var_cols<P, J, L, ST, LL + 1, HIST>(code, c2v, A, y, lps, prs, ch1, ch2);
+    res_var_col<P, J, L, ST, LL, HIST>(code, c2v, c2vz, A, y, lps, prs, ch1, ch2);
+    if constexpr (LL + 1 < L) res_var_cols<P, J, L, ST, LL + 1, HIST>(code, c2v, c2vz, A, y, lps, prs, ch1, ch2);
 }
 
 // Block-wide membership test of vec (shared memory, `words` 64-bit words) in a row space
@@ -380,7 +383,8 @@ __device__ __forceinline__ bool res_in_row_space(uint64_t *vec, int words, const
 // |LLR| of the x and z bits of every variable from the current c2v (the slot engine's FP32
 // keys, base 2), as doubles for the OSD column order.
 template <int P, int J, int L, class ST>
-__device__ void res_abs_llr(const ResCode &code, const typename ST::T *c2v, const float4 lp, double *llr) {
+__device__ void res_abs_llr(const ResCode &code, const typename ST::T *c2v, const typename ST::T *c2vz, const float4 lp,
+                            double *llr) {
     constexpr int m = J * P, n = L * P;
     for (int v = threadIdx.x; v < n; v += blockDim.x) {
         const int l = v / P, y = v - l * P;
@@ -389,7 +393,7 @@ __device__ void res_abs_llr(const ResCode &code, const typename ST::T *c2v, cons
             const unsigned xx = res_map<P>(code.iF[0][j][l], code.iG[0][j][l], static_cast<unsigned>(y));
             const unsigned xz = res_map<P>(code.iF[1][j][l], code.iG[1][j][l], static_cast<unsigned>(y));
             Lam += ST::ld(c2v + l * m + j * P + xx);
-            Mu += ST::ld(c2v + (L + l) * m + j * P + xz);
+            Mu += ST::ld(c2vz + l * m + j * P + xz);
         }
         const float w0 = lp.x, w1 = lp.y - Lam, w2 = lp.z - Mu, w3 = lp.w - Lam - Mu;
         llr[v] = fabsf(res_lse2(w1, w3) - res_lse2(w0, w2));
@@ -402,7 +406,8 @@ __device__ void res_abs_llr(const ResCode &code, const typename ST::T *c2v, cons
 // x-bit and z-bit flips over the last 5 iterations (decision history in A's low bits, / 5),
 // and the unsatisfied X and Z checks at the qubit (/ 3, from psh.est against psh.tgt).
 template <int P, int J, int L, class ST>
-__device__ void res_features(const ResCode &code, const DevCode &dc, const typename ST::T *c2v, const float *A,
+__device__ void res_features(const ResCode &code, const DevCode &dc, const typename ST::T *c2v,
+                             const typename ST::T *c2vz, const float *A,
                              const float4 lp, int it, const PpShared &psh, float *feat) {
     constexpr int m = J * P, n = L * P;
     for (int v = threadIdx.x; v < n; v += blockDim.x) {
@@ -412,7 +417,7 @@ __device__ void res_features(const ResCode &code, const DevCode &dc, const typen
             const unsigned xx = res_map<P>(code.iF[0][j][l], code.iG[0][j][l], static_cast<unsigned>(y));
             const unsigned xz = res_map<P>(code.iF[1][j][l], code.iG[1][j][l], static_cast<unsigned>(y));
             Lam += ST::ld(c2v + l * m + j * P + xx);
-            Mu += ST::ld(c2v + (L + l) * m + j * P + xz);
+            Mu += ST::ld(c2vz + l * m + j * P + xz);
         }
         const float w0 = lp.x, w1 = lp.y - Lam, w2 = lp.z - Mu, w3 = lp.w - Lam - Mu;
         const float mx = fmaxf(fmaxf(w0, w1), fmaxf(w2, w3));
@@ -473,7 +478,8 @@ __device__ __forceinline__ ResPpPtrs res_pp_ptrs(const ResRun &run, unsigned cha
 // with the corrected decisions in A's low bits, only if both syndromes then match exactly.
 template <int P, int J, int L, class ST>
 __device__ __noinline__ bool res_learned_attempt(const ResCode &code, const ResRun &run, unsigned char *smem,
-                                                 typename ST::T *c2v, float *A, const unsigned *syn, const uint8_t *err,
+                                                 typename ST::T *c2v, typename ST::T *c2vz, float *A, const unsigned *syn,
+                                                 const uint8_t *err,
                                                  bool have_err, int it, long long t, const float4 lp) {
     constexpr int m = J * P, n = L * P, mw = (m + 31) / 32;
     const ResPpPtrs q = res_pp_ptrs<P, J, L, ST>(run, smem);
@@ -488,7 +494,7 @@ __device__ __noinline__ bool res_learned_attempt(const ResCode &code, const ResR
         psh.tgt[r] = static_cast<uint8_t>((syn[side * mw + (c >> 5)] >> (c & 31)) & 1u);
     }
     __syncthreads();
-    res_features<P, J, L, ST>(code, run.dc, c2v, A, lp, it, psh, feat);
+    res_features<P, J, L, ST>(code, run.dc, c2v, c2vz, A, lp, it, psh, feat);
     if (run.collect) {
         for (int v = threadIdx.x; v < n; v += blockDim.x) {
             const float *f = feat + static_cast<size_t>(v) * kMlpIn;
@@ -556,7 +562,8 @@ __device__ __noinline__ bool res_learned_attempt(const ResCode &code, const ResR
 // 0 when BP continues.
 template <int P, int J, int L, class ST>
 __device__ __forceinline__ int res_pp_attempt(const ResCode &code, const ResRun &run, const ResPpPtrs &q,
-                                              const typename ST::T *c2v, float *A, const unsigned *syn,
+                                              const typename ST::T *c2v, const typename ST::T *c2vz, float *A,
+                                              const unsigned *syn,
                                               const uint8_t *cur, int it, int mode, int act_k, const float4 lp) {
     constexpr int m = J * P, n = L * P, mw = (m + 31) / 32;
     const PpShared &psh = q.psh;
@@ -569,7 +576,7 @@ __device__ __forceinline__ int res_pp_attempt(const ResCode &code, const ResRun 
         const int side = r >= m, c = r - side * m;
         psh.tgt[r] = static_cast<uint8_t>((syn[side * mw + (c >> 5)] >> (c & 31)) & 1u);
     }
-    res_abs_llr<P, J, L, ST>(code, c2v, lp, llr);
+    res_abs_llr<P, J, L, ST>(code, c2v, c2vz, lp, llr);
     __syncthreads();
     const RingHistory hist{ring, R};
     const PpOutcome o = blk_pp_stages(run.dc, run.ets, hist, run.flip_hist, act_k, it, llr, llr + n, psh, psc);
@@ -594,7 +601,8 @@ __device__ __forceinline__ int res_pp_attempt(const ResCode &code, const ResRun 
 // a finished trial without any flag: not converged, no stage succeeded).
 template <int P, int J, int L, class ST>
 __device__ __noinline__ int res_slow_step(const ResCode &code, const ResRun &run, unsigned char *smem,
-                                          typename ST::T *c2v, float *A, const unsigned *syn, const uint8_t *err,
+                                          typename ST::T *c2v, typename ST::T *c2vz, float *A, const unsigned *syn,
+                                          const uint8_t *err,
                                           bool have_err, int it, long long t, const float4 lp,
                                           unsigned short *us_hist, int *pp_sh, int *ints, bool slow) {
     constexpr int n = L * P;
@@ -610,7 +618,7 @@ __device__ __noinline__ int res_slow_step(const ResCode &code, const ResRun &run
         if (max(us.x, us.y) > kLearnedMaxUnsat) return 0;
         __syncthreads();
         if (threadIdx.x == 0) pp_sh[3] += 1;
-        return res_learned_attempt<P, J, L, ST>(code, run, smem, c2v, A, syn, err, have_err, it, t, lp)
+        return res_learned_attempt<P, J, L, ST>(code, run, smem, c2v, c2vz, A, syn, err, have_err, it, t, lp)
                    ? (kResSyndromeOk | kResLearned) : 0;
     }
     uint8_t *cur = q.ring + static_cast<size_t>(it % R) * n;
@@ -647,12 +655,12 @@ __device__ __noinline__ int res_slow_step(const ResCode &code, const ResRun &run
         max(us.x, us.y) <= kLearnedMaxUnsat) {
         __syncthreads();
         if (threadIdx.x == 0) pp_sh[3] += 1;
-        if (res_learned_attempt<P, J, L, ST>(code, run, smem, c2v, A, syn, err, have_err, it, t, lp))
+        if (res_learned_attempt<P, J, L, ST>(code, run, smem, c2v, c2vz, A, syn, err, have_err, it, t, lp))
             return kResSyndromeOk | kResLearned;
     }
     const int mode = pp_sh[0];
     if (mode) {
-        const int r2 = res_pp_attempt<P, J, L, ST>(code, run, q, c2v, A, syn, cur, it, mode, pp_sh[1], lp);
+        const int r2 = res_pp_attempt<P, J, L, ST>(code, run, q, c2v, c2vz, A, syn, cur, it, mode, pp_sh[1], lp);
         if (r2) return r2;
     }
     return it >= run.max_iter ? -1 : 0;
@@ -662,7 +670,8 @@ __device__ __noinline__ int res_slow_step(const ResCode &code, const ResRun &run
 // P(bit = 1) / P(bit = 0) of the x and z bits from the c2v in shared memory when the trial
 // ends (those of its last variable update when the syndrome is tested only at max_iter).
 template <int P, int J, int L, class ST>
-__device__ __noinline__ void res_write_llr(const ResCode &code, const typename ST::T *c2v, const float4 lp,
+__device__ __noinline__ void res_write_llr(const ResCode &code, const typename ST::T *c2v, const typename ST::T *c2vz,
+                                           const float4 lp,
                                            float *out) {
     constexpr int m = J * P, n = L * P;
     for (int v = threadIdx.x; v < n; v += blockDim.x) {
@@ -670,7 +679,7 @@ __device__ __noinline__ void res_write_llr(const ResCode &code, const typename S
         float Lam = 0.0f, Mu = 0.0f;
         for (int j = 0; j < J; ++j) {
             Lam += ST::ld(c2v + l * m + j * P + res_map<P>(code.iF[0][j][l], code.iG[0][j][l], y));
-            Mu += ST::ld(c2v + (L + l) * m + j * P + res_map<P>(code.iF[1][j][l], code.iG[1][j][l], y));
+            Mu += ST::ld(c2vz + l * m + j * P + res_map<P>(code.iF[1][j][l], code.iG[1][j][l], y));
         }
         const float w0 = lp.x, w1 = lp.y - Lam, w2 = lp.z - Mu, w3 = lp.w - Lam - Mu;
         out[2 * v] = (res_lse2(w1, w3) - res_lse2(w0, w2)) * 0.69314718f;
@@ -699,17 +708,19 @@ __device__ __noinline__ void res_set_prior(int use_prior, const double *prior4, 
     *lpz = static_cast<float>(log2((q[0] + q[1]) / (q[2] + q[3])));
 }
 
-// GC: the c2v live in a per-block global scratch (L2-resident) instead of shared memory -- the
-// FP32-message instantiation, whose 221 KB of c2v per trial do not fit beside the rest.
+// GC: the Z side's c2v live in a per-block global scratch (L2-resident) instead of shared
+// memory -- the FP32-message instantiation, whose 221 KB of c2v per trial do not all fit beside
+// the rest (the X side's 110.6 KB do).
 template <int P, int J, int L, class ST, bool PP, bool LEARNED, bool GC = false>
 __global__ void __launch_bounds__(kResThreads, 1)
     k_resident(const __grid_constant__ ResCode code, const __grid_constant__ ResRun run) {
     extern __shared__ __align__(16) unsigned char res_smem[];
     using T = typename ST::T;
     constexpr int m = J * P, n = L * P, mw = (m + 31) / 32;
-    T *const c2v = GC ? reinterpret_cast<T *>(run.c2v_scratch + run.c2v_stride * blockIdx.x)
-                      : reinterpret_cast<T *>(res_smem);
-    constexpr size_t c2v_bytes = GC ? 0 : (2ull * L * m * sizeof(T) + 15) / 16 * 16;
+    T *const c2v = reinterpret_cast<T *>(res_smem);   // side X, [l][c]
+    T *const c2vz = GC ? reinterpret_cast<T *>(run.c2v_scratch + run.c2v_stride * blockIdx.x)
+                       : c2v + L * m;                   // side Z
+    constexpr size_t c2v_bytes = ((GC ? 1ull : 2ull) * L * m * sizeof(T) + 15) / 16 * 16;
     float *const A = reinterpret_cast<float *>(res_smem + c2v_bytes);
     uint8_t *const err = res_smem + c2v_bytes + 2ull * n * 4;
     unsigned *const syn = reinterpret_cast<unsigned *>(err + (n + 15) / 16 * 16);
@@ -829,7 +840,8 @@ __global__ void __launch_bounds__(kResThreads, 1)
             const int side = r >= m, c = r - side * m;
             const bool neg = (syn[side * mw + (c >> 5)] >> (c & 31)) & 1u;
 #pragma unroll
-            for (int l = 0; l < L; ++l) ST::st(c2v + (side * L + l) * m + c, neg ? -first_sh[side][l] : first_sh[side][l]);
+            for (int l = 0; l < L; ++l)
+                ST::st((side ? c2vz : c2v) + l * m + c, neg ? -first_sh[side][l] : first_sh[side][l]);
         }
         __syncthreads();
 
@@ -851,7 +863,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
             int bx = 0, bz = 0;
             if (it < run.max_iter && !sep && it > 0) {   // iteration 1's check phase is the closed form above
                 bx = res_check_side<P, J, L, ST, 0>(code, c2v, A, syn, fused);
-                bz = res_check_side<P, J, L, ST, 1>(code, c2v, A, syn, fused);
+                bz = res_check_side<P, J, L, ST, 1>(code, c2vz, A, syn, fused);
             } else if (fused) {
                 bx = res_test_side<P, J, L>(code, A, syn, 0);
                 bz = res_test_side<P, J, L>(code, A, syn, 1);
@@ -875,21 +887,21 @@ __global__ void __launch_bounds__(kResThreads, 1)
             if (it >= run.max_iter) break;
             if (sep) {
                 res_check_side<P, J, L, ST, 0>(code, c2v, A, syn, false);
-                res_check_side<P, J, L, ST, 1>(code, c2v, A, syn, false);
+                res_check_side<P, J, L, ST, 1>(code, c2vz, A, syn, false);
                 __syncthreads();
             }
             if (PP && threadIdx.x == 0) us_cnt[(it + 1) & 1][0] = us_cnt[(it + 1) & 1][1] = 0;   // next test's slot
             if constexpr (learned) {
                 unsigned ch1 = 0u, ch2 = 0u;
                 for (int y = threadIdx.x; y < P; y += blockDim.x)
-                    res_var_cols<P, J, L, ST, 0, true>(code, c2v, A, y, &lp_sh, &pr_sh, ch1, ch2);
+                    res_var_cols<P, J, L, ST, 0, true>(code, c2v, c2vz, A, y, &lp_sh, &pr_sh, ch1, ch2);
                 const bool d1 = __syncthreads_or(ch1 & 1u) != 0;
                 const bool d2 = __syncthreads_or(ch2 & 1u) != 0;
                 stall = it + 1 >= 3 && (!d1 || !d2);
             } else {
                 unsigned ch1 = 0u, ch2 = 0u;
                 for (int y = threadIdx.x; y < P; y += blockDim.x)
-                    res_var_cols<P, J, L, ST, 0, false>(code, c2v, A, y, &lp_sh, &pr_sh, ch1, ch2);
+                    res_var_cols<P, J, L, ST, 0, false>(code, c2v, c2vz, A, y, &lp_sh, &pr_sh, ch1, ch2);
                 __syncthreads();
             }
             ++it;
@@ -897,7 +909,8 @@ __global__ void __launch_bounds__(kResThreads, 1)
             // a stall of this iteration, whose c2v are still those its decisions came from
             const bool slow = PP && it >= slow_from;
             if (slow || (learned && stall && it >= run.learned_from && pp_sh[3] < kLearnedTries)) {
-                const int r3 = res_slow_step<P, J, L, ST>(code, run, res_smem, c2v, A, syn, err, have_err, it, t, lp_sh,
+                const int r3 = res_slow_step<P, J, L, ST>(code, run, res_smem, c2v, c2vz, A, syn, err, have_err, it, t,
+                                                         lp_sh,
                                                          us_hist, pp_sh, ints, slow);
                 if (r3 != 0) {
                     rf = r3 < 0 ? 0 : r3;
@@ -907,7 +920,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
             }
         }
         const bool ok = (rf & kResSyndromeOk) != 0;
-        if (run.llr_out) res_write_llr<P, J, L, ST>(code, c2v, lp_sh, run.llr_out + local * n * 2);
+        if (run.llr_out) res_write_llr<P, J, L, ST>(code, c2v, c2vz, lp_sh, run.llr_out + local * n * 2);
 
         // ---- classification (jointbp_ets.cpp:6199-6245): exact, stabilizer-equivalent residual
         const int words = (n + 63) / 64, w32 = 2 * words;

@@ -211,16 +211,18 @@ def test_autotune_picks_a_configuration_that_decodes_identically(decoder):
         assert (r1["iterations"] == r2["iterations"]).all() and (r1["success"] == r2["success"]).all()
 
 
-@pytest.mark.parametrize("pp", [False, True])
-def test_resident_fp32_messages(decoder, oracle, pp):
+@pytest.mark.parametrize("pp,learned", [(False, 0), (True, 0), (True, 6)])
+def test_resident_fp32_messages(decoder, oracle, pp, learned):
     """FP32 messages on the resident tier (asked for explicitly; the messages live in a per-block
     L2-resident scratch): one launch, flags recomputed by the oracle from the returned
     estimates, outcomes against FP64 on the same trials, and AUTO keeps FP32 on the slot engine."""
-    from joint_bp_plus_pp_b200 import Options, sample_reference_errors
+    from joint_bp_plus_pp_b200 import Options, load_flip_model, sample_reference_errors
     p, k = 0.055, 400
     err = sample_reference_errors(decoder.n, 31, 1, k, p)
-    o = Options(precision="fp32", engine="resident", max_iter=200, enable_pp=pp)
+    o = Options(precision="fp32", engine="resident", max_iter=200, enable_pp=pp, learned_from=learned)
+    decoder.set_flip_model(load_flip_model() if learned else None)
     st, res, est = decoder.decode_errors(err, p, o)
+    decoder.set_flip_model(None)
     assert st["trials"] == k and st["kernel_launches"] == 1
     for t in range(0, k, 5):
         ok, exact, stab, success = oracle.classify(err[t], est[t])
