@@ -125,6 +125,14 @@ int jbp_code_info(jbp_ctx *ctx, int *n, int *mx, int *mz, int *rank_x, int *rank
 /* Check lists (check-major, x_var has x_off[mx] entries); sizes from jbp_code_info. */
 int jbp_code_checks(jbp_ctx *ctx, int side, int *off, int *var);
 
+/* Start-up graph checks (check_hx_hz_orthogonality and compute_girth, jointbp_ets.cpp:1070-1171):
+ * odd_pairs = the (X check, Z check) pairs sharing an odd number of variables (0: Hx Hz^T = 0),
+ * girth_x / girth_z = the girth of each side's Tanner graph (0 without a cycle).  Any pointer
+ * may be null.  jbp_graph_checks takes check lists (as jbp_create_from_checks) and needs no GPU. */
+int jbp_code_graph_checks(jbp_ctx *ctx, long long *odd_pairs, int *girth_x, int *girth_z);
+int jbp_graph_checks(int n, int mx, const int *x_off, const int *x_var, int mz, const int *z_off, const int *z_var,
+                     long long *odd_pairs, int *girth_x, int *girth_z);
+
 /* Monte Carlo: trials first_trial .. first_trial+ntrials-1 of base seed `seed` at error rate p.
  * per_trial (host, ntrials entries) and iter_hist (host, max_iter+1 entries) may be null. */
 int jbp_simulate(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed, long long first_trial, long long ntrials,

@@ -125,6 +125,8 @@ def load_library(path=None):
     lib.jbp_decode_syndromes.argtypes = [vp, ctypes.POINTER(COptions), ll, vp, vp, d, vp, vp, ctypes.POINTER(CStats)]
     lib.jbp_decode_errors_llr.argtypes = [vp, ctypes.POINTER(COptions), ll, vp, d, vp, vp, ctypes.POINTER(CStats)]
     lib.jbp_autotune.argtypes = [vp, ctypes.POINTER(COptions), d, ll, ctypes.POINTER(COptions), ctypes.POINTER(d)]
+    lib.jbp_code_graph_checks.argtypes = [vp, ctypes.POINTER(ll), ctypes.POINTER(i), ctypes.POINTER(i)]
+    lib.jbp_graph_checks.argtypes = [i, i, vp, vp, i, vp, vp, ctypes.POINTER(ll), ctypes.POINTER(i), ctypes.POINTER(i)]
     lib.jbp_simulate_mixed.argtypes = [vp, i, ctypes.POINTER(COptions), vp, vp, vp, d, ctypes.POINTER(CStats), vp]
     lib.jbp_decode_errors_device.argtypes = [vp, ctypes.POINTER(COptions), ll, vp, d, vp, vp, ctypes.POINTER(CStats),
                                              vp]
@@ -348,6 +350,17 @@ class Decoder:
                                                              SAMPLER[sampler], capacity, _ptr(x), _ptr(y),
                                                              ctypes.byref(cnt), ctypes.byref(st)))
         return x[:cnt.value], y[:cnt.value], st.as_dict()
+
+
+def graph_checks(n, x_off, x_var, z_off, z_var):
+    """Start-up graph checks of a CSS code given as check lists, on the host (no GPU):
+    {"odd_pairs": X/Z check pairs with an odd overlap (0 = orthogonal), "girth_x", "girth_z"}."""
+    lib = load_library()
+    arr = [np.ascontiguousarray(a, np.int32) for a in (x_off, x_var, z_off, z_var)]
+    odd, gx, gz = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int()
+    _check(lib, lib.jbp_graph_checks(n, len(arr[0]) - 1, _ptr(arr[0]), _ptr(arr[1]), len(arr[2]) - 1, _ptr(arr[2]),
+                                     _ptr(arr[3]), ctypes.byref(odd), ctypes.byref(gx), ctypes.byref(gz)))
+    return {"odd_pairs": odd.value, "girth_x": gx.value, "girth_z": gz.value}
 
 
 def simulate_mixed(decoders, ntrials, p, opts=None, seeds=None, first_trial=None, per_trial=False):

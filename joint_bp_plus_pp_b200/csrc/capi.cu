@@ -124,6 +124,31 @@ int jbp_add_ets_group(jbp_ctx *ctx, int size, const char *label, const char *pat
 
 void jbp_destroy(jbp_ctx *ctx) { delete ctx; }
 
+static void put_graph_checks(const jbp::GraphChecks &g, long long *odd_pairs, int *girth_x, int *girth_z) {
+    if (odd_pairs) *odd_pairs = g.odd_pairs;
+    if (girth_x) *girth_x = g.girth[0];
+    if (girth_z) *girth_z = g.girth[1];
+}
+
+int jbp_code_graph_checks(jbp_ctx *ctx, long long *odd_pairs, int *girth_x, int *girth_z) {
+    if (!ctx) return fail(JBP_ERR_ARG, "null context");
+    put_graph_checks(jbp::graph_checks(ctx->engine.model()), odd_pairs, girth_x, girth_z);
+    return JBP_OK;
+}
+
+int jbp_graph_checks(int n, int mx, const int *x_off, const int *x_var, int mz, const int *z_off, const int *z_var,
+                     long long *odd_pairs, int *girth_x, int *girth_z) {
+    if (!x_off || !z_off || n <= 0 || mx < 0 || mz < 0) return fail(JBP_ERR_ARG, "invalid code arguments");
+    std::vector<int> xo(x_off, x_off + mx + 1), zo(z_off, z_off + mz + 1);
+    if (xo[mx] < 0 || zo[mz] < 0) return fail(JBP_ERR_ARG, "invalid check offsets");
+    std::vector<int> xv(x_var, x_var + xo[mx]), zv(z_var, z_var + zo[mz]);
+    jbp::CodeModel m;
+    std::string e = m.build_from_checks(n, xo, xv, zo, zv);
+    if (!e.empty()) return fail(JBP_ERR_ARG, e);
+    put_graph_checks(jbp::graph_checks(m), odd_pairs, girth_x, girth_z);
+    return JBP_OK;
+}
+
 int jbp_code_info(jbp_ctx *ctx, int *n, int *mx, int *mz, int *rank_x, int *rank_z, int *ets_groups) {
     if (!ctx) return fail(JBP_ERR_ARG, "null context");
     const auto &m = ctx->engine.model();

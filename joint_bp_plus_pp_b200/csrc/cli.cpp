@@ -639,6 +639,15 @@ int main(int argc, char **argv) {
     std::cout << "p=" << std::fixed << std::setprecision(6) << a.p << " n=" << n << " mx=" << mx << " mz=" << mz
               << " rank_x=" << rx << " rank_z=" << rz << " stab_rank=" << rx + rz << " k=" << k
               << " rate=" << (n ? static_cast<double>(k) / n : 0.0) << " ets_groups=" << ng << "\n";
+    {
+        long long odd = 0;
+        int gx = 0, gz = 0;
+        if (jbp_code_graph_checks(ctx, &odd, &gx, &gz) == JBP_OK) {
+            print_section("Graph Checks");
+            std::cout << "hx_hz_orthogonal=" << (odd == 0 ? "true" : "false") << "  hx_hz_odd_pairs=" << odd
+                      << "  girth_x=" << gx << "  girth_z=" << gz << "\n";
+        }
+    }
     const int rc = a.simulate ? simulate(ctx, a, n) : decode_single(ctx, a, n, mx, mz);
     jbp_destroy(ctx);
     return rc;

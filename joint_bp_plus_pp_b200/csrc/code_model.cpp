@@ -310,4 +310,87 @@ std::string CodeModel::load_ets_dir(const std::string &dir) {
     return "";
 }
 
+
+// ------------------------------------------------------------------ start-up graph checks
+
+namespace {
+
+// Check of each edge of a side (edge ids are check-major: chk_off[c] .. chk_off[c+1]-1).
+std::vector<int> edge_checks(const SideGraph &g) {
+    std::vector<int> ec(static_cast<size_t>(g.edges));
+    for (int c = 0; c < g.m; ++c)
+        for (int e = g.chk_off[c]; e < g.chk_off[c + 1]; ++e) ec[e] = c;
+    return ec;
+}
+
+// Pairs (X check, Z check) with an odd overlap: every variable contributes each pair of its
+// X and Z checks once, so a pair's overlap is the number of times it is listed.
+long long odd_overlap_pairs(const SideGraph &x, const SideGraph &z, int n) {
+    const std::vector<int> ecx = edge_checks(x), ecz = edge_checks(z);
+    std::vector<unsigned long long> pairs;
+    for (int v = 0; v < n; ++v)
+        for (int a = x.var_off[v]; a < x.var_off[v + 1]; ++a)
+            for (int b = z.var_off[v]; b < z.var_off[v + 1]; ++b)
+                pairs.push_back(static_cast<unsigned long long>(ecx[x.var_edge[a]]) << 32 |
+                                static_cast<unsigned>(ecz[z.var_edge[b]]));
+    std::sort(pairs.begin(), pairs.end());
+    long long odd = 0;
+    for (size_t i = 0; i < pairs.size();) {
+        size_t j = i;
+        while (j < pairs.size() && pairs[j] == pairs[i]) ++j;
+        odd += (j - i) & 1;
+        i = j;
+    }
+    return odd;
+}
+
+// Girth of a Tanner graph (variables 0..n-1, checks n..n+m-1): breadth-first search from every
+// variable; a non-tree edge between nodes at depths a and b closes a cycle of length a + b + 1
+// through the start's search tree, and the shortest such cycle over all starts is the girth.
+// A search stops expanding nodes at depth >= best/2, where no shorter cycle can close.
+int tanner_girth(const SideGraph &g, int n) {
+    const std::vector<int> ec = edge_checks(g);
+    const int total = n + g.m;
+    std::vector<int> depth(total), parent(total), mark(total, -1), queue(total);
+    int best = 0x7fffffff;
+    for (int s = 0; s < n && best > 4; ++s) {
+        int head = 0, tail = 0;
+        queue[tail++] = s;
+        mark[s] = s;
+        depth[s] = 0;
+        parent[s] = -1;
+        while (head < tail) {
+            const int u = queue[head++];
+            if (2 * depth[u] >= best) continue;
+            auto visit = [&](int w) {
+                if (mark[w] != s) {
+                    mark[w] = s;
+                    depth[w] = depth[u] + 1;
+                    parent[w] = u;
+                    queue[tail++] = w;
+                } else if (w != parent[u]) {
+                    best = std::min(best, depth[u] + depth[w] + 1);
+                }
+            };
+            if (u < n) {
+                for (int k = g.var_off[u]; k < g.var_off[u + 1]; ++k) visit(n + ec[g.var_edge[k]]);
+            } else {
+                const int c = u - n;
+                for (int e = g.chk_off[c]; e < g.chk_off[c + 1]; ++e) visit(g.chk_var[e]);
+            }
+        }
+    }
+    return best == 0x7fffffff ? 0 : best;
+}
+
+}  // namespace
+
+GraphChecks graph_checks(const CodeModel &m) {
+    GraphChecks r;
+    r.odd_pairs = odd_overlap_pairs(m.side[0], m.side[1], m.n);
+    r.girth[0] = tanner_girth(m.side[0], m.n);
+    r.girth[1] = tanner_girth(m.side[1], m.n);
+    return r;
+}
+
 }  // namespace jbp

@@ -69,6 +69,16 @@ struct CodeModel {
 
 std::string ets_read_file(const std::string &path, int P, int n, int expected_vars, char side, EtsTable &out,
                           bool *opened);
+
+// Start-up graph checks of a CSS code (the reference's check_hx_hz_orthogonality and
+// compute_girth, jointbp_ets.cpp:1070-1171): the number of (X check, Z check) pairs that share
+// an odd number of variables (0 for a valid CSS code), and the girth of each side's Tanner
+// graph (0 when it has no cycle).
+struct GraphChecks {
+    long long odd_pairs = 0;
+    int girth[2] = {0, 0};
+};
+GraphChecks graph_checks(const CodeModel &m);
 std::string params_ets_dir(const std::string &params_path);
 
 }  // namespace jbp
