@@ -1,7 +1,8 @@
 // Trial-resident BP: one persistent thread block per SM owns one trial at a time and keeps
-// all of its BP state in shared memory, from sampling to classification.  No message ever
-// travels to HBM; the only global traffic per trial is its error (or syndrome), its result
-// record and, when asked for, its estimate.
+// its BP state in shared memory, from sampling to classification.  No message ever travels to
+// HBM; the only global traffic per trial is its error (or syndrome), its result record and,
+// when asked for, its estimate.  With FP32 message storage (the GC instantiation) the Z side's
+// messages live in a per-block global scratch that stays in L2; everything else as below.
 //
 // Code structure.  The kernel is built for quasi-cyclic codes whose blocks are affine
 // permutations (the APM construction of the reference params file, jointbp_ets.cpp:98-160):
@@ -12,6 +13,7 @@
 // State of the trial in shared memory (shipped code: P = 768, J = 3, L = 12):
 //   c2v[side][l][c]  16-bit LLR (base 2), check-to-variable message of the edge of check c in
 //                    block column l                                    2*12*2304*2 = 110,592 B
+//                    (FP32 storage: the X side here, 12*2304*4 = 110,592 B)
 //   A[side][v]       FP32 "all but one" total of variable v on that side: the variable-to-check
 //                    message of edge (c, v) is A[side][v] - c2v[side][l][c], clamped.  The
 //                    lowest mantissa bit of A carries the hard decision bit of that side.
@@ -25,8 +27,9 @@
 // Arithmetic (FP32, base-2 LLRs, the same model as the slot engine's LLR kernels):
 //   check node, tanh rule in ratio form: u_i = 2^-|y_i|, t_i = (1 - u_i) / (1 + u_i), so the
 //     product of the other edges' t is PN/PD with PN = prod (1 - u_j), PD = prod (1 + u_j), and
-//     the output magnitude log2((1 + T) / (1 - T)) = log2((PD + PN) / (PD - PN)): one ex2 per
-//     input, one rcp and one lg2 per output; prefix/suffix products exclude the edge itself.
+//     the output magnitude log2((1 + T) / (1 - T)) = log2((PD + PN) / (PD - PN)), carried in the
+//     cancellation-free form of res_row_rule: one ex2 per input, one rcp and one lg2 per
+//     output; prefix/suffix products exclude the edge itself.
 //   variable node: Lam = sum of the X c2v, Mu = sum of the Z c2v; log2 weights of I, X, Z, Y
 //     are lp0, lp1 - Lam, lp2 - Mu, lp3 - Lam - Mu (first maximum = hard decision); the x-bit
 //     coupling through the Z side Gx = lse2(lp0, lp2 - Mu) - lse2(lp1, lp3 - Mu) and the z-bit

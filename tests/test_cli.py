@@ -71,6 +71,8 @@ def test_run_summary_equals_reference(name):
     assert r.returncode == 0, r.stderr
     for k in SUMMARY_KEYS:
         assert s[k] == g["summary"][k], (k, s[k], g["summary"][k])
+    # the reference's start-up graph checks line for the shipped code
+    assert "hx_hz_orthogonal=true  hx_hz_odd_pairs=0  girth_x=8  girth_z=8" in r.stdout
 
 
 @pytest.mark.gpu
