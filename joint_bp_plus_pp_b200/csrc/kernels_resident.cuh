@@ -350,8 +350,11 @@ __device__ __forceinline__ void res_var_col(const ResCode &code, const typename 
     if (HIST) {
         const unsigned hx = ((__float_as_uint(A[v]) << 1) | (best & 1u)) & 0x3Fu;
         const unsigned hz = ((__float_as_uint(A[n + v]) << 1) | (best >> 1)) & 0x3Fu;
-        ch1 |= (hx ^ (hx >> 1)) | (hz ^ (hz >> 1));
-        ch2 |= (hx ^ (hx >> 2)) | (hz ^ (hz >> 2));
+        // both sides' histories in one word (x in bits 0-5, z in bits 8-13): bit 0 and bit 8 of
+        // ch1 / ch2 say whether a decision differs from the previous iteration / the one before
+        const unsigned h = hx | (hz << 8);
+        ch1 |= h ^ (h >> 1);
+        ch2 |= h ^ (h >> 2);
         A[v] = __uint_as_float((__float_as_uint(Lam + Gx) & ~0x3Fu) | hx);
         A[n + v] = __uint_as_float((__float_as_uint(Mu + Hz) & ~0x3Fu) | hz);
     } else {
@@ -743,7 +746,9 @@ __global__ void __launch_bounds__(kResThreads, 1)
     const int slow_from = PP ? max(1, llr_from - 2) : 0x7fffffff;
 
     __shared__ double pt_sh;
+    unsigned long long claimed = 0;   // thread 0: the next trial index this block has claimed
     if (threadIdx.x == 0) {
+        claimed = atomicAdd(&run.cnt->next_trial, 1ull);
         res_set_prior(run.use_prior, run.prior4, run.p, &lp_sh, &pr_sh, &lpx_sh, &lpz_sh);
         for (int i = 0; i < 16; ++i) ints[i] = 0;
     }
@@ -751,7 +756,10 @@ __global__ void __launch_bounds__(kResThreads, 1)
 
     for (;;) {
         if (threadIdx.x == 0) {
-            const unsigned long long k = atomicAdd(&run.cnt->next_trial, 1ull);
+            // the index claimed at the previous trial's start; the next claim's latency overlaps
+            // this trial
+            const unsigned long long k = claimed;
+            claimed = atomicAdd(&run.cnt->next_trial, 1ull);
             trial_sh = k < static_cast<unsigned long long>(run.ntrials) ? static_cast<long long>(k) : -1;
             pp_sh[1] = 0;   // act_k
             pp_sh[2] = 0;   // pstate
@@ -898,8 +906,8 @@ __global__ void __launch_bounds__(kResThreads, 1)
                 unsigned ch1 = 0u, ch2 = 0u;
                 for (int y = threadIdx.x; y < P; y += blockDim.x)
                     res_var_cols<P, J, L, ST, 0, true>(code, c2v, c2vz, A, y, &lp_sh, &pr_sh, ch1, ch2);
-                const bool d1 = __syncthreads_or(ch1 & 1u) != 0;
-                const bool d2 = __syncthreads_or(ch2 & 1u) != 0;
+                const bool d1 = __syncthreads_or(ch1 & 0x101u) != 0;
+                const bool d2 = __syncthreads_or(ch2 & 0x101u) != 0;
                 stall = it + 1 >= 3 && (!d1 || !d2);
             } else {
                 unsigned ch1 = 0u, ch2 = 0u;
