@@ -57,7 +57,6 @@ struct MixRun {
     double prior4[4];
     unsigned char *scratch;        // per block, scratch_stride bytes (c2v of the codes that do not fit)
     size_t scratch_stride;
-    unsigned long long *bad_input;
 };
 
 __host__ __device__ inline size_t mix_align(size_t b) { return (b + 15) / 16 * 16; }
