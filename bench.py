@@ -319,10 +319,22 @@ def main():
         # trial-resident kernel: no message traffic to HBM; bound by the special-function unit
         # (MUFU: ex2 per edge input, rcp + lg2 per edge output, 1 ex2 + 2 lg2 per coupling)
         mufu_per_ti = 3 * EDGES + 6 * N_QUBITS
+        mix = {"ex2": EDGES + 2 * N_QUBITS, "rcp": EDGES, "lg2": EDGES + 4 * N_QUBITS}   # per trial-iteration
         kms = agg["device_ms"]
         sm_mhz = clk.get("sm_mhz") or 1965.0
         n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
-        sfu_peak = 16 * n_sm * sm_mhz / 1e3          # Gop/s: 16 MUFU results / clk / SM
+        derived = 16 * n_sm * sm_mhz / 1e3          # Gop/s: 16 MUFU results / clk / SM
+        try:
+            from joint_bp_plus_pp_b200 import measure_sfu
+            sfu = measure_sfu(local)
+            # the rate of the kernel's own mix of the three operations
+            sfu_peak = mufu_per_ti / sum(mix[k] / sfu[k] for k in mix)
+            sfu_kind = ("measured: MUFU microbenchmark (jbp_measure_sfu) ex2 %.0f, lg2 %.0f, rcp %.0f G/s, at the "
+                        "kernel's mix ex2:rcp:lg2 = %d:%d:%d" % (sfu["ex2"], sfu["lg2"], sfu["rcp"], mix["ex2"],
+                                                                 mix["rcp"], mix["lg2"]))
+        except Exception as e:   # the derived figure, said so
+            sfu, sfu_peak = None, derived
+            sfu_kind = f"derived: 16 MUFU results/clk/SM x {n_sm} SMs x median SM clock {sm_mhz:.0f} MHz ({e})"
         achieved = agg["bp_trial_iterations"] * mufu_per_ti / (kms / 1000.0) / 1e9 if kms > 0 else None
         table = args.engine == "table"
         tr = None if table else traffic_tab.get("resident_dram_bytes_per_trial" if args.precision == "fp16"
@@ -332,8 +344,9 @@ def main():
                  else "k_resident (FP32 c2v: X side in shared memory, Z side in a per-block L2-resident scratch)")
         roofline = {"bound": "sfu", "kernel": kname, "achieved": achieved,
                     "peak": sfu_peak, "unit": "Gop/s", "frac": achieved / sfu_peak if achieved else None,
+                    "peak_derived_16_per_clk_sm": derived, "sfu_measured": sfu,
                     "traffic": tr * agg["trials"] / args.steps if tr is not None else None,
-                    "peak_kind": f"derived: 16 MUFU results/clk/SM x {n_sm} SMs x median SM clock {sm_mhz:.0f} MHz",
+                    "peak_kind": sfu_kind,
                     "mufu_ops_per_trial_iteration": mufu_per_ti, "trial_iterations": agg["bp_trial_iterations"],
                     "launches": agg["kernel_launches"], "kernel_ms": kms,
                     "hbm_equivalent_gbs": agg["bp_trial_iterations"] * 2 * 2 * EDGES * 2 / (kms / 1000.0) / 1e9,

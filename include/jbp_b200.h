@@ -185,6 +185,12 @@ int jbp_decode_syndromes_noalloc(jbp_ctx *ctx, const jbp_options *opt, int ntria
  * layout W1[64][8], b1[64], W2[64][64], b2[64], W3[2][64], b3[2] (jbp_mlp_param_count()).
  * Features x are nsamples x 8 floats, labels y nsamples x 2 floats (0/1), host buffers. */
 int jbp_mlp_param_count(void);
+
+/* Measured FP32 special-function throughput of a device (G results/s for the whole GPU) for
+ * ex2, lg2 and rcp (approx, flush-to-zero), the operations of the BP check and variable
+ * rules: the denominators of the SFU roofline the resident and table-driven kernels report.
+ * No counterpart in the reference.  About 10 ms of GPU time. */
+int jbp_measure_sfu(int device, double *ex2_gops, double *lg2_gops, double *rcp_gops);
 /* Gradient of the mean loss (binary cross-entropy with logits, positives weighted by
  * pos_weight, summed over the two outputs) on the GPU; grad_out has jbp_mlp_param_count()
  * entries. */

@@ -127,6 +127,7 @@ def load_library(path=None):
     lib.jbp_autotune.argtypes = [vp, ctypes.POINTER(COptions), d, ll, ctypes.POINTER(COptions), ctypes.POINTER(d)]
     lib.jbp_code_graph_checks.argtypes = [vp, ctypes.POINTER(ll), ctypes.POINTER(i), ctypes.POINTER(i)]
     lib.jbp_graph_checks.argtypes = [i, i, vp, vp, i, vp, vp, ctypes.POINTER(ll), ctypes.POINTER(i), ctypes.POINTER(i)]
+    lib.jbp_measure_sfu.argtypes = [i, ctypes.POINTER(d), ctypes.POINTER(d), ctypes.POINTER(d)]
     lib.jbp_simulate_mixed.argtypes = [vp, i, ctypes.POINTER(COptions), vp, vp, vp, d, ctypes.POINTER(CStats), vp]
     lib.jbp_decode_errors_device.argtypes = [vp, ctypes.POINTER(COptions), ll, vp, d, vp, vp, ctypes.POINTER(CStats),
                                              vp]
@@ -350,6 +351,14 @@ class Decoder:
                                                              SAMPLER[sampler], capacity, _ptr(x), _ptr(y),
                                                              ctypes.byref(cnt), ctypes.byref(st)))
         return x[:cnt.value], y[:cnt.value], st.as_dict()
+
+
+def measure_sfu(device=0):
+    """Measured special-function throughput of a GPU, G results/s: {"ex2", "lg2", "rcp"}."""
+    lib = load_library()
+    r = [ctypes.c_double() for _ in range(3)]
+    _check(lib, lib.jbp_measure_sfu(device, *[ctypes.byref(x) for x in r]))
+    return {"ex2": r[0].value, "lg2": r[1].value, "rcp": r[2].value}
 
 
 def graph_checks(n, x_off, x_var, z_off, z_var):

@@ -28,7 +28,7 @@ NVFLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--ex
                   "-Xptxas", "-warn-spills", f"-I{INCLUDE}"]
 HOSTFLAGS = ["-O2", "-std=c++17", "-fPIC", f"-I{INCLUDE}"]
 
-LIB_SOURCES = ["code_model.cpp", "engine.cu", "capi.cu", "noalloc.cu", "learned.cu"]
+LIB_SOURCES = ["code_model.cpp", "engine.cu", "capi.cu", "noalloc.cu", "learned.cu", "peaks.cu"]
 SHIM_SOURCES = ["jointbp_cuda_shim.cpp"]
 CLI_SOURCES = ["cli.cpp"]
 
