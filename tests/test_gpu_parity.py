@@ -271,3 +271,15 @@ def test_table_engine_refuses_other_sources(decoder, oracle):
         with pytest.raises(JbpError) as e:
             call()
         assert e.value.code == 4, str(e.value)
+
+
+def test_sfu_measurement_is_plausible():
+    """The SFU microbenchmark behind the roofline denominator: each of ex2, lg2, rcp between a
+    quarter and twice 16 results/clk/SM at the device's maximum clock."""
+    import torch
+    from joint_bp_plus_pp_b200 import measure_sfu
+    prop = torch.cuda.get_device_properties(0)
+    r = measure_sfu(0)
+    ceiling = 16 * prop.multi_processor_count * 2.1   # G/s at a clock up to 2.1 GHz
+    for k in ("ex2", "lg2", "rcp"):
+        assert 0.25 * ceiling < r[k] < 2.0 * ceiling, (k, r[k])
