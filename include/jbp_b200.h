@@ -219,8 +219,12 @@ int jbp_collect_stall_states(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed
  * options in *opt) over the launch choices that do not change any decoding result -- the
  * engine (resident where it applies, else slots), the slot engine's trials in flight (4096 ..
  * 32768) and its BP iterations per CUDA-graph launch (2, 4, 8) -- and writes the fastest into
- * *best (a copy of *opt with engine, slots and iters_per_launch set).  best_trials_per_s may
- * be null. */
+ * *best (a copy of *opt with engine, slots and iters_per_launch set).  With
+ * opt->check_interval == 0 it also considers the choices that change results: the syndrome-test
+ * interval among 1, 2 and 4 when post-processing is off (trials stop at a multiple of the
+ * interval, as with the reference's --cuda-check-interval), and for FP32 messages the resident
+ * engine, whose arithmetic differs slightly from the slot engine's.  best_trials_per_s may be
+ * null. */
 int jbp_autotune(jbp_ctx *ctx, const jbp_options *opt, double p, long long probe_trials, jbp_options *best,
                  double *best_trials_per_s);
 

@@ -257,8 +257,8 @@ class Decoder:
                                                  ctypes.byref(rate)))
         inv = {v: k for k, v in ENGINE.items()}
         from dataclasses import replace
-        return replace(opts, engine=inv[best.engine], slots=best.slots, iters_per_launch=best.iters_per_launch), \
-            rate.value
+        return replace(opts, engine=inv[best.engine], slots=best.slots, iters_per_launch=best.iters_per_launch,
+                       check_interval=best.check_interval), rate.value
 
     def decode_errors_llr(self, err, p, opts=None):
         """decode_errors plus the final LLRs (trials x n x 2: x bit, z bit; natural log of

@@ -439,18 +439,31 @@ int jbp_autotune(jbp_ctx *ctx, const jbp_options *opt, double p, long long probe
                  double *best_trials_per_s) {
     if (!ctx || !best || probe_trials <= 0) return fail(JBP_ERR_ARG, "invalid argument");
     const jbp_options base = normalized(opt);
+    // check_interval 0 (asked for explicitly) admits the choices that change results: the
+    // interval of the syndrome test, among 1, 2 and 4, where post-processing is off (it needs a
+    // test every iteration) -- trials then stop at a multiple of the interval -- and, for FP32
+    // messages, the resident engine, whose arithmetic differs slightly from the slot engine's
+    // that AUTO uses for FP32.  Otherwise every candidate decodes as AUTO does.
+    const bool result_changing = opt && opt->check_interval == 0;
+    const bool tune_ci = result_changing && !base.enable_pp;
+    const bool resident_ok = base.precision != JBP_PREC_FP32 || result_changing;
+    std::vector<int> intervals = tune_ci ? std::vector<int>{1, 2, 4} : std::vector<int>{base.check_interval};
     std::vector<jbp_options> cand;
-    jbp_options c = base;
-    c.engine = JBP_ENGINE_RESIDENT;
-    cand.push_back(c);
-    for (int S : {4096, 8192, 16384, 32768})
-        for (int gi : {2, 4, 8}) {
-            c = base;
-            c.engine = JBP_ENGINE_SLOTS;
-            c.slots = S;
-            c.iters_per_launch = gi;
-            cand.push_back(c);
-        }
+    for (int ci : intervals) {
+        jbp_options c = base;
+        c.check_interval = ci;
+        c.engine = JBP_ENGINE_RESIDENT;
+        if (resident_ok) cand.push_back(c);
+        for (int S : {4096, 8192, 16384, 32768})
+            for (int gi : {2, 4, 8}) {
+                c = base;
+                c.check_interval = ci;
+                c.engine = JBP_ENGINE_SLOTS;
+                c.slots = S;
+                c.iters_per_launch = gi;
+                cand.push_back(c);
+            }
+    }
     double best_rate = -1.0;
     for (const jbp_options &o : cand) {
         jbp_stats st;

@@ -59,7 +59,7 @@ void usage(const char *prog) {
               << "  --report-every N (100)  --progress-every N (100)  --progress-tsv FILE  --iter-hist-out FILE\n"
               << "  --ets6-x F --ets6-z F --ets12-x F --ets12-z F --ets-x F --ets-z F --ets8-path4 F\n"
               << "  --cuda --cuda-graph (accepted; decoding always runs on the GPU)  --cuda-device D\n"
-              << "  --cuda-check-warmup N (0)  --cuda-check-interval N (1)\n"
+              << "  --cuda-check-warmup N (0)  --cuda-check-interval N (1; 0 with --autotune: tuned)\n"
               << "Extra options:\n"
               << "  --precision fp64|fp32|fp16 (fp64)  --sampler mt19937|philox (mt19937)\n"
               << "  --slots N (trials in flight, 0 = auto)  --batch N (trials per GPU call, 262144)\n"
@@ -175,7 +175,7 @@ int parse(int argc, char **argv, Args &a) {
             else if (f == "--cuda" || f == "--cuda-graph") {}
             else if (f == "--cuda-device") { VAL(); a.device = std::stoi(v); }
             else if (f == "--cuda-check-warmup") { VAL(); a.check_warmup = std::max(0, std::stoi(v)); }
-            else if (f == "--cuda-check-interval") { VAL(); a.check_interval = std::max(1, std::stoi(v)); }
+            else if (f == "--cuda-check-interval") { VAL(); a.check_interval = std::max(0, std::stoi(v)); }
             else if (f == "--trial-index") { VAL(); a.trial_index = std::stoll(v); }
             else if (f == "--precision") {
                 VAL();
@@ -444,7 +444,8 @@ int simulate(jbp_ctx *ctx, const Args &a, int n) {
         }
         o = best;
         std::cout << "autotune: engine=" << (o.engine == JBP_ENGINE_RESIDENT ? "resident" : "slots")
-                  << " slots=" << o.slots << " iters_per_launch=" << o.iters_per_launch << " probe_trials_per_s="
+                  << " slots=" << o.slots << " iters_per_launch=" << o.iters_per_launch
+                  << " check_interval=" << o.check_interval << " probe_trials_per_s="
                   << std::fixed << std::setprecision(0) << rate << "\n";
     }
     const long long first = a.trial_index >= 0 ? a.trial_index : 1;

@@ -202,7 +202,7 @@ def test_pinned_host_inputs_are_read_in_place(decoder, oracle, engine, prec):
 
 def test_autotune_picks_a_configuration_that_decodes_identically(decoder):
     from joint_bp_plus_pp_b200 import Options
-    for prec, want in (("fp16", "resident"), ("fp64", "slots")):
+    for prec, want in (("fp16", "resident"), ("fp64", "slots"), ("fp32", "slots")):
         o = Options(precision=prec, max_iter=200, enable_pp=False)
         best, rate = decoder.autotune(0.04, o, probe_trials=2048)
         assert rate > 0 and best.engine == want
@@ -232,3 +232,19 @@ def test_resident_fp32_messages(decoder, oracle, pp, learned):
     assert abs(int(res["success"].sum()) - int(r64["success"].sum())) <= 4
     s_auto, _, _ = decoder.decode_errors(err[:8], p, Options(precision="fp32", max_iter=200, enable_pp=pp))
     assert s_auto["kernel_launches"] > 1          # the slot engine: several launches per run
+
+
+def test_autotune_can_choose_the_check_interval(decoder):
+    """With check_interval 0 (post-processing off) the autotuner also picks the syndrome-test
+    interval; the chosen options decode, and trials stop at a multiple of it."""
+    from joint_bp_plus_pp_b200 import Options
+    o = Options(precision="fp32", max_iter=200, enable_pp=False, check_interval=0)
+    best, rate = decoder.autotune(0.04, o, probe_trials=2048)
+    assert rate > 0 and best.check_interval in (1, 2, 4)
+    st, r = decoder.simulate(9, 512, 0.04, best)
+    assert st["trials"] == 512
+    done = r["syndrome_ok"] == 1
+    assert ((r["iterations"][done] - best.check_warmup) % best.check_interval == 0).all()
+    pp, _ = decoder.autotune(0.04, Options(precision="fp16", max_iter=200, enable_pp=True, check_interval=0),
+                             probe_trials=1024)
+    assert pp.check_interval == 1                     # post-processing keeps a test every iteration
