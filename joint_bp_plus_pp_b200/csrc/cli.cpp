@@ -42,7 +42,7 @@ struct Args {
     int precision = JBP_PREC_FP64, sampler = JBP_SAMPLER_MT19937, slots = 0;
     long long batch = 1 << 18;
     int engine = JBP_ENGINE_AUTO, learned_from = 0;
-    std::string flip_model, checks;
+    std::string flip_model, checks, mixed;
     double p_max = 0.0;
     bool autotune = false;
 };
@@ -69,7 +69,9 @@ void usage(const char *prog) {
               << "  shipped data/flip_mlp_params.npy next to the library)\n"
               << "  --checks FILE (a code as check lists instead of --params: 'n mx mz', then one line of\n"
               << "  variables per X check and per Z check)  --p-max P (per-trial p uniform in [p, P))\n"
-              << "  --autotune (time short probes and keep the fastest engine / slots / graph length)\n";
+              << "  --autotune (time short probes and keep the fastest engine / slots / graph length)\n"
+              << "  --mixed FILE1,FILE2,... (with --simulate --no-pp: the codes of these check-list files, --trials\n"
+              << "  trials each with seed --seed + i, in one kernel launch; one Run Summary per code)\n";
 }
 
 // format_scaled_unit / format_latency (jointbp_ets.cpp:203-237)
@@ -201,6 +203,7 @@ int parse(int argc, char **argv, Args &a) {
             } else if (f == "--learned-from") { VAL(); a.learned_from = std::max(0, std::stoi(v)); }
             else if (f == "--flip-model") { VAL(); a.flip_model = v; }
             else if (f == "--checks") { VAL(); a.checks = v; }
+            else if (f == "--mixed") { VAL(); a.mixed = v; }
             else if (f == "--autotune") a.autotune = true;
             else if (f == "--p-max") { VAL(); a.p_max = std::stod(v); }
             else if (f == "--slots") { VAL(); a.slots = std::stoi(v); }
@@ -550,6 +553,107 @@ int simulate(jbp_ctx *ctx, const Args &a, int n) {
     return 0;
 }
 
+// A code as check lists ('n mx mz', then the variables of each X check and of each Z check, one
+// check per line).  Returns false (after a message) when the file cannot be read.
+bool read_checks_file(const std::string &path, int &n, int m[2], std::vector<int> off[2], std::vector<int> var[2]) {
+    std::ifstream in(path);
+    n = 0;
+    m[0] = m[1] = 0;
+    if (!in || !(in >> n >> m[0] >> m[1]) || n <= 0 || m[0] <= 0 || m[1] <= 0) {
+        std::cerr << "Failed to read checks: " << path << "\n";
+        return false;
+    }
+    std::string line;
+    std::getline(in, line);
+    for (int s = 0; s < 2; ++s) {
+        off[s].assign(1, 0);
+        var[s].clear();
+        for (int c = 0; c < m[s]; ++c) {
+            if (!std::getline(in, line)) {
+                std::cerr << "Failed to read checks: " << path << " (too few lines)\n";
+                return false;
+            }
+            std::istringstream ls(line);
+            int v;
+            while (ls >> v) var[s].push_back(v);
+            off[s].push_back(static_cast<int>(var[s].size()));
+        }
+    }
+    return true;
+}
+
+// --mixed: the codes of several check-list files decoded in one launch (jbp_simulate_mixed).
+int simulate_mixed_files(const Args &a) {
+    if (!a.simulate) {
+        std::cerr << "--mixed requires --simulate\n";
+        return 1;
+    }
+    if (a.enable_pp) {
+        std::cerr << "--mixed decodes with plain BP: add --no-pp\n";
+        return 1;
+    }
+    std::vector<std::string> files;
+    std::stringstream ss(a.mixed);
+    for (std::string f; std::getline(ss, f, ',');)
+        if (!f.empty()) files.push_back(f);
+    std::vector<jbp_ctx *> ctxs;
+    auto cleanup = [&]() {
+        for (jbp_ctx *c : ctxs) jbp_destroy(c);
+    };
+    std::vector<int> ns;
+    for (const std::string &f : files) {
+        int n = 0, m[2];
+        std::vector<int> off[2], var[2];
+        if (!read_checks_file(f, n, m, off, var)) {
+            cleanup();
+            return 1;
+        }
+        jbp_ctx *c = nullptr;
+        if (jbp_create_from_checks(n, m[0], off[0].data(), var[0].data(), m[1], off[1].data(), var[1].data(),
+                                   a.device, &c) != JBP_OK) {
+            std::cerr << "init failed: " << f << ": " << jbp_last_error() << "\n";
+            cleanup();
+            return 1;
+        }
+        ctxs.push_back(c);
+        ns.push_back(n);
+    }
+    const int k = static_cast<int>(ctxs.size());
+    std::vector<uint64_t> seeds(k);
+    std::vector<long long> first(k, a.trial_index >= 0 ? a.trial_index : 1), ntrials(k, a.trials);
+    for (int i = 0; i < k; ++i) seeds[i] = a.seed + static_cast<uint64_t>(i);
+    std::vector<jbp_stats> st(k);
+    const jbp_options o = options(a);
+    const auto t0 = std::chrono::steady_clock::now();
+    const int rc = jbp_simulate_mixed(ctxs.data(), k, &o, seeds.data(), first.data(), ntrials.data(), a.p, st.data(),
+                                      nullptr);
+    const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (rc != JBP_OK) {
+        std::cerr << "mixed run failed: " << jbp_last_error() << "\n";
+        cleanup();
+        return 1;
+    }
+    long long total = 0;
+    for (int i = 0; i < k; ++i) {
+        const long long d = st[i].trials;
+        total += d;
+        double lo = 0.0, hi = 0.0;
+        const bool ci = wilson(d, st[i].failures, 1.96, lo, hi);
+        print_section(("Run Summary (" + files[i] + ")").c_str());
+        std::cout << "n=" << ns[i] << " trials=" << d << " failures=" << st[i].failures << " fer=" << std::fixed
+                  << std::setprecision(8) << (d ? static_cast<double>(st[i].failures) / d : 0.0);
+        if (ci) std::cout << " ci95=[" << lo << "," << hi << "]";
+        std::cout << " iters=" << st[i].total_iters << " avg_iter=" << std::setprecision(2)
+                  << (d ? static_cast<double>(st[i].total_iters) / d : 0.0) << " exact_rate=" << std::setprecision(6)
+                  << (d ? static_cast<double>(st[i].exact) / d : 0.0) << "\n";
+    }
+    std::cout << "gpu: mixed launch of " << k << " codes, kernel_launches=" << (k ? st[0].kernel_launches : 0)
+              << " device_ms=" << std::setprecision(2) << (k ? st[0].device_ms : 0.0)
+              << " trials_per_s=" << (elapsed > 0 ? total / elapsed : 0.0) << "\n";
+    cleanup();
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -562,6 +666,7 @@ int main(int argc, char **argv) {
                                                      std::chrono::system_clock::now().time_since_epoch())
                                                      .count());
     }
+    if (!a.mixed.empty()) return simulate_mixed_files(a);
     if (a.params.empty() && a.checks.empty()) {
         std::cerr << "--params is required\n";
         return 1;
@@ -587,28 +692,9 @@ int main(int argc, char **argv) {
     jbp_ctx *ctx = nullptr;
     if (!a.checks.empty()) {
         // a code given as check lists (no ETS tables)
-        std::ifstream in(a.checks);
-        int n = 0, m[2] = {0, 0};
-        if (!in || !(in >> n >> m[0] >> m[1]) || n <= 0 || m[0] <= 0 || m[1] <= 0) {
-            std::cerr << "Failed to read checks: " << a.checks << "\n";
-            return 1;
-        }
-        std::string line;
-        std::getline(in, line);
+        int n = 0, m[2];
         std::vector<int> off[2], var[2];
-        for (int s = 0; s < 2; ++s) {
-            off[s].push_back(0);
-            for (int c = 0; c < m[s]; ++c) {
-                if (!std::getline(in, line)) {
-                    std::cerr << "Failed to read checks: " << a.checks << " (too few lines)\n";
-                    return 1;
-                }
-                std::istringstream ls(line);
-                int v;
-                while (ls >> v) var[s].push_back(v);
-                off[s].push_back(static_cast<int>(var[s].size()));
-            }
-        }
+        if (!read_checks_file(a.checks, n, m, off, var)) return 1;
         if (jbp_create_from_checks(n, m[0], off[0].data(), var[0].data(), m[1], off[1].data(), var[1].data(),
                                    a.device, &ctx) != JBP_OK) {
             std::cerr << "init failed: " << jbp_last_error() << "\n";

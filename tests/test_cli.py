@@ -55,6 +55,16 @@ def test_engine_and_autotune_flags_parse():
     assert "--engine auto|resident|slots|table" in r.stdout and "--autotune" in r.stdout
 
 
+def test_mixed_usage_errors(tmp_path):
+    r = subprocess.run([str(CLI), "--mixed", "a,b", "--simulate"], capture_output=True, text=True)
+    assert r.returncode == 1 and "--mixed decodes with plain BP: add --no-pp" in r.stderr
+    r = subprocess.run([str(CLI), "--mixed", "a,b", "--no-pp"], capture_output=True, text=True)
+    assert r.returncode == 1 and "--mixed requires --simulate" in r.stderr
+    r = subprocess.run([str(CLI), "--mixed", str(tmp_path / "missing.checks"), "--simulate", "--no-pp"],
+                       capture_output=True, text=True)
+    assert r.returncode == 1 and "Failed to read checks" in r.stderr
+
+
 def test_without_gpu_fails_loudly():
     import torch
     if torch.cuda.is_available():

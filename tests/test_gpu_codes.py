@@ -144,3 +144,32 @@ def test_cli_decodes_a_check_list_code(tmp_path):
     assert r.returncode == 0, r.stderr
     s = dict(re.findall(r"(\w+)=(\S+)", [l for l in r.stdout.splitlines() if l.startswith("trials=")][-1]))
     assert s["trials"] == "2000" and 0 < int(s["failures"]) < 2000
+
+
+def test_cli_mixed_launch_equals_the_api(tmp_path):
+    """bin/jointbp_b200 --mixed: two check-list codes in one launch, per-code Run Summaries equal
+    to the C ABI's (same seeds seed + i, same trials)."""
+    import re
+    import subprocess
+    from pathlib import Path
+    from joint_bp_plus_pp_b200 import Decoder, Options, simulate_mixed
+    from joint_bp_plus_pp_b200.codes import write_checks
+    cli = Path(__file__).resolve().parents[1] / "joint_bp_plus_pp_b200" / "bin" / "jointbp_b200"
+    files, decs = [], []
+    for i, nc in enumerate((16, 32)):
+        code = hgp_code(nc, i + 1)
+        f = tmp_path / f"hgp{nc}.checks"
+        write_checks(f, *code)
+        files.append(str(f))
+        decs.append(Decoder.from_checks(*code))
+    r = subprocess.run([str(cli), "--mixed", ",".join(files), "--simulate", "--no-pp", "--p", "0.01", "--p-max", "0.05",
+                        "--trials", "3000", "--max-iter", "100", "--precision", "fp32", "--seed", "40"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = [l for l in r.stdout.splitlines() if l.startswith("n=")]
+    assert len(lines) == 2 and "kernel_launches=1" in r.stdout
+    st, _ = simulate_mixed(decs, [3000, 3000], 0.01, Options(precision="fp32", max_iter=100, enable_pp=False,
+                                                             p_max=0.05), seeds=[40, 41])
+    for line, s in zip(lines, st):
+        d = dict(re.findall(r"(\w+)=(\S+)", line))
+        assert (int(d["trials"]), int(d["failures"]), int(d["iters"])) == (s["trials"], s["failures"], s["total_iters"])
