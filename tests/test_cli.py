@@ -74,7 +74,8 @@ def test_without_gpu_fails_loudly():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["p050_mi50_nopp_s1_t200", "p050_mi200_pp_s305_t40", "p055_mi60_nopp_frz_s21_t60"])
+@pytest.mark.parametrize("name", ["p050_mi50_nopp_s1_t200", "p050_mi200_pp_s305_t40", "p055_mi60_nopp_frz_s21_t60",
+                                  "p050_mi50_nopp_s1_t1000"])
 def test_run_summary_equals_reference(name):
     g = json.loads((GOLDEN / "cli_summaries.json").read_text())[name]
     r, s = run(g["args"] + ["--batch", "64"])
