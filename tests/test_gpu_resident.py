@@ -111,7 +111,8 @@ def test_resident_refuses_what_it_does_not_run(decoder):
 
 # ---------------------------------------------------------------- post-processing in the resident kernel
 
-def test_resident_pp_stage_trials(decoder, oracle):
+@pytest.mark.parametrize("prec", ["fp16", "fp32"])
+def test_resident_pp_stage_trials(decoder, oracle, prec):
     """Errors that make each post-processing stage act (constructed trapping-set errors and
     sampled trials), decoded with the stages inside the resident kernel: its flags agree with
     the oracle's classification of its own estimates, and its outcomes agree with the
@@ -120,7 +121,7 @@ def test_resident_pp_stage_trials(decoder, oracle):
     total = same_est = same_rec = 0
     for (p, mi, fh), cases in sorted(load_stage_trials(decoder.n).items()):
         errs = np.stack([c[1] for c in cases])
-        st, res, est = decoder.decode_errors(errs, p, ropts(max_iter=mi, flip_hist=fh, enable_pp=True))
+        st, res, est = decoder.decode_errors(errs, p, ropts(max_iter=mi, flip_hist=fh, enable_pp=True, precision=prec))
         for (label, err, est_ref, rec), r, e in zip(cases, res, est):
             ok, exact, stab, success = oracle.classify(err, e)
             assert (r["syndrome_ok"], r["exact"], r["success"]) == (ok, exact, success), (label, mi)
@@ -131,14 +132,15 @@ def test_resident_pp_stage_trials(decoder, oracle):
     assert same_rec >= 0.8 * total, (same_rec, total)
 
 
+@pytest.mark.parametrize("prec", ["fp16", "fp32"])
 @pytest.mark.parametrize("name", ["p050_mi200_pp_s305", "p060_mi120_pp_s7"])
-def test_resident_pp_ler_close_to_fp64(decoder, name):
+def test_resident_pp_ler_close_to_fp64(decoder, name, prec):
     from conftest import load_sim_case
     from test_gpu_pp import opts_for
     meta, errs, _ = load_sim_case(name)
     st64, r64, _ = decoder.decode_errors(errs, meta["p"], opts_for(meta), want_est=False)
     st, r, _ = decoder.decode_errors(errs, meta["p"], ropts(max_iter=meta["max_iter"], flip_hist=meta["flip_hist"],
-                                                            enable_pp=True), want_est=False)
+                                                            enable_pp=True, precision=prec), want_est=False)
     assert st["trials"] == len(errs) and st["kernel_launches"] == 1
     assert abs(st["failures"] - st64["failures"]) <= max(3, len(errs) // 4)
     assert (r["success"] != r64["success"]).mean() <= 0.1
