@@ -80,7 +80,8 @@ def test_learned_needs_a_model(decoder):
                                              learned_from=10))
 
 
-def test_trained_model_gain(decoder):
+@pytest.mark.parametrize("prec", ["fp16", "fp32"])
+def test_trained_model_gain(decoder, prec):
     """The shipped model (trained by joint_bp_plus_pp_b200.learned on the decoder's own stalled
     states) against the same decoder without it, on the same 40,000 trials at p=0.045 (max-iter
     300, post-processing on, proposals from iteration 6).  What the network gains: trials that
@@ -92,7 +93,7 @@ def test_trained_model_gain(decoder):
     assert params is not None, "data/flip_mlp_params.npy missing"
     decoder.set_flip_model(params)
     N = 40000
-    base = dict(precision="fp16", engine="resident", max_iter=300, enable_pp=True)
+    base = dict(precision=prec, engine="resident", max_iter=300, enable_pp=True)
     s0, r0 = decoder.simulate(606, N, 0.045, Options(**base))
     s1, r1 = decoder.simulate(606, N, 0.045, Options(learned_from=6, **base))
     decoder.set_flip_model(None)
