@@ -95,7 +95,7 @@ __device__ __forceinline__ int frozen_bit(const DevRun &run, int n, int side, in
 // ------------------------------------------------------------------ FP64, bit-exact
 
 template <int DC, bool DAMP>
-__global__ void __launch_bounds__(256) k_check_f64(DevCode code, DevRun run, DevMsgs msg) {
+__global__ void __launch_bounds__(256, 3) k_check_f64(DevCode code, DevRun run, DevMsgs msg) {
     const int lane = threadIdx.x & 31;
     const int G = run.S / kGroup;
     const int mx = code.s[0].m, M = mx + code.s[1].m;
@@ -205,7 +205,7 @@ __device__ __forceinline__ void store_v2c_f64(double2 *v2c, double2 *v2c_hi, siz
 }
 
 template <int DC, int DV, bool DAMP>
-__global__ void __launch_bounds__(256) k_var_f64(DevCode code, DevRun run, DevMsgs msg, double damping) {
+__global__ void __launch_bounds__(256, 2) k_var_f64(DevCode code, DevRun run, DevMsgs msg, double damping) {
     const int lane = threadIdx.x & 31;
     const int G = run.S / kGroup, n = code.n;
     const unsigned total = static_cast<unsigned>(*run.n_groups) * n;
