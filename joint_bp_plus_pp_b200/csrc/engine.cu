@@ -876,16 +876,20 @@ std::string Engine::mixed_slots() {
     for (int s = 0; s < 2; ++s) {
         const SideGraph &g = model_.side[s];
         const int dv = std::max(1, g.dv_max), dc = g.dc_max, m = g.m, n = model_.n;
-        // variable -> c2v slot, k-major; check -> variable, i-major (both read coalesced)
-        std::vector<int> sl(static_cast<size_t>(n) * dv, -1), ck(static_cast<size_t>(m) * dc);
+        if (n > 65535 || static_cast<long long>(dc) * m > 65535)
+            return "codes above 65,535 variables or message slots per side are not available in the mixed launch";
+        // variable -> c2v slot, k-major; check -> variable, i-major (both 16-bit, read coalesced)
+        std::vector<uint16_t> sl(static_cast<size_t>(n) * dv, static_cast<uint16_t>(kMixNone)),
+            ck(static_cast<size_t>(m) * dc);
         for (int v = 0; v < n; ++v)
             for (int k = g.var_off[v]; k < g.var_off[v + 1]; ++k) {
                 const int e = g.var_edge[k], c = e / dc, pos = e - c * dc;
-                sl[static_cast<size_t>(k - g.var_off[v]) * n + v] = pos * m + c;
+                sl[static_cast<size_t>(k - g.var_off[v]) * n + v] = static_cast<uint16_t>(pos * m + c);
             }
         for (int c = 0; c < m; ++c)
-            for (int i = 0; i < dc; ++i) ck[static_cast<size_t>(i) * m + c] = g.chk_var[static_cast<size_t>(c) * dc + i];
-        int *p = nullptr, *q = nullptr;
+            for (int i = 0; i < dc; ++i)
+                ck[static_cast<size_t>(i) * m + c] = static_cast<uint16_t>(g.chk_var[static_cast<size_t>(c) * dc + i]);
+        uint16_t *p = nullptr, *q = nullptr;
         std::string e = dev_upload(code_allocs_, sl, &p);
         if (e.empty()) e = dev_upload(code_allocs_, ck, &q);
         if (!e.empty()) return e;

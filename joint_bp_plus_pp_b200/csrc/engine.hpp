@@ -119,8 +119,8 @@ private:
 
     int device_ = 0;
     int sm_count_ = 0;
-    const int *mix_slot_[2] = {nullptr, nullptr};   // [dv][n] message slot of each variable's edges
-    const int *mix_chk_[2] = {nullptr, nullptr};    // [dc][m] variable of each check's edges
+    const uint16_t *mix_slot_[2] = {nullptr, nullptr};   // [dv][n] message slot of each variable's edges
+    const uint16_t *mix_chk_[2] = {nullptr, nullptr};    // [dc][m] variable of each check's edges
     unsigned char *mix_scratch_ = nullptr;   // per-block c2v of the codes that do not fit shared memory
     size_t mix_scratch_bytes_ = 0;
     DevCounters *mix_cnt_ = nullptr;         // kMixMaxCodes counters + the work counter

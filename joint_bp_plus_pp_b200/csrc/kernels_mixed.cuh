@@ -11,9 +11,10 @@
 // the code's trial fits beside them (the launch's shared size is the largest such trial), and
 // otherwise in a per-block global scratch that stays in L2.  Neighbours come from tables built
 // on the host: the variable of edge i of check c, chk[i*m + c], and the c2v slot i*m + c of
-// edge k of variable v, slot[k*n + v] (-1 for the missing edges of lower-degree variables).
-// Both are index-major so that a warp's lanes, which take consecutive checks or variables,
-// read them coalesced; the check phase
+// edge k of variable v, slot[k*n + v] (kMixNone for the missing edges of lower-degree
+// variables), both 16-bit (codes up to 65,535 variables and message slots per side, so that
+// more of the tables stay in L1).  Both are index-major so that a warp's lanes, which take
+// consecutive checks or variables, read them coalesced; the check phase
 // reads its c2v row by row the same way, the variable phase gathers, with all of a variable's
 // slot loads issued before its message loads (variable degree at most kMixMaxDv).
 //
@@ -30,11 +31,12 @@ namespace jbp {
 constexpr int kMixThreads = 768;
 constexpr int kMixMaxCodes = 8;
 constexpr int kMixMaxDv = 4;
+constexpr unsigned kMixNone = 0xFFFFu;   // a missing edge in the 16-bit slot table
 
 struct MixCode {
     DevCode dc;                    // n, per-side m / dc / dv, basis rows (classification)
-    const int *chk[2];             // [DC][m] variable of edge i of check c
-    const int *slot[2];            // [dv][n] c2v slot (i*m + c) of each variable's edges, -1 pads
+    const uint16_t *chk[2];        // [DC][m] variable of edge i of check c
+    const uint16_t *slot[2];       // [dv][n] c2v slot (i*m + c) of each variable's edges, kMixNone pads
     unsigned long long seed;
     long long first_trial, ntrials;
     long long item_end;            // work items of codes 0..this one
@@ -73,7 +75,7 @@ __host__ __device__ inline size_t mix_c2v_bytes(int mx, int mz, int dc, size_t s
 // New c2v of check c of one side (its DC edges at c2v[i*m + c]); with `test`, also whether
 // the decisions in A's low bits fail the check.  The stable tanh rule of res_check_row.
 template <int DC, class ST>
-__device__ __forceinline__ bool mix_check_row(const int *__restrict__ chk, typename ST::T *c2v, int m,
+__device__ __forceinline__ bool mix_check_row(const uint16_t *__restrict__ chk, typename ST::T *c2v, int m,
                                               const float *A, int c, unsigned sbit, bool test) {
     // the row's variable indices, loaded together up front where the registers allow it
     constexpr bool kPre = DC <= 8;
@@ -96,7 +98,7 @@ __device__ __forceinline__ bool mix_check_row(const int *__restrict__ chk, typen
 // Syndrome test alone (the decisions in A's low bits against the target): failing checks of
 // this thread on one side.
 template <int DC>
-__device__ __forceinline__ int mix_test_side(const int *__restrict__ chk, int m, const float *A,
+__device__ __forceinline__ int mix_test_side(const uint16_t *__restrict__ chk, int m, const float *A,
                                              const unsigned *syn) {
     int bad = 0;
     for (int c = threadIdx.x; c < m; c += blockDim.x) {
@@ -111,20 +113,20 @@ __device__ __forceinline__ int mix_test_side(const int *__restrict__ chk, int m,
 // Variable v: sums of its X and Z c2v, hard decision, new totals (res_var_col without the
 // decision history).
 template <class ST>
-__device__ __forceinline__ void mix_var(const int *__restrict__ slot_x, int dvx, const int *__restrict__ slot_z,
+__device__ __forceinline__ void mix_var(const uint16_t *__restrict__ slot_x, int dvx, const uint16_t *__restrict__ slot_z,
                                         int dvz, const typename ST::T *c2v_x, const typename ST::T *c2v_z, float *A,
                                         int n, int v, const float4 lp, const float4 pr) {
-    int sx[kMixMaxDv], sz[kMixMaxDv];
+    unsigned sx[kMixMaxDv], sz[kMixMaxDv];
 #pragma unroll
     for (int k = 0; k < kMixMaxDv; ++k) {
-        sx[k] = k < dvx ? __ldg(slot_x + static_cast<size_t>(k) * n + v) : -1;
-        sz[k] = k < dvz ? __ldg(slot_z + static_cast<size_t>(k) * n + v) : -1;
+        sx[k] = k < dvx ? __ldg(slot_x + static_cast<size_t>(k) * n + v) : kMixNone;
+        sz[k] = k < dvz ? __ldg(slot_z + static_cast<size_t>(k) * n + v) : kMixNone;
     }
     float Lam = 0.0f, Mu = 0.0f;
 #pragma unroll
     for (int k = 0; k < kMixMaxDv; ++k) {
-        if (sx[k] >= 0) Lam += ST::ld(c2v_x + sx[k]);
-        if (sz[k] >= 0) Mu += ST::ld(c2v_z + sz[k]);
+        if (sx[k] != kMixNone) Lam += ST::ld(c2v_x + sx[k]);
+        if (sz[k] != kMixNone) Mu += ST::ld(c2v_z + sz[k]);
     }
     const float w0 = lp.x, w1 = lp.y - Lam, w2 = lp.z - Mu, w3 = lp.w - Lam - Mu;
     unsigned best = 0;
@@ -140,18 +142,19 @@ __device__ __forceinline__ void mix_var(const int *__restrict__ slot_x, int dvx,
 
 // Final LLRs of a trial from its c2v (res_write_llr with table neighbours; out of line).
 template <class ST>
-__device__ __noinline__ void mix_write_llr(const int *__restrict__ slot_x, int dvx, const int *__restrict__ slot_z,
+__device__ __noinline__ void mix_write_llr(const uint16_t *__restrict__ slot_x, int dvx,
+                                           const uint16_t *__restrict__ slot_z,
                                            int dvz, const typename ST::T *c2v_x, const typename ST::T *c2v_z, int n,
                                            const float4 lp, float *out) {
     for (int v = threadIdx.x; v < n; v += blockDim.x) {
         float Lam = 0.0f, Mu = 0.0f;
         for (int k = 0; k < dvx; ++k) {
-            const int s = __ldg(slot_x + static_cast<size_t>(k) * n + v);
-            if (s >= 0) Lam += ST::ld(c2v_x + s);
+            const unsigned s = __ldg(slot_x + static_cast<size_t>(k) * n + v);
+            if (s != kMixNone) Lam += ST::ld(c2v_x + s);
         }
         for (int k = 0; k < dvz; ++k) {
-            const int s = __ldg(slot_z + static_cast<size_t>(k) * n + v);
-            if (s >= 0) Mu += ST::ld(c2v_z + s);
+            const unsigned s = __ldg(slot_z + static_cast<size_t>(k) * n + v);
+            if (s != kMixNone) Mu += ST::ld(c2v_z + s);
         }
         const float w0 = lp.x, w1 = lp.y - Lam, w2 = lp.z - Mu, w3 = lp.w - Lam - Mu;
         out[2 * v] = (res_lse2(w1, w3) - res_lse2(w0, w2)) * 0.69314718f;
@@ -242,7 +245,8 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant_
         __syncthreads();
         for (int r = threadIdx.x; r < mx + mz; r += blockDim.x) {
             const int side = r >= mx, c = r - side * mx;
-            const int *ck = mc.chk[side], ms = side ? mz : mx;
+            const uint16_t *ck = mc.chk[side];
+            const int ms = side ? mz : mx;
             unsigned par = 0;
 #pragma unroll
             for (int i = 0; i < DC; ++i) par ^= err[__ldg(ck + static_cast<size_t>(i) * ms + c)];
