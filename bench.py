@@ -214,15 +214,19 @@ def run_reference(args, rank, world):
     for _ in range(args.warmup):
         cpu_reference_rate(args.p, args.max_iter, per_step / 4, not args.no_pp, args.flip_hist)
     vals = []
+    walls = []
     last = None
     for _ in range(args.steps):
+        t0 = time.perf_counter()
         last = cpu_reference_rate(args.p, args.max_iter, per_step, not args.no_pp, args.flip_hist)
+        walls.append((time.perf_counter() - t0) * 1e3)
         vals.append(last["value"])
     value = statistics.median(vals)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference mt19937_64 depolarizing noise)",
-            "impl": "reference",
+            "warmup": args.warmup, "ms_per_step": statistics.median(walls), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (reference mt19937_64 depolarizing noise)", "impl": "reference",
+            "step": "one bounded sample on every host core (the rate probe and the sample itself; wall time)",
             "config": {"workload": workload_name(args, "reference CPU decoder (FP64)"), "p": args.p,
                        "max_iter": args.max_iter, "enable_pp": not args.no_pp, "flip_hist": args.flip_hist},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": last["cores"], "kind": "reference",
