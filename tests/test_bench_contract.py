@@ -1,7 +1,8 @@
 """bench.py's host-side contract, on CPU: the reference arm's JSON line (the keys the
 reported comparison reads), its behaviour off rank 0 and without the reference binary, the
-parse of the reference CLI's run summary, and the clock record built from nvidia-smi samples
-(the throttle reasons that decide whether a timed run stands)."""
+parse of the reference CLI's run summary, the clock record built from nvidia-smi samples
+(the throttle reasons that decide whether a timed run stands), and the Wilson interval of the
+reported failure counts."""
 import json
 import sys
 import types
@@ -113,3 +114,22 @@ def test_clock_record_counts_only_the_timed_region():
 def test_clock_record_without_nvidia_smi():
     rec = bench.ClockSampler(0).stop()
     assert rec["sm_mhz"] is None and rec["reasons"] == ["nvidia-smi unavailable"]
+
+
+def test_package_wilson_interval_matches_reference_cli():
+    """The interval the bench reports beside its failure counts is the reference's Wilson
+    interval (jointbp_ets.cpp:4388-4399): equal, to the CLI's 8 printed decimals, on every
+    golden run summary; clipped to [0, 1]; none for no trials."""
+    from conftest import GOLDEN
+    from joint_bp_plus_pp_b200 import wilson_interval
+    cli = json.loads((GOLDEN / "cli_summaries.json").read_text())
+    assert cli
+    for name, c in cli.items():
+        s = c["summary"]
+        lo, hi = wilson_interval(int(s["trials"]), int(s["failures"]))
+        assert "[" + f"{lo:.8f},{hi:.8f}" + "]" == s["ci95"].replace(" ", ""), name
+    assert wilson_interval(0, 0) is None
+    lo, hi = wilson_interval(655360, 0)
+    assert lo == 0.0 and 5.8e-6 < hi < 5.9e-6
+    lo, hi = wilson_interval(40, 40)
+    assert hi == 1.0 and 0.9 < lo < 1.0
