@@ -163,15 +163,17 @@ int jbp_decode_errors_device(jbp_ctx *ctx, const jbp_options *opt, long long ntr
 
 /* Allocation-free decoding.  No counterpart in the reference: it is for callers that cannot
  * call cudaMalloc while they decode (device memory owned by another allocator, or decoding
- * loops that must not allocate after start-up).  Same decoding as jbp_decode_syndromes
- * (plain BP: enable_pp, freeze_syn and damping must be off), but d_sx (ntrials x mx),
+ * loops that must not allocate after start-up).  It runs the slot engine's kernels: its results
+ * equal jbp_decode_syndromes with engine JBP_ENGINE_SLOTS (engine must be AUTO or SLOTS; plain BP:
+ * enable_pp, freeze_syn, damping and learned_from must be off), but d_sx (ntrials x mx),
  * d_sz (ntrials x mz), d_est_out (ntrials x n, may be null) and d_res (ntrials) are device
  * memory, the work is ordered on `stream`, and all temporary state lives in a fixed device
  * array of JBP_NOALLOC_SCRATCH_BYTES that the library holds on every GPU that loads it until
  * the process exits; the call allocates nothing.  Requests that do not fit (about 32 trials
  * of the shipped code in FP64, 128 in FP32) are rejected with JBP_ERR_ARG.  The first call on
  * a device looks up the array's device address, so make it before any stream capture.  All
- * calls share the array: calls that overlap on the GPU race and must be serialized. */
+ * calls share the array: calls that overlap on the GPU race and must be serialized.  The
+ * options are checked before any CUDA call; the caller's current device is left unchanged. */
 #define JBP_NOALLOC_SCRATCH_BYTES (64u << 20)
 int jbp_decode_syndromes_noalloc(jbp_ctx *ctx, const jbp_options *opt, int ntrials, const uint8_t *d_sx,
                                  const uint8_t *d_sz, double p, uint8_t *d_est_out, jbp_trial_result *d_res,

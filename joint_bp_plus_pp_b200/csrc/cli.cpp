@@ -65,7 +65,7 @@ void usage(const char *prog) {
               << "  --slots N (trials in flight, 0 = auto)  --batch N (trials per GPU call, 262144)\n"
               << "  --ets-dir DIR (default: the params path without extension)\n"
               << "  --engine auto|resident|slots|table (auto)  --learned-from N (0 = off; learned flip proposal at\n"
-              << "  stalls from iteration N, FP16 resident engine)  --flip-model FILE.npy (default: the\n"
+              << "  stalls from iteration N, resident engine with FP32 or FP16 messages)  --flip-model FILE.npy (default: the\n"
               << "  shipped data/flip_mlp_params.npy next to the library)\n"
               << "  --checks FILE (a code as check lists instead of --params: 'n mx mz', then one line of\n"
               << "  variables per X check and per Z check)  --p-max P (per-trial p uniform in [p, P))\n"

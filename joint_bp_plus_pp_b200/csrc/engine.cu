@@ -528,21 +528,27 @@ int Engine::choose_slots(const jbp_options &opt, long long ntrials) const {
     return static_cast<int>(std::max<long long>(S, kGroup));
 }
 
-std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
-    std::memset(&stats, 0, sizeof(stats));
-    const jbp_options &o = rq.opt;
-    if (rq.ntrials <= 0) return "";
+std::string validate_options(const jbp_options &o, double p) {
     if (o.max_iter < 1) return "max_iter must be >= 1";
     if (o.precision < JBP_PREC_FP64 || o.precision > JBP_PREC_FP16) return "unknown precision";
     if (o.use_prior) {
         for (int i = 0; i < 4; ++i)
             if (!(o.prior[i] >= 0.0 && o.prior[i] <= 1.0)) return "prior entries must be in [0, 1]";
-    } else if (!(rq.p > 0.0 && rq.p < 1.0)) {
+    } else if (!(p > 0.0 && p < 1.0)) {
         return "p must be in (0, 1)";
     }
     if (o.damping < 0.0 || o.damping > 1.0) return "damping must be in [0, 1]";
-    if (o.p_max > rq.p && !(o.p_max < 1.0)) return "p_max must be below 1";
+    if (o.p_max > p && !(o.p_max < 1.0)) return "p_max must be below 1";
     if (o.engine < JBP_ENGINE_AUTO || o.engine > JBP_ENGINE_TABLE) return "unknown engine";
+    if (o.watchdog_ms < 0) return "watchdog_ms must be >= 0";
+    return "";
+}
+
+std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
+    std::memset(&stats, 0, sizeof(stats));
+    const jbp_options &o = rq.opt;
+    if (rq.ntrials <= 0) return "";
+    if (std::string bad = validate_options(o, rq.p); !bad.empty()) return bad;
     if (o.engine == JBP_ENGINE_TABLE) {
         if ((rq.source != kSrcPhilox && rq.source != kSrcErrors) || rq.collect)
             return "the table engine is not available for syndrome inputs or the mt19937 sampler "

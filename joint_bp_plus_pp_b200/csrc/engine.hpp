@@ -146,4 +146,8 @@ private:
 
 std::string cuda_err(cudaError_t e, const char *what);
 
+// The option checks every decoding entry point shares (error rate, prior, precision, damping,
+// engine, iteration and time limits): "" when the options are valid, else why not.
+std::string validate_options(const jbp_options &o, double p);
+
 }  // namespace jbp

@@ -17,7 +17,13 @@
 // device address is looked up once per device with cudaGetSymbolAddress (with that device
 // current) on the first call made on it, so that first call should come before any stream
 // capture.  The call itself launches kernels and small copies on the caller's stream and
-// waits on that stream; it calls no cudaMalloc, cudaFree or allocating library routine.
+// waits on that stream; it calls no cudaMalloc, cudaFree or allocating library routine, and
+// it leaves the caller's current device as it found it.
+//
+// It decodes on the slot engine's kernels (the FP64 bit-exact kernels, or the FP32 / FP16
+// LLR kernels), so its results equal jbp_decode_syndromes run with engine SLOTS; with engine
+// AUTO that call may pick the trial-resident kernels instead, whose FP16 / FP32 arithmetic
+// differs slightly.
 #include <cstring>
 #include <mutex>
 #include <sstream>
@@ -126,21 +132,41 @@ size_t layout(const jbp::DevCode &code, int S, int precision, unsigned char *bas
     return cv.off;
 }
 
+// Restores the caller's current device on every return path: embedding callers keep issuing
+// runtime calls on their own device after this call.
+struct DeviceGuard {
+    int saved = -1;
+    DeviceGuard() {
+        if (cudaGetDevice(&saved) != cudaSuccess) {
+            saved = -1;
+            cudaGetLastError();
+        }
+    }
+    ~DeviceGuard() {
+        if (saved >= 0) cudaSetDevice(saved);
+    }
+};
+
 }  // namespace
 
 extern "C" int jbp_decode_syndromes_noalloc(jbp_ctx *ctx, const jbp_options *opt, int ntrials, const uint8_t *d_sx,
                                             const uint8_t *d_sz, double p, uint8_t *d_est_out,
                                             jbp_trial_result *d_res, void *stream) {
     using namespace jbp;
-    if (!ctx || !opt || !d_sx || !d_sz || !d_res || ntrials < 0)
-        return set_last_error(JBP_ERR_ARG, "jbp_decode_syndromes_noalloc: invalid argument");
-    if (ntrials == 0) return JBP_OK;
-    if (opt->max_iter < 1) return set_last_error(JBP_ERR_ARG, "max_iter must be >= 1");
-    if (!opt->use_prior && !(p > 0.0 && p < 1.0)) return set_last_error(JBP_ERR_ARG, "p must be in (0, 1)");
-    if (opt->enable_pp || opt->freeze_syn || opt->damping > 0.0)
+    // options first (no CUDA call is needed to reject them), with the checks of every other entry point
+    if (!opt) return set_last_error(JBP_ERR_ARG, "jbp_decode_syndromes_noalloc: null options");
+    if (std::string bad = validate_options(*opt, p); !bad.empty())
+        return set_last_error(JBP_ERR_ARG, "jbp_decode_syndromes_noalloc: " + bad);
+    if (opt->engine != JBP_ENGINE_AUTO && opt->engine != JBP_ENGINE_SLOTS)
+        return set_last_error(JBP_ERR_UNSUPPORTED,
+                              "jbp_decode_syndromes_noalloc runs the slot engine only (engine AUTO or SLOTS)");
+    if (opt->enable_pp || opt->freeze_syn || opt->damping > 0.0 || opt->learned_from > 0)
         return set_last_error(JBP_ERR_UNSUPPORTED,
                               "jbp_decode_syndromes_noalloc decodes plain BP only (no post-processing, "
-                              "freeze-syn or damping)");
+                              "freeze-syn, damping or learned proposals)");
+    if (!ctx || !d_sx || !d_sz || !d_res || ntrials < 0)
+        return set_last_error(JBP_ERR_ARG, "jbp_decode_syndromes_noalloc: invalid argument");
+    if (ntrials == 0) return JBP_OK;
     const Engine &eng = ctx->engine;
     const DevCode &code = eng.dev_code();
     const auto &gx = eng.model().side[0], &gz = eng.model().side[1];
@@ -163,6 +189,11 @@ extern "C" int jbp_decode_syndromes_noalloc(jbp_ctx *ctx, const jbp_options *opt
            << (JBP_NOALLOC_SCRATCH_BYTES / per_group) * kGroup << " trials of this code at this precision)";
         return set_last_error(JBP_ERR_ARG, os.str());
     }
+    const int sm = eng.sm_count(), tpb = 256;
+    const int classify_tpb = 128;
+    const size_t classify_smem = static_cast<size_t>(classify_tpb / 32) * 2 * code.words * sizeof(uint64_t);
+    if (classify_smem > 48 * 1024) return set_last_error(JBP_ERR_UNSUPPORTED, "code too long for this entry point");
+    DeviceGuard guard;
     cudaError_t e = cudaSetDevice(eng.device());
     if (e != cudaSuccess) return set_last_error(JBP_ERR_CUDA, cuda_err(e, "cudaSetDevice"));
     unsigned char *base = nullptr;
@@ -186,43 +217,50 @@ extern "C" int jbp_decode_syndromes_noalloc(jbp_ctx *ctx, const jbp_options *opt
     r.hist = nullptr;
 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const int sm = eng.sm_count(), tpb = 256;
     const int big_grid = sm * 8;
     const int slot_blocks = (S / kGroup + 7) / 8;
     const int list_grid = (S + tpb - 1) / tpb;
-    const int classify_tpb = 128;
-    const size_t classify_smem = static_cast<size_t>(classify_tpb / 32) * 2 * code.words * sizeof(uint64_t);
-    if (classify_smem > 48 * 1024) return set_last_error(JBP_ERR_UNSUPPORTED, "code too long for this entry point");
+    auto fail_cuda = [](cudaError_t ce) {
+        return set_last_error(JBP_ERR_CUDA, cuda_err(ce, "jbp_decode_syndromes_noalloc"));
+    };
 
     // state that must start at zero: counters (the slot flags, lists and masks are
     // re-initialized by the first kernel)
-    cudaMemsetAsync(r.cnt, 0, sizeof(DevCounters), st);
+    e = cudaMemsetAsync(r.cnt, 0, sizeof(DevCounters), st);
+    if (e != cudaSuccess) return fail_cuda(e);
     k_init_slots<<<list_grid, tpb, 0, st>>>(r);
-    cudaMemsetAsync(r.n_fresh, 0, sizeof(int), st);
+    e = cudaMemsetAsync(r.n_fresh, 0, sizeof(int), st);
+    if (e != cudaSuccess) return fail_cuda(e);
     k_refill<<<list_grid, tpb, 0, st>>>(r, opt->precision);
     k_fresh_syndrome<<<sm * 4, tpb, 0, st>>>(code, r);
-    cudaMemsetAsync(r.n_groups, 0, sizeof(int), st);
+    e = cudaMemsetAsync(r.n_groups, 0, sizeof(int), st);
+    if (e != cudaSuccess) return fail_cuda(e);
     k_groups<<<slot_blocks, tpb, 0, st>>>(r);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda(e);
     unsigned long long done = 0;
     for (int it = 0; it < opt->max_iter && done < static_cast<unsigned long long>(ntrials); ++it) {
         check<<<big_grid, tpb, 0, st>>>(code, r, msg);
         if (opt->precision == JBP_PREC_FP64) var64<<<big_grid, tpb, 0, st>>>(code, r, msg, 0.0);
         else varllr<<<big_grid, tpb, 0, st>>>(code, r, msg, 0.0f);
         k_syndrome_check<<<big_grid, tpb, 0, st>>>(code, r);
-        cudaMemsetAsync(r.n_retired, 0, sizeof(int), st);
+        e = cudaMemsetAsync(r.n_retired, 0, sizeof(int), st);
+        if (e != cudaSuccess) return fail_cuda(e);
         k_retire<<<slot_blocks, tpb, 0, st>>>(r);
         k_classify<<<sm * 2, classify_tpb, classify_smem, st>>>(code, r);
-        cudaMemsetAsync(r.n_groups, 0, sizeof(int), st);
+        e = cudaMemsetAsync(r.n_groups, 0, sizeof(int), st);
+        if (e != cudaSuccess) return fail_cuda(e);
         k_groups<<<slot_blocks, tpb, 0, st>>>(r);
+        e = cudaGetLastError();   // launch errors of this iteration's kernels
+        if (e != cudaSuccess) return fail_cuda(e);
         if ((it & 7) == 7 || it + 1 == opt->max_iter) {
             e = cudaMemcpyAsync(&done, &r.cnt->done, sizeof(done), cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-            if (e != cudaSuccess) return set_last_error(JBP_ERR_CUDA, cuda_err(e, "jbp_decode_syndromes_noalloc"));
+            if (e != cudaSuccess) return fail_cuda(e);
         }
     }
-    e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return set_last_error(JBP_ERR_CUDA, cuda_err(e, "jbp_decode_syndromes_noalloc"));
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail_cuda(e);
     if (done != static_cast<unsigned long long>(ntrials))
         return set_last_error(JBP_ERR_CUDA, "jbp_decode_syndromes_noalloc: not every trial finished (internal error)");
     return JBP_OK;

@@ -103,3 +103,34 @@ def test_no_gpu_is_an_error_not_a_fallback():
     with pytest.raises(JbpError) as ei:
         Decoder.from_params()
     assert ei.value.code == 2
+
+
+def test_noalloc_entry_point_rejects_bad_options_before_any_cuda_call():
+    """jbp_decode_syndromes_noalloc checks its options with the same rules as the other entry
+    points before it touches a device: an unknown precision, an out-of-range prior entry or an
+    error rate outside (0, 1) is JBP_ERR_ARG, an engine other than AUTO or SLOTS (it runs the
+    slot engine's kernels only) is JBP_ERR_UNSUPPORTED, with no context needed to see it."""
+    from joint_bp_plus_pp_b200 import Options, load_library
+    lib = load_library()
+    f = lib.jbp_decode_syndromes_noalloc
+    f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+
+    def call(p=0.05, **kw):
+        co = Options(max_iter=10, enable_pp=False, **kw).to_c()
+        return f(None, ctypes.byref(co), 32, None, None, p, None, None, None)
+
+    co = Options(max_iter=10, enable_pp=False).to_c()
+    co.precision = 7
+    assert f(None, ctypes.byref(co), 32, None, None, 0.05, None, None, None) == 1
+    assert b"unknown precision" in lib.jbp_last_error()
+    co = Options(max_iter=10, enable_pp=False).to_c()
+    co.use_prior = 1
+    co.prior[:] = [0.9, 0.05, 1.5, 0.05]
+    assert f(None, ctypes.byref(co), 32, None, None, 0.05, None, None, None) == 1
+    assert b"prior" in lib.jbp_last_error()
+    assert call(p=1.5) == 1 and b"p must be" in lib.jbp_last_error()
+    assert call(engine="resident") == 4 and b"slot engine" in lib.jbp_last_error()
+    assert call(engine="table") == 4
+    # valid options and no context: an argument error, still before any CUDA call
+    assert call(precision="fp32", engine="slots") == 1 and b"invalid argument" in lib.jbp_last_error()

@@ -51,8 +51,12 @@ def run_noalloc(dec, opts, sx, sz, p):
 
 
 def check_same(dec, opts, err, p):
+    """The allocation-free call runs the slot engine's kernels, so the allocating call it is
+    compared with runs the slot engine too (engine AUTO could pick the trial-resident kernels
+    for FP16, whose arithmetic differs slightly)."""
+    from dataclasses import replace
     sx, sz = syndromes(dec, err)
-    _, exp_res, exp_est = dec.decode_syndromes(sx, sz, p, opts)
+    _, exp_res, exp_est = dec.decode_syndromes(sx, sz, p, replace(opts, engine="slots"))
     res, est = run_noalloc(dec, opts, sx, sz, p)
     assert (est == exp_est).all()
     for f in ("iterations", "syndrome_ok", "bp_ok", "success"):
@@ -67,6 +71,20 @@ def test_noalloc_matches_allocating_entry_point_twice(decoder):
     # second call: other trials and another precision, through the same scratch array
     err2 = sample_reference_errors(decoder.n, 77, 1, 40, 0.06)
     check_same(decoder, Options(precision="fp32", max_iter=40, enable_pp=False), err2, 0.06)
+    # third call: FP16 message storage (the slot engine's FP16 kernels)
+    err3 = sample_reference_errors(decoder.n, 78, 1, 48, 0.05)
+    check_same(decoder, Options(precision="fp16", max_iter=40, enable_pp=False), err3, 0.05)
+
+
+def test_noalloc_leaves_the_callers_device_current(decoder):
+    """The call selects the context's device for its own work and restores the caller's
+    current device before it returns."""
+    import torch
+    from joint_bp_plus_pp_b200 import Options, sample_reference_errors
+    before = torch.cuda.current_device()
+    err = sample_reference_errors(decoder.n, 79, 1, 8, 0.05)
+    check_same(decoder, Options(precision="fp32", max_iter=20, enable_pp=False), err, 0.05)
+    assert torch.cuda.current_device() == before
 
 
 def test_noalloc_rejects_requests_beyond_its_scratch(decoder):
@@ -76,9 +94,15 @@ def test_noalloc_rejects_requests_beyond_its_scratch(decoder):
     lib.jbp_decode_syndromes_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                                  ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
                                                  ctypes.c_void_p]
+    from joint_bp_plus_pp_b200 import TRIAL_DTYPE
     co = Options(precision="fp64", max_iter=10, enable_pp=False).to_c()
-    buf = torch.zeros(16, dtype=torch.uint8, device="cuda")
-    rc = lib.jbp_decode_syndromes_noalloc(decoder._h, ctypes.byref(co), 4096, buf.data_ptr(), buf.data_ptr(), 0.05,
-                                          None, buf.data_ptr(), None)
+    # buffers of the full size of the request, so that even a call that were not rejected
+    # would stay inside them
+    t = 4096
+    d_sx = torch.zeros((t, decoder.mx), dtype=torch.uint8, device="cuda")
+    d_sz = torch.zeros((t, decoder.mz), dtype=torch.uint8, device="cuda")
+    d_res = torch.zeros((t, TRIAL_DTYPE.itemsize), dtype=torch.uint8, device="cuda")
+    rc = lib.jbp_decode_syndromes_noalloc(decoder._h, ctypes.byref(co), t, d_sx.data_ptr(), d_sz.data_ptr(), 0.05,
+                                          None, d_res.data_ptr(), None)
     assert rc == 1
     assert b"scratch" in lib.jbp_last_error()
