@@ -60,6 +60,12 @@ def parse_args():
                     help="trials per code of the mixed-size one-launch run reported beside (0 = skip)")
     ap.add_argument("--learned-from", type=int, default=6,
                     help="stalled trials try the shipped learned flip proposal from this iteration (0 = off)")
+    ap.add_argument("--sweep-trials", type=int, default=131072,
+                    help="trials per p of the no-PP sweep p in {0.01, 0.025, 0.04}, FP32 resident against FP64 on "
+                         "the same trials (0 = skip)")
+    ap.add_argument("--ler-p", type=float, default=0.05, help="error rate of the failure-bearing LER comparison")
+    ap.add_argument("--ler-trials", type=int, default=131072,
+                    help="trials of the LER comparison: this decoder against FP64 BP+PP on the same trials (0 = skip)")
     a = ap.parse_args()
     if a.engine is None:
         a.engine = "slots" if a.precision == "fp64" else "resident"
@@ -234,6 +240,65 @@ def run_reference(args, rank, world):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+SWEEP_P = (0.01, 0.025, 0.04)
+
+
+def p_sweep_leg(dec, args, first_trial):
+    """Config 2 beside the headline: plain BP (--no-pp) at p in {0.01, 0.025, 0.04}, the FP32
+    trial-resident decoder against the FP64 bit-exact decoder on the same Philox trials (the
+    reference's own p matrix, job_full.sh).  Rates from the engines' CUDA-event device times."""
+    from joint_bp_plus_pp_b200 import Options, paired_ler_difference, wilson_interval
+    T = args.sweep_trials
+    out = []
+    for k, p in enumerate(SWEEP_P):
+        first = first_trial + k * T
+        o32 = Options(precision="fp32", engine="resident", max_iter=args.max_iter, enable_pp=False)
+        o64 = Options(precision="fp64", max_iter=args.max_iter, enable_pp=False)
+        # short warm-up runs (buffers, graphs) on other trials
+        dec.simulate(args.seed, 4096, p, o32, first_trial=3 * 10 ** 9, per_trial=False)
+        dec.simulate(args.seed, 4096, p, o64, first_trial=3 * 10 ** 9, per_trial=False)
+        s32, r32 = dec.simulate(args.seed, T, p, o32, first_trial=first)
+        s64, r64 = dec.simulate(args.seed, T, p, o64, first_trial=first)
+        f32, f64 = r32["success"] == 0, r64["success"] == 0
+        d, lo, hi, _, _ = paired_ler_difference(f32, f64)
+        v32 = s32["trials"] / (s32["device_ms"] / 1e3)
+        v64 = s64["trials"] / (s64["device_ms"] / 1e3)
+        out.append({"p": p, "trials": T, "fp32_resident_trials_per_s": v32, "fp64_trials_per_s": v64,
+                    "ratio": v32 / v64, "failures_fp32": int(f32.sum()), "failures_fp64": int(f64.sum()),
+                    "ci95_fp32": list(wilson_interval(T, int(f32.sum()))),
+                    "ci95_fp64": list(wilson_interval(T, int(f64.sum()))),
+                    "ler_difference": d, "ler_difference_ci95": [lo, hi],
+                    "outcome_disagreements": int((f32 != f64).sum()),
+                    "iteration_disagreements": int((r32["iterations"] != r64["iterations"]).sum()),
+                    "avg_iter_fp32": s32["total_iters"] / max(1, s32["trials"]),
+                    "avg_iter_fp64": s64["total_iters"] / max(1, s64["trials"])})
+    return out
+
+
+def ler_check_leg(dec, args, opts, first_trial):
+    """A failure-bearing LER comparison: this run's decoder (opts) against plain FP64 BP+PP on
+    the same Philox trials at an error rate where failures occur, with the reference's Wilson
+    intervals (jointbp_ets.cpp:4388-4399) and a paired interval on the LER difference."""
+    from joint_bp_plus_pp_b200 import Options, paired_ler_difference, wilson_interval
+    T, p = args.ler_trials, args.ler_p
+    o64 = Options(precision="fp64", max_iter=args.max_iter, enable_pp=True, flip_hist=args.flip_hist)
+    sa, ra = dec.simulate(args.seed, T, p, opts, first_trial=first_trial)
+    sb, rb = dec.simulate(args.seed, T, p, o64, first_trial=first_trial)
+    fa, fb = ra["success"] == 0, rb["success"] == 0
+    d, lo, hi, n10, n01 = paired_ler_difference(fa, fb)
+    return {"p": p, "trials": T, "max_iter": args.max_iter,
+            "this": {"trials_per_s": sa["trials"] / (sa["device_ms"] / 1e3), "failures": int(fa.sum()),
+                     "ci95": list(wilson_interval(T, int(fa.sum()))),
+                     "learned": {"attempts": sa["learned_attempts"], "saved": sa["learned_success"]},
+                     "pp_success": sa["pp_success"]},
+            "fp64_bp_pp": {"trials_per_s": sb["trials"] / (sb["device_ms"] / 1e3), "failures": int(fb.sum()),
+                           "ci95": list(wilson_interval(T, int(fb.sum()))), "pp_success": sb["pp_success"]},
+            "ler_difference": d, "ler_difference_ci95": [lo, hi],
+            "interval": "paired Wald interval over the discordant trials",
+            "fails_only_this": n10, "fails_only_fp64": n01,
+            "outcome_disagreements": int((fa != fb).sum())}
 
 
 def workload_name(args, decoder, learned_from=0):
@@ -475,6 +540,18 @@ def main():
                "d2h_bytes_per_step": E * 16, "path": "jbp_decode_errors (host errors, pinned) -> results to host",
                "steps": nsteps, "gpu_launches": e2e_launches}
 
+    # config 2's p sweep (no PP) and a failure-bearing LER comparison, both on trials no other
+    # leg decodes (rank 0)
+    p_sweep = ler_check = None
+    if rank == 0 and args.sweep_trials > 0:
+        t0 = time.perf_counter()
+        p_sweep = {"points": p_sweep_leg(dec, args, 4 * 10 ** 9), "wall_s": None}
+        p_sweep["wall_s"] = round(time.perf_counter() - t0, 2)
+    if rank == 0 and args.ler_trials > 0:
+        t0 = time.perf_counter()
+        ler_check = ler_check_leg(dec, args, opts, 5 * 10 ** 9)
+        ler_check["wall_s"] = round(time.perf_counter() - t0, 2)
+
     cpu = None
     if rank == 0 and world == 1 and args.cpu_seconds > 0:
         cpu = cpu_reference_rate(args.p, args.max_iter, args.cpu_seconds, pp, args.flip_hist)
@@ -513,6 +590,8 @@ def main():
         "fp64": fp64,
         "precision": precision,
         "mixed_sizes_one_launch": mixed,
+        "p_sweep": p_sweep,
+        "ler_check": ler_check,
         "clocks": clk,
         "step_ms": {"host_wall": step_wall, "kernel": step_kernel},
         "e2e": e2e,

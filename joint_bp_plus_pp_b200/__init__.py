@@ -416,6 +416,22 @@ def load_flip_model(path=FLIP_MODEL_PATH):
     return np.load(p).astype(np.float32) if p.exists() else None
 
 
+def paired_ler_difference(fail_a, fail_b, z=1.96):
+    """LER(a) - LER(b) on the same trials with its 95% interval (paired Wald interval from the
+    discordant trials: d = (n10 - n01) / n, var = (n10 + n01 - (n10 - n01)^2 / n) / n^2).
+    fail_a, fail_b: boolean arrays of per-trial failures.  Returns (d, lo, hi, n10, n01)."""
+    a = np.asarray(fail_a, bool)
+    b = np.asarray(fail_b, bool)
+    n = a.size
+    if n == 0 or b.size != n:
+        raise ValueError("two failure arrays of the same nonzero length")
+    n10 = int((a & ~b).sum())
+    n01 = int((~a & b).sum())
+    d = (n10 - n01) / n
+    half = z * max(0.0, n10 + n01 - (n10 - n01) ** 2 / n) ** 0.5 / n
+    return d, d - half, d + half, n10, n01
+
+
 def wilson_interval(n, k, z=1.96):
     """Wilson score interval (jointbp_ets.cpp:4388-4399)."""
     if n <= 0:

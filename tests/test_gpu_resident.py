@@ -101,6 +101,31 @@ def test_resident_explicit_prior_equals_p(decoder):
     assert (e1 == e2).all() and (r1["iterations"] == r2["iterations"]).all()
 
 
+@pytest.mark.parametrize("p", [0.01, 0.025])
+def test_resident_fp32_against_fp64_at_low_p(decoder, p):
+    """Config 2's lower error rates (the reference's p matrix 0.01 / 0.025 / 0.04, plain BP,
+    max-iter 1000): the FP32 trial-resident decoder against the FP64 bit-exact decoder on the
+    same 16,384 trials.  Bars: the same outcome on every trial, the same estimate on >= 99.9%
+    and the same iteration count on >= 99% of them (the LLR arithmetic may move a convergence
+    by an iteration)."""
+    from joint_bp_plus_pp_b200 import Options
+    k = 16384
+    err = decoder.sample_errors(106, 1, k, p, sampler="philox")
+    o32 = Options(precision="fp32", engine="resident", max_iter=1000, enable_pp=False)
+    o64 = Options(precision="fp64", max_iter=1000, enable_pp=False)
+    s32, r32, e32 = decoder.decode_errors(err, p, o32)
+    s64, r64, e64 = decoder.decode_errors(err, p, o64)
+    assert s32["kernel_launches"] == 1 and s32["trials"] == s64["trials"] == k
+    assert (r32["success"] == r64["success"]).all()
+    assert (r32["syndrome_ok"] == r64["syndrome_ok"]).all()
+    same_est = int((e32 == e64).all(axis=1).sum())
+    assert same_est >= 0.999 * k, same_est
+    assert int((r32["iterations"] == r64["iterations"]).sum()) >= 0.99 * k
+    # the same trials through the device sampler: the resident decoder's outcomes are the same
+    _, rs = decoder.simulate(106, k, p, o32, first_trial=1)
+    assert (rs["success"] == r32["success"]).all() and (rs["iterations"] == r32["iterations"]).all()
+
+
 def test_resident_refuses_what_it_does_not_run(decoder):
     from joint_bp_plus_pp_b200 import JbpError
     for bad in (dict(damping=0.2), dict(freeze_syn=True), dict(precision="fp64")):
