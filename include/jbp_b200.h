@@ -64,7 +64,12 @@ typedef struct {
     int check_interval;    /* --cuda-check-interval (default 1, clamped >= 1) */
     int slots;             /* trials in flight; 0 = automatic */
     int iters_per_launch;  /* BP iterations per CUDA-graph launch; 0 = automatic */
-    int watchdog_ms;       /* abort a run after this much wall time (0 = none) */
+    int watchdog_ms;       /* run budget (0 = none): a run that takes longer stops early with
+                              JBP_ERR_TIMEOUT and its stats hold the trials finished within it.
+                              Persistent kernels (resident, table, mixed) check the GPU's global
+                              timer between trials and every 16 BP iterations of a trial, and
+                              abandon unfinished trials; the slot engine checks on the host
+                              between CUDA-graph launches */
     int profile;           /* time the check and variable kernels with CUDA events (jbp_stats) */
     int use_prior;         /* 1: decode with `prior` below instead of normalize(1-p, p/3, p/3, p/3) */
     double prior[4];       /* probabilities of I, X, Z, Y (used as given, as cuda_bp_decode does) */
@@ -108,6 +113,9 @@ typedef struct {
     long long slots;           /* trials in flight used by the run */
     long long learned_attempts;/* learned flip proposals evaluated */
     long long learned_success; /* trials whose accepted learned proposal was a success */
+    double test_ms;            /* with profile (slot engine): device time of all syndrome-test kernel launches */
+    long long syndrome_tests;  /* slot engine: per-trial syndrome tests run (the resident and table kernels
+                                  fuse the test into the next check phase and do not count it) */
 } jbp_stats;
 
 void jbp_default_options(jbp_options *opt);

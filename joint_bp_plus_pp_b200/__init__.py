@@ -28,9 +28,13 @@ ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "I/O error", 4: "unsupporte
 
 
 class JbpError(RuntimeError):
-    def __init__(self, code, msg):
+    """A failed call: `code` is the JBP_ERR_* status; for JBP_ERR_TIMEOUT (5), `stats` holds the
+    counters of the trials that finished within the run budget (None otherwise)."""
+
+    def __init__(self, code, msg, stats=None):
         super().__init__(f"jbp error {code} ({ERRORS.get(code, '?')}): {msg}")
         self.code = code
+        self.stats = stats
 
 
 class COptions(ctypes.Structure):
@@ -63,7 +67,9 @@ class CStats(ctypes.Structure):
                                                                 ("profiled_iterations", ctypes.c_longlong),
                                                                 ("slots", ctypes.c_longlong),
                                                                 ("learned_attempts", ctypes.c_longlong),
-                                                                ("learned_success", ctypes.c_longlong)]
+                                                                ("learned_success", ctypes.c_longlong),
+                                                                ("test_ms", ctypes.c_double),
+                                                                ("syndrome_tests", ctypes.c_longlong)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -148,9 +154,10 @@ def load_library(path=None):
     return lib
 
 
-def _check(lib, rc):
+def _check(lib, rc, stats=None):
     if rc != 0:
-        raise JbpError(rc, lib.jbp_last_error().decode(errors="replace"))
+        raise JbpError(rc, lib.jbp_last_error().decode(errors="replace"),
+                       stats.as_dict() if (rc == 5 and stats is not None) else None)
 
 
 def _ptr(a):
@@ -221,7 +228,7 @@ class Decoder:
         h = np.zeros(opts.max_iter + 1, np.int64) if hist else None
         co = opts.to_c()
         _check(self._lib, self._lib.jbp_simulate(self._h, ctypes.byref(co), seed, first_trial, ntrials, p,
-                                                 SAMPLER[sampler], ctypes.byref(st), _ptr(res), _ptr(h)))
+                                                 SAMPLER[sampler], ctypes.byref(st), _ptr(res), _ptr(h)), st)
         out = st.as_dict()
         if hist:
             out["hist"] = h
@@ -243,7 +250,7 @@ class Decoder:
         st = CStats()
         co = opts.to_c()
         _check(self._lib, self._lib.jbp_decode_errors(self._h, ctypes.byref(co), t, _ptr(err), p, _ptr(est),
-                                                      _ptr(res), ctypes.byref(st)))
+                                                      _ptr(res), ctypes.byref(st)), st)
         return st.as_dict(), res, est
 
     def autotune(self, p, opts=None, probe_trials=16384):
@@ -284,7 +291,7 @@ class Decoder:
         st = CStats()
         co = opts.to_c()
         _check(self._lib, self._lib.jbp_decode_syndromes(self._h, ctypes.byref(co), t, _ptr(sx), _ptr(sz), p,
-                                                         _ptr(est), _ptr(res), ctypes.byref(st)))
+                                                         _ptr(est), _ptr(res), ctypes.byref(st)), st)
         return st.as_dict(), res, est
 
     def decode_errors_device(self, d_err_ptr, ntrials, p, d_est_ptr, d_res_ptr, opts=None, stream=0):

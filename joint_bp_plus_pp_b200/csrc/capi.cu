@@ -194,7 +194,11 @@ int jbp_simulate(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed, long long 
     }
     jbp_stats st;
     std::string e = ctx->engine.run(rq, st);
-    if (!e.empty()) return engine_fail(e);
+    if (!e.empty()) {
+        const int rc = engine_fail(e);
+        if (rc == JBP_ERR_TIMEOUT && stats) *stats = st;   // the trials finished within the budget
+        return rc;
+    }
     if (per_trial && ntrials > 0) {
         cudaError_t ce = cudaMemcpy(per_trial, ctx->d_res, sizeof(jbp_trial_result) * ntrials, cudaMemcpyDeviceToHost);
         if (ce != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(ce, "copy results"));
@@ -234,7 +238,12 @@ int jbp_simulate_mixed(jbp_ctx *const *ctxs, int nctx, const jbp_options *opt, c
             }
     std::vector<jbp_stats> st;
     std::string e = jbp::Engine::run_mixed(rq, st);
-    if (!e.empty()) return engine_fail(e);
+    if (!e.empty()) {
+        const int rc = engine_fail(e);
+        if (rc == JBP_ERR_TIMEOUT)
+            for (int i = 0; i < nctx && i < static_cast<int>(st.size()); ++i) stats[i] = st[i];
+        return rc;
+    }
     for (int i = 0; i < nctx; ++i) {
         if (rq.d_res[i]) {
             cudaError_t ce = cudaMemcpy(per_trial[i], rq.d_res[i], sizeof(jbp_trial_result) * ntrials[i],
@@ -244,6 +253,24 @@ int jbp_simulate_mixed(jbp_ctx *const *ctxs, int nctx, const jbp_options *opt, c
         stats[i] = st[i];
     }
     return JBP_OK;
+}
+
+// Adds the counters and times of one engine run to a running total.
+static void add_stats(jbp_stats &total, const jbp_stats &st) {
+    long long *a = &total.trials;
+    const long long *b = &st.trials;
+    for (int i = 0; i < 15; ++i) a[i] += b[i];
+    total.device_ms += st.device_ms;
+    total.kernel_launches += st.kernel_launches;
+    total.bp_trial_iterations += st.bp_trial_iterations;
+    total.check_ms += st.check_ms;
+    total.var_ms += st.var_ms;
+    total.profiled_iterations += st.profiled_iterations;
+    total.slots = std::max(total.slots, st.slots);
+    total.learned_attempts += st.learned_attempts;
+    total.learned_success += st.learned_success;
+    total.test_ms += st.test_ms;
+    total.syndrome_tests += st.syndrome_tests;
 }
 
 static int decode_host(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *err, const uint8_t *sx,
@@ -320,25 +347,21 @@ static int decode_host(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, 
         }
         jbp_stats st;
         std::string e = ctx->engine.run(rq, st);
-        if (!e.empty()) return engine_fail(e);
+        if (!e.empty()) {
+            const int rc = engine_fail(e);
+            if (rc == JBP_ERR_TIMEOUT && stats) {
+                add_stats(total, st);
+                *stats = total;   // the trials finished within the budget
+            }
+            return rc;
+        }
         ce = cudaMemcpy(res + base, ctx->d_res, sizeof(jbp_trial_result) * cnt, cudaMemcpyDeviceToHost);
         if (ce == cudaSuccess && est_out)
             ce = cudaMemcpy(est_out + base * n, ctx->d_est, static_cast<size_t>(cnt * n), cudaMemcpyDeviceToHost);
         if (ce == cudaSuccess && llr_out)
             ce = cudaMemcpy(llr_out + base * n * 2, ctx->d_llr, sizeof(float) * cnt * n * 2, cudaMemcpyDeviceToHost);
         if (ce != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(ce, "copy results"));
-        long long *a = &total.trials;
-        const long long *b = &st.trials;
-        for (int i = 0; i < 15; ++i) a[i] += b[i];
-        total.device_ms += st.device_ms;
-        total.kernel_launches += st.kernel_launches;
-        total.bp_trial_iterations += st.bp_trial_iterations;
-        total.check_ms += st.check_ms;
-        total.var_ms += st.var_ms;
-        total.profiled_iterations += st.profiled_iterations;
-        total.slots = std::max(total.slots, st.slots);
-        total.learned_attempts += st.learned_attempts;
-        total.learned_success += st.learned_success;
+        add_stats(total, st);
     }
     if (stats) *stats = total;
     return JBP_OK;
@@ -430,7 +453,11 @@ int jbp_decode_errors_device(jbp_ctx *ctx, const jbp_options *opt, long long ntr
     cudaSetDevice(ctx->engine.device());
     jbp_stats st;
     std::string e = ctx->engine.run(rq, st);
-    if (!e.empty()) return engine_fail(e);
+    if (!e.empty()) {
+        const int rc = engine_fail(e);
+        if (rc == JBP_ERR_TIMEOUT && stats) *stats = st;
+        return rc;
+    }
     if (stats) *stats = st;
     return JBP_OK;
 }

@@ -262,6 +262,8 @@ jbp_options options(const Args &a) {
     o.engine = a.engine;
     o.learned_from = a.learned_from;
     o.p_max = a.p_max;
+    // --iter-hist-out reports measured per-phase costs: time the slot engine's kernels
+    if (!a.hist_out.empty()) o.profile = 1;
     return o;
 }
 
@@ -332,6 +334,47 @@ void add_stats(jbp_stats &acc, const jbp_stats &s) {
     acc.exact += s.exact;
     acc.total_iters += s.total_iters;
     acc.device_ms += s.device_ms;
+    acc.kernel_launches += s.kernel_launches;
+    acc.bp_trial_iterations += s.bp_trial_iterations;
+    acc.check_ms += s.check_ms;
+    acc.var_ms += s.var_ms;
+    acc.profiled_iterations += s.profiled_iterations;
+    acc.learned_attempts += s.learned_attempts;
+    acc.learned_success += s.learned_success;
+    acc.test_ms += s.test_ms;
+    acc.syndrome_tests += s.syndrome_tests;
+}
+
+// --iter-hist-out (write_hist_out, jointbp_ets.cpp:4623-4643): "# costs <iter_cost_ms>
+// <check_cost_ms>", then "iterations fraction" lines.  The reference's costs are the CUDA path's
+// BP kernel time per iteration and syndrome-check time per check, and are always 0 there
+// (cuda_costs is never set, jointbp_ets.cpp:4866).  Here they are measured with CUDA events:
+// on the slot engine, the check- and variable-node kernels' device time per trial-iteration and
+// the syndrome-test kernel's device time per trial test, amortized over the batch; on the
+// trial-resident and table kernels, whose phases run inside one launch, the whole kernel's
+// device time per trial-iteration, with no separate syndrome-test cost (the test rides in the
+// next check phase).  A third comment line says which; '#' lines are skipped by readers of the
+// format (visualize_costs.py).
+bool write_hist_out(const std::string &path, const std::vector<long long> &hist, long long total, const jbp_stats &s) {
+    if (path.empty() || total <= 0 || hist.size() <= 1) return true;
+    std::ofstream h(path);
+    if (!h) return false;
+    const bool slots = s.check_ms + s.var_ms > 0.0;
+    const double ti = static_cast<double>(std::max(1LL, s.bp_trial_iterations));
+    const double iter_cost = slots ? (s.check_ms + s.var_ms) / ti : s.device_ms / ti;
+    const double check_cost = slots && s.syndrome_tests > 0 ? s.test_ms / static_cast<double>(s.syndrome_tests) : 0.0;
+    h << "# costs " << std::fixed << std::setprecision(8) << iter_cost << " " << std::setprecision(8) << check_cost
+      << "\n";
+    if (slots)
+        h << "# cost_source slots: check + variable node kernels, device ms per trial-iteration; syndrome-test "
+             "kernel, device ms per trial test (CUDA events, amortized over the batch)\n";
+    else
+        h << "# cost_source resident: whole kernel, device ms per trial-iteration (sampling, BP, post-processing, "
+             "classification); the syndrome test rides in the check phase and has no separate cost\n";
+    h << "# iter fraction\n";
+    for (size_t i = 1; i < hist.size(); ++i)
+        if (hist[i]) h << i << " " << std::setprecision(10) << static_cast<double>(hist[i]) / total << "\n";
+    return true;
 }
 
 void print_section(const char *name) { std::cout << "== " << name << " ==\n"; }
@@ -412,11 +455,36 @@ int decode_single(jbp_ctx *ctx, const Args &a, int n, int mx, int mz) {
         std::cout << "Saved estimate: " << a.est_path << "\n";
     }
     if (!a.hist_out.empty() && a.max_iter >= 1 && r.iterations >= 1 && r.iterations <= a.max_iter) {
-        std::ofstream h(a.hist_out);
-        h << "# costs " << std::fixed << std::setprecision(8) << 0.0 << " " << 0.0 << "\n# iter fraction\n";
-        h << r.iterations << " " << std::setprecision(10) << 1.0 << "\n";
+        std::vector<long long> h1(static_cast<size_t>(a.max_iter) + 1, 0);
+        h1[r.iterations] = 1;
+        if (!write_hist_out(a.hist_out, h1, 1, st)) std::cerr << "Failed to write histogram output: " << a.hist_out << "\n";
     }
     return success ? 0 : 2;
+}
+
+// --progress-tsv (write_progress_tsv, jointbp_ets.cpp:5085-5122): the file holds the latest
+// progress line only (rewritten each time), tab-separated: epoch seconds, trials, failures,
+// pp_success, ETS saves, flip saves, stab_success, avg_iter, iterations, FER, trials/s, and the
+// "PROGRESS | ..." text of format_progress_line (jointbp_ets.cpp:4575-4602).  Written after
+// every GPU batch.
+bool write_progress_tsv(const std::string &path, const jbp_stats &s, double elapsed) {
+    if (s.trials <= 0) return true;
+    std::ofstream out(path, std::ios::trunc);
+    if (!out) return false;
+    const double fer = static_cast<double>(s.failures) / static_cast<double>(s.trials);
+    const double fps = elapsed > 0.0 ? static_cast<double>(s.trials) / elapsed : 0.0;
+    const double avg = static_cast<double>(s.total_iters) / static_cast<double>(s.trials);
+    std::ostringstream line;
+    line << "PROGRESS | trials=" << s.trials << " | failures=" << s.failures << " | pp_success=" << s.pp_success
+         << " | ets_success=" << s.ets_saved << " | flip_success=" << s.flip_pp_success
+         << " | stab_success=" << s.stab_success << " | avg_iter=" << std::setprecision(2) << std::fixed << avg
+         << " | iters=" << s.total_iters << " | FER=" << std::setprecision(6) << fer
+         << " | trials/sec=" << std::setprecision(2) << fps;
+    out << static_cast<long long>(std::time(nullptr)) << "\t" << s.trials << "\t" << s.failures << "\t"
+        << s.pp_success << "\t" << s.ets_saved << "\t" << s.flip_pp_success << "\t" << s.stab_success << "\t"
+        << std::setprecision(2) << std::fixed << avg << "\t" << s.total_iters << "\t" << std::setprecision(6) << fer
+        << "\t" << std::setprecision(2) << fps << "\t" << line.str() << "\n";
+    return static_cast<bool>(out);
 }
 
 void progress_line(std::ostream &os, const jbp_stats &s, double elapsed) {
@@ -454,8 +522,6 @@ int simulate(jbp_ctx *ctx, const Args &a, int n) {
     const long long first = a.trial_index >= 0 ? a.trial_index : 1;
     std::vector<long long> hist(static_cast<size_t>(a.max_iter) + 1, 0), chunk_hist(hist.size());
     std::vector<jbp_trial_result> per;
-    std::ofstream tsv;
-    if (!a.progress_tsv.empty()) tsv.open(a.progress_tsv);
     jbp_stats acc{};
     const auto t0 = std::chrono::steady_clock::now();
     long long done = 0, next_report = a.report_every > 0 ? a.report_every : -1;
@@ -493,13 +559,9 @@ int simulate(jbp_ctx *ctx, const Args &a, int n) {
             progress_line(std::cout, acc, el);
             while (next_report <= done) next_report += a.report_every;
         }
-        if (tsv) {
-            const double fer = static_cast<double>(acc.failures) / acc.trials;
-            tsv << static_cast<long long>(std::time(nullptr)) << "\t" << acc.trials << "\t" << acc.failures << "\t"
-                << acc.pp_success << "\t" << acc.ets_saved << "\t" << acc.flip_pp_success << "\t" << acc.stab_success
-                << "\t" << std::fixed << std::setprecision(2) << static_cast<double>(acc.total_iters) / acc.trials
-                << "\t" << acc.total_iters << "\t" << std::setprecision(6) << fer << "\t" << std::setprecision(2)
-                << (el > 0 ? acc.trials / el : 0.0) << "\tbatch\n";
+        if (!a.progress_tsv.empty() && !write_progress_tsv(a.progress_tsv, acc, el)) {
+            std::cerr << "Failed to write progress TSV: " << a.progress_tsv << "\n";
+            return 1;
         }
     }
     const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -540,16 +602,8 @@ int simulate(jbp_ctx *ctx, const Args &a, int n) {
               << " sampler=" << (a.sampler == JBP_SAMPLER_MT19937 ? "mt19937" : "philox") << " device_ms="
               << std::setprecision(2) << acc.device_ms << " trials_per_s=" << (elapsed > 0 ? d / elapsed : 0.0)
               << "\n";
-    if (!a.hist_out.empty() && d > 0 && hist.size() > 1) {
-        std::ofstream h(a.hist_out);
-        if (!h) {
-            std::cerr << "Failed to write histogram output: " << a.hist_out << "\n";
-        } else {
-            h << "# costs " << std::fixed << std::setprecision(8) << 0.0 << " " << 0.0 << "\n# iter fraction\n";
-            for (size_t i = 1; i < hist.size(); ++i)
-                if (hist[i]) h << i << " " << std::setprecision(10) << static_cast<double>(hist[i]) / d << "\n";
-        }
-    }
+    if (!a.hist_out.empty() && d > 0 && !write_hist_out(a.hist_out, hist, d, acc))
+        std::cerr << "Failed to write histogram output: " << a.hist_out << "\n";
     return 0;
 }
 

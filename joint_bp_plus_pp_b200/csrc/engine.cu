@@ -10,6 +10,7 @@
 #include "kernels_bp.cuh"
 #include "kernels_slots.cuh"
 #include "kernels_pp.cuh"
+#include "kernels_slot_pp.cuh"
 #include "kernels_resident.cuh"
 #include "kernels_mixed.cuh"
 #include "mlp.cuh"
@@ -109,6 +110,7 @@ void fill_stats(const DevCounters &hc, jbp_stats &stats) {
     stats.bp_trial_iterations = static_cast<long long>(hc.bp_trial_iterations);
     stats.learned_attempts = static_cast<long long>(hc.learned_attempts);
     stats.learned_success = static_cast<long long>(hc.learned_success);
+    stats.syndrome_tests = static_cast<long long>(hc.syndrome_tests);
 }
 
 }  // namespace
@@ -376,6 +378,7 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     r.col_y = rq.d_col_y;
     r.col_count = rq.d_col_count;
     r.col_cap = rq.col_cap;
+    r.budget_ns = o.watchdog_ms > 0 ? static_cast<unsigned long long>(o.watchdog_ms) * 1000000ull : 0ull;
     cudaStream_t st = rq.stream;
     cudaEvent_t ev0, ev1;
     JBP_CUDA_TRY(cudaEventCreate(&ev0), "cudaEventCreate");
@@ -397,11 +400,14 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     cudaEventDestroy(ev1);
     if (ce != cudaSuccess) return cuda_err(ce, "resident run");
     if (hc.bad_input) return "error vector has invalid value";
-    if (hc.done != static_cast<unsigned long long>(rq.ntrials)) return "resident run finished an unexpected number of trials";
     fill_stats(hc, stats);
     stats.device_ms = ms;
     stats.kernel_launches = 1;
     stats.slots = grid;
+    if (hc.watchdog)
+        return "watchdog expired: the run budget of " + std::to_string(o.watchdog_ms) + " ms ran out on the device after " +
+               std::to_string(hc.done) + " of " + std::to_string(rq.ntrials) + " trials";
+    if (hc.done != static_cast<unsigned long long>(rq.ntrials)) return "resident run finished an unexpected number of trials";
     return "";
 }
 
@@ -413,7 +419,7 @@ void Engine::free_buffers() {
     cudaFree(buf_.res_iters); cudaFree(buf_.res_flags); cudaFree(buf_.lists); cudaFree(buf_.counts);
     cudaFree(buf_.cnt);
     cudaFree(buf_.it);
-    cudaFree(buf_.llr); cudaFree(buf_.act_k); cudaFree(buf_.pstate); cudaFree(buf_.stall_same);
+    cudaFree(buf_.act_k); cudaFree(buf_.pstate); cudaFree(buf_.stall_same);
     cudaFree(buf_.pp_list); cudaFree(buf_.pp_mode); cudaFree(buf_.us_hist); cudaFree(buf_.dprev);
     cudaFree(buf_.dpprev); cudaFree(buf_.pp_scratch);
     if (buf_.h_done) cudaFreeHost(buf_.h_done);
@@ -485,7 +491,6 @@ std::string Engine::ensure_buffers(int S, int precision, bool damp, bool pp, int
     JBP_CUDA_TRY(cudaMalloc(&buf_.it, sizeof(int)), "cudaMalloc(it)");
     if (pp) {
         const int mmax = std::max(model_.side[0].m, model_.side[1].m);
-        JBP_CUDA_TRY(cudaMalloc(&buf_.llr, sizeof(double) * 2 * S * n), "cudaMalloc(llr)");
         JBP_CUDA_TRY(cudaMalloc(&buf_.act_k, sizeof(int) * S), "cudaMalloc(pp)");
         JBP_CUDA_TRY(cudaMalloc(&buf_.pstate, sizeof(int) * S), "cudaMalloc(pp)");
         JBP_CUDA_TRY(cudaMalloc(&buf_.stall_same, sizeof(int) * S), "cudaMalloc(pp)");
@@ -496,7 +501,7 @@ std::string Engine::ensure_buffers(int S, int precision, bool damp, bool pp, int
         JBP_CUDA_TRY(cudaMalloc(&buf_.dpprev, sizeof(unsigned) * G), "cudaMalloc(pp)");
         JBP_CUDA_TRY(cudaMemsetAsync(buf_.dprev, 0, sizeof(unsigned) * G, st), "memset(pp)");
         JBP_CUDA_TRY(cudaMemsetAsync(buf_.dpprev, 0, sizeof(unsigned) * G, st), "memset(pp)");
-        buf_.pp_stride = pp_scratch_bytes(n, mmax);
+        buf_.pp_stride = slot_pp_scratch_bytes(n, mmax);
         buf_.pp_blocks = std::min(sm_count_, static_cast<int>(S));
         JBP_CUDA_TRY(cudaMalloc(&buf_.pp_scratch, buf_.pp_stride * buf_.pp_blocks), "cudaMalloc(pp scratch)");
     }
@@ -568,9 +573,8 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
         mr.stream = rq.stream;
         std::vector<jbp_stats> st;
         std::string e = run_mixed(mr, st);
-        if (!e.empty()) return e;
-        stats = st[0];
-        return "";
+        if (!st.empty()) stats = st[0];   // also on a run-budget stop: the trials that finished
+        return e;
     }
     if (o.engine != JBP_ENGINE_SLOTS) {
         std::string why;
@@ -657,7 +661,6 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     r.flip_hist = H;
     r.llr_from = std::min(100, o.max_iter);
     if (pp) {
-        r.llr = buf_.llr;
         r.act_k = buf_.act_k;
         r.pstate = buf_.pstate;
         r.stall_same = buf_.stall_same;
@@ -720,13 +723,15 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
             k_stall_compare<<<big_grid, tpb, 0, s>>>(dcode_, r);
             launches += 1;
         }
+        if (e3) cudaEventRecordWithFlags(e3[3], s, cudaEventRecordExternal);
         k_syndrome_check<<<big_grid, tpb, 0, s>>>(dcode_, r);
+        if (e3) cudaEventRecordWithFlags(e3[4], s, cudaEventRecordExternal);
         cudaMemsetAsync(r.n_retired, 0, sizeof(int), s);
         if (pp) cudaMemsetAsync(r.n_pp, 0, sizeof(int), s);
         k_retire<<<slot_blocks, tpb, 0, s>>>(r);
         if (pp) {
             k_postprocess<<<buf_.pp_blocks, kPpThreads,
-                            pp_smem_bytes(n, M, std::max(gx.m, gz.m)), s>>>(dcode_, r);
+                            pp_smem_bytes(n, M, std::max(gx.m, gz.m)), s>>>(dcode_, r, msg, o.precision);
             launches += 1;
         }
         if (rq.d_llr_out) {
@@ -755,7 +760,10 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     GI = std::min(GI, o.max_iter);
     const bool prof = o.profile != 0;
     const int nsets = prof ? 2 : 1;
-    std::vector<cudaEvent_t> pev(prof ? 2 * GI * 3 : 0);
+    // events per iteration: before the check kernel, before the variable kernel, after it, and
+    // around the syndrome-test kernel
+    constexpr int kEv = 5;
+    std::vector<cudaEvent_t> pev(prof ? 2 * GI * kEv : 0);
     for (auto &ev : pev) JBP_CUDA_TRY(cudaEventCreate(&ev), "cudaEventCreate");
     cudaStream_t cap;
     JBP_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -769,7 +777,7 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
         ce = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
         if (ce != cudaSuccess) break;
         for (int i = 0; i < GI; ++i) {
-            cudaEvent_t *e3 = prof ? &pev[(set * GI + i) * 3] : nullptr;
+            cudaEvent_t *e3 = prof ? &pev[(set * GI + i) * kEv] : nullptr;
             enqueue_iteration(cap, e3);
         }
         ce = cudaStreamEndCapture(cap, &graph[set]);
@@ -777,16 +785,19 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
         per_graph = launches - launches_before;
     }
     launches = launches_before;
-    double check_ms = 0.0, var_ms = 0.0;
+    double check_ms = 0.0, var_ms = 0.0, test_ms = 0.0;
     long long prof_iters = 0;
     auto read_profile = [&](long long gidx) {
         if (!prof) return;
         const int set = static_cast<int>(gidx & 1);
         for (int i = 0; i < GI; ++i) {
             float a = 0.0f, b = 0.0f;
-            cudaEvent_t *e3 = &pev[(set * GI + i) * 3];
+            float c = 0.0f;
+            cudaEvent_t *e3 = &pev[(set * GI + i) * kEv];
             if (cudaEventElapsedTime(&a, e3[0], e3[1]) == cudaSuccess &&
-                cudaEventElapsedTime(&b, e3[1], e3[2]) == cudaSuccess) {
+                cudaEventElapsedTime(&b, e3[1], e3[2]) == cudaSuccess &&
+                cudaEventElapsedTime(&c, e3[3], e3[4]) == cudaSuccess) {
+                test_ms += c;
                 check_ms += a;
                 var_ms += b;
                 prof_iters++;
@@ -799,6 +810,7 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     const long long max_graphs = max_iters_total / GI + 2;
     auto t0 = std::chrono::steady_clock::now();
     std::string err;
+    bool timed_out = false;
     if (ce != cudaSuccess) err = cuda_err(ce, "graph capture");
     long long g = 0;
     bool finished = false;
@@ -816,10 +828,14 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
         }
         if (o.watchdog_ms > 0) {
             double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-            if (wall > o.watchdog_ms) { err = "watchdog expired after " + std::to_string(wall) + " ms"; break; }
+            if (wall > o.watchdog_ms) {
+                // the graphs already launched finish; the counters below say how far the run got
+                timed_out = true;
+                break;
+            }
         }
     }
-    if (err.empty() && !finished && g >= 1) {
+    if (err.empty() && !finished && !timed_out && g >= 1) {
         ce = cudaEventSynchronize(poll_ev[(g - 1) & 1]);
         if (ce == cudaSuccess && buf_.h_done[(g - 1) & 1] >= static_cast<unsigned long long>(rq.ntrials)) finished = true;
         if (!finished) err = "run did not complete within the iteration bound (internal error)";
@@ -839,6 +855,10 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
         ce = cudaMemcpy(&hc, buf_.cnt, sizeof(hc), cudaMemcpyDeviceToHost);
         if (ce != cudaSuccess) err = cuda_err(ce, "read counters");
     }
+    const bool timeout_err = err.empty() && timed_out && hc.done < static_cast<unsigned long long>(rq.ntrials);
+    if (timeout_err)
+        err = "watchdog expired: the run budget of " + std::to_string(o.watchdog_ms) + " ms ran out (host check) after " +
+              std::to_string(hc.done) + " of " + std::to_string(rq.ntrials) + " trials";
     for (int set = 0; set < 2; ++set) {
         if (exec[set]) cudaGraphExecDestroy(exec[set]);
         if (graph[set]) cudaGraphDestroy(graph[set]);
@@ -849,15 +869,17 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     cudaEventDestroy(ev1);
     cudaEventDestroy(poll_ev[0]);
     cudaEventDestroy(poll_ev[1]);
-    if (!err.empty()) return err;
+    if (!err.empty() && !timeout_err) return err;
     if (hc.bad_input) return "error vector has invalid value";
     fill_stats(hc, stats);
     stats.device_ms = ms;
     stats.kernel_launches = launches;
     stats.check_ms = check_ms;
     stats.var_ms = var_ms;
+    stats.test_ms = test_ms;
     stats.profiled_iterations = prof_iters;
     stats.slots = S;
+    if (!err.empty()) return err;
     (void)n;
     (void)M;
     return "";
@@ -1008,6 +1030,7 @@ std::string Engine::run_mixed(const MixedRequest &rq, std::vector<jbp_stats> &st
     for (int i = 0; i < 4; ++i) r.prior4[i] = o.prior[i];
     r.scratch = e0.mix_scratch_;
     r.scratch_stride = scratch;
+    r.budget_ns = o.watchdog_ms > 0 ? static_cast<unsigned long long>(o.watchdog_ms) * 1000000ull : 0ull;
     long long end = 0;
     for (int k = 0; k < nc; ++k) {
         const int i = order[k];
@@ -1055,15 +1078,21 @@ std::string Engine::run_mixed(const MixedRequest &rq, std::vector<jbp_stats> &st
     if (ce != cudaSuccess) return cuda_err(ce, "mixed run");
     for (int k = 0; k < nc; ++k)
         if (hc[k].bad_input) return "error vector has invalid value";
+    long long done = 0;
     for (int k = 0; k < nc; ++k) {
         const int i = order[k];
-        if (hc[k].done != static_cast<unsigned long long>(rq.ntrials[i]))
-            return "mixed run finished an unexpected number of trials";
         fill_stats(hc[k], stats[i]);
         stats[i].device_ms = ms;
         stats[i].kernel_launches = 1;
         stats[i].slots = grid;
+        done += static_cast<long long>(hc[k].done);
     }
+    if (hc[0].watchdog)
+        return "watchdog expired: the run budget of " + std::to_string(o.watchdog_ms) + " ms ran out on the device after " +
+               std::to_string(done) + " of " + std::to_string(total) + " trials";
+    for (int k = 0; k < nc; ++k)
+        if (hc[k].done != static_cast<unsigned long long>(rq.ntrials[order[k]]))
+            return "mixed run finished an unexpected number of trials";
     return "";
 }
 

@@ -88,6 +88,7 @@ struct DevCounters {
     unsigned long long watchdog;
     unsigned long long bad_input;   // error bytes outside 0..3 seen in a kSrcErrors source
     unsigned long long learned_attempts, learned_success;   // learned flip proposals tried / saves
+    unsigned long long syndrome_tests;   // slot engine: per-trial syndrome tests run
 };
 
 struct DevRun {
@@ -141,8 +142,7 @@ struct DevRun {
     // post-processing (enabled when pp != 0)
     int pp;
     int flip_hist;                  // flip-history window H (R >= H + 1)
-    int llr_from;                   // first 1-based iteration whose |LLR| is kept: min(100, max_iter)
-    double *llr;                    // [2][S][n] |LLR| of the latest kept iteration
+    int llr_from;                   // first 1-based iteration of the stall triggers: min(100, max_iter)
     int *act_k;                     // [S] iteration the flip window started (0: not started)
     int *pstate;                    // [S] bit0 stall, bit1 oscillation, bit2 us-oscillation active
     int *stall_same;                // [S]

@@ -95,7 +95,6 @@ private:
         // post-processing state (allocated when a run enables it)
         bool pp = false;
         int R = 1;
-        double *llr = nullptr;
         int *act_k = nullptr, *pstate = nullptr, *stall_same = nullptr, *pp_list = nullptr, *pp_mode = nullptr;
         unsigned short *us_hist = nullptr;
         unsigned *dprev = nullptr, *dpprev = nullptr;

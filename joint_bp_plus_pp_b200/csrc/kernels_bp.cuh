@@ -70,12 +70,6 @@ __device__ __forceinline__ void store_est_bits(const DevRun &run, size_t plane, 
     if (lane == 1) run.estz[plane + static_cast<size_t>(group) * n + v] = zm;
 }
 
-// Whether a slot's iteration k1 (1-based) keeps its |LLR| for post-processing: in-loop
-// post-processing starts at iteration 100 or at max_iter (jointbp_ets.cpp:2563).
-__device__ __forceinline__ bool keeps_llr(const DevRun &run, int slot) {
-    return run.pp && run.iter[slot] + 1 >= run.llr_from;
-}
-
 // freeze-syn state of a slot's side in a check kernel: 0 = update normally, 1 = frozen
 // (skip), 2 = frozen at the last check (write the deterministic messages, then skip).
 __device__ __forceinline__ int frozen_state(const DevRun &run, int slot, int side) {
@@ -266,15 +260,8 @@ __global__ void __launch_bounds__(256, 2) k_var_f64(DevCode code, DevRun run, De
             if (t1 > bv) { best = 1; bv = t1; }
             if (t2 > bv) { best = 2; bv = t2; }
             if (t3 > bv) { best = 3; }
-            if (keeps_llr(run, slot)) {
-                // |LLR| of the x and z bits (jointbp_ets.cpp:2484-2492)
-                const double eps = 1e-300;
-                const double px1 = dadd(t1, t3), px0 = dadd(t0, t2), pz1 = dadd(t2, t3), pz0 = dadd(t0, t1);
-                const double lx = dsub(log_dd(px1 > eps ? px1 : eps), log_dd(px0 > eps ? px0 : eps));
-                const double lz = dsub(log_dd(pz1 > eps ? pz1 : eps), log_dd(pz0 > eps ? pz0 : eps));
-                run.llr[static_cast<size_t>(slot) * n + v] = fabs(lx);
-                run.llr[(static_cast<size_t>(run.S) + slot) * n + v] = fabs(lz);
-            }
+            // (the |LLR| keys of the OSD order are computed from the same messages by the block
+            // that post-processes the slot: kernels_slot_pp.cuh)
             double2 *v2cx = static_cast<double2 *>(msg.v2c[0]);
             double2 *v2cz = static_cast<double2 *>(msg.v2c[1]);
             double2 *v2cx_hi = static_cast<double2 *>(msg.v2c_hi[0]);
@@ -456,12 +443,6 @@ __device__ __forceinline__ int var_llr_one(const DevCode &code, const DevRun &ru
     if (w3 > bv) { best = 3; }
     const float Gx = lse2(lp.x, lp.z - Mu) - lse2(lp.y, lp.w - Mu);   // x-bit coupling through Z
     const float Hz = lse2(lp.x, lp.y - Lam) - lse2(lp.z, lp.w - Lam); // z-bit coupling through X
-    if (keeps_llr(run, slot)) {
-        // |LLR| of the x and z bits of the total (base 2; the OSD order is scale-free)
-        const int n = code.n;
-        run.llr[static_cast<size_t>(slot) * n + v] = fabsf(lse2(w1, w3) - lse2(w0, w2));
-        run.llr[(static_cast<size_t>(run.S) + slot) * n + v] = fabsf(lse2(w2, w3) - lse2(w0, w1));
-    }
     const int frz = run.freeze_syn ? run.frz[slot] : 0;
 #pragma unroll
     for (int k = 0; k < DV; ++k) {

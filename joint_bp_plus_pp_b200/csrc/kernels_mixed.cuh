@@ -59,6 +59,7 @@ struct MixRun {
     double prior4[4];
     unsigned char *scratch;        // per block, scratch_stride bytes (c2v of the codes that do not fit)
     size_t scratch_stride;
+    unsigned long long budget_ns;  // run budget as ResRun::budget_ns; stops are counted in code[0].cnt
 };
 
 __host__ __device__ inline size_t mix_align(size_t b) { return (b + 15) / 16 * 16; }
@@ -172,12 +173,20 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant_
     __shared__ float lpx_sh, lpz_sh;
     __shared__ float first_sh[2][DC];   // first-iteration c2v of each position (syndrome bit 0)
     __shared__ int ints[16];
+    __shared__ int abort_sh;   // the run budget ran out during this trial
     if (threadIdx.x < 16) ints[threadIdx.x] = 0;
+    __shared__ unsigned long long deadline_sh;   // global-timer end of the run budget (0 = none)
+    if (threadIdx.x == 0) deadline_sh = run.budget_ns ? dev_globaltimer() + run.budget_ns : 0ull;
     for (;;) {
         if (threadIdx.x == 0) {
             const unsigned long long k = atomicAdd(run.next, 1ull);
             const long long total = run.code[run.ncodes - 1].item_end;
             long long item = k < static_cast<unsigned long long>(total) ? static_cast<long long>(k) : -1;
+            if (item >= 0 && deadline_sh && dev_globaltimer() > deadline_sh) {
+                item = -1;   // the run budget is spent: no further trial
+                atomicAdd(&run.code[0].cnt->watchdog, 1ull);
+            }
+            abort_sh = 0;
             int ci = 0;
             if (item >= 0) {
                 while (item >= run.code[ci].item_end) ++ci;
@@ -288,13 +297,23 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant_
             } else if (fused) {
                 bad = mix_test_side<DC>(mc.chk[0], mx, A, syn) + mix_test_side<DC>(mc.chk[1], mz, A + n, synz);
             }
+            // run budget (as k_resident): thread 0 writes the flag before the barrier, every thread
+            // reads it after it
+            if (threadIdx.x == 0 && it % kResBudgetEvery == kResBudgetEvery - 1 && deadline_sh &&
+                dev_globaltimer() > deadline_sh)
+                abort_sh = 1;
             const bool any = __syncthreads_or(bad) != 0;
             if (fused && !any) { rf = kResSyndromeOk | kResBpOk; iters = it; break; }
-            if (it >= run.max_iter) break;
+            if (it >= run.max_iter || abort_sh) break;
             for (int v = threadIdx.x; v < n; v += blockDim.x)
                 mix_var<ST>(mc.slot[0], dvx, mc.slot[1], dvz, c2v, c2vz, A, n, v, lp, pr);
             __syncthreads();
             ++it;
+        }
+        if (abort_sh && rf == 0 && it < run.max_iter) {
+            // abandoned for the run budget: not classified, not counted; the block stops
+            if (threadIdx.x == 0) atomicAdd(&run.code[0].cnt->watchdog, 1ull);
+            break;
         }
         const bool ok = (rf & kResSyndromeOk) != 0;
         if (mc.llr_out) mix_write_llr<ST>(mc.slot[0], dvx, mc.slot[1], dvz, c2v, c2vz, n, lp, mc.llr_out + local * n * 2);

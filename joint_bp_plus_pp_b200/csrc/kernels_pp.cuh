@@ -676,58 +676,4 @@ __device__ __forceinline__ int pp_result_flags(const PpOutcome &o, bool in_loop_
            (o.osd_ok ? kResOsdOk : 0);
 }
 
-// Post-processing of the pending slots (in-loop attempt at iteration k, or post-BP on the
-// final estimate).  The stage sequence is the same in both; an in-loop attempt keeps the
-// corrected estimate only if both syndromes match, a post-BP run keeps whatever its stages
-// applied.  An in-loop attempt at max_iter that fails is followed by post-BP stages on the
-// same estimate, which repeat its steps exactly; their result is taken from the same pass.
-static __global__ void __launch_bounds__(kPpThreads) k_postprocess(DevCode code, DevRun run) {
-    extern __shared__ unsigned char pp_smem[];
-    const int n = code.n, mx = code.s[0].m, mz = code.s[1].m, M = mx + mz, mmax = mx > mz ? mx : mz;
-    const PpShared sh = pp_shared_carve(pp_smem, n, M, mmax);
-    const PpScratch sc = pp_scratch_carve(run.pp_scratch + run.pp_scratch_stride * blockIdx.x, n, mmax);
-    const int npend = *run.n_pp;
-    const int G = run.S / kGroup;
-    const size_t plane = plane_offset(run, n, 0);
-    for (int q = blockIdx.x; q < npend; q += gridDim.x) {
-        const int slot = run.pp_list[q];
-        const int mode = run.pp_mode[slot];
-        const int k = run.iter[slot];
-        const int group = slot / kGroup, b = slot % kGroup;
-        const size_t row = plane + static_cast<size_t>(group) * n;
-        for (int v = threadIdx.x; v < n; v += blockDim.x)
-            sh.est[v] = static_cast<uint8_t>(((run.estx[row + v] >> b) & 1u) | (((run.estz[row + v] >> b) & 1u) << 1));
-        for (int r = threadIdx.x; r < M; r += blockDim.x)
-            sh.tgt[r] = static_cast<uint8_t>((run.synm[static_cast<size_t>(r) * G + group] >> b) & 1u);
-        __syncthreads();
-        const SlotHistory hist{&run, slot, k};
-        const double *llr = run.llr + static_cast<size_t>(slot) * n;
-        const PpOutcome o = blk_pp_stages(code, run.ets, hist, run.flip_hist, run.act_k[slot], k, llr,
-                                          llr + static_cast<size_t>(run.S) * n, sh, sc);
-        const bool in_loop_success = mode == kPpInLoop && o.ok;
-        const bool post = !in_loop_success && (mode == kPpPost || k >= run.max_iter);
-        if (in_loop_success || post) {
-            // write the corrected decisions back into the slot's bits of the current planes
-            const unsigned bit = 1u << b;
-            for (int v = threadIdx.x; v < n; v += blockDim.x) {
-                const unsigned ox = (run.estx[row + v] >> b) & 1u, oz = (run.estz[row + v] >> b) & 1u;
-                const unsigned nx = sh.est[v] & 1u, nz = (sh.est[v] >> 1) & 1u;
-                if (ox != nx) atomicXor(&run.estx[row + v], bit);
-                if (oz != nz) atomicXor(&run.estz[row + v], bit);
-            }
-        }
-        if (threadIdx.x == 0) {
-            if (in_loop_success || post) run.res_flags[slot] = pp_result_flags(o, in_loop_success);
-            if (in_loop_success) {
-                run.res_iters[slot] = k;
-                if (k < run.max_iter) {
-                    run.flags[slot] = kFinished;
-                    run.retired[atomicAdd(run.n_retired, 1)] = slot;
-                }
-            }
-        }
-        __syncthreads();
-    }
-}
-
 }  // namespace jbp

@@ -100,7 +100,20 @@ struct ResRun {
     float *col_x, *col_y;          // [col_cap][8], [col_cap][2]
     unsigned long long *col_count;
     long long col_cap;
+    // run budget (jbp_options.watchdog_ms): > 0, a block that has run this long (global timer,
+    // from its start) claims no further trial and abandons the one it decodes at its next check
+    // (every kResBudgetEvery iterations); cnt->watchdog counts the blocks that stopped so
+    unsigned long long budget_ns;
 };
+
+constexpr int kResBudgetEvery = 16;   // iterations between two run-budget checks of a block
+
+// Nanoseconds of the GPU's global timer (the run budget of the persistent kernels).
+__device__ __forceinline__ unsigned long long dev_globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 constexpr int kLearnedTries = 3;   // learned proposals per trial at most
 constexpr int kLearnedMaxUnsat = 30;   // ... and only while max(us_x, us_z) is at most this
@@ -746,8 +759,13 @@ __global__ void __launch_bounds__(kResThreads, 1)
     const int slow_from = PP ? max(1, llr_from - 2) : 0x7fffffff;
 
     __shared__ double pt_sh;
+    __shared__ int abort_sh;          // the run budget ran out during this trial
+    // global-timer end of the run budget (0 = none), in shared memory so that the BP loop keeps
+    // no register for it
+    __shared__ unsigned long long deadline_sh;
     unsigned long long claimed = 0;   // thread 0: the next trial index this block has claimed
     if (threadIdx.x == 0) {
+        deadline_sh = run.budget_ns ? dev_globaltimer() + run.budget_ns : 0ull;
         claimed = atomicAdd(&run.cnt->next_trial, 1ull);
         res_set_prior(run.use_prior, run.prior4, run.p, &lp_sh, &pr_sh, &lpx_sh, &lpz_sh);
         for (int i = 0; i < 16; ++i) ints[i] = 0;
@@ -761,6 +779,11 @@ __global__ void __launch_bounds__(kResThreads, 1)
             const unsigned long long k = claimed;
             claimed = atomicAdd(&run.cnt->next_trial, 1ull);
             trial_sh = k < static_cast<unsigned long long>(run.ntrials) ? static_cast<long long>(k) : -1;
+            if (trial_sh >= 0 && deadline_sh && dev_globaltimer() > deadline_sh) {
+                trial_sh = -1;   // the run budget is spent: no further trial
+                atomicAdd(&run.cnt->watchdog, 1ull);
+            }
+            abort_sh = 0;
             pp_sh[1] = 0;   // act_k
             pp_sh[2] = 0;   // pstate
             pp_sh[3] = 0;   // learned proposals tried
@@ -887,6 +910,13 @@ __global__ void __launch_bounds__(kResThreads, 1)
                     if (wz) atomicAdd(&us_cnt[it & 1][1], wz);
                 }
             }
+            // run budget: thread 0 looks at the timer every kResBudgetEvery iterations; the flag
+            // is read by every thread after the barrier below (at the iteration-limit exit, which
+            // keeps the loop's register use as it was) and written again only after the next
+            // variable phase's barrier
+            if (threadIdx.x == 0 && it % kResBudgetEvery == kResBudgetEvery - 1 && deadline_sh &&
+                dev_globaltimer() > deadline_sh)
+                abort_sh = 1;
             const int nbad = __syncthreads_count(bx + bz != 0);
             if (fused) {
                 if (nbad == 0) { rf = kResSyndromeOk | kResBpOk; iters = it; break; }
@@ -895,7 +925,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
                     us_hist[it % 100] =
                         static_cast<unsigned short>(min(max(us_cnt[it & 1][0], us_cnt[it & 1][1]), 65535));
             }
-            if (it >= run.max_iter) break;
+            if (it >= run.max_iter || abort_sh) break;
             if (sep) {
                 res_check_side<P, J, L, ST, 0>(code, c2v, A, syn, false);
                 res_check_side<P, J, L, ST, 1>(code, c2vz, A, syn, false);
@@ -929,6 +959,11 @@ __global__ void __launch_bounds__(kResThreads, 1)
                     break;
                 }
             }
+        }
+        if (abort_sh && rf == 0 && it < run.max_iter) {
+            // abandoned for the run budget: not classified, not counted; the block stops
+            if (threadIdx.x == 0) atomicAdd(&run.cnt->watchdog, 1ull);
+            break;
         }
         const bool ok = (rf & kResSyndromeOk) != 0;
         if (run.llr_out) res_write_llr<P, J, L, ST>(code, c2v, c2vz, lp_sh, run.llr_out + local * n * 2);

@@ -98,6 +98,7 @@ static __global__ void __launch_bounds__(256) k_syndrome_check(DevCode code, Dev
         const bool due = (run.flags[slot] & kRunning) && check_due(run, run.iter[slot] + 1);
         const unsigned due_mask = __ballot_sync(0xffffffffu, due);
         if (!due_mask) continue;
+        if (rb == 0 && lane == 0) atomicAdd(&run.cnt->syndrome_tests, static_cast<unsigned long long>(__popc(due_mask)));
         const int row = rb * 32 + lane;
         unsigned mm[2] = {0u, 0u};
         if (row < M) {

@@ -152,3 +152,44 @@ def test_resident_engine_and_learned_proposal_from_the_cli(tmp_path):
     assert r2.returncode != 0 and "npy" in r2.stderr
     r3, _ = run(base + ["--engine", "bogus"])
     assert r3.returncode != 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("engine,precision", [("slots", "fp64"), ("resident", "fp32")])
+def test_iter_hist_out_costs_and_progress_tsv(tmp_path, decoder, engine, precision):
+    """--iter-hist-out in the reference's format (jointbp_ets.cpp:4623-4643) with measured costs:
+    the fractions sum to 1 and equal the library's histogram of the same trials, the iteration
+    cost is positive (CUDA-event device time per trial-iteration), the syndrome-test cost is
+    positive on the slot engine and 0 on the resident kernel (the test is fused); and
+    --progress-tsv holds the latest line only, in the reference's 12 columns
+    (jointbp_ets.cpp:5085-5122), consistent with the Run Summary."""
+    from joint_bp_plus_pp_b200 import Options
+    h, t = tmp_path / "hist.txt", tmp_path / "progress.tsv"
+    k = 3000
+    r, s = run(["--simulate", "--p", "0.04", "--trials", str(k), "--max-iter", "200", "--seed", "106", "--sampler",
+                "philox", "--precision", precision, "--engine", engine, "--no-pp", "--batch", "1000",
+                "--iter-hist-out", str(h), "--progress-tsv", str(t)])
+    assert r.returncode == 0, r.stderr
+    lines = h.read_text().splitlines()
+    assert lines[0].startswith("# costs ") and lines[-len([l for l in lines if not l.startswith("#")]) - 1] == "# iter fraction"
+    iter_cost, check_cost = (float(x) for x in lines[0].split()[2:4])
+    assert iter_cost > 0.0
+    assert (check_cost > 0.0) if engine == "slots" else (check_cost == 0.0)
+    assert any(l.startswith("# cost_source " + ("slots" if engine == "slots" else "resident")) for l in lines)
+    frac = {int(a): float(b) for a, b in (l.split() for l in lines if not l.startswith("#"))}
+    assert abs(sum(frac.values()) - 1.0) < 1e-8
+    st, _ = decoder.simulate(106, k, 0.04, Options(precision=precision, engine=engine, max_iter=200, enable_pp=False),
+                             per_trial=False, hist=True)
+    hist = st["hist"]
+    assert set(frac) == {i for i in range(1, len(hist)) if hist[i]}
+    for i, f in frac.items():
+        assert abs(f - hist[i] / k) < 1e-9, i
+    assert abs(sum(i * f for i, f in frac.items()) * k - int(s["iters"])) < 1e-3
+    rows = t.read_text().splitlines()
+    assert len(rows) == 1   # rewritten after each of the three batches
+    cols = rows[0].split("\t")
+    assert len(cols) == 12
+    assert int(cols[1]) == k and int(cols[2]) == int(s["failures"]) and int(cols[8]) == int(s["iters"])
+    assert int(cols[3]) == int(s["pp_success"]) and int(cols[6]) == int(s["stab_success"])
+    assert abs(float(cols[7]) - float(s["avg_iter"])) < 0.006
+    assert cols[11].startswith(f"PROGRESS | trials={k} | failures={s['failures']} |")
