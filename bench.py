@@ -361,11 +361,12 @@ def main():
            "bp_trial_iterations": 0, "profiled_iterations": 0, "device_ms": 0.0, "pp_success": 0,
            "learned_attempts": 0, "learned_success": 0}
     first_res = None
-    step_wall, step_kernel = [], []
+    step_wall, step_kernel, step_stats = [], [], []
     for k in range(args.steps):
         t0 = time.perf_counter()
         st, res = dec.simulate(args.seed, B, args.p, opts, first_trial=base + (args.warmup + k) * B,
-                               per_trial=(k == 0))
+                               per_trial=(k == 0), hist=True)
+        step_stats.append(st)
         step_wall.append(round((time.perf_counter() - t0) * 1e3, 2))
         step_kernel.append(round(st["device_ms"], 2))
         if k == 0:
@@ -379,6 +380,10 @@ def main():
     ms, tot = reduce_over_ranks(dist, ev0.elapsed_time(ev1), {"trials": agg["trials"], "failures": agg["failures"]},
                                 dev)
     total_trials = float(tot["trials"])
+    # the whole job's Run Summary: every counter and the iteration histogram of every rank's
+    # timed steps, one int64 all-reduce (outside the timed region)
+    from joint_bp_plus_pp_b200.runsummary import merge_run_summaries, run_summary
+    merged = merge_run_summaries(step_stats, group=(dist is not None) or None)
     value = total_trials / (ms / 1000.0)
 
     peak, peak_kind = measured_peaks()
@@ -560,7 +565,7 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return 0
-    lo, hi = wilson_interval(agg["trials"], agg["failures"])
+    lo, hi = wilson_interval(merged["trials"], merged["failures"])
     
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -585,8 +590,10 @@ def main():
                    "parallelism": f"replica trial ranges x{world}"},
         "gpu_launches": agg["kernel_launches"],
         "roofline": roofline,
-        "ler": {"trials": agg["trials"], "failures": agg["failures"], "ci95": [lo, hi],
-                "avg_iter": agg["total_iters"] / max(1, agg["trials"])},
+        "ler": {"trials": merged["trials"], "failures": merged["failures"], "ci95": [lo, hi],
+                "avg_iter": merged["total_iters"] / max(1, merged["trials"])},
+        "run_summary": dict(run_summary(merged), ranks=world,
+                            iter_hist_nonzero={int(i): int(c) for i, c in enumerate(merged["hist"]) if c}),
         "fp64": fp64,
         "precision": precision,
         "mixed_sizes_one_launch": mixed,

@@ -25,6 +25,7 @@
 #include <sstream>
 #include <string>
 #include <sys/stat.h>
+#include <thread>
 #include <vector>
 
 #include "jbp_b200.h"
@@ -33,6 +34,7 @@ namespace {
 
 struct Args {
     std::string params, sx_path, sz_path, err_path, est_path, hist_out, progress_tsv, ets_dir;
+    std::vector<int> devices;   // --cuda-devices: one context and host thread per entry
     std::string ets6_x, ets6_z, ets12_x, ets12_z, ets8_path4;
     double p = 0.05, damping = 0.0;
     int max_iter = 50, flip_hist = 5, device = 0, check_warmup = 0, check_interval = 1;
@@ -59,6 +61,8 @@ void usage(const char *prog) {
               << "  --report-every N (100)  --progress-every N (100)  --progress-tsv FILE  --iter-hist-out FILE\n"
               << "  --ets6-x F --ets6-z F --ets12-x F --ets12-z F --ets-x F --ets-z F --ets8-path4 F\n"
               << "  --cuda --cuda-graph (accepted; decoding always runs on the GPU)  --cuda-device D\n"
+              << "  --cuda-devices D0,D1,... (with --simulate: one context and host thread per listed device, each\n"
+              << "  decoding a contiguous part of the trial range; one Run Summary of the whole run)\n"
               << "  --cuda-check-warmup N (0)  --cuda-check-interval N (1; 0 with --autotune: tuned)\n"
               << "Extra options:\n"
               << "  --precision fp64|fp32|fp16 (fp64)  --sampler mt19937|philox (mt19937)\n"
@@ -176,6 +180,17 @@ int parse(int argc, char **argv, Args &a) {
             else if (f == "--no-pp") a.enable_pp = false;
             else if (f == "--cuda" || f == "--cuda-graph") {}
             else if (f == "--cuda-device") { VAL(); a.device = std::stoi(v); }
+            else if (f == "--cuda-devices") {
+                VAL();
+                a.devices.clear();
+                std::stringstream ds(v);
+                for (std::string t; std::getline(ds, t, ',');)
+                    if (!t.empty()) a.devices.push_back(std::stoi(t));
+                if (a.devices.empty()) {
+                    std::cerr << "--cuda-devices needs a list of device indices (e.g. 0,1,2,3)\n";
+                    return 1;
+                }
+            }
             else if (f == "--cuda-check-warmup") { VAL(); a.check_warmup = std::max(0, std::stoi(v)); }
             else if (f == "--cuda-check-interval") { VAL(); a.check_interval = std::max(0, std::stoi(v)); }
             else if (f == "--trial-index") { VAL(); a.trial_index = std::stoll(v); }
@@ -495,6 +510,33 @@ void progress_line(std::ostream &os, const jbp_stats &s, double elapsed) {
        << (s.trials ? static_cast<double>(s.total_iters) / s.trials : 0.0) << " gpu_ms=" << s.device_ms << "\n";
 }
 
+// Run Summary (jointbp_ets.cpp:6419-6448), the gpu line and --iter-hist-out of a finished run.
+void print_run_summary(const Args &a, const jbp_stats &acc, const std::vector<long long> &hist, double elapsed) {
+    const long long d = acc.trials;
+    const double fer = d ? static_cast<double>(acc.failures) / d : 0.0;
+    double lo = 0.0, hi = 0.0;
+    const bool ci = wilson(d, acc.failures, 1.96, lo, hi);
+    print_section("Run Summary");
+    std::cout << "trials=" << d << " failures=" << acc.failures << " bp_fail=" << acc.bp_fail
+              << " pp_success=" << acc.pp_success << " flip_pp_success=" << acc.flip_pp_success
+              << " stab_success=" << acc.stab_success << " ets_used=" << acc.ets_used << " ets_saved=" << acc.ets_saved
+              << " ets6_used=" << acc.ets6_used << " ets6_saved=" << acc.ets6_saved << " ets12_used=" << acc.ets12_used
+              << " ets12_saved=" << acc.ets12_saved << " fer=" << std::setprecision(8) << std::fixed << fer;
+    if (ci) std::cout << " ci95=[" << std::setprecision(8) << lo << "," << hi << "]";
+    std::cout << " iters=" << acc.total_iters << " avg_iter=" << std::setprecision(2)
+              << (d ? static_cast<double>(acc.total_iters) / d : 0.0)
+              << " avg_latency=" << latency_str(d ? elapsed / d : 0.0) << " exact_rate=" << std::setprecision(6)
+              << (d ? static_cast<double>(acc.exact) / d : 0.0) << " elapsed_s=" << std::setprecision(2) << elapsed
+              << "s\n";
+    std::cout << "gpu: precision=" << (a.precision == JBP_PREC_FP64 ? "fp64" : a.precision == JBP_PREC_FP32 ? "fp32"
+                                                                                                               : "fp16")
+              << " sampler=" << (a.sampler == JBP_SAMPLER_MT19937 ? "mt19937" : "philox") << " device_ms="
+              << std::setprecision(2) << acc.device_ms << " trials_per_s=" << (elapsed > 0 ? d / elapsed : 0.0)
+              << "\n";
+    if (!a.hist_out.empty() && d > 0 && !write_hist_out(a.hist_out, hist, d, acc))
+        std::cerr << "Failed to write histogram output: " << a.hist_out << "\n";
+}
+
 int simulate(jbp_ctx *ctx, const Args &a, int n) {
     if (a.trials <= 0) {
         std::cerr << "--trials must be positive in --simulate mode\n";
@@ -580,30 +622,64 @@ int simulate(jbp_ctx *ctx, const Args &a, int n) {
         }
         std::cout << "Saved estimate: " << a.est_path << "\n";
     }
-    // Run Summary (jointbp_ets.cpp:6419-6448)
-    const long long d = acc.trials;
-    const double fer = d ? static_cast<double>(acc.failures) / d : 0.0;
-    double lo = 0.0, hi = 0.0;
-    const bool ci = wilson(d, acc.failures, 1.96, lo, hi);
-    print_section("Run Summary");
-    std::cout << "trials=" << d << " failures=" << acc.failures << " bp_fail=" << acc.bp_fail
-              << " pp_success=" << acc.pp_success << " flip_pp_success=" << acc.flip_pp_success
-              << " stab_success=" << acc.stab_success << " ets_used=" << acc.ets_used << " ets_saved=" << acc.ets_saved
-              << " ets6_used=" << acc.ets6_used << " ets6_saved=" << acc.ets6_saved << " ets12_used=" << acc.ets12_used
-              << " ets12_saved=" << acc.ets12_saved << " fer=" << std::setprecision(8) << std::fixed << fer;
-    if (ci) std::cout << " ci95=[" << std::setprecision(8) << lo << "," << hi << "]";
-    std::cout << " iters=" << acc.total_iters << " avg_iter=" << std::setprecision(2)
-              << (d ? static_cast<double>(acc.total_iters) / d : 0.0)
-              << " avg_latency=" << latency_str(d ? elapsed / d : 0.0) << " exact_rate=" << std::setprecision(6)
-              << (d ? static_cast<double>(acc.exact) / d : 0.0) << " elapsed_s=" << std::setprecision(2) << elapsed
-              << "s\n";
-    std::cout << "gpu: precision=" << (a.precision == JBP_PREC_FP64 ? "fp64" : a.precision == JBP_PREC_FP32 ? "fp32"
-                                                                                                               : "fp16")
-              << " sampler=" << (a.sampler == JBP_SAMPLER_MT19937 ? "mt19937" : "philox") << " device_ms="
-              << std::setprecision(2) << acc.device_ms << " trials_per_s=" << (elapsed > 0 ? d / elapsed : 0.0)
-              << "\n";
-    if (!a.hist_out.empty() && d > 0 && !write_hist_out(a.hist_out, hist, d, acc))
-        std::cerr << "Failed to write histogram output: " << a.hist_out << "\n";
+    print_run_summary(a, acc, hist, elapsed);
+    return 0;
+}
+
+// --cuda-devices: the trial range split into contiguous parts, one per listed device (a device
+// may be listed twice), each decoded by its own context on its own host thread in batches of
+// --batch; the counters and histograms are summed into one Run Summary.  Trials are keyed by
+// (seed, trial index), so the summary equals that of one device decoding the whole range.
+int simulate_multi(const std::vector<jbp_ctx *> &ctxs, const Args &a) {
+    if (a.trials <= 0) {
+        std::cerr << "--trials must be positive in --simulate mode\n";
+        return 1;
+    }
+    if (a.min_fails > 0 || !a.est_path.empty() || a.autotune || !a.progress_tsv.empty()) {
+        std::cerr << "--cuda-devices does not take --min-fails, --est, --autotune or --progress-tsv\n";
+        return 1;
+    }
+    const jbp_options o = options(a);
+    const long long first = a.trial_index >= 0 ? a.trial_index : 1;
+    const int D = static_cast<int>(ctxs.size());
+    std::vector<jbp_stats> st(D);
+    std::vector<std::vector<long long>> hist(D, std::vector<long long>(static_cast<size_t>(a.max_iter) + 1, 0));
+    std::vector<std::string> errs(D);
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> pool;
+    for (int d = 0; d < D; ++d) {
+        pool.emplace_back([&, d]() {
+            const long long lo = first + a.trials * d / D, hi = first + a.trials * (d + 1) / D;
+            std::vector<long long> h(hist[d].size());
+            std::memset(&st[d], 0, sizeof(jbp_stats));
+            for (long long b = lo; b < hi; b += a.batch) {
+                const long long cnt = std::min(a.batch, hi - b);
+                jbp_stats s{};
+                std::fill(h.begin(), h.end(), 0);
+                if (jbp_simulate(ctxs[d], &o, a.seed, b, cnt, a.p, a.sampler, &s, nullptr, h.data()) != JBP_OK) {
+                    errs[d] = jbp_last_error();
+                    return;
+                }
+                add_stats(st[d], s);
+                for (size_t i = 0; i < h.size(); ++i) hist[d][i] += h[i];
+            }
+        });
+    }
+    for (auto &t : pool) t.join();
+    for (int d = 0; d < D; ++d)
+        if (!errs[d].empty()) {
+            std::cerr << "simulate failed on device " << a.devices[d] << ": " << errs[d] << "\n";
+            return 1;
+        }
+    const double elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    jbp_stats acc{};
+    std::vector<long long> all(hist[0].size(), 0);
+    for (int d = 0; d < D; ++d) {
+        add_stats(acc, st[d]);
+        for (size_t i = 0; i < all.size(); ++i) all[i] += hist[d][i];
+    }
+    std::cout << "devices=" << D << " trials_per_device=" << (a.trials + D - 1) / D << "\n";
+    print_run_summary(a, acc, all, elapsed);
     return 0;
 }
 
@@ -710,6 +786,44 @@ int simulate_mixed_files(const Args &a) {
 
 }  // namespace
 
+// One decoding context on `device`: the code (params file or check lists), the ETS tables when
+// post-processing is on, and the learned flip model when asked for.  Returns 0, or 1 after a
+// message.
+int create_context(const Args &a, int device, const char *argv0, jbp_ctx **out) {
+    jbp_ctx *ctx = nullptr;
+    if (!a.checks.empty()) {
+        // a code given as check lists (no ETS tables)
+        int n = 0, m[2];
+        std::vector<int> off[2], var[2];
+        if (!read_checks_file(a.checks, n, m, off, var)) return 1;
+        if (jbp_create_from_checks(n, m[0], off[0].data(), var[0].data(), m[1], off[1].data(), var[1].data(),
+                                   device, &ctx) != JBP_OK) {
+            std::cerr << "init failed: " << jbp_last_error() << "\n";
+            return 1;
+        }
+    } else {
+        if (!exists(a.params)) {
+            std::cerr << "Failed to read params: " << a.params << "\n";
+            return 1;
+        }
+        if (jbp_create_from_params(a.params.c_str(), nullptr, device, &ctx) != JBP_OK) {
+            std::cerr << "init failed: " << jbp_last_error() << "\n";
+            return 1;
+        }
+    }
+    if (a.enable_pp && a.checks.empty() && load_ets(ctx, a)) {
+        std::cerr << "ETS load failed: " << jbp_last_error() << "\n";
+        jbp_destroy(ctx);
+        return 1;
+    }
+    if (setup_flip_model(ctx, a, argv0)) {
+        jbp_destroy(ctx);
+        return 1;
+    }
+    *out = ctx;
+    return 0;
+}
+
 int main(int argc, char **argv) {
     Args a;
     const int prc = parse(argc, argv, a);
@@ -743,36 +857,24 @@ int main(int argc, char **argv) {
             return 1;
         }
     }
-    jbp_ctx *ctx = nullptr;
-    if (!a.checks.empty()) {
-        // a code given as check lists (no ETS tables)
-        int n = 0, m[2];
-        std::vector<int> off[2], var[2];
-        if (!read_checks_file(a.checks, n, m, off, var)) return 1;
-        if (jbp_create_from_checks(n, m[0], off[0].data(), var[0].data(), m[1], off[1].data(), var[1].data(),
-                                   a.device, &ctx) != JBP_OK) {
-            std::cerr << "init failed: " << jbp_last_error() << "\n";
-            return 1;
-        }
-    } else {
-        if (!exists(a.params)) {
-            std::cerr << "Failed to read params: " << a.params << "\n";
-            return 1;
-        }
-        if (jbp_create_from_params(a.params.c_str(), nullptr, a.device, &ctx) != JBP_OK) {
-            std::cerr << "init failed: " << jbp_last_error() << "\n";
-            return 1;
-        }
-    }
-    if (a.enable_pp && a.checks.empty() && load_ets(ctx, a)) {
-        std::cerr << "ETS load failed: " << jbp_last_error() << "\n";
-        jbp_destroy(ctx);
+    if (!a.devices.empty() && !a.simulate) {
+        std::cerr << "--cuda-devices requires --simulate\n";
         return 1;
     }
-    if (setup_flip_model(ctx, a, argv[0])) {
-        jbp_destroy(ctx);
-        return 1;
+    std::vector<int> devs = a.devices.empty() ? std::vector<int>{a.device} : a.devices;
+    std::vector<jbp_ctx *> ctxs;
+    auto destroy_all = [&]() {
+        for (jbp_ctx *c : ctxs) jbp_destroy(c);
+    };
+    for (int dev : devs) {
+        jbp_ctx *c = nullptr;
+        if (create_context(a, dev, argv[0], &c)) {
+            destroy_all();
+            return 1;
+        }
+        ctxs.push_back(c);
     }
+    jbp_ctx *ctx = ctxs[0];
     int n = 0, mx = 0, mz = 0, rx = 0, rz = 0, ng = 0;
     jbp_code_info(ctx, &n, &mx, &mz, &rx, &rz, &ng);
     print_section("Code Summary");
@@ -789,7 +891,8 @@ int main(int argc, char **argv) {
                       << "  girth_x=" << gx << "  girth_z=" << gz << "\n";
         }
     }
-    const int rc = a.simulate ? simulate(ctx, a, n) : decode_single(ctx, a, n, mx, mz);
-    jbp_destroy(ctx);
+    const int rc = !a.devices.empty() ? simulate_multi(ctxs, a)
+                   : (a.simulate ? simulate(ctx, a, n) : decode_single(ctx, a, n, mx, mz));
+    destroy_all();
     return rc;
 }

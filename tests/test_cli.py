@@ -193,3 +193,21 @@ def test_iter_hist_out_costs_and_progress_tsv(tmp_path, decoder, engine, precisi
     assert int(cols[3]) == int(s["pp_success"]) and int(cols[6]) == int(s["stab_success"])
     assert abs(float(cols[7]) - float(s["avg_iter"])) < 0.006
     assert cols[11].startswith(f"PROGRESS | trials={k} | failures={s['failures']} |")
+
+
+@pytest.mark.gpu
+def test_cuda_devices_run_summary_equals_one_device(tmp_path):
+    """--cuda-devices splits the trial range over one context and host thread per listed
+    device (here device 0 twice: two contexts decoding concurrently on one GPU) and prints one
+    merged Run Summary: every key equals the single-context run's, and so does the histogram."""
+    args = ["--simulate", "--p", "0.05", "--trials", "20000", "--max-iter", "300", "--seed", "17", "--sampler",
+            "philox", "--precision", "fp32", "--engine", "resident", "--flip-hist", "5", "--batch", "4096"]
+    r1, s1 = run(args + ["--iter-hist-out", str(tmp_path / "h1.txt")])
+    r2, s2 = run(args + ["--cuda-devices", "0,0", "--iter-hist-out", str(tmp_path / "h2.txt")])
+    assert r1.returncode == 0 and r2.returncode == 0, r2.stderr
+    assert "devices=2" in r2.stdout
+    for k in SUMMARY_KEYS:
+        assert s1[k] == s2[k], k
+    rows = lambda p: [l for l in p.read_text().splitlines() if not l.startswith("#")]
+    assert rows(tmp_path / "h1.txt") == rows(tmp_path / "h2.txt")
+    assert int(s1["failures"]) > 0
