@@ -63,6 +63,9 @@ def parse_args():
     ap.add_argument("--sweep-trials", type=int, default=131072,
                     help="trials per p of the no-PP sweep p in {0.01, 0.025, 0.04}, FP32 resident against FP64 on "
                          "the same trials (0 = skip)")
+    ap.add_argument("--ablation-trials", type=int, default=32768,
+                    help="trials per p of the learned-proposal ablation at p 0.045/0.05/0.055: no proposal, the "
+                         "|LLR|-ordered proposal, the network (0 = skip)")
     ap.add_argument("--ler-p", type=float, default=0.05, help="error rate of the failure-bearing LER comparison")
     ap.add_argument("--ler-trials", type=int, default=131072,
                     help="trials of the LER comparison: this decoder against FP64 BP+PP on the same trials (0 = skip)")
@@ -556,6 +559,14 @@ def main():
         t0 = time.perf_counter()
         ler_check = ler_check_leg(dec, args, opts, 5 * 10 ** 9)
         ler_check["wall_s"] = round(time.perf_counter() - t0, 2)
+    ablation = None
+    if rank == 0 and args.ablation_trials > 0 and model is not None and args.precision == "fp32":
+        from joint_bp_plus_pp_b200.learned import ablation as learned_ablation
+        t0 = time.perf_counter()
+        ablation = {"points": learned_ablation(dec, trials=args.ablation_trials, max_iter=args.max_iter,
+                                               learned_from=args.learned_from),
+                    "wall_s": None}
+        ablation["wall_s"] = round(time.perf_counter() - t0, 2)
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_seconds > 0:
@@ -599,6 +610,7 @@ def main():
         "mixed_sizes_one_launch": mixed,
         "p_sweep": p_sweep,
         "ler_check": ler_check,
+        "learned_ablation": ablation,
         "clocks": clk,
         "step_ms": {"host_wall": step_wall, "kernel": step_kernel},
         "e2e": e2e,

@@ -79,6 +79,10 @@ typedef struct {
     int learned_from;      /* > 0: from this iteration on, a stalled trial (decisions unchanged or
                               oscillating) first tries the learned flip proposal set with
                               jbp_set_flip_model (resident engine, post-processing on); 0 = off */
+    int learned_order;     /* column order of that proposal: 0 = the model's scores (default);
+                              1 = the decoder's own |LLR| order (least reliable first), the same
+                              trigger, elimination and acceptance without the network -- the
+                              baseline the network is measured against; needs no model */
 } jbp_options;
 
 /* Per-trial outcome (16 bytes). */

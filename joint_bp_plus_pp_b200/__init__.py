@@ -43,7 +43,7 @@ class COptions(ctypes.Structure):
                 ("check_warmup", ctypes.c_int), ("check_interval", ctypes.c_int), ("slots", ctypes.c_int),
                 ("iters_per_launch", ctypes.c_int), ("watchdog_ms", ctypes.c_int), ("profile", ctypes.c_int),
                 ("use_prior", ctypes.c_int), ("prior", ctypes.c_double * 4), ("engine", ctypes.c_int),
-                ("p_max", ctypes.c_double), ("learned_from", ctypes.c_int)]
+                ("p_max", ctypes.c_double), ("learned_from", ctypes.c_int), ("learned_order", ctypes.c_int)]
 
 
 TRIAL_DTYPE = np.dtype([("iterations", np.int32), ("syndrome_ok", np.uint8), ("bp_ok", np.uint8),
@@ -94,13 +94,15 @@ class Options:
     engine: str = "auto"   # "auto", "resident" (shared-memory trial-resident tier) or "slots"
     learned_from: int = 0  # > 0: stalled trials try the learned flip proposal from this iteration
     p_max: float = 0.0     # > p: per-trial error rate uniform in [p, p_max) (simulate)
+    learned_order: str = "model"   # "model": the network's scores; "llr": |LLR| order (the baseline)
 
     def to_c(self):
         pr = (ctypes.c_double * 4)(*(self.prior or (0.0, 0.0, 0.0, 0.0)))
         return COptions(PREC[self.precision], self.max_iter, self.damping, self.flip_hist, int(self.enable_pp),
                         int(self.freeze_syn), self.check_warmup, self.check_interval, self.slots,
                         self.iters_per_launch, self.watchdog_ms, int(self.profile), int(self.prior is not None), pr,
-                        ENGINE[self.engine], float(self.p_max), int(self.learned_from))
+                        ENGINE[self.engine], float(self.p_max), int(self.learned_from),
+                        {"model": 0, "llr": 1}[self.learned_order])
 
 
 _lib = None

@@ -35,6 +35,7 @@ namespace {
 struct Args {
     std::string params, sx_path, sz_path, err_path, est_path, hist_out, progress_tsv, ets_dir;
     std::vector<int> devices;   // --cuda-devices: one context and host thread per entry
+    int learned_order = 0;      // --learned-order: 0 the model's scores, 1 |LLR| order
     std::string ets6_x, ets6_z, ets12_x, ets12_z, ets8_path4;
     double p = 0.05, damping = 0.0;
     int max_iter = 50, flip_hist = 5, device = 0, check_warmup = 0, check_interval = 1;
@@ -69,7 +70,8 @@ void usage(const char *prog) {
               << "  --slots N (trials in flight, 0 = auto)  --batch N (trials per GPU call, 262144)\n"
               << "  --ets-dir DIR (default: the params path without extension)\n"
               << "  --engine auto|resident|slots|table (auto)  --learned-from N (0 = off; learned flip proposal at\n"
-              << "  stalls from iteration N, resident engine with FP32 or FP16 messages)  --flip-model FILE.npy (default: the\n"
+              << "  stalls from iteration N, resident engine with FP32 or FP16 messages)  --learned-order model|llr (model:\n"
+              << "  columns by the network's scores; llr: by |LLR|, the baseline)  --flip-model FILE.npy (default: the\n"
               << "  shipped data/flip_mlp_params.npy next to the library)\n"
               << "  --checks FILE (a code as check lists instead of --params: 'n mx mz', then one line of\n"
               << "  variables per X check and per Z check)  --p-max P (per-trial p uniform in [p, P))\n"
@@ -180,6 +182,15 @@ int parse(int argc, char **argv, Args &a) {
             else if (f == "--no-pp") a.enable_pp = false;
             else if (f == "--cuda" || f == "--cuda-graph") {}
             else if (f == "--cuda-device") { VAL(); a.device = std::stoi(v); }
+            else if (f == "--learned-order") {
+                VAL();
+                if (v == "model") a.learned_order = 0;
+                else if (v == "llr") a.learned_order = 1;
+                else {
+                    std::cerr << "--learned-order must be model or llr\n";
+                    return 1;
+                }
+            }
             else if (f == "--cuda-devices") {
                 VAL();
                 a.devices.clear();
@@ -276,6 +287,7 @@ jbp_options options(const Args &a) {
     o.slots = a.slots;
     o.engine = a.engine;
     o.learned_from = a.learned_from;
+    o.learned_order = a.learned_order;
     o.p_max = a.p_max;
     // --iter-hist-out reports measured per-phase costs: time the slot engine's kernels
     if (!a.hist_out.empty()) o.profile = 1;
@@ -311,7 +323,7 @@ std::string load_npy_f32(const std::string &path, std::vector<float> &out, size_
 
 // Sets the learned flip model when --learned-from is given (the shipped model by default).
 int setup_flip_model(jbp_ctx *ctx, const Args &a, const char *argv0) {
-    if (a.learned_from <= 0) return 0;
+    if (a.learned_from <= 0 || a.learned_order == 1) return 0;   // the |LLR| order needs no model
     std::string path = a.flip_model;
     if (path.empty()) {
         // <repo>/joint_bp_plus_pp_b200/bin/jointbp_b200 -> ../data/flip_mlp_params.npy

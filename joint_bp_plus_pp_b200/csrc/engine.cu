@@ -315,7 +315,8 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     const int grid = static_cast<int>(std::min<long long>(static_cast<long long>(per_sm) * sm_count_, want));
     const int H = std::max(0, o.flip_hist);
     const bool learned = pp && o.learned_from > 0;
-    if (learned && !rq.collect && !has_mlp_) return "learned flip proposals requested but no model is set";
+    if (learned && !rq.collect && !has_mlp_ && o.learned_order == 0)
+        return "learned flip proposals requested but no model is set";
     const int R = std::max(H + 1, learned ? 6 : 3);   // the kernel's ring size
     size_t stride = 0;
     if (pp) {
@@ -372,6 +373,7 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     r.c2v_scratch = f32 ? res_c2v_scratch_ : nullptr;
     r.c2v_stride = c2v_stride;
     r.learned_from = learned ? o.learned_from : 0;
+    r.learned_order = o.learned_order;
     r.mlp.w = mlp_dev_;
     r.collect = rq.collect ? 1 : 0;
     r.col_x = rq.d_col_x;
@@ -546,6 +548,7 @@ std::string validate_options(const jbp_options &o, double p) {
     if (o.p_max > p && !(o.p_max < 1.0)) return "p_max must be below 1";
     if (o.engine < JBP_ENGINE_AUTO || o.engine > JBP_ENGINE_TABLE) return "unknown engine";
     if (o.watchdog_ms < 0) return "watchdog_ms must be >= 0";
+    if (o.learned_order < 0 || o.learned_order > 1) return "learned_order must be 0 (model) or 1 (|LLR|)";
     return "";
 }
 

@@ -95,6 +95,7 @@ struct ResRun {
     size_t c2v_stride;
     // learned flip proposal (mlp.cuh): tried at stalls from iteration learned_from (0 = off)
     int learned_from;
+    int learned_order;             // 0: the model's scores; 1: |LLR| order (no network)
     MlpDev mlp;
     int collect;                   // 1: record stall-state samples instead of proposing
     float *col_x, *col_y;          // [col_cap][8], [col_cap][2]
@@ -491,6 +492,29 @@ __device__ __forceinline__ ResPpPtrs res_pp_ptrs(const ResRun &run, unsigned cha
     return q;
 }
 
+// The proposal's solve: per side, the columns in ascending key order (key[side * n + v]) enter
+// the incremental GF(2) elimination of the OSD stage over at most kLearnedMaxCols of them; the
+// correction is kept only if unique, of weight <= 30 (the reference's OSD acceptance,
+// jointbp_ets.cpp:3056-3073) and both syndromes then match, with the corrected decisions
+// written into A's low bits.  Returns whether it was accepted.
+__device__ __forceinline__ bool res_learned_solve(const ResRun &run, const PpShared &psh, const PpScratch &psc,
+                                                  const double *key, float *A, int n) {
+    int left = 0;
+    for (int side = 0; side < 2; ++side) {
+        if (blk_side_diff(run.dc, psh, side) == 0) continue;
+        if (!blk_osd_side(run.dc, key + static_cast<size_t>(side) * n, psh, psc, side, kLearnedMaxCols)) ++left;
+    }
+    const bool accepted = left == 0;
+    if (accepted)
+        for (int v = threadIdx.x; v < n; v += blockDim.x) {
+            A[v] = with_bit(A[v], psh.est[v] & 1u);
+            A[n + v] = with_bit(A[n + v], (psh.est[v] >> 1) & 1u);
+        }
+    // a rejected proposal leaves nothing behind: later stages reload the estimate from the ring
+    __syncthreads();
+    return accepted;
+}
+
 // The learned flip proposal on the stalled state of iteration `it` (rare path, kept out of
 // line so that the BP loop's registers are not shaped by it).  In collection mode it records
 // the samples and returns false; otherwise it solves the proposed flip sets and returns true,
@@ -513,6 +537,15 @@ __device__ __noinline__ bool res_learned_attempt(const ResCode &code, const ResR
         psh.tgt[r] = static_cast<uint8_t>((syn[side * mw + (c >> 5)] >> (c & 31)) & 1u);
     }
     __syncthreads();
+    if (run.learned_order == 1 && !run.collect) {
+        // the ablation baseline: the same trigger, elimination and acceptance, with the columns
+        // in the decoder's own reliability order (ascending |LLR| of the current totals)
+        if (threadIdx.x == 0) atomicAdd(&run.cnt->learned_attempts, 1ull);
+        double *key = reinterpret_cast<double *>(feat);
+        res_abs_llr<P, J, L, ST>(code, c2v, c2vz, lp, key);
+        __syncthreads();
+        return res_learned_solve(run, psh, psc, key, A, n);
+    }
     res_features<P, J, L, ST>(code, run.dc, c2v, c2vz, A, lp, it, psh, feat);
     if (run.collect) {
         for (int v = threadIdx.x; v < n; v += blockDim.x) {
@@ -559,20 +592,7 @@ __device__ __noinline__ bool res_learned_attempt(const ResCode &code, const ResR
         key[n + v] = 1.0 / (1.0 + exp(static_cast<double>(logit[2 * v + 1])));
     }
     __syncthreads();
-    int left = 0;
-    for (int side = 0; side < 2; ++side) {
-        if (blk_side_diff(run.dc, psh, side) == 0) continue;
-        if (!blk_osd_side(run.dc, key + static_cast<size_t>(side) * n, psh, psc, side, kLearnedMaxCols)) ++left;
-    }
-    const bool accepted = left == 0;
-    if (accepted)
-        for (int v = threadIdx.x; v < n; v += blockDim.x) {
-            A[v] = with_bit(A[v], psh.est[v] & 1u);
-            A[n + v] = with_bit(A[n + v], (psh.est[v] >> 1) & 1u);
-        }
-    // a rejected proposal leaves nothing behind: later stages reload the estimate from the ring
-    __syncthreads();
-    return accepted;
+    return res_learned_solve(run, psh, psc, key, A, n);
 }
 
 // One post-processing pass (in-loop attempt or post-BP) on the decisions of iteration `it`

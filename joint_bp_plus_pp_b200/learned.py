@@ -7,6 +7,7 @@ MLP is then trained on the GPU by the library's own forward/backward kernels wit
 (jbp_mlp_train) and saved as FP32 parameters.
 
     python -m joint_bp_plus_pp_b200.learned --out data/flip_mlp_params.npy
+    python -m joint_bp_plus_pp_b200.learned ablation [--trials N] [--p P ...]   (what it adds)
 
 The default recipe decodes 100,000 seeded depolarizing trials at each p in {0.04, 0.045, 0.05,
 0.055} on the shipped [[9216,4612]] code (max-iter 100, flip-hist 5) and records the stalls from
@@ -43,7 +44,57 @@ def train(dec, x, y, epochs=12, batch=8192, lr=2e-3, pos_weight=4.0, seed=7):
     return params, hist
 
 
+def ablation(dec, ps=(0.045, 0.05, 0.055), trials=32768, seed=808, max_iter=1000, learned_from=6,
+             precision="fp32", flip_hist=5):
+    """What the learned proposal adds, on the same trials of the same decoder (FP32 trial-resident
+    BP with ETS / flip / OSD post-processing): (a) "none", no proposal; (b) "llr", the proposal's
+    trigger, elimination and acceptance with the columns in the decoder's own |LLR| order (least
+    reliable first); (c) "model", the same with the network's order.  Per p and variant:
+    trials/s (device time), failures with the Wilson interval, proposals tried and accepted,
+    accepted trials that succeed, and mean iterations of the accepted trials; per p, paired LER
+    differences of (c) against (b) and (a).  The set model is used for (c)."""
+    from . import paired_ler_difference, wilson_interval
+    base = dict(precision=precision, engine="resident", max_iter=max_iter, enable_pp=True, flip_hist=flip_hist)
+    variants = {"none": Options(**base),
+                "llr": Options(learned_from=learned_from, learned_order="llr", **base),
+                "model": Options(learned_from=learned_from, **base)}
+    out = []
+    for p in ps:
+        row = {"p": p, "trials": trials, "max_iter": max_iter, "learned_from": learned_from}
+        fails = {}
+        for name, o in variants.items():
+            dec.simulate(seed, 512, p, o, first_trial=10 ** 9, per_trial=False)   # warm-up
+            st, r = dec.simulate(seed, trials, p, o, first_trial=1)
+            acc = (r["ets_used_flags"] & 32) != 0
+            f = r["success"] == 0
+            fails[name] = f
+            tried = int(st["learned_attempts"])
+            row[name] = {"trials_per_s": trials / (st["device_ms"] / 1e3), "failures": int(f.sum()),
+                         "ci95": list(wilson_interval(trials, int(f.sum()))), "attempts": tried,
+                         "accepted": int(acc.sum()), "acceptance": int(acc.sum()) / tried if tried else None,
+                         "accepted_success": int(st["learned_success"]),
+                         "mean_iter_accepted": float(r["iterations"][acc].mean()) if acc.any() else None,
+                         "avg_iter": st["total_iters"] / trials}
+        for a, b in (("model", "llr"), ("model", "none"), ("llr", "none")):
+            d, lo, hi, n10, n01 = paired_ler_difference(fails[a], fails[b])
+            row[f"ler_{a}_minus_{b}"] = {"d": d, "ci95": [lo, hi], "fails_only_" + a: n10, "fails_only_" + b: n01}
+        out.append(row)
+    return out
+
+
 def main(argv=None):
+    if argv is None:
+        argv = sys.argv[1:]
+    if argv and argv[0] == "ablation":
+        ap = argparse.ArgumentParser(prog="python -m joint_bp_plus_pp_b200.learned ablation")
+        ap.add_argument("--trials", type=int, default=32768)
+        ap.add_argument("--p", type=float, nargs="+", default=[0.045, 0.05, 0.055])
+        ap.add_argument("--model", default=str(FLIP_MODEL_PATH))
+        a = ap.parse_args(argv[1:])
+        dec = Decoder.from_params()
+        dec.set_flip_model(np.load(a.model))
+        print(json.dumps(ablation(dec, ps=tuple(a.p), trials=a.trials), indent=1))
+        return 0
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(FLIP_MODEL_PATH))
     ap.add_argument("--trials-per-p", type=int, default=100000)
