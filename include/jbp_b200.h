@@ -83,6 +83,8 @@ typedef struct {
                               1 = the decoder's own |LLR| order (least reliable first), the same
                               trigger, elimination and acceptance without the network -- the
                               baseline the network is measured against; needs no model */
+    int learned_cols;      /* qubits (columns) of that proposal's GF(2) elimination, taken in the
+                              column order above (0 = 512) */
 } jbp_options;
 
 /* Per-trial outcome (16 bytes). */

@@ -374,6 +374,7 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     r.c2v_stride = c2v_stride;
     r.learned_from = learned ? o.learned_from : 0;
     r.learned_order = o.learned_order;
+    r.learned_cols = o.learned_cols > 0 ? std::min(o.learned_cols, rc.n) : kLearnedMaxCols;
     r.mlp.w = mlp_dev_;
     r.collect = rq.collect ? 1 : 0;
     r.col_x = rq.d_col_x;
@@ -549,6 +550,7 @@ std::string validate_options(const jbp_options &o, double p) {
     if (o.engine < JBP_ENGINE_AUTO || o.engine > JBP_ENGINE_TABLE) return "unknown engine";
     if (o.watchdog_ms < 0) return "watchdog_ms must be >= 0";
     if (o.learned_order < 0 || o.learned_order > 1) return "learned_order must be 0 (model) or 1 (|LLR|)";
+    if (o.learned_cols < 0) return "learned_cols must be >= 0";
     return "";
 }
 

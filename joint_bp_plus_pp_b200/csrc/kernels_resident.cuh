@@ -96,6 +96,7 @@ struct ResRun {
     // learned flip proposal (mlp.cuh): tried at stalls from iteration learned_from (0 = off)
     int learned_from;
     int learned_order;             // 0: the model's scores; 1: |LLR| order (no network)
+    int learned_cols;              // columns the proposal's elimination may use
     MlpDev mlp;
     int collect;                   // 1: record stall-state samples instead of proposing
     float *col_x, *col_y;          // [col_cap][8], [col_cap][2]
@@ -118,7 +119,7 @@ __device__ __forceinline__ unsigned long long dev_globaltimer() {
 
 constexpr int kLearnedTries = 3;   // learned proposals per trial at most
 constexpr int kLearnedMaxUnsat = 30;   // ... and only while max(us_x, us_z) is at most this
-constexpr int kLearnedMaxCols = 512;   // ... solved from at most this many of the best-scored qubits
+constexpr int kLearnedMaxCols = 512;   // ... solved from at most this many of the best-scored qubits (default)
 
 // Per-block global scratch of a post-processing run: the GF(2) work areas, the ring of the
 // last R iterations' decisions and the |LLR| keys of the OSD order.
@@ -493,7 +494,7 @@ __device__ __forceinline__ ResPpPtrs res_pp_ptrs(const ResRun &run, unsigned cha
 }
 
 // The proposal's solve: per side, the columns in ascending key order (key[side * n + v]) enter
-// the incremental GF(2) elimination of the OSD stage over at most kLearnedMaxCols of them; the
+// the incremental GF(2) elimination of the OSD stage over at most run.learned_cols of them; the
 // correction is kept only if unique, of weight <= 30 (the reference's OSD acceptance,
 // jointbp_ets.cpp:3056-3073) and both syndromes then match, with the corrected decisions
 // written into A's low bits.  Returns whether it was accepted.
@@ -502,7 +503,7 @@ __device__ __forceinline__ bool res_learned_solve(const ResRun &run, const PpSha
     int left = 0;
     for (int side = 0; side < 2; ++side) {
         if (blk_side_diff(run.dc, psh, side) == 0) continue;
-        if (!blk_osd_side(run.dc, key + static_cast<size_t>(side) * n, psh, psc, side, kLearnedMaxCols)) ++left;
+        if (!blk_osd_side(run.dc, key + static_cast<size_t>(side) * n, psh, psc, side, run.learned_cols)) ++left;
     }
     const bool accepted = left == 0;
     if (accepted)

@@ -45,22 +45,23 @@ def train(dec, x, y, epochs=12, batch=8192, lr=2e-3, pos_weight=4.0, seed=7):
 
 
 def ablation(dec, ps=(0.045, 0.05, 0.055), trials=32768, seed=808, max_iter=1000, learned_from=6,
-             precision="fp32", flip_hist=5):
+             precision="fp32", flip_hist=5, cols=0):
     """What the learned proposal adds, on the same trials of the same decoder (FP32 trial-resident
     BP with ETS / flip / OSD post-processing): (a) "none", no proposal; (b) "llr", the proposal's
     trigger, elimination and acceptance with the columns in the decoder's own |LLR| order (least
     reliable first); (c) "model", the same with the network's order.  Per p and variant:
     trials/s (device time), failures with the Wilson interval, proposals tried and accepted,
     accepted trials that succeed, and mean iterations of the accepted trials; per p, paired LER
-    differences of (c) against (b) and (a).  The set model is used for (c)."""
+    differences of (c) against (b) and (a).  The set model is used for (c); `cols` is the
+    proposal's column budget (0 = the default 512)."""
     from . import paired_ler_difference, wilson_interval
     base = dict(precision=precision, engine="resident", max_iter=max_iter, enable_pp=True, flip_hist=flip_hist)
     variants = {"none": Options(**base),
-                "llr": Options(learned_from=learned_from, learned_order="llr", **base),
-                "model": Options(learned_from=learned_from, **base)}
+                "llr": Options(learned_from=learned_from, learned_order="llr", learned_cols=cols, **base),
+                "model": Options(learned_from=learned_from, learned_cols=cols, **base)}
     out = []
     for p in ps:
-        row = {"p": p, "trials": trials, "max_iter": max_iter, "learned_from": learned_from}
+        row = {"p": p, "trials": trials, "max_iter": max_iter, "learned_from": learned_from, "cols": cols or 512}
         fails = {}
         for name, o in variants.items():
             dec.simulate(seed, 512, p, o, first_trial=10 ** 9, per_trial=False)   # warm-up
@@ -90,10 +91,11 @@ def main(argv=None):
         ap.add_argument("--trials", type=int, default=32768)
         ap.add_argument("--p", type=float, nargs="+", default=[0.045, 0.05, 0.055])
         ap.add_argument("--model", default=str(FLIP_MODEL_PATH))
+        ap.add_argument("--cols", type=int, nargs="+", default=[0], help="column budgets (0 = 512)")
         a = ap.parse_args(argv[1:])
         dec = Decoder.from_params()
         dec.set_flip_model(np.load(a.model))
-        print(json.dumps(ablation(dec, ps=tuple(a.p), trials=a.trials), indent=1))
+        print(json.dumps([ablation(dec, ps=tuple(a.p), trials=a.trials, cols=c) for c in a.cols], indent=1))
         return 0
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(FLIP_MODEL_PATH))
