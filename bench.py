@@ -29,6 +29,8 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 PARAMS = ROOT / "joint_bp_plus_pp_b200" / "data" / "H_P768_J3_L12_dmax3_nc0-3_1-2_seed11579811919164041.txt"
 REF_BIN = ROOT / "oracle" / "_ref" / "jointbp_ets"
+REF_CUDA = {"fp64": ROOT / "oracle" / "_ref" / "jointbp_ets_cuda", "fp32": ROOT / "oracle" / "_ref" / "jointbp_ets_cuda_fp32"}
+DROPIN_BIN = ROOT / "oracle" / "_ref" / "jointbp_ets_dropin"
 N_QUBITS, EDGES = 9216, 2 * 27648
 METRIC = "trials/s at p=0.04 (FP32+learned vs plain FP64 BP+PP, same GPU, equal LER)"
 UNIT = "trials/s"
@@ -66,6 +68,9 @@ def parse_args():
     ap.add_argument("--ablation-trials", type=int, default=32768,
                     help="trials per p of the learned-proposal ablation at p 0.045/0.05/0.055: no proposal, the "
                          "|LLR|-ordered proposal, the network (0 = skip)")
+    ap.add_argument("--ref-gpu-trials", type=int, default=1000,
+                    help="trials of each informative run of the reference's own CUDA path and of this repository's "
+                         "drop-in through the reference CLI (--cuda --no-pp; 0 = skip)")
     ap.add_argument("--ler-p", type=float, default=0.05, help="error rate of the failure-bearing LER comparison")
     ap.add_argument("--ler-trials", type=int, default=131072,
                     help="trials of the LER comparison: this decoder against FP64 BP+PP on the same trials (0 = skip)")
@@ -302,6 +307,35 @@ def ler_check_leg(dec, args, opts, first_trial):
             "interval": "paired Wald interval over the discordant trials",
             "fails_only_this": n10, "fails_only_fp64": n01,
             "outcome_disagreements": int((fa != fb).sum())}
+
+
+def reference_gpu_leg(args):
+    """Informative: the reference's own GPU path (cuda_bp_decode, jointbp_cuda.cu:681-1104, one
+    trial at a time, built unmodified for sm_100a in FP64 and in its FP32 form) against this
+    repository's drop-in for the same boundary (the unmodified reference CLI built with -DUSE_CUDA
+    and linked to lib/libjointbp_cuda.so), on the same command: --simulate --p 0.04 --max-iter 1000
+    --no-pp --cuda [--cuda-graph], the reference's mt19937_64 trials.  Rates are the CLI's own
+    Run Summary (trials / elapsed_s, host sampling included); failures and iterations come from
+    the same summary."""
+    out = {}
+    runs = [("reference_cuda_fp64", REF_CUDA["fp64"], []), ("reference_cuda_fp64_graph", REF_CUDA["fp64"], ["--cuda-graph"]),
+            ("reference_cuda_fp32", REF_CUDA["fp32"], []), ("reference_cuda_fp32_graph", REF_CUDA["fp32"], ["--cuda-graph"]),
+            ("dropin_fp64", DROPIN_BIN, [])]
+    for name, binary, extra in runs:
+        if not binary.exists():
+            out[name] = None
+            continue
+        cmd = [str(binary), "--params", str(PARAMS), "--simulate", "--p", "0.04", "--trials", str(args.ref_gpu_trials),
+               "--max-iter", "1000", "--no-pp", "--cuda", "--seed", str(args.seed), "--report-every", "0"] + extra
+        r = subprocess.run(cmd, capture_output=True, text=True, cwd=str(PARAMS.parent), timeout=600)
+        m = re.search(r"trials=(\d+) failures=(\d+).*?iters=(\d+).*?elapsed_s=([0-9.]+)s", r.stdout)
+        if r.returncode != 0 or not m or "falling back" in r.stderr:
+            out[name] = {"error": (r.stderr or r.stdout)[-300:]}
+            continue
+        t, f, it, el = int(m.group(1)), int(m.group(2)), int(m.group(3)), float(m.group(4))
+        out[name] = {"trials": t, "failures": f, "iters": it, "elapsed_s": el, "trials_per_s": t / el,
+                     "ms_per_trial": 1e3 * el / t}
+    return out
 
 
 def workload_name(args, decoder, learned_from=0):
@@ -559,6 +593,11 @@ def main():
         t0 = time.perf_counter()
         ler_check = ler_check_leg(dec, args, opts, 5 * 10 ** 9)
         ler_check["wall_s"] = round(time.perf_counter() - t0, 2)
+    ref_gpu = None
+    if rank == 0 and args.ref_gpu_trials > 0:
+        t0 = time.perf_counter()
+        ref_gpu = {"runs": reference_gpu_leg(args), "wall_s": None}
+        ref_gpu["wall_s"] = round(time.perf_counter() - t0, 2)
     ablation = None
     if rank == 0 and args.ablation_trials > 0 and model is not None and args.precision == "fp32":
         from joint_bp_plus_pp_b200.learned import ablation as learned_ablation
@@ -611,6 +650,7 @@ def main():
         "p_sweep": p_sweep,
         "ler_check": ler_check,
         "learned_ablation": ablation,
+        "informative": {"reference_gpu_path": ref_gpu},
         "clocks": clk,
         "step_ms": {"host_wall": step_wall, "kernel": step_kernel},
         "e2e": e2e,

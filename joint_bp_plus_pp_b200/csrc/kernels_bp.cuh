@@ -35,17 +35,37 @@ __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a,
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
 
-// normalize_msg (jointbp_ets.cpp:650-657)
+// Correctly rounded quotients m / s of several dividends by one divisor, with one reciprocal
+// instead of one division each.  Markstein's theorem (P. Markstein, "Computation of elementary
+// functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990; Handbook of
+// Floating-Point Arithmetic, the FMA-based division): with y = RN(1/s) and q = RN(m y) within one
+// ulp of m / s, the remainder r = m - s q is exact by one FMA and RN(q + r y) is RN(m / s) --
+// provided nothing underflows or overflows.  The guard keeps m >= 2^-900 and s <= 2^900 (the
+// quotients of a normalization are at most 1, so r and q stay normal); outside it, and for
+// NaN or infinite operands, the plain division runs.  The result is the IEEE quotient either
+// way, so the reference's divisions are reproduced bit for bit (tests/test_division.py checks
+// the sequence against IEEE division on the host).
+__device__ __forceinline__ double recip_for_div(double s) { return s <= 0x1p900 ? __ddiv_rn(1.0, s) : 0.0; }
+__device__ __forceinline__ double div_by_recip(double m, double s, double y) {
+    if (m >= 0x1p-900 && s <= 0x1p900) {
+        const double q = __dmul_rn(m, y);
+        return __fma_rn(__fma_rn(-s, q, m), y, q);
+    }
+    return __ddiv_rn(m, s);
+}
+
+// normalize_msg (jointbp_ets.cpp:650-657): each entry divided by ((m0 + m1) + m2) + m3
 __device__ __forceinline__ void norm4(double &m0, double &m1, double &m2, double &m3) {
     double s = dadd(dadd(dadd(m0, m1), m2), m3);
     if (s <= 0.0) {
         m0 = m1 = m2 = m3 = 0.25;
         return;
     }
-    m0 = ddiv(m0, s);
-    m1 = ddiv(m1, s);
-    m2 = ddiv(m2, s);
-    m3 = ddiv(m3, s);
+    const double y = recip_for_div(s);
+    m0 = div_by_recip(m0, s, y);
+    m1 = div_by_recip(m1, s, y);
+    m2 = div_by_recip(m2, s, y);
+    m3 = div_by_recip(m3, s, y);
 }
 
 __device__ __forceinline__ int warp_global_id() { return (blockIdx.x * blockDim.x + threadIdx.x) >> 5; }

@@ -195,16 +195,17 @@ __host__ __device__ inline size_t res_smem_bytes(int n, int m, int L, size_t sto
 // The check rule on one check of L edges: from the edges' variable-to-check inputs in(l) and
 // the check's syndrome bit, out(l, c2v of edge l) for l = 0 .. L-1.
 //
-// Stable tanh rule.  Per edge u = 2^-|y|, N = 1 - u, D = 1 + u, t = N / D.  A set of edges is
-// carried as (PN, H) with PN = prod N and H = (prod D - prod N) / 2, so prod D = PN + 2H and
-// 1 - T = 2H / prod D.  Joining a set with one edge, H' = D H + u PN = H + u (H + PN) and
-// PN' = PN - u PN: sums of positive terms and one rounding each, which keep full relative
-// precision however close T is to 1.  A single edge has H = u exactly, and H of any set is at
-// least the largest u in it; joining two sets a, b: H = PD_a H_b + PN_b H_a.  The output
-// magnitude log2((1 + T) / (1 - T)) over the other edges is log2(1 + PN / H): it grows like
-// min |y| instead of saturating where 1 - T rounds to zero.  H is zero only when every other
-// edge has u = 0 (|y| above 126), and then PN = 1: the output is +inf before the clamp to
-// kResCmax, as it is whenever all other edges are that reliable, so no input clamp is needed.
+// Stable tanh rule.  Per edge u = 2^-|y|, N = 1 - u, D = 1 + u, t = N / D, so the product of a
+// set's t is T = PN / PD with PN = prod N, PD = prod D.  A set is carried as (H, G) with
+// H = (PD - PN) / 2 and G = (PD + PN) / 2: the empty set is (0, 1), a single edge (u, 1), and
+// joining a set with one edge gives H' = H + u G, G' = G + u H -- sums of positive terms with
+// one rounding each, which keep full relative precision however close T is to 1.  Joining two
+// sets a, b: H = G_a H_b + H_a G_b, G = G_a G_b + H_a H_b.  The output magnitude
+// log2((1 + T) / (1 - T)) over the other edges of a check is log2(G / H) of the set they form: it
+// grows like min |y| instead of saturating where 1 - T rounds to zero.  H is zero only when every
+// other edge has u = 0 (|y| above 126); the output is then +inf before the clamp to kResCmax, as
+// it is whenever all other edges are that reliable, so no input clamp is needed.  (G >= H, so the
+// magnitude is >= 0; its absolute value removes a rounding of G / H to just below 1.)
 template <int L, class In, class Out>
 __device__ __forceinline__ void res_row_rule(In in, unsigned sbit, Out out) {
     float u[L];
@@ -218,27 +219,28 @@ __device__ __forceinline__ void res_row_rule(In in, unsigned sbit, Out out) {
         u[l] = __uint_as_float(__float_as_uint(res_ex2(-fabsf(v))) | sv);
     }
     // suffix sets {l, .., L-1}
-    float sPN[L + 1], sH[L + 1];
-    sPN[L] = 1.0f;
+    float sH[L + 1], sG[L + 1];
     sH[L] = 0.0f;
+    sG[L] = 1.0f;
 #pragma unroll
     for (int l = L - 1; l >= 0; --l) {
         const float au = fabsf(u[l]);
-        sH[l] = fmaf(au, sH[l + 1] + sPN[l + 1], sH[l + 1]);
-        sPN[l] = fmaf(-au, sPN[l + 1], sPN[l + 1]);
+        sH[l] = fmaf(au, sG[l + 1], sH[l + 1]);
+        sG[l] = fmaf(au, sH[l + 1], sG[l + 1]);
     }
     sgn ^= sbit << 31;
     // prefix set {0, .., l-1} joined with the suffix {l+1, .., L-1}
-    float pPN = 1.0f, pH = 0.0f;
+    float pH = 0.0f, pG = 1.0f;
 #pragma unroll
     for (int l = 0; l < L; ++l) {
-        const float ePN = pPN * sPN[l + 1];
-        const float eH = fmaf(fmaf(2.0f, pH, pPN), sH[l + 1], sPN[l + 1] * pH);
-        const float mag = fminf(res_lg2(fmaf(ePN, res_rcp(eH), 1.0f)), kResCmax);
+        const float eG = fmaf(pG, sG[l + 1], pH * sH[l + 1]);
+        const float eH = fmaf(pG, sH[l + 1], pH * sG[l + 1]);
+        const float mag = fminf(fabsf(res_lg2(eG * res_rcp(eH))), kResCmax);
         out(l, __uint_as_float(__float_as_uint(mag) ^ ((sgn ^ __float_as_uint(u[l])) & 0x80000000u)));
         const float au = fabsf(u[l]);
-        pH = fmaf(au, pH + pPN, pH);
-        pPN = fmaf(-au, pPN, pPN);
+        const float nH = fmaf(au, pG, pH);
+        pG = fmaf(au, pH, pG);
+        pH = nH;
     }
 }
 
