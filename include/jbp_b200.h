@@ -85,6 +85,9 @@ typedef struct {
                               baseline the network is measured against; needs no model */
     int learned_cols;      /* qubits (columns) of that proposal's GF(2) elimination, taken in the
                               column order above (0 = 512) */
+    int collect_every;     /* jbp_collect_stall_states: of the qubits that are next to no
+                              unsatisfied check and whose estimate is right, record 1 in this many
+                              (0 = 32; 1 = every qubit, a sample without selection bias) */
 } jbp_options;
 
 /* Per-trial outcome (16 bytes). */
@@ -225,8 +228,9 @@ int jbp_set_flip_model(jbp_ctx *ctx, const float *params);
 /* Training data: runs the Monte Carlo like jbp_simulate (resident engine, post-processing on,
  * opt->learned_from > 0 gives the first stall iteration) and, at every stall where the learned
  * proposal would run, records the features and labels (x-bit / z-bit of error xor estimate) of
- * the qubits next to an unsatisfied check, the qubits whose estimate is wrong and 1 in 32 of
- * the others, up to `capacity` samples.  Decoding itself is unchanged. */
+ * the qubits next to an unsatisfied check, the qubits whose estimate is wrong and 1 in
+ * opt->collect_every (0 = 32) of the others, up to `capacity` samples; stats->learned_attempts
+ * counts the stalls recorded.  Decoding itself is unchanged. */
 int jbp_collect_stall_states(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed, long long first_trial,
                              long long ntrials, double p, int sampler, long long capacity, float *x_out, float *y_out,
                              long long *count_out, jbp_stats *stats);

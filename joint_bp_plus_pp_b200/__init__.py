@@ -44,7 +44,7 @@ class COptions(ctypes.Structure):
                 ("iters_per_launch", ctypes.c_int), ("watchdog_ms", ctypes.c_int), ("profile", ctypes.c_int),
                 ("use_prior", ctypes.c_int), ("prior", ctypes.c_double * 4), ("engine", ctypes.c_int),
                 ("p_max", ctypes.c_double), ("learned_from", ctypes.c_int), ("learned_order", ctypes.c_int),
-                ("learned_cols", ctypes.c_int)]
+                ("learned_cols", ctypes.c_int), ("collect_every", ctypes.c_int)]
 
 
 TRIAL_DTYPE = np.dtype([("iterations", np.int32), ("syndrome_ok", np.uint8), ("bp_ok", np.uint8),
@@ -97,6 +97,7 @@ class Options:
     p_max: float = 0.0     # > p: per-trial error rate uniform in [p, p_max) (simulate)
     learned_order: str = "model"   # "model": the network's scores; "llr": |LLR| order (the baseline)
     learned_cols: int = 0  # qubits the proposal's elimination may use, in that order (0 = 512)
+    collect_every: int = 0  # stall-state collection: 1 in this many quiet, correct qubits (0 = 32)
 
     def to_c(self):
         pr = (ctypes.c_double * 4)(*(self.prior or (0.0, 0.0, 0.0, 0.0)))
@@ -104,7 +105,8 @@ class Options:
                         int(self.freeze_syn), self.check_warmup, self.check_interval, self.slots,
                         self.iters_per_launch, self.watchdog_ms, int(self.profile), int(self.prior is not None), pr,
                         ENGINE[self.engine], float(self.p_max), int(self.learned_from),
-                        {"model": 0, "llr": 1}[self.learned_order], int(self.learned_cols))
+                        {"model": 0, "llr": 1}[self.learned_order], int(self.learned_cols),
+                        int(self.collect_every))
 
 
 _lib = None

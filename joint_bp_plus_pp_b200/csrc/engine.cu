@@ -377,6 +377,7 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     r.learned_cols = o.learned_cols > 0 ? std::min(o.learned_cols, rc.n) : kLearnedMaxCols;
     r.mlp.w = mlp_dev_;
     r.collect = rq.collect ? 1 : 0;
+    r.collect_every = o.collect_every > 0 ? static_cast<unsigned>(o.collect_every) : 32u;
     r.col_x = rq.d_col_x;
     r.col_y = rq.d_col_y;
     r.col_count = rq.d_col_count;
@@ -551,6 +552,7 @@ std::string validate_options(const jbp_options &o, double p) {
     if (o.watchdog_ms < 0) return "watchdog_ms must be >= 0";
     if (o.learned_order < 0 || o.learned_order > 1) return "learned_order must be 0 (model) or 1 (|LLR|)";
     if (o.learned_cols < 0) return "learned_cols must be >= 0";
+    if (o.collect_every < 0) return "collect_every must be >= 0";
     return "";
 }
 

@@ -99,6 +99,7 @@ struct ResRun {
     int learned_cols;              // columns the proposal's elimination may use
     MlpDev mlp;
     int collect;                   // 1: record stall-state samples instead of proposing
+    unsigned collect_every;        // ... 1 in this many of the quiet, correctly decided qubits
     float *col_x, *col_y;          // [col_cap][8], [col_cap][2]
     unsigned long long *col_count;
     long long col_cap;
@@ -551,12 +552,13 @@ __device__ __noinline__ bool res_learned_attempt(const ResCode &code, const ResR
     }
     res_features<P, J, L, ST>(code, run.dc, c2v, c2vz, A, lp, it, psh, feat);
     if (run.collect) {
+        if (threadIdx.x == 0) atomicAdd(&run.cnt->learned_attempts, 1ull);   // stalls recorded
         for (int v = threadIdx.x; v < n; v += blockDim.x) {
             const float *f = feat + static_cast<size_t>(v) * kMlpIn;
             const unsigned lab = have_err ? (err[v] ^ psh.est[v]) : 0u;
             const unsigned h = static_cast<unsigned>(splitmix64(static_cast<unsigned long long>(t) * 1315423911ull +
                                                                 static_cast<unsigned long long>(it) * 9216ull + v));
-            if (!(lab || f[6] + f[7] > 0.0f || (h & 31u) == 0u)) continue;
+            if (!(lab || f[6] + f[7] > 0.0f || h % run.collect_every == 0u)) continue;
             const unsigned long long q = atomicAdd(run.col_count, 1ull);
             if (q >= static_cast<unsigned long long>(run.col_cap)) continue;
             for (int kk = 0; kk < kMlpIn; ++kk) run.col_x[q * kMlpIn + kk] = f[kk];

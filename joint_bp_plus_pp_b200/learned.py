@@ -26,15 +26,19 @@ from . import Decoder, Options, mlp_init, FLIP_MODEL_PATH
 
 
 def collect(dec, ps=(0.04, 0.045, 0.05, 0.055), trials_per_p=100000, max_iter=100, learned_from=6,
-            capacity=2_000_000, seed=20240, flip_hist=5):
+            capacity=2_000_000, seed=20240, flip_hist=5, every=32, precision="fp16"):
+    """Stalled states of the decoder itself: at each stall (up to 3 per trial), the qubits next
+    to an unsatisfied check, the qubits whose estimate is wrong, and 1 in `every` of the others
+    (every = 1: all qubits, so that the labels' rates are those the decoder meets)."""
     xs, ys, info = [], [], []
-    o = Options(precision="fp16", engine="resident", max_iter=max_iter, enable_pp=True, flip_hist=flip_hist,
-                learned_from=learned_from)
+    o = Options(precision=precision, engine="resident", max_iter=max_iter, enable_pp=True, flip_hist=flip_hist,
+                learned_from=learned_from, collect_every=every)
     for i, p in enumerate(ps):
         x, y, st = dec.collect_stall_states(seed + i, trials_per_p, p, o, capacity, first_trial=1)
         xs.append(x)
         ys.append(y)
-        info.append({"p": p, "trials": st["trials"], "samples": len(x), "failures": st["failures"]})
+        info.append({"p": p, "trials": st["trials"], "samples": len(x), "failures": st["failures"],
+                     "stalls": int(st["learned_attempts"]) if "learned_attempts" in st else None})
     return np.concatenate(xs), np.concatenate(ys), info
 
 
@@ -103,17 +107,25 @@ def main(argv=None):
     ap.add_argument("--epochs", type=int, default=12)
     ap.add_argument("--learned-from", type=int, default=6)
     ap.add_argument("--report", default=None, help="JSON summary of the run")
+    ap.add_argument("--p", type=float, nargs="+", default=[0.04, 0.045, 0.05, 0.055])
+    ap.add_argument("--collect-every", type=int, default=32,
+                    help="record 1 in this many of the quiet, correctly decided qubits (1 = all)")
+    ap.add_argument("--capacity", type=int, default=2_000_000, help="samples kept per p at most")
+    ap.add_argument("--pos-weight", type=float, default=4.0)
+    ap.add_argument("--max-iter", type=int, default=100)
     a = ap.parse_args(argv)
     dec = Decoder.from_params()
     t0 = time.time()
-    x, y, info = collect(dec, trials_per_p=a.trials_per_p, learned_from=a.learned_from)
+    x, y, info = collect(dec, ps=tuple(a.p), trials_per_p=a.trials_per_p, learned_from=a.learned_from,
+                         every=a.collect_every, capacity=a.capacity, max_iter=a.max_iter)
     t1 = time.time()
-    params, hist = train(dec, x, y, epochs=a.epochs)
+    params, hist = train(dec, x, y, epochs=a.epochs, pos_weight=a.pos_weight)
     t2 = time.time()
     np.save(a.out, params)
     rep = {"samples": int(len(x)), "positives_x": int(y[:, 0].sum()), "positives_z": int(y[:, 1].sum()),
            "collect": info, "collect_s": t1 - t0, "train_s": t2 - t1, "epoch_loss": [float(v) for v in hist],
-           "learned_from": a.learned_from}
+           "learned_from": a.learned_from, "collect_every": a.collect_every, "pos_weight": a.pos_weight,
+           "max_iter": a.max_iter}
     print(json.dumps(rep))
     if a.report:
         Path(a.report).write_text(json.dumps(rep, indent=1))
