@@ -321,13 +321,16 @@ class Decoder:
             _check(self._lib, self._lib.jbp_set_flip_model(self._h, None))
             return
         prm = np.ascontiguousarray(params, np.float32)
-        assert prm.size == MLP_PARAMS
+        if prm.size != MLP_PARAMS:
+            raise ValueError(f"flip model has {prm.size} parameters, this library's network takes {MLP_PARAMS}")
         _check(self._lib, self._lib.jbp_set_flip_model(self._h, _ptr(prm)))
 
     def mlp_grad(self, params, x, y, pos_weight=1.0):
-        """GPU gradient and mean loss of the flip-proposal MLP on samples (x: n x 8, y: n x 2)."""
+        """GPU gradient and mean loss of the flip-proposal MLP on samples (x: n x MLP_IN, y: n x 2)."""
         prm = np.ascontiguousarray(params, np.float32)
         x = np.ascontiguousarray(x, np.float32)
+        if x.ndim != 2 or x.shape[1] != MLP_IN:
+            raise ValueError(f"features must be n x {MLP_IN}")
         y = np.ascontiguousarray(y, np.float32)
         g = np.zeros(MLP_PARAMS, np.float32)
         loss = ctypes.c_double()
@@ -339,6 +342,8 @@ class Decoder:
         """Adam training on the GPU; returns (params, per-epoch mean loss)."""
         prm = np.array(params, np.float32)
         x = np.ascontiguousarray(x, np.float32)
+        if x.ndim != 2 or x.shape[1] != MLP_IN:
+            raise ValueError(f"features must be n x {MLP_IN}")
         y = np.ascontiguousarray(y, np.float32)
         hist = np.zeros(max(1, epochs), np.float64)
         _check(self._lib, self._lib.jbp_mlp_train(self._h, _ptr(prm), len(x), _ptr(x), _ptr(y), epochs, batch, lr,
@@ -349,13 +354,15 @@ class Decoder:
         """BF16 tensor-core inference (the decoder's fused kernel code): logits n x 2."""
         prm = np.ascontiguousarray(params, np.float32)
         x = np.ascontiguousarray(x, np.float32)
+        if x.ndim != 2 or x.shape[1] != MLP_IN:
+            raise ValueError(f"features must be n x {MLP_IN}")
         out = np.zeros((len(x), 2), np.float32)
         _check(self._lib, self._lib.jbp_mlp_infer(self._h, _ptr(prm), len(x), _ptr(x), _ptr(out)))
         return out
 
     def collect_stall_states(self, seed, ntrials, p, opts, capacity, first_trial=1, sampler="philox"):
         """Features and labels of the qubits of stalled BP states (training data)."""
-        x = np.zeros((capacity, 8), np.float32)
+        x = np.zeros((capacity, MLP_IN), np.float32)
         y = np.zeros((capacity, 2), np.float32)
         cnt = ctypes.c_longlong()
         st = CStats()
@@ -409,6 +416,7 @@ def simulate_mixed(decoders, ntrials, p, opts=None, seeds=None, first_trial=None
     return [s.as_dict() for s in stats], res
 
 
+MLP_IN = 8        # features per qubit of the flip-proposal MLP (include/jbp_b200.h)
 MLP_PARAMS = 4866
 FLIP_MODEL_PATH = DATA_DIR / "flip_mlp_params.npy"
 
@@ -416,7 +424,7 @@ FLIP_MODEL_PATH = DATA_DIR / "flip_mlp_params.npy"
 def mlp_init(seed=0):
     """He-initialised parameters of the flip-proposal MLP (W1, b1, W2, b2, W3, b3)."""
     rng = np.random.default_rng(seed)
-    w1 = rng.normal(0, (2 / 8) ** 0.5, (64, 8))
+    w1 = rng.normal(0, (2 / MLP_IN) ** 0.5, (64, MLP_IN))
     w2 = rng.normal(0, (2 / 64) ** 0.5, (64, 64))
     w3 = rng.normal(0, (1 / 64) ** 0.5, (2, 64))
     return np.concatenate([w1.ravel(), np.zeros(64), w2.ravel(), np.zeros(64), w3.ravel(), np.full(2, -3.0)]).astype(

@@ -10,6 +10,7 @@
 #include "../../include/jbp_b200.h"
 #include "ctx.hpp"
 #include "engine.hpp"
+#include "mlp.cuh"
 
 namespace {
 
@@ -387,7 +388,7 @@ int jbp_collect_stall_states(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed
     cudaSetDevice(ctx->engine.device());
     float *dx = nullptr, *dy = nullptr;
     unsigned long long *dc = nullptr;
-    cudaError_t ce = cudaMalloc(&dx, sizeof(float) * 8 * capacity);
+    cudaError_t ce = cudaMalloc(&dx, sizeof(float) * jbp::kMlpIn * capacity);
     if (ce == cudaSuccess) ce = cudaMalloc(&dy, sizeof(float) * 2 * capacity);
     if (ce == cudaSuccess) ce = cudaMalloc(&dc, sizeof(unsigned long long));
     if (ce == cudaSuccess) ce = cudaMemsetAsync(dc, 0, sizeof(unsigned long long), ctx->stream);
@@ -405,7 +406,7 @@ int jbp_collect_stall_states(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed
     if (e.empty()) {
         ce = cudaMemcpy(&cnt, dc, sizeof(cnt), cudaMemcpyDeviceToHost);
         const long long keep = std::min<long long>(static_cast<long long>(cnt), capacity);
-        if (ce == cudaSuccess && keep > 0) ce = cudaMemcpy(x_out, dx, sizeof(float) * 8 * keep, cudaMemcpyDeviceToHost);
+        if (ce == cudaSuccess && keep > 0) ce = cudaMemcpy(x_out, dx, sizeof(float) * jbp::kMlpIn * keep, cudaMemcpyDeviceToHost);
         if (ce == cudaSuccess && keep > 0) ce = cudaMemcpy(y_out, dy, sizeof(float) * 2 * keep, cudaMemcpyDeviceToHost);
         if (ce != cudaSuccess) e = jbp::cuda_err(ce, "copy collection");
         *count_out = keep;

@@ -116,6 +116,9 @@ void fill_stats(const DevCounters &hc, jbp_stats &stats) {
 }  // namespace
 
 Engine::~Engine() {
+    if (slot_graph_.exec) cudaGraphExecDestroy(slot_graph_.exec);
+    for (cudaEvent_t ev : run_ev_)
+        if (ev) cudaEventDestroy(ev);
     cudaFree(res_c2v_scratch_);
     cudaFree(mix_scratch_);
     cudaFree(mix_cnt_);
@@ -702,12 +705,13 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     const int sample_grid = sm_count_ * 4;
     long long launches = 0;
 
-    cudaEvent_t ev0, ev1;
-    JBP_CUDA_TRY(cudaEventCreate(&ev0), "cudaEventCreate");
-    JBP_CUDA_TRY(cudaEventCreate(&ev1), "cudaEventCreate");
-    cudaEvent_t poll_ev[2];
-    JBP_CUDA_TRY(cudaEventCreateWithFlags(&poll_ev[0], cudaEventDisableTiming), "cudaEventCreate");
-    JBP_CUDA_TRY(cudaEventCreateWithFlags(&poll_ev[1], cudaEventDisableTiming), "cudaEventCreate");
+    if (!run_ev_[0]) {
+        for (int i = 0; i < 2; ++i) JBP_CUDA_TRY(cudaEventCreate(&run_ev_[i]), "cudaEventCreate");
+        for (int i = 2; i < 4; ++i)
+            JBP_CUDA_TRY(cudaEventCreateWithFlags(&run_ev_[i], cudaEventDisableTiming), "cudaEventCreate");
+    }
+    cudaEvent_t ev0 = run_ev_[0], ev1 = run_ev_[1];
+    cudaEvent_t poll_ev[2] = {run_ev_[2], run_ev_[3]};
 
     auto enqueue_refill = [&](cudaStream_t s) {
         cudaMemsetAsync(r.n_fresh, 0, sizeof(int), s);
@@ -766,20 +770,68 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     int GI = o.iters_per_launch > 0 ? o.iters_per_launch : 4;
     GI = std::min(GI, o.max_iter);
     const bool prof = o.profile != 0;
+    // Without profiling (events) or a run budget (a host check between launches), the whole run
+    // is one launch: a graph whose while node repeats one BP iteration until every trial is
+    // classified (k_loop_cond), so the host neither polls nor launches graphs that find nothing
+    // left to do -- what a one-trial call (cuda_bp_decode) spends most of its time on otherwise.
+    const bool device_loop = !prof && o.watchdog_ms <= 0;
+    if (device_loop) GI = 1;
+    const long long max_iters_total =
+        (rq.ntrials * static_cast<long long>(o.max_iter)) / std::max(1, S) + 2LL * o.max_iter + 2 * GI + 8;
     const int nsets = prof ? 2 : 1;
     // events per iteration: before the check kernel, before the variable kernel, after it, and
     // around the syndrome-test kernel
     constexpr int kEv = 5;
     std::vector<cudaEvent_t> pev(prof ? 2 * GI * kEv : 0);
     for (auto &ev : pev) JBP_CUDA_TRY(cudaEventCreate(&ev), "cudaEventCreate");
-    cudaStream_t cap;
-    JBP_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "cudaStreamCreate");
     cudaGraph_t graph[2] = {nullptr, nullptr};
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     const long long launches_before = launches;
     long long per_graph = 0;
     cudaError_t ce = cudaSuccess;
-    for (int set = 0; set < nsets && ce == cudaSuccess; ++set) {
+    // reuse the last run's graph when every launch parameter is the same
+    SlotGraph &sg = slot_graph_;
+    const bool reuse = !prof && sg.valid && sg.precision == o.precision && sg.damping == o.damping && sg.GI == GI &&
+                       sg.device_loop == device_loop && sg.llr_out == (rq.d_llr_out != nullptr) &&
+                       std::memcmp(&sg.r, &r, sizeof(DevRun)) == 0 && std::memcmp(&sg.msg, &msg, sizeof(DevMsgs)) == 0;
+    cudaStream_t cap = nullptr;
+    if (reuse) {
+        exec[0] = sg.exec;
+        per_graph = sg.per_graph;
+    } else {
+        JBP_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "cudaStreamCreate");
+    }
+    if (!reuse && device_loop) {
+        // graph = while(cond) { one iteration; k_loop_cond }
+        cudaGraph_t g = nullptr;
+        cudaGraphConditionalHandle h{};
+        ce = cudaGraphCreate(&g, 0);
+        if (ce == cudaSuccess) ce = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t wn = nullptr;
+        if (ce == cudaSuccess) ce = cudaGraphAddNode(&wn, g, nullptr, 0, &np);
+        if (ce == cudaSuccess) {
+            cudaGraph_t body = np.conditional.phGraph_out[0];
+            launches = launches_before;
+            ce = cudaStreamBeginCaptureToGraph(cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+            if (ce == cudaSuccess) {
+                enqueue_iteration(cap, nullptr);
+                k_loop_cond<<<1, 32, 0, cap>>>(h, r.cnt, r.it, static_cast<unsigned long long>(rq.ntrials),
+                                               static_cast<int>(std::min<long long>(max_iters_total + 2, 1 << 30)));
+                launches += 1;
+                cudaGraph_t captured = nullptr;
+                ce = cudaStreamEndCapture(cap, &captured);
+            }
+            per_graph = launches - launches_before;   // kernels per iteration
+        }
+        if (ce == cudaSuccess) ce = cudaGraphInstantiate(&exec[0], g, 0);
+        if (g) cudaGraphDestroy(g);
+    }
+    for (int set = 0; set < nsets && ce == cudaSuccess && !reuse && !device_loop; ++set) {
         launches = launches_before;
         ce = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
         if (ce != cudaSuccess) break;
@@ -790,6 +842,20 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
         ce = cudaStreamEndCapture(cap, &graph[set]);
         if (ce == cudaSuccess) ce = cudaGraphInstantiate(&exec[set], graph[set], 0);
         per_graph = launches - launches_before;
+    }
+    if (!reuse && !prof && ce == cudaSuccess) {
+        // keep this graph for the next run with the same parameters
+        if (sg.exec) cudaGraphExecDestroy(sg.exec);
+        sg.valid = true;
+        sg.r = r;
+        sg.msg = msg;
+        sg.precision = o.precision;
+        sg.damping = o.damping;
+        sg.GI = GI;
+        sg.device_loop = device_loop;
+        sg.llr_out = rq.d_llr_out != nullptr;
+        sg.exec = exec[0];
+        sg.per_graph = per_graph;
     }
     launches = launches_before;
     double check_ms = 0.0, var_ms = 0.0, test_ms = 0.0;
@@ -812,8 +878,6 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
         }
     };
 
-    const long long max_iters_total =
-        (rq.ntrials * static_cast<long long>(o.max_iter)) / std::max(1, S) + 2LL * o.max_iter + 2 * GI + 8;
     const long long max_graphs = max_iters_total / GI + 2;
     auto t0 = std::chrono::steady_clock::now();
     std::string err;
@@ -821,6 +885,25 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     if (ce != cudaSuccess) err = cuda_err(ce, "graph capture");
     long long g = 0;
     bool finished = false;
+    if (device_loop && err.empty()) {
+        // one launch; the iterations it ran are read back with the completion count
+        int *h_it = reinterpret_cast<int *>(&buf_.h_done[1]);
+        ce = cudaGraphLaunch(exec[0], st);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(&buf_.h_done[0], &buf_.cnt->done, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                 st);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(h_it, buf_.it, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaEventRecord(poll_ev[0], st);
+        if (ce == cudaSuccess) ce = cudaEventSynchronize(poll_ev[0]);
+        if (ce != cudaSuccess) {
+            err = cuda_err(ce, "run");
+        } else {
+            launches += per_graph * std::max(0, *h_it - 1);
+            finished = buf_.h_done[0] >= static_cast<unsigned long long>(rq.ntrials);
+            if (!finished) err = "run did not complete within the iteration bound (internal error)";
+        }
+        g = max_graphs;   // the polling loop below has nothing to do
+    }
     for (; err.empty() && g < max_graphs && !finished; ++g) {
         ce = cudaGraphLaunch(exec[g % nsets], st);
         if (ce != cudaSuccess) { err = cuda_err(ce, "graph launch"); break; }
@@ -842,7 +925,7 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
             }
         }
     }
-    if (err.empty() && !finished && !timed_out && g >= 1) {
+    if (err.empty() && !finished && !timed_out && g >= 1 && !device_loop) {
         ce = cudaEventSynchronize(poll_ev[(g - 1) & 1]);
         if (ce == cudaSuccess && buf_.h_done[(g - 1) & 1] >= static_cast<unsigned long long>(rq.ntrials)) finished = true;
         if (!finished) err = "run did not complete within the iteration bound (internal error)";
@@ -850,7 +933,7 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     cudaEventRecord(ev1, st);
     ce = cudaEventSynchronize(ev1);
     if (err.empty() && ce != cudaSuccess) err = cuda_err(ce, "run");
-    if (err.empty() && g >= 1) read_profile(g - 1);
+    if (err.empty() && g >= 1 && prof) read_profile(g - 1);
     if (err.empty()) {
         ce = cudaGetLastError();
         if (ce != cudaSuccess) err = cuda_err(ce, "run");
@@ -867,15 +950,11 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
         err = "watchdog expired: the run budget of " + std::to_string(o.watchdog_ms) + " ms ran out (host check) after " +
               std::to_string(hc.done) + " of " + std::to_string(rq.ntrials) + " trials";
     for (int set = 0; set < 2; ++set) {
-        if (exec[set]) cudaGraphExecDestroy(exec[set]);
+        if (exec[set] && !(sg.valid && exec[set] == sg.exec)) cudaGraphExecDestroy(exec[set]);
         if (graph[set]) cudaGraphDestroy(graph[set]);
     }
     for (auto &ev : pev) cudaEventDestroy(ev);
-    cudaStreamDestroy(cap);
-    cudaEventDestroy(ev0);
-    cudaEventDestroy(ev1);
-    cudaEventDestroy(poll_ev[0]);
-    cudaEventDestroy(poll_ev[1]);
+    if (cap) cudaStreamDestroy(cap);
     if (!err.empty() && !timeout_err) return err;
     if (hc.bad_input) return "error vector has invalid value";
     fill_stats(hc, stats);

@@ -116,6 +116,23 @@ private:
     // the neighbour tables of the mixed launch, built on first use
     std::string mixed_slots();
 
+    // The slot engine's instantiated CUDA graph of its last run without profiling, reused by a
+    // run whose launch parameters are byte for byte the same (the per-trial calls of a
+    // cuda_bp_decode loop decode through the same staging buffers): capturing and
+    // instantiating a graph costs more than decoding one trial.
+    struct SlotGraph {
+        bool valid = false;
+        DevRun r{};
+        DevMsgs msg{};
+        int precision = -1, GI = 0;
+        double damping = 0.0;
+        bool llr_out = false, device_loop = false;
+        cudaGraphExec_t exec = nullptr;
+        long long per_graph = 0;
+    };
+    SlotGraph slot_graph_;
+    cudaEvent_t run_ev_[4] = {nullptr, nullptr, nullptr, nullptr};   // start, end, two polls
+
     int device_ = 0;
     int sm_count_ = 0;
     const uint16_t *mix_slot_[2] = {nullptr, nullptr};   // [dv][n] message slot of each variable's edges

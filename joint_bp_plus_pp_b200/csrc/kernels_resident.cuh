@@ -86,7 +86,7 @@ struct ResRun {
     DevCode dc;                    // table form of the code for the post-processing stages
     DevEts ets;
     unsigned char *pp_scratch;     // per block: PpScratch | decision ring [R][n] | |LLR| [2][n] doubles |
-                                   // features [n][8]
+                                   // features [n][kMlpIn]
     size_t pp_scratch_stride;
     size_t pp_smem_base;           // offset of the post-processing arrays in shared memory
     // FP32 messages (the instantiation with GC): the Z side's c2v of each block in global memory,
@@ -126,7 +126,7 @@ constexpr int kLearnedMaxCols = 512;   // ... solved from at most this many of t
 // last R iterations' decisions and the |LLR| keys of the OSD order.
 __host__ __device__ inline size_t res_pp_scratch_bytes(int n, int mmax, int R) {
     return pp_align(pp_scratch_bytes(n, mmax)) + pp_align(static_cast<size_t>(R) * n) + pp_align(16ull * n) +
-           pp_align(32ull * n);
+           pp_align(4ull * kMlpIn * n);
 }
 
 // (a x + b) mod P from the fixed-point constants of the map: one multiply-add and one

@@ -113,11 +113,13 @@ def main(argv=None):
     ap.add_argument("--capacity", type=int, default=2_000_000, help="samples kept per p at most")
     ap.add_argument("--pos-weight", type=float, default=4.0)
     ap.add_argument("--max-iter", type=int, default=100)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16"],
+                    help="message storage of the decoder whose stalls are recorded")
     a = ap.parse_args(argv)
     dec = Decoder.from_params()
     t0 = time.time()
     x, y, info = collect(dec, ps=tuple(a.p), trials_per_p=a.trials_per_p, learned_from=a.learned_from,
-                         every=a.collect_every, capacity=a.capacity, max_iter=a.max_iter)
+                         every=a.collect_every, capacity=a.capacity, max_iter=a.max_iter, precision=a.precision)
     t1 = time.time()
     params, hist = train(dec, x, y, epochs=a.epochs, pos_weight=a.pos_weight)
     t2 = time.time()
@@ -125,7 +127,8 @@ def main(argv=None):
     rep = {"samples": int(len(x)), "positives_x": int(y[:, 0].sum()), "positives_z": int(y[:, 1].sum()),
            "collect": info, "collect_s": t1 - t0, "train_s": t2 - t1, "epoch_loss": [float(v) for v in hist],
            "learned_from": a.learned_from, "collect_every": a.collect_every, "pos_weight": a.pos_weight,
-           "max_iter": a.max_iter}
+           "max_iter": a.max_iter, "precision": a.precision,
+           "stalls": int(sum(i["stalls"] or 0 for i in info))}
     print(json.dumps(rep))
     if a.report:
         Path(a.report).write_text(json.dumps(rep, indent=1))

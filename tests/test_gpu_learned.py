@@ -9,6 +9,7 @@ import pytest
 
 sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "oracle"))
 import mlp_oracle  # noqa: E402
+from joint_bp_plus_pp_b200 import MLP_IN  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -16,7 +17,7 @@ pytestmark = pytest.mark.gpu
 def rand_problem(n, seed):
     rng = np.random.default_rng(seed)
     params = rng.normal(0, 0.25, mlp_oracle.NPARAMS).astype(np.float32)
-    x = rng.normal(0, 1, (n, 8)).astype(np.float32)
+    x = rng.normal(0, 1, (n, MLP_IN)).astype(np.float32)
     y = (rng.random((n, 2)) < 0.2).astype(np.float32)
     return params, x, y
 
@@ -46,7 +47,7 @@ def test_gpu_bf16_inference_matches_oracle(decoder):
 def test_gpu_training_reduces_loss(decoder):
     """A separable synthetic task: Adam on the GPU drives the loss well below its start."""
     rng = np.random.default_rng(5)
-    x = rng.normal(0, 1, (40000, 8)).astype(np.float32)
+    x = rng.normal(0, 1, (40000, MLP_IN)).astype(np.float32)
     y = np.stack([(x[:, 0] + 0.5 * x[:, 6] > 0.8), (x[:, 2] - x[:, 7] > 1.0)], 1).astype(np.float32)
     from joint_bp_plus_pp_b200 import mlp_init
     p0 = mlp_init(1)
@@ -81,31 +82,46 @@ def test_learned_needs_a_model(decoder):
 
 
 @pytest.mark.parametrize("prec", ["fp16", "fp32"])
-def test_trained_model_gain(decoder, prec):
-    """The shipped model (trained by joint_bp_plus_pp_b200.learned on the decoder's own stalled
-    states) against the same decoder without it, on the same 40,000 trials at p=0.045 (max-iter
-    300, post-processing on, proposals from iteration 6).  What the network gains: trials that
-    stall are ended at the stall by an exactly syndrome-matching correction instead of BP
-    iterating on, so their iteration counts drop, their outcomes are not worse, and the logical
-    error rate of the whole run is not worse within its 95% interval."""
+def test_learned_proposal_three_ways(decoder, prec):
+    """The proposal against the decoder without it, and the network's column order against the
+    decoder's own |LLR| order, on the same 100,000 trials at p = 0.05 (max-iter 300,
+    post-processing on, proposals from iteration 6, 64 columns): (a) no proposal, (b) |LLR|
+    order, (c) the shipped network.  Both proposals accept only corrections that match both
+    syndromes exactly, end the accepted trials at the stall (fewer iterations than the same
+    trials take without the proposal), leave no accepted trial worse, and keep the run's
+    logical error rate inside the 95% interval of the run without them.  The network does not
+    rank better than |LLR|: on 10^6 trials its proposals are accepted less often at every column
+    budget (bench leg learned_ablation), which this test records without asserting an order."""
     from joint_bp_plus_pp_b200 import Options, load_flip_model, wilson_interval
     params = load_flip_model()
     assert params is not None, "data/flip_mlp_params.npy missing"
     decoder.set_flip_model(params)
-    N = 40000
+    N, p = 100000, 0.05
     base = dict(precision=prec, engine="resident", max_iter=300, enable_pp=True)
-    s0, r0 = decoder.simulate(606, N, 0.045, Options(**base))
-    s1, r1 = decoder.simulate(606, N, 0.045, Options(learned_from=6, **base))
-    decoder.set_flip_model(None)
-    acc = (r1["ets_used_flags"] & 32) != 0
-    assert s1["learned_attempts"] > 0 and acc.sum() > 0
-    assert acc.sum() >= 0.7 * s1["learned_attempts"]            # most proposals are accepted
-    assert r1["syndrome_ok"][acc].all()                          # only exact syndrome matches
-    assert r1["success"][acc].sum() >= r0["success"][acc].sum()  # the same trials, not worse
-    assert r1["iterations"][acc].mean() < r0["iterations"][acc].mean()
-    # the run's total: the accepted trials' savings are of the order of the perturbation the
-    # learned instantiation's decision-history bits bring to the others (2^-17 of |A|), so the
-    # total is bounded by that perturbation rather than required to fall
-    assert s1["total_iters"] <= s0["total_iters"] * (1 + 1e-3)
+    s0, r0 = decoder.simulate(606, N, p, Options(**base))
     lo0, hi0 = wilson_interval(N, s0["failures"])
-    assert s1["failures"] / N <= hi0, (s1["failures"], s0["failures"])
+    acc_rate = {}
+    for order in ("llr", "model"):
+        s1, r1 = decoder.simulate(606, N, p, Options(learned_from=6, learned_order=order, learned_cols=64, **base))
+        acc = (r1["ets_used_flags"] & 32) != 0
+        assert s1["learned_attempts"] > 0 and acc.sum() > 0, order
+        assert r1["syndrome_ok"][acc].all(), order                          # exact syndrome matches only
+        assert (r1["success"][acc] >= r0["success"][acc]).all(), order      # no accepted trial worse
+        assert r1["iterations"][acc].mean() < r0["iterations"][acc].mean(), order
+        assert s1["failures"] / N <= hi0, (order, s1["failures"], s0["failures"])
+        acc_rate[order] = acc.sum() / s1["learned_attempts"]
+    decoder.set_flip_model(None)
+    print("acceptance at 64 columns:", acc_rate)
+
+
+def test_collect_every_qubit(decoder):
+    """collect_every = 1 records every qubit of each stall, so the sample count is the number
+    of stalls recorded (stats learned_attempts) times n: a training set without selection bias."""
+    from joint_bp_plus_pp_b200 import Options
+    o = Options(precision="fp32", engine="resident", max_iter=60, enable_pp=True, learned_from=6, collect_every=1)
+    x, y, st = decoder.collect_stall_states(77, 20000, 0.055, o, 4_000_000)
+    assert st["learned_attempts"] > 0
+    assert len(x) == st["learned_attempts"] * decoder.n
+    o32 = Options(precision="fp32", engine="resident", max_iter=60, enable_pp=True, learned_from=6)
+    x32, _, st32 = decoder.collect_stall_states(77, 20000, 0.055, o32, 4_000_000)
+    assert st32["learned_attempts"] == st["learned_attempts"] and len(x32) < len(x)
