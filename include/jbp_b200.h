@@ -210,6 +210,14 @@ int jbp_mlp_param_count(void);
  * rules: the denominators of the SFU roofline the resident and table-driven kernels report.
  * No counterpart in the reference.  About 10 ms of GPU time. */
 int jbp_measure_sfu(int device, double *ex2_gops, double *lg2_gops, double *rcp_gops);
+/* Device self-check of the FP64 kernels' branch-free reciprocal (three Newton steps from the
+ * hardware approximation and an exact-remainder choice of the nearest double) against the
+ * correctly rounded division 1.0 / s, on n divisors in [2^-900, 2^900] drawn from seed (random
+ * significands, all-ones significands, powers of two and their neighbours).  mismatches gets
+ * the count, first_mismatch (may be null) the index of the first, or -1.  No counterpart in the
+ * reference: the bit-exact FP64 decoder depends on it.  About 1 ms of GPU time per 10^8. */
+int jbp_check_reciprocal(int device, unsigned long long seed, long long n, long long *mismatches,
+                         long long *first_mismatch);
 /* Gradient of the mean loss (binary cross-entropy with logits, positives weighted by
  * pos_weight, summed over the two outputs) on the GPU; grad_out has jbp_mlp_param_count()
  * entries. */

@@ -140,6 +140,7 @@ def load_library(path=None):
     lib.jbp_code_graph_checks.argtypes = [vp, ctypes.POINTER(ll), ctypes.POINTER(i), ctypes.POINTER(i)]
     lib.jbp_graph_checks.argtypes = [i, i, vp, vp, i, vp, vp, ctypes.POINTER(ll), ctypes.POINTER(i), ctypes.POINTER(i)]
     lib.jbp_measure_sfu.argtypes = [i, ctypes.POINTER(d), ctypes.POINTER(d), ctypes.POINTER(d)]
+    lib.jbp_check_reciprocal.argtypes = [i, ctypes.c_ulonglong, ll, ctypes.POINTER(ll), ctypes.POINTER(ll)]
     lib.jbp_simulate_mixed.argtypes = [vp, i, ctypes.POINTER(COptions), vp, vp, vp, d, ctypes.POINTER(CStats), vp]
     lib.jbp_decode_errors_device.argtypes = [vp, ctypes.POINTER(COptions), ll, vp, d, vp, vp, ctypes.POINTER(CStats),
                                              vp]
@@ -379,6 +380,15 @@ def measure_sfu(device=0):
     r = [ctypes.c_double() for _ in range(3)]
     _check(lib, lib.jbp_measure_sfu(device, *[ctypes.byref(x) for x in r]))
     return {"ex2": r[0].value, "lg2": r[1].value, "rcp": r[2].value}
+
+
+def check_reciprocal(n, seed=1, device=0):
+    """Device self-check of the FP64 kernels' branch-free reciprocal against correctly rounded
+    division on n divisors: (mismatches, index of the first or -1)."""
+    lib = load_library()
+    bad, first = ctypes.c_longlong(), ctypes.c_longlong()
+    _check(lib, lib.jbp_check_reciprocal(device, seed, n, ctypes.byref(bad), ctypes.byref(first)))
+    return bad.value, first.value
 
 
 def graph_checks(n, x_off, x_var, z_off, z_var):

@@ -54,6 +54,53 @@ __device__ __forceinline__ double div_by_recip(double m, double s, double y) {
     return __ddiv_rn(m, s);
 }
 
+__device__ __forceinline__ double rcp_approx_f64(double s) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(s));
+    return y;
+}
+
+// RN(1/s) for s in [2^-900, 2^900] without a branch.  Three Newton steps
+// y <- y + y (1 - s y) (two FMAs each; each squares the relative error, so any start better than
+// 2^-10 ends within one ulp) from the hardware approximation, then the choice between y and its
+// two neighbours: with the remainder r = 1 - s y, exact by one FMA, 1/s - y = r / s, so y is the
+// nearest double when -s ulp_below(y) / 2 <= r <= s ulp(y) / 2 (1/s is never a midpoint between
+// two doubles, so no tie arises).  Outside the domain the result is not used (the callers take
+// the exact path there).  tests/native/reciprocal_rn_check.c runs the sequence on the host
+// against IEEE division from perturbed starts; jbp_check_reciprocal compares it on the device
+// with the division intrinsic.
+__device__ __forceinline__ double recip_rn_fast(double s) {
+    double y = rcp_approx_f64(s);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) y = __fma_rn(y, __fma_rn(-s, y, 1.0), y);
+    const double r = __fma_rn(-s, y, 1.0);
+    const long long yb = __double_as_longlong(y);
+    const double ulp = __longlong_as_double((yb & 0x7FF0000000000000ll) - (52ll << 52));
+    const double t_up = __dmul_rn(__dmul_rn(s, ulp), 0.5);
+    const double t_dn = (yb & 0x000FFFFFFFFFFFFFll) == 0 ? __dmul_rn(t_up, 0.5) : t_up;
+    return r > t_up ? __longlong_as_double(yb + 1) : (r < -t_dn ? __longlong_as_double(yb - 1) : y);
+}
+
+// The domain of the branch-free normalization: a divisor in [2^-900, 2^900] and dividends that
+// are 0 or at least 2^-900 (the quotients, at most 1, and the remainders stay normal).
+__device__ __forceinline__ bool fast_div_ok(double m) { return m == 0.0 || m >= 0x1p-900; }
+
+// normalize_msg (jointbp_ets.cpp:650-657) for operands in the fast domain, without branches:
+// one reciprocal (recip_rn_fast) and Markstein's correction per entry (as div_by_recip), so
+// the results are the IEEE quotients.  Clears ok when an operand is outside the domain; the
+// caller then recomputes with norm4.
+__device__ __forceinline__ void norm4_fast(double &m0, double &m1, double &m2, double &m3, bool &ok) {
+    const double s = dadd(dadd(dadd(m0, m1), m2), m3);
+    ok = ok && s >= 0x1p-900 && s <= 0x1p900 && fast_div_ok(m0) && fast_div_ok(m1) && fast_div_ok(m2) &&
+         fast_div_ok(m3);
+    const double y = recip_rn_fast(s);
+    double q;
+    q = __dmul_rn(m0, y); m0 = __fma_rn(__fma_rn(-s, q, m0), y, q);
+    q = __dmul_rn(m1, y); m1 = __fma_rn(__fma_rn(-s, q, m1), y, q);
+    q = __dmul_rn(m2, y); m2 = __fma_rn(__fma_rn(-s, q, m2), y, q);
+    q = __dmul_rn(m3, y); m3 = __fma_rn(__fma_rn(-s, q, m3), y, q);
+}
+
 // normalize_msg (jointbp_ets.cpp:650-657): each entry divided by ((m0 + m1) + m2) + m3
 __device__ __forceinline__ void norm4(double &m0, double &m1, double &m2, double &m3) {
     double s = dadd(dadd(dadd(m0, m1), m2), m3);
@@ -107,6 +154,45 @@ __device__ __forceinline__ int frozen_bit(const DevRun &run, int n, int side, in
 }
 
 // ------------------------------------------------------------------ FP64, bit-exact
+
+// The outputs of one check row (jointbp_ets.cpp:2373-2450): for each edge i the even / odd
+// parity products of the other edges (prefix pe, po times suffix se, so), ordered by the
+// syndrome bit s and normalized by their side's sum.  FAST: the two quotients by one
+// branch-free reciprocal and Markstein's correction (the IEEE quotients inside the fast
+// domain), the row in one basic block; ok is cleared when an operand left the domain and the
+// caller redoes the row with FAST = false (the division itself), which rewrites every output.
+template <int DC, bool FAST>
+__device__ __forceinline__ void check_f64_outputs(const double *se, const double *so, const double *q0,
+                                                  const double *q1, int s, int side, double2 *c2v, bool &ok) {
+    double pe = 1.0, po = 0.0;
+#pragma unroll
+    for (int i = 0; i < DC; ++i) {
+        const double p_even = dadd(dmul(pe, se[i + 1]), dmul(po, so[i + 1]));
+        const double p_odd = dadd(dmul(pe, so[i + 1]), dmul(po, se[i + 1]));
+        const double v0 = s == 0 ? p_even : p_odd;
+        const double v1 = s == 0 ? p_odd : p_even;
+        const double sum = side == 0 ? dadd(dadd(dadd(v0, v1), v0), v1) : dadd(dadd(dadd(v0, v0), v1), v1);
+        double2 out;
+        if (FAST) {
+            ok = ok && sum >= 0x1p-900 && sum <= 0x1p900 && fast_div_ok(v0) && fast_div_ok(v1);
+            const double y = recip_rn_fast(sum);
+            const double a = __dmul_rn(v0, y), b = __dmul_rn(v1, y);
+            out.x = __fma_rn(__fma_rn(-sum, a, v0), y, a);
+            out.y = __fma_rn(__fma_rn(-sum, b, v1), y, b);
+        } else if (sum <= 0.0) {
+            out.x = 0.25;
+            out.y = 0.25;
+        } else {
+            out.x = ddiv(v0, sum);
+            out.y = ddiv(v1, sum);
+        }
+        c2v[i * kGroup] = out;
+        const double ne = dadd(dmul(pe, q0[i]), dmul(po, q1[i]));
+        const double no = dadd(dmul(pe, q1[i]), dmul(po, q0[i]));
+        pe = ne;
+        po = no;
+    }
+}
 
 template <int DC, bool DAMP>
 __global__ void __launch_bounds__(256, 3) k_check_f64(DevCode code, DevRun run, DevMsgs msg) {
@@ -167,28 +253,8 @@ __global__ void __launch_bounds__(256, 3) k_check_f64(DevCode code, DevRun run, 
             so[i] = dadd(dmul(se[i + 1], q1[i]), dmul(so[i + 1], q0[i]));
         }
         const int s = (run.synm[static_cast<size_t>(row) * G + group] >> lane) & 1;
-        double pe = 1.0, po = 0.0;
-#pragma unroll
-        for (int i = 0; i < DC; ++i) {
-            const double p_even = dadd(dmul(pe, se[i + 1]), dmul(po, so[i + 1]));
-            const double p_odd = dadd(dmul(pe, so[i + 1]), dmul(po, se[i + 1]));
-            const double v0 = s == 0 ? p_even : p_odd;
-            const double v1 = s == 0 ? p_odd : p_even;
-            const double sum = side == 0 ? dadd(dadd(dadd(v0, v1), v0), v1) : dadd(dadd(dadd(v0, v0), v1), v1);
-            double2 out;
-            if (sum <= 0.0) {
-                out.x = 0.25;
-                out.y = 0.25;
-            } else {
-                out.x = ddiv(v0, sum);
-                out.y = ddiv(v1, sum);
-            }
-            c2v[i * kGroup] = out;
-            const double ne = dadd(dmul(pe, q0[i]), dmul(po, q1[i]));
-            const double no = dadd(dmul(pe, q1[i]), dmul(po, q0[i]));
-            pe = ne;
-            po = no;
-        }
+        bool ok = true;
+        check_f64_outputs<DC, false>(se, so, q0, q1, s, side, c2v, ok);
     }
 }
 
@@ -218,6 +284,79 @@ __device__ __forceinline__ void store_v2c_f64(double2 *v2c, double2 *v2c_hi, siz
     }
 }
 
+// The variable update of one slot's variable from its incoming messages: (ax, bx) of each X
+// edge and (az, bz) of each Z edge (a padded edge of a lower-degree variable is the identity
+// message (1, 1), which leaves the products unchanged exactly).  Writes the new v2c at offsets
+// ox / oz of the present edges (unless the side is frozen) and returns the hard decision
+// (0..3, the first maximum of the normalized total).  FAST: every normalization through
+// norm4_fast, one basic block for the whole update (the seven normalizations' dependency chains
+// interleave); ok is cleared when an operand left the fast domain, and the caller then redoes
+// the update with FAST = false (norm4), which rewrites the same outputs.
+template <int DV, bool DAMP, bool FAST>
+__device__ __forceinline__ int var_f64_update(const DevRun &run, const DevMsgs &msg, double damping, int slot, int frz,
+                                              const size_t *ox, const size_t *oz, const bool *vx, const bool *vz,
+                                              const double *ax, const double *bx, const double *az,
+                                              const double *bz, bool &ok) {
+    const bool fresh = run.iter[slot] == 0;
+    const double *pr = run.prior + 4 * slot;
+    const double p0 = pr[0], p1 = pr[1], p2 = pr[2], p3 = pr[3];
+    // prefix / suffix products of the X messages (a, b, a, b) and Z messages (a, a, b, b)
+    double PA[DV + 1], PB[DV + 1], SA[DV + 1], SB[DV + 1];
+    double QA[DV + 1], QB[DV + 1], TA[DV + 1], TB[DV + 1];
+    PA[0] = PB[0] = QA[0] = QB[0] = 1.0;
+    SA[DV] = SB[DV] = TA[DV] = TB[DV] = 1.0;
+#pragma unroll
+    for (int k = 0; k < DV; ++k) {
+        PA[k + 1] = dmul(PA[k], ax[k]); PB[k + 1] = dmul(PB[k], bx[k]);
+        QA[k + 1] = dmul(QA[k], az[k]); QB[k + 1] = dmul(QB[k], bz[k]);
+    }
+#pragma unroll
+    for (int k = DV - 1; k >= 0; --k) {
+        SA[k] = dmul(SA[k + 1], ax[k]); SB[k] = dmul(SB[k + 1], bx[k]);
+        TA[k] = dmul(TA[k + 1], az[k]); TB[k] = dmul(TB[k + 1], bz[k]);
+    }
+    const double XA = PA[DV], XB = PB[DV], ZA = QA[DV], ZB = QB[DV];
+    // total = normalize(prior * (PX * PZ)); est = first argmax
+    double t0 = dmul(p0, dmul(XA, ZA)), t1 = dmul(p1, dmul(XB, ZA));
+    double t2 = dmul(p2, dmul(XA, ZB)), t3 = dmul(p3, dmul(XB, ZB));
+    if (FAST) norm4_fast(t0, t1, t2, t3, ok);
+    else norm4(t0, t1, t2, t3);
+    int best = 0;
+    double bv = t0;
+    if (t1 > bv) { best = 1; bv = t1; }
+    if (t2 > bv) { best = 2; bv = t2; }
+    if (t3 > bv) { best = 3; }
+    // (the |LLR| keys of the OSD order are computed from the same messages by the block
+    // that post-processes the slot: kernels_slot_pp.cuh)
+    double2 *v2cx = static_cast<double2 *>(msg.v2c[0]);
+    double2 *v2cz = static_cast<double2 *>(msg.v2c[1]);
+    double2 *v2cx_hi = static_cast<double2 *>(msg.v2c_hi[0]);
+    double2 *v2cz_hi = static_cast<double2 *>(msg.v2c_hi[1]);
+#pragma unroll
+    for (int k = 0; k < DV; ++k) {
+        if (frz & 1) break;
+        if (!vx[k]) continue;
+        const double EA = dmul(PA[k], SA[k + 1]), EB = dmul(PB[k], SB[k + 1]);
+        double n0 = dmul(dmul(p0, EA), ZA), n1 = dmul(dmul(p1, EB), ZA);
+        double n2 = dmul(dmul(p2, EA), ZB), n3 = dmul(dmul(p3, EB), ZB);
+        if (FAST) norm4_fast(n0, n1, n2, n3, ok);
+        else norm4(n0, n1, n2, n3);
+        store_v2c_f64<DAMP>(v2cx, v2cx_hi, ox[k], 0, n0, n1, n2, n3, fresh, pr, damping);
+    }
+#pragma unroll
+    for (int k = 0; k < DV; ++k) {
+        if (frz & 2) break;
+        if (!vz[k]) continue;
+        const double FA = dmul(QA[k], TA[k + 1]), FB = dmul(QB[k], TB[k + 1]);
+        double n0 = dmul(dmul(p0, XA), FA), n1 = dmul(dmul(p1, XB), FA);
+        double n2 = dmul(dmul(p2, XA), FB), n3 = dmul(dmul(p3, XB), FB);
+        if (FAST) norm4_fast(n0, n1, n2, n3, ok);
+        else norm4(n0, n1, n2, n3);
+        store_v2c_f64<DAMP>(v2cz, v2cz_hi, oz[k], 1, n0, n1, n2, n3, fresh, pr, damping);
+    }
+    return best;
+}
+
 template <int DC, int DV, bool DAMP>
 __global__ void __launch_bounds__(256, 2) k_var_f64(DevCode code, DevRun run, DevMsgs msg, double damping) {
     const int lane = threadIdx.x & 31;
@@ -235,9 +374,6 @@ __global__ void __launch_bounds__(256, 2) k_var_f64(DevCode code, DevRun run, De
         if (!__any_sync(0xffffffffu, active)) continue;
         int best = 0;
         if (active) {
-            const bool fresh = run.iter[slot] == 0;
-            const double *pr = run.prior + 4 * slot;
-            const double p0 = pr[0], p1 = pr[1], p2 = pr[2], p3 = pr[3];
             size_t ox[DV], oz[DV];
             bool vx[DV], vz[DV];   // edge present (a variable of lower degree is padded with -1)
             double ax[DV], bx[DV], az[DV], bz[DV];
@@ -249,64 +385,17 @@ __global__ void __launch_bounds__(256, 2) k_var_f64(DevCode code, DevRun run, De
                 ox[k] = vx[k] ? msg_off<DC>(ex, G, group, lane) : 0;
                 oz[k] = vz[k] ? msg_off<DC>(ez, G, group, lane) : 0;
             }
-            // a padded edge is the identity message (1, 1, 1, 1): products are unchanged exactly
 #pragma unroll
             for (int k = 0; k < DV; ++k) {
                 const double2 cx = vx[k] ? c2vx[ox[k]] : make_double2(1.0, 1.0);
                 const double2 cz = vz[k] ? c2vz[oz[k]] : make_double2(1.0, 1.0);
                 ax[k] = cx.x; bx[k] = cx.y; az[k] = cz.x; bz[k] = cz.y;
             }
-            // prefix / suffix products of the X messages (a, b, a, b) and Z messages (a, a, b, b)
-            double PA[DV + 1], PB[DV + 1], SA[DV + 1], SB[DV + 1];
-            double QA[DV + 1], QB[DV + 1], TA[DV + 1], TB[DV + 1];
-            PA[0] = PB[0] = QA[0] = QB[0] = 1.0;
-            SA[DV] = SB[DV] = TA[DV] = TB[DV] = 1.0;
-#pragma unroll
-            for (int k = 0; k < DV; ++k) {
-                PA[k + 1] = dmul(PA[k], ax[k]); PB[k + 1] = dmul(PB[k], bx[k]);
-                QA[k + 1] = dmul(QA[k], az[k]); QB[k + 1] = dmul(QB[k], bz[k]);
-            }
-#pragma unroll
-            for (int k = DV - 1; k >= 0; --k) {
-                SA[k] = dmul(SA[k + 1], ax[k]); SB[k] = dmul(SB[k + 1], bx[k]);
-                TA[k] = dmul(TA[k + 1], az[k]); TB[k] = dmul(TB[k + 1], bz[k]);
-            }
-            const double XA = PA[DV], XB = PB[DV], ZA = QA[DV], ZB = QB[DV];
-            // total = normalize(prior * (PX * PZ)); est = first argmax
-            double t0 = dmul(p0, dmul(XA, ZA)), t1 = dmul(p1, dmul(XB, ZA));
-            double t2 = dmul(p2, dmul(XA, ZB)), t3 = dmul(p3, dmul(XB, ZB));
-            norm4(t0, t1, t2, t3);
-            double bv = t0;
-            if (t1 > bv) { best = 1; bv = t1; }
-            if (t2 > bv) { best = 2; bv = t2; }
-            if (t3 > bv) { best = 3; }
-            // (the |LLR| keys of the OSD order are computed from the same messages by the block
-            // that post-processes the slot: kernels_slot_pp.cuh)
-            double2 *v2cx = static_cast<double2 *>(msg.v2c[0]);
-            double2 *v2cz = static_cast<double2 *>(msg.v2c[1]);
-            double2 *v2cx_hi = static_cast<double2 *>(msg.v2c_hi[0]);
-            double2 *v2cz_hi = static_cast<double2 *>(msg.v2c_hi[1]);
             const int frz = run.freeze_syn ? run.frz[slot] : 0;
-#pragma unroll
-            for (int k = 0; k < DV; ++k) {
-                if (frz & 1) break;
-                if (!vx[k]) continue;
-                const double EA = dmul(PA[k], SA[k + 1]), EB = dmul(PB[k], SB[k + 1]);
-                double n0 = dmul(dmul(p0, EA), ZA), n1 = dmul(dmul(p1, EB), ZA);
-                double n2 = dmul(dmul(p2, EA), ZB), n3 = dmul(dmul(p3, EB), ZB);
-                norm4(n0, n1, n2, n3);
-                store_v2c_f64<DAMP>(v2cx, v2cx_hi, ox[k], 0, n0, n1, n2, n3, fresh, pr, damping);
-            }
-#pragma unroll
-            for (int k = 0; k < DV; ++k) {
-                if (frz & 2) break;
-                if (!vz[k]) continue;
-                const double FA = dmul(QA[k], TA[k + 1]), FB = dmul(QB[k], TB[k + 1]);
-                double n0 = dmul(dmul(p0, XA), FA), n1 = dmul(dmul(p1, XB), FA);
-                double n2 = dmul(dmul(p2, XA), FB), n3 = dmul(dmul(p3, XB), FB);
-                norm4(n0, n1, n2, n3);
-                store_v2c_f64<DAMP>(v2cz, v2cz_hi, oz[k], 1, n0, n1, n2, n3, fresh, pr, damping);
-            }
+            // damped updates (scaled_mix renormalizes inside store_v2c_f64) take the exact path
+            bool ok = !DAMP;
+            if (!DAMP) best = var_f64_update<DV, DAMP, true>(run, msg, damping, slot, frz, ox, oz, vx, vz, ax, bx, az, bz, ok);
+            if (!ok) best = var_f64_update<DV, DAMP, false>(run, msg, damping, slot, frz, ox, oz, vx, vz, ax, bx, az, bz, ok);
         }
         store_est_bits(run, plane, group, n, v, best, active);
     }

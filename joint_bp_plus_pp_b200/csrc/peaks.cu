@@ -2,13 +2,15 @@
 // use -- ex2, lg2 and rcp in FP32 (approx, flush-to-zero), the roofline of the trial-resident
 // and table-driven kernels, which are bound by these and by instruction issue, not by HBM.
 // Every thread runs 8 independent chains of one operation, so the unit, not the latency of a
-// chain, sets the pace; the grid fills every SM.
+// chain, sets the pace; the grid fills every SM.  Also the device self-check of the FP64
+// kernels' branch-free reciprocal against the division intrinsic.
 #include <cuda_runtime.h>
 
 #include <string>
 
 #include "../../include/jbp_b200.h"
 #include "ctx.hpp"
+#include "kernels_bp.cuh"
 
 namespace {
 
@@ -66,7 +68,71 @@ std::string time_op(int sms, float *sink, double *gops) {
     return "";
 }
 
+// Divisor k of the reciprocal self-check: exponent uniform in [-900, 899]; significand random,
+// all ones, zero (a power of two), one ulp above it, or just below all ones, by k mod 8.
+__device__ double check_divisor(unsigned long long seed, unsigned long long k) {
+    unsigned long long h = seed ^ (k * 0x9E3779B97F4A7C15ull);
+    auto mix = [&h]() {
+        h += 0x9E3779B97F4A7C15ull;
+        unsigned long long z = h;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    const unsigned long long e = static_cast<unsigned long long>(-900 + static_cast<int>(mix() % 1800) + 1023) << 52;
+    const unsigned long long ones = (1ull << 52) - 1;
+    unsigned long long frac;
+    switch (k & 7) {
+    case 0: frac = ones; break;
+    case 1: frac = 0; break;
+    case 2: frac = 1; break;
+    case 3: frac = ones - (mix() & 0xFFFF); break;
+    default: frac = mix() & ones; break;
+    }
+    return __longlong_as_double(static_cast<long long>(e | frac));
+}
+
+__global__ void k_check_reciprocal(unsigned long long seed, unsigned long long n, unsigned long long *bad,
+                                   unsigned long long *first_bad) {
+    unsigned long long local = 0;
+    for (unsigned long long k = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+        const double s = check_divisor(seed, k);
+        const double got = jbp::recip_rn_fast(s), want = __ddiv_rn(1.0, s);
+        if (__double_as_longlong(got) != __double_as_longlong(want)) {
+            ++local;
+            atomicMin(first_bad, k);
+        }
+    }
+    if (local) atomicAdd(bad, local);
+}
+
 }  // namespace
+
+extern "C" int jbp_check_reciprocal(int device, unsigned long long seed, long long n, long long *mismatches,
+                                    long long *first_mismatch) {
+    if (n < 0 || !mismatches) return jbp::set_last_error(JBP_ERR_ARG, "n >= 0 and mismatches required");
+    if (cudaSetDevice(device) != cudaSuccess) return jbp::set_last_error(JBP_ERR_CUDA, "cudaSetDevice failed");
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        return jbp::set_last_error(JBP_ERR_CUDA, "device attributes");
+    unsigned long long *d = nullptr;
+    if (cudaMalloc(&d, 2 * sizeof(unsigned long long)) != cudaSuccess)
+        return jbp::set_last_error(JBP_ERR_CUDA, "cudaMalloc(counts)");
+    const unsigned long long init[2] = {0ull, ~0ull};
+    cudaError_t e = cudaMemcpy(d, init, sizeof(init), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_check_reciprocal<<<sms * 8, 256>>>(seed, static_cast<unsigned long long>(n), d, d + 1);
+        e = cudaGetLastError();
+    }
+    unsigned long long h[2] = {0ull, ~0ull};
+    if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return jbp::set_last_error(JBP_ERR_CUDA, std::string("reciprocal check: ") + cudaGetErrorString(e));
+    *mismatches = static_cast<long long>(h[0]);
+    if (first_mismatch) *first_mismatch = h[0] ? static_cast<long long>(h[1]) : -1;
+    return JBP_OK;
+}
 
 extern "C" int jbp_measure_sfu(int device, double *ex2_gops, double *lg2_gops, double *rcp_gops) {
     if (cudaSetDevice(device) != cudaSuccess) return jbp::set_last_error(JBP_ERR_CUDA, "cudaSetDevice failed");
