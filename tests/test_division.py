@@ -41,9 +41,10 @@ def rcp_checker(tmp_path_factory):
 
 @pytest.mark.parametrize("lo,hi", [(-900, 899), (-900, -890), (890, 899), (-2, 2)])
 def test_branch_free_reciprocal_equals_ieee_division(rcp_checker, lo, hi):
-    """recip_rn_fast's sequence (three Newton steps, then the exact-remainder choice among y and
-    its neighbours), started from approximations with relative errors up to 2^-10, gives the
-    correctly rounded 1/s over the fast path's whole domain."""
+    """recip_rn_fast's sequence (two Newton steps, then the exact-remainder choice among y and
+    its neighbours), started from approximations with relative errors up to 2^-16 (the hardware
+    approximation it starts from on the device is within 2^-19.9), gives the correctly rounded
+    1/s over the fast path's whole domain."""
     r = subprocess.run([str(rcp_checker), "3000000", str(lo), str(hi)], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout
     assert "mismatches 0" in r.stdout
