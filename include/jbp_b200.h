@@ -30,6 +30,7 @@ extern "C" {
 #define JBP_ERR_IO 3           /* file missing or malformed */
 #define JBP_ERR_UNSUPPORTED 4  /* combination not built for the GPU */
 #define JBP_ERR_TIMEOUT 5      /* device watchdog expired (see jbp_options.watchdog_ms) */
+#define JBP_ERR_ABORTED 6      /* stopped by jbp_request_abort; stats hold the trials finished */
 
 #define JBP_PREC_FP64 0        /* probability-domain messages, bit-exact with the reference CPU */
 #define JBP_PREC_FP32 1        /* LLR messages in FP32 */
@@ -130,6 +131,19 @@ typedef struct {
 void jbp_default_options(jbp_options *opt);
 const char *jbp_last_error(void);
 const char *jbp_version(void);
+/* Test hook (fault injection on the host): the device or pinned-host allocation `after`
+ * allocations from now (0 = the next one) fails with JBP_ERR_CUDA ("out of memory"), once,
+ * without calling the CUDA runtime; after < 0 turns the hook off.  Process-wide.  Every
+ * allocation failure leaves the context usable: the next call allocates again.  No counterpart
+ * in the reference (whose allocation failures end in its CPU fallback). */
+int jbp_debug_fail_allocation(long long after);
+/* Asks the run in progress on ctx (from any host thread), or the next run if none is in
+ * progress, to stop: the persistent kernels claim no further trial (they look at the flag, a
+ * pinned host word, at every 8th trial they claim and every 16 iterations of a trial past
+ * iteration 64), the slot engine ends its iteration loop, and the run returns JBP_ERR_ABORTED
+ * with the counters of the trials that finished (jbp_stats is filled as for JBP_ERR_TIMEOUT).
+ * The flag clears when that run returns.  No counterpart in the reference. */
+int jbp_request_abort(jbp_ctx *ctx);
 
 int jbp_create_from_params(const char *params_path, const char *ets_dir, int device, jbp_ctx **out);
 int jbp_create_from_checks(int n, int mx, const int *x_off, const int *x_var, int mz, const int *z_off,

@@ -24,12 +24,13 @@ DEFAULT_PARAMS = DATA_DIR / "H_P768_J3_L12_dmax3_nc0-3_1-2_seed11579811919164041
 PREC = {"fp64": 0, "fp32": 1, "fp16": 2}
 SAMPLER = {"philox": 0, "mt19937": 1}
 ENGINE = {"auto": 0, "resident": 1, "slots": 2, "table": 3}
-ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "I/O error", 4: "unsupported", 5: "timeout"}
+ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "I/O error", 4: "unsupported", 5: "timeout", 6: "aborted"}
 
 
 class JbpError(RuntimeError):
-    """A failed call: `code` is the JBP_ERR_* status; for JBP_ERR_TIMEOUT (5), `stats` holds the
-    counters of the trials that finished within the run budget (None otherwise)."""
+    """A failed call: `code` is the JBP_ERR_* status; for JBP_ERR_TIMEOUT (5) and JBP_ERR_ABORTED
+    (6), `stats` holds the counters of the trials that finished before the run stopped (None
+    otherwise)."""
 
     def __init__(self, code, msg, stats=None):
         super().__init__(f"jbp error {code} ({ERRORS.get(code, '?')}): {msg}")
@@ -141,6 +142,8 @@ def load_library(path=None):
     lib.jbp_graph_checks.argtypes = [i, i, vp, vp, i, vp, vp, ctypes.POINTER(ll), ctypes.POINTER(i), ctypes.POINTER(i)]
     lib.jbp_measure_sfu.argtypes = [i, ctypes.POINTER(d), ctypes.POINTER(d), ctypes.POINTER(d)]
     lib.jbp_check_reciprocal.argtypes = [i, ctypes.c_ulonglong, ll, ctypes.POINTER(ll), ctypes.POINTER(ll)]
+    lib.jbp_debug_fail_allocation.argtypes = [ll]
+    lib.jbp_request_abort.argtypes = [vp]
     lib.jbp_simulate_mixed.argtypes = [vp, i, ctypes.POINTER(COptions), vp, vp, vp, d, ctypes.POINTER(CStats), vp]
     lib.jbp_decode_errors_device.argtypes = [vp, ctypes.POINTER(COptions), ll, vp, d, vp, vp, ctypes.POINTER(CStats),
                                              vp]
@@ -164,7 +167,7 @@ def load_library(path=None):
 def _check(lib, rc, stats=None):
     if rc != 0:
         raise JbpError(rc, lib.jbp_last_error().decode(errors="replace"),
-                       stats.as_dict() if (rc == 5 and stats is not None) else None)
+                       stats.as_dict() if (rc in (5, 6) and stats is not None) else None)
 
 
 def _ptr(a):
@@ -316,6 +319,11 @@ class Decoder:
 
     # ------------------------------------------------------------ learned flip proposal
 
+    def request_abort(self):
+        """Stops the run in progress on this decoder (call from another thread), or the next run:
+        it raises JbpError with code 6 and the counters of the trials that finished."""
+        _check(self._lib, self._lib.jbp_request_abort(self._h))
+
     def set_flip_model(self, params):
         """Model used when Options.learned_from > 0 (None removes it)."""
         if params is None:
@@ -380,6 +388,13 @@ def measure_sfu(device=0):
     r = [ctypes.c_double() for _ in range(3)]
     _check(lib, lib.jbp_measure_sfu(device, *[ctypes.byref(x) for x in r]))
     return {"ex2": r[0].value, "lg2": r[1].value, "rcp": r[2].value}
+
+
+def debug_fail_allocation(after):
+    """Test hook: the allocation `after` allocations from now (0 = the next) fails once with
+    JbpError; after < 0 turns the hook off."""
+    lib = load_library()
+    _check(lib, lib.jbp_debug_fail_allocation(int(after)))
 
 
 def check_reciprocal(n, seed=1, device=0):

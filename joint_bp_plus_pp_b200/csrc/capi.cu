@@ -21,11 +21,15 @@ int fail(int code, const std::string &msg) {
     return code;
 }
 
+// Statuses whose jbp_stats hold the trials that finished before the run stopped.
+bool partial_stats(int rc) { return rc == JBP_ERR_TIMEOUT || rc == JBP_ERR_ABORTED; }
+
 int engine_fail(const std::string &msg) {
     if (msg.find("not available") != std::string::npos || msg.find("no GPU kernel") != std::string::npos ||
         msg.find("need a code") != std::string::npos)
         return fail(JBP_ERR_UNSUPPORTED, msg);
     if (msg.find("watchdog") != std::string::npos) return fail(JBP_ERR_TIMEOUT, msg);
+    if (msg.find("aborted by request") != std::string::npos) return fail(JBP_ERR_ABORTED, msg);
     if (msg.find(':') != std::string::npos && msg.find("must") == std::string::npos) return fail(JBP_ERR_CUDA, msg);
     return fail(JBP_ERR_ARG, msg);
 }
@@ -36,7 +40,7 @@ int grow(T **p, size_t *have, size_t need) {
     cudaFree(*p);
     *p = nullptr;
     *have = 0;
-    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), std::max<size_t>(need, 1) * sizeof(T));
+    cudaError_t e = jbp::dev_malloc(reinterpret_cast<void **>(p), std::max<size_t>(need, 1) * sizeof(T));
     if (e != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(e, "cudaMalloc(staging)"));
     *have = need;
     return JBP_OK;
@@ -91,6 +95,17 @@ void jbp_default_options(jbp_options *o) {
 const char *jbp_last_error(void) { return g_last_error.c_str(); }
 
 const char *jbp_version(void) { return "jbp_b200 0.1 (sm_100a)"; }
+
+int jbp_request_abort(jbp_ctx *ctx) {
+    if (!ctx) return fail(JBP_ERR_ARG, "null context");
+    ctx->engine.request_abort();
+    return JBP_OK;
+}
+
+int jbp_debug_fail_allocation(long long after) {
+    jbp::set_alloc_failure(after);
+    return JBP_OK;
+}
 
 int jbp_create_from_params(const char *params_path, const char *ets_dir, int device, jbp_ctx **out) {
     if (!params_path || !out) return fail(JBP_ERR_ARG, "null argument");
@@ -195,21 +210,30 @@ int jbp_simulate(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed, long long 
     }
     jbp_stats st;
     std::string e = ctx->engine.run(rq, st);
+    auto copy_hist = [&]() -> int {
+        std::vector<unsigned long long> h(rq.opt.max_iter + 1);
+        cudaError_t ce = cudaMemcpy(h.data(), ctx->d_hist, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(ce, "copy histogram"));
+        for (size_t i = 0; i < h.size(); ++i) iter_hist[i] = static_cast<long long>(h[i]);
+        return JBP_OK;
+    };
     if (!e.empty()) {
         const int rc = engine_fail(e);
-        if (rc == JBP_ERR_TIMEOUT && stats) *stats = st;   // the trials finished within the budget
+        if (partial_stats(rc)) {
+            // the trials finished before the stop: their counters and iteration histogram (the
+            // per-trial records of the trials that did not finish are not defined, so none are copied)
+            if (iter_hist)
+                if (int hc = copy_hist()) return hc;
+            if (stats) *stats = st;
+        }
         return rc;
     }
     if (per_trial && ntrials > 0) {
         cudaError_t ce = cudaMemcpy(per_trial, ctx->d_res, sizeof(jbp_trial_result) * ntrials, cudaMemcpyDeviceToHost);
         if (ce != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(ce, "copy results"));
     }
-    if (iter_hist) {
-        std::vector<unsigned long long> h(rq.opt.max_iter + 1);
-        cudaError_t ce = cudaMemcpy(h.data(), ctx->d_hist, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost);
-        if (ce != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(ce, "copy histogram"));
-        for (size_t i = 0; i < h.size(); ++i) iter_hist[i] = static_cast<long long>(h[i]);
-    }
+    if (iter_hist)
+        if (int rc = copy_hist()) return rc;
     if (stats) *stats = st;
     return JBP_OK;
 }
@@ -241,7 +265,7 @@ int jbp_simulate_mixed(jbp_ctx *const *ctxs, int nctx, const jbp_options *opt, c
     std::string e = jbp::Engine::run_mixed(rq, st);
     if (!e.empty()) {
         const int rc = engine_fail(e);
-        if (rc == JBP_ERR_TIMEOUT)
+        if (partial_stats(rc))
             for (int i = 0; i < nctx && i < static_cast<int>(st.size()); ++i) stats[i] = st[i];
         return rc;
     }
@@ -350,7 +374,7 @@ static int decode_host(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, 
         std::string e = ctx->engine.run(rq, st);
         if (!e.empty()) {
             const int rc = engine_fail(e);
-            if (rc == JBP_ERR_TIMEOUT && stats) {
+            if (partial_stats(rc) && stats) {
                 add_stats(total, st);
                 *stats = total;   // the trials finished within the budget
             }
@@ -388,9 +412,9 @@ int jbp_collect_stall_states(jbp_ctx *ctx, const jbp_options *opt, uint64_t seed
     cudaSetDevice(ctx->engine.device());
     float *dx = nullptr, *dy = nullptr;
     unsigned long long *dc = nullptr;
-    cudaError_t ce = cudaMalloc(&dx, sizeof(float) * jbp::kMlpIn * capacity);
-    if (ce == cudaSuccess) ce = cudaMalloc(&dy, sizeof(float) * 2 * capacity);
-    if (ce == cudaSuccess) ce = cudaMalloc(&dc, sizeof(unsigned long long));
+    cudaError_t ce = jbp::dev_malloc(&dx, sizeof(float) * jbp::kMlpIn * capacity);
+    if (ce == cudaSuccess) ce = jbp::dev_malloc(&dy, sizeof(float) * 2 * capacity);
+    if (ce == cudaSuccess) ce = jbp::dev_malloc(&dc, sizeof(unsigned long long));
     if (ce == cudaSuccess) ce = cudaMemsetAsync(dc, 0, sizeof(unsigned long long), ctx->stream);
     std::string e;
     jbp_stats st;
@@ -456,7 +480,7 @@ int jbp_decode_errors_device(jbp_ctx *ctx, const jbp_options *opt, long long ntr
     std::string e = ctx->engine.run(rq, st);
     if (!e.empty()) {
         const int rc = engine_fail(e);
-        if (rc == JBP_ERR_TIMEOUT && stats) *stats = st;
+        if (partial_stats(rc) && stats) *stats = st;
         return rc;
     }
     if (stats) *stats = st;

@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <csignal>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -31,6 +32,22 @@
 #include "jbp_b200.h"
 
 namespace {
+
+// Ctrl-C during a simulation: every context is asked to stop (jbp_request_abort, a store to a
+// pinned host word); each run returns the trials that finished, and the Run Summary of those is
+// printed (exit status 130).  The context list is filled before the handler is installed.
+std::vector<jbp_ctx *> g_abort_ctxs;
+volatile std::sig_atomic_t g_interrupted = 0;
+
+extern "C" void on_interrupt(int) {
+    g_interrupted = 1;
+    for (jbp_ctx *c : g_abort_ctxs) jbp_request_abort(c);
+}
+
+void install_interrupt(const std::vector<jbp_ctx *> &ctxs) {
+    g_abort_ctxs = ctxs;
+    std::signal(SIGINT, on_interrupt);
+}
 
 struct Args {
     std::string params, sx_path, sz_path, err_path, est_path, hist_out, progress_tsv, ets_dir;
@@ -579,13 +596,20 @@ int simulate(jbp_ctx *ctx, const Args &a, int n) {
     jbp_stats acc{};
     const auto t0 = std::chrono::steady_clock::now();
     long long done = 0, next_report = a.report_every > 0 ? a.report_every : -1;
-    while (done < a.trials) {
+    while (done < a.trials && !g_interrupted) {
         const long long cnt = std::min(a.batch, a.trials - done);
         jbp_stats st{};
         std::fill(chunk_hist.begin(), chunk_hist.end(), 0);
         if (a.min_fails > 0) per.resize(cnt);
-        if (jbp_simulate(ctx, &o, a.seed, first + done, cnt, a.p, a.sampler, &st, a.min_fails > 0 ? per.data() : nullptr,
-                         chunk_hist.data()) != JBP_OK) {
+        const int rc = jbp_simulate(ctx, &o, a.seed, first + done, cnt, a.p, a.sampler, &st,
+                                    a.min_fails > 0 ? per.data() : nullptr, chunk_hist.data());
+        if (rc == JBP_ERR_ABORTED) {   // interrupted: keep the trials that finished
+            add_stats(acc, st);
+            for (size_t i = 0; i < hist.size(); ++i) hist[i] += chunk_hist[i];
+            done += st.trials;
+            break;
+        }
+        if (rc != JBP_OK) {
             std::cerr << "simulate failed: " << jbp_last_error() << "\n";
             return 1;
         }
@@ -634,8 +658,9 @@ int simulate(jbp_ctx *ctx, const Args &a, int n) {
         }
         std::cout << "Saved estimate: " << a.est_path << "\n";
     }
+    if (g_interrupted) std::cerr << "interrupted: " << done << " of " << a.trials << " trials decoded\n";
     print_run_summary(a, acc, hist, elapsed);
-    return 0;
+    return g_interrupted ? 130 : 0;
 }
 
 // --cuda-devices: the trial range split into contiguous parts, one per listed device (a device
@@ -668,7 +693,14 @@ int simulate_multi(const std::vector<jbp_ctx *> &ctxs, const Args &a) {
                 const long long cnt = std::min(a.batch, hi - b);
                 jbp_stats s{};
                 std::fill(h.begin(), h.end(), 0);
-                if (jbp_simulate(ctxs[d], &o, a.seed, b, cnt, a.p, a.sampler, &s, nullptr, h.data()) != JBP_OK) {
+                if (g_interrupted) return;
+                const int rc = jbp_simulate(ctxs[d], &o, a.seed, b, cnt, a.p, a.sampler, &s, nullptr, h.data());
+                if (rc == JBP_ERR_ABORTED) {   // interrupted: keep the trials that finished
+                    add_stats(st[d], s);
+                    for (size_t i = 0; i < h.size(); ++i) hist[d][i] += h[i];
+                    return;
+                }
+                if (rc != JBP_OK) {
                     errs[d] = jbp_last_error();
                     return;
                 }
@@ -691,8 +723,9 @@ int simulate_multi(const std::vector<jbp_ctx *> &ctxs, const Args &a) {
         for (size_t i = 0; i < all.size(); ++i) all[i] += hist[d][i];
     }
     std::cout << "devices=" << D << " trials_per_device=" << (a.trials + D - 1) / D << "\n";
+    if (g_interrupted) std::cerr << "interrupted: " << acc.trials << " of " << a.trials << " trials decoded\n";
     print_run_summary(a, acc, all, elapsed);
-    return 0;
+    return g_interrupted ? 130 : 0;
 }
 
 // A code as check lists ('n mx mz', then the variables of each X check and of each Z check, one
@@ -903,8 +936,11 @@ int main(int argc, char **argv) {
                       << "  girth_x=" << gx << "  girth_z=" << gz << "\n";
         }
     }
+    install_interrupt(ctxs);
     const int rc = !a.devices.empty() ? simulate_multi(ctxs, a)
                    : (a.simulate ? simulate(ctx, a, n) : decode_single(ctx, a, n, mx, mz));
+    std::signal(SIGINT, SIG_DFL);   // no abort request may reach a destroyed context
+    g_abort_ctxs.clear();
     destroy_all();
     return rc;
 }

@@ -2,6 +2,7 @@
 #include "engine.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <memory>
 #include <chrono>
 #include <cstring>
@@ -23,6 +24,37 @@ std::string cuda_err(cudaError_t e, const char *what) {
     return os.str();
 }
 
+namespace {
+std::atomic<long long> g_fail_after{-1};
+
+// true when the allocation being made is the one the hook fails
+bool take_alloc_failure() {
+    long long k = g_fail_after.load();
+    while (k >= 0) {
+        if (g_fail_after.compare_exchange_weak(k, k - 1)) return k == 0;
+    }
+    return false;
+}
+}  // namespace
+
+void set_alloc_failure(long long after) { g_fail_after.store(after < 0 ? -1 : after); }
+
+cudaError_t dev_malloc_bytes(void **p, size_t bytes) {
+    if (take_alloc_failure()) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaMalloc(p, bytes);
+}
+
+cudaError_t host_malloc_pinned(void **p, size_t bytes) {
+    if (take_alloc_failure()) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaHostAlloc(p, bytes, cudaHostAllocMapped);
+}
+
 #define JBP_CUDA_TRY(expr, what)                                  \
     do {                                                          \
         cudaError_t e_ = (expr);                                  \
@@ -35,7 +67,7 @@ template <typename T>
 std::string dev_upload(std::vector<void *> &allocs, const std::vector<T> &h, T **out) {
     *out = nullptr;
     size_t bytes = sizeof(T) * std::max<size_t>(h.size(), 1);
-    JBP_CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(out), bytes), "cudaMalloc(code)");
+    JBP_CUDA_TRY(dev_malloc(reinterpret_cast<void **>(out), bytes), "cudaMalloc(code)");
     allocs.push_back(*out);
     if (!h.empty()) JBP_CUDA_TRY(cudaMemcpy(*out, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice), "upload code");
     return "";
@@ -116,6 +148,7 @@ void fill_stats(const DevCounters &hc, jbp_stats &stats) {
 }  // namespace
 
 Engine::~Engine() {
+    if (abort_host_) cudaFreeHost(const_cast<int *>(abort_host_));
     if (slot_graph_.exec) cudaGraphExecDestroy(slot_graph_.exec);
     for (cudaEvent_t ev : run_ev_)
         if (ev) cudaEventDestroy(ev);
@@ -141,6 +174,14 @@ std::string Engine::init(CodeModel model, int device) {
     JBP_CUDA_TRY(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device), "device attributes");
     JBP_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin_, cudaDevAttrMaxSharedMemoryPerBlockOptin, device),
                  "device attributes");
+    {
+        int *flag = nullptr, *dflag = nullptr;
+        JBP_CUDA_TRY(host_malloc(&flag, sizeof(int)), "cudaHostAlloc(abort flag)");
+        abort_host_ = flag;
+        *abort_host_ = 0;
+        JBP_CUDA_TRY(cudaHostGetDevicePointer(reinterpret_cast<void **>(&dflag), flag, 0), "abort flag");
+        abort_dev_ = dflag;
+    }
     dcode_.n = model_.n;
     dcode_.words = (model_.n + 63) / 64;
     for (int s = 0; s < 2; ++s) {
@@ -265,7 +306,7 @@ std::string Engine::set_flip_model(const float *params) {
         return "";
     }
     JBP_CUDA_TRY(cudaSetDevice(device_), "cudaSetDevice");
-    if (!mlp_dev_) JBP_CUDA_TRY(cudaMalloc(&mlp_dev_, sizeof(uint32_t) * kMlpDevWords), "cudaMalloc(mlp)");
+    if (!mlp_dev_) JBP_CUDA_TRY(dev_malloc(&mlp_dev_, sizeof(uint32_t) * kMlpDevWords), "cudaMalloc(mlp)");
     std::vector<uint32_t> packed(kMlpDevWords);
     mlp_pack(params, packed.data());
     JBP_CUDA_TRY(cudaMemcpy(mlp_dev_, packed.data(), sizeof(uint32_t) * kMlpDevWords, cudaMemcpyHostToDevice),
@@ -295,7 +336,7 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     std::memset(&stats, 0, sizeof(stats));
     const jbp_options &o = rq.opt;
     JBP_CUDA_TRY(cudaSetDevice(device_), "cudaSetDevice");
-    if (!res_cnt_) JBP_CUDA_TRY(cudaMalloc(&res_cnt_, sizeof(DevCounters)), "cudaMalloc(counters)");
+    if (!res_cnt_) JBP_CUDA_TRY(dev_malloc(&res_cnt_, sizeof(DevCounters)), "cudaMalloc(counters)");
     const ResCode &rc = *rcode_;
     const bool pp = o.enable_pp != 0;
     // FP16 messages in shared memory; FP32 messages in a per-block global scratch (L2)
@@ -331,7 +372,7 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
             cudaFree(res_pp_scratch_);
             res_pp_scratch_ = nullptr;
             res_pp_bytes_ = 0;
-            JBP_CUDA_TRY(cudaMalloc(&res_pp_scratch_, need), "cudaMalloc(post-processing scratch)");
+            JBP_CUDA_TRY(dev_malloc(&res_pp_scratch_, need), "cudaMalloc(post-processing scratch)");
             res_pp_bytes_ = need;
         }
     }
@@ -342,7 +383,7 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
             cudaFree(res_c2v_scratch_);
             res_c2v_scratch_ = nullptr;
             res_c2v_bytes_ = 0;
-            JBP_CUDA_TRY(cudaMalloc(&res_c2v_scratch_, c2v_stride * grid), "cudaMalloc(message scratch)");
+            JBP_CUDA_TRY(dev_malloc(&res_c2v_scratch_, c2v_stride * grid), "cudaMalloc(message scratch)");
             res_c2v_bytes_ = c2v_stride * grid;
         }
     }
@@ -386,6 +427,7 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     r.col_count = rq.d_col_count;
     r.col_cap = rq.col_cap;
     r.budget_ns = o.watchdog_ms > 0 ? static_cast<unsigned long long>(o.watchdog_ms) * 1000000ull : 0ull;
+    r.abort_flag = abort_dev_;
     cudaStream_t st = rq.stream;
     cudaEvent_t ev0, ev1;
     JBP_CUDA_TRY(cudaEventCreate(&ev0), "cudaEventCreate");
@@ -414,6 +456,8 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     if (hc.watchdog)
         return "watchdog expired: the run budget of " + std::to_string(o.watchdog_ms) + " ms ran out on the device after " +
                std::to_string(hc.done) + " of " + std::to_string(rq.ntrials) + " trials";
+    if (hc.aborted)
+        return "aborted by request after " + std::to_string(hc.done) + " of " + std::to_string(rq.ntrials) + " trials";
     if (hc.done != static_cast<unsigned long long>(rq.ntrials)) return "resident run finished an unexpected number of trials";
     return "";
 }
@@ -478,49 +522,49 @@ std::string Engine::ensure_buffers(int S, int precision, bool damp, bool pp, int
     const size_t es = msg_elem_bytes(precision);
     for (int s = 0; s < 2; ++s) {
         const size_t bytes = es * static_cast<size_t>(model_.side[s].edges) * S;
-        JBP_CUDA_TRY(cudaMalloc(&buf_.msg[s], bytes), "cudaMalloc(c2v)");
-        JBP_CUDA_TRY(cudaMalloc(&buf_.msg[2 + s], bytes), "cudaMalloc(v2c)");
-        if (precision == JBP_PREC_FP64 && damp) JBP_CUDA_TRY(cudaMalloc(&buf_.msg[4 + s], bytes), "cudaMalloc(v2c hi)");
+        JBP_CUDA_TRY(dev_malloc(&buf_.msg[s], bytes), "cudaMalloc(c2v)");
+        JBP_CUDA_TRY(dev_malloc(&buf_.msg[2 + s], bytes), "cudaMalloc(v2c)");
+        if (precision == JBP_PREC_FP64 && damp) JBP_CUDA_TRY(dev_malloc(&buf_.msg[4 + s], bytes), "cudaMalloc(v2c hi)");
         buf_.msg_bytes += bytes * (precision == JBP_PREC_FP64 && damp ? 3 : 2);
     }
-    JBP_CUDA_TRY(cudaMalloc(&buf_.trial, sizeof(long long) * S), "cudaMalloc(slots)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.iter, sizeof(int) * S), "cudaMalloc(slots)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.flags, sizeof(int) * S), "cudaMalloc(slots)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.frz, sizeof(int) * S), "cudaMalloc(slots)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.unsat, sizeof(int) * 2 * S), "cudaMalloc(slots)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.prior, sizeof(double) * 4 * S), "cudaMalloc(slots)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.slot_p, sizeof(double) * S), "cudaMalloc(slots)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.lprior, sizeof(float) * 8 * S), "cudaMalloc(slots)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.err, static_cast<size_t>(n) * S), "cudaMalloc(err)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.trial, sizeof(long long) * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.iter, sizeof(int) * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.flags, sizeof(int) * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.frz, sizeof(int) * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.unsat, sizeof(int) * 2 * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.prior, sizeof(double) * 4 * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.slot_p, sizeof(double) * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.lprior, sizeof(float) * 8 * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.err, static_cast<size_t>(n) * S), "cudaMalloc(err)");
     const size_t G = static_cast<size_t>(S) / kGroup;
-    JBP_CUDA_TRY(cudaMalloc(&buf_.estx, sizeof(unsigned) * R * G * n), "cudaMalloc(est)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.estz, sizeof(unsigned) * R * G * n), "cudaMalloc(est)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.it, sizeof(int)), "cudaMalloc(it)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.estx, sizeof(unsigned) * R * G * n), "cudaMalloc(est)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.estz, sizeof(unsigned) * R * G * n), "cudaMalloc(est)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.it, sizeof(int)), "cudaMalloc(it)");
     if (pp) {
         const int mmax = std::max(model_.side[0].m, model_.side[1].m);
-        JBP_CUDA_TRY(cudaMalloc(&buf_.act_k, sizeof(int) * S), "cudaMalloc(pp)");
-        JBP_CUDA_TRY(cudaMalloc(&buf_.pstate, sizeof(int) * S), "cudaMalloc(pp)");
-        JBP_CUDA_TRY(cudaMalloc(&buf_.stall_same, sizeof(int) * S), "cudaMalloc(pp)");
-        JBP_CUDA_TRY(cudaMalloc(&buf_.pp_list, sizeof(int) * S), "cudaMalloc(pp)");
-        JBP_CUDA_TRY(cudaMalloc(&buf_.pp_mode, sizeof(int) * S), "cudaMalloc(pp)");
-        JBP_CUDA_TRY(cudaMalloc(&buf_.us_hist, sizeof(unsigned short) * 100 * S), "cudaMalloc(pp)");
-        JBP_CUDA_TRY(cudaMalloc(&buf_.dprev, sizeof(unsigned) * G), "cudaMalloc(pp)");
-        JBP_CUDA_TRY(cudaMalloc(&buf_.dpprev, sizeof(unsigned) * G), "cudaMalloc(pp)");
+        JBP_CUDA_TRY(dev_malloc(&buf_.act_k, sizeof(int) * S), "cudaMalloc(pp)");
+        JBP_CUDA_TRY(dev_malloc(&buf_.pstate, sizeof(int) * S), "cudaMalloc(pp)");
+        JBP_CUDA_TRY(dev_malloc(&buf_.stall_same, sizeof(int) * S), "cudaMalloc(pp)");
+        JBP_CUDA_TRY(dev_malloc(&buf_.pp_list, sizeof(int) * S), "cudaMalloc(pp)");
+        JBP_CUDA_TRY(dev_malloc(&buf_.pp_mode, sizeof(int) * S), "cudaMalloc(pp)");
+        JBP_CUDA_TRY(dev_malloc(&buf_.us_hist, sizeof(unsigned short) * 100 * S), "cudaMalloc(pp)");
+        JBP_CUDA_TRY(dev_malloc(&buf_.dprev, sizeof(unsigned) * G), "cudaMalloc(pp)");
+        JBP_CUDA_TRY(dev_malloc(&buf_.dpprev, sizeof(unsigned) * G), "cudaMalloc(pp)");
         JBP_CUDA_TRY(cudaMemsetAsync(buf_.dprev, 0, sizeof(unsigned) * G, st), "memset(pp)");
         JBP_CUDA_TRY(cudaMemsetAsync(buf_.dpprev, 0, sizeof(unsigned) * G, st), "memset(pp)");
         buf_.pp_stride = slot_pp_scratch_bytes(n, mmax);
         buf_.pp_blocks = std::min(sm_count_, static_cast<int>(S));
-        JBP_CUDA_TRY(cudaMalloc(&buf_.pp_scratch, buf_.pp_stride * buf_.pp_blocks), "cudaMalloc(pp scratch)");
+        JBP_CUDA_TRY(dev_malloc(&buf_.pp_scratch, buf_.pp_stride * buf_.pp_blocks), "cudaMalloc(pp scratch)");
     }
-    JBP_CUDA_TRY(cudaMalloc(&buf_.synm, sizeof(unsigned) * G * M), "cudaMalloc(syn)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.synm, sizeof(unsigned) * G * M), "cudaMalloc(syn)");
     JBP_CUDA_TRY(cudaMemsetAsync(buf_.synm, 0, sizeof(unsigned) * G * M, st), "memset(syn)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.unsat_mask, sizeof(unsigned) * 2 * G), "cudaMalloc(unsat)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.res_iters, sizeof(int) * S), "cudaMalloc(slots)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.res_flags, sizeof(int) * S), "cudaMalloc(slots)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.lists, sizeof(int) * (3 * S)), "cudaMalloc(lists)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.counts, sizeof(int) * 4), "cudaMalloc(lists)");
-    JBP_CUDA_TRY(cudaMalloc(&buf_.cnt, sizeof(DevCounters)), "cudaMalloc(counters)");
-    JBP_CUDA_TRY(cudaMallocHost(&buf_.h_done, sizeof(unsigned long long) * 2), "cudaMallocHost");
+    JBP_CUDA_TRY(dev_malloc(&buf_.unsat_mask, sizeof(unsigned) * 2 * G), "cudaMalloc(unsat)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.res_iters, sizeof(int) * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.res_flags, sizeof(int) * S), "cudaMalloc(slots)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.lists, sizeof(int) * (3 * S)), "cudaMalloc(lists)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.counts, sizeof(int) * 4), "cudaMalloc(lists)");
+    JBP_CUDA_TRY(dev_malloc(&buf_.cnt, sizeof(DevCounters)), "cudaMalloc(counters)");
+    JBP_CUDA_TRY(host_malloc(&buf_.h_done, sizeof(unsigned long long) * 2), "cudaMallocHost");
     // the memsets above are ordered on the run's stream (no device-wide synchronization: another
     // context may be capturing a graph on another host thread)
     buf_.S = S;
@@ -559,7 +603,22 @@ std::string validate_options(const jbp_options &o, double p) {
     return "";
 }
 
+// A request to abort applies to the run in progress (or the next run): it is cleared when that
+// run returns, on every path.
 std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
+    std::string e = run_dispatch(rq, stats);
+    clear_abort();
+    return e;
+}
+
+std::string Engine::run_mixed(const MixedRequest &rq, std::vector<jbp_stats> &stats) {
+    std::string e = run_mixed_impl(rq, stats);
+    for (Engine *eng : rq.engines)
+        if (eng) eng->clear_abort();
+    return e;
+}
+
+std::string Engine::run_dispatch(const RunRequest &rq, jbp_stats &stats) {
     std::memset(&stats, 0, sizeof(stats));
     const jbp_options &o = rq.opt;
     if (rq.ntrials <= 0) return "";
@@ -582,7 +641,7 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
         mr.d_llr = {rq.d_llr_out};
         mr.stream = rq.stream;
         std::vector<jbp_stats> st;
-        std::string e = run_mixed(mr, st);
+        std::string e = run_mixed_impl(mr, st);
         if (!st.empty()) stats = st[0];   // also on a run-budget stop: the trials that finished
         return e;
     }
@@ -821,7 +880,8 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
             if (ce == cudaSuccess) {
                 enqueue_iteration(cap, nullptr);
                 k_loop_cond<<<1, 32, 0, cap>>>(h, r.cnt, r.it, static_cast<unsigned long long>(rq.ntrials),
-                                               static_cast<int>(std::min<long long>(max_iters_total + 2, 1 << 30)));
+                                               static_cast<int>(std::min<long long>(max_iters_total + 2, 1 << 30)),
+                                               abort_dev_);
                 launches += 1;
                 cudaGraph_t captured = nullptr;
                 ce = cudaStreamEndCapture(cap, &captured);
@@ -881,7 +941,7 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     const long long max_graphs = max_iters_total / GI + 2;
     auto t0 = std::chrono::steady_clock::now();
     std::string err;
-    bool timed_out = false;
+    bool timed_out = false, aborted = false;
     if (ce != cudaSuccess) err = cuda_err(ce, "graph capture");
     long long g = 0;
     bool finished = false;
@@ -900,7 +960,8 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
         } else {
             launches += per_graph * std::max(0, *h_it - 1);
             finished = buf_.h_done[0] >= static_cast<unsigned long long>(rq.ntrials);
-            if (!finished) err = "run did not complete within the iteration bound (internal error)";
+            if (!finished && abort_requested()) aborted = true;   // k_loop_cond saw the flag
+            else if (!finished) err = "run did not complete within the iteration bound (internal error)";
         }
         g = max_graphs;   // the polling loop below has nothing to do
     }
@@ -924,8 +985,12 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
                 break;
             }
         }
+        if (!finished && abort_requested()) {
+            aborted = true;
+            break;
+        }
     }
-    if (err.empty() && !finished && !timed_out && g >= 1 && !device_loop) {
+    if (err.empty() && !finished && !timed_out && !aborted && g >= 1 && !device_loop) {
         ce = cudaEventSynchronize(poll_ev[(g - 1) & 1]);
         if (ce == cudaSuccess && buf_.h_done[(g - 1) & 1] >= static_cast<unsigned long long>(rq.ntrials)) finished = true;
         if (!finished) err = "run did not complete within the iteration bound (internal error)";
@@ -949,13 +1014,16 @@ std::string Engine::run(const RunRequest &rq, jbp_stats &stats) {
     if (timeout_err)
         err = "watchdog expired: the run budget of " + std::to_string(o.watchdog_ms) + " ms ran out (host check) after " +
               std::to_string(hc.done) + " of " + std::to_string(rq.ntrials) + " trials";
+    const bool abort_err = err.empty() && aborted && hc.done < static_cast<unsigned long long>(rq.ntrials);
+    if (abort_err)
+        err = "aborted by request after " + std::to_string(hc.done) + " of " + std::to_string(rq.ntrials) + " trials";
     for (int set = 0; set < 2; ++set) {
         if (exec[set] && !(sg.valid && exec[set] == sg.exec)) cudaGraphExecDestroy(exec[set]);
         if (graph[set]) cudaGraphDestroy(graph[set]);
     }
     for (auto &ev : pev) cudaEventDestroy(ev);
     if (cap) cudaStreamDestroy(cap);
-    if (!err.empty() && !timeout_err) return err;
+    if (!err.empty() && !timeout_err && !abort_err) return err;
     if (hc.bad_input) return "error vector has invalid value";
     fill_stats(hc, stats);
     stats.device_ms = ms;
@@ -986,7 +1054,10 @@ std::string Engine::sample_errors(unsigned long long seed, long long first, long
 // ---------------------------------------------------------------- mixed-size launch
 
 std::string Engine::mixed_slots() {
-    if (mix_slot_[0]) return "";
+    if (mix_slot_[0] && mix_slot_[1]) return "";
+    // both sides' tables are published together, only when every upload succeeded (a failed
+    // upload leaves none set, and the next call builds them again)
+    uint16_t *slot_tab[2] = {nullptr, nullptr}, *chk_tab[2] = {nullptr, nullptr};
     for (int s = 0; s < 2; ++s) {
         const SideGraph &g = model_.side[s];
         const int dv = std::max(1, g.dv_max), dc = g.dc_max, m = g.m, n = model_.n;
@@ -1003,12 +1074,13 @@ std::string Engine::mixed_slots() {
         for (int c = 0; c < m; ++c)
             for (int i = 0; i < dc; ++i)
                 ck[static_cast<size_t>(i) * m + c] = static_cast<uint16_t>(g.chk_var[static_cast<size_t>(c) * dc + i]);
-        uint16_t *p = nullptr, *q = nullptr;
-        std::string e = dev_upload(code_allocs_, sl, &p);
-        if (e.empty()) e = dev_upload(code_allocs_, ck, &q);
+        std::string e = dev_upload(code_allocs_, sl, &slot_tab[s]);
+        if (e.empty()) e = dev_upload(code_allocs_, ck, &chk_tab[s]);
         if (!e.empty()) return e;
-        mix_slot_[s] = p;
-        mix_chk_[s] = q;
+    }
+    for (int s = 0; s < 2; ++s) {
+        mix_slot_[s] = slot_tab[s];
+        mix_chk_[s] = chk_tab[s];
     }
     return "";
 }
@@ -1021,7 +1093,7 @@ void *mixed_kernel(int precision) {
 }
 }  // namespace
 
-std::string Engine::run_mixed(const MixedRequest &rq, std::vector<jbp_stats> &stats) {
+std::string Engine::run_mixed_impl(const MixedRequest &rq, std::vector<jbp_stats> &stats) {
     const int nc = static_cast<int>(rq.engines.size());
     stats.assign(static_cast<size_t>(std::max(nc, 0)), jbp_stats{});
     for (jbp_stats &s : stats) std::memset(&s, 0, sizeof(s));
@@ -1099,10 +1171,10 @@ std::string Engine::run_mixed(const MixedRequest &rq, std::vector<jbp_stats> &st
         cudaFree(e0.mix_scratch_);
         e0.mix_scratch_ = nullptr;
         e0.mix_scratch_bytes_ = 0;
-        JBP_CUDA_TRY(cudaMalloc(&e0.mix_scratch_, scratch * grid), "cudaMalloc(mixed scratch)");
+        JBP_CUDA_TRY(dev_malloc(&e0.mix_scratch_, scratch * grid), "cudaMalloc(mixed scratch)");
         e0.mix_scratch_bytes_ = scratch * grid;
     }
-    if (!e0.mix_cnt_) JBP_CUDA_TRY(cudaMalloc(&e0.mix_cnt_, sizeof(DevCounters) * (kMixMaxCodes + 1)),
+    if (!e0.mix_cnt_) JBP_CUDA_TRY(dev_malloc(&e0.mix_cnt_, sizeof(DevCounters) * (kMixMaxCodes + 1)),
                                    "cudaMalloc(mixed counters)");
     MixRun r{};
     r.ncodes = nc;
@@ -1117,6 +1189,7 @@ std::string Engine::run_mixed(const MixedRequest &rq, std::vector<jbp_stats> &st
     r.scratch = e0.mix_scratch_;
     r.scratch_stride = scratch;
     r.budget_ns = o.watchdog_ms > 0 ? static_cast<unsigned long long>(o.watchdog_ms) * 1000000ull : 0ull;
+    r.abort_flag = e0.abort_dev_;
     long long end = 0;
     for (int k = 0; k < nc; ++k) {
         const int i = order[k];
@@ -1176,6 +1249,8 @@ std::string Engine::run_mixed(const MixedRequest &rq, std::vector<jbp_stats> &st
     if (hc[0].watchdog)
         return "watchdog expired: the run budget of " + std::to_string(o.watchdog_ms) + " ms ran out on the device after " +
                std::to_string(done) + " of " + std::to_string(total) + " trials";
+    if (hc[0].aborted)
+        return "aborted by request after " + std::to_string(done) + " of " + std::to_string(total) + " trials";
     for (int k = 0; k < nc; ++k)
         if (hc[k].done != static_cast<unsigned long long>(rq.ntrials[order[k]]))
             return "mixed run finished an unexpected number of trials";

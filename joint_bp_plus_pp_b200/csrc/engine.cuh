@@ -89,6 +89,7 @@ struct DevCounters {
     unsigned long long bad_input;   // error bytes outside 0..3 seen in a kSrcErrors source
     unsigned long long learned_attempts, learned_success;   // learned flip proposals tried / saves
     unsigned long long syndrome_tests;   // slot engine: per-trial syndrome tests run
+    unsigned long long aborted;          // blocks (persistent kernels) that stopped on the abort flag
 };
 
 struct DevRun {

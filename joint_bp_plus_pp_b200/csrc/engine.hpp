@@ -71,6 +71,14 @@ public:
     // Learned flip proposal parameters (FP32, mlp.cuh layout); null removes the model.
     std::string set_flip_model(const float *params);
     int sm_count() const { return sm_count_; }
+    // Asks the run in progress (or the next run) to stop; any host thread (jbp_request_abort).
+    void request_abort() {
+        if (abort_host_) *abort_host_ = 1;
+    }
+    bool abort_requested() const { return abort_host_ && *abort_host_ != 0; }
+    void clear_abort() {
+        if (abort_host_) *abort_host_ = 0;
+    }
     // One launch over the codes of rq.engines; stats[i] for code i.
     static std::string run_mixed(const MixedRequest &rq, std::vector<jbp_stats> &stats);
 
@@ -106,6 +114,8 @@ private:
     // Trial-resident tier (kernels_resident.cuh): whether a run can use it, and the run.
     bool resident_applies(const jbp_options &o, std::string *why) const;
     std::string run_resident(const RunRequest &rq, jbp_stats &stats);
+    std::string run_dispatch(const RunRequest &rq, jbp_stats &stats);
+    static std::string run_mixed_impl(const MixedRequest &rq, std::vector<jbp_stats> &stats);
     std::string build_res_code();
 
     std::string ensure_buffers(int S, int precision, bool damp, bool pp, int R, cudaStream_t st);
@@ -135,6 +145,8 @@ private:
 
     int device_ = 0;
     int sm_count_ = 0;
+    volatile int *abort_host_ = nullptr;   // jbp_request_abort's flag, mapped pinned host memory
+    const volatile int *abort_dev_ = nullptr;   // ... the device's address of it (the kernels poll it)
     const uint16_t *mix_slot_[2] = {nullptr, nullptr};   // [dv][n] message slot of each variable's edges
     const uint16_t *mix_chk_[2] = {nullptr, nullptr};    // [dc][m] variable of each check's edges
     unsigned char *mix_scratch_ = nullptr;   // per-block c2v of the codes that do not fit shared memory
@@ -161,6 +173,22 @@ private:
 };
 
 std::string cuda_err(cudaError_t e, const char *what);
+
+// Every device and (mapped) pinned-host allocation of the library goes through these, so that the test
+// hook jbp_debug_fail_allocation can make the n-th one fail (cudaErrorMemoryAllocation, without
+// calling the runtime): the failure path of each allocation site is exercised from the host.
+cudaError_t dev_malloc_bytes(void **p, size_t bytes);
+cudaError_t host_malloc_pinned(void **p, size_t bytes);
+template <class T>
+inline cudaError_t dev_malloc(T **p, size_t bytes) {
+    return dev_malloc_bytes(reinterpret_cast<void **>(p), bytes);
+}
+template <class T>
+inline cudaError_t host_malloc(T **p, size_t bytes) {
+    return host_malloc_pinned(reinterpret_cast<void **>(p), bytes);
+}
+// after >= 0: the allocation that many allocations from now fails (0 = the next), once; < 0: off.
+void set_alloc_failure(long long after);
 
 // The option checks every decoding entry point shares (error rate, prior, precision, damping,
 // engine, iteration and time limits): "" when the options are valid, else why not.

@@ -60,6 +60,7 @@ struct MixRun {
     unsigned char *scratch;        // per block, scratch_stride bytes (c2v of the codes that do not fit)
     size_t scratch_stride;
     unsigned long long budget_ns;  // run budget as ResRun::budget_ns; stops are counted in code[0].cnt
+    const volatile int *abort_flag;   // as ResRun::abort_flag (the first context's), read at item claims
 };
 
 __host__ __device__ inline size_t mix_align(size_t b) { return (b + 15) / 16 * 16; }
@@ -173,7 +174,7 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant_
     __shared__ float lpx_sh, lpz_sh;
     __shared__ float first_sh[2][DC];   // first-iteration c2v of each position (syndrome bit 0)
     __shared__ int ints[16];
-    __shared__ int abort_sh;   // the run budget ran out during this trial
+    __shared__ int abort_sh;   // 1: the run budget ran out during this trial; 2: abort requested
     if (threadIdx.x < 16) ints[threadIdx.x] = 0;
     __shared__ unsigned long long deadline_sh;   // global-timer end of the run budget (0 = none)
     if (threadIdx.x == 0) deadline_sh = run.budget_ns ? dev_globaltimer() + run.budget_ns : 0ull;
@@ -185,6 +186,9 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant_
             if (item >= 0 && deadline_sh && dev_globaltimer() > deadline_sh) {
                 item = -1;   // the run budget is spent: no further trial
                 atomicAdd(&run.code[0].cnt->watchdog, 1ull);
+            } else if (item >= 0 && k % kResAbortEvery == 0 && *run.abort_flag) {
+                item = -1;   // abort requested: no further trial
+                atomicAdd(&run.code[0].cnt->aborted, 1ull);
             }
             abort_sh = 0;
             int ci = 0;
@@ -299,9 +303,10 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant_
             }
             // run budget (as k_resident): thread 0 writes the flag before the barrier, every thread
             // reads it after it
-            if (threadIdx.x == 0 && it % kResBudgetEvery == kResBudgetEvery - 1 && deadline_sh &&
-                dev_globaltimer() > deadline_sh)
-                abort_sh = 1;
+            if (threadIdx.x == 0 && it % kResBudgetEvery == kResBudgetEvery - 1) {
+                if (deadline_sh && dev_globaltimer() > deadline_sh) abort_sh = 1;
+                else if (it >= kResAbortFrom && *run.abort_flag) abort_sh = 2;
+            }
             const bool any = __syncthreads_or(bad) != 0;
             if (fused && !any) { rf = kResSyndromeOk | kResBpOk; iters = it; break; }
             if (it >= run.max_iter || abort_sh) break;
@@ -312,7 +317,8 @@ __global__ void __launch_bounds__(kMixThreads, 1) k_mixed(const __grid_constant_
         }
         if (abort_sh && rf == 0 && it < run.max_iter) {
             // abandoned for the run budget: not classified, not counted; the block stops
-            if (threadIdx.x == 0) atomicAdd(&run.code[0].cnt->watchdog, 1ull);
+            if (threadIdx.x == 0)
+                atomicAdd(abort_sh == 2 ? &run.code[0].cnt->aborted : &run.code[0].cnt->watchdog, 1ull);
             break;
         }
         const bool ok = (rf & kResSyndromeOk) != 0;

@@ -107,9 +107,15 @@ struct ResRun {
     // from its start) claims no further trial and abandons the one it decodes at its next check
     // (every kResBudgetEvery iterations); cnt->watchdog counts the blocks that stopped so
     unsigned long long budget_ns;
+    // jbp_request_abort's flag (pinned host memory): a block that sees it set claims no further
+    // trial; it looks at every kResAbortEvery-th claim and, in a trial past iteration
+    // kResAbortFrom, every kResBudgetEvery iterations; cnt->aborted counts the blocks that stopped
+    const volatile int *abort_flag;
 };
 
 constexpr int kResBudgetEvery = 16;   // iterations between two run-budget checks of a block
+constexpr unsigned long long kResAbortEvery = 8;   // trial claims between two reads of the abort flag
+constexpr int kResAbortFrom = 64;      // iteration from which a long trial also reads it
 
 // Nanoseconds of the GPU's global timer (the run budget of the persistent kernels).
 __device__ __forceinline__ unsigned long long dev_globaltimer() {
@@ -784,7 +790,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
     const int slow_from = PP ? max(1, llr_from - 2) : 0x7fffffff;
 
     __shared__ double pt_sh;
-    __shared__ int abort_sh;          // the run budget ran out during this trial
+    __shared__ int abort_sh;          // 1: the run budget ran out during this trial; 2: abort requested
     // global-timer end of the run budget (0 = none), in shared memory so that the BP loop keeps
     // no register for it
     __shared__ unsigned long long deadline_sh;
@@ -807,6 +813,9 @@ __global__ void __launch_bounds__(kResThreads, 1)
             if (trial_sh >= 0 && deadline_sh && dev_globaltimer() > deadline_sh) {
                 trial_sh = -1;   // the run budget is spent: no further trial
                 atomicAdd(&run.cnt->watchdog, 1ull);
+            } else if (trial_sh >= 0 && k % kResAbortEvery == 0 && *run.abort_flag) {
+                trial_sh = -1;   // abort requested: no further trial
+                atomicAdd(&run.cnt->aborted, 1ull);
             }
             abort_sh = 0;
             pp_sh[1] = 0;   // act_k
@@ -939,9 +948,10 @@ __global__ void __launch_bounds__(kResThreads, 1)
             // is read by every thread after the barrier below (at the iteration-limit exit, which
             // keeps the loop's register use as it was) and written again only after the next
             // variable phase's barrier
-            if (threadIdx.x == 0 && it % kResBudgetEvery == kResBudgetEvery - 1 && deadline_sh &&
-                dev_globaltimer() > deadline_sh)
-                abort_sh = 1;
+            if (threadIdx.x == 0 && it % kResBudgetEvery == kResBudgetEvery - 1) {
+                if (deadline_sh && dev_globaltimer() > deadline_sh) abort_sh = 1;
+                else if (it >= kResAbortFrom && *run.abort_flag) abort_sh = 2;
+            }
             const int nbad = __syncthreads_count(bx + bz != 0);
             if (fused) {
                 if (nbad == 0) { rf = kResSyndromeOk | kResBpOk; iters = it; break; }
@@ -987,7 +997,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
         }
         if (abort_sh && rf == 0 && it < run.max_iter) {
             // abandoned for the run budget: not classified, not counted; the block stops
-            if (threadIdx.x == 0) atomicAdd(&run.cnt->watchdog, 1ull);
+            if (threadIdx.x == 0) atomicAdd(abort_sh == 2 ? &run.cnt->aborted : &run.cnt->watchdog, 1ull);
             break;
         }
         const bool ok = (rf & kResSyndromeOk) != 0;

@@ -622,11 +622,13 @@ static __global__ void k_fresh_syndrome(DevCode code, DevRun run) {
 }
 
 // The condition of the slot engine's device-side iteration loop (a CUDA graph while node whose
-// body is one BP iteration): go on while trials are left and the iteration bound, which every
-// run reaches only by an internal error, is not.
+// body is one BP iteration): go on while trials are left, the iteration bound, which every
+// run reaches only by an internal error, is not, and no abort is requested (jbp_request_abort's
+// flag, a pinned host word).
 static __global__ void k_loop_cond(cudaGraphConditionalHandle h, const DevCounters *cnt, const int *it,
-                                   unsigned long long ntrials, int it_bound) {
-    if (threadIdx.x == 0) cudaGraphSetConditional(h, (cnt->done < ntrials && *it < it_bound) ? 1u : 0u);
+                                   unsigned long long ntrials, int it_bound, const volatile int *abort_flag) {
+    if (threadIdx.x == 0)
+        cudaGraphSetConditional(h, (cnt->done < ntrials && *it < it_bound && !*abort_flag) ? 1u : 0u);
 }
 
 // Compacts the groups that still hold a running slot and advances the global iteration

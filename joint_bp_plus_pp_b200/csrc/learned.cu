@@ -169,7 +169,7 @@ struct DevBuf {
 };
 
 std::string alloc(DevBuf &b, size_t bytes) {
-    cudaError_t e = cudaMalloc(&b.p, std::max<size_t>(bytes, 16));
+    cudaError_t e = jbp::dev_malloc(&b.p, std::max<size_t>(bytes, 16));
     return e == cudaSuccess ? "" : cuda_err(e, "cudaMalloc(mlp)");
 }
 
