@@ -232,6 +232,13 @@ int jbp_measure_sfu(int device, double *ex2_gops, double *lg2_gops, double *rcp_
  * reference: the bit-exact FP64 decoder depends on it.  About 1 ms of GPU time per 10^8. */
 int jbp_check_reciprocal(int device, unsigned long long seed, long long n, long long *mismatches,
                          long long *first_mismatch);
+/* Device self-check of the us-signal oscillation test of the post-processing trigger
+ * (detect_us_oscillation, jointbp_ets.cpp:2021-2053): the one-pass form the slot engine uses
+ * and the warp-parallel form of the trial-resident kernel against the rule as written, on n
+ * seeded histories (constant, noisy, alternating, ramps, spikes, steps).  mismatches gets the
+ * disagreements, fired (may be null) how many histories the rule accepts. */
+int jbp_check_us_oscillation(int device, unsigned long long seed, long long n, long long *mismatches,
+                             long long *fired);
 /* Gradient of the mean loss (binary cross-entropy with logits, positives weighted by
  * pos_weight, summed over the two outputs) on the GPU; grad_out has jbp_mlp_param_count()
  * entries. */

@@ -144,6 +144,7 @@ def load_library(path=None):
     lib.jbp_check_reciprocal.argtypes = [i, ctypes.c_ulonglong, ll, ctypes.POINTER(ll), ctypes.POINTER(ll)]
     lib.jbp_debug_fail_allocation.argtypes = [ll]
     lib.jbp_request_abort.argtypes = [vp]
+    lib.jbp_check_us_oscillation.argtypes = [i, ctypes.c_ulonglong, ll, ctypes.POINTER(ll), ctypes.POINTER(ll)]
     lib.jbp_simulate_mixed.argtypes = [vp, i, ctypes.POINTER(COptions), vp, vp, vp, d, ctypes.POINTER(CStats), vp]
     lib.jbp_decode_errors_device.argtypes = [vp, ctypes.POINTER(COptions), ll, vp, d, vp, vp, ctypes.POINTER(CStats),
                                              vp]
@@ -395,6 +396,15 @@ def debug_fail_allocation(after):
     JbpError; after < 0 turns the hook off."""
     lib = load_library()
     _check(lib, lib.jbp_debug_fail_allocation(int(after)))
+
+
+def check_us_oscillation(n, seed=1, device=0):
+    """Device self-check of the two forms of the us-signal oscillation test against the rule as
+    the reference states it: (mismatches, histories the rule accepts)."""
+    lib = load_library()
+    bad, fired = ctypes.c_longlong(), ctypes.c_longlong()
+    _check(lib, lib.jbp_check_us_oscillation(device, seed, n, ctypes.byref(bad), ctypes.byref(fired)))
+    return bad.value, fired.value
 
 
 def check_reciprocal(n, seed=1, device=0):

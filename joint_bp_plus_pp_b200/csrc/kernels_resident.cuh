@@ -685,19 +685,24 @@ __device__ __noinline__ int res_slow_step(const ResCode &code, const ResRun &run
     }
     const bool same = __syncthreads_and(s1) != 0;
     const bool pp2 = __syncthreads_and(s2) != 0;
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
+        // the triggers, in warp 0 (the us-signal test over its 100 samples by the whole warp)
         const int sig = max(us.x, us.y);
-        us_hist[it % 100] = static_cast<unsigned short>(min(sig, 65535));
-        const bool osc = pp2 && !same;
+        if (threadIdx.x == 0) us_hist[it % 100] = static_cast<unsigned short>(min(sig, 65535));
+        __syncwarp();
         const bool allow = it >= 100 || it == run.max_iter;
         int st = pp_sh[2];
-        bool act = false;
-        if (!(st & 1) && (same || it == run.max_iter) && allow) { st |= 1; act = true; }
-        if (!(st & 2) && osc && allow) { st |= 2; act = true; }
-        if (!(st & 4) && allow && us_oscillation(us_hist, it)) { st |= 4; act = true; }
-        pp_sh[2] = st;
-        if (act && pp_sh[1] == 0 && run.flip_hist > 0) pp_sh[1] = it;
-        pp_sh[0] = (st && sig <= 20) ? kPpInLoop : (it >= run.max_iter ? kPpPost : 0);
+        const bool us_osc = !(st & 4) && allow && us_oscillation_warp(us_hist, it);   // warp-uniform
+        if (threadIdx.x == 0) {
+            const bool osc = pp2 && !same;
+            bool act = false;
+            if (!(st & 1) && (same || it == run.max_iter) && allow) { st |= 1; act = true; }
+            if (!(st & 2) && osc && allow) { st |= 2; act = true; }
+            if (us_osc) { st |= 4; act = true; }
+            pp_sh[2] = st;
+            if (act && pp_sh[1] == 0 && run.flip_hist > 0) pp_sh[1] = it;
+            pp_sh[0] = (st && sig <= 20) ? kPpInLoop : (it >= run.max_iter ? kPpPost : 0);
+        }
     }
     __syncthreads();
     // learned flip proposal at a stall (decisions unchanged or oscillating)

@@ -163,37 +163,89 @@ static __global__ void __launch_bounds__(256) k_stall_compare(DevCode code, DevR
     }
 }
 
-// Counts the finished iteration; a slot retires when its checked syndrome matches or it
-// reaches max_iter (the CPU's iteration accounting, jointbp_ets.cpp:2733-2735, 3078).
 // detect_us_oscillation (jointbp_ets.cpp:2021-2053) over the last 100 samples of
 // max(us_x, us_z), kept by iteration number modulo 100 (samples k1-99 .. k1).
 static __device__ bool us_oscillation(const unsigned short *h, int k1) {
     if (k1 < 100) return false;
-    int mn = h[(k1 - 99) % 100], mx = mn;
-    long long sum = 0;
-    for (int j = k1 - 99; j <= k1; ++j) {
-        const int v = h[j % 100];
+    // one pass over the window k1-99 .. k1 (ring position advanced without a division per entry):
+    // range, sum, and the sign changes of the successive differences
+    int idx = (k1 - 99) % 100;
+    int prev = h[idx], mn = prev, mx = prev;
+    long long sum = prev;
+    int prev_sign = 0, turns = 0;
+    for (int i = 1; i < 100; ++i) {
+        if (++idx == 100) idx = 0;
+        const int v = h[idx];
         mn = v < mn ? v : mn;
         mx = v > mx ? v : mx;
         sum += v;
+        const int d = v - prev;
+        const int sg = d > 0 ? 1 : (d < 0 ? -1 : 0);
+        if (sg) {
+            if (prev_sign && sg != prev_sign) turns++;
+            prev_sign = sg;
+        }
+        prev = v;
     }
     const double mean = static_cast<double>(sum) / 100.0;
     if (mean <= 0.0) return false;
     int min_range = static_cast<int>(mean * 0.2);
     if (min_range < 10) min_range = 10;
     if (mx - mn < min_range) return false;
-    int prev_sign = 0, turns = 0;
-    for (int j = k1 - 98; j <= k1; ++j) {
-        const int d = static_cast<int>(h[j % 100]) - static_cast<int>(h[(j - 1) % 100]);
-        const int sg = d > 0 ? 1 : (d < 0 ? -1 : 0);
-        if (sg) {
-            if (prev_sign && sg != prev_sign) turns++;
-            prev_sign = sg;
-        }
-    }
     return turns >= 2;
 }
 
+// us_oscillation computed by the 32 lanes of a warp (all call it; every lane gets the result).
+// Each lane takes window entries lane, lane + 32, ...; min, max and sum reduce exactly.  Two or
+// more sign changes among the nonzero signs of the successive differences happen exactly when
+// both signs occur and each sign occurs after some occurrence of the other (a sequence with at
+// most one change is all of one sign, then all of the other): with P and N the positions of
+// the rises and falls, maxP > minN and maxN > minP.
+static __device__ bool us_oscillation_warp(const unsigned short *h, int k1) {
+    if (k1 < 100) return false;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, base = k1 - 99;
+    int mn = 0x7fffffff, mx = -1, sum = 0;
+    unsigned rise[4], fall[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int i = c * 32 + lane;
+        int d = 0;
+        if (i < 100) {
+            const int v = h[(base + i) % 100];
+            mn = v < mn ? v : mn;
+            mx = v > mx ? v : mx;
+            sum += v;
+            if (i > 0) d = v - static_cast<int>(h[(base + i - 1) % 100]);
+        }
+        rise[c] = __ballot_sync(full, d > 0);
+        fall[c] = __ballot_sync(full, d < 0);
+    }
+    mn = __reduce_min_sync(full, mn);
+    mx = __reduce_max_sync(full, mx);
+    sum = __reduce_add_sync(full, sum);
+    const double mean = static_cast<double>(sum) / 100.0;
+    if (mean <= 0.0) return false;
+    int min_range = static_cast<int>(mean * 0.2);
+    if (min_range < 10) min_range = 10;
+    if (mx - mn < min_range) return false;
+    int minP = -1, maxP = -1, minN = -1, maxN = -1;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        if (rise[c]) {
+            if (minP < 0) minP = c * 32 + __ffs(rise[c]) - 1;
+            maxP = c * 32 + 31 - __clz(rise[c]);
+        }
+        if (fall[c]) {
+            if (minN < 0) minN = c * 32 + __ffs(fall[c]) - 1;
+            maxN = c * 32 + 31 - __clz(fall[c]);
+        }
+    }
+    return minP >= 0 && minN >= 0 && maxP > minN && maxN > minP;
+}
+
+// Counts the finished iteration; a slot retires when its checked syndrome matches or it
+// reaches max_iter (the CPU's iteration accounting, jointbp_ets.cpp:2733-2735, 3078).
 static __global__ void k_retire(DevRun run) {
     const int gi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (gi >= *run.n_groups) return;

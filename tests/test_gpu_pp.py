@@ -109,3 +109,14 @@ def test_llr_precisions_with_pp_run(decoder, prec):
     st, r, _ = decoder.decode_errors(errs, meta["p"], opts_for(meta, prec), want_est=False)
     assert st["trials"] == len(errs)
     assert abs(st["failures"] - st64["failures"]) <= max(3, len(errs) // 4)
+
+
+def test_us_oscillation_forms_agree_with_the_rule():
+    """The one-pass and warp-parallel forms of the us-signal oscillation trigger give the
+    reference rule's answer (jointbp_ets.cpp:2021-2053) on 2,000,000 seeded histories, of which
+    a good share fire and a good share do not (ramps, i.e. one turn, included)."""
+    from joint_bp_plus_pp_b200 import check_us_oscillation
+    n = 2_000_000
+    bad, fired = check_us_oscillation(n, seed=5)
+    assert bad == 0
+    assert 0.1 * n < fired < 0.9 * n, fired
