@@ -320,13 +320,26 @@ __device__ __forceinline__ int var_f64_update(const DevRun &run, const DevMsgs &
     // total = normalize(prior * (PX * PZ)); est = first argmax
     double t0 = dmul(p0, dmul(XA, ZA)), t1 = dmul(p1, dmul(XB, ZA));
     double t2 = dmul(p2, dmul(XA, ZB)), t3 = dmul(p3, dmul(XB, ZB));
-    if (FAST) norm4_fast(t0, t1, t2, t3, ok);
-    else norm4(t0, t1, t2, t3);
     int best = 0;
-    double bv = t0;
-    if (t1 > bv) { best = 1; bv = t1; }
-    if (t2 > bv) { best = 2; bv = t2; }
-    if (t3 > bv) { best = 3; }
+    if (FAST) {
+        // The total serves only its first maximum.  Normalizing divides by one positive sum: it
+        // keeps the order and merges only values within a rounding of each other, so when every
+        // earlier entry is below the maximum by a relative 2^-50 (two roundings of 2^-53 cannot
+        // close that gap) and the maximum is normal, the first maximum of the unnormalized total
+        // is that of the normalized one.  Otherwise the exact path decides.
+        double bv = t0;
+        if (t1 > bv) { best = 1; bv = t1; }
+        if (t2 > bv) { best = 2; bv = t2; }
+        if (t3 > bv) { best = 3; bv = t3; }
+        const double lim = dmul(bv, 1.0 - 0x1p-50);
+        ok = ok && bv >= 0x1p-1000 && (best < 1 || t0 < lim) && (best < 2 || t1 < lim) && (best < 3 || t2 < lim);
+    } else {
+        norm4(t0, t1, t2, t3);
+        double bv = t0;
+        if (t1 > bv) { best = 1; bv = t1; }
+        if (t2 > bv) { best = 2; bv = t2; }
+        if (t3 > bv) { best = 3; }
+    }
     // (the |LLR| keys of the OSD order are computed from the same messages by the block
     // that post-processes the slot: kernels_slot_pp.cuh)
     double2 *v2cx = static_cast<double2 *>(msg.v2c[0]);

@@ -140,8 +140,9 @@ def test_resident_refuses_what_it_does_not_run(decoder):
 def test_resident_pp_stage_trials(decoder, oracle, prec):
     """Errors that make each post-processing stage act (constructed trapping-set errors and
     sampled trials), decoded with the stages inside the resident kernel: its flags agree with
-    the oracle's classification of its own estimates, and its outcomes agree with the
-    reference's FP64 records on nearly every case (the BP before the stages is FP32)."""
+    the oracle's classification of its own estimates, and its estimates and records agree with
+    the reference's FP64 records on at least 97% and 94% of the cases (the BP before the stages
+    is FP32 / FP16)."""
     from test_gpu_pp import gpu_record, golden_record, load_stage_trials
     total = same_est = same_rec = 0
     for (p, mi, fh), cases in sorted(load_stage_trials(decoder.n).items()):
@@ -153,8 +154,11 @@ def test_resident_pp_stage_trials(decoder, oracle, prec):
             total += 1
             same_est += bool((e == est_ref).all())
             same_rec += gpu_record(r) == golden_record(rec)
-    assert same_est >= 0.85 * total, (same_est, total)
-    assert same_rec >= 0.8 * total, (same_rec, total)
+    # measured on a B200: same estimate 178 / 181 (FP16 and FP32), same record 172 / 181 (FP16),
+    # 175 / 181 (FP32); the rest are trapping-set cases on which the FP32 / FP16 BP before the
+    # stages leaves a different state from the FP64 BP, so a stage sees other decisions
+    assert same_est >= 0.97 * total, (same_est, total)
+    assert same_rec >= 0.94 * total, (same_rec, total)
 
 
 @pytest.mark.parametrize("prec", ["fp16", "fp32"])
@@ -167,8 +171,10 @@ def test_resident_pp_ler_close_to_fp64(decoder, name, prec):
     st, r, _ = decoder.decode_errors(errs, meta["p"], ropts(max_iter=meta["max_iter"], flip_hist=meta["flip_hist"],
                                                             enable_pp=True, precision=prec), want_est=False)
     assert st["trials"] == len(errs) and st["kernel_launches"] == 1
-    assert abs(st["failures"] - st64["failures"]) <= max(3, len(errs) // 4)
-    assert (r["success"] != r64["success"]).mean() <= 0.1
+    # measured on a B200: 0 / 0 failures of 40 (p = 0.05) and 21 / 21 of 24 (p = 0.06), no outcome
+    # disagreement, in both precisions
+    assert abs(st["failures"] - st64["failures"]) <= 2
+    assert (r["success"] != r64["success"]).sum() <= 2
 
 
 def test_resident_pp_saves_trials(decoder):
