@@ -192,10 +192,16 @@ __host__ __device__ inline size_t res_base_bytes(int n, int m, int L, size_t sto
     const size_t syn = (2ull * ((m + 31) / 32) + 3) / 4 * 4 * 4;
     return c2v + A + err + syn + 64;
 }
+// The slow path's decision planes (post-processing instantiations): the x and z decisions of
+// the last three iterations, 32 qubits per word, after the post-processing arrays.
+__host__ __device__ inline size_t res_plane_bytes(int n) { return 3ull * 2 * ((n + 31) / 32) * 4; }
+__host__ __device__ inline size_t res_plane_offset(size_t pp_smem_base, int n, int m) {
+    return pp_smem_base + pp_smem_bytes(n, 2 * m, m) + 256;
+}
 __host__ __device__ inline size_t res_smem_bytes(int n, int m, int L, size_t store_bytes, bool pp,
                                                  int c2v_sides_in_smem = 2) {
     const size_t base = res_base_bytes(n, m, L, store_bytes, c2v_sides_in_smem);
-    return pp ? pp_align(base) + pp_smem_bytes(n, 2 * m, m) + 256 : base;
+    return pp ? res_plane_offset(pp_align(base), n, m) + res_plane_bytes(n) : base;
 }
 
 
@@ -657,7 +663,6 @@ __device__ __noinline__ int res_slow_step(const ResCode &code, const ResRun &run
                                           unsigned short *us_hist, int *pp_sh, int *ints, bool slow) {
     constexpr int n = L * P;
     const ResPpPtrs q = res_pp_ptrs<P, J, L, ST>(run, smem);
-    const uint8_t *ring = q.ring;
     const int R = q.R;
     const int2 us = res_block_sum2(res_test_side<P, J, L>(code, A, syn, 0), res_test_side<P, J, L>(code, A, syn, 1),
                                    ints);
@@ -671,17 +676,29 @@ __device__ __noinline__ int res_slow_step(const ResCode &code, const ResRun &run
         return res_learned_attempt<P, J, L, ST>(code, run, smem, c2v, c2vz, A, syn, err, have_err, it, t, lp)
                    ? (kResSyndromeOk | kResLearned) : 0;
     }
+    // this iteration's decisions: a byte per qubit in the global ring (the flip window reads it)
+    // and x / z bit planes in shared memory, 32 qubits per word, for the stall tests
+    constexpr int W = (n + 31) / 32;
+    uint32_t *planes = reinterpret_cast<uint32_t *>(smem + res_plane_offset(run.pp_smem_base, n, J * P));
+    uint32_t *pc = planes + (it % 3) * 2 * W;
+    const uint32_t *pl1 = planes + ((it + 2) % 3) * 2 * W, *pl2 = planes + ((it + 1) % 3) * 2 * W;
     uint8_t *cur = q.ring + static_cast<size_t>(it % R) * n;
-    for (int v = threadIdx.x; v < n; v += blockDim.x)
-        cur[v] = static_cast<uint8_t>((__float_as_uint(A[v]) & 1u) | ((__float_as_uint(A[n + v]) & 1u) << 1));
+    for (int base = (threadIdx.x >> 5) * 32; base < n; base += blockDim.x) {
+        const int v = base + (threadIdx.x & 31);
+        const unsigned xb = v < n ? __float_as_uint(A[v]) & 1u : 0u, zb = v < n ? __float_as_uint(A[n + v]) & 1u : 0u;
+        if (v < n) cur[v] = static_cast<uint8_t>(xb | (zb << 1));
+        const unsigned xw = __ballot_sync(0xffffffffu, xb), zw = __ballot_sync(0xffffffffu, zb);
+        if ((threadIdx.x & 31) == 0) {
+            pc[base >> 5] = xw;
+            pc[W + (base >> 5)] = zw;
+        }
+    }
     __syncthreads();
-    // est == prev_est / prev_prev_est (jointbp_ets.cpp:2555-2556)
-    const uint8_t *p1 = ring + static_cast<size_t>((it - 1) % R) * n;
-    const uint8_t *p2 = ring + static_cast<size_t>((it - 2 + R) % R) * n;
+    // est == prev_est / prev_prev_est (jointbp_ets.cpp:2555-2556), word by word
     bool s1 = it >= 2, s2 = it >= 3;
-    for (int v = threadIdx.x; v < n; v += blockDim.x) {
-        if (s1) s1 = cur[v] == p1[v];
-        if (s2) s2 = cur[v] == p2[v];
+    for (int w = threadIdx.x; w < 2 * W; w += blockDim.x) {
+        if (s1) s1 = pc[w] == pl1[w];
+        if (s2) s2 = pc[w] == pl2[w];
     }
     const bool same = __syncthreads_and(s1) != 0;
     const bool pp2 = __syncthreads_and(s2) != 0;
