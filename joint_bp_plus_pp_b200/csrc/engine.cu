@@ -12,6 +12,7 @@
 #include "kernels_slots.cuh"
 #include "kernels_pp.cuh"
 #include "kernels_slot_pp.cuh"
+#include "kernels_single.cuh"
 #include "kernels_resident.cuh"
 #include "kernels_mixed.cuh"
 #include "mlp.cuh"
@@ -78,11 +79,13 @@ std::string dev_upload(std::vector<void *> &allocs, const std::vector<T> &h, T *
 using CheckFn = void (*)(DevCode, DevRun, DevMsgs);
 using VarF64Fn = void (*)(DevCode, DevRun, DevMsgs, double);
 using VarLlrFn = void (*)(DevCode, DevRun, DevMsgs, float);
+using SingleFn = void (*)(SingleRun);
 
 struct KernelSet {
     CheckFn check = nullptr;
     VarF64Fn var64 = nullptr;
     VarLlrFn varllr = nullptr;
+    SingleFn single64 = nullptr;   // one FP64 trial per cooperative launch
 };
 
 template <int DC, int DV>
@@ -91,6 +94,7 @@ KernelSet kernels_for(int precision, bool damp) {
     if (precision == JBP_PREC_FP64) {
         k.check = damp ? k_check_f64<DC, true> : k_check_f64<DC, false>;
         k.var64 = damp ? k_var_f64<DC, DV, true> : k_var_f64<DC, DV, false>;
+        k.single64 = k_single_f64<DC, DV>;
     } else if (precision == JBP_PREC_FP32) {
         k.check = k_check_llr<float, DC>;
         k.varllr = damp ? k_var_llr<float, DC, DV, true> : k_var_llr<float, DC, DV, false>;
@@ -149,6 +153,10 @@ void fill_stats(const DevCounters &hc, jbp_stats &stats) {
 
 Engine::~Engine() {
     if (abort_host_) cudaFreeHost(const_cast<int *>(abort_host_));
+    for (void *p : single_msg_) cudaFree(p);
+    cudaFree(single_est_);
+    cudaFree(single_ctl_);
+    cudaFree(single_cnt_);
     if (slot_graph_.exec) cudaGraphExecDestroy(slot_graph_.exec);
     for (cudaEvent_t ev : run_ev_)
         if (ev) cudaEventDestroy(ev);
@@ -462,6 +470,97 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     return "";
 }
 
+// The single-trial path takes FP64 decodes of up to kSingleMaxTrials given syndromes with plain
+// undamped BP and no profile, run budget, frozen sides or per-trial error rate -- the calls of
+// the drop-in's cuda_bp_decode -- unless the slot engine is asked for by name.
+constexpr long long kSingleMaxTrials = 3;
+
+bool Engine::single_applies(const RunRequest &rq) const {
+    const jbp_options &o = rq.opt;
+    return o.engine == JBP_ENGINE_AUTO && o.precision == JBP_PREC_FP64 && !o.enable_pp && o.damping <= 0.0 &&
+           !o.freeze_syn && !o.profile && o.watchdog_ms <= 0 && !(o.p_max > rq.p) && rq.source == kSrcSyndromes &&
+           rq.ntrials >= 1 && rq.ntrials <= kSingleMaxTrials && !rq.d_llr_out && !rq.collect;
+}
+
+std::string Engine::run_single(const RunRequest &rq, jbp_stats &stats) {
+    const jbp_options &o = rq.opt;
+    const SideGraph &gx = model_.side[0], &gz = model_.side[1];
+    KernelSet ks;
+    if (!select_kernels(gx.dc_max, gx.dv_max, JBP_PREC_FP64, false, ks) || !ks.single64)
+        return "no single-trial kernel for this code";
+    const int n = model_.n;
+    for (int s = 0; s < 2; ++s) {
+        const size_t bytes = sizeof(double2) * static_cast<size_t>(model_.side[s].edges);
+        if (!single_msg_[s]) JBP_CUDA_TRY(dev_malloc(&single_msg_[s], bytes), "cudaMalloc(single-trial messages)");
+        if (!single_msg_[2 + s])
+            JBP_CUDA_TRY(dev_malloc(&single_msg_[2 + s], bytes), "cudaMalloc(single-trial messages)");
+    }
+    if (!single_ctl_) JBP_CUDA_TRY(dev_malloc(&single_ctl_, sizeof(int) * 8), "cudaMalloc(single-trial control)");
+    if (!single_cnt_) JBP_CUDA_TRY(dev_malloc(&single_cnt_, sizeof(DevCounters)), "cudaMalloc(counters)");
+    if (!rq.d_est_out && !single_est_)
+        JBP_CUDA_TRY(dev_malloc(&single_est_, static_cast<size_t>(n)), "cudaMalloc(single-trial decisions)");
+    SingleRun sr{};
+    sr.code = dcode_;
+    sr.max_iter = o.max_iter;
+    sr.check_warmup = std::max(0, o.check_warmup);
+    sr.check_interval = std::max(1, o.check_interval);
+    if (o.use_prior) {
+        for (int i = 0; i < 4; ++i) sr.prior[i] = o.prior[i];
+    } else {
+        // normalize(1-p, p/3, p/3, p/3) as the slot engine's refill and jointbp_ets.cpp:5484-5485
+        double p0 = 1.0 - rq.p, p1 = rq.p / 3.0, p2 = p1, p3 = p1;
+        const double s = ((p0 + p1) + p2) + p3;
+        if (s <= 0.0) { p0 = p1 = p2 = p3 = 0.25; }
+        else { p0 = p0 / s; p1 = p1 / s; p2 = p2 / s; p3 = p3 / s; }
+        sr.prior[0] = p0; sr.prior[1] = p1; sr.prior[2] = p2; sr.prior[3] = p3;
+    }
+    for (int s = 0; s < 2; ++s) {
+        sr.c2v[s] = static_cast<double2 *>(single_msg_[s]);
+        sr.v2c[s] = static_cast<double2 *>(single_msg_[2 + s]);
+    }
+    sr.bar = reinterpret_cast<unsigned *>(single_ctl_);
+    sr.bad = single_ctl_ + 2;
+    sr.err = single_ctl_ + 4;
+    sr.cnt = single_cnt_;
+    sr.hist = rq.d_hist;
+    sr.res_out = rq.d_res_out;
+    cudaStream_t st = rq.stream;
+    if (!run_ev_[0]) {
+        for (int i = 0; i < 2; ++i) JBP_CUDA_TRY(cudaEventCreate(&run_ev_[i]), "cudaEventCreate");
+        for (int i = 2; i < 4; ++i)
+            JBP_CUDA_TRY(cudaEventCreateWithFlags(&run_ev_[i], cudaEventDisableTiming), "cudaEventCreate");
+    }
+    cudaError_t ce = cudaEventRecord(run_ev_[0], st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(single_ctl_, 0, sizeof(int) * 8, st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(single_cnt_, 0, sizeof(DevCounters), st);
+    const int mx = gx.m, mz = gz.m;
+    for (long long t = 0; t < rq.ntrials && ce == cudaSuccess; ++t) {
+        sr.sx = rq.d_sx + t * mx;
+        sr.sz = rq.d_sz + t * mz;
+        sr.est = rq.d_est_out ? rq.d_est_out + t * n : single_est_;
+        sr.local = t;
+        void *args[] = {&sr};
+        ce = cudaLaunchCooperativeKernel(reinterpret_cast<void *>(ks.single64), kSingleBlocks, kSingleThreads, args, 0,
+                                         st);
+    }
+    if (ce == cudaSuccess) ce = cudaEventRecord(run_ev_[1], st);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(run_ev_[1]);
+    int ctl[8] = {};
+    DevCounters hc{};
+    if (ce == cudaSuccess) ce = cudaMemcpy(ctl, single_ctl_, sizeof(ctl), cudaMemcpyDeviceToHost);
+    if (ce == cudaSuccess) ce = cudaMemcpy(&hc, single_cnt_, sizeof(hc), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return cuda_err(ce, "single-trial run");
+    if (ctl[4]) return "single-trial run: a grid barrier waited longer than its limit (internal error)";
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, run_ev_[0], run_ev_[1]);
+    fill_stats(hc, stats);
+    stats.device_ms = ms;
+    stats.kernel_launches = rq.ntrials;
+    stats.slots = 1;
+    if (hc.done != static_cast<unsigned long long>(rq.ntrials)) return "single-trial run finished an unexpected number of trials";
+    return "";
+}
+
 void Engine::free_buffers() {
     for (void *&p : buf_.msg) { cudaFree(p); p = nullptr; }
     cudaFree(buf_.trial); cudaFree(buf_.iter); cudaFree(buf_.flags); cudaFree(buf_.frz); cudaFree(buf_.unsat);
@@ -664,6 +763,7 @@ std::string Engine::run_dispatch(const RunRequest &rq, jbp_stats &stats) {
         return "no GPU kernel built for check degree " + std::to_string(gx.dc_max) + " / variable degree " +
                std::to_string(gx.dv_max);
     JBP_CUDA_TRY(cudaSetDevice(device_), "cudaSetDevice");
+    if (ks.single64 && single_applies(rq)) return run_single(rq, stats);
     const int S = choose_slots(o, rq.ntrials);
     const int H = std::max(0, o.flip_hist);
     const int R = pp ? std::max(H + 1, 3) : 1;

@@ -115,6 +115,9 @@ private:
     bool resident_applies(const jbp_options &o, std::string *why) const;
     std::string run_resident(const RunRequest &rq, jbp_stats &stats);
     std::string run_dispatch(const RunRequest &rq, jbp_stats &stats);
+    // one or a few FP64 trials, each in one cooperative launch (kernels_single.cuh)
+    bool single_applies(const RunRequest &rq) const;
+    std::string run_single(const RunRequest &rq, jbp_stats &stats);
     static std::string run_mixed_impl(const MixedRequest &rq, std::vector<jbp_stats> &stats);
     std::string build_res_code();
 
@@ -146,6 +149,12 @@ private:
     int device_ = 0;
     int sm_count_ = 0;
     volatile int *abort_host_ = nullptr;   // jbp_request_abort's flag, mapped pinned host memory
+    // the single-trial FP64 path: messages [c2v x, c2v z, v2c x, v2c z], decisions when the caller
+    // gives no buffer, barrier / test counters / error flag, counters
+    void *single_msg_[4] = {};
+    uint8_t *single_est_ = nullptr;
+    int *single_ctl_ = nullptr;
+    DevCounters *single_cnt_ = nullptr;
     const volatile int *abort_dev_ = nullptr;   // ... the device's address of it (the kernels poll it)
     const uint16_t *mix_slot_[2] = {nullptr, nullptr};   // [dv][n] message slot of each variable's edges
     const uint16_t *mix_chk_[2] = {nullptr, nullptr};    // [dc][m] variable of each check's edges

@@ -156,15 +156,21 @@ __device__ __forceinline__ int frozen_bit(const DevRun &run, int n, int side, in
 
 // ------------------------------------------------------------------ FP64, bit-exact
 
-// The outputs of one check row (jointbp_ets.cpp:2373-2450): for each edge i the even / odd
-// parity products of the other edges (prefix pe, po times suffix se, so), ordered by the
-// syndrome bit s and normalized by their side's sum.  FAST: the two quotients by one
-// branch-free reciprocal and Markstein's correction (the IEEE quotients inside the fast
-// domain), the row in one basic block; ok is cleared when an operand left the domain and the
-// caller redoes the row with FAST = false (the division itself), which rewrites every output.
-template <int DC, bool FAST>
-__device__ __forceinline__ void check_f64_outputs(const double *se, const double *so, const double *q0,
-                                                  const double *q1, int s, int side, double2 *c2v, bool &ok) {
+// The outputs of one check row (jointbp_ets.cpp:2373-2450) from its edges' (q0, q1): suffix
+// parities (se, so), then for each edge i the even / odd parity of the other edges (prefix pe,
+// po times suffix), ordered by the syndrome bit s and normalized by its side's sum;
+// out[i * stride] gets edge i's (a, b).
+template <int DC>
+__device__ __forceinline__ void check_f64_row(const double *q0, const double *q1, int s, int side, double2 *out,
+                                              size_t stride) {
+    double se[DC + 1], so[DC + 1];
+    se[DC] = 1.0;
+    so[DC] = 0.0;
+#pragma unroll
+    for (int i = DC - 1; i >= 0; --i) {
+        se[i] = dadd(dmul(se[i + 1], q0[i]), dmul(so[i + 1], q1[i]));
+        so[i] = dadd(dmul(se[i + 1], q1[i]), dmul(so[i + 1], q0[i]));
+    }
     double pe = 1.0, po = 0.0;
 #pragma unroll
     for (int i = 0; i < DC; ++i) {
@@ -173,21 +179,15 @@ __device__ __forceinline__ void check_f64_outputs(const double *se, const double
         const double v0 = s == 0 ? p_even : p_odd;
         const double v1 = s == 0 ? p_odd : p_even;
         const double sum = side == 0 ? dadd(dadd(dadd(v0, v1), v0), v1) : dadd(dadd(dadd(v0, v0), v1), v1);
-        double2 out;
-        if (FAST) {
-            ok = ok && sum >= 0x1p-900 && sum <= 0x1p900 && fast_div_ok(v0) && fast_div_ok(v1);
-            const double y = recip_rn_fast(sum);
-            const double a = __dmul_rn(v0, y), b = __dmul_rn(v1, y);
-            out.x = __fma_rn(__fma_rn(-sum, a, v0), y, a);
-            out.y = __fma_rn(__fma_rn(-sum, b, v1), y, b);
-        } else if (sum <= 0.0) {
-            out.x = 0.25;
-            out.y = 0.25;
+        double2 o;
+        if (sum <= 0.0) {
+            o.x = 0.25;
+            o.y = 0.25;
         } else {
-            out.x = ddiv(v0, sum);
-            out.y = ddiv(v1, sum);
+            o.x = ddiv(v0, sum);
+            o.y = ddiv(v1, sum);
         }
-        c2v[i * kGroup] = out;
+        out[i * stride] = o;
         const double ne = dadd(dmul(pe, q0[i]), dmul(po, q1[i]));
         const double no = dadd(dmul(pe, q1[i]), dmul(po, q0[i]));
         pe = ne;
@@ -245,17 +245,8 @@ __global__ void __launch_bounds__(256, 3) k_check_f64(DevCode code, DevRun run, 
             if (side == 0) { q0[i] = dadd(m0, m2); q1[i] = dadd(m1, m3); }
             else { q0[i] = dadd(m0, m1); q1[i] = dadd(m2, m3); }
         }
-        double se[DC + 1], so[DC + 1];
-        se[DC] = 1.0;
-        so[DC] = 0.0;
-#pragma unroll
-        for (int i = DC - 1; i >= 0; --i) {
-            se[i] = dadd(dmul(se[i + 1], q0[i]), dmul(so[i + 1], q1[i]));
-            so[i] = dadd(dmul(se[i + 1], q1[i]), dmul(so[i + 1], q0[i]));
-        }
         const int s = (run.synm[static_cast<size_t>(row) * G + group] >> lane) & 1;
-        bool ok = true;
-        check_f64_outputs<DC, false>(se, so, q0, q1, s, side, c2v, ok);
+        check_f64_row<DC>(q0, q1, s, side, c2v, kGroup);
     }
 }
 

@@ -283,3 +283,32 @@ def test_sfu_measurement_is_plausible():
     ceiling = 16 * prop.multi_processor_count * 2.1   # G/s at a clock up to 2.1 GHz
     for k in ("ex2", "lg2", "rcp"):
         assert 0.25 * ceiling < r[k] < 2.0 * ceiling, (k, r[k])
+
+
+@pytest.mark.parametrize("warmup,interval", [(0, 1), (3, 2), (0, 4)])
+def test_single_trial_path_equals_slot_engine(decoder, oracle, warmup, interval):
+    """FP64 decodes of one to three syndromes (the drop-in's cuda_bp_decode calls) run each
+    trial's whole BP loop in one cooperative launch (kernels_single.cuh); decisions, iteration
+    counts and outcomes equal the slot engine's on the same 64 syndromes, for the test schedule
+    given (warmup, interval) and for a caller's explicit prior."""
+    from dataclasses import replace
+    from joint_bp_plus_pp_b200 import Options
+    p = 0.045
+    err = decoder.sample_errors(77, 1, 64, p)
+    sx = np.stack([oracle.syndrome(e)[0] for e in err])
+    sz = np.stack([oracle.syndrome(e)[1] for e in err])
+    base = Options(precision="fp64", max_iter=200, enable_pp=False, check_warmup=warmup, check_interval=interval)
+    _, r_ref, e_ref = decoder.decode_syndromes(sx, sz, p, replace(base, engine="slots"))
+    for k in (1, 2, 3):
+        for i in range(0, 64, k):
+            st, r, e = decoder.decode_syndromes(sx[i:i + k], sz[i:i + k], p, base)
+            assert st["kernel_launches"] == len(r) and st["slots"] == 1   # the single-trial path ran
+            assert (e == e_ref[i:i + k]).all(), (k, i)
+            for f in ("iterations", "syndrome_ok", "success"):
+                assert (r[f] == r_ref[i:i + k][f]).all(), (f, k, i)
+    q = (1 - p, p / 3, p / 3, p / 3)
+    s = ((q[0] + q[1]) + q[2]) + q[3]
+    pri = replace(base, prior=tuple(x / s for x in q))
+    _, r1, e1 = decoder.decode_syndromes(sx[:2], sz[:2], 0.2, pri)
+    _, r2, e2 = decoder.decode_syndromes(sx[:2], sz[:2], 0.2, replace(pri, engine="slots"))
+    assert (e1 == e2).all() and (r1["iterations"] == r2["iterations"]).all()
