@@ -195,6 +195,43 @@ __device__ __forceinline__ void check_f64_row(const double *q0, const double *q1
     }
 }
 
+// check_f64_row with the two quotients of each output by one branch-free reciprocal and
+// Markstein's correction (recip_rn_fast; the IEEE quotients inside the fast domain), the row in
+// one basic block.  Returns false, after writing outputs that must not be used, when an operand
+// is outside the domain (a sum outside [2^-900, 2^900], a dividend below 2^-900 and not 0): the
+// caller then rewrites the row with check_f64_row.
+template <int DC>
+__device__ __forceinline__ bool check_f64_row_fast(const double *q0, const double *q1, int s, int side,
+                                                   double2 *out, size_t stride) {
+    double se[DC + 1], so[DC + 1];
+    se[DC] = 1.0;
+    so[DC] = 0.0;
+#pragma unroll
+    for (int i = DC - 1; i >= 0; --i) {
+        se[i] = dadd(dmul(se[i + 1], q0[i]), dmul(so[i + 1], q1[i]));
+        so[i] = dadd(dmul(se[i + 1], q1[i]), dmul(so[i + 1], q0[i]));
+    }
+    bool ok = true;
+    double pe = 1.0, po = 0.0;
+#pragma unroll
+    for (int i = 0; i < DC; ++i) {
+        const double p_even = dadd(dmul(pe, se[i + 1]), dmul(po, so[i + 1]));
+        const double p_odd = dadd(dmul(pe, so[i + 1]), dmul(po, se[i + 1]));
+        const double v0 = s == 0 ? p_even : p_odd;
+        const double v1 = s == 0 ? p_odd : p_even;
+        const double sum = side == 0 ? dadd(dadd(dadd(v0, v1), v0), v1) : dadd(dadd(dadd(v0, v0), v1), v1);
+        ok = ok && sum >= 0x1p-900 && sum <= 0x1p900 && fast_div_ok(v0) && fast_div_ok(v1);
+        const double y = recip_rn_fast(sum);
+        const double a = __dmul_rn(v0, y), b = __dmul_rn(v1, y);
+        out[i * stride] = make_double2(__fma_rn(__fma_rn(-sum, a, v0), y, a), __fma_rn(__fma_rn(-sum, b, v1), y, b));
+        const double ne = dadd(dmul(pe, q0[i]), dmul(po, q1[i]));
+        const double no = dadd(dmul(pe, q1[i]), dmul(po, q0[i]));
+        pe = ne;
+        po = no;
+    }
+    return ok;
+}
+
 template <int DC, bool DAMP>
 __global__ void __launch_bounds__(256, 3) k_check_f64(DevCode code, DevRun run, DevMsgs msg) {
     const int lane = threadIdx.x & 31;

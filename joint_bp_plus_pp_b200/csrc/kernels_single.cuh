@@ -94,7 +94,38 @@ __global__ void __launch_bounds__(kSingleThreads) k_single_f64(const __grid_cons
     }
     int iters = run.max_iter, tests = 0;
     bool ok = false;
+    // the check schedule of the slot engine's check_due (1-based iteration k1)
+    auto due = [&](int k1) {
+        return k1 >= run.max_iter || (k1 > run.check_warmup && (k1 - run.check_warmup) % run.check_interval == 0);
+    };
+    // whether the decisions in run.est fail check ch of a side (jointbp_ets.cpp:2521-2525)
+    auto fails = [&](int side, int ch) -> int {
+        const int dc = code.s[side].dc;
+        unsigned par = 0;
+        for (int i = 0; i < dc; ++i) {
+            const int v = __ldg(code.s[side].chk_var + static_cast<size_t>(ch) * dc + i);
+            if (v >= 0) par ^= (run.est[v] >> side) & 1u;
+        }
+        return par != static_cast<unsigned>((side ? run.sz : run.sx)[ch] & 1);
+    };
+    // adds this block's failing checks to the test's count in bad[tests & 1] and clears the
+    // other entry (last read before the previous barrier) for the next test
+    auto post_count = [&](int bad) {
+        bad = __reduce_add_sync(0xffffffffu, bad);
+        if ((threadIdx.x & 31) == 0 && bad) atomicAdd(&bad_sh, bad);
+        __syncthreads();
+        if (threadIdx.x == 0 && bad_sh) atomicAdd(&run.bad[tests & 1], bad_sh);
+        if (tid == 0) run.bad[(tests + 1) & 1] = 0;
+    };
     for (int it = 0; it < run.max_iter; ++it) {
+        // the test of iteration it's decisions (1-based) rides in this check phase, which reads
+        // the same decisions; when they satisfy both syndromes, the phase's messages are unused
+        const bool test_now = it >= 1 && due(it);
+        if (test_now) {
+            if (threadIdx.x == 0) bad_sh = 0;
+            __syncthreads();
+        }
+        int bad = 0;
         // check phase: new c2v of every check row (jointbp_ets.cpp:2373-2449)
         for (int row = tid; row < M; row += nthreads) {
             const int side = row >= mx, ch = side ? row - mx : row;
@@ -113,9 +144,21 @@ __global__ void __launch_bounds__(kSingleThreads) k_single_f64(const __grid_cons
                 }
             }
             const int s = (side ? run.sz : run.sx)[ch] & 1;
-            check_f64_row<DC>(q0, q1, s, side, run.c2v[side] + static_cast<size_t>(ch) * DC, 1);
+            double2 *out = run.c2v[side] + static_cast<size_t>(ch) * DC;
+            if (!check_f64_row_fast<DC>(q0, q1, s, side, out, 1)) check_f64_row<DC>(q0, q1, s, side, out, 1);
+            if (test_now) bad += fails(side, ch);
         }
+        if (test_now) post_count(bad);
         if (!grid_barrier(run.bar, run.err)) return;
+        if (test_now) {
+            const int total_bad = *reinterpret_cast<volatile int *>(&run.bad[tests & 1]);
+            ++tests;
+            if (total_bad == 0) {
+                ok = true;
+                iters = it;
+                break;
+            }
+        }
         // variable phase: decisions and new v2c (jointbp_ets.cpp:2451-2519)
         for (int v = tid; v < n; v += nthreads) {
             size_t ox[DV], oz[DV];
@@ -138,37 +181,20 @@ __global__ void __launch_bounds__(kSingleThreads) k_single_f64(const __grid_cons
             run.est[v] = static_cast<uint8_t>(best);
         }
         if (!grid_barrier(run.bar, run.err)) return;
-        // syndrome test of the decisions when due (jointbp_ets.cpp:2521-2525, the check schedule
-        // of the slot engine's check_due)
-        const int k1 = it + 1;
-        if (k1 >= run.max_iter || (k1 > run.check_warmup && (k1 - run.check_warmup) % run.check_interval == 0)) {
+        if (it + 1 == run.max_iter) {
+            // the last iteration's decisions have no check phase after them: a test of their own
             if (threadIdx.x == 0) bad_sh = 0;
             __syncthreads();
-            int bad = 0;
+            int lbad = 0;
             for (int row = tid; row < M; row += nthreads) {
                 const int side = row >= mx, ch = side ? row - mx : row;
-                const int dc = code.s[side].dc;
-                unsigned par = 0;
-                for (int i = 0; i < dc; ++i) {
-                    const int v = __ldg(code.s[side].chk_var + static_cast<size_t>(ch) * dc + i);
-                    if (v >= 0) par ^= (run.est[v] >> side) & 1u;
-                }
-                bad += par != static_cast<unsigned>((side ? run.sz : run.sx)[ch] & 1);
+                lbad += fails(side, ch);
             }
-            bad = __reduce_add_sync(0xffffffffu, bad);
-            if ((threadIdx.x & 31) == 0 && bad) atomicAdd(&bad_sh, bad);
-            __syncthreads();
-            // the count of this test in bad[tests & 1]; the other entry, last read before the
-            // previous barrier, is cleared for the next test
-            if (threadIdx.x == 0 && bad_sh) atomicAdd(&run.bad[tests & 1], bad_sh);
-            if (tid == 0) run.bad[(tests + 1) & 1] = 0;
+            post_count(lbad);
             if (!grid_barrier(run.bar, run.err)) return;
-            const int total_bad = *reinterpret_cast<volatile int *>(&run.bad[tests & 1]);
-            ++tests;
-            if (total_bad == 0) {
+            if (*reinterpret_cast<volatile int *>(&run.bad[tests & 1]) == 0) {
                 ok = true;
-                iters = k1;
-                break;
+                iters = run.max_iter;
             }
         }
     }
