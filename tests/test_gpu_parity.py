@@ -312,3 +312,24 @@ def test_single_trial_path_equals_slot_engine(decoder, oracle, warmup, interval)
     _, r1, e1 = decoder.decode_syndromes(sx[:2], sz[:2], 0.2, pri)
     _, r2, e2 = decoder.decode_syndromes(sx[:2], sz[:2], 0.2, replace(pri, engine="slots"))
     assert (e1 == e2).all() and (r1["iterations"] == r2["iterations"]).all()
+
+
+@pytest.mark.parametrize("max_iter,warmup,interval", [(1, 0, 1), (2, 0, 4), (5, 1, 2), (5, 0, 3)])
+def test_single_trial_path_short_runs(decoder, oracle, max_iter, warmup, interval):
+    """The single-trial path at a few iterations, where the last iteration's test (no check
+    phase after it) decides most trials: decisions and records equal the slot engine's."""
+    from dataclasses import replace
+    from joint_bp_plus_pp_b200 import Options
+    p = 0.04
+    err = decoder.sample_errors(91, 1, 24, p)
+    sx = np.stack([oracle.syndrome(e)[0] for e in err])
+    sz = np.stack([oracle.syndrome(e)[1] for e in err])
+    base = Options(precision="fp64", max_iter=max_iter, enable_pp=False, check_warmup=warmup,
+                   check_interval=interval)
+    _, r_ref, e_ref = decoder.decode_syndromes(sx, sz, p, replace(base, engine="slots"))
+    for i in range(24):
+        st, r, e = decoder.decode_syndromes(sx[i:i + 1], sz[i:i + 1], p, base)
+        assert st["slots"] == 1
+        assert (e[0] == e_ref[i]).all(), i
+        for f in ("iterations", "syndrome_ok", "success"):
+            assert r[f][0] == r_ref[f][i], (f, i)
