@@ -183,6 +183,11 @@ std::string Engine::init(CodeModel model, int device) {
     JBP_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin_, cudaDevAttrMaxSharedMemoryPerBlockOptin, device),
                  "device attributes");
     {
+        int coop = 0;
+        JBP_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device), "device attributes");
+        coop_launch_ = coop != 0;
+    }
+    {
         int *flag = nullptr, *dflag = nullptr;
         JBP_CUDA_TRY(host_malloc(&flag, sizeof(int)), "cudaHostAlloc(abort flag)");
         abort_host_ = flag;
@@ -477,7 +482,7 @@ constexpr long long kSingleMaxTrials = 3;
 
 bool Engine::single_applies(const RunRequest &rq) const {
     const jbp_options &o = rq.opt;
-    return o.engine == JBP_ENGINE_AUTO && o.precision == JBP_PREC_FP64 && !o.enable_pp && o.damping <= 0.0 &&
+    return coop_launch_ && o.engine == JBP_ENGINE_AUTO && o.precision == JBP_PREC_FP64 && !o.enable_pp && o.damping <= 0.0 &&
            !o.freeze_syn && !o.profile && o.watchdog_ms <= 0 && !(o.p_max > rq.p) && rq.source == kSrcSyndromes &&
            rq.ntrials >= 1 && rq.ntrials <= kSingleMaxTrials && !rq.d_llr_out && !rq.collect;
 }

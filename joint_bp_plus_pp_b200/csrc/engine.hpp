@@ -151,6 +151,7 @@ private:
     volatile int *abort_host_ = nullptr;   // jbp_request_abort's flag, mapped pinned host memory
     // the single-trial FP64 path: messages [c2v x, c2v z, v2c x, v2c z], decisions when the caller
     // gives no buffer, barrier / test counters / error flag, counters
+    bool coop_launch_ = false;   // the device runs cooperative launches (the single-trial path)
     void *single_msg_[4] = {};
     uint8_t *single_est_ = nullptr;
     int *single_ctl_ = nullptr;
