@@ -298,6 +298,9 @@ static void add_stats(jbp_stats &total, const jbp_stats &st) {
     total.syndrome_tests += st.syndrome_tests;
 }
 
+// Calls of at most this many trials from unmapped host syndromes stage through pinned memory.
+constexpr long long kStagedTrials = 3;
+
 static int decode_host(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *err, const uint8_t *sx,
                        const uint8_t *sz, double p, uint8_t *est_out, jbp_trial_result *res, jbp_stats *stats,
                        float *llr_out = nullptr) {
@@ -335,6 +338,7 @@ static int decode_host(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, 
         rq.first_trial = 0;
         rq.ntrials = cnt;
         cudaError_t ce;
+        bool host_copied = false;
         if (err && m_err) {
             rq.source = jbp::kSrcErrors;
             rq.d_err = m_err + base * n;
@@ -348,6 +352,33 @@ static int decode_host(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, 
             rq.source = jbp::kSrcSyndromes;
             rq.d_sx = m_sx + base * mx;
             rq.d_sz = m_sz + base * mz;
+        } else if (cnt <= kStagedTrials && !llr_out) {
+            // a call of a few trials (the drop-in decodes one per call): inputs through pinned
+            // staging on the context's stream, and the results, when the engine's single-trial
+            // path runs, copied back behind its launches, so that the call waits once
+            if (!sx || !sz) return fail(JBP_ERR_ARG, "null syndrome");
+            const size_t in = static_cast<size_t>(cnt * (mx + mz)), in_al = (in + 15) / 16 * 16;
+            const size_t res_b = sizeof(jbp_trial_result) * cnt, res_al = (res_b + 15) / 16 * 16;
+            const size_t need = in_al + res_al + (est_out ? static_cast<size_t>(cnt * n) : 0);
+            if (ctx->h_stage_bytes < need) {
+                if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+                ctx->h_stage = nullptr;
+                ctx->h_stage_bytes = 0;
+                ce = jbp::host_malloc(&ctx->h_stage, need);
+                if (ce != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(ce, "cudaHostAlloc(staging)"));
+                ctx->h_stage_bytes = need;
+            }
+            if (int rc = grow(&ctx->d_in, &ctx->in_bytes, in)) return rc;
+            std::memcpy(ctx->h_stage, sx + base * mx, static_cast<size_t>(cnt * mx));
+            std::memcpy(ctx->h_stage + cnt * mx, sz + base * mz, static_cast<size_t>(cnt * mz));
+            ce = cudaMemcpyAsync(ctx->d_in, ctx->h_stage, in, cudaMemcpyHostToDevice, ctx->stream);
+            if (ce != cudaSuccess) return fail(JBP_ERR_CUDA, jbp::cuda_err(ce, "copy syndromes"));
+            rq.source = jbp::kSrcSyndromes;
+            rq.d_sx = ctx->d_in;
+            rq.d_sz = ctx->d_in + cnt * mx;
+            rq.h_res_out = reinterpret_cast<jbp_trial_result *>(ctx->h_stage + in_al);
+            rq.h_est_out = est_out ? ctx->h_stage + in_al + res_al : nullptr;
+            rq.host_copied = &host_copied;
         } else {
             if (!sx || !sz) return fail(JBP_ERR_ARG, "null syndrome");
             if (int rc = grow(&ctx->d_in, &ctx->in_bytes, static_cast<size_t>(cnt * mx))) return rc;
@@ -373,12 +404,21 @@ static int decode_host(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, 
         jbp_stats st;
         std::string e = ctx->engine.run(rq, st);
         if (!e.empty()) {
+            // a run that stopped before its launches leaves the staged input copy to finish
+            // before the staging is reused
+            if (rq.host_copied) cudaStreamSynchronize(ctx->stream);
             const int rc = engine_fail(e);
             if (partial_stats(rc) && stats) {
                 add_stats(total, st);
                 *stats = total;   // the trials finished within the budget
             }
             return rc;
+        }
+        if (host_copied) {
+            std::memcpy(res + base, rq.h_res_out, sizeof(jbp_trial_result) * cnt);
+            if (est_out) std::memcpy(est_out + base * n, rq.h_est_out, static_cast<size_t>(cnt * n));
+            add_stats(total, st);
+            continue;
         }
         ce = cudaMemcpy(res + base, ctx->d_res, sizeof(jbp_trial_result) * cnt, cudaMemcpyDeviceToHost);
         if (ce == cudaSuccess && est_out)

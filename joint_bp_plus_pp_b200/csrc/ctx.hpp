@@ -23,6 +23,9 @@ struct jbp_ctx {
     size_t hist_count = 0;
     float *d_llr = nullptr;
     size_t llr_count = 0;
+    // pinned host staging of calls of a few trials (inputs, then results)
+    unsigned char *h_stage = nullptr;
+    size_t h_stage_bytes = 0;
     ~jbp_ctx() {
         if (stream) cudaStreamDestroy(stream);
         cudaFree(d_in);
@@ -31,6 +34,7 @@ struct jbp_ctx {
         cudaFree(d_res);
         cudaFree(d_hist);
         cudaFree(d_llr);
+        if (h_stage) cudaFreeHost(h_stage);
     }
 };
 

@@ -155,8 +155,8 @@ Engine::~Engine() {
     if (abort_host_) cudaFreeHost(const_cast<int *>(abort_host_));
     for (void *p : single_msg_) cudaFree(p);
     cudaFree(single_est_);
-    cudaFree(single_ctl_);
-    cudaFree(single_cnt_);
+    cudaFree(single_ctl_);   // single_cnt_ lies in the same allocation
+    if (single_host_) cudaFreeHost(single_host_);
     if (slot_graph_.exec) cudaGraphExecDestroy(slot_graph_.exec);
     for (cudaEvent_t ev : run_ev_)
         if (ev) cudaEventDestroy(ev);
@@ -500,8 +500,13 @@ std::string Engine::run_single(const RunRequest &rq, jbp_stats &stats) {
         if (!single_msg_[2 + s])
             JBP_CUDA_TRY(dev_malloc(&single_msg_[2 + s], bytes), "cudaMalloc(single-trial messages)");
     }
-    if (!single_ctl_) JBP_CUDA_TRY(dev_malloc(&single_ctl_, sizeof(int) * 8), "cudaMalloc(single-trial control)");
-    if (!single_cnt_) JBP_CUDA_TRY(dev_malloc(&single_cnt_, sizeof(DevCounters)), "cudaMalloc(counters)");
+    constexpr size_t state_bytes = kSingleCntOffset + sizeof(DevCounters);
+    static_assert(sizeof(int) * 8 <= kSingleCntOffset, "control words before the counters");
+    if (!single_ctl_) {
+        JBP_CUDA_TRY(dev_malloc(&single_ctl_, state_bytes), "cudaMalloc(single-trial control)");
+        single_cnt_ = reinterpret_cast<DevCounters *>(reinterpret_cast<unsigned char *>(single_ctl_) + kSingleCntOffset);
+    }
+    if (!single_host_) JBP_CUDA_TRY(host_malloc(&single_host_, state_bytes), "cudaHostAlloc(single-trial control)");
     if (!rq.d_est_out && !single_est_)
         JBP_CUDA_TRY(dev_malloc(&single_est_, static_cast<size_t>(n)), "cudaMalloc(single-trial decisions)");
     SingleRun sr{};
@@ -536,8 +541,7 @@ std::string Engine::run_single(const RunRequest &rq, jbp_stats &stats) {
             JBP_CUDA_TRY(cudaEventCreateWithFlags(&run_ev_[i], cudaEventDisableTiming), "cudaEventCreate");
     }
     cudaError_t ce = cudaEventRecord(run_ev_[0], st);
-    if (ce == cudaSuccess) ce = cudaMemsetAsync(single_ctl_, 0, sizeof(int) * 8, st);
-    if (ce == cudaSuccess) ce = cudaMemsetAsync(single_cnt_, 0, sizeof(DevCounters), st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(single_ctl_, 0, state_bytes, st);
     const int mx = gx.m, mz = gz.m;
     for (long long t = 0; t < rq.ntrials && ce == cudaSuccess; ++t) {
         sr.sx = rq.d_sx + t * mx;
@@ -549,12 +553,22 @@ std::string Engine::run_single(const RunRequest &rq, jbp_stats &stats) {
                                          st);
     }
     if (ce == cudaSuccess) ce = cudaEventRecord(run_ev_[1], st);
-    if (ce == cudaSuccess) ce = cudaEventSynchronize(run_ev_[1]);
-    int ctl[8] = {};
-    DevCounters hc{};
-    if (ce == cudaSuccess) ce = cudaMemcpy(ctl, single_ctl_, sizeof(ctl), cudaMemcpyDeviceToHost);
-    if (ce == cudaSuccess) ce = cudaMemcpy(&hc, single_cnt_, sizeof(hc), cudaMemcpyDeviceToHost);
+    // control words, counters and the caller's host copies queued behind the launches: one wait
+    // for the whole call
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(single_host_, single_ctl_, state_bytes, cudaMemcpyDeviceToHost, st);
+    const bool copy_res = rq.h_res_out && rq.d_res_out, copy_est = rq.h_est_out && rq.d_est_out;
+    if (ce == cudaSuccess && copy_res)
+        ce = cudaMemcpyAsync(rq.h_res_out, rq.d_res_out, sizeof(jbp_trial_result) * rq.ntrials, cudaMemcpyDeviceToHost,
+                             st);
+    if (ce == cudaSuccess && copy_est)
+        ce = cudaMemcpyAsync(rq.h_est_out, rq.d_est_out, static_cast<size_t>(rq.ntrials) * n, cudaMemcpyDeviceToHost,
+                             st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
     if (ce != cudaSuccess) return cuda_err(ce, "single-trial run");
+    int ctl[8];
+    DevCounters hc;
+    std::memcpy(ctl, single_host_, sizeof(ctl));
+    std::memcpy(&hc, single_host_ + kSingleCntOffset, sizeof(hc));
     if (ctl[4]) return "single-trial run: a grid barrier waited longer than its limit (internal error)";
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, run_ev_[0], run_ev_[1]);
@@ -563,6 +577,7 @@ std::string Engine::run_single(const RunRequest &rq, jbp_stats &stats) {
     stats.kernel_launches = rq.ntrials;
     stats.slots = 1;
     if (hc.done != static_cast<unsigned long long>(rq.ntrials)) return "single-trial run finished an unexpected number of trials";
+    if (rq.host_copied) *rq.host_copied = (copy_res || !rq.h_res_out) && (copy_est || !rq.h_est_out);
     return "";
 }
 

@@ -28,6 +28,12 @@ struct RunRequest {
     jbp_trial_result *d_res_out = nullptr;
     unsigned long long *d_hist = nullptr;
     cudaStream_t stream = nullptr;
+    // Optional pinned host buffers for copies of d_res_out / d_est_out.  The single-trial path
+    // queues those copies behind its launches and waits once for all of them, then sets
+    // *host_copied; other paths leave the buffers and the flag alone.
+    jbp_trial_result *h_res_out = nullptr;
+    uint8_t *h_est_out = nullptr;
+    bool *host_copied = nullptr;
     // stall-state collection for training the learned proposal (device buffers)
     bool collect = false;
     float *d_col_x = nullptr, *d_col_y = nullptr;
@@ -117,6 +123,7 @@ private:
     std::string run_dispatch(const RunRequest &rq, jbp_stats &stats);
     // one or a few FP64 trials, each in one cooperative launch (kernels_single.cuh)
     bool single_applies(const RunRequest &rq) const;
+    static constexpr size_t kSingleCntOffset = 64;   // single_cnt_ within the control allocation
     std::string run_single(const RunRequest &rq, jbp_stats &stats);
     static std::string run_mixed_impl(const MixedRequest &rq, std::vector<jbp_stats> &stats);
     std::string build_res_code();
@@ -154,8 +161,11 @@ private:
     bool coop_launch_ = false;   // the device runs cooperative launches (the single-trial path)
     void *single_msg_[4] = {};
     uint8_t *single_est_ = nullptr;
+    // the single-trial path's barrier, test counts and error flag (single_ctl_, 8 ints) and its
+    // counters (single_cnt_) in one allocation, copied back in one transfer to single_host_
     int *single_ctl_ = nullptr;
     DevCounters *single_cnt_ = nullptr;
+    unsigned char *single_host_ = nullptr;   // pinned
     const volatile int *abort_dev_ = nullptr;   // ... the device's address of it (the kernels poll it)
     const uint16_t *mix_slot_[2] = {nullptr, nullptr};   // [dv][n] message slot of each variable's edges
     const uint16_t *mix_chk_[2] = {nullptr, nullptr};    // [dc][m] variable of each check's edges

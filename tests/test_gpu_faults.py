@@ -11,6 +11,7 @@ usable and decodes exactly as before.
 import threading
 import time
 
+import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -23,14 +24,36 @@ def _cfgs():
         "resident_fp32_learned": Options(precision="fp32", engine="resident", max_iter=300, enable_pp=True,
                                          learned_from=6),
         "table_fp32": Options(precision="fp32", engine="table", max_iter=300, enable_pp=False),
+        # calls of two syndromes each: pinned staging and the single-trial FP64 path
+        "single_fp64_syndromes": Options(precision="fp64", max_iter=300, enable_pp=False),
     }
 
 
+def _syndromes(dec, err):
+    out = []
+    for side in (0, 1):
+        off, var = dec.checks(side)
+        bits = (err >> side) & 1
+        dc = int(off[1] - off[0])
+        out.append((bits[:, var].reshape(err.shape[0], -1, dc).sum(axis=2) % 2).astype(np.uint8))
+    return out
+
+
 def _run(dec, opts):
+    if opts.engine == "auto" and opts.precision == "fp64" and not opts.enable_pp:
+        err = dec.sample_errors(106, 3, 8, 0.045)
+        sx, sz = _syndromes(dec, err)
+        recs, ests = [], []
+        for i in range(0, 8, 2):
+            st, r, e = dec.decode_syndromes(sx[i:i + 2], sz[i:i + 2], 0.045, opts)
+            assert st["slots"] == 1   # the single-trial path ran
+            recs.append(r)
+            ests.append(e)
+        return np.concatenate(ests), np.concatenate(recs)
     return dec.simulate(106, 1024, 0.045, opts, first_trial=3)
 
 
-@pytest.mark.parametrize("name", ["slots_fp64_pp", "resident_fp32_learned", "table_fp32"])
+@pytest.mark.parametrize("name", ["slots_fp64_pp", "resident_fp32_learned", "table_fp32", "single_fp64_syndromes"])
 def test_every_allocation_failure_is_reported_and_recovered(name):
     """The k-th allocation of creating a context and running it fails, for every k until the
     path completes: each failure comes back as JBP_ERR_CUDA "out of memory" (never a crash or a
