@@ -477,14 +477,16 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
 
 // The single-trial path takes FP64 decodes of up to kSingleMaxTrials given syndromes with plain
 // undamped BP and no profile, run budget, frozen sides or per-trial error rate -- the calls of
-// the drop-in's cuda_bp_decode -- unless the slot engine is asked for by name.
-constexpr long long kSingleMaxTrials = 3;
+// the drop-in's cuda_bp_decode -- unless the slot engine is asked for by name.  The iteration
+// limit keeps a launch's barrier count within the 31 bits of its barrier word.
+constexpr int kSingleMaxIter = 1000000;
 
 bool Engine::single_applies(const RunRequest &rq) const {
     const jbp_options &o = rq.opt;
     return coop_launch_ && o.engine == JBP_ENGINE_AUTO && o.precision == JBP_PREC_FP64 && !o.enable_pp && o.damping <= 0.0 &&
            !o.freeze_syn && !o.profile && o.watchdog_ms <= 0 && !(o.p_max > rq.p) && rq.source == kSrcSyndromes &&
-           rq.ntrials >= 1 && rq.ntrials <= kSingleMaxTrials && !rq.d_llr_out && !rq.collect;
+           rq.ntrials >= 1 && rq.ntrials <= kSingleMaxTrials && o.max_iter <= kSingleMaxIter && !rq.d_llr_out &&
+           !rq.collect;
 }
 
 std::string Engine::run_single(const RunRequest &rq, jbp_stats &stats) {
@@ -528,9 +530,10 @@ std::string Engine::run_single(const RunRequest &rq, jbp_stats &stats) {
         sr.c2v[s] = static_cast<double2 *>(single_msg_[s]);
         sr.v2c[s] = static_cast<double2 *>(single_msg_[2 + s]);
     }
-    sr.bar = reinterpret_cast<unsigned *>(single_ctl_);
-    sr.bad = single_ctl_ + 2;
-    sr.err = single_ctl_ + 4;
+    static_assert(sizeof(unsigned long long) * kSingleMaxTrials <= sizeof(int) * kSingleErrWord &&
+                      kSingleErrWord < 8,
+                  "barrier words, then the error flag, within the eight control words");
+    sr.err = single_ctl_ + kSingleErrWord;
     sr.cnt = single_cnt_;
     sr.hist = rq.d_hist;
     sr.res_out = rq.d_res_out;
@@ -548,6 +551,7 @@ std::string Engine::run_single(const RunRequest &rq, jbp_stats &stats) {
         sr.sz = rq.d_sz + t * mz;
         sr.est = rq.d_est_out ? rq.d_est_out + t * n : single_est_;
         sr.local = t;
+        sr.bar = reinterpret_cast<unsigned long long *>(single_ctl_) + t;   // zeroed above, one per launch
         void *args[] = {&sr};
         ce = cudaLaunchCooperativeKernel(reinterpret_cast<void *>(ks.single64), kSingleBlocks, kSingleThreads, args, 0,
                                          st);
@@ -569,7 +573,8 @@ std::string Engine::run_single(const RunRequest &rq, jbp_stats &stats) {
     DevCounters hc;
     std::memcpy(ctl, single_host_, sizeof(ctl));
     std::memcpy(&hc, single_host_ + kSingleCntOffset, sizeof(hc));
-    if (ctl[4]) return "single-trial run: a grid barrier waited longer than its limit (internal error)";
+    if (ctl[kSingleErrWord])
+        return "single-trial run: a grid barrier waited longer than its limit (internal error)";
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, run_ev_[0], run_ev_[1]);
     fill_stats(hc, stats);

@@ -287,10 +287,12 @@ __global__ void __launch_bounds__(256, 3) k_check_f64(DevCode code, DevRun run, 
     }
 }
 
+// sign: OR-ed into the bits of the undamped message's first value (0, or the sign bit carrying a
+// decision bit: probabilities are never negative, so the magnitude stays exact)
 template <bool DAMP>
 __device__ __forceinline__ void store_v2c_f64(double2 *v2c, double2 *v2c_hi, size_t idx, int side, double n0,
                                               double n1, double n2, double n3, bool fresh, const double *pr,
-                                              double damping) {
+                                              double damping, unsigned long long sign = 0ull) {
     if (DAMP) {
         if (damping > 0.0) {
             double o0, o1, o2, o3;
@@ -309,7 +311,9 @@ __device__ __forceinline__ void store_v2c_f64(double2 *v2c, double2 *v2c_hi, siz
         v2c[idx] = make_double2(n0, n1);
         v2c_hi[idx] = make_double2(n2, n3);
     } else {
-        v2c[idx] = side == 0 ? make_double2(dadd(n0, n2), dadd(n1, n3)) : make_double2(dadd(n0, n1), dadd(n2, n3));
+        double2 m = side == 0 ? make_double2(dadd(n0, n2), dadd(n1, n3)) : make_double2(dadd(n0, n1), dadd(n2, n3));
+        if (sign) m.x = __longlong_as_double(static_cast<long long>(static_cast<unsigned long long>(__double_as_longlong(m.x)) | sign));
+        v2c[idx] = m;
     }
 }
 
@@ -320,8 +324,10 @@ __device__ __forceinline__ void store_v2c_f64(double2 *v2c, double2 *v2c_hi, siz
 // (0..3, the first maximum of the normalized total).  FAST: every normalization through
 // norm4_fast, one basic block for the whole update (the seven normalizations' dependency chains
 // interleave); ok is cleared when an operand left the fast domain, and the caller then redoes
-// the update with FAST = false (norm4), which rewrites the same outputs.
-template <int DV, bool DAMP, bool FAST>
+// the update with FAST = false (norm4), which rewrites the same outputs.  SIGN (undamped only):
+// each X message carries the decision's x bit in the sign of its first value, each Z message
+// the z bit, for a check phase that tests the syndrome from the messages it reads.
+template <int DV, bool DAMP, bool FAST, bool SIGN = false>
 __device__ __forceinline__ int var_f64_update(const DevRun &run, const DevMsgs &msg, double damping, int slot, int frz,
                                               const size_t *ox, const size_t *oz, const bool *vx, const bool *vz,
                                               const double *ax, const double *bx, const double *az,
@@ -383,7 +389,8 @@ __device__ __forceinline__ int var_f64_update(const DevRun &run, const DevMsgs &
         double n2 = dmul(dmul(p2, EA), ZB), n3 = dmul(dmul(p3, EB), ZB);
         if (FAST) norm4_fast(n0, n1, n2, n3, ok);
         else norm4(n0, n1, n2, n3);
-        store_v2c_f64<DAMP>(v2cx, v2cx_hi, ox[k], 0, n0, n1, n2, n3, fresh, pr, damping);
+        store_v2c_f64<DAMP>(v2cx, v2cx_hi, ox[k], 0, n0, n1, n2, n3, fresh, pr, damping,
+                            SIGN ? static_cast<unsigned long long>(best & 1) << 63 : 0ull);
     }
 #pragma unroll
     for (int k = 0; k < DV; ++k) {
@@ -394,7 +401,8 @@ __device__ __forceinline__ int var_f64_update(const DevRun &run, const DevMsgs &
         double n2 = dmul(dmul(p2, XA), FB), n3 = dmul(dmul(p3, XB), FB);
         if (FAST) norm4_fast(n0, n1, n2, n3, ok);
         else norm4(n0, n1, n2, n3);
-        store_v2c_f64<DAMP>(v2cz, v2cz_hi, oz[k], 1, n0, n1, n2, n3, fresh, pr, damping);
+        store_v2c_f64<DAMP>(v2cz, v2cz_hi, oz[k], 1, n0, n1, n2, n3, fresh, pr, damping,
+                            SIGN ? static_cast<unsigned long long>((best >> 1) & 1) << 63 : 0ull);
     }
     return best;
 }
