@@ -1,8 +1,10 @@
 // One FP64 trial per launch, for calls that decode one or a few trials -- the drop-in's
 // cuda_bp_decode decodes one trial per call (jointbp_cuda.cu:681-1104).  A cooperative launch of
-// a few dozen blocks runs the whole BP loop of the trial: the check phase with one thread per
-// check row, the variable phase with one thread per variable and the syndrome test, separated by
-// a grid barrier, instead of the slot engine's per-iteration kernels over warps of 32 slots of
+// small blocks, about one per SM, runs the whole BP loop of the trial: the check phase with one
+// thread per check row, the variable phase with one thread per variable and the syndrome test,
+// separated by a grid barrier (the phases are bound by the latency of each thread's FP64 chain,
+// 23 cycles per dependent operation, so spreading them over the SMs shortens nothing but the
+// wait for issue slots), instead of the slot engine's per-iteration kernels over warps of 32 slots of
 // which one would be busy.  The arithmetic is the slot engine's FP64 path (check_f64_row,
 // var_f64_update), so decisions and iteration counts are the same bit for bit.  Messages stay in
 // L2, position-major ([side][pos][check]) so that a warp's check rows read and write them
@@ -16,8 +18,8 @@
 
 namespace jbp {
 
-constexpr int kSingleThreads = 256;
-constexpr int kSingleBlocks = 36;
+constexpr int kSingleThreads = 64;
+constexpr int kSingleBlocks = 144;   // about one block per SM: the phases are latency-bound per thread
 constexpr int kSingleMaxTrials = 3;      // trials (launches) of one run, each with its own barrier word
 constexpr int kSingleErrWord = 6;        // int index of the error flag among the control words
 constexpr unsigned long long kGridBarrierWaitNs = 1000000000ull;   // a barrier gives up after 1 s
