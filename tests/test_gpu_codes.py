@@ -173,3 +173,33 @@ def test_cli_mixed_launch_equals_the_api(tmp_path):
     for line, s in zip(lines, st):
         d = dict(re.findall(r"(\w+)=(\S+)", line))
         assert (int(d["trials"]), int(d["failures"]), int(d["iters"])) == (s["trials"], s["failures"], s["total_iters"])
+
+
+@pytest.mark.parametrize("n_classical", [32, 96])
+def test_single_trial_path_on_hgp_codes(n_classical):
+    """FP64 calls of one and two syndromes (the single-trial cooperative launch) on hypergraph
+    products -- checks of weight 7, variables of degree 3 and 4 padded to 4; at classical n = 96
+    the code has 14,400 qubits, more than the launch's threads, so threads take a second
+    variable and second check rows -- decode as the slot engine does: estimates, iteration
+    counts and outcomes."""
+    from dataclasses import replace
+    from joint_bp_plus_pp_b200 import Decoder, Options
+    n, xo, xv, zo, zv = hgp_code(n_classical, 1)
+    dec = Decoder.from_checks(n, xo, xv, zo, zv)
+    p, k = 0.06, 12
+    err = dec.sample_errors(21, 1, k, p)
+    syn = []
+    for side in (0, 1):
+        off, var = dec.checks(side)
+        bits = (err >> side) & 1
+        syn.append((bits[:, var].reshape(k, -1, int(off[1] - off[0])).sum(axis=2) % 2).astype(np.uint8))
+    base = Options(precision="fp64", max_iter=60, enable_pp=False)
+    _, r_ref, e_ref = dec.decode_syndromes(syn[0], syn[1], p, replace(base, engine="slots"))
+    for step in (1, 2):
+        for i in range(0, k, step):
+            st, r, e = dec.decode_syndromes(syn[0][i:i + step], syn[1][i:i + step], p, base)
+            assert st["slots"] == 1   # the single-trial path ran
+            assert (e == e_ref[i:i + step]).all(), (step, i)
+            for f in ("iterations", "syndrome_ok"):
+                assert (r[f] == r_ref[i:i + step][f]).all(), (f, step, i)
+    dec.close()
