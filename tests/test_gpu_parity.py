@@ -333,3 +333,24 @@ def test_single_trial_path_short_runs(decoder, oracle, max_iter, warmup, interva
         assert (e[0] == e_ref[i]).all(), i
         for f in ("iterations", "syndrome_ok", "success"):
             assert r[f][0] == r_ref[f][i], (f, i)
+
+
+def test_staged_small_calls_on_other_engines(decoder, oracle):
+    """Calls of one to three syndromes stage their inputs through pinned memory; when the run
+    does not take the single-trial path (the slot engine by name, FP32 messages, damping) the
+    results come back by the ordinary copies and equal those of one batched call."""
+    from dataclasses import replace
+    from joint_bp_plus_pp_b200 import Options
+    p = 0.05
+    err = decoder.sample_errors(55, 1, 9, p)
+    sx = np.stack([oracle.syndrome(e)[0] for e in err])
+    sz = np.stack([oracle.syndrome(e)[1] for e in err])
+    for o in (Options(precision="fp64", engine="slots", max_iter=100, enable_pp=False),
+              Options(precision="fp32", max_iter=100, enable_pp=False),
+              Options(precision="fp64", max_iter=100, enable_pp=False, damping=0.25)):
+        _, r_all, e_all = decoder.decode_syndromes(sx, sz, p, o)
+        for k in (1, 3):
+            for i in range(0, 9, k):
+                st, r, e = decoder.decode_syndromes(sx[i:i + k], sz[i:i + k], p, o)
+                assert (e == e_all[i:i + k]).all(), (o, k, i)
+                assert (r["iterations"] == r_all[i:i + k]["iterations"]).all(), (o, k, i)
