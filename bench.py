@@ -313,21 +313,26 @@ def reference_gpu_leg(args):
     """Informative: the reference's own GPU path (cuda_bp_decode, jointbp_cuda.cu:681-1104, one
     trial at a time, built unmodified for sm_100a in FP64 and in its FP32 form) against this
     repository's drop-in for the same boundary (the unmodified reference CLI built with -DUSE_CUDA
-    and linked to lib/libjointbp_cuda.so), on the same command: --simulate --p 0.04 --max-iter 1000
+    and linked to lib/libjointbp_cuda.so; FP64, and FP32 LLR messages through
+    JBP_CUDA_PRECISION=fp32), on the same command: --simulate --p 0.04 --max-iter 1000
     --no-pp --cuda [--cuda-graph], the reference's mt19937_64 trials.  Rates are the CLI's own
     Run Summary (trials / elapsed_s, host sampling included); failures and iterations come from
     the same summary."""
     out = {}
-    runs = [("reference_cuda_fp64", REF_CUDA["fp64"], []), ("reference_cuda_fp64_graph", REF_CUDA["fp64"], ["--cuda-graph"]),
-            ("reference_cuda_fp32", REF_CUDA["fp32"], []), ("reference_cuda_fp32_graph", REF_CUDA["fp32"], ["--cuda-graph"]),
-            ("dropin_fp64", DROPIN_BIN, [])]
-    for name, binary, extra in runs:
+    runs = [("reference_cuda_fp64", REF_CUDA["fp64"], [], None),
+            ("reference_cuda_fp64_graph", REF_CUDA["fp64"], ["--cuda-graph"], None),
+            ("reference_cuda_fp32", REF_CUDA["fp32"], [], None),
+            ("reference_cuda_fp32_graph", REF_CUDA["fp32"], ["--cuda-graph"], None),
+            ("dropin_fp64", DROPIN_BIN, [], None),
+            ("dropin_fp32", DROPIN_BIN, [], {"JBP_CUDA_PRECISION": "fp32"})]
+    for name, binary, extra, env in runs:
         if not binary.exists():
             out[name] = None
             continue
         cmd = [str(binary), "--params", str(PARAMS), "--simulate", "--p", "0.04", "--trials", str(args.ref_gpu_trials),
                "--max-iter", "1000", "--no-pp", "--cuda", "--seed", str(args.seed), "--report-every", "0"] + extra
-        r = subprocess.run(cmd, capture_output=True, text=True, cwd=str(PARAMS.parent), timeout=600)
+        r = subprocess.run(cmd, capture_output=True, text=True, cwd=str(PARAMS.parent), timeout=600,
+                           env=dict(os.environ, **env) if env else None)
         m = re.search(r"trials=(\d+) failures=(\d+).*?iters=(\d+).*?elapsed_s=([0-9.]+)s", r.stdout)
         if r.returncode != 0 or not m or "falling back" in r.stderr:
             out[name] = {"error": (r.stderr or r.stdout)[-300:]}

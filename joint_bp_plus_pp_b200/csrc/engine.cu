@@ -85,7 +85,7 @@ struct KernelSet {
     CheckFn check = nullptr;
     VarF64Fn var64 = nullptr;
     VarLlrFn varllr = nullptr;
-    SingleFn single64 = nullptr;   // one FP64 trial per cooperative launch
+    SingleFn single = nullptr;   // one trial per cooperative launch (FP64, FP32)
 };
 
 template <int DC, int DV>
@@ -94,10 +94,11 @@ KernelSet kernels_for(int precision, bool damp) {
     if (precision == JBP_PREC_FP64) {
         k.check = damp ? k_check_f64<DC, true> : k_check_f64<DC, false>;
         k.var64 = damp ? k_var_f64<DC, DV, true> : k_var_f64<DC, DV, false>;
-        k.single64 = k_single_f64<DC, DV>;
+        k.single = k_single_f64<DC, DV>;
     } else if (precision == JBP_PREC_FP32) {
         k.check = k_check_llr<float, DC>;
         k.varllr = damp ? k_var_llr<float, DC, DV, true> : k_var_llr<float, DC, DV, false>;
+        k.single = k_single_llr<DC, DV>;
     } else {
         k.check = k_check_llr<__half, DC>;
         k.varllr = damp ? k_var_llr<__half, DC, DV, true> : k_var_llr<__half, DC, DV, false>;
@@ -475,7 +476,7 @@ std::string Engine::run_resident(const RunRequest &rq, jbp_stats &stats) {
     return "";
 }
 
-// The single-trial path takes FP64 decodes of up to kSingleMaxTrials given syndromes with plain
+// The single-trial path takes FP64 and FP32 decodes of up to kSingleMaxTrials given syndromes with plain
 // undamped BP and no profile, run budget, frozen sides or per-trial error rate -- the calls of
 // the drop-in's cuda_bp_decode -- unless the slot engine is asked for by name.  The iteration
 // limit keeps a launch's barrier count within the 31 bits of its barrier word.
@@ -483,7 +484,8 @@ constexpr int kSingleMaxIter = 1000000;
 
 bool Engine::single_applies(const RunRequest &rq) const {
     const jbp_options &o = rq.opt;
-    return coop_launch_ && o.engine == JBP_ENGINE_AUTO && o.precision == JBP_PREC_FP64 && !o.enable_pp && o.damping <= 0.0 &&
+    return coop_launch_ && o.engine == JBP_ENGINE_AUTO && (o.precision == JBP_PREC_FP64 || o.precision == JBP_PREC_FP32) &&
+           !o.enable_pp && o.damping <= 0.0 &&
            !o.freeze_syn && !o.profile && o.watchdog_ms <= 0 && !(o.p_max > rq.p) && rq.source == kSrcSyndromes &&
            rq.ntrials >= 1 && rq.ntrials <= kSingleMaxTrials && o.max_iter <= kSingleMaxIter && !rq.d_llr_out &&
            !rq.collect;
@@ -493,7 +495,7 @@ std::string Engine::run_single(const RunRequest &rq, jbp_stats &stats) {
     const jbp_options &o = rq.opt;
     const SideGraph &gx = model_.side[0], &gz = model_.side[1];
     KernelSet ks;
-    if (!select_kernels(gx.dc_max, gx.dv_max, JBP_PREC_FP64, false, ks) || !ks.single64)
+    if (!select_kernels(gx.dc_max, gx.dv_max, o.precision, false, ks) || !ks.single)
         return "no single-trial kernel for this code";
     const int n = model_.n;
     for (int s = 0; s < 2; ++s) {
@@ -553,7 +555,7 @@ std::string Engine::run_single(const RunRequest &rq, jbp_stats &stats) {
         sr.local = t;
         sr.bar = reinterpret_cast<unsigned long long *>(single_ctl_) + t;   // zeroed above, one per launch
         void *args[] = {&sr};
-        ce = cudaLaunchCooperativeKernel(reinterpret_cast<void *>(ks.single64), kSingleBlocks, kSingleThreads, args, 0,
+        ce = cudaLaunchCooperativeKernel(reinterpret_cast<void *>(ks.single), kSingleBlocks, kSingleThreads, args, 0,
                                          st);
     }
     if (ce == cudaSuccess) ce = cudaEventRecord(run_ev_[1], st);
@@ -788,7 +790,7 @@ std::string Engine::run_dispatch(const RunRequest &rq, jbp_stats &stats) {
         return "no GPU kernel built for check degree " + std::to_string(gx.dc_max) + " / variable degree " +
                std::to_string(gx.dv_max);
     JBP_CUDA_TRY(cudaSetDevice(device_), "cudaSetDevice");
-    if (ks.single64 && single_applies(rq)) return run_single(rq, stats);
+    if (ks.single && single_applies(rq)) return run_single(rq, stats);
     const int S = choose_slots(o, rq.ntrials);
     const int H = std::max(0, o.flip_hist);
     const int R = pp ? std::max(H + 1, 3) : 1;

@@ -493,6 +493,44 @@ __device__ __forceinline__ float lse2(float a, float b) {
 
 __device__ __forceinline__ float clamp_llr(float x) { return fminf(fmaxf(x, -kLlrInMax), kLlrInMax); }
 
+// The LLR check rule on one check of DC edges: from the edges' variable-to-check inputs in(i)
+// (base-2 LLRs) and the check's target syndrome bit, out(i, c2v of edge i).  Stable tanh rule
+// (PN, Q = prod D - prod N) over u = 2^-|y|, N = 1 - u, D = 1 + u: the output
+// log2((2 PN + Q) / Q) keeps its precision when the product of the other edges' tanh is close
+// to 1 (see kernels_resident.cuh).
+template <int DC, class In, class Out>
+__device__ __forceinline__ void llr_check_row(In in, unsigned sbit, Out out) {
+    float u[DC];
+    unsigned sgn = sbit << 31;
+#pragma unroll
+    for (int i = 0; i < DC; ++i) {
+        const float y = in(i);
+        const unsigned sy = __float_as_uint(y) & 0x80000000u;
+        sgn ^= sy;
+        u[i] = __uint_as_float(__float_as_uint(ex2_approx(-fminf(fabsf(y), kLlrInMax))) | sy);
+    }
+    float sPN[DC + 1], sQ[DC + 1];
+    sPN[DC] = 1.0f;
+    sQ[DC] = 0.0f;
+#pragma unroll
+    for (int i = DC - 1; i >= 0; --i) {
+        const float au = fabsf(u[i]);
+        sQ[i] = fmaf(1.0f + au, sQ[i + 1], sPN[i + 1] * (au + au));
+        sPN[i] = (1.0f - au) * sPN[i + 1];
+    }
+    float pPN = 1.0f, pQ = 0.0f;
+#pragma unroll
+    for (int i = 0; i < DC; ++i) {
+        const float ePN = pPN * sPN[i + 1];
+        const float eQ = fmaf(pPN + pQ, sQ[i + 1], sPN[i + 1] * pQ);
+        const float mag = fminf(lg2_approx(fmaf(2.0f, ePN, eQ) * rcp_approx(eQ)), kLlrMax);
+        out(i, __uint_as_float(__float_as_uint(mag) ^ ((sgn ^ __float_as_uint(u[i])) & 0x80000000u)));
+        const float au = fabsf(u[i]);
+        pQ = fmaf(pPN + pQ, au + au, (1.0f - au) * pQ);
+        pPN *= 1.0f - au;
+    }
+}
+
 template <typename T, int DC>
 __global__ void __launch_bounds__(256) k_check_llr(DevCode code, DevRun run, DevMsgs msg) {
     const int lane = threadIdx.x & 31;
@@ -524,43 +562,39 @@ __global__ void __launch_bounds__(256) k_check_llr(DevCode code, DevRun run, Dev
             continue;
         }
         const float lp = run.lprior[8 * slot + 4 + side];
-        // stable tanh rule (PN, Q = prod D - prod N) over u = 2^-|y|, N = 1 - u, D = 1 + u:
-        // the output log2((2 PN + Q) / Q) keeps its precision when the product of the other
-        // edges' tanh is close to 1 (see kernels_resident.cuh)
-        float u[DC];
-        unsigned sgn = ((run.synm[static_cast<size_t>(row) * G + group] >> lane) & 1u) << 31;
-#pragma unroll
-        for (int i = 0; i < DC; ++i) {
-            const float y = fresh ? lp : ld_msg<T>(v2c + i * kGroup);
-            const unsigned sy = __float_as_uint(y) & 0x80000000u;
-            sgn ^= sy;
-            u[i] = __uint_as_float(__float_as_uint(ex2_approx(-fminf(fabsf(y), kLlrInMax))) | sy);
-        }
-        float sPN[DC + 1], sQ[DC + 1];
-        sPN[DC] = 1.0f;
-        sQ[DC] = 0.0f;
-#pragma unroll
-        for (int i = DC - 1; i >= 0; --i) {
-            const float au = fabsf(u[i]);
-            sQ[i] = fmaf(1.0f + au, sQ[i + 1], sPN[i + 1] * (au + au));
-            sPN[i] = (1.0f - au) * sPN[i + 1];
-        }
-        float pPN = 1.0f, pQ = 0.0f;
-#pragma unroll
-        for (int i = 0; i < DC; ++i) {
-            const float ePN = pPN * sPN[i + 1];
-            const float eQ = fmaf(pPN + pQ, sQ[i + 1], sPN[i + 1] * pQ);
-            const float mag = fminf(lg2_approx(fmaf(2.0f, ePN, eQ) * rcp_approx(eQ)), kLlrMax);
-            st_msg<T>(c2v + i * kGroup,
-                      __uint_as_float(__float_as_uint(mag) ^ ((sgn ^ __float_as_uint(u[i])) & 0x80000000u)));
-            const float au = fabsf(u[i]);
-            pQ = fmaf(pPN + pQ, au + au, (1.0f - au) * pQ);
-            pPN *= 1.0f - au;
-        }
+        const unsigned sbit = (run.synm[static_cast<size_t>(row) * G + group] >> lane) & 1u;
+        llr_check_row<DC>([&](int i) { return fresh ? lp : ld_msg<T>(v2c + i * kGroup); }, sbit,
+                          [&](int i, float y) { st_msg<T>(c2v + i * kGroup, y); });
     }
 }
 
 __device__ __forceinline__ float sigm2(float y) { return rcp_approx(1.0f + ex2_approx(-y)); }
+
+// The LLR variable rule of one variable from its incoming c2v (lx of the X edges, lz of the Z
+// edges; 0 for a padded edge) and its log prior weights lp (I, X, Z, Y): the hard decision
+// (first maximum, returned) and the undamped extrinsic outputs with the 4-ary coupling of the
+// two sides.
+template <int DV>
+__device__ __forceinline__ int var_llr_core(const float *lx, const float *lz, float4 lp, float *outx, float *outz) {
+    float Lam = 0.0f, Mu = 0.0f;
+#pragma unroll
+    for (int k = 0; k < DV; ++k) { Lam += lx[k]; Mu += lz[k]; }
+    // log2 weights of I, X, Z, Y up to a common constant; first maximum wins
+    const float w0 = lp.x, w1 = lp.y - Lam, w2 = lp.z - Mu, w3 = lp.w - Lam - Mu;
+    int best = 0;
+    float bv = w0;
+    if (w1 > bv) { best = 1; bv = w1; }
+    if (w2 > bv) { best = 2; bv = w2; }
+    if (w3 > bv) { best = 3; }
+    const float Gx = lse2(lp.x, lp.z - Mu) - lse2(lp.y, lp.w - Mu);   // x-bit coupling through Z
+    const float Hz = lse2(lp.x, lp.y - Lam) - lse2(lp.z, lp.w - Lam); // z-bit coupling through X
+#pragma unroll
+    for (int k = 0; k < DV; ++k) {
+        outx[k] = clamp_llr(Lam - lx[k] + Gx);
+        outz[k] = clamp_llr(Mu - lz[k] + Hz);
+    }
+    return best;
+}
 
 // One variable of the LLR variable update: sums of the incoming X and Z messages, hard
 // decision, and the extrinsic outputs with the 4-ary coupling of the two sides.
@@ -589,24 +623,14 @@ __device__ __forceinline__ int var_llr_one(const DevCode &code, const DevRun &ru
         lx[k] = vx[k] ? ld_msg<T>(c2vx + ox[k]) : 0.0f;
         lz[k] = vz[k] ? ld_msg<T>(c2vz + oz[k]) : 0.0f;
     }
-    float Lam = 0.0f, Mu = 0.0f;
-#pragma unroll
-    for (int k = 0; k < DV; ++k) { Lam += lx[k]; Mu += lz[k]; }
     const float4 lp = *reinterpret_cast<const float4 *>(run.lprior + 8 * slot);
-    // log2 weights of I, X, Z, Y up to a common constant; first maximum wins
-    const float w0 = lp.x, w1 = lp.y - Lam, w2 = lp.z - Mu, w3 = lp.w - Lam - Mu;
-    int best = 0;
-    float bv = w0;
-    if (w1 > bv) { best = 1; bv = w1; }
-    if (w2 > bv) { best = 2; bv = w2; }
-    if (w3 > bv) { best = 3; }
-    const float Gx = lse2(lp.x, lp.z - Mu) - lse2(lp.y, lp.w - Mu);   // x-bit coupling through Z
-    const float Hz = lse2(lp.x, lp.y - Lam) - lse2(lp.z, lp.w - Lam); // z-bit coupling through X
+    float outx[DV], outz[DV];
+    const int best = var_llr_core<DV>(lx, lz, lp, outx, outz);
     const int frz = run.freeze_syn ? run.frz[slot] : 0;
 #pragma unroll
     for (int k = 0; k < DV; ++k) {
-        float ox_v = clamp_llr(Lam - lx[k] + Gx);
-        float oz_v = clamp_llr(Mu - lz[k] + Hz);
+        float ox_v = outx[k];
+        float oz_v = outz[k];
         if (DAMP) {
             // scaled_mix on the binary marginal: q0 = (1-d) q0_new + d q0_old
             const bool fresh = run.iter[slot] == 0;

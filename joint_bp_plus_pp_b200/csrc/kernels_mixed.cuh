@@ -89,7 +89,10 @@ __device__ __forceinline__ bool mix_check_row(const uint16_t *__restrict__ chk, 
     unsigned par = 0u;
     res_row_rule<DC>(
         [&](int i) {
-            const float a = A[kPre ? vv[i] : __ldg(chk + static_cast<size_t>(i) * m + c)];
+            int v;
+            if constexpr (kPre) v = vv[i];
+            else v = __ldg(chk + static_cast<size_t>(i) * m + c);
+            const float a = A[v];
             par ^= __float_as_uint(a);
             return a - ST::ld(c2v + static_cast<size_t>(i) * m + c);
         },

@@ -1,4 +1,5 @@
-// One FP64 trial per launch, for calls that decode one or a few trials -- the drop-in's
+// One trial per launch (FP64, and the FP32 LLR form at the end of this file), for calls that
+// decode one or a few trials -- the drop-in's
 // cuda_bp_decode decodes one trial per call (jointbp_cuda.cu:681-1104).  A cooperative launch of
 // small blocks, about one per SM, runs the whole BP loop of the trial: the check phase with one
 // thread per check row, the variable phase with one thread per variable and the syndrome test,
@@ -30,7 +31,7 @@ struct SingleRun {
     const uint8_t *sx, *sz;         // target syndrome bits, one byte per check (bit 0)
     double prior[4];                // normalized prior of the trial
     int max_iter, check_warmup, check_interval;
-    double2 *c2v[2], *v2c[2];       // [side][pos * m_side + check]
+    double2 *c2v[2], *v2c[2];       // [side][pos * m_side + check] (k_single_llr: float / uint2 entries)
     uint8_t *est;                   // [n] decisions (0..3): the caller's output buffer
     // this launch's barrier word, zero at launch: arrivals in bits 0-30, the error bit 31, and in
     // bits 32-63 the number of (block, test) pairs in which the block found a failing check
@@ -209,6 +210,114 @@ __global__ void __launch_bounds__(kSingleThreads, 1) k_single_f64(const __grid_c
 #pragma unroll
                 for (int i = 0; i < DC; ++i) par ^= static_cast<unsigned long long>(__double_as_longlong(v2c[static_cast<size_t>(i) * ms].x));
                 lbad |= static_cast<int>(par >> 63) != ((side ? run.sz : run.sx)[ch] & 1);
+            }
+            if (!grid_sync(run.bar, run.err, lbad, true, target, flags_seen, any_bad)) return;
+            if (!any_bad) {
+                ok = true;
+                iters = run.max_iter;
+            }
+        }
+    }
+    if (tid == 0)
+        account_trial(run.cnt, run.hist, run.res_out, run.max_iter, run.local, iters,
+                      ok ? (kResSyndromeOk | kResBpOk) : 0, ok, ok, false, false);
+}
+
+// The FP32 form: the slot engine's LLR arithmetic (llr_check_row, var_llr_core, the log prior of
+// llr_prior_entry) on FP32 messages, so that decisions and iteration counts equal those of the
+// slot engine's FP32 decoder.  The run's message arrays hold, position-major, FP32 c2v and v2c
+// pairs (message bits, the variable's decision bit of that side): an LLR's sign is its own, so
+// the decision bit travels beside it, in the same 8-byte store.
+template <int DC, int DV>
+__global__ void __launch_bounds__(kSingleThreads, 1) k_single_llr(const __grid_constant__ SingleRun run) {
+    const DevCode &code = run.code;
+    const int mx = code.s[0].m, mz = code.s[1].m, M = mx + mz, n = code.n;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthreads = gridDim.x * blockDim.x;
+    float *const c2vx = reinterpret_cast<float *>(run.c2v[0]), *const c2vz = reinterpret_cast<float *>(run.c2v[1]);
+    uint2 *const v2cx = reinterpret_cast<uint2 *>(run.v2c[0]), *const v2cz = reinterpret_cast<uint2 *>(run.v2c[1]);
+    __shared__ float lp_sh[6];
+    if (threadIdx.x < 6) lp_sh[threadIdx.x] = llr_prior_entry(threadIdx.x, run.prior[0], run.prior[1], run.prior[2], run.prior[3]);
+    __syncthreads();
+    const float4 lp = make_float4(lp_sh[0], lp_sh[1], lp_sh[2], lp_sh[3]);
+    const float lpx = lp_sh[4], lpz = lp_sh[5];
+    size_t var_ox[DV], var_oz[DV];
+    bool var_vx[DV], var_vz[DV];
+    auto edges_of = [&](int v, size_t *ox, size_t *oz, bool *vx, bool *vz) {
+#pragma unroll
+        for (int k = 0; k < DV; ++k) {
+            const int ex = __ldg(code.s[0].var_edge + v * DV + k), ez = __ldg(code.s[1].var_edge + v * DV + k);
+            vx[k] = ex >= 0;
+            vz[k] = ez >= 0;
+            ox[k] = vx[k] ? single_msg_off<DC>(ex, mx) : 0;
+            oz[k] = vz[k] ? single_msg_off<DC>(ez, mz) : 0;
+        }
+    };
+    if (tid < n) edges_of(tid, var_ox, var_oz, var_vx, var_vz);
+    unsigned target = 0, flags_seen = 0;
+    bool any_bad = false;
+    int iters = run.max_iter;
+    bool ok = false;
+    auto due = [&](int k1) {
+        return k1 >= run.max_iter || (k1 > run.check_warmup && (k1 - run.check_warmup) % run.check_interval == 0);
+    };
+    for (int it = 0; it < run.max_iter; ++it) {
+        const bool test_now = it >= 1 && due(it);
+        int bad = 0;
+        for (int row = tid; row < M; row += nthreads) {
+            const int side = row >= mx, ch = side ? row - mx : row, ms = side ? mz : mx;
+            const unsigned s = (side ? run.sz : run.sx)[ch] & 1;
+            const uint2 *in = (side ? v2cz : v2cx) + ch;
+            float *out = (side ? c2vz : c2vx) + ch;
+            const float lp_in = side ? lpz : lpx;
+            unsigned par = 0;
+            llr_check_row<DC>(
+                [&](int i) -> float {
+                    if (it == 0) return lp_in;
+                    const uint2 q = in[static_cast<size_t>(i) * ms];
+                    par ^= q.y;
+                    return __uint_as_float(q.x);
+                },
+                s, [&](int i, float y) { out[static_cast<size_t>(i) * ms] = y; });
+            if (test_now) bad |= par != s;
+        }
+        if (!grid_sync(run.bar, run.err, bad, test_now, target, flags_seen, any_bad)) return;
+        if (test_now && !any_bad) {
+            ok = true;
+            iters = it;
+            break;
+        }
+        for (int v = tid; v < n; v += nthreads) {
+            size_t ox[DV], oz[DV];
+            bool vx[DV], vz[DV];
+            if (v == tid) {
+#pragma unroll
+                for (int k = 0; k < DV; ++k) { ox[k] = var_ox[k]; oz[k] = var_oz[k]; vx[k] = var_vx[k]; vz[k] = var_vz[k]; }
+            } else {
+                edges_of(v, ox, oz, vx, vz);
+            }
+            float lx[DV], lz[DV], outx[DV], outz[DV];
+#pragma unroll
+            for (int k = 0; k < DV; ++k) {
+                lx[k] = vx[k] ? c2vx[ox[k]] : 0.0f;
+                lz[k] = vz[k] ? c2vz[oz[k]] : 0.0f;
+            }
+            const int best = var_llr_core<DV>(lx, lz, lp, outx, outz);
+#pragma unroll
+            for (int k = 0; k < DV; ++k) {
+                if (vx[k]) v2cx[ox[k]] = make_uint2(__float_as_uint(outx[k]), static_cast<unsigned>(best & 1));
+                if (vz[k]) v2cz[oz[k]] = make_uint2(__float_as_uint(outz[k]), static_cast<unsigned>(best >> 1));
+            }
+            run.est[v] = static_cast<uint8_t>(best);
+        }
+        if (!grid_sync(run.bar, run.err, 0, false, target, flags_seen, any_bad)) return;
+        if (it + 1 == run.max_iter) {
+            int lbad = 0;
+            for (int row = tid; row < M; row += nthreads) {
+                const int side = row >= mx, ch = side ? row - mx : row, ms = side ? mz : mx;
+                unsigned par = 0;
+#pragma unroll
+                for (int i = 0; i < DC; ++i) par ^= (side ? v2cz : v2cx)[static_cast<size_t>(i) * ms + ch].y;
+                lbad |= par != static_cast<unsigned>((side ? run.sz : run.sx)[ch] & 1);
             }
             if (!grid_sync(run.bar, run.err, lbad, true, target, flags_seen, any_bad)) return;
             if (!any_bad) {

@@ -480,6 +480,20 @@ static __global__ void k_classify(DevCode code, DevRun run) {
 }
 
 // Hands the next trials of the source to the retired (or never used) slots.
+// Entry i (0..5) of the LLR prior of a normalized prior (p0..p3 of I, X, Z, Y): the base-2 log
+// weights (0..3) and the base-2 prior LLRs of the x bit (4) and the z bit (5) that seed the
+// fresh v2c messages of the LLR decoders.
+__device__ __forceinline__ float llr_prior_entry(int i, double p0, double p1, double p2, double p3) {
+    switch (i) {
+    case 0: return static_cast<float>(log2(p0));
+    case 1: return static_cast<float>(log2(p1));
+    case 2: return static_cast<float>(log2(p2));
+    case 3: return static_cast<float>(log2(p3));
+    case 4: return static_cast<float>(log2((p0 + p2) / (p1 + p3)));
+    default: return static_cast<float>(log2((p0 + p1) / (p2 + p3)));
+    }
+}
+
 static __global__ void k_refill(DevRun run, int precision) {
     const int nret = *run.n_retired;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nret; r += gridDim.x * blockDim.x) {
@@ -513,12 +527,7 @@ static __global__ void k_refill(DevRun run, int precision) {
             } else {
                 // base-2 log prior and the prior LLRs (base 2) that seed fresh v2c messages
                 float *lp = run.lprior + 8 * slot;
-                lp[0] = static_cast<float>(log2(p0));
-                lp[1] = static_cast<float>(log2(p1));
-                lp[2] = static_cast<float>(log2(p2));
-                lp[3] = static_cast<float>(log2(p3));
-                lp[4] = static_cast<float>(log2((p0 + p2) / (p1 + p3)));   // x-bit
-                lp[5] = static_cast<float>(log2((p0 + p1) / (p2 + p3)));   // z-bit
+                for (int i = 0; i < 6; ++i) lp[i] = llr_prior_entry(i, p0, p1, p2, p3);
                 lp[6] = lp[7] = 0.0f;
             }
             run.fresh[atomicAdd(run.n_fresh, 1)] = slot;

@@ -175,9 +175,10 @@ def test_cli_mixed_launch_equals_the_api(tmp_path):
         assert (int(d["trials"]), int(d["failures"]), int(d["iters"])) == (s["trials"], s["failures"], s["total_iters"])
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("n_classical", [32, 96])
-def test_single_trial_path_on_hgp_codes(n_classical):
-    """FP64 calls of one and two syndromes (the single-trial cooperative launch) on hypergraph
+def test_single_trial_path_on_hgp_codes(n_classical, precision):
+    """FP64 and FP32 calls of one and two syndromes (the single-trial cooperative launch) on hypergraph
     products -- checks of weight 7, variables of degree 3 and 4 padded to 4; at classical n = 96
     the code has 14,400 qubits, more than the launch's threads, so threads take a second
     variable and second check rows -- decode as the slot engine does: estimates, iteration
@@ -193,7 +194,7 @@ def test_single_trial_path_on_hgp_codes(n_classical):
         off, var = dec.checks(side)
         bits = (err >> side) & 1
         syn.append((bits[:, var].reshape(k, -1, int(off[1] - off[0])).sum(axis=2) % 2).astype(np.uint8))
-    base = Options(precision="fp64", max_iter=60, enable_pp=False)
+    base = Options(precision=precision, max_iter=60, enable_pp=False)
     _, r_ref, e_ref = dec.decode_syndromes(syn[0], syn[1], p, replace(base, engine="slots"))
     for step in (1, 2):
         for i in range(0, k, step):

@@ -337,8 +337,9 @@ def test_single_trial_path_short_runs(decoder, oracle, max_iter, warmup, interva
 
 def test_staged_small_calls_on_other_engines(decoder, oracle):
     """Calls of one to three syndromes stage their inputs through pinned memory; when the run
-    does not take the single-trial path (the slot engine by name, FP32 messages, damping) the
-    results come back by the ordinary copies and equal those of one batched call."""
+    does not take the single-trial path (the slot engine by name, FP16 messages on the resident
+    engine, damping) the results come back by the ordinary copies and equal those of one
+    batched call."""
     from dataclasses import replace
     from joint_bp_plus_pp_b200 import Options
     p = 0.05
@@ -346,7 +347,7 @@ def test_staged_small_calls_on_other_engines(decoder, oracle):
     sx = np.stack([oracle.syndrome(e)[0] for e in err])
     sz = np.stack([oracle.syndrome(e)[1] for e in err])
     for o in (Options(precision="fp64", engine="slots", max_iter=100, enable_pp=False),
-              Options(precision="fp32", max_iter=100, enable_pp=False),
+              Options(precision="fp16", max_iter=100, enable_pp=False),
               Options(precision="fp64", max_iter=100, enable_pp=False, damping=0.25)):
         _, r_all, e_all = decoder.decode_syndromes(sx, sz, p, o)
         for k in (1, 3):
@@ -354,3 +355,27 @@ def test_staged_small_calls_on_other_engines(decoder, oracle):
                 st, r, e = decoder.decode_syndromes(sx[i:i + k], sz[i:i + k], p, o)
                 assert (e == e_all[i:i + k]).all(), (o, k, i)
                 assert (r["iterations"] == r_all[i:i + k]["iterations"]).all(), (o, k, i)
+
+
+@pytest.mark.parametrize("warmup,interval", [(0, 1), (3, 2)])
+def test_single_trial_fp32_equals_slot_engine(decoder, oracle, warmup, interval):
+    """FP32 decodes of one to three syndromes take the single-trial path too (the drop-in's
+    cuda_bp_decode with JBP_CUDA_PRECISION=fp32): the slot engine's LLR arithmetic in one
+    cooperative launch per trial, so decisions, iteration counts and outcomes equal the slot
+    engine's FP32 decoder on the same 48 syndromes."""
+    from dataclasses import replace
+    from joint_bp_plus_pp_b200 import Options
+    p = 0.05
+    err = decoder.sample_errors(78, 1, 48, p)
+    sx = np.stack([oracle.syndrome(e)[0] for e in err])
+    sz = np.stack([oracle.syndrome(e)[1] for e in err])
+    base = Options(precision="fp32", max_iter=200, enable_pp=False, check_warmup=warmup, check_interval=interval)
+    _, r_ref, e_ref = decoder.decode_syndromes(sx, sz, p, replace(base, engine="slots"))
+    assert 0 < int(r_ref["syndrome_ok"].sum())
+    for k in (1, 2, 3):
+        for i in range(0, 48, k):
+            st, r, e = decoder.decode_syndromes(sx[i:i + k], sz[i:i + k], p, base)
+            assert st["kernel_launches"] == len(r) and st["slots"] == 1   # the single-trial path ran
+            assert (e == e_ref[i:i + k]).all(), (k, i)
+            for f in ("iterations", "syndrome_ok", "success"):
+                assert (r[f] == r_ref[i:i + k][f]).all(), (f, k, i)
