@@ -175,7 +175,10 @@ int jbp_decode_errors(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, c
                       uint8_t *est_out, jbp_trial_result *res, jbp_stats *stats);
 
 /* Decode syndromes (host buffers): sx is ntrials x mx bits (one byte each), sz ntrials x mz.
- * success/exact/stab fields stay 0 (no true error). */
+ * success/exact/stab fields stay 0 (no true error).  Calls of at most three trials (the
+ * drop-in's cuda_bp_decode decodes one) copy their inputs through pinned memory the context
+ * keeps; FP64 and FP32 ones without post-processing, damping, frozen sides, profile or run
+ * budget decode each trial in one cooperative launch and wait once for the whole call. */
 int jbp_decode_syndromes(jbp_ctx *ctx, const jbp_options *opt, long long ntrials, const uint8_t *sx,
                          const uint8_t *sz, double p, uint8_t *est_out, jbp_trial_result *res, jbp_stats *stats);
 
