@@ -491,6 +491,19 @@ bool Engine::single_applies(const RunRequest &rq) const {
            !rq.collect;
 }
 
+// Whether every block of a single-trial launch can be resident at once on this device (a
+// cooperative launch needs it; a partition with few SMs decodes on the slot engine instead).
+bool Engine::single_fits(const void *fn) {
+    for (const auto &f : single_fit_)
+        if (f.first == fn) return f.second;
+    int per_sm = 0;
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSingleThreads, 0);
+    if (e != cudaSuccess) cudaGetLastError();   // the query's own error: the slot engine then decodes
+    const bool fits = e == cudaSuccess && static_cast<long long>(per_sm) * sm_count_ >= kSingleBlocks;
+    single_fit_.emplace_back(fn, fits);
+    return fits;
+}
+
 std::string Engine::run_single(const RunRequest &rq, jbp_stats &stats) {
     const jbp_options &o = rq.opt;
     const SideGraph &gx = model_.side[0], &gz = model_.side[1];
@@ -790,7 +803,8 @@ std::string Engine::run_dispatch(const RunRequest &rq, jbp_stats &stats) {
         return "no GPU kernel built for check degree " + std::to_string(gx.dc_max) + " / variable degree " +
                std::to_string(gx.dv_max);
     JBP_CUDA_TRY(cudaSetDevice(device_), "cudaSetDevice");
-    if (ks.single && single_applies(rq)) return run_single(rq, stats);
+    if (ks.single && single_applies(rq) && single_fits(reinterpret_cast<const void *>(ks.single)))
+        return run_single(rq, stats);
     const int S = choose_slots(o, rq.ntrials);
     const int H = std::max(0, o.flip_hist);
     const int R = pp ? std::max(H + 1, 3) : 1;

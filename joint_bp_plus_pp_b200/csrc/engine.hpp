@@ -123,6 +123,8 @@ private:
     std::string run_dispatch(const RunRequest &rq, jbp_stats &stats);
     // one or a few FP64 trials, each in one cooperative launch (kernels_single.cuh)
     bool single_applies(const RunRequest &rq) const;
+    bool single_fits(const void *fn);
+    std::vector<std::pair<const void *, bool>> single_fit_;   // per kernel: all blocks co-resident
     static constexpr size_t kSingleCntOffset = 64;   // single_cnt_ within the control allocation
     std::string run_single(const RunRequest &rq, jbp_stats &stats);
     static std::string run_mixed_impl(const MixedRequest &rq, std::vector<jbp_stats> &stats);
