@@ -379,3 +379,10 @@ def test_single_trial_fp32_equals_slot_engine(decoder, oracle, warmup, interval)
             assert (e == e_ref[i:i + k]).all(), (k, i)
             for f in ("iterations", "syndrome_ok", "success"):
                 assert (r[f] == r_ref[i:i + k][f]).all(), (f, k, i)
+    # a caller's explicit prior (the drop-in passes one with every call)
+    q = (1 - p, p / 3, p / 3, p / 3)
+    s = ((q[0] + q[1]) + q[2]) + q[3]
+    pri = replace(base, prior=tuple(x / s for x in q))
+    st, r1, e1 = decoder.decode_syndromes(sx[:2], sz[:2], 0.2, pri)
+    _, r2, e2 = decoder.decode_syndromes(sx[:2], sz[:2], 0.2, replace(pri, engine="slots"))
+    assert st["slots"] == 1 and (e1 == e2).all() and (r1["iterations"] == r2["iterations"]).all()
